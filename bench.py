@@ -1,0 +1,453 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the B200 column-radiation path: all-sky LW + SW forward.
+
+Metric: columns/s (one column = gas optics + cloud optics + solver + broadband reduction +
+heating rates for LW 256 and SW 224 g-points over nlay layers), FP32, synthetic seeded
+atmospheres and tables with the reference schema (the real RRTMGP tables are not available).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--path staged|fused] [--ncol C] [--nlay L]
+
+One process per GPU (torchrun for N > 1); columns are sharded across ranks with no exchange
+(weak scaling: every rank owns ncol columns).  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+sys.path[:0] = [str(REPO), str(REPO / "rte-rrtmgp-cpp_b200")]
+
+import numpy as np  # noqa: E402
+
+METRIC = "columns/s (all-sky LW+SW, 1 B200) plain FP64 vs FP32+adjoint at stated W/m2 err"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--path", default="staged", choices=["staged", "fused"])
+    ap.add_argument("--ncol", type=int, default=8192)
+    ap.add_argument("--nlay", type=int, default=128)
+    ap.add_argument("--seed", type=int, default=42)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def measured_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        lines = Path(self.file.name).read_text().strip().splitlines()
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def bytes_per_column(nlay, glw=256, gsw=224, nb_lw=16, nb_sw=14, B=4):
+    """Algorithmic HBM bytes per column of each staged kernel (inputs read once, outputs
+    written once; k-tables are L2 resident and counted zero)."""
+    L, V = nlay, nlay + 1
+    return {
+        "gas_optics_lw": ((6 * L + 3) + 4 * L * glw + 2 * glw) * B,
+        "gas_optics_sw": ((4 * L + 1) + 3 * L * gsw) * B,
+        "lw_solver": (4 * L * glw + glw + nb_lw + 2 * V * glw) * B,
+        "sw_solver": (3 * L * gsw + 1 + gsw + 2 * nb_sw + 3 * V * gsw) * B,
+        "broadband_lw": (2 * V * glw + 3 * V) * B,
+        "broadband_sw": (3 * V * gsw + 4 * V) * B,
+        "cloud_lw": (4 * L + L * nb_lw) * B,
+        "cloud_sw": (4 * L + 3 * L * nb_sw) * B,
+        "add_to_lw": (2 * L * glw + L * nb_lw) * B,
+        "add_to_sw": (6 * L * gsw + 3 * L * nb_sw) * B,
+        "delta_sw": (6 * L * nb_sw) * B,
+        "heating": (4 * V + L) * B * 2,
+    }
+
+
+def ncu_traffic():
+    """dram bytes per column of each kernel from the committed ncu summary, if any."""
+    p = REPO / "profiles" / "ncu_traffic.txt"
+    out = {}
+    if p.exists():
+        for ln in p.read_text().splitlines():
+            parts = ln.split()
+            if len(parts) >= 2 and not ln.startswith("#"):
+                try:
+                    out[parts[0]] = float(parts[1])
+                except ValueError:
+                    pass
+    return out
+
+
+def cpu_baseline(args, tables, seconds):
+    """The oracle (FP64 C++ port of the reference path) on the host cores."""
+    from oracle import oracle as O
+    from rrtmgp_b200 import synthetic as S
+    ncores = os.cpu_count() or 1
+    O.set_threads(ncores)
+    klw = O.GasOptics(tables["lw"], S.ATM_GASES)
+    ksw = O.GasOptics(tables["sw"], S.ATM_GASES)
+    clw = O.CloudOptics(tables["cloud_lw"])
+    csw = O.CloudOptics(tables["cloud_sw"])
+
+    def run(nc):
+        atm = S.make_atmosphere(nc, args.nlay, seed=args.seed, clouds=True)
+        t0 = time.perf_counter()
+        O.forward_lw(klw, clw, atm)
+        O.forward_sw(ksw, csw, atm)
+        return time.perf_counter() - t0
+
+    probe = 64
+    dt = run(probe)
+    nc = int(min(args.ncol, max(probe, probe * seconds / max(dt, 1e-6) / 2)))
+    reps, tot = 0, 0.0
+    while tot < seconds * 0.5 or reps < 1:
+        tot += run(nc)
+        reps += 1
+    return {"value": reps * nc / tot, "unit": "columns/s", "cores": ncores, "kind": "port",
+            "sample": f"{reps} x {nc} columns of the {args.nlay}-layer all-sky LW+SW forward, FP64, "
+                      f"OpenMP over columns"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from rrtmgp_b200 import synthetic as S
+    tables = {"lw": S.make_kdist("lw"), "sw": S.make_kdist("sw"),
+              "cloud_lw": S.make_cloud_luts("lw"), "cloud_sw": S.make_cloud_luts("sw")}
+    from oracle import oracle as O
+    ncores = os.cpu_count() or 1
+    O.set_threads(ncores)
+    klw = O.GasOptics(tables["lw"], S.ATM_GASES)
+    ksw = O.GasOptics(tables["sw"], S.ATM_GASES)
+    clw = O.CloudOptics(tables["cloud_lw"])
+    csw = O.CloudOptics(tables["cloud_sw"])
+    # Bounded sample per step so that warmup + steps finish within a few minutes.
+    nc = min(args.ncol, 512)
+    atm = S.make_atmosphere(nc, args.nlay, seed=args.seed, clouds=True)
+    for _ in range(args.warmup):
+        O.forward_lw(klw, clw, atm)
+        O.forward_sw(ksw, csw, atm)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.forward_lw(klw, clw, atm)
+        O.forward_sw(ksw, csw, atm)
+    dt = (time.perf_counter() - t0) / args.steps
+    value = nc / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "columns/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"all-sky LW+SW forward, ncol={args.ncol}, nlay={args.nlay}", "ncol": args.ncol,
+                   "nlay": args.nlay, "sample_ncol_per_step": nc},
+        "cpu_baseline": {"value": value, "unit": "columns/s", "cores": ncores, "kind": "port",
+                         "sample": f"{nc} columns per step of the {args.nlay}-layer all-sky LW+SW forward "
+                                   f"(FP64 C++ restatement of the reference path; the reference's own CPU "
+                                   f"build needs the absent rte-rrtmgp Fortran, gfortran, netCDF and Boost)"},
+        "e2e": {"value": value, "unit": "columns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    from rrtmgp_b200 import synthetic as S
+    from rrtmgp_b200.solver import Radiation_solver, atm_to_device
+
+    tables = {"lw": S.make_kdist("lw"), "sw": S.make_kdist("sw"),
+              "cloud_lw": S.make_cloud_luts("lw"), "cloud_sw": S.make_cloud_luts("sw")}
+    atm_np = S.make_atmosphere(args.ncol, args.nlay, seed=args.seed + rank, clouds=True)
+    solver = Radiation_solver(tables["lw"], tables["sw"], tables["cloud_lw"], tables["cloud_sw"], S.ATM_GASES)
+    atm = atm_to_device(atm_np, torch.float32, dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+
+    stages = {}
+
+    def evpair():
+        return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def step(timed_events=None):
+        if timed_events is None:
+            solver.solve_lw(atm)
+            solver.solve_sw(atm)
+            return
+        a, b = timed_events
+        a.record(stream)
+        solver.solve_lw(atm)
+        solver.solve_sw(atm)
+        b.record(stream)
+
+    # Per-stage timing pass (same kernels, events around each stage) for the roofline.
+    def staged_breakdown(reps):
+        import ctypes as C
+        from rrtmgp_b200 import _abi, api
+        lib = _abi.load()
+        res = {}
+        b_lw = solver._buffers((args.ncol, args.nlay, torch.float32), atm["play"], args.ncol, args.nlay, "lw")
+        ncol, nlay = args.ncol, args.nlay
+        P = api._ptr
+        s = api._stream()
+        arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay)
+
+        def t_gas_lw():
+            lib.rrtmgp_b200_gas_optics_lw_f32(solver.klw.handle, ncol, nlay, P(atm["play"]), P(atm["plev"]),
+                                              P(atm["tlay"]), P(atm["tsfc"]), P(atm["tlev"]), None, arr,
+                                              len(atm["gases"]), P(b_lw["tau"]), P(b_lw["lay_src"]),
+                                              P(b_lw["lev_src_inc"]), P(b_lw["lev_src_dec"]), P(b_lw["sfc_src"]),
+                                              P(b_lw["sfc_src_jac"]), s)
+
+        def t_lw_solver():
+            lib.rrtmgp_b200_rte_lw_f32(solver.klw.bands.handle, ncol, nlay, 1, P(b_lw["tau"]), P(b_lw["lay_src"]),
+                                       P(b_lw["lev_src_inc"]), P(b_lw["lev_src_dec"]), P(b_lw["sfc_src"]),
+                                       P(atm["emis_sfc"]), None, 1, P(b_lw["gpt_up"]), P(b_lw["gpt_dn"]), s)
+
+        b_sw = solver._buffers((args.ncol, args.nlay, torch.float32), atm["play"], args.ncol, args.nlay, "sw")
+
+        def t_gas_sw():
+            lib.rrtmgp_b200_gas_optics_sw_f32(solver.ksw.handle, ncol, nlay, P(atm["play"]), P(atm["plev"]),
+                                              P(atm["tlay"]), None, arr, len(atm["gases"]), P(b_sw["tau"]),
+                                              P(b_sw["ssa"]), P(b_sw["g"]), P(b_sw["toa_src"]), s)
+
+        def t_sw_solver():
+            lib.rrtmgp_b200_rte_sw_f32(solver.ksw.bands.handle, ncol, nlay, 1, P(b_sw["tau"]), P(b_sw["ssa"]),
+                                       P(b_sw["g"]), P(atm["mu0"]), P(b_sw["toa_src"]), P(atm["sfc_alb_dir"]),
+                                       P(atm["sfc_alb_dif"]), None, P(b_sw["gpt_up"]), P(b_sw["gpt_dn"]),
+                                       P(b_sw["gpt_dir"]), C.c_void_p(b_sw["ws"].data_ptr()),
+                                       C.c_size_t(b_sw["ws"].numel()), s)
+
+        def t_bb_lw():
+            lib.rrtmgp_b200_fluxes_broadband_f32(ncol, nlay + 1, 256, P(b_lw["gpt_up"]), P(b_lw["gpt_dn"]), None,
+                                                 P(b_lw["flux_up"]), P(b_lw["flux_dn"]), None, P(b_lw["flux_net"]), s)
+
+        for name, fn in (("gas_optics_lw", t_gas_lw), ("lw_solver", t_lw_solver), ("gas_optics_sw", t_gas_sw),
+                         ("sw_solver", t_sw_solver), ("broadband_lw", t_bb_lw)):
+            ms = []
+            for _ in range(reps):
+                flush.zero_()
+                e0, e1 = evpair()
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            res[name] = float(np.mean(ms))
+        return res
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    evs = [evpair() for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()          # L2 flush between timed steps (outside the events)
+        step(evs[i])
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = float(np.sum(step_ms))
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * args.ncol * args.steps / (total_ms * 1e-3)
+
+    # Per-kernel durations and roofline of the dominant kernel.
+    breakdown = staged_breakdown(3)
+    bpc = bytes_per_column(args.nlay)
+    dom = max(breakdown, key=breakdown.get)
+    peak, peak_kind = measured_peaks()
+    achieved = bpc[dom] * args.ncol / (breakdown[dom] * 1e-3) / 1e9
+    traffic = ncu_traffic()
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": traffic[dom] * args.ncol if dom in traffic else None,
+                "algorithmic_bytes": bpc[dom] * args.ncol,
+                "kernel_ms": {k: round(v, 4) for k, v in breakdown.items()}}
+
+    # End to end through the public API with host buffers (pinned), copies in the timed region.
+    in_keys = ["play", "plev", "tlay", "tlev", "tsfc", "lwp", "iwp", "rel", "rei", "mu0", "emis_sfc",
+               "sfc_alb_dir", "sfc_alb_dif"]
+    host_in = {k: atm[k].cpu().pin_memory() for k in in_keys}
+    host_gas = {k: v.cpu().pin_memory() for k, v in atm["gases"].items()}
+    out_lw = solver.solve_lw(atm)
+    out_sw = solver.solve_sw(atm)
+    host_out = {("lw", k): v.cpu().pin_memory() for k, v in out_lw.items()}
+    host_out.update({("sw", k): v.cpu().pin_memory() for k, v in out_sw.items()})
+    h2d = sum(v.numel() * v.element_size() for v in host_in.values()) + \
+        sum(v.numel() * v.element_size() for v in host_gas.values())
+    d2h = sum(v.numel() * v.element_size() for v in host_out.values())
+
+    def e2e_step():
+        for k in in_keys:
+            atm[k].copy_(host_in[k], non_blocking=True)
+        for k in host_gas:
+            atm["gases"][k].copy_(host_gas[k], non_blocking=True)
+        o1 = solver.solve_lw(atm)
+        o2 = solver.solve_sw(atm)
+        for k, v in o1.items():
+            host_out[("lw", k)].copy_(v, non_blocking=True)
+        for k, v in o2.items():
+            host_out[("sw", k)].copy_(v, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ee = [evpair() for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        ee[i][0].record(stream)
+        e2e_step()
+        ee[i][1].record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = float(np.sum([a.elapsed_time(b) for a, b in ee]))
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.ncol * args.steps / (float(t.item()) * 1e-3)
+
+    # Plain FP64 GPU forward of the same build (the denominator of the FP32 target).
+    fp64 = None
+    if not args.no_fp64:
+        atm64 = atm_to_device(atm_np, torch.float64, dev)
+        solver.solve_lw(atm64)
+        solver.solve_sw(atm64)
+        torch.cuda.synchronize()
+        nrep = max(2, args.steps // 3)
+        e64 = [evpair() for _ in range(nrep)]
+        for i in range(nrep):
+            flush.zero_()
+            e64[i][0].record(stream)
+            solver.solve_lw(atm64)
+            solver.solve_sw(atm64)
+            e64[i][1].record(stream)
+        torch.cuda.synchronize()
+        ms64 = float(np.mean([a.elapsed_time(b) for a, b in e64]))
+        fp64 = {"value": args.ncol / (ms64 * 1e-3), "unit": "columns/s", "ms_per_step": ms64}
+        del atm64
+        solver._bufs = {k: v for k, v in solver._bufs.items() if k[0][2] != torch.float64}
+
+    launches_per_step = 6 + 8  # LW: gas, cloud, add_to, rte, reduce, heating; SW: + spread, delta
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args, tables, args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "columns/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"all-sky LW+SW forward (gas+cloud optics, rte_lw, rte_sw, broadband fluxes, "
+                                   f"heating rates), ncol={args.ncol} per GPU, nlay={args.nlay}, 256 LW / 224 SW "
+                                   f"g-points, synthetic tables",
+                       "ncol": args.ncol, "nlay": args.nlay, "path": args.path,
+                       "l2": "flushed between timed steps (256 MiB write outside the events)",
+                       "parallelism": f"columns sharded over {world} GPU(s), no exchange"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "columns/s", "h2d_bytes_per_step": h2d * world,
+                    "d2h_bytes_per_step": d2h * world},
+            "gpu_launches": launches_per_step * args.steps,
+            "fp64_forward": fp64,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

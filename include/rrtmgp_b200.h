@@ -1,0 +1,330 @@
+/*
+ * rrtmgp_b200.h -- C ABI of the B200 column-radiation hot path (RTE+RRTMGP).
+ *
+ * Plain C: opaque handles, plain pointers and sizes, an int status return, a cudaStream_t
+ * passed as void*.  Every array argument of a compute entry point is a DEVICE pointer in
+ * the reference's layout: Fortran order with the column index fastest, i.e. the flat
+ * memory of the reference's Array_gpu<Float,N> (include/Array.h:41-63 of rte-rrtmgp-cpp):
+ *
+ *   (ncol, nlay)        p_lay, t_lay, col_dry, vmr fields, lwp, iwp, re_liq, re_ice
+ *   (ncol, nlev)        p_lev, t_lev, broadband fluxes
+ *   (ncol, nlay, ngpt)  tau, ssa, g, Planck sources      (ngpt may be nband for clouds)
+ *   (ncol, nlev, ngpt)  g-point fluxes
+ *   (ncol, ngpt)        surface sources, toa_src, incident fluxes
+ *   (nband, ncol)       sfc_emis, sfc_alb_dir, sfc_alb_dif (band fastest, as the reference)
+ *
+ * Entry points come in _f32 (the product arithmetic) and _f64 (same kernels instantiated in
+ * double: the "plain FP64 GPU forward" baseline) variants.  Nothing here allocates device
+ * memory inside a compute call: tables live in handles created once, temporaries come from
+ * a caller-supplied workspace whose size a *_workspace_bytes() query returns.  No call
+ * synchronises the stream; errors in arguments are reported synchronously by the status
+ * code and rrtmgp_b200_last_error().
+ *
+ * Each declaration names the reference interface it replaces (file:line in rte-rrtmgp-cpp).
+ */
+#ifndef RRTMGP_B200_H
+#define RRTMGP_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RRTMGP_B200_ABI_VERSION 1
+
+enum rrtmgp_b200_status {
+    RRTMGP_B200_OK = 0,
+    RRTMGP_B200_ERR_ARG = 1,          /* null pointer, bad shape, bad enum             */
+    RRTMGP_B200_ERR_RANGE = 2,        /* input outside the table range (range check)   */
+    RRTMGP_B200_ERR_MISSING_GAS = 3,  /* key species or h2o absent                     */
+    RRTMGP_B200_ERR_CUDA = 4,         /* CUDA runtime error (launch / copy)            */
+    RRTMGP_B200_ERR_ALLOC = 5,        /* allocation failed at handle creation          */
+    RRTMGP_B200_ERR_UNSUPPORTED = 6,  /* option not supported                          */
+    RRTMGP_B200_ERR_WORKSPACE = 7     /* caller workspace missing or too small         */
+};
+
+/* Message of the last failing call on this host thread ("" if none). */
+const char* rrtmgp_b200_last_error(void);
+int rrtmgp_b200_abi_version(void);
+
+/* ------------------------------------------------------------------------------------ */
+/* Coefficient tables, as read from an RRTMGP k-distribution netCDF file.                */
+/* Replaces the 35-argument constructors Gas_optics_rrtmgp_gpu::Gas_optics_rrtmgp_gpu    */
+/* (include/Gas_optics_rrtmgp.h:293-364) fed by load_and_init_gas_optics                 */
+/* (src_test/Radiation_solver.cpp:70-284).  Host pointers, double, C order = netCDF     */
+/* dimension order (the memory the reference's Array<Float,N> holds after reading).      */
+/* ------------------------------------------------------------------------------------ */
+typedef struct rrtmgp_b200_kdist_tables {
+    int ngas;                /* absorber                                                 */
+    int nband, ngpt;         /* bnd, gpt                                                 */
+    int ntemp, npres, neta;  /* temperature, pressure, mixing_fraction                  */
+    int nminor_absorber;     /* minor_absorber                                           */
+    int nint_lower, nint_upper;           /* minor_absorber_intervals_lower/upper        */
+    int ncontrib_lower, ncontrib_upper;   /* contributors_lower/upper                    */
+    int nplanck_temp;        /* temperature_Planck (0 for a shortwave file)              */
+
+    const char* const* gas_names;          /* [ngas]                                     */
+    const int* key_species;                /* (nband, 2 atmos_layer, 2 pair), 1-based    */
+    const int* band_lims_gpt;              /* (nband, 2), 1-based inclusive              */
+    const double* band_lims_wvn;           /* (nband, 2)                                 */
+    const double* press_ref;               /* [npres], Pa, decreasing                    */
+    double press_ref_trop;
+    const double* temp_ref;                /* [ntemp], K, increasing                     */
+    double temp_ref_p, temp_ref_t;
+    const double* vmr_ref;                 /* (ntemp, ngas+1, 2); index 0 = dry air      */
+    const double* kmajor;                  /* (ntemp, npres+1, neta, ngpt)               */
+    const double* kminor_lower;            /* (ntemp, neta, ncontrib_lower)              */
+    const double* kminor_upper;            /* (ntemp, neta, ncontrib_upper)              */
+    const char* const* gas_minor;          /* [nminor_absorber]                          */
+    const char* const* identifier_minor;   /* [nminor_absorber]                          */
+    const char* const* minor_gases_lower;  /* [nint_lower]                               */
+    const char* const* minor_gases_upper;  /* [nint_upper]                               */
+    const int* minor_limits_gpt_lower;     /* (nint_lower, 2), 1-based                   */
+    const int* minor_limits_gpt_upper;     /* (nint_upper, 2)                            */
+    const int* minor_scales_with_density_lower;  /* [nint_lower] 0/1                     */
+    const int* minor_scales_with_density_upper;
+    const char* const* scaling_gas_lower;  /* [nint_lower] ("" = none)                   */
+    const char* const* scaling_gas_upper;
+    const int* scale_by_complement_lower;  /* [nint_lower] 0/1                           */
+    const int* scale_by_complement_upper;
+    const int* kminor_start_lower;         /* [nint_lower], 1-based                      */
+    const int* kminor_start_upper;
+    /* longwave only (NULL for shortwave) */
+    const double* totplnk;                 /* (nband, nplanck_temp)                      */
+    const double* planck_frac;             /* (ntemp, npres+1, neta, ngpt)               */
+    /* shortwave only (NULL for longwave) */
+    const double* solar_source_quiet;      /* [ngpt]                                     */
+    const double* solar_source_facular;    /* [ngpt]                                     */
+    const double* solar_source_sunspot;    /* [ngpt]                                     */
+    double tsi_default, mg_default, sb_default;
+    const double* rayl_lower;              /* (ntemp, neta, ngpt) or NULL                */
+    const double* rayl_upper;              /* (ntemp, neta, ngpt) or NULL                */
+} rrtmgp_b200_kdist_tables;
+
+typedef struct rrtmgp_b200_kdist_t* rrtmgp_b200_kdist;
+typedef struct rrtmgp_b200_cloud_t* rrtmgp_b200_cloud;
+typedef struct rrtmgp_b200_bands_t* rrtmgp_b200_bands;
+
+/* Gas_optics_rrtmgp_gpu ctor + init_abs_coeffs (src/Gas_optics_rrtmgp.cpp:391-742,
+ * src_cuda/Gas_optics_rrtmgp.cu:427-803): keeps the gases also listed in available_gases,
+ * drops absent minor absorbers, builds flavors/gpoint_flavor, re-lays the tables out
+ * g-point fastest in FP32 and FP64 on the current device.  Errors: MISSING_GAS when a key
+ * species is not available ("Gas optics: required gas X is missing", :241-243). */
+int rrtmgp_b200_kdist_create(const rrtmgp_b200_kdist_tables* tables,
+                             const char* const* available_gases, int n_available,
+                             rrtmgp_b200_kdist* out);
+void rrtmgp_b200_kdist_destroy(rrtmgp_b200_kdist k);
+
+typedef struct rrtmgp_b200_kdist_info {
+    int ngas, nflav, nband, ngpt, ntemp, npres, neta, nplanck_temp;
+    int nminor_lower, nminor_upper;        /* after reduction                            */
+    int is_longwave;                        /* source_is_internal()                       */
+    int has_rayleigh;
+    double press_ref_min, press_ref_max;   /* get_press_ref_min/max (Gas_optics_rrtmgp.h) */
+    double temp_ref_min, temp_ref_max;     /* get_temp_min/max                           */
+    double tsi;                             /* get_tsi() (Gas_optics_rrtmgp.cpp:1347-1356) */
+} rrtmgp_b200_kdist_info;
+int rrtmgp_b200_kdist_get_info(rrtmgp_b200_kdist k, rrtmgp_b200_kdist_info* info);
+/* Name of reduced gas i (0-based) into buf. */
+int rrtmgp_b200_kdist_gas_name(rrtmgp_b200_kdist k, int i, char* buf, int buflen);
+/* Band/g-point discretisation of the k-distribution (Optical_props_gpu base). */
+rrtmgp_b200_bands rrtmgp_b200_kdist_bands(rrtmgp_b200_kdist k);
+/* set_solar_variability (Gas_optics_rrtmgp.cpp:745-760); SW only. */
+int rrtmgp_b200_kdist_set_solar_variability(rrtmgp_b200_kdist k, double mg_index, double sb_index);
+/* Host copy of solar_source [ngpt] (double); SW only. */
+int rrtmgp_b200_kdist_solar_source(rrtmgp_b200_kdist k, double* out_host);
+
+/* Band / g-point discretisation: Optical_props_gpu(band_lims_wvn, band_lims_gpt)
+ * (include/Optical_props.h:176-211).  band_lims_gpt host (nband, 2), 1-based. */
+int rrtmgp_b200_bands_create(int nband, const int* band_lims_gpt_host, rrtmgp_b200_bands* out);
+void rrtmgp_b200_bands_destroy(rrtmgp_b200_bands b);
+int rrtmgp_b200_bands_get(rrtmgp_b200_bands b, int* nband, int* ngpt);
+
+/* Gas concentration entry: the reference's Gas_concs_gpu map name -> Array_gpu<Float,2>
+ * (include/Gas_concs.h:67-91).  dim1 x dim2 = 1x1 (scalar), 1 x nlay (profile) or
+ * ncol x nlay (field), column fastest; vmr is a device pointer of the call's precision. */
+typedef struct rrtmgp_b200_gas_conc {
+    const char* name;
+    const void* vmr;
+    int dim1, dim2;
+} rrtmgp_b200_gas_conc;
+
+/* ------------------------------------------------------------------------------------ */
+/* Gas optics                                                                            */
+/* ------------------------------------------------------------------------------------ */
+/* Gas_optics_rrtmgp_gpu::get_col_dry (src_cuda/Gas_optics_rrtmgp.cu:806-903). */
+int rrtmgp_b200_get_col_dry_f32(int ncol, int nlay, const float* vmr_h2o, const float* plev,
+                                float* col_dry, void* stream);
+int rrtmgp_b200_get_col_dry_f64(int ncol, int nlay, const double* vmr_h2o, const double* plev,
+                                double* col_dry, void* stream);
+
+/* Longwave gas_optics (include/Gas_optics_rrtmgp.h:389-398; src_cuda/Gas_optics_rrtmgp.cu
+ * :907-943 + compute_gas_taus :980-1148 + source :1167-1202).  col_dry may be NULL (then
+ * computed in-kernel from h2o and plev exactly as get_col_dry).  Outputs: tau, lay_src,
+ * lev_src_inc, lev_src_dec (ncol,nlay,ngpt); sfc_src, sfc_src_jac (ncol,ngpt). */
+int rrtmgp_b200_gas_optics_lw_f32(rrtmgp_b200_kdist k, int ncol, int nlay,
+        const float* play, const float* plev, const float* tlay, const float* tsfc,
+        const float* tlev, const float* col_dry,
+        const rrtmgp_b200_gas_conc* gases, int ngases,
+        float* tau, float* lay_src, float* lev_src_inc, float* lev_src_dec,
+        float* sfc_src, float* sfc_src_jac, void* stream);
+int rrtmgp_b200_gas_optics_lw_f64(rrtmgp_b200_kdist k, int ncol, int nlay,
+        const double* play, const double* plev, const double* tlay, const double* tsfc,
+        const double* tlev, const double* col_dry,
+        const rrtmgp_b200_gas_conc* gases, int ngases,
+        double* tau, double* lay_src, double* lev_src_inc, double* lev_src_dec,
+        double* sfc_src, double* sfc_src_jac, void* stream);
+
+/* Shortwave gas_optics (include/Gas_optics_rrtmgp.h:400-408; Gas_optics_rrtmgp.cu:947-977).
+ * Outputs tau, ssa, g (ncol,nlay,ngpt) and toa_src (ncol,ngpt) = solar_source spread. */
+int rrtmgp_b200_gas_optics_sw_f32(rrtmgp_b200_kdist k, int ncol, int nlay,
+        const float* play, const float* plev, const float* tlay, const float* col_dry,
+        const rrtmgp_b200_gas_conc* gases, int ngases,
+        float* tau, float* ssa, float* g, float* toa_src, void* stream);
+int rrtmgp_b200_gas_optics_sw_f64(rrtmgp_b200_kdist k, int ncol, int nlay,
+        const double* play, const double* plev, const double* tlay, const double* col_dry,
+        const rrtmgp_b200_gas_conc* gases, int ngases,
+        double* tau, double* ssa, double* g, double* toa_src, void* stream);
+
+/* Range check of Gas_optics_rrtmgp::gas_optics (src/Gas_optics_rrtmgp.cpp:812-827), which
+ * the reference GPU path skips.  tlev/tsfc may be NULL (shortwave).  Synchronises the
+ * stream; returns RRTMGP_B200_ERR_RANGE with the failing field named in last_error. */
+int rrtmgp_b200_check_range_f32(rrtmgp_b200_kdist k, int ncol, int nlay, const float* play,
+        const float* plev, const float* tlay, const float* tlev, const float* tsfc,
+        const float* col_dry, void* stream);
+int rrtmgp_b200_check_range_f64(rrtmgp_b200_kdist k, int ncol, int nlay, const double* play,
+        const double* plev, const double* tlay, const double* tlev, const double* tsfc,
+        const double* col_dry, void* stream);
+
+/* ------------------------------------------------------------------------------------ */
+/* Cloud optics: Cloud_optics_gpu (include/Cloud_optics.h:80-131; src_cuda/Cloud_optics.cu) */
+/* ------------------------------------------------------------------------------------ */
+typedef struct rrtmgp_b200_cloud_tables {
+    int nband, nsize_liq, nsize_ice, nrghice;
+    const double* band_lims_wvn;     /* (nband, 2)                                        */
+    double radliq_lwr, radliq_upr, radliq_fac;
+    double radice_lwr, radice_upr, radice_fac;
+    const double* lut_extliq;        /* (nband, nsize_liq)                                */
+    const double* lut_ssaliq;
+    const double* lut_asyliq;
+    const double* lut_extice;        /* (nrghice, nband, nsize_ice)                       */
+    const double* lut_ssaice;
+    const double* lut_asyice;
+} rrtmgp_b200_cloud_tables;
+
+/* Cloud_optics_gpu ctor (src_cuda/Cloud_optics.cu:130-179): ice roughness icergh = 2. */
+int rrtmgp_b200_cloud_create(const rrtmgp_b200_cloud_tables* t, rrtmgp_b200_cloud* out);
+void rrtmgp_b200_cloud_destroy(rrtmgp_b200_cloud c);
+
+/* cloud_optics 1scl (Cloud_optics.cu:257-329): tau (ncol,nlay,nband) = absorption tau. */
+int rrtmgp_b200_cloud_optics_1scl_f32(rrtmgp_b200_cloud c, int ncol, int nlay,
+        const float* clwp, const float* ciwp, const float* reliq, const float* reice,
+        float* tau, void* stream);
+int rrtmgp_b200_cloud_optics_1scl_f64(rrtmgp_b200_cloud c, int ncol, int nlay,
+        const double* clwp, const double* ciwp, const double* reliq, const double* reice,
+        double* tau, void* stream);
+/* cloud_optics 2str (Cloud_optics.cu:181-253): tau, ssa, g (ncol,nlay,nband). */
+int rrtmgp_b200_cloud_optics_2str_f32(rrtmgp_b200_cloud c, int ncol, int nlay,
+        const float* clwp, const float* ciwp, const float* reliq, const float* reice,
+        float* tau, float* ssa, float* g, void* stream);
+int rrtmgp_b200_cloud_optics_2str_f64(rrtmgp_b200_cloud c, int ncol, int nlay,
+        const double* clwp, const double* ciwp, const double* reliq, const double* reice,
+        double* tau, double* ssa, double* g, void* stream);
+
+/* ------------------------------------------------------------------------------------ */
+/* Optical-property arithmetic (src_cuda/Optical_props.cu:93-165)                        */
+/* ------------------------------------------------------------------------------------ */
+/* Optical_props_2str_gpu::delta_scale with f = g^2 (optical_props_kernels.cu:139-160). */
+int rrtmgp_b200_delta_scale_2str_f32(int ncol, int nlay, int ngpt, float* tau, float* ssa,
+                                     float* g, void* stream);
+int rrtmgp_b200_delta_scale_2str_f64(int ncol, int nlay, int ngpt, double* tau, double* ssa,
+                                     double* g, void* stream);
+/* add_to(Optical_props_1scl_gpu&, const Optical_props_1scl_gpu&) (Optical_props.cu:93-116):
+ * ngpt_in == ngpt adds g-point by g-point, ngpt_in == nband broadcasts by band through
+ * the bands' g-point limits; anything else is ERR_ARG (the reference's runtime_error). */
+int rrtmgp_b200_add_to_1scl_f32(rrtmgp_b200_bands b, int ncol, int nlay, float* tau_inout,
+                                const float* tau_in, int ngpt_in, void* stream);
+int rrtmgp_b200_add_to_1scl_f64(rrtmgp_b200_bands b, int ncol, int nlay, double* tau_inout,
+                                const double* tau_in, int ngpt_in, void* stream);
+/* add_to(Optical_props_2str_gpu&, const Optical_props_2str_gpu&) (Optical_props.cu:119-145). */
+int rrtmgp_b200_add_to_2str_f32(rrtmgp_b200_bands b, int ncol, int nlay,
+        float* tau_inout, float* ssa_inout, float* g_inout,
+        const float* tau_in, const float* ssa_in, const float* g_in, int ngpt_in, void* stream);
+int rrtmgp_b200_add_to_2str_f64(rrtmgp_b200_bands b, int ncol, int nlay,
+        double* tau_inout, double* ssa_inout, double* g_inout,
+        const double* tau_in, const double* ssa_in, const double* g_in, int ngpt_in, void* stream);
+
+/* ------------------------------------------------------------------------------------ */
+/* Solvers                                                                               */
+/* ------------------------------------------------------------------------------------ */
+/* Rte_lw_gpu::rte_lw (include/Rte_lw.h:65-73; src_cuda/Rte_lw.cu:81-152) with the
+ * no-scattering solver (rte_solver_kernels.cu:16-185; mo_rte_solver_kernels.F90:58-265).
+ * sfc_emis (nband, ncol); inc_flux (ncol, ngpt) or NULL (zero); n_gauss_angles 1..4
+ * (Gauss-Jacobi secants and weights of Rte_lw.cu:87-101; the reference GPU path supports
+ * only 1).  Outputs gpt_flux_up, gpt_flux_dn (ncol, nlay+1, ngpt). */
+int rrtmgp_b200_rte_lw_f32(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1,
+        const float* tau, const float* lay_src, const float* lev_src_inc,
+        const float* lev_src_dec, const float* sfc_src, const float* sfc_emis,
+        const float* inc_flux, int n_gauss_angles, float* gpt_flux_up, float* gpt_flux_dn,
+        void* stream);
+int rrtmgp_b200_rte_lw_f64(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1,
+        const double* tau, const double* lay_src, const double* lev_src_inc,
+        const double* lev_src_dec, const double* sfc_src, const double* sfc_emis,
+        const double* inc_flux, int n_gauss_angles, double* gpt_flux_up, double* gpt_flux_dn,
+        void* stream);
+
+/* Rte_sw_gpu::rte_sw (include/Rte_sw.h:65-75; src_cuda/Rte_sw.cu:116-161), two-stream +
+ * adding (rte_solver_kernels.cu:188-278,535-647; F90 :512-606,996-1228).  mu0 (ncol);
+ * inc_flux_dir (ncol, ngpt); sfc_alb_dir/dif (nband, ncol); inc_flux_dif (ncol, ngpt) or
+ * NULL.  Outputs gpt_flux_up, gpt_flux_dn (total = diffuse + direct), gpt_flux_dir
+ * (ncol, nlay+1, ngpt).  workspace: device scratch of rrtmgp_b200_rte_sw_workspace_bytes().*/
+size_t rrtmgp_b200_rte_sw_workspace_bytes(int ncol, int nlay, int ngpt, int fp64);
+int rrtmgp_b200_rte_sw_f32(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1,
+        const float* tau, const float* ssa, const float* g, const float* mu0,
+        const float* inc_flux_dir, const float* sfc_alb_dir, const float* sfc_alb_dif,
+        const float* inc_flux_dif, float* gpt_flux_up, float* gpt_flux_dn, float* gpt_flux_dir,
+        void* workspace, size_t workspace_bytes, void* stream);
+int rrtmgp_b200_rte_sw_f64(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1,
+        const double* tau, const double* ssa, const double* g, const double* mu0,
+        const double* inc_flux_dir, const double* sfc_alb_dir, const double* sfc_alb_dif,
+        const double* inc_flux_dif, double* gpt_flux_up, double* gpt_flux_dn,
+        double* gpt_flux_dir, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------------------------------------ */
+/* Flux reductions (src_cuda/Fluxes.cu:39-136; fluxes_kernels.cu:26-113)                 */
+/* ------------------------------------------------------------------------------------ */
+/* Fluxes_broadband_gpu::reduce: sums over g (compensated), net = dn - up.  gpt_flux_dn_dir
+ * and flux_dn_dir may be NULL (the 2-array overload). */
+int rrtmgp_b200_fluxes_broadband_f32(int ncol, int nlev, int ngpt, const float* gpt_flux_up,
+        const float* gpt_flux_dn, const float* gpt_flux_dn_dir, float* flux_up, float* flux_dn,
+        float* flux_dn_dir, float* flux_net, void* stream);
+int rrtmgp_b200_fluxes_broadband_f64(int ncol, int nlev, int ngpt, const double* gpt_flux_up,
+        const double* gpt_flux_dn, const double* gpt_flux_dn_dir, double* flux_up,
+        double* flux_dn, double* flux_dn_dir, double* flux_net, void* stream);
+/* Fluxes_byband_gpu::reduce: band sums over band_lims_gpt(1,b)..band_lims_gpt(2,b)
+ * inclusive, as mo_fluxes_byband_kernels.F90:21-79 (the reference CUDA kernel
+ * fluxes_kernels.cu:78-86 starts one g-point late).  Outputs (ncol, nlev, nband); the
+ * dn_dir pair may be NULL. */
+int rrtmgp_b200_fluxes_byband_f32(rrtmgp_b200_bands b, int ncol, int nlev,
+        const float* gpt_flux_up, const float* gpt_flux_dn, const float* gpt_flux_dn_dir,
+        float* bnd_flux_up, float* bnd_flux_dn, float* bnd_flux_dn_dir, float* bnd_flux_net,
+        void* stream);
+int rrtmgp_b200_fluxes_byband_f64(rrtmgp_b200_bands b, int ncol, int nlev,
+        const double* gpt_flux_up, const double* gpt_flux_dn, const double* gpt_flux_dn_dir,
+        double* bnd_flux_up, double* bnd_flux_dn, double* bnd_flux_dn_dir,
+        double* bnd_flux_net, void* stream);
+/* Heating rate [K/day] per layer from broadband fluxes (no reference counterpart):
+ * HR(l) = g0 / cp_dry * (Fnet(l) - Fnet(l+1)) / (p(l+1) - p(l)) * 86400, i.e. the net
+ * downward flux converging in the layer over its mass, for either vertical orientation;
+ * Fnet = dn - up, g0 = 9.80665 m s-2, cp_dry = 1004.64 J kg-1 K-1. */
+int rrtmgp_b200_heating_rate_f32(int ncol, int nlay, const float* flux_up, const float* flux_dn,
+        const float* plev, float* heating_rate, void* stream);
+int rrtmgp_b200_heating_rate_f64(int ncol, int nlay, const double* flux_up,
+        const double* flux_dn, const double* plev, double* heating_rate, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RRTMGP_B200_H */

@@ -1,0 +1,127 @@
+// Internal definitions shared by the rrtmgp_b200 CUDA sources.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "rrtmgp_b200.h"
+
+namespace rrtmgp_b200 {
+
+// ---------------------------------------------------------------------------------------
+// Error reporting: every C-ABI entry point returns a status and stores a message here.
+// ---------------------------------------------------------------------------------------
+void set_error(const std::string& msg);
+int fail(int status, const std::string& msg);
+int cuda_status(cudaError_t err, const char* where);
+
+#define RB_CHECK_ARG(cond, msg) \
+    do { if (!(cond)) return ::rrtmgp_b200::fail(RRTMGP_B200_ERR_ARG, (msg)); } while (0)
+#define RB_CUDA(call, where) \
+    do { cudaError_t e_ = (call); if (e_ != cudaSuccess) return ::rrtmgp_b200::cuda_status(e_, (where)); } while (0)
+#define RB_LAUNCH(where) \
+    do { cudaError_t e_ = cudaGetLastError(); if (e_ != cudaSuccess) return ::rrtmgp_b200::cuda_status(e_, (where)); } while (0)
+
+inline int ceil_div(long a, long b) { return int((a + b - 1) / b); }
+
+constexpr int kMaxGases = 24;          // gases in one k-distribution after reduction
+constexpr int kMaxBandGpt = 32;        // g-points per band handled in registers/shared mem
+constexpr int kMaxBands = 64;
+
+// ---------------------------------------------------------------------------------------
+// Device-resident k-distribution in one precision.  All tables are g-point fastest so that
+// the g-points of a band at one (T, p, eta) corner are contiguous.
+// ---------------------------------------------------------------------------------------
+template <typename T>
+struct KdistView {
+    int ngas, nband, ngpt, ntemp, npres, neta, nflav, nplanck;
+    int idx_h2o;                    // 1-based index into col_gas (0 = dry air)
+    int has_rayleigh, is_lw;
+    T press_ref_log0, press_ref_log_delta, press_ref_trop_log;
+    T temp_ref_min, temp_ref_delta, totplnk_delta;
+    const T* temp_ref;              // [ntemp]
+    const T* vmr_ref;               // [ntemp][ngas+1][2]
+    const int* flavor;              // [nflav][2]   gas indices (0 = dry air)
+    const int* band_flav;           // [nband][2]   0-based flavor per band and atmosphere
+    const int* band_lims;           // [nband][2]   0-based [start, end)
+    const int* gpt2band;            // [ngpt]       0-based
+    const T* kmajor;                // [ntemp][npres+1][neta][ngpt]
+    const T* planck_frac;           // [ntemp][npres+1][neta][ngpt]
+    const T* totplnk;               // [nband][nplanck]
+    const T* krayl;                 // [2][ntemp][neta][ngpt]
+    const T* solar_source;          // [ngpt]
+    // Minor absorbers, per atmosphere a = 0 (lower, tropo) / 1 (upper).
+    int nminor[2];
+    int ncontrib[2];
+    const int* minor_gstart[2];     // [nminor]   0-based
+    const int* minor_gend[2];       // [nminor]   exclusive
+    const int* minor_kstart[2];     // [nminor]   0-based contributor offset
+    const int* minor_flav[2];       // [nminor]   0-based flavor (of g-point gstart)
+    const int* minor_gas[2];        // [nminor]   col_gas index
+    const int* minor_sgas[2];       // [nminor]   col_gas index of scaling gas, <= 0 none
+    const int* minor_flags[2];      // [nminor]   bit0 scales_with_density, bit1 complement
+    const int* band_minor_begin[2]; // [nband+1]  CSR into band_minor_list
+    const int* band_minor_list[2];  // intervals overlapping each band
+    const T* kminor[2];             // [ntemp][neta][ncontrib]
+    int minor_in_band;              // every interval lies inside one band
+};
+
+}  // namespace rrtmgp_b200
+
+// Opaque handle structs (C ABI).
+struct rrtmgp_b200_bands_t {
+    int nband = 0, ngpt = 0;
+    std::vector<int> band_lims_host;  // (nband, 2) 1-based
+    int* d_band_lims = nullptr;       // [nband][2] 0-based [start, end)
+    int* d_gpt2band = nullptr;        // [ngpt] 0-based
+    bool owned_by_parent = false;
+};
+
+struct rrtmgp_b200_kdist_t {
+    rrtmgp_b200_kdist_info info{};
+    std::vector<std::string> gas_names;  // reduced, trimmed
+    rrtmgp_b200_bands_t bands;
+    rrtmgp_b200::KdistView<float> v32{};
+    rrtmgp_b200::KdistView<double> v64{};
+    std::vector<void*> allocations;
+    std::vector<double> solar_quiet, solar_fac, solar_spot, solar_source;
+    float* d_solar32 = nullptr;
+    double* d_solar64 = nullptr;
+    int* d_flags = nullptr;   // range-check result word
+    int device = 0;
+};
+
+struct rrtmgp_b200_cloud_t {
+    int nband = 0, nsize_liq = 0, nsize_ice = 0;
+    double radliq_lwr = 0, radice_lwr = 0, liq_step = 0, ice_step = 0;
+    float* lut32 = nullptr;   // [6][nband][nsize]: extliq, ssaliq, asyliq (nsize_liq) then ice
+    double* lut64 = nullptr;
+    rrtmgp_b200_bands_t bands;  // one g-point per band
+};
+
+namespace rrtmgp_b200 {
+template <typename T> const KdistView<T>& view(const rrtmgp_b200_kdist_t* k);
+template <> inline const KdistView<float>& view<float>(const rrtmgp_b200_kdist_t* k) { return k->v32; }
+template <> inline const KdistView<double>& view<double>(const rrtmgp_b200_kdist_t* k) { return k->v64; }
+
+template <typename T> const T* cloud_lut(const rrtmgp_b200_cloud_t* c);
+template <> inline const float* cloud_lut<float>(const rrtmgp_b200_cloud_t* c) { return c->lut32; }
+template <> inline const double* cloud_lut<double>(const rrtmgp_b200_cloud_t* c) { return c->lut64; }
+
+// Gas concentration descriptors passed to kernels by value.
+template <typename T>
+struct GasSet {
+    const T* vmr[kMaxGases];   // indexed by reduced gas (0-based)
+    int mode[kMaxGases];       // 0 scalar, 1 profile (per layer), 2 field (ncol, nlay)
+};
+
+template <typename T>
+int make_gas_set(const rrtmgp_b200_kdist_t* k, int ncol, int nlay,
+                 const rrtmgp_b200_gas_conc* gases, int ngases, GasSet<T>& out);
+
+inline cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+}  // namespace rrtmgp_b200

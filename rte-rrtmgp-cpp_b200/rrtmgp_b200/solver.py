@@ -1,0 +1,141 @@
+"""Column-radiation driver: the sequence of Radiation_solver_longwave/shortwave::solve_gpu
+(src_test/Radiation_solver.cu:419-657, :683-950) over the C ABI.
+
+LW: gas_optics -> cloud_optics (1scl) -> add_to by band -> rte_lw -> broadband reduce.
+SW: gas_optics -> toa_src x tsi_scaling -> cloud_optics (2str) -> delta_scale -> add_to by
+band -> rte_sw -> broadband reduce.  Both add heating rates.  Buffers are allocated once per
+(ncol, nlay, dtype) and reused, so repeated solves launch kernels only.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import api
+
+ATM_KEYS_2D = ("play", "plev", "tlay", "tlev", "lwp", "iwp", "rel", "rei")
+
+
+class Radiation_solver:
+    def __init__(self, kdist_lw: dict, kdist_sw: dict, cloud_lw: dict | None, cloud_sw: dict | None,
+                 available_gases, delta_cloud: bool = True):
+        self.klw = api.Gas_optics_rrtmgp(kdist_lw, available_gases)
+        self.ksw = api.Gas_optics_rrtmgp(kdist_sw, available_gases)
+        self.clw = api.Cloud_optics(cloud_lw) if cloud_lw is not None else None
+        self.csw = api.Cloud_optics(cloud_sw) if cloud_sw is not None else None
+        self.delta_cloud = delta_cloud
+        self._bufs = {}
+
+    def _buffers(self, key, like, ncol, nlay, kind):
+        b = self._bufs.get((key, kind))
+        if b is not None:
+            return b
+        dt, dev = like.dtype, like.device
+        nlev = nlay + 1
+        if kind == "lw":
+            ng = self.klw.get_ngpt()
+            b = {k: torch.empty((ng, nlay, ncol), dtype=dt, device=dev)
+                 for k in ("tau", "lay_src", "lev_src_inc", "lev_src_dec")}
+            b["sfc_src"] = torch.empty((ng, ncol), dtype=dt, device=dev)
+            b["sfc_src_jac"] = torch.empty((ng, ncol), dtype=dt, device=dev)
+            b["cloud_tau"] = torch.empty((self.klw.get_nband(), nlay, ncol), dtype=dt, device=dev)
+            b["gpt_up"] = torch.empty((ng, nlev, ncol), dtype=dt, device=dev)
+            b["gpt_dn"] = torch.empty((ng, nlev, ncol), dtype=dt, device=dev)
+        else:
+            ng = self.ksw.get_ngpt()
+            b = {k: torch.empty((ng, nlay, ncol), dtype=dt, device=dev) for k in ("tau", "ssa", "g")}
+            b["toa_src"] = torch.empty((ng, ncol), dtype=dt, device=dev)
+            nb = self.ksw.get_nband()
+            b.update({k: torch.empty((nb, nlay, ncol), dtype=dt, device=dev) for k in ("c_tau", "c_ssa", "c_g")})
+            for k in ("gpt_up", "gpt_dn", "gpt_dir"):
+                b[k] = torch.empty((ng, nlev, ncol), dtype=dt, device=dev)
+            b["ws"] = api.Rte_sw.workspace(ncol, nlay, ng, like).clone()
+        for k in ("flux_up", "flux_dn", "flux_net", "flux_dn_dir"):
+            b[k] = torch.empty((nlev, ncol), dtype=dt, device=dev)
+        b["heating_rate"] = torch.empty((nlay, ncol), dtype=dt, device=dev)
+        self._bufs[(key, kind)] = b
+        return b
+
+    def solve_lw(self, atm: dict, with_clouds: bool = True, top_at_1: bool = True):
+        """atm: torch tensors play, plev, tlay, tlev (nlay[+1], ncol), tsfc (ncol), emis_sfc
+        (ncol, nband), gases {name: tensor}, lwp/iwp/rel/rei (nlay, ncol)."""
+        from . import _abi
+        import ctypes as C
+        play = atm["play"]
+        nlay, ncol = play.shape
+        key = (ncol, nlay, play.dtype)
+        b = self._buffers(key, play, ncol, nlay, "lw")
+        lib = _abi.load()
+        sfx = api._sfx(play)
+        s = api._stream()
+        P = api._ptr
+        arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay)
+        _abi.check(getattr(lib, "rrtmgp_b200_gas_optics_lw" + sfx)(
+            self.klw.handle, ncol, nlay, P(play), P(atm["plev"]), P(atm["tlay"]), P(atm["tsfc"]), P(atm["tlev"]),
+            None, arr, len(atm["gases"]), P(b["tau"]), P(b["lay_src"]), P(b["lev_src_inc"]), P(b["lev_src_dec"]),
+            P(b["sfc_src"]), P(b["sfc_src_jac"]), s))
+        if with_clouds and self.clw is not None:
+            _abi.check(getattr(lib, "rrtmgp_b200_cloud_optics_1scl" + sfx)(
+                self.clw.handle, ncol, nlay, P(atm["lwp"]), P(atm["iwp"]), P(atm["rel"]), P(atm["rei"]),
+                P(b["cloud_tau"]), s))
+            _abi.check(getattr(lib, "rrtmgp_b200_add_to_1scl" + sfx)(
+                self.klw.bands.handle, ncol, nlay, P(b["tau"]), P(b["cloud_tau"]), self.klw.get_nband(), s))
+        _abi.check(getattr(lib, "rrtmgp_b200_rte_lw" + sfx)(
+            self.klw.bands.handle, ncol, nlay, int(top_at_1), P(b["tau"]), P(b["lay_src"]), P(b["lev_src_inc"]),
+            P(b["lev_src_dec"]), P(b["sfc_src"]), P(atm["emis_sfc"]), None, 1, P(b["gpt_up"]), P(b["gpt_dn"]), s))
+        _abi.check(getattr(lib, "rrtmgp_b200_fluxes_broadband" + sfx)(
+            ncol, nlay + 1, self.klw.get_ngpt(), P(b["gpt_up"]), P(b["gpt_dn"]), None, P(b["flux_up"]),
+            P(b["flux_dn"]), None, P(b["flux_net"]), s))
+        _abi.check(getattr(lib, "rrtmgp_b200_heating_rate" + sfx)(
+            ncol, nlay, P(b["flux_up"]), P(b["flux_dn"]), P(atm["plev"]), P(b["heating_rate"]), s))
+        return {k: b[k] for k in ("flux_up", "flux_dn", "flux_net", "heating_rate")}
+
+    def solve_sw(self, atm: dict, with_clouds: bool = True, top_at_1: bool = True):
+        """atm additionally needs mu0 (ncol), sfc_alb_dir / sfc_alb_dif (ncol, nband) and
+        optionally tsi_scaling (ncol)."""
+        from . import _abi
+        play = atm["play"]
+        nlay, ncol = play.shape
+        key = (ncol, nlay, play.dtype)
+        b = self._buffers(key, play, ncol, nlay, "sw")
+        lib = _abi.load()
+        sfx = api._sfx(play)
+        s = api._stream()
+        P = api._ptr
+        arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay)
+        _abi.check(getattr(lib, "rrtmgp_b200_gas_optics_sw" + sfx)(
+            self.ksw.handle, ncol, nlay, P(play), P(atm["plev"]), P(atm["tlay"]), None, arr, len(atm["gases"]),
+            P(b["tau"]), P(b["ssa"]), P(b["g"]), P(b["toa_src"]), s))
+        if "tsi_scaling" in atm and atm["tsi_scaling"] is not None:
+            b["toa_src"].mul_(atm["tsi_scaling"][None, :])
+        nb = self.ksw.get_nband()
+        if with_clouds and self.csw is not None:
+            _abi.check(getattr(lib, "rrtmgp_b200_cloud_optics_2str" + sfx)(
+                self.csw.handle, ncol, nlay, P(atm["lwp"]), P(atm["iwp"]), P(atm["rel"]), P(atm["rei"]),
+                P(b["c_tau"]), P(b["c_ssa"]), P(b["c_g"]), s))
+            if self.delta_cloud:
+                _abi.check(getattr(lib, "rrtmgp_b200_delta_scale_2str" + sfx)(
+                    ncol, nlay, nb, P(b["c_tau"]), P(b["c_ssa"]), P(b["c_g"]), s))
+            _abi.check(getattr(lib, "rrtmgp_b200_add_to_2str" + sfx)(
+                self.ksw.bands.handle, ncol, nlay, P(b["tau"]), P(b["ssa"]), P(b["g"]), P(b["c_tau"]),
+                P(b["c_ssa"]), P(b["c_g"]), nb, s))
+        import ctypes as C
+        _abi.check(getattr(lib, "rrtmgp_b200_rte_sw" + sfx)(
+            self.ksw.bands.handle, ncol, nlay, int(top_at_1), P(b["tau"]), P(b["ssa"]), P(b["g"]), P(atm["mu0"]),
+            P(b["toa_src"]), P(atm["sfc_alb_dir"]), P(atm["sfc_alb_dif"]), None, P(b["gpt_up"]), P(b["gpt_dn"]),
+            P(b["gpt_dir"]), C.c_void_p(b["ws"].data_ptr()), C.c_size_t(b["ws"].numel()), s))
+        _abi.check(getattr(lib, "rrtmgp_b200_fluxes_broadband" + sfx)(
+            ncol, nlay + 1, self.ksw.get_ngpt(), P(b["gpt_up"]), P(b["gpt_dn"]), P(b["gpt_dir"]), P(b["flux_up"]),
+            P(b["flux_dn"]), P(b["flux_dn_dir"]), P(b["flux_net"]), s))
+        _abi.check(getattr(lib, "rrtmgp_b200_heating_rate" + sfx)(
+            ncol, nlay, P(b["flux_up"]), P(b["flux_dn"]), P(atm["plev"]), P(b["heating_rate"]), s))
+        return {k: b[k] for k in ("flux_up", "flux_dn", "flux_dn_dir", "flux_net", "heating_rate")}
+
+
+def atm_to_device(atm: dict, dtype, device):
+    """Convert a synthetic atmosphere (numpy, rrtmgp_b200.synthetic layout) to torch."""
+    out = {}
+    for k in ATM_KEYS_2D + ("tsfc", "mu0", "tsi_scaling", "emis_sfc", "sfc_alb_dir", "sfc_alb_dif"):
+        out[k] = torch.as_tensor(atm[k], dtype=dtype, device=device).contiguous()
+    out["gases"] = {k: torch.as_tensor(v.reshape(1) if v.size == 1 else v, dtype=dtype, device=device).contiguous()
+                    for k, v in atm["gases"].items()}
+    return out

@@ -1,0 +1,65 @@
+"""CPU tests of the C ABI boundary: the library loads without a GPU and exports every
+function include/rrtmgp_b200.h declares; the Python table marshalling is consistent."""
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+
+from rrtmgp_b200 import _abi, synthetic as S
+
+HEADER = Path(__file__).resolve().parent.parent / "include" / "rrtmgp_b200.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(rrtmgp_b200_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declarations_match_binding():
+    assert sorted(_abi.declared_symbols()) == declared_functions()
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(str(_abi.LIB_PATH))
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+    assert lib.rrtmgp_b200_abi_version() == 1
+
+
+def test_binding_signatures_load():
+    lib = _abi.load()
+    assert lib.rrtmgp_b200_last_error() is not None
+
+
+def test_workspace_query_needs_no_gpu():
+    lib = _abi.load()
+    assert lib.rrtmgp_b200_rte_sw_workspace_bytes(10, 20, 30, 0) == 4 * 10 * 20 * 30 * 4
+    assert lib.rrtmgp_b200_rte_sw_workspace_bytes(10, 20, 30, 1) == 4 * 10 * 20 * 30 * 8
+
+
+def test_null_arguments_are_rejected_without_gpu():
+    lib = _abi.load()
+    st = lib.rrtmgp_b200_kdist_create(None, None, 0, None)
+    assert st == _abi.ERR_ARG
+    assert b"null" in lib.rrtmgp_b200_last_error()
+
+
+def test_table_struct_dimensions(tables):
+    t, keep = _abi.kdist_tables(tables["lw"])
+    assert (t.nband, t.ngpt, t.ntemp, t.npres, t.neta) == (16, 256, 14, 59, 9)
+    assert t.nplanck_temp == 196 and t.ncontrib_lower == tables["lw"]["kminor_lower"].shape[2]
+    ts, keep2 = _abi.kdist_tables(tables["sw"])
+    assert ts.nplanck_temp == 0 and bool(ts.rayl_lower) and not bool(ts.totplnk)
+    c, keep3 = _abi.cloud_tables(tables["cloud_sw"])
+    assert (c.nband, c.nsize_liq, c.nsize_ice, c.nrghice) == (14, 20, 18, 3)
+
+
+def test_synthetic_atmosphere_layout():
+    atm = S.make_atmosphere(7, 9, seed=1)
+    assert atm["play"].shape == (9, 7) and atm["plev"].shape == (10, 7)
+    assert np.all(np.diff(atm["plev"][:, 0]) > 0)  # top_at_1: pressure increases with index
+    assert atm["plev"][0, 0] >= S.PRESS_REF_MIN
+    flip = S.make_atmosphere(7, 9, seed=1, top_at_1=False)
+    assert np.all(np.diff(flip["plev"][:, 0]) < 0)

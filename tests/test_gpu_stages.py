@@ -1,0 +1,305 @@
+"""GPU parity of every per-stage C-ABI entry point against the FP64 oracle.
+
+Each test runs the CUDA kernels through the C ABI (rrtmgp_b200.api -> librrtmgp_b200.so) and
+the oracle on identical seeded inputs.  Tolerances: FP64 kernels agree with the oracle to
+1e-10 relative (reordering of sums only); FP32 kernels to the stated relative tolerance of
+single precision interpolation.  Shapes are ragged (ncol not a multiple of 32) on purpose.
+"""
+import numpy as np
+import pytest
+
+from rrtmgp_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+NCOL, NLAY = 37, 23
+RTOL = {"f64": 1e-10, "f32": 2e-4}
+
+
+def T(x, dt, dev):
+    import torch
+    return torch.as_tensor(np.ascontiguousarray(x), dtype=dt, device=dev)
+
+
+def N(t):
+    return t.detach().double().cpu().numpy()
+
+
+def dtypes():
+    import torch
+    return {"f32": torch.float32, "f64": torch.float64}
+
+
+def cmp(name, got, ref, prec, floor_frac=1e-6):
+    ref = np.asarray(ref, np.float64)
+    got = np.asarray(got, np.float64)
+    floor = max(floor_frac * np.max(np.abs(ref)), 1e-300)
+    err = np.max(np.abs(got - ref) / (np.abs(ref) + floor))
+    assert err <= RTOL[prec], f"{name}: max rel err {err:.3e} > {RTOL[prec]} ({prec})"
+
+
+def gas_dict(atm, dt, dev, profile_o3=False):
+    out = {}
+    for k, v in atm["gases"].items():
+        if v.size == 1:
+            out[k] = T(v.reshape(1), dt, dev)
+        elif profile_o3 and k == "o3":
+            out[k] = T(v[:, 0].copy(), dt, dev)
+        else:
+            out[k] = T(v, dt, dev)
+    return out
+
+
+@pytest.fixture(scope="module")
+def api(gpu):
+    from rrtmgp_b200 import api
+    return api
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+@pytest.mark.parametrize("top_at_1", [True, False])
+@pytest.mark.parametrize("with_col_dry", [False, True])
+def test_gas_optics_lw(api, oracle_mod, tables, gpu, prec, top_at_1, with_col_dry):
+    dt = dtypes()[prec]
+    atm = S.make_atmosphere(NCOL, NLAY, seed=11, clouds=False, top_at_1=top_at_1)
+    cd = S.col_dry_from(atm["gases"]["h2o"], atm["plev"]) if with_col_dry else None
+    ref = oracle_mod.GasOptics(tables["lw"], S.ATM_GASES).gas_optics_lw(
+        atm["play"], atm["plev"], atm["tlay"], atm["tsfc"], atm["gases"], atm["tlev"], cd)
+    kd = api.Gas_optics_rrtmgp(tables["lw"], S.ATM_GASES)
+    got = kd.gas_optics_lw(T(atm["play"], dt, gpu), T(atm["plev"], dt, gpu), T(atm["tlay"], dt, gpu),
+                           T(atm["tsfc"], dt, gpu), gas_dict(atm, dt, gpu), T(atm["tlev"], dt, gpu),
+                           None if cd is None else T(cd, dt, gpu))
+    for k in ("tau", "lay_src", "lev_src_inc", "lev_src_dec", "sfc_src", "sfc_src_jac"):
+        cmp(k, N(got[k]), ref[k], prec)
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+@pytest.mark.parametrize("top_at_1", [True, False])
+def test_gas_optics_sw(api, oracle_mod, tables, gpu, prec, top_at_1):
+    dt = dtypes()[prec]
+    atm = S.make_atmosphere(NCOL, NLAY, seed=12, clouds=False, top_at_1=top_at_1)
+    ref = oracle_mod.GasOptics(tables["sw"], S.ATM_GASES).gas_optics_sw(
+        atm["play"], atm["plev"], atm["tlay"], atm["gases"])
+    kd = api.Gas_optics_rrtmgp(tables["sw"], S.ATM_GASES)
+    got = kd.gas_optics_sw(T(atm["play"], dt, gpu), T(atm["plev"], dt, gpu), T(atm["tlay"], dt, gpu),
+                           gas_dict(atm, dt, gpu, profile_o3=False))
+    for k in ("tau", "ssa", "toa_src"):
+        cmp(k, N(got[k]), ref[k], prec)
+    assert float(got["g"].abs().max()) == 0.0
+
+
+def test_gas_profile_and_scalar_inputs(api, oracle_mod, tables, gpu):
+    """Gas_concs accepts scalars, (1, nlay) profiles and (ncol, nlay) fields."""
+    import torch
+    atm = S.make_atmosphere(NCOL, NLAY, seed=13, clouds=False)
+    o3p = atm["gases"]["o3"][:, :1]
+    atm["gases"]["o3"] = np.repeat(o3p, NCOL, axis=1)
+    ref = oracle_mod.GasOptics(tables["sw"], S.ATM_GASES).gas_optics_sw(atm["play"], atm["plev"], atm["tlay"], atm["gases"])
+    kd = api.Gas_optics_rrtmgp(tables["sw"], S.ATM_GASES)
+    g = gas_dict(atm, torch.float64, gpu, profile_o3=True)
+    got = kd.gas_optics_sw(T(atm["play"], torch.float64, gpu), T(atm["plev"], torch.float64, gpu),
+                           T(atm["tlay"], torch.float64, gpu), g)
+    cmp("tau", N(got["tau"]), ref["tau"], "f64")
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_col_dry(api, gpu, prec):
+    dt = dtypes()[prec]
+    atm = S.make_atmosphere(NCOL, NLAY, seed=14)
+    got = api.Gas_optics_rrtmgp.get_col_dry(T(atm["gases"]["h2o"], dt, gpu), T(atm["plev"], dt, gpu))
+    cmp("col_dry", N(got), S.col_dry_from(atm["gases"]["h2o"], atm["plev"]), prec)
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+@pytest.mark.parametrize("kind", ["lw", "sw"])
+def test_cloud_optics(api, oracle_mod, tables, gpu, prec, kind):
+    dt = dtypes()[prec]
+    atm = S.make_atmosphere(NCOL, NLAY, seed=15, clouds=True)
+    two = kind == "sw"
+    ref = oracle_mod.CloudOptics(tables["cloud_" + kind]).cloud_optics(atm["lwp"], atm["iwp"], atm["rel"], atm["rei"], two)
+    c = api.Cloud_optics(tables["cloud_" + kind])
+    got = c.cloud_optics(*(T(atm[k], dt, gpu) for k in ("lwp", "iwp", "rel", "rei")), two_stream=two)
+    for k in ref:
+        cmp(k, N(got[k]), ref[k], prec)
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_delta_scale_and_add_to(api, oracle_mod, tables, gpu, prec):
+    dt = dtypes()[prec]
+    rng = np.random.default_rng(3)
+    kd = api.Gas_optics_rrtmgp(tables["sw"], S.ATM_GASES)
+    nb, ng = 14, 224
+    gas = {"tau": rng.uniform(0, 2, (ng, NLAY, NCOL)), "ssa": rng.uniform(0, 1, (ng, NLAY, NCOL)),
+           "g": rng.uniform(0, 0.9, (ng, NLAY, NCOL))}
+    cld = {"tau": rng.uniform(0, 5, (nb, NLAY, NCOL)), "ssa": rng.uniform(0.5, 1, (nb, NLAY, NCOL)),
+           "g": rng.uniform(0.7, 0.9, (nb, NLAY, NCOL))}
+    cld["tau"][:, ::3] = 0.0
+    ref_c = {k: v.copy() for k, v in cld.items()}
+    oracle_mod.delta_scale(ref_c["tau"], ref_c["ssa"], ref_c["g"])
+    got_c = {k: T(v, dt, gpu) for k, v in cld.items()}
+    api.delta_scale(got_c["tau"], got_c["ssa"], got_c["g"])
+    for k in cld:
+        cmp("delta_" + k, N(got_c[k]), ref_c[k], prec)
+    ref_g = {k: v.copy() for k, v in gas.items()}
+    oracle_mod.add_to(tables["sw"]["bnd_limits_gpt"], ref_g, ref_c)
+    got_g = {k: T(v, dt, gpu) for k, v in gas.items()}
+    api.add_to(kd.bands, got_g, got_c)
+    for k in gas:
+        cmp("add_" + k, N(got_g[k]), ref_g[k], prec)
+    # g-point by g-point, 1scl
+    ref1 = {"tau": gas["tau"].copy()}
+    oracle_mod.add_to(None, ref1, {"tau": gas["tau"]})
+    got1 = {"tau": T(gas["tau"], dt, gpu)}
+    api.add_to(kd.bands, got1, {"tau": T(gas["tau"], dt, gpu)})
+    cmp("add_1scl", N(got1["tau"]), ref1["tau"], prec)
+
+
+def test_add_to_rejects_incompatible_shapes(api, tables, gpu):
+    import torch
+    from rrtmgp_b200._abi import RrtmgpError, ERR_ARG
+    kd = api.Gas_optics_rrtmgp(tables["sw"], S.ATM_GASES)
+    a = {"tau": torch.zeros((224, 2, 3), dtype=torch.float64, device=gpu)}
+    b = {"tau": torch.zeros((13, 2, 3), dtype=torch.float64, device=gpu)}
+    with pytest.raises(RrtmgpError) as e:
+        api.add_to(kd.bands, a, b)
+    assert e.value.status == ERR_ARG and "incompatible band" in str(e.value)
+
+
+def _lw_inputs(tables, oracle_mod, top_at_1, seed):
+    atm = S.make_atmosphere(NCOL, NLAY, seed=seed, clouds=False, top_at_1=top_at_1)
+    go = oracle_mod.GasOptics(tables["lw"], S.ATM_GASES).gas_optics_lw(
+        atm["play"], atm["plev"], atm["tlay"], atm["tsfc"], atm["gases"], atm["tlev"])
+    return atm, go
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+@pytest.mark.parametrize("top_at_1", [True, False])
+@pytest.mark.parametrize("nmu", [1, 3])
+@pytest.mark.parametrize("with_inc", [False, True])
+def test_rte_lw(api, oracle_mod, tables, gpu, prec, top_at_1, nmu, with_inc):
+    dt = dtypes()[prec]
+    atm, go = _lw_inputs(tables, oracle_mod, top_at_1, 21)
+    rng = np.random.default_rng(5)
+    emis = rng.uniform(0.8, 1.0, (NCOL, 16))
+    inc = rng.uniform(0, 2, (256, NCOL)) if with_inc else None
+    bl = tables["lw"]["bnd_limits_gpt"]
+    up, dn = oracle_mod.rte_lw(bl, go["tau"], top_at_1, go, emis, inc, nmu)
+    kd = api.Gas_optics_rrtmgp(tables["lw"], S.ATM_GASES)
+    src = {k: T(v, dt, gpu) for k, v in go.items()}
+    gu, gd = api.Rte_lw.rte_lw(kd.bands, src["tau"], top_at_1, src, T(emis, dt, gpu),
+                               None if inc is None else T(inc, dt, gpu), nmu)
+    cmp("flux_up", N(gu), up, prec)
+    cmp("flux_dn", N(gd), dn, prec, floor_frac=1e-4)
+
+
+def test_rte_lw_large_nlay_without_smem_stash(api, oracle_mod, tables, gpu):
+    """nlay large enough that the up-sweep stash does not fit in shared memory in FP64."""
+    import torch
+    dt = torch.float64
+    ncol, nlay = 5, 400
+    atm = S.make_atmosphere(ncol, nlay, seed=2, clouds=False)
+    go = oracle_mod.GasOptics(tables["lw"], S.ATM_GASES).gas_optics_lw(
+        atm["play"], atm["plev"], atm["tlay"], atm["tsfc"], atm["gases"], atm["tlev"])
+    emis = np.full((ncol, 16), 0.95)
+    up, dn = oracle_mod.rte_lw(tables["lw"]["bnd_limits_gpt"], go["tau"], True, go, emis)
+    kd = api.Gas_optics_rrtmgp(tables["lw"], S.ATM_GASES)
+    src = {k: T(v, dt, gpu) for k, v in go.items()}
+    gu, gd = api.Rte_lw.rte_lw(kd.bands, src["tau"], True, src, T(emis, dt, gpu))
+    cmp("flux_up", N(gu), up, "f64")
+    cmp("flux_dn", N(gd), dn, "f64", floor_frac=1e-4)
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+@pytest.mark.parametrize("top_at_1", [True, False])
+@pytest.mark.parametrize("with_dif", [False, True])
+def test_rte_sw(api, oracle_mod, tables, gpu, prec, top_at_1, with_dif):
+    dt = dtypes()[prec]
+    atm = S.make_atmosphere(NCOL, NLAY, seed=31, clouds=True, top_at_1=top_at_1)
+    ko = oracle_mod.GasOptics(tables["sw"], S.ATM_GASES)
+    go = ko.gas_optics_sw(atm["play"], atm["plev"], atm["tlay"], atm["gases"])
+    c = oracle_mod.CloudOptics(tables["cloud_sw"]).cloud_optics(atm["lwp"], atm["iwp"], atm["rel"], atm["rei"], True)
+    oracle_mod.delta_scale(c["tau"], c["ssa"], c["g"])
+    bl = tables["sw"]["bnd_limits_gpt"]
+    oracle_mod.add_to(bl, go, c)
+    rng = np.random.default_rng(9)
+    alb_dir = rng.uniform(0.05, 0.3, (NCOL, 14))
+    alb_dif = rng.uniform(0.05, 0.3, (NCOL, 14))
+    inc_dif = rng.uniform(0, 1, (224, NCOL)) if with_dif else None
+    up, dn, dr = oracle_mod.rte_sw(bl, go["tau"], go["ssa"], go["g"], top_at_1, atm["mu0"], go["toa_src"],
+                                   alb_dir, alb_dif, inc_dif)
+    kd = api.Gas_optics_rrtmgp(tables["sw"], S.ATM_GASES)
+    gu, gd, gr = api.Rte_sw.rte_sw(kd.bands, T(go["tau"], dt, gpu), T(go["ssa"], dt, gpu), T(go["g"], dt, gpu),
+                                   top_at_1, T(atm["mu0"], dt, gpu), T(go["toa_src"], dt, gpu),
+                                   T(alb_dir, dt, gpu), T(alb_dif, dt, gpu),
+                                   None if inc_dif is None else T(inc_dif, dt, gpu))
+    tol_floor = 1e-4
+    cmp("flux_dir", N(gr), dr, prec, tol_floor)
+    cmp("flux_dn", N(gd), dn, prec, tol_floor)
+    cmp("flux_up", N(gu), up, prec, tol_floor)
+
+
+def test_rte_sw_workspace_required(api, tables, gpu):
+    import torch
+    from rrtmgp_b200._abi import RrtmgpError, ERR_WORKSPACE
+    kd = api.Gas_optics_rrtmgp(tables["sw"], S.ATM_GASES)
+    z = torch.zeros((224, 3, 2), dtype=torch.float32, device=gpu)
+    m = torch.ones(2, dtype=torch.float32, device=gpu)
+    a = torch.zeros((2, 14), dtype=torch.float32, device=gpu)
+    s = torch.ones((224, 2), dtype=torch.float32, device=gpu)
+    small = torch.empty(16, dtype=torch.uint8, device=gpu)
+    with pytest.raises(RrtmgpError) as e:
+        api.Rte_sw.rte_sw(kd.bands, z, z, z, True, m, s, a, a, workspace=small)
+    assert e.value.status == ERR_WORKSPACE
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_fluxes_and_heating_rate(api, oracle_mod, tables, gpu, prec):
+    dt = dtypes()[prec]
+    rng = np.random.default_rng(4)
+    up = rng.uniform(0, 20, (224, NLAY + 1, NCOL))
+    dn = rng.uniform(0, 20, (224, NLAY + 1, NCOL))
+    dr = rng.uniform(0, 20, (224, NLAY + 1, NCOL))
+    ref = oracle_mod.fluxes_broadband(up, dn, dr)
+    got = api.Fluxes_broadband.reduce(T(up, dt, gpu), T(dn, dt, gpu), T(dr, dt, gpu))
+    for k in ref:
+        cmp(k, N(got[k]), ref[k], prec, floor_frac=1e-3)
+    kd = api.Gas_optics_rrtmgp(tables["sw"], S.ATM_GASES)
+    bl = tables["sw"]["bnd_limits_gpt"]
+    refb = oracle_mod.fluxes_byband(bl, up, dn, dr)
+    gotb = api.Fluxes_byband.reduce(kd.bands, T(up, dt, gpu), T(dn, dt, gpu), T(dr, dt, gpu))
+    for k in refb:
+        cmp(k, N(gotb[k]), refb[k], prec, floor_frac=1e-3)
+    atm = S.make_atmosphere(NCOL, NLAY, seed=3)
+    hr = api.heating_rate(got["flux_up"], got["flux_dn"], T(atm["plev"], dt, gpu))
+    href = oracle_mod.heating_rate(N(got["flux_up"]), N(got["flux_dn"]), atm["plev"])
+    cmp("heating_rate", N(hr), href, "f64" if prec == "f64" else "f32", floor_frac=1e-3)
+
+
+def test_range_check(api, tables, gpu):
+    import torch
+    from rrtmgp_b200._abi import RrtmgpError, ERR_RANGE
+    kd = api.Gas_optics_rrtmgp(tables["lw"], S.ATM_GASES)
+    atm = S.make_atmosphere(8, 6, seed=1)
+    args = [T(atm[k], torch.float64, gpu) for k in ("play", "plev", "tlay", "tlev")]
+    kd.check_range(args[0], args[1], args[2], args[3], T(atm["tsfc"], torch.float64, gpu))
+    bad = atm["tlay"].copy()
+    bad[2, 3] = 400.0
+    with pytest.raises(RrtmgpError) as e:
+        kd.check_range(args[0], args[1], T(bad, torch.float64, gpu), args[3])
+    assert e.value.status == ERR_RANGE and "tlay is out of range" in str(e.value)
+
+
+def test_missing_gas_is_reported(api, tables, gpu):
+    import torch
+    from rrtmgp_b200._abi import RrtmgpError, ERR_MISSING_GAS
+    with pytest.raises(RrtmgpError) as e:
+        api.Gas_optics_rrtmgp(tables["lw"], ["h2o", "o3"])
+    assert e.value.status == ERR_MISSING_GAS and "required gas co2 is missing" in str(e.value)
+    kd = api.Gas_optics_rrtmgp(tables["sw"], S.ATM_GASES)
+    atm = S.make_atmosphere(4, 5, seed=1)
+    g = gas_dict(atm, torch.float64, gpu)
+    del g["ch4"]
+    with pytest.raises(RrtmgpError) as e:
+        kd.gas_optics_sw(T(atm["play"], torch.float64, gpu), T(atm["plev"], torch.float64, gpu),
+                         T(atm["tlay"], torch.float64, gpu), g)
+    assert e.value.status == ERR_MISSING_GAS

@@ -82,6 +82,17 @@ __device__ __forceinline__ LayerInterp<T> layer_interp(const KdistView<T>& k, T 
     return li;
 }
 
+// Fractional eta position inside cell j (1-based).  FP64 keeps the reference's
+// fmod(loceta, 1) (gas_optics_rrtmgp_kernels.cu:277).  That expression drops to 0 when
+// loceta reaches neta-1 while jeta stays clamped at neta-1, a jump from the value at the
+// last eta node to the one below it; in FP32 eta = 1 - 2e-9 rounds to exactly 1 (e.g. the
+// (h2o, o3) flavor near the surface) and the jump changes tau by up to 40%.  The FP32 path
+// therefore uses loceta - (j - 1), which equals fmod(loceta, 1) for every loceta < neta-1
+// and is continuous at eta = 1.
+template <typename T> __device__ __forceinline__ T eta_fraction(T loceta, int j);
+template <> __device__ __forceinline__ double eta_fraction<double>(double loceta, int) { return fmod(loceta, 1.0); }
+template <> __device__ __forceinline__ float eta_fraction<float>(float loceta, int j) { return loceta - float(j - 1); }
+
 template <typename T>
 struct FlavorWeights {
     int j0, j1;    // jeta for the two temperatures (1-based)
@@ -105,8 +116,10 @@ __device__ __forceinline__ FlavorWeights<T> flavor_weights(const KdistView<T>& k
         const T cm = c1 + ratio * c2;
         const T eta = cm > two_tmin ? c1 / cm : T(0.5);
         const T loceta = eta * T(k.neta - 1);
-        const int j = min(int(loceta) + 1, k.neta - 1);
-        const T feta = fmod(loceta, T(1));
+        // max(1, .) only guards memory for invalid (negative) concentrations; for valid
+        // inputs eta lies in [0, 1] and this is the reference's min(int(loceta)+1, neta-1).
+        const int j = max(1, min(int(loceta) + 1, k.neta - 1));
+        const T feta = eta_fraction<T>(loceta, j);
         const T ftt = T(1 - itemp) + T(2 * itemp - 1) * li.ftemp;
         w.fm[2 * itemp] = (T(1) - feta) * ftt;
         w.fm[2 * itemp + 1] = feta * ftt;

@@ -48,6 +48,7 @@ __global__ void lw_solver_kernel(int ncol, int nlay, int nband, int top_at_1, in
         // Downward sweep.
         if (imu == 0) flux_dn[fbase + size_t(top) * ncol] = two_pi_w * radn;
         else flux_dn[fbase + size_t(top) * ncol] += two_pi_w * radn;
+#pragma unroll 4
         for (int j = 0; j < nlay; ++j) {
             const int l = top_at_1 ? j : nlay - 1 - j;
             const size_t i = base + size_t(l) * ncol;
@@ -67,6 +68,7 @@ __global__ void lw_solver_kernel(int ncol, int nlay, int nband, int top_at_1, in
         if (imu == 0) flux_up[fbase + size_t(sfc) * ncol] = two_pi_w * rup;
         else flux_up[fbase + size_t(sfc) * ncol] += two_pi_w * rup;
         // Upward sweep.
+#pragma unroll 4
         for (int j = nlay - 1; j >= 0; --j) {
             const int l = top_at_1 ? j : nlay - 1 - j;
             T tr, sup;

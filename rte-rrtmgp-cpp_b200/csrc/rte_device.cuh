@@ -24,16 +24,43 @@ template <typename T> __device__ __forceinline__ T pi_value() { return T(3.14159
 
 // Transmissivity and linear-in-tau level sources of one layer for one angle
 // (lw_solver_noscat_step_1_kernel, rte_solver_kernels.cu:116-125; Clough et al. 1992).
+// FP64 uses the reference expressions.  In FP32, (1 - T)/tau - T cancels to a relative error
+// of eps/tau for thin layers, so the FP32 path takes 1 - T = -expm1(-tau) and, below
+// tau = 0.1, the series of fact = sum_n (-1)^(n+1) n/(n+1)! tau^n to n = 6
+// (truncation < 2e-11 relative), which equals the reference's 2-term series where that
+// one is used.
 template <typename T>
-__device__ __forceinline__ void lw_layer(T tau, T D, T lay, T lev_dn, T lev_up, T& trans, T& src_dn, T& src_up)
+__device__ __forceinline__ void lw_layer(T tau, T D, T lay, T lev_dn, T lev_up, T& trans, T& src_dn, T& src_up);
+
+template <>
+__device__ __forceinline__ void lw_layer<double>(double tau, double D, double lay, double lev_dn, double lev_up,
+                                                 double& trans, double& src_dn, double& src_up)
 {
-    const T eps = eps_value<T>();
-    const T tl = tau * D;
+    const double eps = DBL_EPSILON;
+    const double tl = tau * D;
     trans = exp(-tl);
-    const T fact = (tl > T(0) && (tl * tl) > eps) ? (T(1) - trans) / tl - trans
-                                                   : tl * (T(0.5) - T(1) / T(3) * tl);
-    src_dn = (T(1) - trans) * lev_dn + T(2) * fact * (lay - lev_dn);
-    src_up = (T(1) - trans) * lev_up + T(2) * fact * (lay - lev_up);
+    const double fact = (tl > 0. && (tl * tl) > eps) ? (1. - trans) / tl - trans : tl * (0.5 - 1. / 3. * tl);
+    src_dn = (1. - trans) * lev_dn + 2. * fact * (lay - lev_dn);
+    src_up = (1. - trans) * lev_up + 2. * fact * (lay - lev_up);
+}
+
+template <>
+__device__ __forceinline__ void lw_layer<float>(float tau, float D, float lay, float lev_dn, float lev_up,
+                                               float& trans, float& src_dn, float& src_up)
+{
+    const float tl = tau * D;
+    const float em1 = expm1f(-tl);
+    const float omt = -em1;  // 1 - trans
+    trans = 1.f + em1;
+    float fact;
+    if (tl < 0.1f) {
+        // tau/2 - tau^2/3 + tau^3/8 - tau^4/30 + tau^5/144 - tau^6/840
+        fact = tl * (0.5f + tl * (-1.f / 3.f + tl * (0.125f + tl * (-1.f / 30.f + tl * (1.f / 144.f - tl * (1.f / 840.f))))));
+    } else {
+        fact = omt / tl - trans;
+    }
+    src_dn = omt * lev_dn + 2.f * fact * (lay - lev_dn);
+    src_up = omt * lev_up + 2.f * fact * (lay - lev_up);
 }
 
 template <typename T> __device__ __forceinline__ T k_min_value();

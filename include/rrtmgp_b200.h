@@ -291,6 +291,27 @@ int rrtmgp_b200_rte_sw_f64(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1
         const double* inc_flux_dif, double* gpt_flux_up, double* gpt_flux_dn,
         double* gpt_flux_dir, void* workspace, size_t workspace_bytes, void* stream);
 
+/* Shortwave solver that allocates nothing and needs no workspace argument.  No counterpart
+ * in the reference.  It is for callers that cannot obtain device memory themselves -- for
+ * example a Fortran or C host model bound through this ABI whose device memory is owned by
+ * its OpenACC/OpenMP runtime or by a fixed memory plan, where an extra cudaMalloc is not
+ * available or would synchronise the device.  Same arguments and results as
+ * rrtmgp_b200_rte_sw_f32 minus the workspace; the scratch is a 16 MiB array compiled into
+ * this library, which every GPU that loads the library holds until the process exits.
+ * Limit: ncol * nlay * ngpt <= RRTMGP_B200_SW_STATIC_SCRATCH_MAX_ELEMS, else
+ * RRTMGP_B200_ERR_WORKSPACE and nothing is launched (split the columns into smaller calls).
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture.  All calls share the
+ * one array, so calls that overlap on the GPU (concurrent streams, or several host threads)
+ * race and must be serialised by the caller.  No slot of the scratch needs to start at zero:
+ * each call writes every slot it reads. */
+#define RRTMGP_B200_SW_STATIC_SCRATCH_MAX_ELEMS (1048576)
+int rrtmgp_b200_rte_sw_static_scratch_f32(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1,
+        const float* tau, const float* ssa, const float* g, const float* mu0,
+        const float* inc_flux_dir, const float* sfc_alb_dir, const float* sfc_alb_dif,
+        const float* inc_flux_dif, float* gpt_flux_up, float* gpt_flux_dn, float* gpt_flux_dir,
+        void* stream);
+
 /* ------------------------------------------------------------------------------------ */
 /* Flux reductions (src_cuda/Fluxes.cu:39-136; fluxes_kernels.cu:26-113)                 */
 /* ------------------------------------------------------------------------------------ */

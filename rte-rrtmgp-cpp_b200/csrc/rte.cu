@@ -6,6 +6,7 @@
 // shortwave adding recurrences use a caller workspace plus the output arrays themselves.
 #include <algorithm>
 #include <cfloat>
+#include <mutex>
 
 #include "common.cuh"
 #include "rte_device.cuh"
@@ -237,6 +238,62 @@ int rte_sw(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const T* tau, 
     return RRTMGP_B200_OK;
 }
 
+// Shortwave solver scratch for callers that cannot allocate device memory themselves.
+// Lives in this file-scope device array: RRTMGP_B200_SW_STATIC_SCRATCH_MAX_ELEMS entries per
+// workspace slice, four slices, i.e. 16 MiB that every GPU which loads this library keeps
+// until the process exits.  Host code must not hand the array's name to a kernel (on the host
+// it is only a stand-in); the device address is looked up once per device below.
+constexpr size_t kSwStaticElems = RRTMGP_B200_SW_STATIC_SCRATCH_MAX_ELEMS;
+static __device__ __align__(256) float g_sw_static_scratch[4 * kSwStaticElems];
+
+std::mutex g_sw_static_mu;
+float* g_sw_static_ptr[64] = {};
+
+// Device address of g_sw_static_scratch on the current device, resolved with
+// cudaGetSymbolAddress on the first call made with that device current.
+int sw_static_scratch(float** out)
+{
+    int dev = 0;
+    RB_CUDA(cudaGetDevice(&dev), "rte_sw_static_scratch: cudaGetDevice");
+    if (dev < 0 || dev >= 64) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "rte_sw_static_scratch: device ordinal >= 64");
+    std::lock_guard<std::mutex> lock(g_sw_static_mu);
+    if (!g_sw_static_ptr[dev]) {
+        void* p = nullptr;
+        RB_CUDA(cudaGetSymbolAddress(&p, g_sw_static_scratch), "rte_sw_static_scratch: cudaGetSymbolAddress");
+        g_sw_static_ptr[dev] = static_cast<float*>(p);
+    }
+    *out = g_sw_static_ptr[dev];
+    return RRTMGP_B200_OK;
+}
+
+int rte_sw_static(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const float* tau, const float* ssa,
+                  const float* g, const float* mu0, const float* inc_dir, const float* alb_dir,
+                  const float* alb_dif, const float* inc_dif, float* flux_up, float* flux_dn, float* flux_dir,
+                  void* stream)
+{
+    RB_CHECK_ARG(b, "rte_sw_static_scratch: null bands");
+    RB_CHECK_ARG(ncol > 0 && nlay > 0, "rte_sw_static_scratch: ncol and nlay must be > 0");
+    const size_t elems = size_t(ncol) * nlay * b->ngpt;
+    if (elems > kSwStaticElems)
+        return fail(RRTMGP_B200_ERR_WORKSPACE,
+                    "rte_sw_static_scratch: ncol*nlay*ngpt = " + std::to_string(elems) + " exceeds the built-in "
+                    "scratch of " + std::to_string(kSwStaticElems) + " elements; split the columns or use rte_sw_f32");
+    RB_CHECK_ARG(tau && ssa && g && mu0 && inc_dir && alb_dir && alb_dif && flux_up && flux_dn && flux_dir,
+                 "rte_sw_static_scratch: null array");
+    float* ws = nullptr;
+    const int st = sw_static_scratch(&ws);
+    if (st != RRTMGP_B200_OK) return st;
+    // The kernel reads the four slices with a stride of ncol*nlay*ngpt, so the slices are
+    // packed at that stride inside the static array; every slot is written before it is read
+    // within the call, so nothing needs clearing.
+    const dim3 grid(ceil_div(ncol, 64), b->ngpt);
+    sw_solver_kernel<float, double><<<grid, 64, 0, as_stream(stream)>>>(
+        ncol, nlay, b->ngpt, b->nband, top_at_1, b->d_gpt2band, tau, ssa, g, mu0, inc_dir, alb_dir, alb_dif,
+        inc_dif, flux_up, flux_dn, flux_dir, ws);
+    RB_LAUNCH("sw_solver_kernel (static scratch)");
+    return RRTMGP_B200_OK;
+}
+
 }  // namespace
 }  // namespace rrtmgp_b200
 
@@ -266,5 +323,10 @@ int rrtmgp_b200_rte_sw_f64(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1
         const double* sfc_alb_dir, const double* sfc_alb_dif, const double* inc_flux_dif, double* up,
         double* dn, double* dir, void* ws, size_t ws_bytes, void* s)
 { return rte_sw<double>(b, ncol, nlay, top_at_1, tau, ssa, g, mu0, inc_flux_dir, sfc_alb_dir, sfc_alb_dif, inc_flux_dif, up, dn, dir, ws, ws_bytes, s); }
+
+int rrtmgp_b200_rte_sw_static_scratch_f32(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const float* tau,
+        const float* ssa, const float* g, const float* mu0, const float* inc_flux_dir, const float* sfc_alb_dir,
+        const float* sfc_alb_dif, const float* inc_flux_dif, float* up, float* dn, float* dir, void* s)
+{ return rte_sw_static(b, ncol, nlay, top_at_1, tau, ssa, g, mu0, inc_flux_dir, sfc_alb_dir, sfc_alb_dif, inc_flux_dif, up, dn, dir, s); }
 
 }  // extern "C"

@@ -344,6 +344,23 @@ int rrtmgp_b200_heating_rate_f32(int ncol, int nlay, const float* flux_up, const
 int rrtmgp_b200_heating_rate_f64(int ncol, int nlay, const double* flux_up,
         const double* flux_dn, const double* plev, double* heating_rate, void* stream);
 
+/* ------------------------------------------------------------------------------------ */
+/* Fused column forward (FP32 product path)                                              */
+/* ------------------------------------------------------------------------------------ */
+/* Longwave column forward: the sequence of Radiation_solver_longwave::solve_gpu
+ * (src_test/Radiation_solver.cu:467-615) -- gas_optics, cloud_optics (1scl, added by band;
+ * skipped when cloud is NULL), rte_lw (one angle) and Fluxes_broadband::reduce -- plus heating
+ * rates, in one kernel that keeps every (layer, g-point) quantity on chip.  Outputs
+ * flux_up, flux_dn, flux_net (ncol, nlay+1) and heating_rate (ncol, nlay) [K/day].  The
+ * vertical orientation is taken per column from play.  chunk: layers per warp (8 or 16;
+ * 0 picks the tuned default).  nlay <= 16 * chunk. */
+int rrtmgp_b200_forward_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int ncol, int nlay,
+        const float* play, const float* plev, const float* tlay, const float* tlev,
+        const float* tsfc, const float* col_dry, const rrtmgp_b200_gas_conc* gases, int ngases,
+        const float* lwp, const float* iwp, const float* rel, const float* rei,
+        const float* sfc_emis, float* flux_up, float* flux_dn, float* flux_net,
+        float* heating_rate, int chunk, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

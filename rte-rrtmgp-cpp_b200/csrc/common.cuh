@@ -67,6 +67,11 @@ struct KdistView {
     const int* band_minor_list[2];  // intervals overlapping each band
     const T* kminor[2];             // [ntemp][neta][ncontrib]
     int minor_in_band;              // every interval lies inside one band
+    // Fused-kernel metadata: g-points are processed in groups of 32 (one per lane).
+    int ngroups;                    // ceil(ngpt / 32)
+    int max_group_bands;            // most bands touched by one group
+    int max_band_minor;             // most minor intervals in one (band, atmosphere)
+    const int* group_band0;         // [ngroups] first band of each group
 };
 
 }  // namespace rrtmgp_b200

@@ -190,11 +190,25 @@ int fill_view(rrtmgp_b200_kdist_t* k, KdistView<T>& v, const rrtmgp_b200_kdist_t
         kmin[atm] = conv<T>(m.kminor.data(), m.kminor.size());
         a.add(kmin[atm], &v.kminor[atm]);
     }
-    int in_band = 1;
-    for (int atm = 0; atm < 2; ++atm)
+    int in_band = 1, max_minor = 0;
+    for (int atm = 0; atm < 2; ++atm) {
         for (size_t i = 0; i < mh[atm].gstart.size(); ++i)
             if (g2b[mh[atm].gstart[i]] != g2b[mh[atm].gend[i] - 1]) in_band = 0;
+        for (int b = 0; b < t->nband; ++b)
+            max_minor = std::max(max_minor, mh[atm].band_begin[b + 1] - mh[atm].band_begin[b]);
+    }
     v.minor_in_band = in_band;
+    v.max_band_minor = max_minor;
+    v.ngroups = (t->ngpt + 31) / 32;
+    std::vector<int> gb0(v.ngroups);
+    int max_gb = 0;
+    for (int gg = 0; gg < v.ngroups; ++gg) {
+        const int g0 = 32 * gg, g1 = std::min(t->ngpt, g0 + 32) - 1;
+        gb0[gg] = g2b[g0];
+        max_gb = std::max(max_gb, g2b[g1] - g2b[g0] + 1);
+    }
+    v.max_group_bands = max_gb;
+    a.add(gb0, &v.group_band0);
     return a.upload(k->allocations);
 }
 

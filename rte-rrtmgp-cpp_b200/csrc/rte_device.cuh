@@ -63,6 +63,24 @@ __device__ __forceinline__ void lw_layer<float>(float tau, float D, float lay, f
     src_up = omt * lev_up + 2.f * fact * (lay - lev_up);
 }
 
+// FP32 layer terms for the fused kernels: returns omt = 1 - T (accurate for thin layers)
+// and the two sources, with the same arithmetic as lw_layer<float>.
+__device__ __forceinline__ void lw_layer_omt(float tau, float D, float lay, float lev_dn, float lev_up,
+                                             float& omt, float& src_dn, float& src_up)
+{
+    const float tl = tau * D;
+    const float em1 = expm1f(-tl);
+    omt = -em1;
+    const float trans = 1.f + em1;
+    float fact;
+    if (tl < 0.1f)
+        fact = tl * (0.5f + tl * (-1.f / 3.f + tl * (0.125f + tl * (-1.f / 30.f + tl * (1.f / 144.f - tl * (1.f / 840.f))))));
+    else
+        fact = omt / tl - trans;
+    src_dn = omt * lev_dn + 2.f * fact * (lay - lev_dn);
+    src_up = omt * lev_up + 2.f * fact * (lay - lev_up);
+}
+
 template <typename T> __device__ __forceinline__ T k_min_value();
 template <> __device__ __forceinline__ float k_min_value<float>() { return 1.e-4f; }
 template <> __device__ __forceinline__ double k_min_value<double>() { return 1.e-12; }

@@ -131,6 +131,43 @@ class Radiation_solver:
         return {k: b[k] for k in ("flux_up", "flux_dn", "flux_dn_dir", "flux_net", "heating_rate")}
 
 
+class Fused_solver:
+    """FP32 column forward through the fused kernels (rrtmgp_b200_forward_lw_f32 / _sw_f32):
+    same inputs and outputs as Radiation_solver.solve_lw / solve_sw, no g-point arrays."""
+
+    def __init__(self, base: Radiation_solver, chunk: int = 0):
+        self.base = base
+        self.chunk = chunk
+        self._out = {}
+
+    def _outputs(self, kind, like, ncol, nlay):
+        key = (kind, ncol, nlay, like.device)
+        o = self._out.get(key)
+        if o is None:
+            o = {k: torch.empty((nlay + 1, ncol), dtype=torch.float32, device=like.device)
+                 for k in ("flux_up", "flux_dn", "flux_net", "flux_dn_dir")}
+            o["heating_rate"] = torch.empty((nlay, ncol), dtype=torch.float32, device=like.device)
+            self._out[key] = o
+        return o
+
+    def solve_lw(self, atm: dict, with_clouds: bool = True):
+        from . import _abi
+        play = atm["play"]
+        assert play.dtype == torch.float32, "the fused path is FP32"
+        nlay, ncol = play.shape
+        o = self._outputs("lw", play, ncol, nlay)
+        P = api._ptr
+        arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay)
+        c = self.base.clw if (with_clouds and self.base.clw is not None) else None
+        _abi.check(_abi.load().rrtmgp_b200_forward_lw_f32(
+            self.base.klw.handle, c.handle if c else None, ncol, nlay, P(play), P(atm["plev"]), P(atm["tlay"]),
+            P(atm["tlev"]), P(atm["tsfc"]), None, arr, len(atm["gases"]),
+            P(atm["lwp"]) if c else None, P(atm["iwp"]) if c else None, P(atm["rel"]) if c else None,
+            P(atm["rei"]) if c else None, P(atm["emis_sfc"]), P(o["flux_up"]), P(o["flux_dn"]), P(o["flux_net"]),
+            P(o["heating_rate"]), int(self.chunk), api._stream()))
+        return {k: o[k] for k in ("flux_up", "flux_dn", "flux_net", "heating_rate")}
+
+
 def atm_to_device(atm: dict, dtype, device):
     """Convert a synthetic atmosphere (numpy, rrtmgp_b200.synthetic layout) to torch."""
     out = {}

@@ -72,6 +72,18 @@ struct KdistView {
     int max_group_bands;            // most bands touched by one group
     int max_band_minor;             // most minor intervals in one (band, atmosphere)
     const int* group_band0;         // [ngroups] first band of each group
+    // Corner-packed copies for the fused FP32 kernels (NULL in the FP64 view):
+    //   kmaj4/pfrac4 [t][p][eta][g], p < npres, eta < neta-1: (k(e,p), k(e+1,p), k(e,p+1), k(e+1,p+1))
+    //   kmin2[a]     [t][eta][c], eta < neta-1: (k(e), k(e+1))
+    //   krayl2       [a][t][eta][g], eta < neta-1: (k(e), k(e+1))
+    //   minor_g[a]   [g]: x = number of intervals covering g (<= 3), y/z/w = (c << 4) | slot,
+    //                slot = position of the interval in its band's list, c = contributor.
+    const float4* kmaj4;
+    const float4* pfrac4;
+    const float2* kmin2[2];
+    const float2* krayl2;
+    const int4* minor_g[2];
+    int max_minor_per_g;            // most intervals covering one g-point (fused kernels: <= 3)
 };
 
 }  // namespace rrtmgp_b200

@@ -3,48 +3,24 @@
 // (ncol, nlay, ngpt) array.  The staged equivalent is the sequence of
 // Radiation_solver_longwave::solve_gpu (src_test/Radiation_solver.cu:467-615).
 //
-// Mapping: one CTA per column.  Lane l of every warp handles g-point 32*group + l, so the
-// table gathers of a warp are two contiguous 64-byte runs (one per band).  Warp w owns the
-// layer chunk [w*CL, (w+1)*CL) (counted from the top of the atmosphere).  For each group of
-// 32 g-points:
-//   1. each warp builds one record per (layer, band) of its chunk in shared memory: table
-//      offsets and interpolation weights (interpolation_kernel), minor-absorber scalings,
-//      band Planck functions and the cloud optical depth;
-//   2. pass 1: per (layer, g-point) tau, Planck fraction, transmissivity and the two
+// Per group of 32 g-points (see fused_common.cuh for the thread mapping):
+//   1. each warp writes the records of its layer chunk;
+//   2. pass 1: per (layer, g-point) tau, Planck fraction, 1 - transmissivity and the two
 //      linear-in-tau sources (lw_solver_noscat step 1) stay in registers; the warp composes
 //      its chunk's affine down and up maps x -> A x + B and publishes them;
 //   3. after one barrier every thread composes the maps of the other chunks to get its
-//      chunk's incoming down and up radiances (the surface term is the reference's
-//      radn_dn * (1 - emis) + emis * sfc_src);
-//   4. pass 2 re-sweeps the registers, producing the level radiances and the per-layer
-//      absorbed radiance omt * (I_dn(top) + I_up(bottom)) - S_dn - S_up, which gives heating
-//      rates without differencing two nearly equal level fluxes;
+//      chunk's incoming down and up radiances (surface: radn_dn * (1 - emis) + emis * sfc_src);
+//   4. pass 2 re-sweeps the registers: level radiances and the per-layer absorbed radiance
+//      omt * (I_dn(top) + I_up(bottom)) - S_dn - S_up, which gives heating rates without
+//      differencing two nearly equal FP32 level fluxes;
 //   5. a warp reduce-scatter (31 shuffles per 32 values) sums over the 32 g-points and every
 //      lane accumulates one level (or layer) in FP64.
-#include <cfloat>
-#include <cmath>
-
-#include "common.cuh"
-#include "rte_device.cuh"
+#include "fused_common.cuh"
 
 namespace rrtmgp_b200 {
 namespace {
 
-constexpr int kMaxMinor = 6;
-
-struct LwRec {
-    int kb0, kb1;        // offsets of corners (t0, p0, e0) and (t1, p0, e1) in [t][p][eta][g]
-    int r0, r2;          // kminor row offsets of (t0, e0) and (t1, e1) in [t][eta][c]
-    int nmin, nc;        // minor intervals in this (band, atmosphere), contributors
-    int mgs[kMaxMinor], mge[kMaxMinor], mks[kMaxMinor];
-    int a, pad;
-    float wmaj[8];       // col_mix x fmajor
-    float wpl[8];        // fmajor (Planck fractions)
-    float fm[4];         // fminor
-    float scal[kMaxMinor];
-    float pl_lay, pl_top, pl_bot, pl_sfc, tau_cld;
-    float pad2[3];
-};
+using namespace fused;
 
 struct CloudArgs {
     CloudLut<float> L;
@@ -55,87 +31,38 @@ struct CloudArgs {
     int present;
 };
 
-// Reduce-scatter of N per-lane values over the 32 lanes: afterwards lane L holds in v[0] the
-// warp total of value L >> log2(32/N) (N <= 32).
-template <int N, int OFF>
-struct ReduceScatter {
-    static __device__ __forceinline__ void run(float* v, int lane)
-    {
-        constexpr int H = N / 2;
-        const bool upper = (lane & OFF) != 0;
-#pragma unroll
-        for (int i = 0; i < H; ++i) {
-            const float send = upper ? v[i] : v[i + H];
-            const float keep = upper ? v[i + H] : v[i];
-            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, OFF);
-        }
-        ReduceScatter<H, OFF / 2>::run(v, lane);
-    }
-};
-template <int OFF>
-struct ReduceScatter<1, OFF> {
-    static __device__ __forceinline__ void run(float* v, int lane)
-    {
-        v[0] += __shfl_xor_sync(0xffffffffu, v[0], OFF);
-        ReduceScatter<1, OFF / 2>::run(v, lane);
-    }
-};
-template <>
-struct ReduceScatter<1, 0> {
-    static __device__ __forceinline__ void run(float*, int) {}
-};
-
-__device__ __forceinline__ void build_record(const KdistView<float>& k, LwRec& R, int jj, int b, int nlay,
-                                             const int* sm_i, const float* sm_f, const float* sm_cg,
-                                             const float* sm_cld, float tsfc)
+// Layer transmissivity complement and sources in FP32: series below tau = 0.1 (7 and 6 terms,
+// truncation < 2e-11 relative), exp/divide intrinsics above where no cancellation occurs.
+// Same physics as lw_solver_noscat_step_1_kernel (rte_solver_kernels.cu:116-125).
+__device__ __forceinline__ void lw_layer_fast(float tau, float D, float lay, float ldn, float lup, float& omt,
+                                              float& sdn, float& sup)
 {
-    LayerInterp<float> li;
-    li.jt = sm_i[4 * jj + 0];
-    li.jp = sm_i[4 * jj + 1];
-    li.itropo = sm_i[4 * jj + 2];
-    li.ftemp = sm_f[8 * jj + 0];
-    li.fpress = sm_f[8 * jj + 1];
-    const float p = sm_f[8 * jj + 2], t = sm_f[8 * jj + 3];
-    const float* cg = sm_cg + jj;
-    const int flav = k.band_flav[2 * b + li.itropo];
-    const FlavorWeights<float> fw = flavor_weights(k, flav, li, cg, nlay);
-    const MajorCorners<float> mc = major_corners(k, k.kmajor, li, fw);
-    R.kb0 = int(mc.c[0] - k.kmajor);
-    R.kb1 = int(mc.c[4] - k.kmajor);
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        R.wmaj[q] = fw.cm[q / 4] * mc.fmaj[q];
-        R.wpl[q] = mc.fmaj[q];
+    const float tl = tau * D;
+    float fact;
+    if (tl < 0.1f) {
+        omt = tl * (1.f + tl * (-0.5f + tl * (1.f / 6.f + tl * (-1.f / 24.f + tl * (1.f / 120.f +
+              tl * (-1.f / 720.f + tl * (1.f / 5040.f)))))));
+        fact = tl * (0.5f + tl * (-1.f / 3.f + tl * (0.125f + tl * (-1.f / 30.f + tl * (1.f / 144.f -
+               tl * (1.f / 840.f))))));
+    } else {
+        const float trans = __expf(-tl);
+        omt = 1.f - trans;
+        fact = __fdividef(omt, tl) - trans;
     }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) R.fm[q] = fw.fm[q];
-    const int a = li.itropo;
-    const int nc = k.ncontrib[a];
-    R.a = a;
-    R.nc = nc;
-    R.r0 = ((li.jt - 1) * k.neta + fw.j0 - 1) * nc;
-    R.r2 = (li.jt * k.neta + fw.j1 - 1) * nc;
-    int n = 0;
-    for (int ii = k.band_minor_begin[a][b]; ii < k.band_minor_begin[a][b + 1] && n < kMaxMinor; ++ii, ++n) {
-        const int im = k.band_minor_list[a][ii];
-        R.scal[n] = minor_scaling(k, a, im, cg, nlay, p, t);
-        R.mgs[n] = k.minor_gstart[a][im];
-        R.mge[n] = k.minor_gend[a][im];
-        R.mks[n] = k.minor_kstart[a][im];
-    }
-    R.nmin = n;
-    const float* tp = k.totplnk + size_t(b) * k.nplanck;
-    R.pl_lay = interpolate1D(t, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp);
-    R.pl_top = interpolate1D(sm_f[8 * jj + 4], k.temp_ref_min, k.totplnk_delta, k.nplanck, tp);
-    R.pl_bot = interpolate1D(sm_f[8 * jj + 5], k.temp_ref_min, k.totplnk_delta, k.nplanck, tp);
-    R.pl_sfc = (jj == nlay - 1) ? interpolate1D(tsfc, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp) : 0.f;
-    R.tau_cld = sm_cld ? sm_cld[b * nlay + jj] : 0.f;
+    sdn = omt * ldn + 2.f * fact * (lay - ldn);
+    sup = omt * lup + 2.f * fact * (lay - lup);
 }
 
-// Word offset of the chunk-map area, rounded up to 4 words so that it is float4 aligned.
-__host__ __device__ __forceinline__ int lw_maps_offset(int nlay, int ngas, int nband)
+__device__ __forceinline__ void build_lw_record(const KdistView<float>& k, Rec& R, const LayerState& s,
+                                                const float* cg, int nlay, int b, float tau_cld, bool bottom,
+                                                float tsfc)
 {
-    return ((12 + ngas + 1 + nband) * nlay + 3) & ~3;
+    record_weights(k, R, s, cg, nlay, b);
+    const float* tp = k.totplnk + size_t(b) * k.nplanck;
+    R.aux = make_float4(interpolate1D(s.t, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp),
+                        interpolate1D(s.t_top, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp),
+                        interpolate1D(s.t_bot, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp), tau_cld);
+    R.pl_sfc = bottom ? interpolate1D(tsfc, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp) : 0.f;
 }
 
 template <int CL>
@@ -153,40 +80,17 @@ lw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const CloudA
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int NW = blockDim.x >> 5;
     const int nband = k.nband;
-
-    // Shared memory carve-up (4-byte words).
-    int* sm_i = reinterpret_cast<int*>(smem_raw);                 // [nlay][4]: jt, jp, itropo
-    float* sm_f = reinterpret_cast<float*>(sm_i + 4 * nlay);      // [nlay][8]: ftemp, fpress, p, t, Ttop, Tbot, dp
-    float* sm_cg = sm_f + 8 * nlay;                               // [ngas+1][nlay]
-    float* sm_cld = sm_cg + (k.ngas + 1) * nlay;                  // [nband][nlay]
-    float* sm_maps = reinterpret_cast<float*>(smem_raw) + lw_maps_offset(nlay, k.ngas, nband);  // [NW][32][4]
-    float* sm_sfc = sm_maps + NW * 32 * 4;                        // [32]
-    LwRec* recs = reinterpret_cast<LwRec*>(sm_sfc + 32);
-    const int nrec_w = CL * k.max_group_bands;
-    LwRec* myrecs = recs + w * nrec_w;
+    const SmemLayout SL = smem_layout(nlay, k.ngas, nband, 1, NW, 1, CL, k.max_group_bands);
+    LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
+    float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
+    float* sm_cld = reinterpret_cast<float*>(smem_raw + SL.cloud);
+    float4* sm_maps = reinterpret_cast<float4*>(smem_raw + SL.maps);
+    float* sm_sfc = reinterpret_cast<float*>(smem_raw + SL.sfc);
+    Rec* recs = reinterpret_cast<Rec*>(smem_raw + SL.recs) + w * CL * k.max_group_bands;
 
     const bool top_at_1 = play[icol] < play[icol + size_t(nlay - 1) * ncol];
     const float ts = tsfc[icol];
-
-    // Per-layer state, layers counted from the top (j).
-    for (int j = threadIdx.x; j < nlay; j += blockDim.x) {
-        const int l = top_at_1 ? j : nlay - 1 - j;
-        const size_t cl = icol + size_t(l) * ncol;
-        const float p = play[cl], t = tlay[cl];
-        fill_col_gas(k, gs, ncol, nlay, icol, l, plev, col_dry_in, sm_cg + j, nlay);
-        const LayerInterp<float> li = layer_interp(k, p, t);
-        sm_i[4 * j + 0] = li.jt;
-        sm_i[4 * j + 1] = li.jp;
-        sm_i[4 * j + 2] = li.itropo;
-        const int lt = top_at_1 ? j : nlay - j, lb = top_at_1 ? j + 1 : nlay - 1 - j;
-        sm_f[8 * j + 0] = li.ftemp;
-        sm_f[8 * j + 1] = li.fpress;
-        sm_f[8 * j + 2] = p;
-        sm_f[8 * j + 3] = t;
-        sm_f[8 * j + 4] = tlev[icol + size_t(lt) * ncol];
-        sm_f[8 * j + 5] = tlev[icol + size_t(lb) * ncol];
-        sm_f[8 * j + 6] = fabsf(plev[icol + size_t(lb) * ncol] - plev[icol + size_t(lt) * ncol]);
-    }
+    setup_layers(k, gs, ncol, nlay, icol, top_at_1, play, plev, tlay, tlev, col_dry_in, st, sm_cg);
     for (int idx = threadIdx.x; idx < nlay * nband; idx += blockDim.x) {
         const int j = idx % nlay, b = idx / nlay;
         float tau = 0.f, s, g;
@@ -202,7 +106,6 @@ lw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const CloudA
 
     const float D = 1.66f;                 // single-angle secant (Rte_lw.cpp:101-113)
     const int ngpt = k.ngpt;
-    const int o1 = ngpt, o2 = k.neta * ngpt, o3 = o2 + ngpt;
     double acc_lev = 0.0, acc_div = 0.0, acc_bot_up = 0.0, acc_bot_dn = 0.0;
 
     for (int gg = 0; gg < k.ngroups; ++gg) {
@@ -211,17 +114,19 @@ lw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const CloudA
         const int b0 = k.group_band0[gg];
         const int gband = gv ? k.gpt2band[g] : b0;
         const int slot = gband - b0;
+        const int4 mg0 = gv ? __ldg(k.minor_g[0] + g) : make_int4(0, 0, 0, 0);
+        const int4 mg1 = gv ? __ldg(k.minor_g[1] + g) : make_int4(0, 0, 0, 0);
 
         // 1. records of this warp's chunk
-        for (int r = lane; r < nrec_w; r += 32) {
+        for (int r = lane; r < CL * k.max_group_bands; r += 32) {
             const int jj = w * CL + (r % CL);
             const int b = b0 + r / CL;
             if (jj < nlay && b < nband && k.band_lims[2 * b] < 32 * gg + 32)
-                build_record(k, myrecs[r], jj, b, nlay, sm_i, sm_f, sm_cg, sm_cld, ts);
+                build_lw_record(k, recs[r], st[jj], sm_cg + jj, nlay, b, sm_cld[b * nlay + jj], jj == nlay - 1, ts);
         }
         __syncwarp();
 
-        // 2. pass 1: optical properties and sources in registers, chunk maps
+        // 2. pass 1
         float omt[CL], sdn[CL], sup[CL];
         float Ad = 1.f, Bd = 0.f;
 #pragma unroll
@@ -229,28 +134,13 @@ lw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const CloudA
             const int j = w * CL + i;
             omt[i] = 0.f; sdn[i] = 0.f; sup[i] = 0.f;
             if (j < nlay && gv) {
-                const LwRec& R = myrecs[slot * CL + i];
-                const float* KM = k.kmajor;
-                float tau = R.wmaj[0] * __ldg(KM + R.kb0 + g) + R.wmaj[1] * __ldg(KM + R.kb0 + o1 + g) +
-                            R.wmaj[2] * __ldg(KM + R.kb0 + o2 + g) + R.wmaj[3] * __ldg(KM + R.kb0 + o3 + g) +
-                            R.wmaj[4] * __ldg(KM + R.kb1 + g) + R.wmaj[5] * __ldg(KM + R.kb1 + o1 + g) +
-                            R.wmaj[6] * __ldg(KM + R.kb1 + o2 + g) + R.wmaj[7] * __ldg(KM + R.kb1 + o3 + g);
-                const float* KN = k.kminor[R.a];
-                for (int n = 0; n < R.nmin; ++n) {
-                    if (g >= R.mgs[n] && g < R.mge[n]) {
-                        const int c = R.mks[n] + g - R.mgs[n];
-                        tau += R.scal[n] * (R.fm[0] * __ldg(KN + R.r0 + c) + R.fm[1] * __ldg(KN + R.r0 + R.nc + c) +
-                                            R.fm[2] * __ldg(KN + R.r2 + c) + R.fm[3] * __ldg(KN + R.r2 + R.nc + c));
-                    }
-                }
-                tau += R.tau_cld;
-                const float* PF = k.planck_frac;
-                const float pfrac =
-                    (R.wpl[0] * __ldg(PF + R.kb0 + g) + R.wpl[1] * __ldg(PF + R.kb0 + o1 + g) +
-                     R.wpl[2] * __ldg(PF + R.kb0 + o2 + g) + R.wpl[3] * __ldg(PF + R.kb0 + o3 + g)) +
-                    (R.wpl[4] * __ldg(PF + R.kb1 + g) + R.wpl[5] * __ldg(PF + R.kb1 + o1 + g) +
-                     R.wpl[6] * __ldg(PF + R.kb1 + o2 + g) + R.wpl[7] * __ldg(PF + R.kb1 + o3 + g));
-                lw_layer_omt(tau, D, pfrac * R.pl_lay, pfrac * R.pl_bot, pfrac * R.pl_top, omt[i], sdn[i], sup[i]);
+                const Rec& R = recs[slot * CL + i];
+                const float tau = tau_abs(k, R, g, R.a ? mg1 : mg0) + R.aux.w;
+                const float4 p0 = __ldg(k.pfrac4 + size_t(R.kb.x) * ngpt + g);
+                const float4 p1 = __ldg(k.pfrac4 + size_t(R.kb.y) * ngpt + g);
+                const float pfrac = (R.wpl0.x * p0.x + R.wpl0.y * p0.y + R.wpl0.z * p0.z + R.wpl0.w * p0.w) +
+                                    (R.wpl1.x * p1.x + R.wpl1.y * p1.y + R.wpl1.z * p1.z + R.wpl1.w * p1.w);
+                lw_layer_fast(tau, D, pfrac * R.aux.x, pfrac * R.aux.z, pfrac * R.aux.y, omt[i], sdn[i], sup[i]);
                 if (j == nlay - 1) sm_sfc[lane] = pfrac * R.pl_sfc;
             } else if (j == nlay - 1) {
                 sm_sfc[lane] = 0.f;
@@ -264,26 +154,25 @@ lw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const CloudA
             Au = (1.f - omt[i]) * Au;
             Bu = (1.f - omt[i]) * Bu + sup[i];
         }
-        reinterpret_cast<float4*>(sm_maps)[w * 32 + lane] = make_float4(Ad, Bd, Au, Bu);
+        sm_maps[w * 32 + lane] = make_float4(Ad, Bd, Au, Bu);
         __syncthreads();
 
-        // 3. incoming radiances of the chunk
-        float x = 0.f;  // no incident longwave flux at the top
-        float xin = 0.f;
+        // 3. incoming radiances of the chunk (no incident longwave flux at the top)
+        float x = 0.f, xin = 0.f;
         for (int c = 0; c < NW; ++c) {
             if (c == w) xin = x;
-            const float4 m = reinterpret_cast<const float4*>(sm_maps)[c * 32 + lane];
+            const float4 m = sm_maps[c * 32 + lane];
             x = m.x * x + m.y;
         }
-        const float emis = gv ? sfc_emis[gband + size_t(icol) * nband] : 0.f;
+        const float emis = gv ? __ldg(sfc_emis + gband + size_t(icol) * nband) : 0.f;
         const float S = x * (1.f - emis) + emis * sm_sfc[lane];
         float y = S;
         for (int c = NW - 1; c > w; --c) {
-            const float4 m = reinterpret_cast<const float4*>(sm_maps)[c * 32 + lane];
+            const float4 m = sm_maps[c * 32 + lane];
             y = m.z * y + m.w;
         }
 
-        // 4. pass 2: level radiances and layer absorption
+        // 4. pass 2
         float v[2 * CL], dv[CL];
         float rd = xin;
 #pragma unroll
@@ -304,19 +193,13 @@ lw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const CloudA
         acc_lev += double(v[0]);
         acc_div += double(dv[0]);
         if (w == NW - 1) {
-            float bu = S, bd = rd;
-#pragma unroll
-            for (int off = 16; off >= 1; off >>= 1) {
-                bu += __shfl_xor_sync(0xffffffffu, bu, off);
-                bd += __shfl_xor_sync(0xffffffffu, bd, off);
-            }
-            acc_bot_up += double(bu);
-            acc_bot_dn += double(bd);
+            acc_bot_up += double(warp_sum(S));
+            acc_bot_dn += double(warp_sum(rd));
         }
         __syncthreads();
     }
 
-    // Outputs.  Fluxes = 2 pi w * sum of radiances with w = 0.5.
+    // Outputs.  Fluxes = 2 pi w * (sum of radiances) with w = 0.5.
     const double pi = 3.14159265358979323846;
     constexpr int SH_LEV = (CL == 16) ? 0 : 1;   // lane L holds value L >> SH_LEV
     constexpr int SH_DIV = (CL == 16) ? 1 : 2;
@@ -338,7 +221,7 @@ lw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const CloudA
         if (jl < nlay && (lane >> SH_DIV) < CL) {
             const int l = top_at_1 ? jl : nlay - 1 - jl;
             const double g0_cp = 9.80665 / 1004.64;
-            heating_rate[icol + size_t(l) * ncol] = float(g0_cp * 86400.0 * pi * acc_div / double(sm_f[8 * jl + 6]));
+            heating_rate[icol + size_t(l) * ncol] = float(g0_cp * 86400.0 * pi * acc_div / double(st[jl].dp));
         }
     }
     if (w == NW - 1 && lane == 0) {
@@ -351,14 +234,6 @@ lw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const CloudA
 }
 
 template <int CL>
-size_t lw_forward_smem(const KdistView<float>& v, int nlay)
-{
-    const int NW = (nlay + CL - 1) / CL;
-    return sizeof(float) * (size_t(lw_maps_offset(nlay, v.ngas, v.nband)) + NW * 32 * 4 + 32) +
-           sizeof(LwRec) * size_t(NW) * CL * v.max_group_bands;
-}
-
-template <int CL>
 int launch_lw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay, const float* play,
                       const float* plev, const float* tlay, const float* tlev, const float* tsfc, const float* col_dry,
                       const GasSet<float>& gs, const float* lwp, const float* iwp, const float* rel, const float* rei,
@@ -367,7 +242,7 @@ int launch_lw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
     const KdistView<float>& v = k->v32;
     const int NW = (nlay + CL - 1) / CL;
     RB_CHECK_ARG(NW <= 16, "forward_lw: nlay too large for the fused kernel (at most 16 chunks)");
-    const size_t smem = lw_forward_smem<CL>(v, nlay);
+    const size_t smem = smem_layout(nlay, v.ngas, v.nband, 1, NW, 1, CL, v.max_group_bands).total;
     if (smem > 220 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "forward_lw: shared memory need exceeds 220 KB");
     static bool attr = false;
     if (!attr) {
@@ -403,7 +278,7 @@ int forward_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     RB_CHECK_ARG(!c || (lwp && iwp && rel && rei), "forward_lw: cloud arrays required with a cloud handle");
     RB_CHECK_ARG(!c || c->nband == k->info.nband, "forward_lw: cloud and gas band counts differ");
     const KdistView<float>& v = k->v32;
-    if (!v.minor_in_band || v.max_band_minor > kMaxMinor || v.max_group_bands > 32 / 4)
+    if (!v.minor_in_band || v.max_band_minor > kMaxMinor || v.max_minor_per_g > 3 || v.max_group_bands > 8)
         return fail(RRTMGP_B200_ERR_UNSUPPORTED, "forward_lw: k-distribution layout not supported by the fused kernel");
     GasSet<float> gs;
     int st = make_gas_set<float>(k, ncol, nlay, gases, ngases, gs);

@@ -1,0 +1,193 @@
+// Building blocks shared by the fused FP32 column-forward kernels (longwave and shortwave).
+//
+// Mapping (both kernels): one CTA per column; lane l of every warp handles g-point
+// 32*group + l; warp w owns the layer chunk [w*CL, (w+1)*CL) counted from the top of the
+// atmosphere.  Per group of 32 g-points each warp first writes one record per (layer, band)
+// of its chunk to shared memory (table offsets and interpolation weights of
+// interpolation_kernel, minor scalings, band Planck values, cloud properties); the per
+// (layer, g-point) work then reads its record with 128-bit shared loads and the tables with
+// 128-bit corner-packed global loads (KdistView::kmaj4 & co.).
+#pragma once
+
+#include <cfloat>
+#include <cmath>
+
+#include "common.cuh"
+#include "rte_device.cuh"
+
+namespace rrtmgp_b200 {
+namespace fused {
+
+constexpr int kMaxMinor = 8;   // minor intervals per (band, atmosphere) held in a record
+
+// Per-layer state kept in shared memory for the whole kernel (layers counted from the top).
+struct __align__(16) LayerState {
+    int jt, jp, itropo, pad;
+    float ftemp, fpress, p, t;
+    float t_top, t_bot, dp, pad2;
+};
+
+// Per (layer, band) record.
+struct __align__(16) Rec {
+    int4 kb;          // x, y: packed kmaj4/pfrac4 rows of (t0, p0, e0) and (t1, p0, e1);
+                      // z, w: kmin2 rows of (t0, e0) and (t1, e1)
+    float4 wmaj0, wmaj1;   // col_mix x fmajor (major absorption weights)
+    float4 wpl0, wpl1;     // fmajor (Planck fractions; SW: unused)
+    float4 fm;             // fminor (minor and Rayleigh weights)
+    float4 aux;            // LW: pl_lay, pl_top, pl_bot, tau_cloud
+                           // SW: col_dry + col_h2o (Rayleigh), cloud tau, ssa, g
+    float scal[kMaxMinor]; // minor scaling of each interval in the band's list
+    float pl_sfc;          // LW surface Planck function (bottom layer only)
+    int a;                 // 0 lower / 1 upper atmosphere
+    int pad[2];
+};
+
+// Reduce-scatter of N per-lane values over 32 lanes: afterwards lane L holds in v[0] the warp
+// total of value L >> log2(32 / N) (N <= 32, a power of two).
+template <int N, int OFF>
+struct ReduceScatter {
+    static __device__ __forceinline__ void run(float* v, int lane)
+    {
+        constexpr int H = N / 2;
+        const bool upper = (lane & OFF) != 0;
+#pragma unroll
+        for (int i = 0; i < H; ++i) {
+            const float send = upper ? v[i] : v[i + H];
+            const float keep = upper ? v[i + H] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, OFF);
+        }
+        ReduceScatter<H, OFF / 2>::run(v, lane);
+    }
+};
+template <int OFF>
+struct ReduceScatter<1, OFF> {
+    static __device__ __forceinline__ void run(float* v, int lane)
+    {
+        v[0] += __shfl_xor_sync(0xffffffffu, v[0], OFF);
+        ReduceScatter<1, OFF / 2>::run(v, lane);
+    }
+};
+template <>
+struct ReduceScatter<1, 0> {
+    static __device__ __forceinline__ void run(float*, int) {}
+};
+
+__device__ __forceinline__ float warp_sum(float x)
+{
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+    return x;
+}
+
+// Interpolation part of a record (interpolation_kernel, gas_optics_rrtmgp_kernels.cu:256-291)
+// for band b at layer state s.
+__device__ __forceinline__ void record_weights(const KdistView<float>& k, Rec& R, const LayerState& s,
+                                               const float* cg, int cgs, int b)
+{
+    LayerInterp<float> li;
+    li.jt = s.jt;
+    li.jp = s.jp;
+    li.itropo = s.itropo;
+    li.ftemp = s.ftemp;
+    li.fpress = s.fpress;
+    const int flav = k.band_flav[2 * b + li.itropo];
+    const FlavorWeights<float> fw = flavor_weights(k, flav, li, cg, cgs);
+    const int ne1 = k.neta - 1, np = k.npres;
+    const int p0 = li.jp + li.itropo - 1;
+    R.kb.x = ((li.jt - 1) * np + p0) * ne1 + (fw.j0 - 1);
+    R.kb.y = (li.jt * np + p0) * ne1 + (fw.j1 - 1);
+    const int a = li.itropo;
+    const int nc = k.ncontrib[a] > 0 ? k.ncontrib[a] : 1;
+    R.kb.z = ((li.jt - 1) * ne1 + (fw.j0 - 1)) * nc;
+    R.kb.w = (li.jt * ne1 + (fw.j1 - 1)) * nc;
+    const float fp = li.fpress, f1 = 1.f - li.fpress;
+    R.wpl0 = make_float4(f1 * fw.fm[0], f1 * fw.fm[1], fp * fw.fm[0], fp * fw.fm[1]);
+    R.wpl1 = make_float4(f1 * fw.fm[2], f1 * fw.fm[3], fp * fw.fm[2], fp * fw.fm[3]);
+    R.wmaj0 = make_float4(fw.cm[0] * R.wpl0.x, fw.cm[0] * R.wpl0.y, fw.cm[0] * R.wpl0.z, fw.cm[0] * R.wpl0.w);
+    R.wmaj1 = make_float4(fw.cm[1] * R.wpl1.x, fw.cm[1] * R.wpl1.y, fw.cm[1] * R.wpl1.z, fw.cm[1] * R.wpl1.w);
+    R.fm = make_float4(fw.fm[0], fw.fm[1], fw.fm[2], fw.fm[3]);
+    R.a = a;
+    int n = 0;
+    for (int ii = k.band_minor_begin[a][b]; ii < k.band_minor_begin[a][b + 1] && n < kMaxMinor; ++ii, ++n)
+        R.scal[n] = minor_scaling(k, a, k.band_minor_list[a][ii], cg, cgs, s.p, s.t);
+}
+
+// Absorption optical depth of g-point g from a record: major (8 corners via two float4 loads)
+// plus the minor intervals covering g (minor_g list), as gas_optical_depths_major/minor.
+__device__ __forceinline__ float tau_abs(const KdistView<float>& k, const Rec& R, int g, int4 mg)
+{
+    const int ngpt = k.ngpt;
+    const float4 c0 = __ldg(k.kmaj4 + size_t(R.kb.x) * ngpt + g);
+    const float4 c1 = __ldg(k.kmaj4 + size_t(R.kb.y) * ngpt + g);
+    float tau = R.wmaj0.x * c0.x + R.wmaj0.y * c0.y + R.wmaj0.z * c0.z + R.wmaj0.w * c0.w +
+                R.wmaj1.x * c1.x + R.wmaj1.y * c1.y + R.wmaj1.z * c1.z + R.wmaj1.w * c1.w;
+    if (mg.x > 0) {
+        const float2* kn = k.kmin2[R.a];
+#pragma unroll
+        for (int n = 0; n < 3; ++n) {
+            if (n < mg.x) {
+                const int code = n == 0 ? mg.y : (n == 1 ? mg.z : mg.w);
+                const int c = code >> 4;
+                const float2 lo = __ldg(kn + R.kb.z + c);
+                const float2 hi = __ldg(kn + R.kb.w + c);
+                tau += R.scal[code & 15] * (R.fm.x * lo.x + R.fm.y * lo.y + R.fm.z * hi.x + R.fm.w * hi.y);
+            }
+        }
+    }
+    return tau;
+}
+
+// Fill the per-layer state of column icol (layers counted from the top) and col_gas.
+__device__ __forceinline__ void setup_layers(const KdistView<float>& k, const GasSet<float>& gs, int ncol,
+                                             int nlay, int icol, bool top_at_1, const float* __restrict__ play,
+                                             const float* __restrict__ plev, const float* __restrict__ tlay,
+                                             const float* __restrict__ tlev, const float* __restrict__ col_dry,
+                                             LayerState* st, float* cg)
+{
+    for (int j = threadIdx.x; j < nlay; j += blockDim.x) {
+        const int l = top_at_1 ? j : nlay - 1 - j;
+        const size_t cl = icol + size_t(l) * ncol;
+        const float p = play[cl], t = tlay[cl];
+        fill_col_gas(k, gs, ncol, nlay, icol, l, plev, col_dry, cg + j, nlay);
+        const LayerInterp<float> li = layer_interp(k, p, t);
+        const int lt = top_at_1 ? j : nlay - j, lb = top_at_1 ? j + 1 : nlay - 1 - j;
+        LayerState s;
+        s.jt = li.jt;
+        s.jp = li.jp;
+        s.itropo = li.itropo;
+        s.pad = 0;
+        s.ftemp = li.ftemp;
+        s.fpress = li.fpress;
+        s.p = p;
+        s.t = t;
+        s.t_top = tlev ? tlev[icol + size_t(lt) * ncol] : 0.f;
+        s.t_bot = tlev ? tlev[icol + size_t(lb) * ncol] : 0.f;
+        s.dp = fabsf(plev[icol + size_t(lb) * ncol] - plev[icol + size_t(lt) * ncol]);
+        s.pad2 = 0.f;
+        st[j] = s;
+    }
+}
+
+// Shared-memory offsets (bytes) of the fused kernels, all 16-byte aligned.
+struct SmemLayout {
+    size_t state, cg, cloud, maps, sfc, recs, total;
+};
+
+__host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+__host__ __device__ __forceinline__ SmemLayout smem_layout(int nlay, int ngas, int nband, int ncloud_vals, int NW,
+                                                           int nmaps, int CL, int nbands_per_group)
+{
+    SmemLayout L;
+    L.state = 0;
+    L.cg = align16(L.state + sizeof(LayerState) * size_t(nlay));
+    L.cloud = align16(L.cg + sizeof(float) * size_t(ngas + 1) * nlay);
+    L.maps = align16(L.cloud + sizeof(float) * size_t(ncloud_vals) * nband * nlay);
+    L.sfc = align16(L.maps + sizeof(float4) * size_t(NW) * 32 * nmaps);
+    L.recs = align16(L.sfc + sizeof(float) * 64);
+    L.total = align16(L.recs + sizeof(Rec) * size_t(NW) * CL * nbands_per_group);
+    return L;
+}
+
+}  // namespace fused
+}  // namespace rrtmgp_b200

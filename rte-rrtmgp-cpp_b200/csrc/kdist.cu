@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -209,6 +210,74 @@ int fill_view(rrtmgp_b200_kdist_t* k, KdistView<T>& v, const rrtmgp_b200_kdist_t
     }
     v.max_group_bands = max_gb;
     a.add(gb0, &v.group_band0);
+
+    // Corner-packed tables for the fused FP32 kernels.
+    v.max_minor_per_g = 0;
+    std::vector<float4> km4, pf4;
+    std::vector<float2> kn2[2], kr2;
+    std::vector<int4> mg[2];
+    if (std::is_same<T, float>::value) {
+        const int nt = t->ntemp, np = t->npres, np1 = t->npres + 1, ne = t->neta, ng = t->ngpt;
+        auto pack4 = [&](const double* src, std::vector<float4>& dst) {
+            dst.resize(size_t(nt) * np * (ne - 1) * ng);
+            auto at = [&](int it, int ip, int ie, int ig) { return float(src[((size_t(it) * np1 + ip) * ne + ie) * ng + ig]); };
+            for (int it = 0; it < nt; ++it)
+                for (int ip = 0; ip < np; ++ip)
+                    for (int ie = 0; ie < ne - 1; ++ie)
+                        for (int ig = 0; ig < ng; ++ig)
+                            dst[((size_t(it) * np + ip) * (ne - 1) + ie) * ng + ig] =
+                                make_float4(at(it, ip, ie, ig), at(it, ip, ie + 1, ig), at(it, ip + 1, ie, ig),
+                                            at(it, ip + 1, ie + 1, ig));
+        };
+        pack4(t->kmajor, km4);
+        if (t->planck_frac) pack4(t->planck_frac, pf4);
+        for (int atm = 0; atm < 2; ++atm) {
+            const MinorHost& m = mh[atm];
+            const int nc = std::max(m.ncontrib, 1);
+            kn2[atm].resize(size_t(nt) * (ne - 1) * nc);
+            for (int it = 0; it < nt; ++it)
+                for (int ie = 0; ie < ne - 1; ++ie)
+                    for (int c = 0; c < nc; ++c)
+                        kn2[atm][(size_t(it) * (ne - 1) + ie) * nc + c] =
+                            make_float2(float(m.kminor[(size_t(it) * ne + ie) * nc + c]),
+                                        float(m.kminor[(size_t(it) * ne + ie + 1) * nc + c]));
+            // Intervals covering each g-point, as (contributor, slot in the band's list).
+            mg[atm].assign(ng, make_int4(0, 0, 0, 0));
+            for (int b = 0; b < t->nband; ++b)
+                for (int s = m.band_begin[b]; s < m.band_begin[b + 1]; ++s) {
+                    const int im = m.band_list[s];
+                    const int slot = s - m.band_begin[b];
+                    for (int g = m.gstart[im]; g < m.gend[im]; ++g) {
+                        int4& e = mg[atm][g];
+                        const int code = ((m.kstart[im] + g - m.gstart[im]) << 4) | slot;
+                        if (e.x == 0) e.y = code;
+                        else if (e.x == 1) e.z = code;
+                        else if (e.x == 2) e.w = code;
+                        e.x = std::min(e.x + 1, 4);  // 4 marks "more than 3": fused kernels refuse
+                        v.max_minor_per_g = std::max(v.max_minor_per_g, e.x);
+                    }
+                }
+        }
+        if (info.has_rayleigh) {
+            kr2.resize(size_t(2) * nt * (ne - 1) * ng);
+            for (int atm = 0; atm < 2; ++atm) {
+                const double* r = atm == 0 ? t->rayl_lower : t->rayl_upper;
+                for (int it = 0; it < nt; ++it)
+                    for (int ie = 0; ie < ne - 1; ++ie)
+                        for (int ig = 0; ig < ng; ++ig)
+                            kr2[((size_t(atm) * nt + it) * (ne - 1) + ie) * ng + ig] =
+                                make_float2(float(r[(size_t(it) * ne + ie) * ng + ig]),
+                                            float(r[(size_t(it) * ne + ie + 1) * ng + ig]));
+            }
+        }
+    }
+    a.add(km4, &v.kmaj4);
+    a.add(pf4, &v.pfrac4);
+    a.add(kn2[0], &v.kmin2[0]);
+    a.add(kn2[1], &v.kmin2[1]);
+    a.add(kr2, &v.krayl2);
+    a.add(mg[0], &v.minor_g[0]);
+    a.add(mg[1], &v.minor_g[1]);
     return a.upload(k->allocations);
 }
 

@@ -360,6 +360,21 @@ int rrtmgp_b200_forward_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int
         const float* lwp, const float* iwp, const float* rel, const float* rei,
         const float* sfc_emis, float* flux_up, float* flux_dn, float* flux_net,
         float* heating_rate, int chunk, void* stream);
+/* Shortwave column forward: the sequence of Radiation_solver_shortwave::solve_gpu
+ * (src_test/Radiation_solver.cu:683-950) -- gas_optics with Rayleigh, toa_src scaled by
+ * tsi_scaling (NULL: 1), cloud_optics (2str; delta-scaled when delta_cloud != 0; skipped when
+ * cloud is NULL) added by band, rte_sw (two-stream + adding, no incident diffuse flux) and
+ * Fluxes_broadband::reduce -- plus heating rates, in one kernel.  mu0 (ncol) > 0; surface
+ * albedos (nband, ncol) in the reference's column-fastest order.  Outputs flux_up, flux_dn
+ * (direct included), flux_dn_dir, flux_net (ncol, nlay+1) and heating_rate (ncol, nlay).
+ * chunk: layers per warp (8 or 16; 0 picks the tuned default).  nlay <= 16 * chunk. */
+int rrtmgp_b200_forward_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int ncol, int nlay,
+        const float* play, const float* plev, const float* tlay, const float* col_dry,
+        const rrtmgp_b200_gas_conc* gases, int ngases, const float* lwp, const float* iwp,
+        const float* rel, const float* rei, int delta_cloud, const float* mu0,
+        const float* tsi_scaling, const float* sfc_alb_dir, const float* sfc_alb_dif,
+        float* flux_up, float* flux_dn, float* flux_dn_dir, float* flux_net,
+        float* heating_rate, int chunk, void* stream);
 
 #ifdef __cplusplus
 }

@@ -62,7 +62,7 @@ __device__ __forceinline__ void build_lw_record(const KdistView<float>& k, Rec& 
     R.aux = make_float4(interpolate1D(s.t, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp),
                         interpolate1D(s.t_top, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp),
                         interpolate1D(s.t_bot, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp), tau_cld);
-    R.pl_sfc = bottom ? interpolate1D(tsfc, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp) : 0.f;
+    R.aux2 = bottom ? interpolate1D(tsfc, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp) : 0.f;
 }
 
 template <int CL>
@@ -141,7 +141,7 @@ lw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const CloudA
                 const float pfrac = (R.wpl0.x * p0.x + R.wpl0.y * p0.y + R.wpl0.z * p0.z + R.wpl0.w * p0.w) +
                                     (R.wpl1.x * p1.x + R.wpl1.y * p1.y + R.wpl1.z * p1.z + R.wpl1.w * p1.w);
                 lw_layer_fast(tau, D, pfrac * R.aux.x, pfrac * R.aux.z, pfrac * R.aux.y, omt[i], sdn[i], sup[i]);
-                if (j == nlay - 1) sm_sfc[lane] = pfrac * R.pl_sfc;
+                if (j == nlay - 1) sm_sfc[lane] = pfrac * R.aux2;
             } else if (j == nlay - 1) {
                 sm_sfc[lane] = 0.f;
             }

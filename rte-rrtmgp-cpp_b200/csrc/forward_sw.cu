@@ -1,0 +1,442 @@
+// Fused shortwave forward: gas optics (major + minor absorption, Rayleigh) + cloud optics
+// (2str, delta-scaled, added by band) + two-stream layer coefficients + adding method +
+// broadband fluxes + heating rates for whole columns, with no (ncol, nlay, ngpt) array.
+// The staged equivalent is Radiation_solver_shortwave::solve_gpu
+// (src_test/Radiation_solver.cu:683-950) followed by the heating-rate formula.
+//
+// Thread mapping as in the longwave kernel (fused_common.cuh): one CTA per column, lane =
+// g-point of the current group of 32, warp w = layer chunk [w*CL, (w+1)*CL) from the top.
+//
+// Per group of 32 g-points:
+//   1. pass 1 (per layer, in registers): optical properties, two-stream coefficients
+//      (R, T, Rdir, Tdir, Tnoscat) and the layer absorptances; the chunk's direct-beam
+//      transmission product PT and its adding composite (R_up, R_dn, T, U, D) with sources
+//      relative to a unit direct flux at the chunk top;
+//   2. barrier; every warp forms its direct flux at the chunk top from the PT of the chunks
+//      above, emits the direct fluxes and direct absorption of its layers and scales its
+//      composite's sources to absolute values;
+//   3. barrier; every warp walks the composites from the surface up: albedo and upward
+//      source at its chunk bottom, and the affine maps fd_bot = F fd_top + G of the chunks
+//      above it, composed into its incident diffuse flux;
+//   4. pass 2 (bottom-up within the chunk): albedo and source per level (adding_kernel);
+//      pass 3 (top-down): diffuse down/up fluxes per level and per-layer diffuse absorption;
+//   5. warp reduce-scatter over the 32 g-points, FP64 accumulation per lane.
+// Heating rates use the per-layer absorbed flux (direct: F_dir (1 - Tn - Rdir - Tdir);
+// diffuse: (F_dn(top) + F_up(bottom)) (1 - R - T)), which equals the net-flux divergence of
+// the adding solution but keeps its relative accuracy in the ~0.1 Pa top layers.
+#include "fused_common.cuh"
+#include "optics_device.cuh"
+
+namespace rrtmgp_b200 {
+namespace {
+
+using namespace fused;
+
+struct SwCloudArgs {
+    CloudLut<float> L;
+    const float* lwp;
+    const float* iwp;
+    const float* rel;
+    const float* rei;
+    int present;
+    int delta;
+};
+
+// 1 - exp(-x) and exp(-x) for x >= 0, each with a small relative error: Taylor series of
+// 1 - exp(-x) through x^8 below 0.5 (truncation < 1.4e-8 relative), the exp intrinsic above.
+__device__ __forceinline__ void one_minus_exp(float x, float& E, float& e)
+{
+    if (x < 0.5f) {
+        E = x * (1.f - x * (1.f / 2.f - x * (1.f / 6.f - x * (1.f / 24.f - x * (1.f / 120.f - x * (1.f / 720.f -
+            x * (1.f / 5040.f - x * (1.f / 40320.f))))))));
+        e = 1.f - E;
+    } else {
+        e = __expf(-x);
+        E = 1.f - e;
+    }
+}
+
+// Layer coefficients of the PIFM two-stream (sw_2stream_function, rte_solver_kernels.cu:
+// 535-584) in FP32.  The reference expressions lose all relative accuracy in FP32 for thin and
+// for conservatively scattering layers (O(1) terms cancelling to O(tau)); here they are
+// rearranged with E1 = 1 - exp(-k tau), E2 = 1 - exp(-2 k tau), En = 1 - exp(-tau/mu0) so
+// that the constant parts cancel analytically (same values in exact arithmetic):
+//   gamma1 - gamma2 = 2 (1 - w0),  1 - Rdif - Tdif = rt (k E1^2 + 2 (1 - w0) E2),
+//   Rdir bracket = E2 (alpha2 - k^2 mu0 gamma3) + k (gamma3 - mu0 alpha2) (E1^2 + 2 e1 En),
+//   Tdir bracket = Tn E2 (alpha1 + k^2 mu0 gamma4) + k (gamma4 + mu0 alpha1) (E1^2 - (1 + e2) En),
+// the Tdir bracket taking the reference form when both exponentials are small (thick layers).
+// Near the removable singularity k mu0 = 1 (|1 - (k mu0)^2| < 0.02) Rdir and Tdir come from
+// the reference expressions in FP64 (FP64 island).  omw = 1 - w0 is passed separately, formed
+// from absorption optical depths, so it keeps its accuracy for w0 -> 1.  Clamps and k_min are
+// those of the FP64 reference (DBL_EPSILON, 1e-12).
+__device__ __forceinline__ void sw_layer_fast(float tau, float w0, float omw, float g, float mu0, float mu0_inv,
+                                              float& R, float& T, float& Rdir, float& Tdir, float& Tn,
+                                              float& adif, float& adir)
+{
+    const float g1 = (8.f - w0 * (5.f + 3.f * g)) * .25f;
+    const float g2 = 3.f * (w0 * (1.f - g)) * .25f;
+    const float g3 = (2.f - 3.f * mu0 * g) * .25f;
+    const float g4 = 1.f - g3;
+    const float a1 = g1 * g4 + g2 * g3;
+    const float a2 = g1 * g3 + g2 * g4;
+    const float kk = 2.f * omw * (2.f - .5f * w0 * (1.f + 3.f * g));
+    const float k = sqrtf(fmaxf(kk, 1.e-12f));
+    float E1, e1, En;
+    one_minus_exp(k * tau, E1, e1);
+    one_minus_exp(tau * mu0_inv, En, Tn);
+    const float E2 = E1 * (2.f - E1);
+    const float e2 = e1 * e1;
+    const float rt = 1.f / (k * (1.f + e2) + g1 * E2);
+    R = rt * g2 * E2;
+    T = rt * 2.f * k * e1;
+    adif = rt * (k * E1 * E1 + 2.f * omw * E2);
+    const float km = k * mu0;
+    const float fact = (1.f - km) * (1.f + km);
+    if (fabsf(fact) < 0.02f) {
+        double Rd, Td, Rr, Tr, Tn64;
+        sw_two_stream<double>(double(tau), double(w0), double(g), double(mu0), Rd, Td, Rr, Tr, Tn64);
+        Rdir = float(Rr);
+        Tdir = float(Tr);
+    } else {
+        const float rt2 = w0 * rt / fact;
+        const float br = E2 * (a2 - k * km * g3) + k * (g3 - mu0 * a2) * (E1 * E1 + 2.f * e1 * En);
+        float bt;
+        if (e1 < .5f && Tn < .5f)
+            bt = (1.f + km) * (a1 + k * g4) * Tn - (1.f - km) * (a1 - k * g4) * e2 * Tn - 2.f * (k * g4 + a1 * km) * e1;
+        else
+            bt = Tn * E2 * (a1 + k * km * g4) + k * (g4 + mu0 * a1) * (E1 * E1 - (1.f + e2) * En);
+        Rdir = rt2 * br;
+        Tdir = -rt2 * bt;
+    }
+    const float tmin = 2.220446049250313e-16f;
+    Rdir = fmaxf(tmin, fminf(Rdir, En));
+    const float rest = En - Rdir;
+    Tdir = fmaxf(tmin, fminf(Tdir, rest));
+    adir = fmaxf(0.f, rest - Tdir);
+}
+
+__device__ __forceinline__ void build_sw_record(const KdistView<float>& k, Rec& R, const LayerState& s,
+                                                const float* cg, int nlay, int b, const SwCloudArgs& cld,
+                                                size_t cl)
+{
+    record_weights(k, R, s, cg, nlay, b);
+    float tau = 0.f, ssa = 0.f, g = 0.f;
+    if (cld.present) {
+        const CloudPoint<float> cp = cloud_point(cld.L, cld.lwp[cl], cld.iwp[cl], cld.rel[cl], cld.rei[cl]);
+        cloud_band<float, true>(cld.L, cp, b, tau, ssa, g);
+        const float ta = tau * (1.f - ssa);   // invariant under delta scaling
+        if (cld.delta) delta_scale_point(tau, ssa, g);
+        R.aux2 = ta;
+    } else {
+        R.aux2 = 0.f;
+    }
+    const float ts = tau * ssa;
+    R.aux = make_float4(cg[0] + cg[k.idx_h2o * nlay], tau, ts, ts * g);
+}
+
+template <int CL>
+__global__ void __launch_bounds__(512)
+sw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const SwCloudArgs cld, int ncol, int nlay,
+                  const float* __restrict__ play, const float* __restrict__ plev, const float* __restrict__ tlay,
+                  const float* __restrict__ col_dry_in, const float* __restrict__ mu0_in,
+                  const float* __restrict__ tsi_scaling, const float* __restrict__ alb_dir,
+                  const float* __restrict__ alb_dif, float* __restrict__ flux_up, float* __restrict__ flux_dn,
+                  float* __restrict__ flux_dir, float* __restrict__ flux_net, float* __restrict__ heating_rate)
+{
+    static_assert(CL == 8 || CL == 16, "chunk length");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int icol = blockIdx.x;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int NW = blockDim.x >> 5;
+    const int nband = k.nband;
+    const SmemLayout SL = smem_layout(nlay, k.ngas, nband, 0, NW, 3, CL, k.max_group_bands);
+    LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
+    float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
+    float* sm_pt = reinterpret_cast<float*>(smem_raw + SL.maps);                  // [NW][32]
+    float4* sm_comp = reinterpret_cast<float4*>(smem_raw + SL.maps) + NW * 32;     // [NW][32]
+    float* sm_compd = reinterpret_cast<float*>(sm_comp + NW * 32);                // [NW][32]
+    Rec* recs = reinterpret_cast<Rec*>(smem_raw + SL.recs) + w * CL * k.max_group_bands;
+
+    const bool top_at_1 = play[icol] < play[icol + size_t(nlay - 1) * ncol];
+    const float mu0 = mu0_in[icol];
+    const float mu0_inv = 1.f / mu0;
+    const float tsi = tsi_scaling ? tsi_scaling[icol] : 1.f;
+    setup_layers(k, gs, ncol, nlay, icol, top_at_1, play, plev, tlay, nullptr, col_dry_in, st, sm_cg);
+    __syncthreads();
+
+    const int ngpt = k.ngpt;
+    constexpr int SH = (CL == 16) ? 0 : 1;          // lane L holds reduced value L >> SH
+    double acc_a = 0.0, acc_b = 0.0, acc_c = 0.0;   // see the output section
+    double acc_sfc_dir = 0.0, acc_sfc_dn = 0.0, acc_sfc_up = 0.0;
+
+    for (int gg = 0; gg < k.ngroups; ++gg) {
+        const int g = 32 * gg + lane;
+        const bool gv = g < ngpt;
+        const int b0 = k.group_band0[gg];
+        const int gband = gv ? k.gpt2band[g] : b0;
+        const int slot = gband - b0;
+        const int4 mg0 = gv ? __ldg(k.minor_g[0] + g) : make_int4(0, 0, 0, 0);
+        const int4 mg1 = gv ? __ldg(k.minor_g[1] + g) : make_int4(0, 0, 0, 0);
+
+        for (int r = lane; r < CL * k.max_group_bands; r += 32) {
+            const int jj = w * CL + (r % CL);
+            const int b = b0 + r / CL;
+            if (jj < nlay && b < nband && k.band_lims[2 * b] < 32 * gg + 32) {
+                const int l = top_at_1 ? jj : nlay - 1 - jj;
+                build_sw_record(k, recs[r], st[jj], sm_cg + jj, nlay, b, cld, icol + size_t(l) * ncol);
+            }
+        }
+        __syncwarp();
+
+        // 1. pass 1
+        float vR[CL], vT[CL], vSu[CL], vSd[CL], vAd[CL], vP[CL], vAdir[CL];
+        float P = 1.f;
+        float cRu = 0.f, cRd = 0.f, cT = 1.f, cU = 0.f, cD = 0.f;
+#pragma unroll
+        for (int i = 0; i < CL; ++i) {
+            const int j = w * CL + i;
+            float R = 0.f, T = 1.f, Rdir = 0.f, Tdir = 0.f, Tn = 1.f, adif = 0.f, adir = 0.f;
+            if (j < nlay && gv) {
+                const Rec& Rc = recs[slot * CL + i];
+                const float ta = tau_abs(k, Rc, g, Rc.a ? mg1 : mg0);
+                const float2 r0 = __ldg(k.krayl2 + size_t(Rc.kr[0]) * ngpt + g);
+                const float2 r1 = __ldg(k.krayl2 + size_t(Rc.kr[1]) * ngpt + g);
+                const float tr = (Rc.fm.x * r0.x + Rc.fm.y * r0.y + Rc.fm.z * r1.x + Rc.fm.w * r1.y) * Rc.aux.x;
+                const float tau = ta + tr + Rc.aux.y;
+                const float ts = tr + Rc.aux.z;
+                float w0 = 0.f, omw = 1.f;
+                if (tau > 2.f * FLT_MIN) {
+                    const float inv = 1.f / tau;
+                    w0 = ts * inv;
+                    omw = (ta + Rc.aux2) * inv;
+                }
+                const float gasy = Rc.aux.w / fmaxf(ts, 3.f * FLT_MIN);
+                sw_layer_fast(tau, w0, omw, gasy, mu0, mu0_inv, R, T, Rdir, Tdir, Tn, adif, adir);
+            }
+            vR[i] = R;
+            vT[i] = T;
+            vP[i] = P;
+            vSu[i] = Rdir * P;
+            vSd[i] = Tdir * P;
+            vAd[i] = adif;
+            vAdir[i] = adir * P;
+            // Add layer i below the composite of layers 0..i-1.
+            const float den = 1.f / fmaf(-cRd, R, 1.f);
+            const float nRu = cRu + cT * cT * R * den;
+            const float nRd = R + T * T * cRd * den;
+            const float nU = cU + cT * (vSu[i] + R * cD) * den;
+            const float nD = vSd[i] + T * (cD + cRd * vSu[i]) * den;
+            cT = cT * T * den;
+            cRu = nRu;
+            cRd = nRd;
+            cU = nU;
+            cD = nD;
+            P *= Tn;
+        }
+        sm_pt[w * 32 + lane] = P;
+        __syncthreads();
+
+        // 2. direct flux at the chunk top and at the surface
+        const float toa = gv ? __ldg(k.solar_source + g) * tsi * mu0 : 0.f;
+        float dtop = toa;
+        for (int c = 0; c < w; ++c) dtop *= sm_pt[c * 32 + lane];
+        float dsfc = dtop;
+        for (int c = w; c < NW; ++c) dsfc *= sm_pt[c * 32 + lane];
+        {
+            float v[2 * CL];
+#pragma unroll
+            for (int i = 0; i < CL; ++i) {
+                v[i] = dtop * vP[i];
+                v[CL + i] = dtop * vAdir[i];
+            }
+            ReduceScatter<2 * CL, 16>::run(v, lane);
+            acc_a += double(v[0]);
+        }
+        sm_comp[w * 32 + lane] = make_float4(cRu, cRd, cT, cU * dtop);
+        sm_compd[w * 32 + lane] = cD * dtop;
+        __syncthreads();
+
+        // 3. albedo and source at this chunk's bottom; incident diffuse flux at its top
+        const float ad = gv ? __ldg(alb_dir + gband + size_t(icol) * nband) : 0.f;
+        const float af = gv ? __ldg(alb_dif + gband + size_t(icol) * nband) : 0.f;
+        float alb = af, src = dsfc * ad;
+        float alb_in = af, src_in = src;
+        float fa = 1.f, fb = 0.f;
+        for (int c = NW - 1; c >= 0; --c) {
+            if (c == w) {
+                alb_in = alb;
+                src_in = src;
+                if (w == 0) break;
+            }
+            const float4 m = sm_comp[c * 32 + lane];
+            const float D = sm_compd[c * 32 + lane];
+            const float den = 1.f / fmaf(-m.y, alb, 1.f);
+            if (c < w) {
+                const float F = m.z * den, G = fmaf(m.y, src, D) * den;
+                fb = fmaf(fa, G, fb);
+                fa *= F;
+            }
+            const float nalb = m.x + m.z * m.z * alb * den;
+            src = m.w + m.z * fmaf(alb, D, src) * den;
+            alb = nalb;
+        }
+
+        // 4. pass 2 (bottom-up): albedo and upward source per level
+        float vA[CL];
+        {
+            float a = alb_in, s = src_in;
+#pragma unroll
+            for (int i = CL - 1; i >= 0; --i) {
+                const float su = vSu[i] * dtop, sd = vSd[i] * dtop;
+                const float den = 1.f / fmaf(-vR[i], a, 1.f);
+                const float na = vR[i] + vT[i] * vT[i] * a * den;
+                const float ns = su + vT[i] * fmaf(a, sd, s) * den;
+                vSd[i] = sd;
+                vSu[i] = ns;
+                vA[i] = na;
+                a = na;
+                s = ns;
+            }
+        }
+        // pass 3 (top-down): diffuse fluxes and diffuse absorption
+        float vUp[2 * CL], vDn[2 * CL];
+        float fd = fb;
+#pragma unroll
+        for (int i = 0; i < CL; ++i) {
+            const float a_n = (i + 1 < CL) ? vA[i + 1] : alb_in;
+            const float s_n = (i + 1 < CL) ? vSu[i + 1] : src_in;
+            const float fu = fmaf(fd, vA[i], vSu[i]);
+            const float den = 1.f / fmaf(-vR[i], a_n, 1.f);
+            const float fdn = (vT[i] * fd + vR[i] * s_n + vSd[i]) * den;
+            const float fun = fmaf(fdn, a_n, s_n);
+            vUp[i] = fu;
+            vUp[CL + i] = (fd + fun) * vAd[i];
+            vDn[i] = fd;
+            vDn[CL + i] = 0.f;
+            fd = fdn;
+        }
+        if (w == NW - 1) {
+            acc_sfc_dir += double(warp_sum(dsfc));
+            acc_sfc_dn += double(warp_sum(fd));
+            acc_sfc_up += double(warp_sum(fmaf(fd, alb_in, src_in)));
+        }
+        ReduceScatter<2 * CL, 16>::run(vUp, lane);
+        ReduceScatter<2 * CL, 16>::run(vDn, lane);
+        acc_b += double(vUp[0]);
+        acc_c += double(vDn[0]);
+    }
+
+    // Outputs.  Lane L holds value v = L >> SH of the reduced arrays: v < CL is level
+    // w*CL + v (acc_a: direct, acc_b: up, acc_c: diffuse down), v >= CL is layer
+    // w*CL + v - CL (acc_a + acc_b: absorbed flux).
+    const int v = lane >> SH;
+    if ((lane & ((1 << SH) - 1)) == 0) {
+        if (v < CL) {
+            const int jl = w * CL + v;
+            if (jl < nlay) {
+                const int al = top_at_1 ? jl : nlay - jl;
+                const size_t o = icol + size_t(al) * ncol;
+                const double dn = acc_c + acc_a;
+                flux_up[o] = float(acc_b);
+                flux_dn[o] = float(dn);
+                flux_dir[o] = float(acc_a);
+                flux_net[o] = float(dn - acc_b);
+            }
+        } else {
+            const int jl = w * CL + v - CL;
+            if (jl < nlay) {
+                const int l = top_at_1 ? jl : nlay - 1 - jl;
+                const double g0_cp = 9.80665 / 1004.64;
+                heating_rate[icol + size_t(l) * ncol] = float(g0_cp * 86400.0 * (acc_a + acc_b) / double(st[jl].dp));
+            }
+        }
+    }
+    if (w == NW - 1 && lane == 0) {
+        const int al = top_at_1 ? nlay : 0;
+        const size_t o = icol + size_t(al) * ncol;
+        const double dn = acc_sfc_dn + acc_sfc_dir;
+        flux_up[o] = float(acc_sfc_up);
+        flux_dn[o] = float(dn);
+        flux_dir[o] = float(acc_sfc_dir);
+        flux_net[o] = float(dn - acc_sfc_up);
+    }
+}
+
+template <int CL>
+int launch_sw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay, const float* play,
+                      const float* plev, const float* tlay, const float* col_dry, const GasSet<float>& gs,
+                      const float* lwp, const float* iwp, const float* rel, const float* rei, int delta,
+                      const float* mu0, const float* tsi, const float* alb_dir, const float* alb_dif, float* up,
+                      float* dn, float* dir, float* net, float* hr, cudaStream_t stream)
+{
+    const KdistView<float>& v = k->v32;
+    const int NW = (nlay + CL - 1) / CL;
+    RB_CHECK_ARG(NW <= 16, "forward_sw: nlay too large for the fused kernel (at most 16 chunks)");
+    const size_t smem = smem_layout(nlay, v.ngas, v.nband, 0, NW, 3, CL, v.max_group_bands).total;
+    if (smem > 220 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "forward_sw: shared memory need exceeds 220 KB");
+    static bool attr = false;
+    if (!attr) {
+        RB_CUDA(cudaFuncSetAttribute(sw_forward_kernel<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024),
+                "forward_sw attribute");
+        attr = true;
+    }
+    SwCloudArgs ca{};
+    if (c) {
+        ca.L = CloudLut<float>{c->nband, c->nsize_liq, c->nsize_ice, float(c->radliq_lwr), float(c->liq_step),
+                               float(c->radice_lwr), float(c->ice_step), c->lut32};
+        ca.lwp = lwp; ca.iwp = iwp; ca.rel = rel; ca.rei = rei;
+        ca.present = 1;
+        ca.delta = delta;
+    }
+    sw_forward_kernel<CL><<<ncol, NW * 32, smem, stream>>>(v, gs, ca, ncol, nlay, play, plev, tlay, col_dry, mu0, tsi,
+                                                             alb_dir, alb_dif, up, dn, dir, net, hr);
+    RB_LAUNCH("sw_forward_kernel");
+    return RRTMGP_B200_OK;
+}
+
+}  // namespace
+
+int forward_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay, const float* play,
+                   const float* plev, const float* tlay, const float* col_dry, const rrtmgp_b200_gas_conc* gases,
+                   int ngases, const float* lwp, const float* iwp, const float* rel, const float* rei,
+                   int delta_cloud, const float* mu0, const float* tsi_scaling, const float* sfc_alb_dir,
+                   const float* sfc_alb_dif, float* flux_up, float* flux_dn, float* flux_dn_dir, float* flux_net,
+                   float* heating_rate, int chunk, void* stream)
+{
+    RB_CHECK_ARG(k && !k->info.is_longwave, "forward_sw: need a shortwave k-distribution");
+    RB_CHECK_ARG(ncol > 0 && nlay > 1, "forward_sw: ncol > 0 and nlay > 1 required");
+    RB_CHECK_ARG(play && plev && tlay && mu0 && sfc_alb_dir && sfc_alb_dif && flux_up && flux_dn && flux_dn_dir &&
+                 flux_net && heating_rate, "forward_sw: null array");
+    RB_CHECK_ARG(!c || (lwp && iwp && rel && rei), "forward_sw: cloud arrays required with a cloud handle");
+    RB_CHECK_ARG(!c || c->nband == k->info.nband, "forward_sw: cloud and gas band counts differ");
+    const KdistView<float>& v = k->v32;
+    if (!v.minor_in_band || v.max_band_minor > kMaxMinor || v.max_minor_per_g > 3 || v.max_group_bands > 8 ||
+        !v.krayl2)
+        return fail(RRTMGP_B200_ERR_UNSUPPORTED, "forward_sw: k-distribution layout not supported by the fused kernel");
+    GasSet<float> gs;
+    int st = make_gas_set<float>(k, ncol, nlay, gases, ngases, gs);
+    if (st) return st;
+    cudaStream_t s = as_stream(stream);
+    const int cl = chunk ? chunk : 8;
+    if (cl == 16)
+        return launch_sw_forward<16>(k, c, ncol, nlay, play, plev, tlay, col_dry, gs, lwp, iwp, rel, rei, delta_cloud,
+                                     mu0, tsi_scaling, sfc_alb_dir, sfc_alb_dif, flux_up, flux_dn, flux_dn_dir,
+                                     flux_net, heating_rate, s);
+    return launch_sw_forward<8>(k, c, ncol, nlay, play, plev, tlay, col_dry, gs, lwp, iwp, rel, rei, delta_cloud, mu0,
+                                tsi_scaling, sfc_alb_dir, sfc_alb_dif, flux_up, flux_dn, flux_dn_dir, flux_net,
+                                heating_rate, s);
+}
+
+}  // namespace rrtmgp_b200
+
+extern "C" int rrtmgp_b200_forward_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
+        const float* play, const float* plev, const float* tlay, const float* col_dry,
+        const rrtmgp_b200_gas_conc* gases, int ngases, const float* lwp, const float* iwp, const float* rel,
+        const float* rei, int delta_cloud, const float* mu0, const float* tsi_scaling, const float* sfc_alb_dir,
+        const float* sfc_alb_dif, float* flux_up, float* flux_dn, float* flux_dn_dir, float* flux_net,
+        float* heating_rate, int chunk, void* stream)
+{
+    return rrtmgp_b200::forward_sw_f32(k, c, ncol, nlay, play, plev, tlay, col_dry, gases, ngases, lwp, iwp, rel, rei,
+                                       delta_cloud, mu0, tsi_scaling, sfc_alb_dir, sfc_alb_dif, flux_up, flux_dn,
+                                       flux_dn_dir, flux_net, heating_rate, chunk, stream);
+}

@@ -37,9 +37,10 @@ struct __align__(16) Rec {
     float4 aux;            // LW: pl_lay, pl_top, pl_bot, tau_cloud
                            // SW: col_dry + col_h2o (Rayleigh), cloud tau, ssa, g
     float scal[kMaxMinor]; // minor scaling of each interval in the band's list
-    float pl_sfc;          // LW surface Planck function (bottom layer only)
+    float aux2;            // LW: surface Planck function (bottom layer only)
+                           // SW: cloud absorption optical depth tau_c * (1 - ssa_c)
     int a;                 // 0 lower / 1 upper atmosphere
-    int pad[2];
+    int kr[2];             // krayl2 rows of (a, t0, e0) and (a, t1, e1)
 };
 
 // Reduce-scatter of N per-lane values over 32 lanes: afterwards lane L holds in v[0] the warp
@@ -98,6 +99,7 @@ __device__ __forceinline__ void record_weights(const KdistView<float>& k, Rec& R
     R.kb.y = (li.jt * np + p0) * ne1 + (fw.j1 - 1);
     const int a = li.itropo;
     const int nc = k.ncontrib[a] > 0 ? k.ncontrib[a] : 1;
+    // kmin2 rows; the Rayleigh rows (krayl2, [a][t][eta][g]) follow the same (t, eta) corners.
     R.kb.z = ((li.jt - 1) * ne1 + (fw.j0 - 1)) * nc;
     R.kb.w = (li.jt * ne1 + (fw.j1 - 1)) * nc;
     const float fp = li.fpress, f1 = 1.f - li.fpress;
@@ -107,6 +109,8 @@ __device__ __forceinline__ void record_weights(const KdistView<float>& k, Rec& R
     R.wmaj1 = make_float4(fw.cm[1] * R.wpl1.x, fw.cm[1] * R.wpl1.y, fw.cm[1] * R.wpl1.z, fw.cm[1] * R.wpl1.w);
     R.fm = make_float4(fw.fm[0], fw.fm[1], fw.fm[2], fw.fm[3]);
     R.a = a;
+    R.kr[0] = (a * k.ntemp + li.jt - 1) * ne1 + (fw.j0 - 1);
+    R.kr[1] = (a * k.ntemp + li.jt) * ne1 + (fw.j1 - 1);
     int n = 0;
     for (int ii = k.band_minor_begin[a][b]; ii < k.band_minor_begin[a][b + 1] && n < kMaxMinor; ++ii, ++n)
         R.scal[n] = minor_scaling(k, a, k.band_minor_list[a][ii], cg, cgs, s.p, s.t);

@@ -198,6 +198,8 @@ _SIGS = {
     "rrtmgp_b200_rte_sw_static_scratch_f32": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "rrtmgp_b200_forward_lw_f32": (_I, [_P, _P, _I, _I, _P, _P, _P, _P, _P, _P, C.POINTER(GasConc), _I,
                                         _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
+    "rrtmgp_b200_forward_sw_f32": (_I, [_P, _P, _I, _I, _P, _P, _P, _P, C.POINTER(GasConc), _I,
+                                        _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
 }
 SW_STATIC_SCRATCH_MAX_ELEMS = 1048576
 _FP_SIGS = {

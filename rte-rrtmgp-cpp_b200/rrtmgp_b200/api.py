@@ -48,6 +48,13 @@ def _empty(shape, like):
     return torch.empty(shape, dtype=like.dtype, device=like.device)
 
 
+def _release(fn, handle):
+    """Destroy a native handle; a no-op once the interpreter has torn the modules down."""
+    lib = getattr(_abi, "_lib", None) if _abi is not None else None
+    if lib is not None and handle is not None:
+        getattr(lib, fn)(handle)
+
+
 class Bands:
     """Optical_props_gpu band/g-point discretisation (include/Optical_props.h:176-211)."""
 
@@ -69,9 +76,9 @@ class Bands:
         b._own = True
         return b
 
-    def __del__(self):
-        if getattr(self, "_own", False) and _abi._lib is not None:
-            _abi._lib.rrtmgp_b200_bands_destroy(self.handle)
+    def __del__(self, _release=_release):
+        if getattr(self, "_own", False):
+            _release("rrtmgp_b200_bands_destroy", self.handle)
 
 
 class Gas_optics_rrtmgp:
@@ -95,9 +102,9 @@ class Gas_optics_rrtmgp:
         self.bands = Bands(lib.rrtmgp_b200_kdist_bands(h), owner=self)
         self.band_lims_gpt = tables["bnd_limits_gpt"]
 
-    def __del__(self):
-        if getattr(self, "handle", None) is not None and _abi._lib is not None:
-            _abi._lib.rrtmgp_b200_kdist_destroy(self.handle)
+    def __del__(self, _release=_release):
+        if getattr(self, "handle", None) is not None:
+            _release("rrtmgp_b200_kdist_destroy", self.handle)
             self.handle = None
 
     def get_ngpt(self):
@@ -185,9 +192,9 @@ class Cloud_optics:
         self.handle = h
         self.nband = t.nband
 
-    def __del__(self):
-        if getattr(self, "handle", None) is not None and _abi._lib is not None:
-            _abi._lib.rrtmgp_b200_cloud_destroy(self.handle)
+    def __del__(self, _release=_release):
+        if getattr(self, "handle", None) is not None:
+            _release("rrtmgp_b200_cloud_destroy", self.handle)
             self.handle = None
 
     def cloud_optics(self, clwp, ciwp, reliq, reice, two_stream=True):

@@ -6,7 +6,10 @@ heating rates for LW 256 and SW 224 g-points over nlay layers), FP32, synthetic 
 atmospheres and tables with the reference schema (the real RRTMGP tables are not available).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--path staged|fused] [--ncol C] [--nlay L]
+                  [--path fused|staged] [--ncol C] [--nlay L]
+
+--path fused (default) runs the product path: one fused kernel per LW and per SW solve.
+--path staged runs the reference-shaped per-stage kernels over (g, lay, col) arrays.
 
 One process per GPU (torchrun for N > 1); columns are sharded across ranks with no exchange
 (weak scaling: every rank owns ncol columns).  Rank 0 prints one JSON line.
@@ -35,10 +38,10 @@ L2_FLUSH_BYTES = 256 << 20
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--path", default="staged", choices=["staged", "fused"])
+    ap.add_argument("--path", default="fused", choices=["staged", "fused"])
     ap.add_argument("--ncol", type=int, default=8192)
     ap.add_argument("--nlay", type=int, default=128)
     ap.add_argument("--seed", type=int, default=42)
@@ -57,7 +60,7 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled every 100 ms during the timed region."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -73,7 +76,7 @@ class ClockSampler:
             self.file = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+                 "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
 
@@ -125,6 +128,52 @@ def bytes_per_column(nlay, glw=256, gsw=224, nb_lw=16, nb_sw=14, B=4):
         "delta_sw": (6 * L * nb_sw) * B,
         "heating": (4 * V + L) * B * 2,
     }
+
+
+def fused_flops_per_column(nlay, glw=256, gsw=224):
+    """Algorithmic FP32 FLOPs (FMA = 2) per column of the fused kernels, counted from the
+    kernel source per (layer, g-point): LW 79 (major 16, minor 10, cloud 1, Planck fraction 16,
+    sources 3, layer terms 15, chunk maps 7, pass 2 8, reduction 3) plus 1 exp and 1 divide;
+    SW 210 (major 16, minor 10, Rayleigh 9, combine 7, two-stream 108, adding composite 26,
+    direct outputs 4, passes 2/3 26, reduction 4) plus 1 sqrt, 2 exp and 6 divides.
+    Transcendentals and divides are not counted as FLOPs."""
+    return {"lw_forward_kernel": 79 * nlay * glw, "sw_forward_kernel": 210 * nlay * gsw}
+
+
+def fused_bytes_per_column(nlay, nb_lw=16, nb_sw=14, B=4):
+    """HBM bytes per column the fused kernels must move: inputs once, outputs once.  Inputs:
+    play, tlay, plev (+ tlev, tsfc for LW), lwp/iwp/rel/rei, the h2o and o3 fields (the other
+    gases are scalars), emissivity or mu0/tsi/albedos; outputs: the level fluxes and the
+    layer heating rates."""
+    L, V = nlay, nlay + 1
+    lw_in = (2 * L + 2 * V + 1 + 4 * L + 2 * L + nb_lw) * B
+    lw_out = (3 * V + L) * B
+    sw_in = (2 * L + V + 4 * L + 2 * L + 2 + 2 * nb_sw) * B
+    sw_out = (4 * V + L) * B
+    return {"lw_forward_kernel": lw_in + lw_out, "sw_forward_kernel": sw_in + sw_out}
+
+
+def fp32_peak(torch, dev, stream):
+    """FP32 FMA throughput of this GPU measured with the library's FMA probe (TFLOP/s)."""
+    from rrtmgp_b200 import _abi
+    lib = _abi.load()
+    import ctypes as C
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+    blocks, iters = nsm * 4, 4096
+    out = torch.empty(blocks, dtype=torch.float32, device=dev)
+    s = C.c_void_p(stream.cuda_stream)
+    for _ in range(2):
+        _abi.check(lib.rrtmgp_b200_fp32_fma_probe(blocks, iters, C.c_void_p(out.data_ptr()), s))
+    best = None
+    for _ in range(5):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        _abi.check(lib.rrtmgp_b200_fp32_fma_probe(blocks, iters, C.c_void_p(out.data_ptr()), s))
+        b.record(stream)
+        b.synchronize()
+        ms = a.elapsed_time(b)
+        best = ms if best is None else min(best, ms)
+    return blocks * 512.0 * iters * 256.0 / (best * 1e-3) / 1e12
 
 
 def ncu_traffic():
@@ -240,7 +289,7 @@ def main():
     solver = Radiation_solver(tables["lw"], tables["sw"], tables["cloud_lw"], tables["cloud_sw"], S.ATM_GASES)
     fused = Fused_solver(solver)
     run_lw = fused.solve_lw if args.path == "fused" else solver.solve_lw
-    run_sw = solver.solve_sw
+    run_sw = fused.solve_sw if args.path == "fused" else solver.solve_sw
     atm = atm_to_device(atm_np, torch.float32, dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
@@ -255,9 +304,10 @@ def main():
             run_lw(atm)
             run_sw(atm)
             return
-        a, b = timed_events
+        a, m, b = timed_events
         a.record(stream)
         run_lw(atm)
+        m.record(stream)
         run_sw(atm)
         b.record(stream)
 
@@ -326,7 +376,7 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     sampler.start()
-    evs = [evpair() for _ in range(args.steps)]
+    evs = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(3)) for _ in range(args.steps)]
     for i in range(args.steps):
         flush.zero_()          # L2 flush between timed steps (outside the events)
         step(evs[i])
@@ -335,7 +385,9 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     clocks = sampler.stop()
-    step_ms = [a.elapsed_time(b) for a, b in evs]
+    step_ms = [a.elapsed_time(b) for a, m, b in evs]
+    lw_ms = float(np.mean([a.elapsed_time(m) for a, m, b in evs]))
+    sw_ms = float(np.mean([m.elapsed_time(b) for a, m, b in evs]))
     total_ms = float(np.sum(step_ms))
     t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
     if world > 1:
@@ -345,17 +397,35 @@ def main():
     value = world * args.ncol * args.steps / (total_ms * 1e-3)
 
     # Per-kernel durations and roofline of the dominant kernel.
-    breakdown = staged_breakdown(3)
-    bpc = bytes_per_column(args.nlay)
-    dom = max(breakdown, key=breakdown.get)
-    peak, peak_kind = measured_peaks()
-    achieved = bpc[dom] * args.ncol / (breakdown[dom] * 1e-3) / 1e9
     traffic = ncu_traffic()
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": traffic[dom] * args.ncol if dom in traffic else None,
-                "algorithmic_bytes": bpc[dom] * args.ncol,
-                "kernel_ms": {k: round(v, 4) for k, v in breakdown.items()}}
+    hbm_peak, peak_kind = measured_peaks()
+    if args.path == "fused":
+        # One kernel per solve: the events around each solve inside the timed steps time it.
+        breakdown = {"lw_forward_kernel": lw_ms, "sw_forward_kernel": sw_ms}
+        dom = max(breakdown, key=breakdown.get)
+        fpc = fused_flops_per_column(args.nlay)
+        bpc = fused_bytes_per_column(args.nlay)
+        peak_tf = fp32_peak(torch, dev, stream)
+        achieved = fpc[dom] * args.ncol / (breakdown[dom] * 1e-3) / 1e12
+        hbm_ach = bpc[dom] * args.ncol / (breakdown[dom] * 1e-3) / 1e9
+        roofline = {"bound": "fp32", "kernel": dom, "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
+                    "frac": achieved / peak_tf,
+                    "peak_source": "measured: FP32 FMA probe (rrtmgp_b200_fp32_fma_probe) on this GPU",
+                    "traffic": traffic[dom] * args.ncol if dom in traffic else None,
+                    "algorithmic_flops": fpc[dom] * args.ncol, "algorithmic_bytes": bpc[dom] * args.ncol,
+                    "hbm": {"achieved": hbm_ach, "peak": hbm_peak, "unit": "GB/s", "frac": hbm_ach / hbm_peak,
+                            "peak_source": peak_kind},
+                    "kernel_ms": {k: round(v, 4) for k, v in breakdown.items()}}
+    else:
+        breakdown = staged_breakdown(3)
+        bpc = bytes_per_column(args.nlay)
+        dom = max(breakdown, key=breakdown.get)
+        achieved = bpc[dom] * args.ncol / (breakdown[dom] * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                    "frac": achieved / hbm_peak, "peak_source": peak_kind,
+                    "traffic": traffic[dom] * args.ncol if dom in traffic else None,
+                    "algorithmic_bytes": bpc[dom] * args.ncol,
+                    "kernel_ms": {k: round(v, 4) for k, v in breakdown.items()}}
 
     # End to end through the public API with host buffers (pinned), copies in the timed region.
     in_keys = ["play", "plev", "tlay", "tlev", "tsfc", "lwp", "iwp", "rel", "rei", "mu0", "emis_sfc",
@@ -417,11 +487,20 @@ def main():
             e64[i][1].record(stream)
         torch.cuda.synchronize()
         ms64 = float(np.mean([a.elapsed_time(b) for a, b in e64]))
-        fp64 = {"value": args.ncol / (ms64 * 1e-3), "unit": "columns/s", "ms_per_step": ms64}
+        # Accuracy of the timed FP32 path against this FP64 forward on the bench workload.
+        r_lw, r_sw = solver.solve_lw(atm64), solver.solve_sw(atm64)
+        f_lw, f_sw = run_lw(atm), run_sw(atm)
+        ferr = max(float((f[k].double() - r[k]).abs().max()) for f, r in ((f_lw, r_lw), (f_sw, r_sw))
+                   for k in ("flux_up", "flux_dn", "flux_net"))
+        herr = max(float((f["heating_rate"].double() - r["heating_rate"]).abs().max())
+                   for f, r in ((f_lw, r_lw), (f_sw, r_sw)))
+        fp64 = {"value": args.ncol / (ms64 * 1e-3), "unit": "columns/s", "ms_per_step": ms64,
+                "fp32_max_flux_err_w_m2": ferr, "fp32_max_heating_rate_err_k_day": herr}
         del atm64
         solver._bufs = {k: v for k, v in solver._bufs.items() if k[0][2] != torch.float64}
 
-    launches_per_step = 6 + 8  # LW: gas, cloud, add_to, rte, reduce, heating; SW: + spread, delta
+    # staged: LW gas, cloud, add_to, rte, reduce, heating; SW the same + spread, delta.
+    launches_per_step = 2 if args.path == "fused" else 6 + 8
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, tables, args.cpu_seconds)

@@ -376,6 +376,12 @@ int rrtmgp_b200_forward_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int
         float* flux_up, float* flux_dn, float* flux_dn_dir, float* flux_net,
         float* heating_rate, int chunk, void* stream);
 
+/* No reference counterpart: FP32 FMA throughput probe used as the FP32-pipe roofline
+ * denominator by the benchmark.  blocks x 512 threads, iters x 128 FMAs per thread
+ * (FLOP = blocks * 512 * iters * 256); out (blocks floats) is written only in a case that
+ * does not occur. */
+int rrtmgp_b200_fp32_fma_probe(int blocks, int iters, float* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

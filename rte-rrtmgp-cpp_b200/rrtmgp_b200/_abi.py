@@ -200,6 +200,7 @@ _SIGS = {
                                         _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
     "rrtmgp_b200_forward_sw_f32": (_I, [_P, _P, _I, _I, _P, _P, _P, _P, C.POINTER(GasConc), _I,
                                         _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
+    "rrtmgp_b200_fp32_fma_probe": (_I, [_I, _I, _P, _P]),
 }
 SW_STATIC_SCRATCH_MAX_ELEMS = 1048576
 _FP_SIGS = {

@@ -33,22 +33,22 @@ struct CloudArgs {
 
 // Layer transmissivity complement and sources in FP32: series below tau = 0.1 (7 and 6 terms,
 // truncation < 2e-11 relative), exp/divide intrinsics above where no cancellation occurs.
-// Same physics as lw_solver_noscat_step_1_kernel (rte_solver_kernels.cu:116-125).
+// Both forms are evaluated and one is selected, so the warp does not diverge.  Same physics
+// as lw_solver_noscat_step_1_kernel (rte_solver_kernels.cu:116-125).
 __device__ __forceinline__ void lw_layer_fast(float tau, float D, float lay, float ldn, float lup, float& omt,
                                               float& sdn, float& sup)
 {
     const float tl = tau * D;
-    float fact;
-    if (tl < 0.1f) {
-        omt = tl * (1.f + tl * (-0.5f + tl * (1.f / 6.f + tl * (-1.f / 24.f + tl * (1.f / 120.f +
-              tl * (-1.f / 720.f + tl * (1.f / 5040.f)))))));
-        fact = tl * (0.5f + tl * (-1.f / 3.f + tl * (0.125f + tl * (-1.f / 30.f + tl * (1.f / 144.f -
-               tl * (1.f / 840.f))))));
-    } else {
-        const float trans = __expf(-tl);
-        omt = 1.f - trans;
-        fact = __fdividef(omt, tl) - trans;
-    }
+    const float s_omt = tl * (1.f + tl * (-0.5f + tl * (1.f / 6.f + tl * (-1.f / 24.f + tl * (1.f / 120.f +
+                        tl * (-1.f / 720.f + tl * (1.f / 5040.f)))))));
+    const float s_fact = tl * (0.5f + tl * (-1.f / 3.f + tl * (0.125f + tl * (-1.f / 30.f + tl * (1.f / 144.f -
+                         tl * (1.f / 840.f))))));
+    const float trans = __expf(-tl);
+    const float e_omt = 1.f - trans;
+    const float e_fact = __fdividef(e_omt, tl) - trans;
+    const bool thin = tl < 0.1f;
+    omt = thin ? s_omt : e_omt;
+    const float fact = thin ? s_fact : e_fact;
     sdn = omt * ldn + 2.f * fact * (lay - ldn);
     sup = omt * lup + 2.f * fact * (lay - lup);
 }
@@ -114,8 +114,10 @@ lw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const CloudA
         const int b0 = k.group_band0[gg];
         const int gband = gv ? k.gpt2band[g] : b0;
         const int slot = gband - b0;
-        const int4 mg0 = gv ? __ldg(k.minor_g[0] + g) : make_int4(0, 0, 0, 0);
-        const int4 mg1 = gv ? __ldg(k.minor_g[1] + g) : make_int4(0, 0, 0, 0);
+        const int4 mg0 = minor_entry(k.minor_g[0], g, gv);
+        const int4 mg1 = minor_entry(k.minor_g[1], g, gv);
+        const int nm0 = __reduce_max_sync(0xffffffffu, mg0.x);
+        const int nm1 = __reduce_max_sync(0xffffffffu, mg1.x);
 
         // 1. records of this warp's chunk
         for (int r = lane; r < CL * k.max_group_bands; r += 32) {
@@ -135,9 +137,9 @@ lw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const CloudA
             omt[i] = 0.f; sdn[i] = 0.f; sup[i] = 0.f;
             if (j < nlay && gv) {
                 const Rec& R = recs[slot * CL + i];
-                const float tau = tau_abs(k, R, g, R.a ? mg1 : mg0) + R.aux.w;
-                const float4 p0 = __ldg(k.pfrac4 + size_t(R.kb.x) * ngpt + g);
-                const float4 p1 = __ldg(k.pfrac4 + size_t(R.kb.y) * ngpt + g);
+                const float tau = tau_abs(k, R, g, R.a ? mg1 : mg0, R.a ? nm1 : nm0) + R.aux.w;
+                const float4 p0 = __ldg(k.pfrac4 + (R.kb.x + g));
+                const float4 p1 = __ldg(k.pfrac4 + (R.kb.y + g));
                 const float pfrac = (R.wpl0.x * p0.x + R.wpl0.y * p0.y + R.wpl0.z * p0.z + R.wpl0.w * p0.w) +
                                     (R.wpl1.x * p1.x + R.wpl1.y * p1.y + R.wpl1.z * p1.z + R.wpl1.w * p1.w);
                 lw_layer_fast(tau, D, pfrac * R.aux.x, pfrac * R.aux.z, pfrac * R.aux.y, omt[i], sdn[i], sup[i]);

@@ -44,16 +44,15 @@ struct SwCloudArgs {
 
 // 1 - exp(-x) and exp(-x) for x >= 0, each with a small relative error: Taylor series of
 // 1 - exp(-x) through x^8 below 0.5 (truncation < 1.4e-8 relative), the exp intrinsic above.
+// Both are evaluated and selected (no divergence between the lanes of a warp).
 __device__ __forceinline__ void one_minus_exp(float x, float& E, float& e)
 {
-    if (x < 0.5f) {
-        E = x * (1.f - x * (1.f / 2.f - x * (1.f / 6.f - x * (1.f / 24.f - x * (1.f / 120.f - x * (1.f / 720.f -
-            x * (1.f / 5040.f - x * (1.f / 40320.f))))))));
-        e = 1.f - E;
-    } else {
-        e = __expf(-x);
-        E = 1.f - e;
-    }
+    const float Es = x * (1.f - x * (1.f / 2.f - x * (1.f / 6.f - x * (1.f / 24.f - x * (1.f / 120.f - x * (1.f / 720.f -
+                     x * (1.f / 5040.f - x * (1.f / 40320.f))))))));
+    const float ex = __expf(-x);
+    const bool small = x < 0.5f;
+    E = small ? Es : 1.f - ex;
+    e = small ? 1.f - Es : ex;
 }
 
 // Layer coefficients of the PIFM two-stream (sw_2stream_function, rte_solver_kernels.cu:
@@ -68,7 +67,8 @@ __device__ __forceinline__ void one_minus_exp(float x, float& E, float& e)
 // Near the removable singularity k mu0 = 1 (|1 - (k mu0)^2| < 0.02) Rdir and Tdir come from
 // the reference expressions in FP64 (FP64 island).  omw = 1 - w0 is passed separately, formed
 // from absorption optical depths, so it keeps its accuracy for w0 -> 1.  Clamps and k_min are
-// those of the FP64 reference (DBL_EPSILON, 1e-12).
+// those of the FP64 reference (DBL_EPSILON, 1e-12).  Divisions and the square root use the
+// approximate intrinsics (a few ulp; the operands are normal numbers).
 __device__ __forceinline__ void sw_layer_fast(float tau, float w0, float omw, float g, float mu0, float mu0_inv,
                                               float& R, float& T, float& Rdir, float& Tdir, float& Tn,
                                               float& adif, float& adir)
@@ -80,13 +80,14 @@ __device__ __forceinline__ void sw_layer_fast(float tau, float w0, float omw, fl
     const float a1 = g1 * g4 + g2 * g3;
     const float a2 = g1 * g3 + g2 * g4;
     const float kk = 2.f * omw * (2.f - .5f * w0 * (1.f + 3.f * g));
-    const float k = sqrtf(fmaxf(kk, 1.e-12f));
+    const float kkc = fmaxf(kk, 1.e-12f);
+    const float k = kkc * rsqrtf(kkc);
     float E1, e1, En;
     one_minus_exp(k * tau, E1, e1);
     one_minus_exp(tau * mu0_inv, En, Tn);
     const float E2 = E1 * (2.f - E1);
     const float e2 = e1 * e1;
-    const float rt = 1.f / (k * (1.f + e2) + g1 * E2);
+    const float rt = __fdividef(1.f, k * (1.f + e2) + g1 * E2);
     R = rt * g2 * E2;
     T = rt * 2.f * k * e1;
     adif = rt * (k * E1 * E1 + 2.f * omw * E2);
@@ -98,13 +99,12 @@ __device__ __forceinline__ void sw_layer_fast(float tau, float w0, float omw, fl
         Rdir = float(Rr);
         Tdir = float(Tr);
     } else {
-        const float rt2 = w0 * rt / fact;
+        const float rt2 = __fdividef(w0 * rt, fact);
         const float br = E2 * (a2 - k * km * g3) + k * (g3 - mu0 * a2) * (E1 * E1 + 2.f * e1 * En);
-        float bt;
-        if (e1 < .5f && Tn < .5f)
-            bt = (1.f + km) * (a1 + k * g4) * Tn - (1.f - km) * (a1 - k * g4) * e2 * Tn - 2.f * (k * g4 + a1 * km) * e1;
-        else
-            bt = Tn * E2 * (a1 + k * km * g4) + k * (g4 + mu0 * a1) * (E1 * E1 - (1.f + e2) * En);
+        const float bt_thick =
+            (1.f + km) * (a1 + k * g4) * Tn - (1.f - km) * (a1 - k * g4) * e2 * Tn - 2.f * (k * g4 + a1 * km) * e1;
+        const float bt_thin = Tn * E2 * (a1 + k * km * g4) + k * (g4 + mu0 * a1) * (E1 * E1 - (1.f + e2) * En);
+        const float bt = (e1 < .5f && Tn < .5f) ? bt_thick : bt_thin;
         Rdir = rt2 * br;
         Tdir = -rt2 * bt;
     }
@@ -175,8 +175,10 @@ sw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
         const int b0 = k.group_band0[gg];
         const int gband = gv ? k.gpt2band[g] : b0;
         const int slot = gband - b0;
-        const int4 mg0 = gv ? __ldg(k.minor_g[0] + g) : make_int4(0, 0, 0, 0);
-        const int4 mg1 = gv ? __ldg(k.minor_g[1] + g) : make_int4(0, 0, 0, 0);
+        const int4 mg0 = minor_entry(k.minor_g[0], g, gv);
+        const int4 mg1 = minor_entry(k.minor_g[1], g, gv);
+        const int nm0 = __reduce_max_sync(0xffffffffu, mg0.x);
+        const int nm1 = __reduce_max_sync(0xffffffffu, mg1.x);
 
         for (int r = lane; r < CL * k.max_group_bands; r += 32) {
             const int jj = w * CL + (r % CL);
@@ -198,19 +200,19 @@ sw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
             float R = 0.f, T = 1.f, Rdir = 0.f, Tdir = 0.f, Tn = 1.f, adif = 0.f, adir = 0.f;
             if (j < nlay && gv) {
                 const Rec& Rc = recs[slot * CL + i];
-                const float ta = tau_abs(k, Rc, g, Rc.a ? mg1 : mg0);
-                const float2 r0 = __ldg(k.krayl2 + size_t(Rc.kr[0]) * ngpt + g);
-                const float2 r1 = __ldg(k.krayl2 + size_t(Rc.kr[1]) * ngpt + g);
+                const float ta = tau_abs(k, Rc, g, Rc.a ? mg1 : mg0, Rc.a ? nm1 : nm0);
+                const float2 r0 = __ldg(k.krayl2 + (Rc.kr[0] + g));
+                const float2 r1 = __ldg(k.krayl2 + (Rc.kr[1] + g));
                 const float tr = (Rc.fm.x * r0.x + Rc.fm.y * r0.y + Rc.fm.z * r1.x + Rc.fm.w * r1.y) * Rc.aux.x;
                 const float tau = ta + tr + Rc.aux.y;
                 const float ts = tr + Rc.aux.z;
                 float w0 = 0.f, omw = 1.f;
                 if (tau > 2.f * FLT_MIN) {
-                    const float inv = 1.f / tau;
+                    const float inv = __fdividef(1.f, tau);
                     w0 = ts * inv;
                     omw = (ta + Rc.aux2) * inv;
                 }
-                const float gasy = Rc.aux.w / fmaxf(ts, 3.f * FLT_MIN);
+                const float gasy = __fdividef(Rc.aux.w, fmaxf(ts, 3.f * FLT_MIN));
                 sw_layer_fast(tau, w0, omw, gasy, mu0, mu0_inv, R, T, Rdir, Tdir, Tn, adif, adir);
             }
             vR[i] = R;
@@ -221,7 +223,7 @@ sw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
             vAd[i] = adif;
             vAdir[i] = adir * P;
             // Add layer i below the composite of layers 0..i-1.
-            const float den = 1.f / fmaf(-cRd, R, 1.f);
+            const float den = __fdividef(1.f, fmaf(-cRd, R, 1.f));
             const float nRu = cRu + cT * cT * R * den;
             const float nRd = R + T * T * cRd * den;
             const float nU = cU + cT * (vSu[i] + R * cD) * den;
@@ -270,7 +272,7 @@ sw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
             }
             const float4 m = sm_comp[c * 32 + lane];
             const float D = sm_compd[c * 32 + lane];
-            const float den = 1.f / fmaf(-m.y, alb, 1.f);
+            const float den = __fdividef(1.f, fmaf(-m.y, alb, 1.f));
             if (c < w) {
                 const float F = m.z * den, G = fmaf(m.y, src, D) * den;
                 fb = fmaf(fa, G, fb);
@@ -288,7 +290,7 @@ sw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
 #pragma unroll
             for (int i = CL - 1; i >= 0; --i) {
                 const float su = vSu[i] * dtop, sd = vSd[i] * dtop;
-                const float den = 1.f / fmaf(-vR[i], a, 1.f);
+                const float den = __fdividef(1.f, fmaf(-vR[i], a, 1.f));
                 const float na = vR[i] + vT[i] * vT[i] * a * den;
                 const float ns = su + vT[i] * fmaf(a, sd, s) * den;
                 vSd[i] = sd;
@@ -306,7 +308,7 @@ sw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
             const float a_n = (i + 1 < CL) ? vA[i + 1] : alb_in;
             const float s_n = (i + 1 < CL) ? vSu[i + 1] : src_in;
             const float fu = fmaf(fd, vA[i], vSu[i]);
-            const float den = 1.f / fmaf(-vR[i], a_n, 1.f);
+            const float den = __fdividef(1.f, fmaf(-vR[i], a_n, 1.f));
             const float fdn = (vT[i] * fd + vR[i] * s_n + vSd[i]) * den;
             const float fun = fmaf(fdn, a_n, s_n);
             vUp[i] = fu;

@@ -29,8 +29,8 @@ struct __align__(16) LayerState {
 
 // Per (layer, band) record.
 struct __align__(16) Rec {
-    int4 kb;          // x, y: packed kmaj4/pfrac4 rows of (t0, p0, e0) and (t1, p0, e1);
-                      // z, w: kmin2 rows of (t0, e0) and (t1, e1)
+    int4 kb;          // x, y: element offsets (row * ngpt) of the kmaj4/pfrac4 rows of
+                      //       (t0, p0, e0) and (t1, p0, e1); z, w: kmin2 row offsets of (t0, e0), (t1, e1)
     float4 wmaj0, wmaj1;   // col_mix x fmajor (major absorption weights)
     float4 wpl0, wpl1;     // fmajor (Planck fractions; SW: unused)
     float4 fm;             // fminor (minor and Rayleigh weights)
@@ -40,7 +40,7 @@ struct __align__(16) Rec {
     float aux2;            // LW: surface Planck function (bottom layer only)
                            // SW: cloud absorption optical depth tau_c * (1 - ssa_c)
     int a;                 // 0 lower / 1 upper atmosphere
-    int kr[2];             // krayl2 rows of (a, t0, e0) and (a, t1, e1)
+    int kr[2];             // element offsets (row * ngpt) of the krayl2 rows of (a, t0, e0), (a, t1, e1)
 };
 
 // Reduce-scatter of N per-lane values over 32 lanes: afterwards lane L holds in v[0] the warp
@@ -95,8 +95,8 @@ __device__ __forceinline__ void record_weights(const KdistView<float>& k, Rec& R
     const FlavorWeights<float> fw = flavor_weights(k, flav, li, cg, cgs);
     const int ne1 = k.neta - 1, np = k.npres;
     const int p0 = li.jp + li.itropo - 1;
-    R.kb.x = ((li.jt - 1) * np + p0) * ne1 + (fw.j0 - 1);
-    R.kb.y = (li.jt * np + p0) * ne1 + (fw.j1 - 1);
+    R.kb.x = (((li.jt - 1) * np + p0) * ne1 + (fw.j0 - 1)) * k.ngpt;
+    R.kb.y = ((li.jt * np + p0) * ne1 + (fw.j1 - 1)) * k.ngpt;
     const int a = li.itropo;
     const int nc = k.ncontrib[a] > 0 ? k.ncontrib[a] : 1;
     // kmin2 rows; the Rayleigh rows (krayl2, [a][t][eta][g]) follow the same (t, eta) corners.
@@ -109,8 +109,8 @@ __device__ __forceinline__ void record_weights(const KdistView<float>& k, Rec& R
     R.wmaj1 = make_float4(fw.cm[1] * R.wpl1.x, fw.cm[1] * R.wpl1.y, fw.cm[1] * R.wpl1.z, fw.cm[1] * R.wpl1.w);
     R.fm = make_float4(fw.fm[0], fw.fm[1], fw.fm[2], fw.fm[3]);
     R.a = a;
-    R.kr[0] = (a * k.ntemp + li.jt - 1) * ne1 + (fw.j0 - 1);
-    R.kr[1] = (a * k.ntemp + li.jt) * ne1 + (fw.j1 - 1);
+    R.kr[0] = ((a * k.ntemp + li.jt - 1) * ne1 + (fw.j0 - 1)) * k.ngpt;
+    R.kr[1] = ((a * k.ntemp + li.jt) * ne1 + (fw.j1 - 1)) * k.ngpt;
     int n = 0;
     for (int ii = k.band_minor_begin[a][b]; ii < k.band_minor_begin[a][b + 1] && n < kMaxMinor; ++ii, ++n)
         R.scal[n] = minor_scaling(k, a, k.band_minor_list[a][ii], cg, cgs, s.p, s.t);
@@ -118,27 +118,37 @@ __device__ __forceinline__ void record_weights(const KdistView<float>& k, Rec& R
 
 // Absorption optical depth of g-point g from a record: major (8 corners via two float4 loads)
 // plus the minor intervals covering g (minor_g list), as gas_optical_depths_major/minor.
-__device__ __forceinline__ float tau_abs(const KdistView<float>& k, const Rec& R, int g, int4 mg)
+// nmax = most intervals over the warp's lanes (warp-uniform loop bound); lanes with fewer
+// intervals read a valid entry and discard it with a select, so the loop does not diverge.
+__device__ __forceinline__ float tau_abs(const KdistView<float>& k, const Rec& R, int g, int4 mg, int nmax)
 {
-    const int ngpt = k.ngpt;
-    const float4 c0 = __ldg(k.kmaj4 + size_t(R.kb.x) * ngpt + g);
-    const float4 c1 = __ldg(k.kmaj4 + size_t(R.kb.y) * ngpt + g);
+    const float4 c0 = __ldg(k.kmaj4 + (R.kb.x + g));
+    const float4 c1 = __ldg(k.kmaj4 + (R.kb.y + g));
     float tau = R.wmaj0.x * c0.x + R.wmaj0.y * c0.y + R.wmaj0.z * c0.z + R.wmaj0.w * c0.w +
                 R.wmaj1.x * c1.x + R.wmaj1.y * c1.y + R.wmaj1.z * c1.z + R.wmaj1.w * c1.w;
-    if (mg.x > 0) {
-        const float2* kn = k.kmin2[R.a];
+    const float2* kn = k.kmin2[R.a];
 #pragma unroll
-        for (int n = 0; n < 3; ++n) {
-            if (n < mg.x) {
-                const int code = n == 0 ? mg.y : (n == 1 ? mg.z : mg.w);
-                const int c = code >> 4;
-                const float2 lo = __ldg(kn + R.kb.z + c);
-                const float2 hi = __ldg(kn + R.kb.w + c);
-                tau += R.scal[code & 15] * (R.fm.x * lo.x + R.fm.y * lo.y + R.fm.z * hi.x + R.fm.w * hi.y);
-            }
+    for (int n = 0; n < 3; ++n) {
+        if (n < nmax) {
+            const int code = n == 0 ? mg.y : (n == 1 ? mg.z : mg.w);
+            const int c = code >> 4;
+            const float2 lo = __ldg(kn + (R.kb.z + c));
+            const float2 hi = __ldg(kn + (R.kb.w + c));
+            const float t = R.scal[code & 15] * (R.fm.x * lo.x + R.fm.y * lo.y + R.fm.z * hi.x + R.fm.w * hi.y);
+            tau += (n < mg.x) ? t : 0.f;
         }
     }
     return tau;
+}
+
+// minor_g entry of g-point g with unused slots set to the first used one (or to contributor 0,
+// slot 0), so that tau_abs can read every slot below the warp's maximum count.
+__device__ __forceinline__ int4 minor_entry(const int4* mgt, int g, bool valid)
+{
+    int4 m = valid ? __ldg(mgt + g) : make_int4(0, 0, 0, 0);
+    if (m.x < 2) m.z = m.y;
+    if (m.x < 3) m.w = m.y;
+    return m;
 }
 
 // Fill the per-layer state of column icol (layers counted from the top) and col_gas.

@@ -376,6 +376,27 @@ int rrtmgp_b200_forward_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int
         float* flux_up, float* flux_dn, float* flux_dn_dir, float* flux_net,
         float* heating_rate, int chunk, void* stream);
 
+/* Longwave adjoint of rrtmgp_b200_forward_lw_f32 (no reference counterpart; the reference
+ * has only the disabled surface Jacobian of lw_transport_noscat_kernel,
+ * rte_solver_kernels.cu:56-91, Rte_lw.cu:133).  Same inputs as the forward plus the seeds of
+ * L = sum(seed_flux_up * flux_up + seed_flux_dn * flux_dn) + sum(seed_heating_rate * HR)
+ * ((ncol, nlay+1), (ncol, nlay+1), (ncol, nlay); NULL = zero; fold a flux_net seed in as
+ * dn += s, up -= s).  Writes dL/dx for x = tlay, h2o and o3 volume mixing ratios (ncol, nlay),
+ * tlev (ncol, nlay+1), tsfc (ncol), and lwp, iwp, rel, rei (ncol, nlay; zero where the water
+ * path is not positive).  Any output may be NULL.  The vmr gradients treat each gas as a
+ * (ncol, nlay) field whatever its given shape; with col_dry == NULL the dry-air column's
+ * dependence on h2o is included.  Forward optical properties are recomputed per group of
+ * 32 g-points on chip, nothing is stored between forward and adjoint.  chunk: 8 or 16
+ * layers per warp (0 = 8); the k-distribution's bands must hold 16 or more g-points each. */
+int rrtmgp_b200_adjoint_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int ncol, int nlay,
+        const float* play, const float* plev, const float* tlay, const float* tlev,
+        const float* tsfc, const float* col_dry, const rrtmgp_b200_gas_conc* gases, int ngases,
+        const float* lwp, const float* iwp, const float* rel, const float* rei,
+        const float* sfc_emis, const float* seed_flux_up, const float* seed_flux_dn,
+        const float* seed_heating_rate, float* grad_tlay, float* grad_tlev, float* grad_tsfc,
+        float* grad_h2o, float* grad_o3, float* grad_lwp, float* grad_iwp, float* grad_rel,
+        float* grad_rei, int chunk, void* stream);
+
 /* No reference counterpart: FP32 FMA throughput probe used as the FP32-pipe roofline
  * denominator by the benchmark.  blocks x 512 threads, iters x 128 FMAs per thread
  * (FLOP = blocks * 512 * iters * 256); out (blocks floats) is written only in a case that

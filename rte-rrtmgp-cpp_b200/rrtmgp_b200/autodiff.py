@@ -1,0 +1,122 @@
+"""Differentiable column radiation: torch.autograd.Function wrappers of the fused FP32
+forward kernels whose backward calls the hand-written adjoint kernels through the C ABI
+(rrtmgp_b200_adjoint_lw_f32).
+
+    out = longwave(fused_solver, atm)            # dict of flux_up, flux_dn, flux_net, heating_rate
+    loss = (out["heating_rate"] * w).sum()
+    loss.backward()                              # atm["tlay"].grad, atm["gases"]["h2o"].grad, ...
+
+Differentiable inputs: tlay, tlev, tsfc, the h2o and o3 volume mixing ratios, and (with
+clouds) lwp, iwp, rel, rei.  Pressures, emissivity and the other gases are constants.  The
+backward recomputes the optical properties on chip (nothing of the forward is kept but its
+inputs), so memory does not grow with the number of g-points.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from . import _abi, api
+
+_DIFF_KEYS = ("tlay", "tlev", "tsfc", "h2o", "o3", "lwp", "iwp", "rel", "rei")
+
+
+def _reduce_to(grad, like):
+    """Sum a (nlay, ncol) field gradient down to the shape of a scalar / profile input."""
+    if grad is None or like is None:
+        return None
+    if like.numel() == grad.numel():
+        return grad.reshape(like.shape)
+    if like.numel() == 1:
+        return grad.sum().reshape(like.shape)
+    return grad.sum(dim=1).reshape(like.shape)   # profile: one value per layer
+
+
+class _LongwaveFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, fused, static, tlay, tlev, tsfc, h2o, o3, lwp, iwp, rel, rei):
+        atm = dict(static)
+        atm.update(tlay=tlay, tlev=tlev, tsfc=tsfc, lwp=lwp, iwp=iwp, rel=rel, rei=rei)
+        gases = dict(static["gases"])
+        gases["h2o"], gases["o3"] = h2o, o3
+        atm["gases"] = gases
+        clouds = lwp is not None
+        out = fused.solve_lw(atm, with_clouds=clouds)
+        res = tuple(out[k].clone() for k in ("flux_up", "flux_dn", "flux_net", "heating_rate"))
+        ctx.fused, ctx.atm, ctx.clouds = fused, atm, clouds
+        ctx.save_for_backward(tlay, tlev, tsfc, h2o, o3)
+        return res
+
+    @staticmethod
+    def backward(ctx, g_up, g_dn, g_net, g_hr):
+        atm, fused = ctx.atm, ctx.fused
+        play = atm["play"]
+        nlay, ncol = play.shape
+        dev = play.device
+
+        def seed(g):
+            return None if g is None else g.float().contiguous()
+
+        up, dn, net = seed(g_up), seed(g_dn), seed(g_net)
+        if net is not None:
+            up = -net if up is None else up - net
+            dn = net if dn is None else dn + net
+        hr = seed(g_hr)
+        grads = {k: torch.empty((nlay, ncol), dtype=torch.float32, device=dev)
+                 for k in ("tlay", "h2o", "o3", "lwp", "iwp", "rel", "rei")}
+        grads["tlev"] = torch.empty((nlay + 1, ncol), dtype=torch.float32, device=dev)
+        grads["tsfc"] = torch.empty((ncol,), dtype=torch.float32, device=dev)
+        P = api._ptr
+        arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay)
+        c = fused.base.clw if ctx.clouds else None
+        cl = (lambda k: P(atm[k])) if c else (lambda k: None)
+        _abi.check(_abi.load().rrtmgp_b200_adjoint_lw_f32(
+            fused.base.klw.handle, c.handle if c else None, ncol, nlay, P(play), P(atm["plev"]), P(atm["tlay"]),
+            P(atm["tlev"]), P(atm["tsfc"]), None, arr, len(atm["gases"]), cl("lwp"), cl("iwp"), cl("rel"),
+            cl("rei"), P(atm["emis_sfc"]), P(up), P(dn), P(hr), P(grads["tlay"]), P(grads["tlev"]),
+            P(grads["tsfc"]), P(grads["h2o"]), P(grads["o3"]), P(grads["lwp"]) if c else None,
+            P(grads["iwp"]) if c else None, P(grads["rel"]) if c else None, P(grads["rei"]) if c else None,
+            0, api._stream()))
+        tlay, tlev, tsfc, h2o, o3 = ctx.saved_tensors
+        out = [None, None, grads["tlay"], grads["tlev"], grads["tsfc"], _reduce_to(grads["h2o"], h2o),
+               _reduce_to(grads["o3"], o3)]
+        out += [grads[k] if ctx.clouds else None for k in ("lwp", "iwp", "rel", "rei")]
+        return tuple(out)
+
+
+def longwave(fused, atm: dict, with_clouds: bool = True):
+    """Differentiable fused FP32 longwave solve.  atm as for Fused_solver.solve_lw; its
+    tlay, tlev, tsfc, gases["h2o"], gases["o3"], lwp, iwp, rel, rei may require grad."""
+    clouds = with_clouds and fused.base.clw is not None
+    static = {k: v for k, v in atm.items() if k not in _DIFF_KEYS}
+    static["gases"] = {k: v for k, v in atm["gases"].items()}
+    up, dn, net, hr = _LongwaveFn.apply(
+        fused, static, atm["tlay"], atm["tlev"], atm["tsfc"], atm["gases"]["h2o"], atm["gases"]["o3"],
+        atm["lwp"] if clouds else None, atm["iwp"] if clouds else None, atm["rel"] if clouds else None,
+        atm["rei"] if clouds else None)
+    return {"flux_up": up, "flux_dn": dn, "flux_net": net, "heating_rate": hr}
+
+
+def adjoint_lw(fused, atm: dict, seed_up=None, seed_dn=None, seed_hr=None, with_clouds: bool = True, chunk: int = 0):
+    """Direct call of the longwave adjoint: dict of gradients of
+    sum(seed_up * flux_up + seed_dn * flux_dn + seed_hr * heating_rate)."""
+    play = atm["play"]
+    nlay, ncol = play.shape
+    dev = play.device
+    c = fused.base.clw if (with_clouds and fused.base.clw is not None) else None
+    grads = {k: torch.empty((nlay, ncol), dtype=torch.float32, device=dev)
+             for k in ("tlay", "h2o", "o3", "lwp", "iwp", "rel", "rei")}
+    grads["tlev"] = torch.empty((nlay + 1, ncol), dtype=torch.float32, device=dev)
+    grads["tsfc"] = torch.empty((ncol,), dtype=torch.float32, device=dev)
+    P = api._ptr
+    arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay)
+    cl = (lambda k: P(atm[k])) if c else (lambda k: None)
+    _abi.check(_abi.load().rrtmgp_b200_adjoint_lw_f32(
+        fused.base.klw.handle, c.handle if c else None, ncol, nlay, P(play), P(atm["plev"]), P(atm["tlay"]),
+        P(atm["tlev"]), P(atm["tsfc"]), None, arr, len(atm["gases"]), cl("lwp"), cl("iwp"), cl("rel"), cl("rei"),
+        P(atm["emis_sfc"]), P(seed_up), P(seed_dn), P(seed_hr), P(grads["tlay"]), P(grads["tlev"]),
+        P(grads["tsfc"]), P(grads["h2o"]), P(grads["o3"]), P(grads["lwp"]) if c else None,
+        P(grads["iwp"]) if c else None, P(grads["rel"]) if c else None, P(grads["rei"]) if c else None,
+        int(chunk), api._stream()))
+    return grads

@@ -1,0 +1,176 @@
+"""Adjoint kernels against FP64 central finite differences of the oracle.
+
+L = sum(seed_up * flux_up + seed_dn * flux_dn + seed_hr * heating_rate) with random seeds;
+the FP32 adjoint gradient of every input element is compared with (L(x+h) - L(x-h)) / 2h of
+the FP64 oracle forward, h = 1e-4 |x| (1e-3 |x| for the vmr fields; central differences),
+wherever |x| >= 1e-5 max|x| of its field (below that the FD resolves nothing).  Columns
+are independent, so one perturbation of a whole layer (or level) row gives the derivative of
+every column's own loss at once.  Bound: |adjoint - FD| <= GRAD_RTOL * max |FD| of that field
+(the FP32 forward itself agrees with FP64 to ~1e-5 relative; the rest is FD truncation and
+the rare cell or table node crossed by the step).  Also checks the torch.autograd path.
+"""
+import copy
+
+import numpy as np
+import pytest
+
+from rrtmgp_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+GRAD_RTOL = 3e-3
+REL_STEP = 1e-4
+REL_STEP_VMR = 1e-3   # tau is linear in the gas columns inside an interpolation cell
+
+
+def _seeds(nlay, ncol, rng):
+    return {"flux_up": rng.normal(size=(nlay + 1, ncol)), "flux_dn": rng.normal(size=(nlay + 1, ncol)),
+            "heating_rate": rng.normal(size=(nlay, ncol)) * 0.1}
+
+
+def _loss_cols(out, seeds):
+    return sum((seeds[k] * out[k]).sum(axis=0) for k in seeds)
+
+
+def _get(atm, key):
+    return atm["gases"][key] if key in ("h2o", "o3") else atm[key]
+
+
+def _fd(fwd, atm, seeds, key, rows=None):
+    """Per-column central differences of the FP64 loss w.r.t. every element of atm[key]."""
+    base = _get(atm, key)
+    grad = np.zeros_like(base, dtype=np.float64)
+    nrow = 1 if base.ndim == 1 else base.shape[0]
+    for j in (range(nrow) if rows is None else rows):
+        lp, lm = None, None
+        vals = base if base.ndim == 1 else base[j]
+        h = (REL_STEP_VMR if key in ("h2o", "o3") else REL_STEP) * np.maximum(np.abs(vals), 1e-30)
+        for sgn in (1.0, -1.0):
+            a = copy.deepcopy(atm)
+            arr = _get(a, key)
+            if arr.ndim == 1:
+                arr += sgn * h
+            else:
+                arr[j] += sgn * h
+            l = _loss_cols(fwd(a), seeds)
+            if sgn > 0:
+                lp = l
+            else:
+                lm = l
+        g = (lp - lm) / (2 * h)
+        if base.ndim == 1:
+            grad[:] = g
+        else:
+            grad[j] = g
+    return grad
+
+
+def _informative(x):
+    """Elements whose relative-step FD is meaningful: h2o and o3 fall to ~1e-20 (o3 to 0) near
+    the model top, where a relative step moves the loss by less than the FP64 oracle resolves
+    (its thin-layer source term carries ~eps/tau of noise)."""
+    return np.abs(x) >= 1e-5 * np.max(np.abs(x))
+
+
+def _check(name, got, ref, mask=None):
+    got = np.asarray(got, np.float64)
+    if mask is not None:
+        got, ref = got[mask], ref[mask]
+    scale = np.max(np.abs(ref))
+    assert scale > 0, f"{name}: zero reference gradient"
+    err = np.max(np.abs(got - ref)) / scale
+    assert err <= GRAD_RTOL, f"{name}: max |adjoint - FD| / max|FD| = {err:.3e}"
+
+
+def _lw_setup(tables, oracle_mod, ncol, nlay, seed, clouds, top_at_1=True):
+    atm = S.make_atmosphere(ncol, nlay, seed=seed, clouds=clouds, top_at_1=top_at_1)
+    kd = oracle_mod.GasOptics(tables["lw"], S.ATM_GASES)
+    cl = oracle_mod.CloudOptics(tables["cloud_lw"]) if clouds else None
+    return atm, (lambda a: oracle_mod.forward_lw(kd, cl, a))
+
+
+def _gpu_grads(tables, atm, seeds, clouds, chunk=0):
+    import torch
+    from rrtmgp_b200.autodiff import adjoint_lw
+    from rrtmgp_b200.solver import Fused_solver, Radiation_solver, atm_to_device
+    base = Radiation_solver(tables["lw"], tables["sw"], tables["cloud_lw"], tables["cloud_sw"], S.ATM_GASES)
+    fused = Fused_solver(base)
+    d = atm_to_device(atm, torch.float32, "cuda")
+    t = {k: torch.as_tensor(v, dtype=torch.float32, device="cuda").contiguous() for k, v in seeds.items()}
+    g = adjoint_lw(fused, d, t["flux_up"], t["flux_dn"], t["heating_rate"], with_clouds=clouds, chunk=chunk)
+    torch.cuda.synchronize()
+    return {k: v.double().cpu().numpy() for k, v in g.items()}
+
+
+@pytest.mark.parametrize("top_at_1", [True, False])
+@pytest.mark.parametrize("chunk", [8, 16])
+def test_lw_adjoint_matches_fd(oracle_mod, tables, gpu, top_at_1, chunk):
+    rng = np.random.default_rng(3)
+    ncol, nlay = 3, 24
+    atm, fwd = _lw_setup(tables, oracle_mod, ncol, nlay, seed=21, clouds=True, top_at_1=top_at_1)
+    seeds = _seeds(nlay, ncol, rng)
+    got = _gpu_grads(tables, atm, seeds, True, chunk)
+    for key in ("tlay", "tlev", "tsfc", "h2o", "o3"):
+        _check(f"d/d{key}", got[key], _fd(fwd, atm, seeds, key), _informative(_get(atm, key)))
+    cloudy_l = atm["lwp"] > 0
+    cloudy_i = atm["iwp"] > 0
+    if cloudy_l.any():
+        _check("d/dlwp", got["lwp"], _fd(fwd, atm, seeds, "lwp"), cloudy_l)
+        _check("d/drel", got["rel"], _fd(fwd, atm, seeds, "rel"), cloudy_l)
+    if cloudy_i.any():
+        _check("d/diwp", got["iwp"], _fd(fwd, atm, seeds, "iwp"), cloudy_i)
+        _check("d/drei", got["rei"], _fd(fwd, atm, seeds, "rei"), cloudy_i)
+
+
+def test_lw_adjoint_heating_rate_only_clear(oracle_mod, tables, gpu):
+    """Seed on heating rates only (the ~0.1 Pa top layers dominate), clear sky, 60 layers."""
+    rng = np.random.default_rng(4)
+    ncol, nlay = 2, 60
+    atm, fwd = _lw_setup(tables, oracle_mod, ncol, nlay, seed=22, clouds=False)
+    seeds = {"heating_rate": rng.normal(size=(nlay, ncol))}
+    import torch
+    from rrtmgp_b200.autodiff import adjoint_lw
+    from rrtmgp_b200.solver import Fused_solver, Radiation_solver, atm_to_device
+    base = Radiation_solver(tables["lw"], tables["sw"], tables["cloud_lw"], tables["cloud_sw"], S.ATM_GASES)
+    d = atm_to_device(atm, torch.float32, "cuda")
+    g = adjoint_lw(Fused_solver(base), d, None, None,
+                   torch.as_tensor(seeds["heating_rate"], dtype=torch.float32, device="cuda"), with_clouds=False)
+    for key in ("tlay", "h2o", "o3", "tlev"):
+        _check(f"HR d/d{key}", g[key].double().cpu().numpy(), _fd(fwd, atm, seeds, key), _informative(_get(atm, key)))
+
+
+def test_lw_autograd_directional(oracle_mod, tables, gpu):
+    """torch.autograd through the fused forward: grad . v against a directional central FD."""
+    import torch
+    from rrtmgp_b200.autodiff import longwave
+    from rrtmgp_b200.solver import Fused_solver, Radiation_solver, atm_to_device
+    rng = np.random.default_rng(5)
+    ncol, nlay = 16, 40
+    atm, fwd = _lw_setup(tables, oracle_mod, ncol, nlay, seed=23, clouds=True)
+    seeds = _seeds(nlay, ncol, rng)
+    base = Radiation_solver(tables["lw"], tables["sw"], tables["cloud_lw"], tables["cloud_sw"], S.ATM_GASES)
+    fused = Fused_solver(base)
+    d = atm_to_device(atm, torch.float32, "cuda")
+    leaves = [d["tlay"], d["tlev"], d["tsfc"], d["gases"]["h2o"], d["gases"]["o3"]]
+    for t in leaves:
+        t.requires_grad_(True)
+    out = longwave(fused, d)
+    loss = sum((torch.as_tensor(seeds[k], dtype=torch.float32, device="cuda") * out[k]).sum() for k in seeds)
+    loss.backward()
+    dirs = {"tlay": rng.normal(size=atm["tlay"].shape), "tlev": rng.normal(size=atm["tlev"].shape),
+            "tsfc": rng.normal(size=atm["tsfc"].shape), "h2o": rng.normal(size=atm["gases"]["h2o"].shape),
+            "o3": rng.normal(size=atm["gases"]["o3"].shape)}
+    scale = {"tlay": 1e-2, "tlev": 1e-2, "tsfc": 1e-2, "h2o": 1e-4, "o3": 1e-4}   # relative step per field
+    ad = 0.0
+    for key, t in zip(("tlay", "tlev", "tsfc", "h2o", "o3"), leaves):
+        ad += float((t.grad.double().cpu().numpy() * dirs[key] * scale[key] * np.abs(_get(atm, key))).sum())
+
+    def shifted(eps):
+        a = copy.deepcopy(atm)
+        for key in dirs:
+            arr = _get(a, key)
+            arr += eps * dirs[key] * scale[key] * np.abs(arr)
+        return _loss_cols(fwd(a), seeds).sum()
+
+    eps = 1e-3
+    fd = (shifted(eps) - shifted(-eps)) / (2 * eps)
+    assert abs(ad - fd) <= 2e-3 * abs(fd), f"directional derivative: autograd {ad:.6e} vs FD {fd:.6e}"

@@ -397,6 +397,24 @@ int rrtmgp_b200_adjoint_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int
         float* grad_h2o, float* grad_o3, float* grad_lwp, float* grad_iwp, float* grad_rel,
         float* grad_rei, int chunk, void* stream);
 
+/* Shortwave adjoint of rrtmgp_b200_forward_sw_f32 (no reference counterpart).  Same inputs as
+ * the forward plus the seeds of L = sum(seed_flux_up * flux_up + seed_flux_dn * flux_dn +
+ * seed_flux_dn_dir * flux_dn_dir) + sum(seed_heating_rate * HR) ((ncol, nlay+1) x 3,
+ * (ncol, nlay); NULL = zero; flux_dn includes the direct beam; fold a flux_net seed in as
+ * dn += s, up -= s).  Writes dL/dx for x = tlay, h2o and o3 volume mixing ratios, lwp, iwp,
+ * rel, rei (ncol, nlay) and the surface albedos (nband, ncol).  Any output may be NULL.  One
+ * thread-block cluster of ceil(nlay / 64) CTAs per column (nlay <= 512); the forward optical
+ * properties are recomputed on chip per group of 32 g-points. */
+int rrtmgp_b200_adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int ncol, int nlay,
+        const float* play, const float* plev, const float* tlay, const float* col_dry,
+        const rrtmgp_b200_gas_conc* gases, int ngases, const float* lwp, const float* iwp,
+        const float* rel, const float* rei, int delta_cloud, const float* mu0,
+        const float* tsi_scaling, const float* sfc_alb_dir, const float* sfc_alb_dif,
+        const float* seed_flux_up, const float* seed_flux_dn, const float* seed_flux_dn_dir,
+        const float* seed_heating_rate, float* grad_tlay, float* grad_h2o, float* grad_o3,
+        float* grad_lwp, float* grad_iwp, float* grad_rel, float* grad_rei,
+        float* grad_sfc_alb_dir, float* grad_sfc_alb_dif, void* stream);
+
 /* No reference counterpart: FP32 FMA throughput probe used as the FP32-pipe roofline
  * denominator by the benchmark.  blocks x 512 threads, iters x 128 FMAs per thread
  * (FLOP = blocks * 512 * iters * 256); out (blocks floats) is written only in a case that

@@ -1,0 +1,797 @@
+// Hand-written adjoint of the fused shortwave column forward (forward_sw.cu): gradients of
+//   L = sum_l (a_l F_up,l + b_l F_dn,l + c_l F_dir,l) + sum_i e_i HR_i
+// (F_dn includes the direct beam) with respect to the layer temperatures, the h2o and o3
+// volume mixing ratios, the cloud water paths and effective radii, and the surface albedos.
+// No reference counterpart exists.
+//
+// Layout: one thread-block cluster per column, CS = ceil(nlay / 64) CTAs of 8 warps; warp
+// w of CTA r owns the 8-layer chunk W = 8 r + w.  With 8 warps per CTA every thread has up to
+// 255 registers, enough to keep the ~16 per-layer values of the reverse sweeps of a chunk in
+// registers; chunk composites are exchanged through distributed shared memory with cluster
+// barriers.  Per group of 32 g-points the forward is recomputed (records, optical properties,
+// two-stream, direct beam, adding: as forward_sw.cu) and then reversed:
+//   F_i   (adjoint of the diffuse downward flux fd_i, bottom up)
+//         Fraw_i = T_i den_i Fc_(i+1) + b_i + h_i adif_i + a_i ubar_i^0,
+//         Fc_(i+1) = Fraw_(i+1) + h_i adif_i a_(i+1)
+//   (Abar, Sbar)_i (adjoints of the albedo a_i and upward source s_i, top down)
+//         Abar_(i+1) = (T den)^2 Abar_i + T den^2 (sdn + R s_(i+1)) Sbar_i + fd_(i+1) (R den Fc_(i+1) + ubar_(i+1))
+//         Sbar_(i+1) = T den Sbar_i + R den Fc_(i+1) + ubar_(i+1),  ubar_l = a_l + h_(l-1) adif_(l-1)
+//   Dbar_i (adjoint of the direct flux, bottom up)
+//         Dbar_i = b_i + c_i + h_i adir_i + sup_bar_i Rdir_i + sdn_bar_i Tdir_i + Tn_i Dbar_(i+1)
+// (den_i = 1 / (1 - R_i a_(i+1)), h_i = g/cp 86400 e_i / dp_i; HR is the per-layer absorbed
+// flux A_i = F_dir,i adir_i + (fd_i + fu_(i+1)) adif_i as in the forward).  Each recurrence is
+// affine in its adjoint (the albedo/source pair is 2x2 upper triangular), so chunks compose
+// exactly like the forward.  Per layer the adjoints of (R, T, Rdir, Tdir, Tn, adif, adir)
+// go through the two-stream (3-tangent dual numbers on the forward's FP32 formulas; FP64
+// central differences of the reference expressions in the k mu0 = 1 island), the
+// gas/Rayleigh/cloud combination, and the gas-optics interpolation (adjoint_common.cuh).
+#include <cooperative_groups.h>
+
+#include "adjoint_common.cuh"
+#include "dual.cuh"
+#include "sw_common.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace rrtmgp_b200 {
+namespace {
+
+using namespace fused;
+
+constexpr int kWPC = 8;            // warps per CTA
+constexpr int kCL = 8;             // layers per warp
+constexpr int kLPC = kWPC * kCL;   // layers per CTA
+
+struct SwAdjOut {
+    float* tlay;
+    float* h2o;
+    float* o3;
+    float* lwp;
+    float* iwp;
+    float* rel;
+    float* rei;
+    float* alb_dir;
+    float* alb_dif;
+};
+
+using D3 = Dual<3>;
+using D4 = Dual<4>;
+
+__device__ __forceinline__ void one_minus_exp_d(const D3& x, D3& E, D3& e)
+{
+    float Ev, ev;
+    one_minus_exp(x.v, Ev, ev);
+    E.v = Ev;
+    e.v = ev;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        E.d[i] = ev * x.d[i];
+        e.d[i] = -ev * x.d[i];
+    }
+}
+
+// sw_layer_fast (sw_common.cuh) with derivatives w.r.t. (tau, w0, g); omw = 1 - w0 moves with
+// w0.  out: R, T, Rdir, Tdir, Tn, adif, adir.
+__device__ __forceinline__ void sw_layer_dual(float tau, float w0, float omw, float g, float mu0, float mu0_inv,
+                                              D3 out[7])
+{
+    const D3 tw = dvar<3>(tau, 0), W = dvar<3>(w0, 1), G = dvar<3>(g, 2);
+    D3 O = dconst<3>(omw);
+    O.d[1] = -1.f;
+    const D3 g1 = 0.25f * (8.f - W * (5.f + 3.f * G));
+    const D3 g2 = 0.75f * (W * (1.f - G));
+    const D3 g3 = 0.25f * (2.f - (3.f * mu0) * G);
+    const D3 g4 = 1.f - g3;
+    const D3 a1 = g1 * g4 + g2 * g3;
+    const D3 a2 = g1 * g3 + g2 * g4;
+    const D3 kk = (2.f * O) * (2.f - 0.5f * (W * (1.f + 3.f * G)));
+    const D3 kkc = kk.v > 1.e-12f ? kk : dconst<3>(1.e-12f);
+    D3 k;
+    k.v = kkc.v * rsqrtf(kkc.v);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) k.d[i] = kkc.d[i] * 0.5f / k.v;
+    D3 E1, e1, En, Tn;
+    one_minus_exp_d(k * tw, E1, e1);
+    one_minus_exp_d(mu0_inv * tw, En, Tn);
+    const D3 E2 = E1 * (2.f - E1);
+    const D3 e2 = e1 * e1;
+    const D3 rt = ddiv(dconst<3>(1.f), k * (1.f + e2) + g1 * E2, true);
+    const D3 R = rt * g2 * E2;
+    const D3 T = rt * (2.f * k) * e1;
+    const D3 adif = rt * (k * E1 * E1 + (2.f * O) * E2);
+    const D3 km = mu0 * k;
+    const D3 fact = (1.f - km) * (1.f + km);
+    D3 Rdir, Tdir;
+    if (fabsf(fact.v) < 0.02f) {
+        // FP64 island (as the forward): reference expressions in double, central differences
+        double Rd, Td, Rr, Tr, Tn64;
+        sw_two_stream<double>(double(tau), double(w0), double(g), double(mu0), Rd, Td, Rr, Tr, Tn64);
+        Rdir = dconst<3>(float(Rr));
+        Tdir = dconst<3>(float(Tr));
+        const double ht = 1e-6 * fmax(double(tau), 1e-12), hw = 1e-6, hg = 1e-6;
+        const double steps[3] = {ht, hw, hg};
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            double Rp, Tp, Rm, Tm, x0, x1, x2;
+            sw_two_stream<double>(double(tau) + (i == 0 ? steps[i] : 0.0), double(w0) + (i == 1 ? steps[i] : 0.0),
+                                  double(g) + (i == 2 ? steps[i] : 0.0), double(mu0), x0, x1, Rp, Tp, x2);
+            sw_two_stream<double>(double(tau) - (i == 0 ? steps[i] : 0.0), double(w0) - (i == 1 ? steps[i] : 0.0),
+                                  double(g) - (i == 2 ? steps[i] : 0.0), double(mu0), x0, x1, Rm, Tm, x2);
+            Rdir.d[i] = float((Rp - Rm) / (2.0 * steps[i]));
+            Tdir.d[i] = float((Tp - Tm) / (2.0 * steps[i]));
+        }
+    } else {
+        const D3 rt2 = ddiv(W * rt, fact, true);
+        const D3 br = E2 * (a2 - k * km * g3) + k * (g3 - mu0 * a2) * (E1 * E1 + 2.f * (e1 * En));
+        const D3 bt_thick = (1.f + km) * (a1 + k * g4) * Tn - (1.f - km) * (a1 - k * g4) * e2 * Tn -
+                            2.f * ((k * g4 + a1 * km) * e1);
+        const D3 bt_thin = Tn * E2 * (a1 + k * km * g4) + k * (g4 + mu0 * a1) * (E1 * E1 - (1.f + e2) * En);
+        const D3 bt = (e1.v < .5f && Tn.v < .5f) ? bt_thick : bt_thin;
+        Rdir = rt2 * br;
+        Tdir = -(rt2 * bt);
+    }
+    const D3 tmin = dconst<3>(2.220446049250313e-16f);
+    Rdir = dmax(tmin, dmin(Rdir, En));
+    const D3 rest = En - Rdir;
+    Tdir = dmax(tmin, dmin(Tdir, rest));
+    const D3 adir = dmax(dconst<3>(0.f), rest - Tdir);
+    out[0] = R;
+    out[1] = T;
+    out[2] = Rdir;
+    out[3] = Tdir;
+    out[4] = Tn;
+    out[5] = adif;
+    out[6] = adir;
+}
+
+// Cloud optics of band b (2str, optionally delta-scaled) as duals over (lwp, iwp, rel, rei):
+// returns tau', tau' ssa', tau' ssa' g' as used by the SW record.
+__device__ __forceinline__ void cloud_sw_dual(const CloudLut<float>& L, int delta, float lwp, float iwp, float rel,
+                                              float rei, int b, D4& tau, D4& ts, D4& tsg)
+{
+    const CloudPoint<float> c = cloud_point(L, lwp, iwp, rel, rei);
+    const size_t nl = size_t(L.nband) * L.nsl, ni = size_t(L.nband) * L.nsi;
+    D4 lt = dconst<4>(0.f), lts = dconst<4>(0.f), ltg = dconst<4>(0.f);
+    D4 it = dconst<4>(0.f), its = dconst<4>(0.f), itg = dconst<4>(0.f);
+    auto lerp = [](const float* t, int i, const D4& f) {
+        const float d = t[i + 1] - t[i];
+        D4 r;
+        r.v = t[i] + f.v * d;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) r.d[q] = f.d[q] * d;
+        return r;
+    };
+    if (c.lwp > 0.f) {
+        D4 fl = dconst<4>(c.fl);
+        fl.d[2] = 1.f / L.liq_step;
+        const float* le = L.lut + size_t(b) * L.nsl;
+        lt = dvar<4>(c.lwp, 0) * lerp(le, c.il, fl);
+        lts = lt * lerp(le + nl, c.il, fl);
+        ltg = lts * lerp(le + 2 * nl, c.il, fl);
+    }
+    if (c.iwp > 0.f) {
+        D4 fi = dconst<4>(c.fi);
+        fi.d[3] = 1.f / L.ice_step;
+        const float* ie = L.lut + 3 * nl + size_t(b) * L.nsi;
+        it = dvar<4>(c.iwp, 1) * lerp(ie, c.ii, fi);
+        its = it * lerp(ie + ni, c.ii, fi);
+        itg = its * lerp(ie + 2 * ni, c.ii, fi);
+    }
+    const float eps = FLT_EPSILON;
+    D4 t = lt + it;
+    const D4 s_num = lts + its;
+    D4 ssa = ddiv(s_num, t.v > eps ? t : dconst<4>(eps), false);
+    D4 g = ddiv(ltg + itg, s_num.v > eps ? s_num : dconst<4>(eps), false);
+    if (delta) {
+        const float e3 = 3.f * FLT_MIN;
+        const D4 f = g * g;
+        const D4 wf = ssa * f;
+        t = t * (1.f - wf);
+        const D4 d1 = 1.f - wf, d2 = 1.f - f;
+        ssa = ddiv(ssa - wf, d1.v > e3 ? d1 : dconst<4>(e3), false);
+        g = ddiv(g - f, d2.v > e3 ? d2 : dconst<4>(e3), false);
+    }
+    tau = t;
+    ts = t * ssa;
+    tsg = ts * g;
+}
+
+struct SwAdjLayout {
+    size_t state, cg, seeds, clsum, albacc, x1, x2, x3, x4, x5, recs, drecs, total;
+};
+
+__host__ __device__ __forceinline__ SwAdjLayout sw_adj_layout(int ngas, int nband, int mgb)
+{
+    SwAdjLayout L;
+    L.state = 0;
+    L.cg = align16(L.state + sizeof(LayerState) * kLPC);
+    L.seeds = align16(L.cg + sizeof(float) * size_t(ngas + 1) * kLPC);
+    L.clsum = align16(L.seeds + sizeof(float) * (4 * (kLPC + 1)));
+    L.albacc = align16(L.clsum + sizeof(float) * size_t(nband) * kLPC * 3);
+    L.x1 = align16(L.albacc + sizeof(double) * size_t(nband) * 2);
+    L.x2 = align16(L.x1 + sizeof(float) * kWPC * 32);
+    L.x3 = align16(L.x2 + sizeof(float4) * kWPC * 32 * 2);
+    L.x4 = align16(L.x3 + sizeof(float2) * kWPC * 32);
+    L.x5 = align16(L.x4 + sizeof(float4) * kWPC * 32 * 2);
+    L.recs = align16(L.x5 + sizeof(float2) * kWPC * 32);
+    L.drecs = align16(L.recs + sizeof(Rec) * size_t(kWPC) * kCL * mgb);
+    L.total = align16(L.drecs + sizeof(DRec) * size_t(kWPC) * kCL * mgb);
+    return L;
+}
+
+template <typename Tp>
+__device__ __forceinline__ Tp* remote(cg::cluster_group& cl, Tp* p, int rank)
+{
+    return cl.map_shared_rank(p, rank);
+}
+
+__global__ void __launch_bounds__(256, 1)
+sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwCloudArgs cld, int ncol, int nlay, int CS,
+                  int idx_o3, int cd_internal, const float* __restrict__ play, const float* __restrict__ plev,
+                  const float* __restrict__ tlay, const float* __restrict__ col_dry_in,
+                  const float* __restrict__ mu0_in, const float* __restrict__ tsi_scaling,
+                  const float* __restrict__ alb_dir, const float* __restrict__ alb_dif,
+                  const float* __restrict__ seed_up, const float* __restrict__ seed_dn,
+                  const float* __restrict__ seed_dir, const float* __restrict__ seed_hr, const SwAdjOut out)
+{
+    constexpr int CL = kCL;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = int(cluster.block_rank());
+    const int icol = blockIdx.x / CS;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int Wg = rank * kWPC + w;
+    const int NWt = CS * kWPC;
+    const int L_end = NWt * CL;
+    const int j0 = rank * kLPC;          // first global layer of this CTA
+    const int nband = k.nband, mgb = k.max_group_bands;
+    const SwAdjLayout SL = sw_adj_layout(k.ngas, nband, mgb);
+    LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
+    float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
+    float* sm_al = reinterpret_cast<float*>(smem_raw + SL.seeds);   // seed F_up per local level (0..64)
+    float* sm_be = sm_al + (kLPC + 1);                                // seed F_dn
+    float* sm_ga = sm_be + (kLPC + 1);                                // seed F_dir
+    float* sm_hh = sm_ga + (kLPC + 1);                                // h per local layer
+    float* sm_cl = reinterpret_cast<float*>(smem_raw + SL.clsum);     // [band][layer][3] cloud adjoint sums
+    double* sm_alb = reinterpret_cast<double*>(smem_raw + SL.albacc); // [band][2]
+    float* sm_x1 = reinterpret_cast<float*>(smem_raw + SL.x1);
+    float4* sm_x2a = reinterpret_cast<float4*>(smem_raw + SL.x2);
+    float* sm_x2b = reinterpret_cast<float*>(sm_x2a + kWPC * 32);
+    float2* sm_x3 = reinterpret_cast<float2*>(smem_raw + SL.x3);
+    float4* sm_x4a = reinterpret_cast<float4*>(smem_raw + SL.x4);
+    float* sm_x4b = reinterpret_cast<float*>(sm_x4a + kWPC * 32);
+    float2* sm_x5 = reinterpret_cast<float2*>(smem_raw + SL.x5);
+    Rec* recs = reinterpret_cast<Rec*>(smem_raw + SL.recs) + w * CL * mgb;
+    DRec* drecs = reinterpret_cast<DRec*>(smem_raw + SL.drecs) + w * CL * mgb;
+
+    const bool top_at_1 = play[icol] < play[icol + size_t(nlay - 1) * ncol];
+    const float mu0 = mu0_in[icol];
+    const float mu0_inv = 1.f / mu0;
+    const float tsi = tsi_scaling ? tsi_scaling[icol] : 1.f;
+    auto seed_at = [&](const float* s, int lev) -> float {   // global level (top down) -> seed
+        if (!s || lev > nlay) return 0.f;
+        return s[icol + size_t(top_at_1 ? lev : nlay - lev) * ncol];
+    };
+
+    // ---- per-CTA set-up: its 64 layers ----
+    for (int jl = threadIdx.x; jl < kLPC; jl += blockDim.x) {
+        const int j = j0 + jl;
+        if (j >= nlay) continue;
+        const int l = top_at_1 ? j : nlay - 1 - j;
+        const size_t cl = icol + size_t(l) * ncol;
+        const float p = play[cl], t = tlay[cl];
+        fill_col_gas(k, gs, ncol, nlay, icol, l, plev, col_dry_in, sm_cg + jl, kLPC);
+        const LayerInterp<float> li = layer_interp(k, p, t);
+        const int lt = top_at_1 ? j : nlay - j, lb = top_at_1 ? j + 1 : nlay - 1 - j;
+        LayerState s;
+        s.jt = li.jt; s.jp = li.jp; s.itropo = li.itropo; s.pad = 0;
+        s.ftemp = li.ftemp; s.fpress = li.fpress; s.p = p; s.t = t;
+        s.t_top = 0.f; s.t_bot = 0.f;
+        s.dp = fabsf(plev[icol + size_t(lb) * ncol] - plev[icol + size_t(lt) * ncol]);
+        s.pad2 = 0.f;
+        st[jl] = s;
+    }
+    for (int ll = threadIdx.x; ll <= kLPC; ll += blockDim.x) {
+        sm_al[ll] = seed_at(seed_up, j0 + ll);
+        sm_be[ll] = seed_at(seed_dn, j0 + ll);
+        sm_ga[ll] = seed_at(seed_dir, j0 + ll);
+    }
+    for (int i = threadIdx.x; i < nband * kLPC * 3; i += blockDim.x) sm_cl[i] = 0.f;
+    for (int i = threadIdx.x; i < nband * 2; i += blockDim.x) sm_alb[i] = 0.0;
+    __syncthreads();
+    for (int jl = threadIdx.x; jl < kLPC; jl += blockDim.x) {
+        const int j = j0 + jl;
+        float h = 0.f;
+        if (j < nlay && seed_hr) {
+            const int l = top_at_1 ? j : nlay - 1 - j;
+            h = float(9.80665 / 1004.64 * 86400.0 * double(seed_hr[icol + size_t(l) * ncol]) / double(st[jl].dp));
+        }
+        sm_hh[jl] = h;
+    }
+    __syncthreads();
+
+    const int ngpt = k.ngpt;
+    // top / bottom boundary seeds (every thread walks the whole column)
+    const float al0 = seed_at(seed_up, 0);
+    const float alN = seed_at(seed_up, nlay), beN = seed_at(seed_dn, nlay), gaN = seed_at(seed_dir, nlay);
+    double acc_q = 0.0;   // RS<32> accumulator: lane L holds [T | H | O | -][L >> 3], layer L & 7
+    constexpr float m_dry = 0.028964f, m_h2o = 0.018016f;
+
+    for (int gg = 0; gg < k.ngroups; ++gg) {
+        const int g = 32 * gg + lane;
+        const bool gv = g < ngpt;
+        const int b0 = k.group_band0[gg];
+        const int gband = gv ? k.gpt2band[g] : b0;
+        const int slot = gband - b0;
+        const int4 mg0 = minor_entry(k.minor_g[0], g, gv);
+        const int4 mg1 = minor_entry(k.minor_g[1], g, gv);
+        const int nm0 = __reduce_max_sync(0xffffffffu, mg0.x);
+        const int nm1 = __reduce_max_sync(0xffffffffu, mg1.x);
+        const float ad = gv ? __ldg(alb_dir + gband + size_t(icol) * nband) : 0.f;
+        const float af = gv ? __ldg(alb_dif + gband + size_t(icol) * nband) : 0.f;
+
+        for (int r = lane; r < CL * mgb; r += 32) {
+            const int jl = w * CL + (r % CL);
+            const int jj = j0 + jl;
+            const int b = b0 + r / CL;
+            if (jj < nlay && b < nband && k.band_lims[2 * b] < 32 * gg + 32) {
+                const int l = top_at_1 ? jj : nlay - 1 - jj;
+                Rec& R = recs[r];
+                DRec& DR = drecs[r];
+                const LayerState s = st[jl];
+                build_sw_record(k, R, s, sm_cg + jl, kLPC, b, cld, icol + size_t(l) * ncol);
+                build_drec(k, DR, s, sm_cg + jl, kLPC, b, R.scal, idx_o3, cd_internal);
+                const float cd = sm_cg[jl];
+                const float vh = sm_cg[k.idx_h2o * kLPC + jl] / cd;
+                const float dcd_h = cd_internal ? -cd * m_h2o / (m_dry + m_h2o * vh) : 0.f;
+                DR.dB = make_float4(dcd_h * (1.f + vh) + cd, 0.f, 0.f, 0.f);   // d col_rayl / d vmr_h2o
+            }
+        }
+        __syncwarp();
+
+        // ---- forward pass 1 (recomputed): optical properties and two-stream per layer ----
+        float vTau[CL], vW0[CL], vOmw[CL], vG[CL];
+        float vR[CL], vT[CL], vRd[CL], vTd[CL], vTn[CL], vAf[CL], vAr[CL], vP[CL];
+        float P = 1.f;
+        float cRu = 0.f, cRd = 0.f, cT = 1.f, cU = 0.f, cD = 0.f;
+#pragma unroll
+        for (int i = 0; i < CL; ++i) {
+            const int jl = w * CL + i;
+            const int j = j0 + jl;
+            float R = 0.f, T = 1.f, Rdir = 0.f, Tdir = 0.f, Tn = 1.f, adif = 0.f, adir = 0.f;
+            float tau = 0.f, w0 = 0.f, omw = 1.f, gasy = 0.f;
+            if (j < nlay && gv) {
+                const Rec& Rc = recs[slot * CL + i];
+                const float ta = tau_abs(k, Rc, g, Rc.a ? mg1 : mg0, Rc.a ? nm1 : nm0);
+                const float2 r0 = __ldg(k.krayl2 + (Rc.kr[0] + g));
+                const float2 r1 = __ldg(k.krayl2 + (Rc.kr[1] + g));
+                const float tr = (Rc.fm.x * r0.x + Rc.fm.y * r0.y + Rc.fm.z * r1.x + Rc.fm.w * r1.y) * Rc.aux.x;
+                tau = ta + tr + Rc.aux.y;
+                const float ts = tr + Rc.aux.z;
+                if (tau > 2.f * FLT_MIN) {
+                    const float inv = __fdividef(1.f, tau);
+                    w0 = ts * inv;
+                    omw = (ta + Rc.aux2) * inv;
+                }
+                gasy = __fdividef(Rc.aux.w, fmaxf(ts, 3.f * FLT_MIN));
+                sw_layer_fast(tau, w0, omw, gasy, mu0, mu0_inv, R, T, Rdir, Tdir, Tn, adif, adir);
+            }
+            vTau[i] = tau; vW0[i] = w0; vOmw[i] = omw; vG[i] = gasy;
+            vR[i] = R; vT[i] = T; vRd[i] = Rdir; vTd[i] = Tdir; vTn[i] = Tn; vAf[i] = adif; vAr[i] = adir;
+            vP[i] = P;
+            const float su = Rdir * P, sd = Tdir * P;
+            const float den = __fdividef(1.f, fmaf(-cRd, R, 1.f));
+            const float nRu = cRu + cT * cT * R * den;
+            const float nRd = R + T * T * cRd * den;
+            const float nU = cU + cT * (su + R * cD) * den;
+            const float nD = sd + T * (cD + cRd * su) * den;
+            cT = cT * T * den;
+            cRu = nRu; cRd = nRd; cU = nU; cD = nD;
+            P *= Tn;
+        }
+        sm_x1[w * 32 + lane] = P;
+        cluster.sync();
+
+        // ---- X1: direct flux at the chunk top and the surface ----
+        const float toa = gv ? __ldg(k.solar_source + g) * tsi * mu0 : 0.f;
+        float dtop = toa;
+        for (int c = 0; c < Wg; ++c) dtop *= remote(cluster, sm_x1, c / kWPC)[(c % kWPC) * 32 + lane];
+        float dsfc = dtop;
+        for (int c = Wg; c < NWt; ++c) dsfc *= remote(cluster, sm_x1, c / kWPC)[(c % kWPC) * 32 + lane];
+        sm_x2a[w * 32 + lane] = make_float4(cRu, cRd, cT, cU * dtop);
+        sm_x2b[w * 32 + lane] = cD * dtop;
+        cluster.sync();
+
+        // ---- X2: albedo / source at the chunk bottom, incident diffuse flux at its top ----
+        float alb = af, src = dsfc * ad;
+        float alb_in = af, src_in = src;
+        float fa = 1.f, fb = 0.f;
+        for (int c = NWt - 1; c >= 0; --c) {
+            if (c == Wg) {
+                alb_in = alb;
+                src_in = src;
+                if (Wg == 0) break;
+            }
+            const float4 m = remote(cluster, sm_x2a, c / kWPC)[(c % kWPC) * 32 + lane];
+            const float Dc = remote(cluster, sm_x2b, c / kWPC)[(c % kWPC) * 32 + lane];
+            const float den = __fdividef(1.f, fmaf(-m.y, alb, 1.f));
+            if (c < Wg) {
+                const float F = m.z * den, G = fmaf(m.y, src, Dc) * den;
+                fb = fmaf(fa, G, fb);
+                fa *= F;
+            }
+            const float nalb = m.x + m.z * m.z * alb * den;
+            src = m.w + m.z * fmaf(alb, Dc, src) * den;
+            alb = nalb;
+        }
+        // direct flux per level (level i = top of layer i)
+        float vDir[CL];
+#pragma unroll
+        for (int i = 0; i < CL; ++i) vDir[i] = dtop * vP[i];
+
+        // ---- forward pass 2 (bottom up): albedo a_i and source s_i per level ----
+        float vA[CL], vS[CL];
+        {
+            float a = alb_in, s = src_in;
+#pragma unroll
+            for (int i = CL - 1; i >= 0; --i) {
+                const float su = vRd[i] * vDir[i], sd = vTd[i] * vDir[i];
+                const float den = __fdividef(1.f, fmaf(-vR[i], a, 1.f));
+                const float na = vR[i] + vT[i] * vT[i] * a * den;
+                const float ns = su + vT[i] * fmaf(a, sd, s) * den;
+                vA[i] = na;
+                vS[i] = ns;
+                a = na;
+                s = ns;
+            }
+        }
+        // ---- forward pass 3 (top down): diffuse downward flux fd per level ----
+        float vFd[CL];
+        float fd = fb;
+#pragma unroll
+        for (int i = 0; i < CL; ++i) {
+            vFd[i] = fd;
+            const float a_n = (i + 1 < CL) ? vA[i + 1] : alb_in;
+            const float s_n = (i + 1 < CL) ? vS[i + 1] : src_in;
+            const float den = __fdividef(1.f, fmaf(-vR[i], a_n, 1.f));
+            fd = (vT[i] * fd + vR[i] * s_n + vTd[i] * vDir[i]) * den;
+        }
+        const float fd_bot = fd;
+
+        // ---- R3 composite (Fraw bottom -> top of chunk) ----
+        {
+            float A3 = 1.f, B3 = 0.f;
+#pragma unroll
+            for (int i = CL - 1; i >= 0; --i) {
+                const int jl = w * CL + i;
+                const float a_n = (i + 1 < CL) ? vA[i + 1] : alb_in;
+                const float den = __fdividef(1.f, fmaf(-vR[i], a_n, 1.f));
+                const float c = vT[i] * den;
+                const float h = sm_hh[jl];
+                const float off = c * h * vAf[i] * a_n + sm_be[jl] + h * vAf[i] + sm_al[jl] * vA[i];
+                A3 *= c;
+                B3 = c * B3 + off;
+            }
+            sm_x3[w * 32 + lane] = make_float2(A3, B3);
+        }
+        cluster.sync();
+        float Fraw = (L_end == nlay) ? beN + alN * af : 0.f;
+        for (int c = NWt - 1; c > Wg; --c) {
+            const float2 m = remote(cluster, sm_x3, c / kWPC)[(c % kWPC) * 32 + lane];
+            Fraw = m.x * Fraw + m.y;
+        }
+        // R3 resweep: complete F at the bottom level of every layer
+        float vFc[CL];
+#pragma unroll
+        for (int i = CL - 1; i >= 0; --i) {
+            const int jl = w * CL + i;
+            const float a_n = (i + 1 < CL) ? vA[i + 1] : alb_in;
+            const float den = __fdividef(1.f, fmaf(-vR[i], a_n, 1.f));
+            const float h = sm_hh[jl];
+            const float Fc = Fraw + h * vAf[i] * a_n;
+            vFc[i] = Fc;
+            Fraw = vT[i] * den * Fc + sm_be[jl] + h * vAf[i] + sm_al[jl] * vA[i];
+        }
+
+        // ---- R2 composite (top -> bottom of chunk), (Abar, Sbar) ----
+        {
+            float cP = 1.f, cQ = 0.f, cR = 1.f, cUo = 0.f, cV = 0.f;
+#pragma unroll
+            for (int i = 0; i < CL; ++i) {
+                const int jl = w * CL + i;
+                const float a_n = (i + 1 < CL) ? vA[i + 1] : alb_in;
+                const float s_n = (i + 1 < CL) ? vS[i + 1] : src_in;
+                const float fd_n = (i + 1 < CL) ? vFd[i + 1] : fd_bot;
+                const float den = __fdividef(1.f, fmaf(-vR[i], a_n, 1.f));
+                const float td = vT[i] * den;
+                const float ub = sm_al[jl + 1] + sm_hh[jl] * vAf[i];
+                const float p = td * td, q = td * den * (vTd[i] * vDir[i] + vR[i] * s_n), r = td;
+                const float u = fd_n * (vR[i] * den * vFc[i] + ub), v = vFc[i] * vR[i] * den + ub;
+                const float nP = p * cP, nQ = p * cQ + q * cR, nU = p * cUo + q * cV + u;
+                const float nR = r * cR, nV = r * cV + v;
+                cP = nP; cQ = nQ; cUo = nU; cR = nR; cV = nV;
+            }
+            sm_x4a[w * 32 + lane] = make_float4(cP, cQ, cR, cUo);
+            sm_x4b[w * 32 + lane] = cV;
+        }
+        cluster.sync();
+        float Ab = 0.f, Sb = al0, Ab_in = 0.f, Sb_in = al0;
+        for (int c = 0; c < NWt; ++c) {
+            if (c == Wg) { Ab_in = Ab; Sb_in = Sb; }
+            const float4 m = remote(cluster, sm_x4a, c / kWPC)[(c % kWPC) * 32 + lane];
+            const float v = remote(cluster, sm_x4b, c / kWPC)[(c % kWPC) * 32 + lane];
+            const float nA = m.x * Ab + m.y * Sb + m.w;
+            Sb = m.z * Sb + v;
+            Ab = nA;
+        }
+        const float AbN = Ab, SbN = Sb;   // at level nlay (padding is the identity)
+        // R2 resweep: layer adjoints of R, T, sup, sdn
+        float vRb[CL], vTb[CL], vSub[CL], vSdb[CL], vAfb[CL];
+        {
+            float A_ = Ab_in, S_ = Sb_in;
+#pragma unroll
+            for (int i = 0; i < CL; ++i) {
+                const int jl = w * CL + i;
+                const float a_n = (i + 1 < CL) ? vA[i + 1] : alb_in;
+                const float s_n = (i + 1 < CL) ? vS[i + 1] : src_in;
+                const float fd_n = (i + 1 < CL) ? vFd[i + 1] : fd_bot;
+                const float den = __fdividef(1.f, fmaf(-vR[i], a_n, 1.f));
+                const float T = vT[i], R = vR[i], sdn = vTd[i] * vDir[i], Fc = vFc[i];
+                const float num_fd = T * vFd[i] + R * s_n + sdn;              // fd_(i+1) / den
+                const float denb = A_ * T * T * a_n + S_ * T * (s_n + a_n * sdn) + Fc * num_fd;
+                vRb[i] = A_ + denb * a_n * den * den + Fc * s_n * den;
+                vTb[i] = A_ * 2.f * T * a_n * den + S_ * den * (s_n + a_n * sdn) + Fc * vFd[i] * den;
+                vSub[i] = S_;
+                vSdb[i] = S_ * T * den * a_n + Fc * den;
+                const float fu_n = fd_n * a_n + s_n;
+                vAfb[i] = sm_hh[jl] * (vFd[i] + fu_n);
+                // advance to level i + 1
+                const float td = T * den;
+                const float ub = sm_al[jl + 1] + sm_hh[jl] * vAf[i];
+                const float nA = td * td * A_ + td * den * (sdn + R * s_n) * S_ + fd_n * (R * den * Fc + ub);
+                S_ = td * S_ + Fc * R * den + ub;
+                A_ = nA;
+            }
+        }
+        // surface albedo adjoints (same in every warp; one warp of one CTA accumulates them)
+        if (rank == 0 && w == 0) {
+            const float gad = SbN * dsfc, gaf = AbN;
+            for (int s = 0; s < 2; ++s) {
+                const float vd = warp_sum((gv && slot == s) ? gad : 0.f);
+                const float vf = warp_sum((gv && slot == s) ? gaf : 0.f);
+                const int b = b0 + s;
+                if (lane == 0 && s < mgb && b < nband && k.band_lims[2 * b] < 32 * gg + 32) {
+                    sm_alb[2 * b] += double(vd);
+                    sm_alb[2 * b + 1] += double(vf);
+                }
+            }
+        }
+
+        // ---- R1 composite (Dbar bottom -> top of chunk) ----
+        {
+            float A5 = 1.f, B5 = 0.f;
+#pragma unroll
+            for (int i = CL - 1; i >= 0; --i) {
+                const int jl = w * CL + i;
+                const float e = sm_be[jl] + sm_ga[jl] + sm_hh[jl] * vAr[i] + vSub[i] * vRd[i] + vSdb[i] * vTd[i];
+                A5 *= vTn[i];
+                B5 = vTn[i] * B5 + e;
+            }
+            sm_x5[w * 32 + lane] = make_float2(A5, B5);
+        }
+        cluster.sync();
+        float Db = SbN * ad + ((L_end == nlay) ? beN + gaN : 0.f);
+        for (int c = NWt - 1; c > Wg; --c) {
+            const float2 m = remote(cluster, sm_x5, c / kWPC)[(c % kWPC) * 32 + lane];
+            Db = m.x * Db + m.y;
+        }
+
+        // ---- R1 resweep + local adjoints per layer ----
+        float gT[CL], gH[CL], gO[CL], gC0[CL], gC1[CL], gC2[CL];
+#pragma unroll
+        for (int i = CL - 1; i >= 0; --i) {
+            const int jl = w * CL + i;
+            const int j = j0 + jl;
+            const float dir = vDir[i];
+            const float Tnb = Db * dir, Rdb = vSub[i] * dir, Tdb = vSdb[i] * dir, Arb = sm_hh[jl] * dir;
+            Db = sm_be[jl] + sm_ga[jl] + sm_hh[jl] * vAr[i] + vSub[i] * vRd[i] + vSdb[i] * vTd[i] + vTn[i] * Db;
+            gT[i] = 0.f; gH[i] = 0.f; gO[i] = 0.f; gC0[i] = 0.f; gC1[i] = 0.f; gC2[i] = 0.f;
+            if (j < nlay && gv) {
+                D3 o[7];
+                sw_layer_dual(vTau[i], vW0[i], vOmw[i], vG[i], mu0, mu0_inv, o);
+                const float bars[7] = {vRb[i], vTb[i], Rdb, Tdb, Tnb, vAfb[i], Arb};
+                float taub = 0.f, w0b = 0.f, gb = 0.f;
+#pragma unroll
+                for (int q = 0; q < 7; ++q) {
+                    taub += bars[q] * o[q].d[0];
+                    w0b += bars[q] * o[q].d[1];
+                    gb += bars[q] * o[q].d[2];
+                }
+                // combination: tau = ta + tr + tc, w0 = (tr + tsc) / tau, g = tsgc / (tr + tsc)
+                const Rec& Rc = recs[slot * CL + i];
+                const DRec& DR = drecs[slot * CL + i];
+                const float tau = vTau[i], w0 = vW0[i], omw = vOmw[i];
+                const bool okt = tau > 2.f * FLT_MIN;
+                const float ts = w0 * tau;
+                const bool oks = ts > 3.f * FLT_MIN;
+                const float itau = okt ? __fdividef(1.f, tau) : 0.f;
+                const float its = oks ? __fdividef(1.f, ts) : 0.f;
+                const float tab = taub - w0b * w0 * itau;                                // d/d ta
+                const float trb = taub + w0b * omw * itau - gb * vG[i] * its;            // d/d tr
+                const float tcb = taub - w0b * w0 * itau;                                // d/d tau_cloud
+                const float tscb = w0b * itau - gb * vG[i] * its;                        // d/d (tau ssa)_cloud
+                const float tsgb = gb * its;                                             // d/d (tau ssa g)_cloud
+                float gt = 0.f, gh = 0.f, go = 0.f;
+                tau_abs_adjoint(k, Rc, DR, g, Rc.a ? mg1 : mg0, Rc.a ? nm1 : nm0, tab, gt, gh, go);
+                // Rayleigh: tr = col_rayl * (fm . krayl corners)
+                const float2 r0 = __ldg(k.krayl2 + (Rc.kr[0] + g));
+                const float2 r1 = __ldg(k.krayl2 + (Rc.kr[1] + g));
+                const float4 kr = make_float4(r0.x, r0.y, r1.x, r1.y);
+                const float colr = Rc.aux.x;
+                gt += trb * colr * dot4(DR.fmT, kr);
+                gh += trb * (colr * dot4(DR.fmH, kr) + DR.dB.x * dot4(Rc.fm, kr));
+                go += trb * colr * dot4(DR.fmO, kr);
+                gT[i] = gt; gH[i] = gh; gO[i] = go;
+                gC0[i] = tcb; gC1[i] = tscb; gC2[i] = tsgb;
+            }
+        }
+
+        // ---- sums over the 32 g-points ----
+        {
+            float v[32];
+#pragma unroll
+            for (int i = 0; i < CL; ++i) { v[i] = gT[i]; v[8 + i] = gH[i]; v[16 + i] = gO[i]; v[24 + i] = 0.f; }
+            ReduceScatter<32, 16>::run(v, lane);
+            acc_q += double(v[0]);
+        }
+        {
+            // cloud: [tc s0 | tc s1 | tsc s0 | tsc s1] then [tsg s0 | tsg s1]
+            float v[32];
+#pragma unroll
+            for (int i = 0; i < CL; ++i) {
+                v[i] = slot == 0 ? gC0[i] : 0.f;
+                v[8 + i] = slot == 1 ? gC0[i] : 0.f;
+                v[16 + i] = slot == 0 ? gC1[i] : 0.f;
+                v[24 + i] = slot == 1 ? gC1[i] : 0.f;
+            }
+            ReduceScatter<32, 16>::run(v, lane);
+            {
+                const int q = lane >> 4, sl = (lane >> 3) & 1, jl = w * CL + (lane & 7), b = b0 + sl;
+                if (j0 + jl < nlay && b < nband && k.band_lims[2 * b] < 32 * gg + 32)
+                    sm_cl[(b * kLPC + jl) * 3 + q] += v[0];
+            }
+            float u[16];
+#pragma unroll
+            for (int i = 0; i < CL; ++i) { u[i] = slot == 0 ? gC2[i] : 0.f; u[8 + i] = slot == 1 ? gC2[i] : 0.f; }
+            ReduceScatter<16, 16>::run(u, lane);
+            {
+                const int vi = lane >> 1, sl = vi >> 3, jl = w * CL + (vi & 7), b = b0 + sl;
+                if ((lane & 1) == 0 && j0 + jl < nlay && b < nband && k.band_lims[2 * b] < 32 * gg + 32)
+                    sm_cl[(b * kLPC + jl) * 3 + 2] += u[0];
+            }
+        }
+        cluster.sync();   // maps and cloud sums are reused by the next group
+    }
+
+    // ---- outputs ----
+    {
+        const int q = lane >> 3, jl = w * kCL + (lane & 7), j = j0 + jl;
+        if (q < 3 && j < nlay) {
+            const size_t o = icol + size_t(top_at_1 ? j : nlay - 1 - j) * ncol;
+            float* dst = q == 0 ? out.tlay : (q == 1 ? out.h2o : out.o3);
+            if (dst) dst[o] = float(acc_q);
+        }
+    }
+    for (int jl = threadIdx.x; jl < kLPC; jl += blockDim.x) {
+        const int j = j0 + jl;
+        if (j >= nlay) continue;
+        const int l = top_at_1 ? j : nlay - 1 - j;
+        const size_t cl = icol + size_t(l) * ncol;
+        float gl = 0.f, gi = 0.f, grl = 0.f, gri = 0.f;
+        if (cld.present) {
+            const float lw = cld.lwp[cl], iw = cld.iwp[cl], rl = cld.rel[cl], ri = cld.rei[cl];
+            for (int b = 0; b < nband; ++b) {
+                const float* sb = sm_cl + (b * kLPC + jl) * 3;
+                if (sb[0] == 0.f && sb[1] == 0.f && sb[2] == 0.f) continue;
+                D4 tc, tsc, tsg;
+                cloud_sw_dual(cld.L, cld.delta, lw, iw, rl, ri, b, tc, tsc, tsg);
+                gl += sb[0] * tc.d[0] + sb[1] * tsc.d[0] + sb[2] * tsg.d[0];
+                gi += sb[0] * tc.d[1] + sb[1] * tsc.d[1] + sb[2] * tsg.d[1];
+                grl += sb[0] * tc.d[2] + sb[1] * tsc.d[2] + sb[2] * tsg.d[2];
+                gri += sb[0] * tc.d[3] + sb[1] * tsc.d[3] + sb[2] * tsg.d[3];
+            }
+        }
+        if (out.lwp) out.lwp[cl] = gl;
+        if (out.iwp) out.iwp[cl] = gi;
+        if (out.rel) out.rel[cl] = grl;
+        if (out.rei) out.rei[cl] = gri;
+    }
+    if (rank == 0) {
+        for (int b = threadIdx.x; b < nband; b += blockDim.x) {
+            if (out.alb_dir) out.alb_dir[b + size_t(icol) * nband] = float(sm_alb[2 * b]);
+            if (out.alb_dif) out.alb_dif[b + size_t(icol) * nband] = float(sm_alb[2 * b + 1]);
+        }
+    }
+    cluster.sync();   // no CTA leaves while its shared memory may still be read remotely
+}
+
+}  // namespace
+
+int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay, const float* play, const float* plev,
+                   const float* tlay, const float* col_dry, const rrtmgp_b200_gas_conc* gases, int ngases,
+                   const float* lwp, const float* iwp, const float* rel, const float* rei, int delta_cloud,
+                   const float* mu0, const float* tsi_scaling, const float* sfc_alb_dir, const float* sfc_alb_dif,
+                   const float* seed_up, const float* seed_dn, const float* seed_dir, const float* seed_hr,
+                   float* g_tlay, float* g_h2o, float* g_o3, float* g_lwp, float* g_iwp, float* g_rel, float* g_rei,
+                   float* g_alb_dir, float* g_alb_dif, void* stream)
+{
+    RB_CHECK_ARG(k && !k->info.is_longwave, "adjoint_sw: need a shortwave k-distribution");
+    RB_CHECK_ARG(ncol > 0 && nlay > 1, "adjoint_sw: ncol > 0 and nlay > 1 required");
+    RB_CHECK_ARG(play && plev && tlay && mu0 && sfc_alb_dir && sfc_alb_dif, "adjoint_sw: null input array");
+    RB_CHECK_ARG(!c || (lwp && iwp && rel && rei), "adjoint_sw: cloud arrays required with a cloud handle");
+    RB_CHECK_ARG(!c || c->nband == k->info.nband, "adjoint_sw: cloud and gas band counts differ");
+    const KdistView<float>& v = k->v32;
+    if (!v.minor_in_band || v.max_band_minor > kMaxMinor || v.max_minor_per_g > 3 || v.max_group_bands > 2 ||
+        !v.krayl2)
+        return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_sw: k-distribution layout not supported by the adjoint kernel");
+    const int CS = (nlay + kLPC - 1) / kLPC;
+    RB_CHECK_ARG(CS <= 8, "adjoint_sw: nlay too large (at most 512 layers)");
+    GasSet<float> gs;
+    int st = make_gas_set<float>(k, ncol, nlay, gases, ngases, gs);
+    if (st) return st;
+    int idx_o3 = 0;
+    for (size_t i = 0; i < k->gas_names.size(); ++i)
+        if (k->gas_names[i] == "o3") idx_o3 = int(i) + 1;
+    const size_t smem = sw_adj_layout(v.ngas, v.nband, v.max_group_bands).total;
+    if (smem > 227 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_sw: shared memory need exceeds 227 KB");
+    static bool attr = false;
+    if (!attr) {
+        RB_CUDA(cudaFuncSetAttribute(sw_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
+                "adjoint_sw attribute");
+        attr = true;
+    }
+    SwCloudArgs ca{};
+    if (c) {
+        ca.L = CloudLut<float>{c->nband, c->nsize_liq, c->nsize_ice, float(c->radliq_lwr), float(c->liq_step),
+                               float(c->radice_lwr), float(c->ice_step), c->lut32};
+        ca.lwp = lwp; ca.iwp = iwp; ca.rel = rel; ca.rei = rei;
+        ca.present = 1;
+        ca.delta = delta_cloud;
+    }
+    const SwAdjOut out{g_tlay, g_h2o, g_o3, g_lwp, g_iwp, g_rel, g_rei, g_alb_dir, g_alb_dif};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(ncol) * CS);
+    cfg.blockDim = dim3(kWPC * 32);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = as_stream(stream);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = unsigned(CS);
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    RB_CUDA(cudaLaunchKernelEx(&cfg, sw_adjoint_kernel, v, gs, ca, ncol, nlay, CS, idx_o3, col_dry ? 0 : 1, play, plev,
+                               tlay, col_dry, mu0, tsi_scaling, sfc_alb_dir, sfc_alb_dif, seed_up, seed_dn, seed_dir,
+                               seed_hr, out),
+            "sw_adjoint_kernel launch");
+    return RRTMGP_B200_OK;
+}
+
+}  // namespace rrtmgp_b200
+
+extern "C" int rrtmgp_b200_adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
+        const float* play, const float* plev, const float* tlay, const float* col_dry,
+        const rrtmgp_b200_gas_conc* gases, int ngases, const float* lwp, const float* iwp, const float* rel,
+        const float* rei, int delta_cloud, const float* mu0, const float* tsi_scaling, const float* sfc_alb_dir,
+        const float* sfc_alb_dif, const float* seed_flux_up, const float* seed_flux_dn, const float* seed_flux_dn_dir,
+        const float* seed_heating_rate, float* grad_tlay, float* grad_h2o, float* grad_o3, float* grad_lwp,
+        float* grad_iwp, float* grad_rel, float* grad_rei, float* grad_sfc_alb_dir, float* grad_sfc_alb_dif,
+        void* stream)
+{
+    return rrtmgp_b200::adjoint_sw_f32(k, c, ncol, nlay, play, plev, tlay, col_dry, gases, ngases, lwp, iwp, rel, rei,
+                                       delta_cloud, mu0, tsi_scaling, sfc_alb_dir, sfc_alb_dif, seed_flux_up,
+                                       seed_flux_dn, seed_flux_dn_dir, seed_heating_rate, grad_tlay, grad_h2o, grad_o3,
+                                       grad_lwp, grad_iwp, grad_rel, grad_rei, grad_sfc_alb_dir, grad_sfc_alb_dif,
+                                       stream);
+}

@@ -24,115 +24,12 @@
 // Heating rates use the per-layer absorbed flux (direct: F_dir (1 - Tn - Rdir - Tdir);
 // diffuse: (F_dn(top) + F_up(bottom)) (1 - R - T)), which equals the net-flux divergence of
 // the adding solution but keeps its relative accuracy in the ~0.1 Pa top layers.
-#include "fused_common.cuh"
-#include "optics_device.cuh"
+#include "sw_common.cuh"
 
 namespace rrtmgp_b200 {
 namespace {
 
 using namespace fused;
-
-struct SwCloudArgs {
-    CloudLut<float> L;
-    const float* lwp;
-    const float* iwp;
-    const float* rel;
-    const float* rei;
-    int present;
-    int delta;
-};
-
-// 1 - exp(-x) and exp(-x) for x >= 0, each with a small relative error: Taylor series of
-// 1 - exp(-x) through x^8 below 0.5 (truncation < 1.4e-8 relative), the exp intrinsic above.
-// Both are evaluated and selected (no divergence between the lanes of a warp).
-__device__ __forceinline__ void one_minus_exp(float x, float& E, float& e)
-{
-    const float Es = x * (1.f - x * (1.f / 2.f - x * (1.f / 6.f - x * (1.f / 24.f - x * (1.f / 120.f - x * (1.f / 720.f -
-                     x * (1.f / 5040.f - x * (1.f / 40320.f))))))));
-    const float ex = __expf(-x);
-    const bool small = x < 0.5f;
-    E = small ? Es : 1.f - ex;
-    e = small ? 1.f - Es : ex;
-}
-
-// Layer coefficients of the PIFM two-stream (sw_2stream_function, rte_solver_kernels.cu:
-// 535-584) in FP32.  The reference expressions lose all relative accuracy in FP32 for thin and
-// for conservatively scattering layers (O(1) terms cancelling to O(tau)); here they are
-// rearranged with E1 = 1 - exp(-k tau), E2 = 1 - exp(-2 k tau), En = 1 - exp(-tau/mu0) so
-// that the constant parts cancel analytically (same values in exact arithmetic):
-//   gamma1 - gamma2 = 2 (1 - w0),  1 - Rdif - Tdif = rt (k E1^2 + 2 (1 - w0) E2),
-//   Rdir bracket = E2 (alpha2 - k^2 mu0 gamma3) + k (gamma3 - mu0 alpha2) (E1^2 + 2 e1 En),
-//   Tdir bracket = Tn E2 (alpha1 + k^2 mu0 gamma4) + k (gamma4 + mu0 alpha1) (E1^2 - (1 + e2) En),
-// the Tdir bracket taking the reference form when both exponentials are small (thick layers).
-// Near the removable singularity k mu0 = 1 (|1 - (k mu0)^2| < 0.02) Rdir and Tdir come from
-// the reference expressions in FP64 (FP64 island).  omw = 1 - w0 is passed separately, formed
-// from absorption optical depths, so it keeps its accuracy for w0 -> 1.  Clamps and k_min are
-// those of the FP64 reference (DBL_EPSILON, 1e-12).  Divisions and the square root use the
-// approximate intrinsics (a few ulp; the operands are normal numbers).
-__device__ __forceinline__ void sw_layer_fast(float tau, float w0, float omw, float g, float mu0, float mu0_inv,
-                                              float& R, float& T, float& Rdir, float& Tdir, float& Tn,
-                                              float& adif, float& adir)
-{
-    const float g1 = (8.f - w0 * (5.f + 3.f * g)) * .25f;
-    const float g2 = 3.f * (w0 * (1.f - g)) * .25f;
-    const float g3 = (2.f - 3.f * mu0 * g) * .25f;
-    const float g4 = 1.f - g3;
-    const float a1 = g1 * g4 + g2 * g3;
-    const float a2 = g1 * g3 + g2 * g4;
-    const float kk = 2.f * omw * (2.f - .5f * w0 * (1.f + 3.f * g));
-    const float kkc = fmaxf(kk, 1.e-12f);
-    const float k = kkc * rsqrtf(kkc);
-    float E1, e1, En;
-    one_minus_exp(k * tau, E1, e1);
-    one_minus_exp(tau * mu0_inv, En, Tn);
-    const float E2 = E1 * (2.f - E1);
-    const float e2 = e1 * e1;
-    const float rt = __fdividef(1.f, k * (1.f + e2) + g1 * E2);
-    R = rt * g2 * E2;
-    T = rt * 2.f * k * e1;
-    adif = rt * (k * E1 * E1 + 2.f * omw * E2);
-    const float km = k * mu0;
-    const float fact = (1.f - km) * (1.f + km);
-    if (fabsf(fact) < 0.02f) {
-        double Rd, Td, Rr, Tr, Tn64;
-        sw_two_stream<double>(double(tau), double(w0), double(g), double(mu0), Rd, Td, Rr, Tr, Tn64);
-        Rdir = float(Rr);
-        Tdir = float(Tr);
-    } else {
-        const float rt2 = __fdividef(w0 * rt, fact);
-        const float br = E2 * (a2 - k * km * g3) + k * (g3 - mu0 * a2) * (E1 * E1 + 2.f * e1 * En);
-        const float bt_thick =
-            (1.f + km) * (a1 + k * g4) * Tn - (1.f - km) * (a1 - k * g4) * e2 * Tn - 2.f * (k * g4 + a1 * km) * e1;
-        const float bt_thin = Tn * E2 * (a1 + k * km * g4) + k * (g4 + mu0 * a1) * (E1 * E1 - (1.f + e2) * En);
-        const float bt = (e1 < .5f && Tn < .5f) ? bt_thick : bt_thin;
-        Rdir = rt2 * br;
-        Tdir = -rt2 * bt;
-    }
-    const float tmin = 2.220446049250313e-16f;
-    Rdir = fmaxf(tmin, fminf(Rdir, En));
-    const float rest = En - Rdir;
-    Tdir = fmaxf(tmin, fminf(Tdir, rest));
-    adir = fmaxf(0.f, rest - Tdir);
-}
-
-__device__ __forceinline__ void build_sw_record(const KdistView<float>& k, Rec& R, const LayerState& s,
-                                                const float* cg, int nlay, int b, const SwCloudArgs& cld,
-                                                size_t cl)
-{
-    record_weights(k, R, s, cg, nlay, b);
-    float tau = 0.f, ssa = 0.f, g = 0.f;
-    if (cld.present) {
-        const CloudPoint<float> cp = cloud_point(cld.L, cld.lwp[cl], cld.iwp[cl], cld.rel[cl], cld.rei[cl]);
-        cloud_band<float, true>(cld.L, cp, b, tau, ssa, g);
-        const float ta = tau * (1.f - ssa);   // invariant under delta scaling
-        if (cld.delta) delta_scale_point(tau, ssa, g);
-        R.aux2 = ta;
-    } else {
-        R.aux2 = 0.f;
-    }
-    const float ts = tau * ssa;
-    R.aux = make_float4(cg[0] + cg[k.idx_h2o * nlay], tau, ts, ts * g);
-}
 
 template <int CL>
 __global__ void __launch_bounds__(512)

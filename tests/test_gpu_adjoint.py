@@ -174,3 +174,106 @@ def test_lw_autograd_directional(oracle_mod, tables, gpu):
     eps = 1e-3
     fd = (shifted(eps) - shifted(-eps)) / (2 * eps)
     assert abs(ad - fd) <= 2e-3 * abs(fd), f"directional derivative: autograd {ad:.6e} vs FD {fd:.6e}"
+
+
+# ---------------------------------------------------------------------------------------------
+# Shortwave
+# ---------------------------------------------------------------------------------------------
+def _sw_setup(tables, oracle_mod, ncol, nlay, seed, clouds, top_at_1=True):
+    rng = np.random.default_rng(seed)
+    atm = S.make_atmosphere(ncol, nlay, seed=seed, clouds=clouds, top_at_1=top_at_1)
+    nb = atm["sfc_alb_dir"].shape[1]
+    atm["sfc_alb_dir"] = rng.uniform(0.05, 0.6, (ncol, nb))
+    atm["sfc_alb_dif"] = rng.uniform(0.05, 0.6, (ncol, nb))
+    atm["mu0"] = np.linspace(0.15, 0.95, ncol)
+    kd = oracle_mod.GasOptics(tables["sw"], S.ATM_GASES)
+    cl = oracle_mod.CloudOptics(tables["cloud_sw"]) if clouds else None
+    return atm, (lambda a: oracle_mod.forward_sw(kd, cl, a))
+
+
+def _sw_seeds(nlay, ncol, rng):
+    s = _seeds(nlay, ncol, rng)
+    s["flux_dn_dir"] = rng.normal(size=(nlay + 1, ncol))
+    return s
+
+
+def _fd_bands(fwd, atm, seeds, key):
+    """Per-column FD w.r.t. each band of a (ncol, nband) surface field."""
+    base = atm[key]
+    grad = np.zeros_like(base)
+    for b in range(base.shape[1]):
+        h = REL_STEP * np.abs(base[:, b])
+        ls = []
+        for sgn in (1.0, -1.0):
+            a = copy.deepcopy(atm)
+            a[key][:, b] += sgn * h
+            ls.append(_loss_cols(fwd(a), seeds))
+        grad[:, b] = (ls[0] - ls[1]) / (2 * h)
+    return grad
+
+
+def _gpu_grads_sw(tables, atm, seeds, clouds):
+    import torch
+    from rrtmgp_b200.autodiff import adjoint_sw
+    from rrtmgp_b200.solver import Fused_solver, Radiation_solver, atm_to_device
+    base = Radiation_solver(tables["lw"], tables["sw"], tables["cloud_lw"], tables["cloud_sw"], S.ATM_GASES)
+    d = atm_to_device(atm, torch.float32, "cuda")
+    t = {k: torch.as_tensor(v, dtype=torch.float32, device="cuda").contiguous() for k, v in seeds.items()}
+    g = adjoint_sw(Fused_solver(base), d, t.get("flux_up"), t.get("flux_dn"), t.get("flux_dn_dir"),
+                   t.get("heating_rate"), with_clouds=clouds)
+    torch.cuda.synchronize()
+    return {k: v.double().cpu().numpy() for k, v in g.items()}
+
+
+@pytest.mark.parametrize("nlay", [24, 80])   # 80 layers: a cluster of two CTAs per column
+@pytest.mark.parametrize("top_at_1", [True, False])
+def test_sw_adjoint_matches_fd(oracle_mod, tables, gpu, nlay, top_at_1):
+    rng = np.random.default_rng(6)
+    ncol = 3
+    atm, fwd = _sw_setup(tables, oracle_mod, ncol, nlay, seed=31 + nlay, clouds=True, top_at_1=top_at_1)
+    seeds = _sw_seeds(nlay, ncol, rng)
+    got = _gpu_grads_sw(tables, atm, seeds, True)
+    for key in ("tlay", "h2o", "o3"):
+        _check(f"sw d/d{key}", got[key], _fd(fwd, atm, seeds, key), _informative(_get(atm, key)))
+    for key in ("sfc_alb_dir", "sfc_alb_dif"):
+        _check(f"sw d/d{key}", got[key], _fd_bands(fwd, atm, seeds, key))
+    cloudy_l, cloudy_i = atm["lwp"] > 0, atm["iwp"] > 0
+    if cloudy_l.any():
+        _check("sw d/dlwp", got["lwp"], _fd(fwd, atm, seeds, "lwp"), cloudy_l)
+        _check("sw d/drel", got["rel"], _fd(fwd, atm, seeds, "rel"), cloudy_l)
+    if cloudy_i.any():
+        _check("sw d/diwp", got["iwp"], _fd(fwd, atm, seeds, "iwp"), cloudy_i)
+        _check("sw d/drei", got["rei"], _fd(fwd, atm, seeds, "rei"), cloudy_i)
+
+
+def test_sw_autograd_directional(oracle_mod, tables, gpu):
+    import torch
+    from rrtmgp_b200.autodiff import shortwave
+    from rrtmgp_b200.solver import Fused_solver, Radiation_solver, atm_to_device
+    rng = np.random.default_rng(7)
+    ncol, nlay = 16, 40
+    atm, fwd = _sw_setup(tables, oracle_mod, ncol, nlay, seed=41, clouds=True)
+    seeds = _sw_seeds(nlay, ncol, rng)
+    base = Radiation_solver(tables["lw"], tables["sw"], tables["cloud_lw"], tables["cloud_sw"], S.ATM_GASES)
+    d = atm_to_device(atm, torch.float32, "cuda")
+    leaves = [d["tlay"], d["gases"]["h2o"], d["gases"]["o3"]]
+    for t in leaves:
+        t.requires_grad_(True)
+    out = shortwave(Fused_solver(base), d)
+    loss = sum((torch.as_tensor(seeds[k], dtype=torch.float32, device="cuda") * out[k]).sum() for k in seeds)
+    loss.backward()
+    dirs = {k: rng.normal(size=_get(atm, k).shape) for k in ("tlay", "h2o", "o3")}
+    scale = {"tlay": 1e-2, "h2o": 1e-3, "o3": 1e-3}
+    ad = sum(float((t.grad.double().cpu().numpy() * dirs[k] * scale[k] * np.abs(_get(atm, k))).sum())
+             for k, t in zip(("tlay", "h2o", "o3"), leaves))
+
+    def shifted(eps):
+        a = copy.deepcopy(atm)
+        for k in dirs:
+            arr = _get(a, k)
+            arr += eps * dirs[k] * scale[k] * np.abs(arr)
+        return _loss_cols(fwd(a), seeds).sum()
+
+    eps = 1e-3
+    fd = (shifted(eps) - shifted(-eps)) / (2 * eps)
+    assert abs(ad - fd) <= 2e-3 * abs(fd), f"directional derivative: autograd {ad:.6e} vs FD {fd:.6e}"

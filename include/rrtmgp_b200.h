@@ -367,7 +367,7 @@ int rrtmgp_b200_forward_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int
  * Fluxes_broadband::reduce -- plus heating rates, in one kernel.  mu0 (ncol) > 0; surface
  * albedos (nband, ncol) in the reference's column-fastest order.  Outputs flux_up, flux_dn
  * (direct included), flux_dn_dir, flux_net (ncol, nlay+1) and heating_rate (ncol, nlay).
- * chunk: layers per warp (8 or 16; 0 picks the tuned default).  nlay <= 16 * chunk. */
+ * chunk: layers per warp (8 or 16; 0: 8 up to 128 layers, else 16).  nlay <= 16 * chunk. */
 int rrtmgp_b200_forward_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int ncol, int nlay,
         const float* play, const float* plev, const float* tlay, const float* col_dry,
         const rrtmgp_b200_gas_conc* gases, int ngases, const float* lwp, const float* iwp,

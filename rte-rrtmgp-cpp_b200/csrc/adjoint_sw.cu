@@ -70,6 +70,26 @@ __device__ __forceinline__ void one_minus_exp_d(const D3& x, D3& E, D3& e)
     }
 }
 
+// FP64 island of the two-stream (|1 - (k mu0)^2| < 0.02, as the forward): Rdir and Tdir from
+// the reference expressions in double and their central differences in (tau, w0, g).  Rare
+// (strongly absorbing g-points at mu0 near 1/k), so kept out of line: one copy of the code.
+__device__ __noinline__ void island_fp64(float tau, float w0, float g, float mu0, float* rd, float* td)
+{
+    double Rd, Td, Rr, Tr, Tn64;
+    sw_two_stream<double>(double(tau), double(w0), double(g), double(mu0), Rd, Td, Rr, Tr, Tn64);
+    rd[0] = float(Rr);
+    td[0] = float(Tr);
+    const double steps[3] = {1e-6 * fmax(double(tau), 1e-12), 1e-6, 1e-6};
+    for (int i = 0; i < 3; ++i) {
+        double Rp, Tp, Rm, Tm, x0, x1, x2;
+        const double dt = i == 0 ? steps[0] : 0.0, dw = i == 1 ? steps[1] : 0.0, dg = i == 2 ? steps[2] : 0.0;
+        sw_two_stream<double>(double(tau) + dt, double(w0) + dw, double(g) + dg, double(mu0), x0, x1, Rp, Tp, x2);
+        sw_two_stream<double>(double(tau) - dt, double(w0) - dw, double(g) - dg, double(mu0), x0, x1, Rm, Tm, x2);
+        rd[1 + i] = float((Rp - Rm) / (2.0 * steps[i]));
+        td[1 + i] = float((Tp - Tm) / (2.0 * steps[i]));
+    }
+}
+
 // sw_layer_fast (sw_common.cuh) with derivatives w.r.t. (tau, w0, g); omw = 1 - w0 moves with
 // w0.  out: R, T, Rdir, Tdir, Tn, adif, adir.
 __device__ __forceinline__ void sw_layer_dual(float tau, float w0, float omw, float g, float mu0, float mu0_inv,
@@ -103,22 +123,14 @@ __device__ __forceinline__ void sw_layer_dual(float tau, float w0, float omw, fl
     const D3 fact = (1.f - km) * (1.f + km);
     D3 Rdir, Tdir;
     if (fabsf(fact.v) < 0.02f) {
-        // FP64 island (as the forward): reference expressions in double, central differences
-        double Rd, Td, Rr, Tr, Tn64;
-        sw_two_stream<double>(double(tau), double(w0), double(g), double(mu0), Rd, Td, Rr, Tr, Tn64);
-        Rdir = dconst<3>(float(Rr));
-        Tdir = dconst<3>(float(Tr));
-        const double ht = 1e-6 * fmax(double(tau), 1e-12), hw = 1e-6, hg = 1e-6;
-        const double steps[3] = {ht, hw, hg};
+        float rd[4], td[4];
+        island_fp64(tau, w0, g, mu0, rd, td);
+        Rdir.v = rd[0];
+        Tdir.v = td[0];
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-            double Rp, Tp, Rm, Tm, x0, x1, x2;
-            sw_two_stream<double>(double(tau) + (i == 0 ? steps[i] : 0.0), double(w0) + (i == 1 ? steps[i] : 0.0),
-                                  double(g) + (i == 2 ? steps[i] : 0.0), double(mu0), x0, x1, Rp, Tp, x2);
-            sw_two_stream<double>(double(tau) - (i == 0 ? steps[i] : 0.0), double(w0) - (i == 1 ? steps[i] : 0.0),
-                                  double(g) - (i == 2 ? steps[i] : 0.0), double(mu0), x0, x1, Rm, Tm, x2);
-            Rdir.d[i] = float((Rp - Rm) / (2.0 * steps[i]));
-            Tdir.d[i] = float((Tp - Tm) / (2.0 * steps[i]));
+            Rdir.d[i] = rd[1 + i];
+            Tdir.d[i] = td[1 + i];
         }
     } else {
         const D3 rt2 = ddiv(W * rt, fact, true);
@@ -142,6 +154,43 @@ __device__ __forceinline__ void sw_layer_dual(float tau, float w0, float omw, fl
     out[4] = Tn;
     out[5] = adif;
     out[6] = adir;
+}
+
+// Adjoint of one (layer, g-point) from the adjoints of its two-stream outputs (R, T, Rdir,
+// Tdir, Tn, adif, adir) to the optical inputs of the layer: gas absorption tau (x), Rayleigh
+// tau (y), cloud tau (z), cloud tau*ssa (w) and cloud tau*ssa*g (v).  The combination is
+// tau = ta + tr + tc, w0 = (tr + tsc) / tau, g = tsgc / (tr + tsc).  Out of line: the
+// caller's per-layer loop is unrolled, this body is emitted once.
+struct LocalAdj {
+    float ta, tr, tc, tsc, tsg;
+};
+
+__device__ __noinline__ LocalAdj sw_local_adjoint(float tau, float w0, float omw, float gasy, float mu0, float mu0_inv,
+                                                  float Rb, float Tb, float Rdb, float Tdb, float Tnb, float Afb,
+                                                  float Arb)
+{
+    D3 o[7];
+    sw_layer_dual(tau, w0, omw, gasy, mu0, mu0_inv, o);
+    const float bars[7] = {Rb, Tb, Rdb, Tdb, Tnb, Afb, Arb};
+    float taub = 0.f, w0b = 0.f, gb = 0.f;
+#pragma unroll
+    for (int q = 0; q < 7; ++q) {
+        taub += bars[q] * o[q].d[0];
+        w0b += bars[q] * o[q].d[1];
+        gb += bars[q] * o[q].d[2];
+    }
+    const bool okt = tau > 2.f * FLT_MIN;
+    const float ts = w0 * tau;
+    const bool oks = ts > 3.f * FLT_MIN;
+    const float itau = okt ? __fdividef(1.f, tau) : 0.f;
+    const float its = oks ? __fdividef(1.f, ts) : 0.f;
+    LocalAdj r;
+    r.ta = taub - w0b * w0 * itau;
+    r.tr = taub + w0b * omw * itau - gb * gasy * its;
+    r.tc = taub - w0b * w0 * itau;
+    r.tsc = w0b * itau - gb * gasy * its;
+    r.tsg = gb * its;
+    return r;
 }
 
 // Cloud optics of band b (2str, optionally delta-scaled) as duals over (lwp, iwp, rel, rei):
@@ -200,7 +249,7 @@ struct SwAdjLayout {
     size_t state, cg, seeds, clsum, albacc, x1, x2, x3, x4, x5, recs, drecs, total;
 };
 
-__host__ __device__ __forceinline__ SwAdjLayout sw_adj_layout(int ngas, int nband, int mgb)
+__host__ __device__ __forceinline__ SwAdjLayout sw_adj_layout(int ngas, int nband, int mgb, int CS)
 {
     SwAdjLayout L;
     L.state = 0;
@@ -209,11 +258,13 @@ __host__ __device__ __forceinline__ SwAdjLayout sw_adj_layout(int ngas, int nban
     L.clsum = align16(L.seeds + sizeof(float) * (4 * (kLPC + 1)));
     L.albacc = align16(L.clsum + sizeof(float) * size_t(nband) * kLPC * 3);
     L.x1 = align16(L.albacc + sizeof(double) * size_t(nband) * 2);
-    L.x2 = align16(L.x1 + sizeof(float) * kWPC * 32);
-    L.x3 = align16(L.x2 + sizeof(float4) * kWPC * 32 * 2);
-    L.x4 = align16(L.x3 + sizeof(float2) * kWPC * 32);
-    L.x5 = align16(L.x4 + sizeof(float4) * kWPC * 32 * 2);
-    L.recs = align16(L.x5 + sizeof(float2) * kWPC * 32);
+    // chunk maps of every chunk of the cluster (each warp pushes its map to all CTAs)
+    const size_t nw = size_t(kWPC) * CS * 32;
+    L.x2 = align16(L.x1 + sizeof(float) * nw);
+    L.x3 = align16(L.x2 + (sizeof(float4) + sizeof(float)) * nw);
+    L.x4 = align16(L.x3 + sizeof(float2) * nw);
+    L.x5 = align16(L.x4 + (sizeof(float4) + sizeof(float)) * nw);
+    L.recs = align16(L.x5 + sizeof(float2) * nw);
     L.drecs = align16(L.recs + sizeof(Rec) * size_t(kWPC) * kCL * mgb);
     L.total = align16(L.drecs + sizeof(DRec) * size_t(kWPC) * kCL * mgb);
     return L;
@@ -245,7 +296,7 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
     const int L_end = NWt * CL;
     const int j0 = rank * kLPC;          // first global layer of this CTA
     const int nband = k.nband, mgb = k.max_group_bands;
-    const SwAdjLayout SL = sw_adj_layout(k.ngas, nband, mgb);
+    const SwAdjLayout SL = sw_adj_layout(k.ngas, nband, mgb, CS);
     LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
     float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
     float* sm_al = reinterpret_cast<float*>(smem_raw + SL.seeds);   // seed F_up per local level (0..64)
@@ -256,10 +307,10 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
     double* sm_alb = reinterpret_cast<double*>(smem_raw + SL.albacc); // [band][2]
     float* sm_x1 = reinterpret_cast<float*>(smem_raw + SL.x1);
     float4* sm_x2a = reinterpret_cast<float4*>(smem_raw + SL.x2);
-    float* sm_x2b = reinterpret_cast<float*>(sm_x2a + kWPC * 32);
+    float* sm_x2b = reinterpret_cast<float*>(sm_x2a + NWt * 32);
     float2* sm_x3 = reinterpret_cast<float2*>(smem_raw + SL.x3);
     float4* sm_x4a = reinterpret_cast<float4*>(smem_raw + SL.x4);
-    float* sm_x4b = reinterpret_cast<float*>(sm_x4a + kWPC * 32);
+    float* sm_x4b = reinterpret_cast<float*>(sm_x4a + NWt * 32);
     float2* sm_x5 = reinterpret_cast<float2*>(smem_raw + SL.x5);
     Rec* recs = reinterpret_cast<Rec*>(smem_raw + SL.recs) + w * CL * mgb;
     DRec* drecs = reinterpret_cast<DRec*>(smem_raw + SL.drecs) + w * CL * mgb;
@@ -389,17 +440,19 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
             cRu = nRu; cRd = nRd; cU = nU; cD = nD;
             P *= Tn;
         }
-        sm_x1[w * 32 + lane] = P;
+        for (int rr = 0; rr < CS; ++rr) remote(cluster, sm_x1, rr)[Wg * 32 + lane] = P;
         cluster.sync();
 
         // ---- X1: direct flux at the chunk top and the surface ----
         const float toa = gv ? __ldg(k.solar_source + g) * tsi * mu0 : 0.f;
         float dtop = toa;
-        for (int c = 0; c < Wg; ++c) dtop *= remote(cluster, sm_x1, c / kWPC)[(c % kWPC) * 32 + lane];
+        for (int c = 0; c < Wg; ++c) dtop *= sm_x1[c * 32 + lane];
         float dsfc = dtop;
-        for (int c = Wg; c < NWt; ++c) dsfc *= remote(cluster, sm_x1, c / kWPC)[(c % kWPC) * 32 + lane];
-        sm_x2a[w * 32 + lane] = make_float4(cRu, cRd, cT, cU * dtop);
-        sm_x2b[w * 32 + lane] = cD * dtop;
+        for (int c = Wg; c < NWt; ++c) dsfc *= sm_x1[c * 32 + lane];
+        for (int rr = 0; rr < CS; ++rr) {
+            remote(cluster, sm_x2a, rr)[Wg * 32 + lane] = make_float4(cRu, cRd, cT, cU * dtop);
+            remote(cluster, sm_x2b, rr)[Wg * 32 + lane] = cD * dtop;
+        }
         cluster.sync();
 
         // ---- X2: albedo / source at the chunk bottom, incident diffuse flux at its top ----
@@ -412,8 +465,8 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
                 src_in = src;
                 if (Wg == 0) break;
             }
-            const float4 m = remote(cluster, sm_x2a, c / kWPC)[(c % kWPC) * 32 + lane];
-            const float Dc = remote(cluster, sm_x2b, c / kWPC)[(c % kWPC) * 32 + lane];
+            const float4 m = sm_x2a[c * 32 + lane];
+            const float Dc = sm_x2b[c * 32 + lane];
             const float den = __fdividef(1.f, fmaf(-m.y, alb, 1.f));
             if (c < Wg) {
                 const float F = m.z * den, G = fmaf(m.y, src, Dc) * den;
@@ -472,12 +525,12 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
                 A3 *= c;
                 B3 = c * B3 + off;
             }
-            sm_x3[w * 32 + lane] = make_float2(A3, B3);
+            for (int rr = 0; rr < CS; ++rr) remote(cluster, sm_x3, rr)[Wg * 32 + lane] = make_float2(A3, B3);
         }
         cluster.sync();
         float Fraw = (L_end == nlay) ? beN + alN * af : 0.f;
         for (int c = NWt - 1; c > Wg; --c) {
-            const float2 m = remote(cluster, sm_x3, c / kWPC)[(c % kWPC) * 32 + lane];
+            const float2 m = sm_x3[c * 32 + lane];
             Fraw = m.x * Fraw + m.y;
         }
         // R3 resweep: complete F at the bottom level of every layer
@@ -511,15 +564,17 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
                 const float nR = r * cR, nV = r * cV + v;
                 cP = nP; cQ = nQ; cUo = nU; cR = nR; cV = nV;
             }
-            sm_x4a[w * 32 + lane] = make_float4(cP, cQ, cR, cUo);
-            sm_x4b[w * 32 + lane] = cV;
+            for (int rr = 0; rr < CS; ++rr) {
+                remote(cluster, sm_x4a, rr)[Wg * 32 + lane] = make_float4(cP, cQ, cR, cUo);
+                remote(cluster, sm_x4b, rr)[Wg * 32 + lane] = cV;
+            }
         }
         cluster.sync();
         float Ab = 0.f, Sb = al0, Ab_in = 0.f, Sb_in = al0;
         for (int c = 0; c < NWt; ++c) {
             if (c == Wg) { Ab_in = Ab; Sb_in = Sb; }
-            const float4 m = remote(cluster, sm_x4a, c / kWPC)[(c % kWPC) * 32 + lane];
-            const float v = remote(cluster, sm_x4b, c / kWPC)[(c % kWPC) * 32 + lane];
+            const float4 m = sm_x4a[c * 32 + lane];
+            const float v = sm_x4b[c * 32 + lane];
             const float nA = m.x * Ab + m.y * Sb + m.w;
             Sb = m.z * Sb + v;
             Ab = nA;
@@ -577,12 +632,12 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
                 A5 *= vTn[i];
                 B5 = vTn[i] * B5 + e;
             }
-            sm_x5[w * 32 + lane] = make_float2(A5, B5);
+            for (int rr = 0; rr < CS; ++rr) remote(cluster, sm_x5, rr)[Wg * 32 + lane] = make_float2(A5, B5);
         }
         cluster.sync();
         float Db = SbN * ad + ((L_end == nlay) ? beN + gaN : 0.f);
         for (int c = NWt - 1; c > Wg; --c) {
-            const float2 m = remote(cluster, sm_x5, c / kWPC)[(c % kWPC) * 32 + lane];
+            const float2 m = sm_x5[c * 32 + lane];
             Db = m.x * Db + m.y;
         }
 
@@ -597,30 +652,11 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
             Db = sm_be[jl] + sm_ga[jl] + sm_hh[jl] * vAr[i] + vSub[i] * vRd[i] + vSdb[i] * vTd[i] + vTn[i] * Db;
             gT[i] = 0.f; gH[i] = 0.f; gO[i] = 0.f; gC0[i] = 0.f; gC1[i] = 0.f; gC2[i] = 0.f;
             if (j < nlay && gv) {
-                D3 o[7];
-                sw_layer_dual(vTau[i], vW0[i], vOmw[i], vG[i], mu0, mu0_inv, o);
-                const float bars[7] = {vRb[i], vTb[i], Rdb, Tdb, Tnb, vAfb[i], Arb};
-                float taub = 0.f, w0b = 0.f, gb = 0.f;
-#pragma unroll
-                for (int q = 0; q < 7; ++q) {
-                    taub += bars[q] * o[q].d[0];
-                    w0b += bars[q] * o[q].d[1];
-                    gb += bars[q] * o[q].d[2];
-                }
-                // combination: tau = ta + tr + tc, w0 = (tr + tsc) / tau, g = tsgc / (tr + tsc)
+                const LocalAdj la = sw_local_adjoint(vTau[i], vW0[i], vOmw[i], vG[i], mu0, mu0_inv, vRb[i], vTb[i],
+                                                     Rdb, Tdb, Tnb, vAfb[i], Arb);
                 const Rec& Rc = recs[slot * CL + i];
                 const DRec& DR = drecs[slot * CL + i];
-                const float tau = vTau[i], w0 = vW0[i], omw = vOmw[i];
-                const bool okt = tau > 2.f * FLT_MIN;
-                const float ts = w0 * tau;
-                const bool oks = ts > 3.f * FLT_MIN;
-                const float itau = okt ? __fdividef(1.f, tau) : 0.f;
-                const float its = oks ? __fdividef(1.f, ts) : 0.f;
-                const float tab = taub - w0b * w0 * itau;                                // d/d ta
-                const float trb = taub + w0b * omw * itau - gb * vG[i] * its;            // d/d tr
-                const float tcb = taub - w0b * w0 * itau;                                // d/d tau_cloud
-                const float tscb = w0b * itau - gb * vG[i] * its;                        // d/d (tau ssa)_cloud
-                const float tsgb = gb * its;                                             // d/d (tau ssa g)_cloud
+                const float tab = la.ta, trb = la.tr, tcb = la.tc, tscb = la.tsc, tsgb = la.tsg;
                 float gt = 0.f, gh = 0.f, go = 0.f;
                 tau_abs_adjoint(k, Rc, DR, g, Rc.a ? mg1 : mg0, Rc.a ? nm1 : nm0, tab, gt, gh, go);
                 // Rayleigh: tr = col_rayl * (fm . krayl corners)
@@ -742,7 +778,7 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     int idx_o3 = 0;
     for (size_t i = 0; i < k->gas_names.size(); ++i)
         if (k->gas_names[i] == "o3") idx_o3 = int(i) + 1;
-    const size_t smem = sw_adj_layout(v.ngas, v.nband, v.max_group_bands).total;
+    const size_t smem = sw_adj_layout(v.ngas, v.nband, v.max_group_bands, CS).total;
     if (smem > 227 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_sw: shared memory need exceeds 227 KB");
     static bool attr = false;
     if (!attr) {

@@ -316,7 +316,7 @@ int forward_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     int st = make_gas_set<float>(k, ncol, nlay, gases, ngases, gs);
     if (st) return st;
     cudaStream_t s = as_stream(stream);
-    const int cl = chunk ? chunk : 8;
+    const int cl = chunk ? chunk : (nlay > 128 ? 16 : 8);
     if (cl == 16)
         return launch_sw_forward<16>(k, c, ncol, nlay, play, plev, tlay, col_dry, gs, lwp, iwp, rel, rei, delta_cloud,
                                      mu0, tsi_scaling, sfc_alb_dir, sfc_alb_dif, flux_up, flux_dn, flux_dn_dir,

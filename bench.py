@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=42)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     return ap.parse_args()
 
@@ -280,12 +281,13 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
 
+    from rrtmgp_b200 import shard
     from rrtmgp_b200 import synthetic as S
     from rrtmgp_b200.solver import Fused_solver, Radiation_solver, atm_to_device
 
     tables = {"lw": S.make_kdist("lw"), "sw": S.make_kdist("sw"),
               "cloud_lw": S.make_cloud_luts("lw"), "cloud_sw": S.make_cloud_luts("sw")}
-    atm_np = S.make_atmosphere(args.ncol, args.nlay, seed=args.seed + rank, clouds=True)
+    atm_np = S.make_atmosphere(args.ncol, args.nlay, seed=shard.rank_seed(args.seed, rank), clouds=True)
     solver = Radiation_solver(tables["lw"], tables["sw"], tables["cloud_lw"], tables["cloud_sw"], S.ATM_GASES)
     fused = Fused_solver(solver)
     run_lw = fused.solve_lw if args.path == "fused" else solver.solve_lw
@@ -389,12 +391,9 @@ def main():
     lw_ms = float(np.mean([a.elapsed_time(m) for a, m, b in evs]))
     sw_ms = float(np.mean([m.elapsed_time(b) for a, m, b in evs]))
     total_ms = float(np.sum(step_ms))
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = shard.max_over_ranks(total_ms, dist if world > 1 else None, dev)
     ms_per_step = total_ms / args.steps
-    value = world * args.ncol * args.steps / (total_ms * 1e-3)
+    value = shard.weak_scaling_rate(args.ncol, world, args.steps, total_ms)
 
     # Per-kernel durations and roofline of the dominant kernel.
     traffic = ncu_traffic()
@@ -465,10 +464,53 @@ def main():
         ee[i][1].record(stream)
     torch.cuda.synchronize()
     e2e_ms = float(np.sum([a.elapsed_time(b) for a, b in ee]))
-    t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.ncol * args.steps / (float(t.item()) * 1e-3)
+    e2e_value = shard.weak_scaling_rate(args.ncol, world, args.steps,
+                                        shard.max_over_ranks(e2e_ms, dist if world > 1 else None, dev))
+
+    # FP32 forward + hand-written adjoint (LW and SW), seeded on every output: the path the
+    # FP32 target is stated on.  Same columns, L2 flushed between steps, events per kernel.
+    fwd_adj = None
+    if args.path == "fused" and not args.no_adjoint:
+        from rrtmgp_b200.autodiff import adjoint_lw, adjoint_sw
+        nlev = args.nlay + 1
+        gen = torch.Generator(device=dev).manual_seed(args.seed)
+        sd = {k: torch.randn(shape, generator=gen, device=dev) for k, shape in
+              (("up", (nlev, args.ncol)), ("dn", (nlev, args.ncol)), ("dir", (nlev, args.ncol)),
+               ("hr", (args.nlay, args.ncol)))}
+
+        def fa_step():
+            run_lw(atm)
+            adjoint_lw(fused, atm, sd["up"], sd["dn"], sd["hr"])
+            run_sw(atm)
+            adjoint_sw(fused, atm, sd["up"], sd["dn"], sd["dir"], sd["hr"])
+
+        for _ in range(2):
+            fa_step()
+        torch.cuda.synchronize()
+        nrep = max(2, args.steps // 5)
+        ev = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(5)) for _ in range(nrep)]
+        for i in range(nrep):
+            flush.zero_()
+            e = ev[i]
+            e[0].record(stream)
+            run_lw(atm)
+            e[1].record(stream)
+            adjoint_lw(fused, atm, sd["up"], sd["dn"], sd["hr"])
+            e[2].record(stream)
+            run_sw(atm)
+            e[3].record(stream)
+            adjoint_sw(fused, atm, sd["up"], sd["dn"], sd["dir"], sd["hr"])
+            e[4].record(stream)
+        torch.cuda.synchronize()
+        parts = [float(np.mean([e[q].elapsed_time(e[q + 1]) for e in ev])) for q in range(4)]
+        tot = float(np.sum(parts))
+        tot = shard.max_over_ranks(tot, dist if world > 1 else None, dev)
+        fwd_adj = {"value": shard.weak_scaling_rate(args.ncol, world, 1, tot), "unit": "columns/s",
+                   "ms_per_step": tot, "steps": nrep, "gpu_launches_per_step": 4,
+                   "kernel_ms": {"lw_forward_kernel": round(parts[0], 4), "lw_adjoint_kernel": round(parts[1], 4),
+                                 "sw_forward_kernel": round(parts[2], 4), "sw_adjoint_kernel": round(parts[3], 4)},
+                   "gradients": "flux/heating-rate seeds -> tlay, tlev, tsfc, h2o, o3, lwp, iwp, rel, rei (LW); "
+                                "tlay, h2o, o3, lwp, iwp, rel, rei, surface albedos (SW)"}
 
     # Plain FP64 GPU forward of the same build (the denominator of the FP32 target).
     fp64 = None
@@ -522,6 +564,7 @@ def main():
                     "d2h_bytes_per_step": d2h * world},
             "gpu_launches": launches_per_step * args.steps,
             "fp64_forward": fp64,
+            "forward_adjoint": fwd_adj,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

@@ -415,6 +415,80 @@ int rrtmgp_b200_adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int
         float* grad_lwp, float* grad_iwp, float* grad_rel, float* grad_rei,
         float* grad_sfc_alb_dir, float* grad_sfc_alb_dif, void* stream);
 
+/* ---- Batched forward of many independent column grids ------------------------------------
+ * No reference counterpart as one call: the reference's driver runs one grid at a time and
+ * splits its columns into blocks of n_col_block (src_test/Radiation_solver.cu:467-615 and
+ * :683-950 called per block from src_test/test_rte_rrtmgp.cu).  A batch describes up to
+ * thousands of grids of uneven ncol / nlay whose device arrays stay fixed; one run computes
+ * the longwave and shortwave forwards of every grid (the same results as
+ * rrtmgp_b200_forward_lw_f32 / _sw_f32 per grid) in ONE persistent kernel launch: each CTA
+ * takes tiles of (grid, domain, columns) from a device work counter, ordered by decreasing
+ * tile cost.  A tile runs columns_per_cta columns side by side, each on
+ * ceil(nlay / chunk) warps with its own hardware barrier.  The tile shape (chunk, columns)
+ * of every (domain, 8-layer bin) comes from a built-in heuristic, from
+ * rrtmgp_b200_batch_autotune, or from rrtmgp_b200_batch_set_plan (a cached result). */
+typedef struct rrtmgp_b200_batch_grid {
+    int ncol, nlay;                    /* nlay <= 256                                        */
+    const float* play;                 /* (ncol, nlay), column fastest, device                */
+    const float* plev;                 /* (ncol, nlay+1)                                      */
+    const float* tlay;                 /* (ncol, nlay)                                        */
+    const float* tlev;                 /* (ncol, nlay+1), longwave only                       */
+    const float* tsfc;                 /* (ncol), longwave only                               */
+    const float* col_dry;              /* (ncol, nlay) or NULL (from h2o and plev)            */
+    const rrtmgp_b200_gas_conc* gases; /* host array, read by rrtmgp_b200_batch_create;        */
+    int ngases;                        /* the vmr arrays it points to must stay valid          */
+    const float* lwp;                  /* (ncol, nlay) x 4, or all NULL: clear sky             */
+    const float* iwp;
+    const float* rel;
+    const float* rei;
+    const float* sfc_emis;             /* (nband_lw, ncol)                                    */
+    float* lw_flux_up;                 /* (ncol, nlay+1) x 3 and (ncol, nlay); lw_flux_up     */
+    float* lw_flux_dn;                 /* NULL: no longwave for this grid                     */
+    float* lw_flux_net;
+    float* lw_heating_rate;
+    const float* mu0;                  /* (ncol) > 0                                          */
+    const float* tsi_scaling;          /* (ncol) or NULL                                      */
+    const float* sfc_alb_dir;          /* (nband_sw, ncol)                                    */
+    const float* sfc_alb_dif;
+    float* sw_flux_up;                 /* (ncol, nlay+1) x 4 and (ncol, nlay); sw_flux_up     */
+    float* sw_flux_dn;                 /* NULL: no shortwave for this grid                    */
+    float* sw_flux_dn_dir;
+    float* sw_flux_net;
+    float* sw_heating_rate;
+} rrtmgp_b200_batch_grid;
+
+typedef struct rrtmgp_b200_batch_t* rrtmgp_b200_batch;
+
+#define RRTMGP_B200_BATCH_PERSISTENT 0  /* one persistent launch (work counter reset first)  */
+#define RRTMGP_B200_BATCH_GRAPH 1       /* the same, replayed from a captured CUDA graph     */
+#define RRTMGP_B200_BATCH_PER_GRID 2    /* one fused launch per grid and domain (comparison) */
+
+/* k_lw / k_sw: longwave / shortwave k-distributions (either may be NULL when no grid needs
+ * that domain); cloud_lw / cloud_sw: cloud LUTs (NULL: clear sky for every grid). */
+int rrtmgp_b200_batch_create(rrtmgp_b200_kdist k_lw, rrtmgp_b200_cloud cloud_lw,
+        rrtmgp_b200_kdist k_sw, rrtmgp_b200_cloud cloud_sw, int delta_cloud,
+        const rrtmgp_b200_batch_grid* grids, int ngrids, rrtmgp_b200_batch* out);
+int rrtmgp_b200_batch_destroy(rrtmgp_b200_batch b);
+/* Runs every grid once on stream (mode: RRTMGP_B200_BATCH_*).  One run may be in flight per
+ * batch.  The first GRAPH run (and the first after a plan change) captures the graph. */
+int rrtmgp_b200_batch_run(rrtmgp_b200_batch b, int mode, void* stream);
+/* Times every candidate tile shape of every (domain, 8-layer bin) that the batch holds on a
+ * replicated sample of its widest grid in that bin (persistent launches on stream, `reps`
+ * timed runs each, the fastest counts) and keeps the fastest.  Synchronous.  Run it with the
+ * inputs filled: the sample writes the outputs of the sampled grids. */
+int rrtmgp_b200_batch_autotune(rrtmgp_b200_batch b, int reps, void* stream);
+/* Tile shape of domain (0 longwave, 1 shortwave) for nlay in [8 bin - 7, 8 bin], bin 1..32:
+ * chunk (8 or 16 layers per warp), columns per CTA, and the time of one tile in
+ * microseconds (the work order key; 0 before any autotune).  set_plan validates the shape. */
+int rrtmgp_b200_batch_get_plan(rrtmgp_b200_batch b, int domain, int bin, int* chunk, int* columns,
+        float* tile_us);
+int rrtmgp_b200_batch_set_plan(rrtmgp_b200_batch b, int domain, int bin, int chunk, int columns,
+        float tile_us);
+/* Work description of the current plan: total tiles, persistent CTAs, dynamic shared memory
+ * per CTA (bytes) and kernel launches per run of each mode (persistent, per grid). */
+int rrtmgp_b200_batch_stats(rrtmgp_b200_batch b, long long* ntiles, int* ctas, int* smem_bytes,
+        int* launches_persistent, int* launches_per_grid);
+
 /* No reference counterpart: FP32 FMA throughput probe used as the FP32-pipe roofline
  * denominator by the benchmark.  blocks x 512 threads, iters x 128 FMAs per thread
  * (FLOP = blocks * 512 * iters * 256); out (blocks floats) is written only in a case that

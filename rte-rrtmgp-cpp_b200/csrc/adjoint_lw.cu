@@ -159,7 +159,8 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
     const double pi = 3.14159265358979323846;
     const bool top_at_1 = play[icol] < play[icol + size_t(nlay - 1) * ncol];
     const float ts = tsfc[icol];
-    setup_layers(k, gs, ncol, nlay, icol, top_at_1, play, plev, tlay, tlev, col_dry_in, st, sm_cg);
+    setup_layers(k, gs, ncol, nlay, icol, top_at_1, play, plev, tlay, tlev, col_dry_in, st, sm_cg, threadIdx.x,
+                 blockDim.x);
     for (int idx = threadIdx.x; idx < nlay * nband; idx += blockDim.x) {
         const int j = idx % nlay, b = idx / nlay;
         float tau = 0.f, s, g;

@@ -1,69 +1,11 @@
-// Fused longwave forward: gas optics + cloud optics (1scl, added by band) + no-scattering
-// solver + broadband fluxes + heating rates for whole columns, without materialising any
-// (ncol, nlay, ngpt) array.  The staged equivalent is the sequence of
-// Radiation_solver_longwave::solve_gpu (src_test/Radiation_solver.cu:467-615).
-//
-// Per group of 32 g-points (see fused_common.cuh for the thread mapping):
-//   1. each warp writes the records of its layer chunk;
-//   2. pass 1: per (layer, g-point) tau, Planck fraction, 1 - transmissivity and the two
-//      linear-in-tau sources (lw_solver_noscat step 1) stay in registers; the warp composes
-//      its chunk's affine down and up maps x -> A x + B and publishes them;
-//   3. after one barrier every thread composes the maps of the other chunks to get its
-//      chunk's incoming down and up radiances (surface: radn_dn * (1 - emis) + emis * sfc_src);
-//   4. pass 2 re-sweeps the registers: level radiances and the per-layer absorbed radiance
-//      omt * (I_dn(top) + I_up(bottom)) - S_dn - S_up, which gives heating rates without
-//      differencing two nearly equal FP32 level fluxes;
-//   5. a warp reduce-scatter (31 shuffles per 32 values) sums over the 32 g-points and every
-//      lane accumulates one level (or layer) in FP64.
-#include "fused_common.cuh"
+// Fused longwave forward kernel (one CTA per column) and its launcher; the per-column
+// algorithm is in lw_column.cuh.
+#include "lw_column.cuh"
 
 namespace rrtmgp_b200 {
 namespace {
 
 using namespace fused;
-
-struct CloudArgs {
-    CloudLut<float> L;
-    const float* lwp;
-    const float* iwp;
-    const float* rel;
-    const float* rei;
-    int present;
-};
-
-// Layer transmissivity complement and sources in FP32: series below tau = 0.1 (7 and 6 terms,
-// truncation < 2e-11 relative), exp/divide intrinsics above where no cancellation occurs.
-// Both forms are evaluated and one is selected, so the warp does not diverge.  Same physics
-// as lw_solver_noscat_step_1_kernel (rte_solver_kernels.cu:116-125).
-__device__ __forceinline__ void lw_layer_fast(float tau, float D, float lay, float ldn, float lup, float& omt,
-                                              float& sdn, float& sup)
-{
-    const float tl = tau * D;
-    const float s_omt = tl * (1.f + tl * (-0.5f + tl * (1.f / 6.f + tl * (-1.f / 24.f + tl * (1.f / 120.f +
-                        tl * (-1.f / 720.f + tl * (1.f / 5040.f)))))));
-    const float s_fact = tl * (0.5f + tl * (-1.f / 3.f + tl * (0.125f + tl * (-1.f / 30.f + tl * (1.f / 144.f -
-                         tl * (1.f / 840.f))))));
-    const float trans = __expf(-tl);
-    const float e_omt = 1.f - trans;
-    const float e_fact = __fdividef(e_omt, tl) - trans;
-    const bool thin = tl < 0.1f;
-    omt = thin ? s_omt : e_omt;
-    const float fact = thin ? s_fact : e_fact;
-    sdn = omt * ldn + 2.f * fact * (lay - ldn);
-    sup = omt * lup + 2.f * fact * (lay - lup);
-}
-
-__device__ __forceinline__ void build_lw_record(const KdistView<float>& k, Rec& R, const LayerState& s,
-                                                const float* cg, int nlay, int b, float tau_cld, bool bottom,
-                                                float tsfc)
-{
-    record_weights(k, R, s, cg, nlay, b);
-    const float* tp = k.totplnk + size_t(b) * k.nplanck;
-    R.aux = make_float4(interpolate1D(s.t, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp),
-                        interpolate1D(s.t_top, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp),
-                        interpolate1D(s.t_bot, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp), tau_cld);
-    R.aux2 = bottom ? interpolate1D(tsfc, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp) : 0.f;
-}
 
 template <int CL>
 __global__ void __launch_bounds__(512)
@@ -74,165 +16,9 @@ lw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const CloudA
                   float* __restrict__ flux_up, float* __restrict__ flux_dn, float* __restrict__ flux_net,
                   float* __restrict__ heating_rate)
 {
-    static_assert(CL == 8 || CL == 16, "chunk length");
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int icol = blockIdx.x;
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int NW = blockDim.x >> 5;
-    const int nband = k.nband;
-    const SmemLayout SL = smem_layout(nlay, k.ngas, nband, 1, NW, 1, CL, k.max_group_bands);
-    LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
-    float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
-    float* sm_cld = reinterpret_cast<float*>(smem_raw + SL.cloud);
-    float4* sm_maps = reinterpret_cast<float4*>(smem_raw + SL.maps);
-    float* sm_sfc = reinterpret_cast<float*>(smem_raw + SL.sfc);
-    Rec* recs = reinterpret_cast<Rec*>(smem_raw + SL.recs) + w * CL * k.max_group_bands;
-
-    const bool top_at_1 = play[icol] < play[icol + size_t(nlay - 1) * ncol];
-    const float ts = tsfc[icol];
-    setup_layers(k, gs, ncol, nlay, icol, top_at_1, play, plev, tlay, tlev, col_dry_in, st, sm_cg);
-    for (int idx = threadIdx.x; idx < nlay * nband; idx += blockDim.x) {
-        const int j = idx % nlay, b = idx / nlay;
-        float tau = 0.f, s, g;
-        if (cld.present) {
-            const int l = top_at_1 ? j : nlay - 1 - j;
-            const size_t cl = icol + size_t(l) * ncol;
-            const CloudPoint<float> cp = cloud_point(cld.L, cld.lwp[cl], cld.iwp[cl], cld.rel[cl], cld.rei[cl]);
-            cloud_band<float, false>(cld.L, cp, b, tau, s, g);
-        }
-        sm_cld[b * nlay + j] = tau;
-    }
-    __syncthreads();
-
-    const float D = 1.66f;                 // single-angle secant (Rte_lw.cpp:101-113)
-    const int ngpt = k.ngpt;
-    double acc_lev = 0.0, acc_div = 0.0, acc_bot_up = 0.0, acc_bot_dn = 0.0;
-
-    for (int gg = 0; gg < k.ngroups; ++gg) {
-        const int g = 32 * gg + lane;
-        const bool gv = g < ngpt;
-        const int b0 = k.group_band0[gg];
-        const int gband = gv ? k.gpt2band[g] : b0;
-        const int slot = gband - b0;
-        const int4 mg0 = minor_entry(k.minor_g[0], g, gv);
-        const int4 mg1 = minor_entry(k.minor_g[1], g, gv);
-        const int nm0 = __reduce_max_sync(0xffffffffu, mg0.x);
-        const int nm1 = __reduce_max_sync(0xffffffffu, mg1.x);
-
-        // 1. records of this warp's chunk
-        for (int r = lane; r < CL * k.max_group_bands; r += 32) {
-            const int jj = w * CL + (r % CL);
-            const int b = b0 + r / CL;
-            if (jj < nlay && b < nband && k.band_lims[2 * b] < 32 * gg + 32)
-                build_lw_record(k, recs[r], st[jj], sm_cg + jj, nlay, b, sm_cld[b * nlay + jj], jj == nlay - 1, ts);
-        }
-        __syncwarp();
-
-        // 2. pass 1
-        float omt[CL], sdn[CL], sup[CL];
-        float Ad = 1.f, Bd = 0.f;
-#pragma unroll
-        for (int i = 0; i < CL; ++i) {
-            const int j = w * CL + i;
-            omt[i] = 0.f; sdn[i] = 0.f; sup[i] = 0.f;
-            if (j < nlay && gv) {
-                const Rec& R = recs[slot * CL + i];
-                const float tau = tau_abs(k, R, g, R.a ? mg1 : mg0, R.a ? nm1 : nm0) + R.aux.w;
-                const float4 p0 = __ldg(k.pfrac4 + (R.kb.x + g));
-                const float4 p1 = __ldg(k.pfrac4 + (R.kb.y + g));
-                const float pfrac = (R.wpl0.x * p0.x + R.wpl0.y * p0.y + R.wpl0.z * p0.z + R.wpl0.w * p0.w) +
-                                    (R.wpl1.x * p1.x + R.wpl1.y * p1.y + R.wpl1.z * p1.z + R.wpl1.w * p1.w);
-                lw_layer_fast(tau, D, pfrac * R.aux.x, pfrac * R.aux.z, pfrac * R.aux.y, omt[i], sdn[i], sup[i]);
-                if (j == nlay - 1) sm_sfc[lane] = pfrac * R.aux2;
-            } else if (j == nlay - 1) {
-                sm_sfc[lane] = 0.f;
-            }
-            Ad = (1.f - omt[i]) * Ad;
-            Bd = (1.f - omt[i]) * Bd + sdn[i];
-        }
-        float Au = 1.f, Bu = 0.f;
-#pragma unroll
-        for (int i = CL - 1; i >= 0; --i) {
-            Au = (1.f - omt[i]) * Au;
-            Bu = (1.f - omt[i]) * Bu + sup[i];
-        }
-        sm_maps[w * 32 + lane] = make_float4(Ad, Bd, Au, Bu);
-        __syncthreads();
-
-        // 3. incoming radiances of the chunk (no incident longwave flux at the top)
-        float x = 0.f, xin = 0.f;
-        for (int c = 0; c < NW; ++c) {
-            if (c == w) xin = x;
-            const float4 m = sm_maps[c * 32 + lane];
-            x = m.x * x + m.y;
-        }
-        const float emis = gv ? __ldg(sfc_emis + gband + size_t(icol) * nband) : 0.f;
-        const float S = x * (1.f - emis) + emis * sm_sfc[lane];
-        float y = S;
-        for (int c = NW - 1; c > w; --c) {
-            const float4 m = sm_maps[c * 32 + lane];
-            y = m.z * y + m.w;
-        }
-
-        // 4. pass 2
-        float v[2 * CL], dv[CL];
-        float rd = xin;
-#pragma unroll
-        for (int i = 0; i < CL; ++i) {
-            v[CL + i] = rd;  // down radiance at the top of layer i
-            rd = (1.f - omt[i]) * rd + sdn[i];
-        }
-        float ru = y;
-#pragma unroll
-        for (int i = CL - 1; i >= 0; --i) {
-            dv[i] = omt[i] * (v[CL + i] + ru) - sdn[i] - sup[i];
-            ru = (1.f - omt[i]) * ru + sup[i];
-            v[i] = ru;       // up radiance at the top of layer i
-        }
-        // 5. sums over the 32 g-points of the group
-        ReduceScatter<2 * CL, 16>::run(v, lane);
-        ReduceScatter<CL, 16>::run(dv, lane);
-        acc_lev += double(v[0]);
-        acc_div += double(dv[0]);
-        if (w == NW - 1) {
-            acc_bot_up += double(warp_sum(S));
-            acc_bot_dn += double(warp_sum(rd));
-        }
-        __syncthreads();
-    }
-
-    // Outputs.  Fluxes = 2 pi w * (sum of radiances) with w = 0.5.
-    const double pi = 3.14159265358979323846;
-    constexpr int SH_LEV = (CL == 16) ? 0 : 1;   // lane L holds value L >> SH_LEV
-    constexpr int SH_DIV = (CL == 16) ? 1 : 2;
-    const int vidx = lane >> SH_LEV;
-    const double other = __shfl_xor_sync(0xffffffffu, acc_lev, CL << SH_LEV);
-    if ((lane & ((1 << SH_LEV) - 1)) == 0 && vidx < CL) {
-        const int jl = w * CL + vidx;
-        if (jl < nlay) {
-            const int al = top_at_1 ? jl : nlay - jl;
-            const size_t o = icol + size_t(al) * ncol;
-            const double up = pi * acc_lev, dn = pi * other;
-            flux_up[o] = float(up);
-            flux_dn[o] = float(dn);
-            flux_net[o] = float(dn - up);
-        }
-    }
-    if ((lane & ((1 << SH_DIV) - 1)) == 0) {
-        const int jl = w * CL + (lane >> SH_DIV);
-        if (jl < nlay && (lane >> SH_DIV) < CL) {
-            const int l = top_at_1 ? jl : nlay - 1 - jl;
-            const double g0_cp = 9.80665 / 1004.64;
-            heating_rate[icol + size_t(l) * ncol] = float(g0_cp * 86400.0 * pi * acc_div / double(st[jl].dp));
-        }
-    }
-    if (w == NW - 1 && lane == 0) {
-        const int al = top_at_1 ? nlay : 0;
-        const size_t o = icol + size_t(al) * ncol;
-        flux_up[o] = float(pi * acc_bot_up);
-        flux_dn[o] = float(pi * acc_bot_dn);
-        flux_net[o] = float(pi * (acc_bot_dn - acc_bot_up));
-    }
+    lw_forward_column<CL>(whole_cta(smem_raw), k, gs, cld, ncol, nlay, blockIdx.x, play, plev, tlay, tlev, tsfc,
+                          col_dry_in, sfc_emis, flux_up, flux_dn, flux_net, heating_rate);
 }
 
 template <int CL>

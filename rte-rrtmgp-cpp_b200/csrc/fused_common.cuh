@@ -151,14 +151,38 @@ __device__ __forceinline__ int4 minor_entry(const int4* mgt, int g, bool valid)
     return m;
 }
 
-// Fill the per-layer state of column icol (layers counted from the top) and col_gas.
+// A set of whole warps that computes one column together: either the whole CTA (barrier 0)
+// or a slice of a persistent CTA with its own hardware barrier and shared-memory region.
+struct Team {
+    unsigned char* smem;   // the team's shared-memory region (16-byte aligned)
+    int tid;               // thread index within the team
+    int nthreads;          // multiple of 32
+    int bar;               // hardware barrier id (0 = __syncthreads of the whole CTA)
+    __device__ __forceinline__ int warp() const { return tid >> 5; }
+    __device__ __forceinline__ int nwarps() const { return nthreads >> 5; }
+    __device__ __forceinline__ void sync() const
+    {
+        if (bar == 0)
+            __syncthreads();
+        else
+            asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(nthreads) : "memory");
+    }
+};
+
+__device__ __forceinline__ Team whole_cta(unsigned char* smem)
+{
+    return Team{smem, int(threadIdx.x), int(blockDim.x), 0};
+}
+
+// Fill the per-layer state of column icol (layers counted from the top) and col_gas; threads
+// tid, tid + nthr, ... of the calling team take one layer each.
 __device__ __forceinline__ void setup_layers(const KdistView<float>& k, const GasSet<float>& gs, int ncol,
                                              int nlay, int icol, bool top_at_1, const float* __restrict__ play,
                                              const float* __restrict__ plev, const float* __restrict__ tlay,
                                              const float* __restrict__ tlev, const float* __restrict__ col_dry,
-                                             LayerState* st, float* cg)
+                                             LayerState* st, float* cg, int tid, int nthr)
 {
-    for (int j = threadIdx.x; j < nlay; j += blockDim.x) {
+    for (int j = tid; j < nlay; j += nthr) {
         const int l = top_at_1 ? j : nlay - 1 - j;
         const size_t cl = icol + size_t(l) * ncol;
         const float p = play[cl], t = tlay[cl];

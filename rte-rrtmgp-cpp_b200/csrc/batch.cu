@@ -30,7 +30,6 @@ using namespace fused;
 constexpr int kBatchThreads = 512;   // 16 warps per persistent CTA
 constexpr int kBatchWarps = kBatchThreads / 32;
 constexpr int kMaxBins = 32;         // nlay <= 256 in 8-layer bins
-constexpr int kMaxSmem = 226 * 1024;     // dynamic; leaves room for the static words
 constexpr int kMaxTeams = 15;        // hardware barriers 1..15 (0 is __syncthreads)
 
 // One (grid, domain) work item as the persistent kernel reads it.
@@ -39,7 +38,8 @@ struct BatchItem {
     int domain;        // 0 longwave, 1 shortwave
     int cl, W, P;      // chunk length, warps per column, columns per tile
     int team_smem;     // bytes of shared memory per team (16-byte multiple)
-    int cloudy;
+    int cloudy, delta;
+    CloudLut<float> lut;
     const float *play, *plev, *tlay, *tlev, *tsfc, *col_dry;
     const float *lwp, *iwp, *rel, *rei;
     const float *emis;                           // longwave
@@ -48,16 +48,82 @@ struct BatchItem {
     GasSet<float> gs;
 };
 
+// Per-warp view of the current tile: which column the warp's team computes, where the team's
+// warps and shared memory start, its hardware barrier.
+struct WarpSlot {
+    int icol, first_warp, nwarps, bar, smem_off, active, pad0, pad1;
+};
+
+// The current tile's item and warp slots, staged in shared memory at every tile.
+__shared__ BatchItem g_item;
+__shared__ WarpSlot g_slot[kBatchWarps];
+
+__device__ __forceinline__ int warp_uniform(int v) { return __reduce_max_sync(0xffffffffu, v); }
+
+// Team context.  Its values are made warp-uniform (redux) once per tile, so that the compiler
+// keeps them in uniform registers and the column code keeps its uniform branches and address
+// arithmetic, as with blockIdx / blockDim in the per-grid kernels.
+struct TeamCtx {
+    int ic, fw, nw, bar, soff;
+    __device__ __forceinline__ int icol() const { return ic; }
+    __device__ __forceinline__ int warp() const { return int(threadIdx.x >> 5) - fw; }
+    __device__ __forceinline__ int nwarps() const { return nw; }
+    __device__ __forceinline__ int tid() const { return int(threadIdx.x) - 32 * fw; }
+    __device__ __forceinline__ int nthreads() const { return 32 * nw; }
+    __device__ __forceinline__ unsigned char* smem() const
+    {
+        extern __shared__ __align__(16) unsigned char smem_raw[];
+        return smem_raw + soff;
+    }
+    __device__ __forceinline__ void sync() const
+    {
+        asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(32 * nw) : "memory");
+    }
+};
+
+// Item arguments: the sizes as warp-uniform values, the arrays read from the staged item where
+// they are used (setup, once per group of g-points, outputs).
+struct ItemIo {
+    int nc, nl;
+    __device__ __forceinline__ int ncol() const { return nc; }
+    __device__ __forceinline__ int nlay() const { return nl; }
+    __device__ __forceinline__ const float* play() const { return g_item.play; }
+    __device__ __forceinline__ const float* plev() const { return g_item.plev; }
+    __device__ __forceinline__ const float* tlay() const { return g_item.tlay; }
+    __device__ __forceinline__ const float* tlev() const { return g_item.tlev; }
+    __device__ __forceinline__ const float* tsfc() const { return g_item.tsfc; }
+    __device__ __forceinline__ const float* col_dry() const { return g_item.col_dry; }
+    __device__ __forceinline__ const float* emis() const { return g_item.emis; }
+    __device__ __forceinline__ const float* mu0() const { return g_item.mu0; }
+    __device__ __forceinline__ const float* tsi() const { return g_item.tsi; }
+    __device__ __forceinline__ const float* alb_dir() const { return g_item.alb_dir; }
+    __device__ __forceinline__ const float* alb_dif() const { return g_item.alb_dif; }
+    __device__ __forceinline__ float* up() const { return g_item.up; }
+    __device__ __forceinline__ float* dn() const { return g_item.dn; }
+    __device__ __forceinline__ float* dir() const { return g_item.dir; }
+    __device__ __forceinline__ float* net() const { return g_item.net; }
+    __device__ __forceinline__ float* hr() const { return g_item.hr; }
+    __device__ __forceinline__ const GasSet<float>& gs() const { return g_item.gs; }
+    __device__ __forceinline__ CloudArgs cloud() const
+    {
+        return CloudArgs{g_item.lut, g_item.lwp, g_item.iwp, g_item.rel, g_item.rei, g_item.cloudy};
+    }
+};
+
+struct SwItemIo : ItemIo {
+    __device__ __forceinline__ SwCloudArgs cloud() const
+    {
+        return SwCloudArgs{g_item.lut, g_item.lwp, g_item.iwp, g_item.rel, g_item.rei, g_item.cloudy, g_item.delta};
+    }
+};
+
 __global__ void __launch_bounds__(kBatchThreads, 1)
-batch_forward_kernel(const KdistView<float> klw, const KdistView<float> ksw, const CloudLut<float> llw,
-                     const CloudLut<float> lsw, int delta, const BatchItem* __restrict__ items,
+batch_forward_kernel(const KdistView<float> klw, const KdistView<float> ksw, const BatchItem* __restrict__ items,
                      const long long* __restrict__ tile_start, int nitems, unsigned long long* __restrict__ counter)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ long long s_tile;
     __shared__ int s_item;
     const long long ntiles = tile_start[nitems];
-    const int warp = threadIdx.x >> 5;
     for (;;) {
         if (threadIdx.x == 0) {
             const long long t = (long long)atomicAdd(counter, 1ull);
@@ -73,33 +139,45 @@ batch_forward_kernel(const KdistView<float> klw, const KdistView<float> ksw, con
         const long long t = s_tile;
         const int ii = s_item;
         if (t >= ntiles) break;
-        const BatchItem& it = items[ii];
-        const int W = it.W;
-        const int team = warp / W;
-        if (team < it.P) {
+        // stage the item and the warp slots of this tile
+        const int* src = reinterpret_cast<const int*>(items + ii);
+        for (int q = threadIdx.x; q < int(sizeof(BatchItem) / 4); q += blockDim.x)
+            reinterpret_cast<int*>(&g_item)[q] = __ldg(src + q);
+        if (threadIdx.x < kBatchWarps) {
+            const BatchItem& it = items[ii];
+            const int team = int(threadIdx.x) / it.W;
             const int icol = int(t - tile_start[ii]) * it.P + team;
-            if (icol < it.ncol) {
-                const Team T{smem_raw + size_t(team) * it.team_smem, int(threadIdx.x) - team * W * 32, W * 32,
-                             1 + team};
-                if (it.domain == 0) {
-                    const CloudArgs ca{llw, it.lwp, it.iwp, it.rel, it.rei, it.cloudy};
-                    if (it.cl == 8)
-                        lw_forward_column<8>(T, klw, it.gs, ca, it.ncol, it.nlay, icol, it.play, it.plev, it.tlay,
-                                             it.tlev, it.tsfc, it.col_dry, it.emis, it.up, it.dn, it.net, it.hr);
-                    else
-                        lw_forward_column<16>(T, klw, it.gs, ca, it.ncol, it.nlay, icol, it.play, it.plev, it.tlay,
-                                              it.tlev, it.tsfc, it.col_dry, it.emis, it.up, it.dn, it.net, it.hr);
-                } else {
-                    const SwCloudArgs ca{lsw, it.lwp, it.iwp, it.rel, it.rei, it.cloudy, delta};
-                    if (it.cl == 8)
-                        sw_forward_column<8>(T, ksw, it.gs, ca, it.ncol, it.nlay, icol, it.play, it.plev, it.tlay,
-                                             it.col_dry, it.mu0, it.tsi, it.alb_dir, it.alb_dif, it.up, it.dn,
-                                             it.dir, it.net, it.hr);
-                    else
-                        sw_forward_column<16>(T, ksw, it.gs, ca, it.ncol, it.nlay, icol, it.play, it.plev, it.tlay,
-                                              it.col_dry, it.mu0, it.tsi, it.alb_dir, it.alb_dif, it.up, it.dn,
-                                              it.dir, it.net, it.hr);
-                }
+            WarpSlot sl;
+            sl.icol = icol;
+            sl.first_warp = team * it.W;
+            sl.nwarps = it.W;
+            sl.bar = 1 + team;
+            sl.smem_off = team * it.team_smem;
+            sl.active = team < it.P && icol < it.ncol;
+            sl.pad0 = sl.pad1 = 0;
+            g_slot[threadIdx.x] = sl;
+        }
+        __syncthreads();
+        const WarpSlot& q = g_slot[threadIdx.x >> 5];
+        if (warp_uniform(q.active)) {
+            // The shared-memory offset is rebuilt from a 16-byte count so that the compiler knows
+            // its alignment (with an unknown low part, the column code ran ~15% slower).
+            const TeamCtx cx{warp_uniform(q.icol), warp_uniform(q.first_warp), warp_uniform(q.nwarps),
+                             warp_uniform(q.bar), warp_uniform(q.smem_off >> 4) << 4};
+            const int domain = warp_uniform(g_item.domain), cl = warp_uniform(g_item.cl);
+            const int nc = warp_uniform(g_item.ncol), nl = warp_uniform(g_item.nlay);
+            if (domain == 0) {
+                const ItemIo io{nc, nl};
+                if (cl == 8)
+                    lw_forward_column<8>(cx, klw, io);
+                else
+                    lw_forward_column<16>(cx, klw, io);
+            } else {
+                const SwItemIo io{{nc, nl}};
+                if (cl == 8)
+                    sw_forward_column<8>(cx, ksw, io);
+                else
+                    sw_forward_column<16>(cx, ksw, io);
             }
         }
         __syncthreads();
@@ -158,6 +236,7 @@ struct rrtmgp_b200_batch_t {
     std::vector<BatchItem> items;      // unplanned items (cl, W, P, team_smem set by plan())
     TileShape shape[2][kMaxBins + 1];  // [domain][bin]
     int nsm = 0, device = 0;
+    int max_smem = 0;                  // dynamic shared memory per CTA the kernel may use
     // planned state
     bool dirty = true;
     std::vector<BatchItem> order;      // planned items in work order
@@ -192,7 +271,7 @@ int max_columns(const rrtmgp_b200_batch_t* b, int domain, int nlay, int cl)
     const int W = ceil_div_i(nlay, cl);
     if (W > kBatchWarps) return 0;
     const size_t per = team_smem_bytes(b, domain, nlay, cl);
-    return int(std::min<size_t>(std::min(kBatchWarps / W, kMaxTeams), kMaxSmem / per));
+    return int(std::min<size_t>(std::min(kBatchWarps / W, kMaxTeams), size_t(b->max_smem) / per));
 }
 
 // Shape of (domain, bin) for a grid of nlay layers: the stored shape when it fits, else the
@@ -311,8 +390,7 @@ int launch_persistent(rrtmgp_b200_batch_t* b, const BatchItem* d_items, const lo
     const int ctas = int(std::min<long long>(b->nsm, std::max<long long>(ntiles, 1)));
     const KdistView<float> klw = b->k[0] ? b->k[0]->v32 : KdistView<float>{};
     const KdistView<float> ksw = b->k[1] ? b->k[1]->v32 : KdistView<float>{};
-    batch_forward_kernel<<<ctas, kBatchThreads, smem, s>>>(klw, ksw, lut_of(b->c[0]), lut_of(b->c[1]), b->delta,
-                                                          d_items, d_starts, nitems, b->d_counter);
+    batch_forward_kernel<<<ctas, kBatchThreads, smem, s>>>(klw, ksw, d_items, d_starts, nitems, b->d_counter);
     RB_LAUNCH("batch_forward_kernel");
     return RRTMGP_B200_OK;
 }
@@ -325,7 +403,7 @@ int run_per_grid(rrtmgp_b200_batch_t* b, cudaStream_t s)
             int st = forward_lw_f32(b->k[0], cloudy ? b->c[0] : nullptr, g.ncol, g.nlay, g.play, g.plev, g.tlay,
                                     g.tlev, g.tsfc, g.col_dry, g.gases, g.ngases, g.lwp, g.iwp, g.rel, g.rei,
                                     g.sfc_emis, g.lw_flux_up, g.lw_flux_dn, g.lw_flux_net, g.lw_heating_rate,
-                                    g.nlay > 128 ? 16 : 8, s);
+                                    0, s);
             if (st) return st;
         }
         if (g.sw_flux_up) {
@@ -366,6 +444,7 @@ int batch_create(rrtmgp_b200_kdist klw, rrtmgp_b200_cloud clw, rrtmgp_b200_kdist
         RB_CHECK_ARG(!cloudy || (g.iwp && g.rel && g.rei), at + "cloud arrays must be all set or all NULL");
         RB_CHECK_ARG(g.lw_flux_up || g.sw_flux_up, at + "neither longwave nor shortwave outputs");
         BatchItem base{};
+        base.delta = delta;
         base.ncol = g.ncol;
         base.nlay = g.nlay;
         base.play = g.play;
@@ -383,6 +462,7 @@ int batch_create(rrtmgp_b200_kdist klw, rrtmgp_b200_cloud clw, rrtmgp_b200_kdist
             BatchItem it = base;
             it.domain = 0;
             it.cloudy = cloudy && clw;
+            it.lut = lut_of(clw);
             it.tlev = g.tlev;
             it.tsfc = g.tsfc;
             it.emis = g.sfc_emis;
@@ -401,6 +481,7 @@ int batch_create(rrtmgp_b200_kdist klw, rrtmgp_b200_cloud clw, rrtmgp_b200_kdist
             BatchItem it = base;
             it.domain = 1;
             it.cloudy = cloudy && csw;
+            it.lut = lut_of(csw);
             it.mu0 = g.mu0;
             it.tsi = g.tsi_scaling;
             it.alb_dir = g.sfc_alb_dir;
@@ -425,14 +506,19 @@ int batch_create(rrtmgp_b200_kdist klw, rrtmgp_b200_cloud clw, rrtmgp_b200_kdist
         b->grids.push_back(g);
     }
     for (size_t i = 0; i < b->grids.size(); ++i) b->grids[i].gases = b->gases[i].data();
+    RB_CUDA(cudaGetDevice(&b->device), "batch_create");
+    RB_CUDA(cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->device), "batch_create");
+    int optin = 0;
+    RB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device), "batch_create");
+    cudaFuncAttributes fa{};
+    RB_CUDA(cudaFuncGetAttributes(&fa, batch_forward_kernel), "batch_create");
+    b->max_smem = optin - int(fa.sharedSizeBytes);
+    RB_CUDA(cudaFuncSetAttribute(batch_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, b->max_smem),
+            "batch_create: kernel attribute");
     for (const BatchItem& it : b->items)
         if (!shape_for(b.get(), it.domain, it.nlay).cl)
             return fail(RRTMGP_B200_ERR_UNSUPPORTED, "batch_create: shared memory need too large for nlay = " +
                                                          std::to_string(it.nlay));
-    RB_CUDA(cudaGetDevice(&b->device), "batch_create");
-    RB_CUDA(cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->device), "batch_create");
-    RB_CUDA(cudaFuncSetAttribute(batch_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem),
-            "batch_create: kernel attribute");
     if (cudaMalloc(&b->d_counter, sizeof(unsigned long long)) != cudaSuccess) {
         cudaGetLastError();
         return fail(RRTMGP_B200_ERR_ALLOC, "batch_create: counter allocation failed");

@@ -8,17 +8,9 @@ namespace {
 using namespace fused;
 
 template <int CL>
-__global__ void __launch_bounds__(512)
-lw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const CloudArgs cld, int ncol, int nlay,
-                  const float* __restrict__ play, const float* __restrict__ plev, const float* __restrict__ tlay,
-                  const float* __restrict__ tlev, const float* __restrict__ tsfc,
-                  const float* __restrict__ col_dry_in, const float* __restrict__ sfc_emis,
-                  float* __restrict__ flux_up, float* __restrict__ flux_dn, float* __restrict__ flux_net,
-                  float* __restrict__ heating_rate)
+__global__ void __launch_bounds__(512) lw_forward_kernel(const KdistView<float> k, const LwGridIo io)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    lw_forward_column<CL>(whole_cta(smem_raw), k, gs, cld, ncol, nlay, blockIdx.x, play, plev, tlay, tlev, tsfc,
-                          col_dry_in, sfc_emis, flux_up, flux_dn, flux_net, heating_rate);
+    lw_forward_column<CL>(CtaCtx{}, k, io);
 }
 
 template <int CL>
@@ -45,8 +37,8 @@ int launch_lw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
         ca.lwp = lwp; ca.iwp = iwp; ca.rel = rel; ca.rei = rei;
         ca.present = 1;
     }
-    lw_forward_kernel<CL><<<ncol, NW * 32, smem, stream>>>(v, gs, ca, ncol, nlay, play, plev, tlay, tlev, tsfc,
-                                                             col_dry, emis, up, dn, net, hr);
+    LwGridIo io{ncol, nlay, play, plev, tlay, tlev, tsfc, col_dry, emis, up, dn, net, hr, gs, ca};
+    lw_forward_kernel<CL><<<ncol, NW * 32, smem, stream>>>(v, io);
     RB_LAUNCH("lw_forward_kernel");
     return RRTMGP_B200_OK;
 }

@@ -8,17 +8,9 @@ namespace {
 using namespace fused;
 
 template <int CL>
-__global__ void __launch_bounds__(512)
-sw_forward_kernel(const KdistView<float> k, const GasSet<float> gs, const SwCloudArgs cld, int ncol, int nlay,
-                  const float* __restrict__ play, const float* __restrict__ plev, const float* __restrict__ tlay,
-                  const float* __restrict__ col_dry_in, const float* __restrict__ mu0_in,
-                  const float* __restrict__ tsi_scaling, const float* __restrict__ alb_dir,
-                  const float* __restrict__ alb_dif, float* __restrict__ flux_up, float* __restrict__ flux_dn,
-                  float* __restrict__ flux_dir, float* __restrict__ flux_net, float* __restrict__ heating_rate)
+__global__ void __launch_bounds__(512) sw_forward_kernel(const KdistView<float> k, const SwGridIo io)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    sw_forward_column<CL>(whole_cta(smem_raw), k, gs, cld, ncol, nlay, blockIdx.x, play, plev, tlay, col_dry_in,
-                          mu0_in, tsi_scaling, alb_dir, alb_dif, flux_up, flux_dn, flux_dir, flux_net, heating_rate);
+    sw_forward_column<CL>(CtaCtx{}, k, io);
 }
 
 template <int CL>
@@ -47,8 +39,8 @@ int launch_sw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
         ca.present = 1;
         ca.delta = delta;
     }
-    sw_forward_kernel<CL><<<ncol, NW * 32, smem, stream>>>(v, gs, ca, ncol, nlay, play, plev, tlay, col_dry, mu0, tsi,
-                                                             alb_dir, alb_dif, up, dn, dir, net, hr);
+    SwGridIo io{ncol, nlay, play, plev, tlay, col_dry, mu0, tsi, alb_dir, alb_dif, up, dn, dir, net, hr, gs, ca};
+    sw_forward_kernel<CL><<<ncol, NW * 32, smem, stream>>>(v, io);
     RB_LAUNCH("sw_forward_kernel");
     return RRTMGP_B200_OK;
 }

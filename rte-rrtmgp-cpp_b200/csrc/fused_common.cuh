@@ -151,28 +151,22 @@ __device__ __forceinline__ int4 minor_entry(const int4* mgt, int g, bool valid)
     return m;
 }
 
-// A set of whole warps that computes one column together: either the whole CTA (barrier 0)
-// or a slice of a persistent CTA with its own hardware barrier and shared-memory region.
-struct Team {
-    unsigned char* smem;   // the team's shared-memory region (16-byte aligned)
-    int tid;               // thread index within the team
-    int nthreads;          // multiple of 32
-    int bar;               // hardware barrier id (0 = __syncthreads of the whole CTA)
-    __device__ __forceinline__ int warp() const { return tid >> 5; }
-    __device__ __forceinline__ int nwarps() const { return nthreads >> 5; }
-    __device__ __forceinline__ void sync() const
+// Context of a fused column computation when the whole CTA computes column blockIdx.x: every
+// value is a special register or a launch constant, so none occupies a register across the
+// column.  The batched kernel supplies its own context type with the same members.
+struct CtaCtx {
+    __device__ __forceinline__ int icol() const { return blockIdx.x; }
+    __device__ __forceinline__ int warp() const { return threadIdx.x >> 5; }
+    __device__ __forceinline__ int nwarps() const { return blockDim.x >> 5; }
+    __device__ __forceinline__ int tid() const { return threadIdx.x; }
+    __device__ __forceinline__ int nthreads() const { return blockDim.x; }
+    __device__ __forceinline__ unsigned char* smem() const
     {
-        if (bar == 0)
-            __syncthreads();
-        else
-            asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(nthreads) : "memory");
+        extern __shared__ __align__(16) unsigned char smem_raw[];
+        return smem_raw;
     }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
 };
-
-__device__ __forceinline__ Team whole_cta(unsigned char* smem)
-{
-    return Team{smem, int(threadIdx.x), int(blockDim.x), 0};
-}
 
 // Fill the per-layer state of column icol (layers counted from the top) and col_gas; threads
 // tid, tid + nthr, ... of the calling team take one layer each.

@@ -30,6 +30,30 @@ struct CloudArgs {
     int present;
 };
 
+// Arguments of the per-grid longwave kernel (passed by value: kernel parameters).
+struct LwGridIo {
+    int ncol_, nlay_;
+    const float *play_, *plev_, *tlay_, *tlev_, *tsfc_, *col_dry_, *emis_;
+    float *up_, *dn_, *net_, *hr_;
+    GasSet<float> gs_;
+    CloudArgs cld_;
+    __device__ __forceinline__ int ncol() const { return ncol_; }
+    __device__ __forceinline__ int nlay() const { return nlay_; }
+    __device__ __forceinline__ const float* play() const { return play_; }
+    __device__ __forceinline__ const float* plev() const { return plev_; }
+    __device__ __forceinline__ const float* tlay() const { return tlay_; }
+    __device__ __forceinline__ const float* tlev() const { return tlev_; }
+    __device__ __forceinline__ const float* tsfc() const { return tsfc_; }
+    __device__ __forceinline__ const float* col_dry() const { return col_dry_; }
+    __device__ __forceinline__ const float* emis() const { return emis_; }
+    __device__ __forceinline__ float* up() const { return up_; }
+    __device__ __forceinline__ float* dn() const { return dn_; }
+    __device__ __forceinline__ float* net() const { return net_; }
+    __device__ __forceinline__ float* hr() const { return hr_; }
+    __device__ __forceinline__ const GasSet<float>& gs() const { return gs_; }
+    __device__ __forceinline__ const CloudArgs& cloud() const { return cld_; }
+};
+
 // Layer transmissivity complement and sources in FP32: series below tau = 0.1 (7 and 6 terms,
 // truncation < 2e-11 relative), exp/divide intrinsics above where no cancellation occurs.
 // Both forms are evaluated and one is selected, so the warp does not diverge.  Same physics
@@ -64,52 +88,57 @@ __device__ __forceinline__ void build_lw_record(const KdistView<float>& k, Rec& 
     R.aux2 = bottom ? interpolate1D(tsfc, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp) : 0.f;
 }
 
-// One column (icol of a grid of ncol columns) by team T: T.nwarps() warps of CL layers each,
-// nlay <= T.nwarps() * CL (chunks past nlay are identity layers).
-template <int CL>
-__device__ __forceinline__ void lw_forward_column(const Team& T, const KdistView<float>& k,
-                                                  const GasSet<float>& gs,                                                   const CloudArgs& cld, int ncol, int nlay, int icol,
-                                                  const float* __restrict__ play, const float* __restrict__ plev,
-                                                  const float* __restrict__ tlay, const float* __restrict__ tlev,
-                                                  const float* __restrict__ tsfc, const float* __restrict__ col_dry_in,
-                                                  const float* __restrict__ sfc_emis, float* __restrict__ flux_up,
-                                                  float* __restrict__ flux_dn, float* __restrict__ flux_net,
-                                                  float* __restrict__ heating_rate)
+// One column by the warps that context cx names (cx.nwarps() warps of CL layers each,
+// nlay <= cx.nwarps() * CL; chunks past nlay are identity layers).  Context and arguments are
+// read through accessors at every use (cx: column index, warp, shared memory, barrier; io: grid
+// sizes, arrays, gas set, cloud arrays) so that the batched kernel, which keeps them in shared
+// memory, holds no register for them across the column (see LwGridIo / CtaCtx for the per-grid
+// kernel, where they are launch constants).
+template <int CL, class Cx, class Io>
+__device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<float>& k, const Io& io)
 {
     static_assert(CL == 8 || CL == 16, "chunk length");
-    unsigned char* const smem_raw = T.smem;
-    const int w = T.warp(), lane = T.tid & 31;
-    const int NW = T.nwarps();
+    const int lane = threadIdx.x & 31;
     const int nband = k.nband;
-    const SmemLayout SL = smem_layout(nlay, k.ngas, nband, 1, NW, 1, CL, k.max_group_bands);
+    const SmemLayout SL = smem_layout(io.nlay(), k.ngas, nband, 1, cx.nwarps(), 1, CL, k.max_group_bands);
+    unsigned char* const smem_raw = cx.smem();
     LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
     float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
     float* sm_cld = reinterpret_cast<float*>(smem_raw + SL.cloud);
     float4* sm_maps = reinterpret_cast<float4*>(smem_raw + SL.maps);
     float* sm_sfc = reinterpret_cast<float*>(smem_raw + SL.sfc);
-    Rec* recs = reinterpret_cast<Rec*>(smem_raw + SL.recs) + w * CL * k.max_group_bands;
+    Rec* recs = reinterpret_cast<Rec*>(smem_raw + SL.recs) + cx.warp() * CL * k.max_group_bands;
 
-    const bool top_at_1 = play[icol] < play[icol + size_t(nlay - 1) * ncol];
-    const float ts = tsfc[icol];
-    setup_layers(k, gs, ncol, nlay, icol, top_at_1, play, plev, tlay, tlev, col_dry_in, st, sm_cg, T.tid, T.nthreads);
-    for (int idx = T.tid; idx < nlay * nband; idx += T.nthreads) {
-        const int j = idx % nlay, b = idx / nlay;
-        float tau = 0.f, s, g;
-        if (cld.present) {
-            const int l = top_at_1 ? j : nlay - 1 - j;
-            const size_t cl = icol + size_t(l) * ncol;
-            const CloudPoint<float> cp = cloud_point(cld.L, cld.lwp[cl], cld.iwp[cl], cld.rel[cl], cld.rei[cl]);
-            cloud_band<float, false>(cld.L, cp, b, tau, s, g);
+    bool top_at_1;
+    float ts;
+    {
+        const int icol = cx.icol(), ncol = io.ncol(), nlay = io.nlay();
+        const float* play = io.play();
+        top_at_1 = play[icol] < play[icol + size_t(nlay - 1) * ncol];
+        ts = io.tsfc()[icol];
+        setup_layers(k, io.gs(), ncol, nlay, icol, top_at_1, play, io.plev(), io.tlay(), io.tlev(), io.col_dry(), st,
+                     sm_cg, cx.tid(), cx.nthreads());
+        const CloudArgs cld = io.cloud();
+        for (int idx = cx.tid(); idx < nlay * nband; idx += cx.nthreads()) {
+            const int j = idx % nlay, b = idx / nlay;
+            float tau = 0.f, s, g;
+            if (cld.present) {
+                const int l = top_at_1 ? j : nlay - 1 - j;
+                const size_t cl = icol + size_t(l) * ncol;
+                const CloudPoint<float> cp = cloud_point(cld.L, cld.lwp[cl], cld.iwp[cl], cld.rel[cl], cld.rei[cl]);
+                cloud_band<float, false>(cld.L, cp, b, tau, s, g);
+            }
+            sm_cld[b * nlay + j] = tau;
         }
-        sm_cld[b * nlay + j] = tau;
     }
-    T.sync();
+    cx.sync();
 
     const float D = 1.66f;                 // single-angle secant (Rte_lw.cpp:101-113)
     const int ngpt = k.ngpt;
     double acc_lev = 0.0, acc_div = 0.0, acc_bot_up = 0.0, acc_bot_dn = 0.0;
 
     for (int gg = 0; gg < k.ngroups; ++gg) {
+        const int nlay = io.nlay();
         const int g = 32 * gg + lane;
         const bool gv = g < ngpt;
         const int b0 = k.group_band0[gg];
@@ -122,7 +151,7 @@ __device__ __forceinline__ void lw_forward_column(const Team& T, const KdistView
 
         // 1. records of this warp's chunk
         for (int r = lane; r < CL * k.max_group_bands; r += 32) {
-            const int jj = w * CL + (r % CL);
+            const int jj = cx.warp() * CL + (r % CL);
             const int b = b0 + r / CL;
             if (jj < nlay && b < nband && k.band_lims[2 * b] < 32 * gg + 32)
                 build_lw_record(k, recs[r], st[jj], sm_cg + jj, nlay, b, sm_cld[b * nlay + jj], jj == nlay - 1, ts);
@@ -132,9 +161,10 @@ __device__ __forceinline__ void lw_forward_column(const Team& T, const KdistView
         // 2. pass 1
         float omt[CL], sdn[CL], sup[CL];
         float Ad = 1.f, Bd = 0.f;
+        const int j0 = cx.warp() * CL;
 #pragma unroll
         for (int i = 0; i < CL; ++i) {
-            const int j = w * CL + i;
+            const int j = j0 + i;
             omt[i] = 0.f; sdn[i] = 0.f; sup[i] = 0.f;
             if (j < nlay && gv) {
                 const Rec& R = recs[slot * CL + i];
@@ -157,17 +187,18 @@ __device__ __forceinline__ void lw_forward_column(const Team& T, const KdistView
             Au = (1.f - omt[i]) * Au;
             Bu = (1.f - omt[i]) * Bu + sup[i];
         }
-        sm_maps[w * 32 + lane] = make_float4(Ad, Bd, Au, Bu);
-        T.sync();
+        sm_maps[cx.warp() * 32 + lane] = make_float4(Ad, Bd, Au, Bu);
+        cx.sync();
 
         // 3. incoming radiances of the chunk (no incident longwave flux at the top)
+        const int w = cx.warp(), NW = cx.nwarps();
         float x = 0.f, xin = 0.f;
         for (int c = 0; c < NW; ++c) {
             if (c == w) xin = x;
             const float4 m = sm_maps[c * 32 + lane];
             x = m.x * x + m.y;
         }
-        const float emis = gv ? __ldg(sfc_emis + gband + size_t(icol) * nband) : 0.f;
+        const float emis = gv ? __ldg(io.emis() + gband + size_t(cx.icol()) * nband) : 0.f;
         const float S = x * (1.f - emis) + emis * sm_sfc[lane];
         float y = S;
         for (int c = NW - 1; c > w; --c) {
@@ -199,10 +230,15 @@ __device__ __forceinline__ void lw_forward_column(const Team& T, const KdistView
             acc_bot_up += double(warp_sum(S));
             acc_bot_dn += double(warp_sum(rd));
         }
-        T.sync();
+        cx.sync();
     }
 
     // Outputs.  Fluxes = 2 pi w * (sum of radiances) with w = 0.5.
+    const int w = cx.warp(), NW = cx.nwarps(), icol = cx.icol(), ncol = io.ncol(), nlay = io.nlay();
+    float* const flux_up = io.up();
+    float* const flux_dn = io.dn();
+    float* const flux_net = io.net();
+    float* const heating_rate = io.hr();
     const double pi = 3.14159265358979323846;
     constexpr int SH_LEV = (CL == 16) ? 0 : 1;   // lane L holds value L >> SH_LEV
     constexpr int SH_DIV = (CL == 16) ? 1 : 2;

@@ -30,39 +30,63 @@
 namespace rrtmgp_b200 {
 namespace fused {
 
-// One column (icol of a grid of ncol columns) by team T: T.nwarps() warps of CL layers each,
-// nlay <= T.nwarps() * CL (chunks past nlay are identity layers).
-template <int CL>
-__device__ __forceinline__ void sw_forward_column(const Team& T, const KdistView<float>& k,
-                                                  const GasSet<float>& gs,                                                   const SwCloudArgs& cld, int ncol, int nlay, int icol,
-                                                  const float* __restrict__ play, const float* __restrict__ plev,
-                                                  const float* __restrict__ tlay, const float* __restrict__ col_dry_in,
-                                                  const float* __restrict__ mu0_in,
-                                                  const float* __restrict__ tsi_scaling,
-                                                  const float* __restrict__ alb_dir, const float* __restrict__ alb_dif,
-                                                  float* __restrict__ flux_up, float* __restrict__ flux_dn,
-                                                  float* __restrict__ flux_dir, float* __restrict__ flux_net,
-                                                  float* __restrict__ heating_rate)
+// Arguments of the per-grid shortwave kernel (passed by value: kernel parameters).
+struct SwGridIo {
+    int ncol_, nlay_;
+    const float *play_, *plev_, *tlay_, *col_dry_, *mu0_, *tsi_, *alb_dir_, *alb_dif_;
+    float *up_, *dn_, *dir_, *net_, *hr_;
+    GasSet<float> gs_;
+    SwCloudArgs cld_;
+    __device__ __forceinline__ int ncol() const { return ncol_; }
+    __device__ __forceinline__ int nlay() const { return nlay_; }
+    __device__ __forceinline__ const float* play() const { return play_; }
+    __device__ __forceinline__ const float* plev() const { return plev_; }
+    __device__ __forceinline__ const float* tlay() const { return tlay_; }
+    __device__ __forceinline__ const float* col_dry() const { return col_dry_; }
+    __device__ __forceinline__ const float* mu0() const { return mu0_; }
+    __device__ __forceinline__ const float* tsi() const { return tsi_; }
+    __device__ __forceinline__ const float* alb_dir() const { return alb_dir_; }
+    __device__ __forceinline__ const float* alb_dif() const { return alb_dif_; }
+    __device__ __forceinline__ float* up() const { return up_; }
+    __device__ __forceinline__ float* dn() const { return dn_; }
+    __device__ __forceinline__ float* dir() const { return dir_; }
+    __device__ __forceinline__ float* net() const { return net_; }
+    __device__ __forceinline__ float* hr() const { return hr_; }
+    __device__ __forceinline__ const GasSet<float>& gs() const { return gs_; }
+    __device__ __forceinline__ const SwCloudArgs& cloud() const { return cld_; }
+};
+
+// One column by the warps that context cx names (cx.nwarps() warps of CL layers each,
+// nlay <= cx.nwarps() * CL; chunks past nlay are identity layers).  Context and arguments are
+// read through accessors at every use, as in lw_forward_column.
+template <int CL, class Cx, class Io>
+__device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<float>& k, const Io& io)
 {
     static_assert(CL == 8 || CL == 16, "chunk length");
-    unsigned char* const smem_raw = T.smem;
-    const int w = T.warp(), lane = T.tid & 31;
-    const int NW = T.nwarps();
+    const int lane = threadIdx.x & 31;
     const int nband = k.nband;
-    const SmemLayout SL = smem_layout(nlay, k.ngas, nband, 0, NW, 3, CL, k.max_group_bands);
+    const SmemLayout SL = smem_layout(io.nlay(), k.ngas, nband, 0, cx.nwarps(), 3, CL, k.max_group_bands);
+    unsigned char* const smem_raw = cx.smem();
     LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
     float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
-    float* sm_pt = reinterpret_cast<float*>(smem_raw + SL.maps);                  // [NW][32]
-    float4* sm_comp = reinterpret_cast<float4*>(smem_raw + SL.maps) + NW * 32;     // [NW][32]
-    float* sm_compd = reinterpret_cast<float*>(sm_comp + NW * 32);                // [NW][32]
-    Rec* recs = reinterpret_cast<Rec*>(smem_raw + SL.recs) + w * CL * k.max_group_bands;
+    float* sm_pt = reinterpret_cast<float*>(smem_raw + SL.maps);                            // [NW][32]
+    float4* sm_comp = reinterpret_cast<float4*>(smem_raw + SL.maps) + cx.nwarps() * 32;     // [NW][32]
+    float* sm_compd = reinterpret_cast<float*>(sm_comp + cx.nwarps() * 32);                 // [NW][32]
+    Rec* recs = reinterpret_cast<Rec*>(smem_raw + SL.recs) + cx.warp() * CL * k.max_group_bands;
 
-    const bool top_at_1 = play[icol] < play[icol + size_t(nlay - 1) * ncol];
-    const float mu0 = mu0_in[icol];
+    bool top_at_1;
+    float mu0, tsi;
+    {
+        const int icol = cx.icol(), ncol = io.ncol(), nlay = io.nlay();
+        const float* play = io.play();
+        top_at_1 = play[icol] < play[icol + size_t(nlay - 1) * ncol];
+        mu0 = io.mu0()[icol];
+        tsi = io.tsi() ? io.tsi()[icol] : 1.f;
+        setup_layers(k, io.gs(), ncol, nlay, icol, top_at_1, play, io.plev(), io.tlay(), nullptr, io.col_dry(), st,
+                     sm_cg, cx.tid(), cx.nthreads());
+    }
     const float mu0_inv = 1.f / mu0;
-    const float tsi = tsi_scaling ? tsi_scaling[icol] : 1.f;
-    setup_layers(k, gs, ncol, nlay, icol, top_at_1, play, plev, tlay, nullptr, col_dry_in, st, sm_cg, T.tid, T.nthreads);
-    T.sync();
+    cx.sync();
 
     const int ngpt = k.ngpt;
     constexpr int SH = (CL == 16) ? 0 : 1;          // lane L holds reduced value L >> SH
@@ -70,6 +94,7 @@ __device__ __forceinline__ void sw_forward_column(const Team& T, const KdistView
     double acc_sfc_dir = 0.0, acc_sfc_dn = 0.0, acc_sfc_up = 0.0;
 
     for (int gg = 0; gg < k.ngroups; ++gg) {
+        const int nlay = io.nlay();
         const int g = 32 * gg + lane;
         const bool gv = g < ngpt;
         const int b0 = k.group_band0[gg];
@@ -81,11 +106,12 @@ __device__ __forceinline__ void sw_forward_column(const Team& T, const KdistView
         const int nm1 = __reduce_max_sync(0xffffffffu, mg1.x);
 
         for (int r = lane; r < CL * k.max_group_bands; r += 32) {
-            const int jj = w * CL + (r % CL);
+            const int jj = cx.warp() * CL + (r % CL);
             const int b = b0 + r / CL;
             if (jj < nlay && b < nband && k.band_lims[2 * b] < 32 * gg + 32) {
                 const int l = top_at_1 ? jj : nlay - 1 - jj;
-                build_sw_record(k, recs[r], st[jj], sm_cg + jj, nlay, b, cld, icol + size_t(l) * ncol);
+                build_sw_record(k, recs[r], st[jj], sm_cg + jj, nlay, b, io.cloud(),
+                                cx.icol() + size_t(l) * io.ncol());
             }
         }
         __syncwarp();
@@ -94,9 +120,10 @@ __device__ __forceinline__ void sw_forward_column(const Team& T, const KdistView
         float vR[CL], vT[CL], vSu[CL], vSd[CL], vAd[CL], vP[CL], vAdir[CL];
         float P = 1.f;
         float cRu = 0.f, cRd = 0.f, cT = 1.f, cU = 0.f, cD = 0.f;
+        const int j0 = cx.warp() * CL;
 #pragma unroll
         for (int i = 0; i < CL; ++i) {
-            const int j = w * CL + i;
+            const int j = j0 + i;
             float R = 0.f, T = 1.f, Rdir = 0.f, Tdir = 0.f, Tn = 1.f, adif = 0.f, adir = 0.f;
             if (j < nlay && gv) {
                 const Rec& Rc = recs[slot * CL + i];
@@ -135,10 +162,11 @@ __device__ __forceinline__ void sw_forward_column(const Team& T, const KdistView
             cD = nD;
             P *= Tn;
         }
-        sm_pt[w * 32 + lane] = P;
-        T.sync();
+        sm_pt[cx.warp() * 32 + lane] = P;
+        cx.sync();
 
         // 2. direct flux at the chunk top and at the surface
+        const int w = cx.warp(), NW = cx.nwarps();
         const float toa = gv ? __ldg(k.solar_source + g) * tsi * mu0 : 0.f;
         float dtop = toa;
         for (int c = 0; c < w; ++c) dtop *= sm_pt[c * 32 + lane];
@@ -156,11 +184,11 @@ __device__ __forceinline__ void sw_forward_column(const Team& T, const KdistView
         }
         sm_comp[w * 32 + lane] = make_float4(cRu, cRd, cT, cU * dtop);
         sm_compd[w * 32 + lane] = cD * dtop;
-        T.sync();
+        cx.sync();
 
         // 3. albedo and source at this chunk's bottom; incident diffuse flux at its top
-        const float ad = gv ? __ldg(alb_dir + gband + size_t(icol) * nband) : 0.f;
-        const float af = gv ? __ldg(alb_dif + gband + size_t(icol) * nband) : 0.f;
+        const float ad = gv ? __ldg(io.alb_dir() + gband + size_t(cx.icol()) * nband) : 0.f;
+        const float af = gv ? __ldg(io.alb_dif() + gband + size_t(cx.icol()) * nband) : 0.f;
         float alb = af, src = dsfc * ad;
         float alb_in = af, src_in = src;
         float fa = 1.f, fb = 0.f;
@@ -231,6 +259,12 @@ __device__ __forceinline__ void sw_forward_column(const Team& T, const KdistView
     // Outputs.  Lane L holds value v = L >> SH of the reduced arrays: v < CL is level
     // w*CL + v (acc_a: direct, acc_b: up, acc_c: diffuse down), v >= CL is layer
     // w*CL + v - CL (acc_a + acc_b: absorbed flux).
+    const int w = cx.warp(), NW = cx.nwarps(), icol = cx.icol(), ncol = io.ncol(), nlay = io.nlay();
+    float* const flux_up = io.up();
+    float* const flux_dn = io.dn();
+    float* const flux_dir = io.dir();
+    float* const flux_net = io.net();
+    float* const heating_rate = io.hr();
     const int v = lane >> SH;
     if ((lane & ((1 << SH) - 1)) == 0) {
         if (v < CL) {

@@ -1,6 +1,7 @@
 """Batched forward of uneven grids in one persistent launch (rrtmgp_b200_batch_*).
 
-Parity: with the per-grid chunk rule (8 layers per warp up to 128 layers, else 16) the batched
+Parity: with the per-grid chunk rule (longwave 16 layers per warp; shortwave 8 up to 128
+layers, else 16) the batched
 results equal the per-grid fused launches to FP32 rounding (the same per-column code, compiled
 in another kernel, may contract multiply-adds differently: SAME_TOL), whatever the number of
 columns per CTA; the persistent launch and its graph replay agree bit for bit; every tile
@@ -46,10 +47,11 @@ def _atms(gpu, grids=GRIDS, seed=0):
 
 
 def _rule_plan(bf):
-    """The per-grid chunk rule with the most columns per CTA that fit."""
+    """The per-grid chunk rule (longwave 16; shortwave 8 up to 128 layers, else 16) with the most
+    columns per CTA that fit."""
     for d in bf.domains():
         for b in bf.bins():
-            cl = 8 if b <= 16 else 16
+            cl = 16 if d == 0 else (8 if b <= 16 else 16)
             w = -(-8 * b // cl)
             for p in range(min(16 // w, 15), 0, -1):
                 try:

@@ -387,7 +387,9 @@ int rrtmgp_b200_forward_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int
  * (ncol, nlay) field whatever its given shape; with col_dry == NULL the dry-air column's
  * dependence on h2o is included.  Forward optical properties are recomputed per group of
  * 32 g-points on chip, nothing is stored between forward and adjoint.  chunk: 8 or 16
- * layers per warp (0 = 8); the k-distribution's bands must hold 16 or more g-points each. */
+ * layers per warp (0 = 8); the k-distribution's bands must hold 16 or more g-points each.
+ * One CTA per column up to 128 layers (chunk 16: up to what its shared memory holds); deeper
+ * columns (chunk 8, nlay <= 512) run on a thread-block cluster of ceil(nlay / 128) CTAs. */
 int rrtmgp_b200_adjoint_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int ncol, int nlay,
         const float* play, const float* plev, const float* tlay, const float* tlev,
         const float* tsfc, const float* col_dry, const rrtmgp_b200_gas_conc* gases, int ngases,

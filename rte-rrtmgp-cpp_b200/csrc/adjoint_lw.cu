@@ -19,7 +19,11 @@
 //   Sdn_bar = I_bar(i+1) - h,  Sup_bar = U_bar(i) - h,  S_sfc_bar = emis U_bar(N)
 // then through the linear-in-tau sources (omt(x), fact(x), x = tau D), the Planck fraction
 // and band Planck functions, and the gas-optics interpolation (adjoint_common.cuh).
+#include <cooperative_groups.h>
+
 #include "adjoint_common.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace rrtmgp_b200 {
 namespace {
@@ -108,27 +112,39 @@ struct AdjLayout {
     size_t state, cg, cld, taubar, seeds, levbot, maps, sfc, recs, drecs, total;
 };
 
-__host__ __device__ __forceinline__ AdjLayout adj_layout(int nlay, int ngas, int nband, int NW, int CL, int mgb)
+// Shared memory of one CTA: LPC local layers (LPC + 1 local levels), maps of all NWt chunks of
+// the column, records of its NWc warps.
+__host__ __device__ __forceinline__ AdjLayout adj_layout(int LPC, int ngas, int nband, int NWc, int NWt, int CL,
+                                                         int mgb)
 {
     AdjLayout L;
     L.state = 0;
-    L.cg = align16(L.state + sizeof(LayerState) * size_t(nlay));
-    L.cld = align16(L.cg + sizeof(float) * size_t(ngas + 1) * nlay);
-    L.taubar = align16(L.cld + sizeof(float) * size_t(nband) * nlay);
-    L.seeds = align16(L.taubar + sizeof(float) * size_t(nband) * nlay);
-    L.levbot = align16(L.seeds + sizeof(float) * size_t(3 * nlay + 2));
+    L.cg = align16(L.state + sizeof(LayerState) * size_t(LPC));
+    L.cld = align16(L.cg + sizeof(float) * size_t(ngas + 1) * LPC);
+    L.taubar = align16(L.cld + sizeof(float) * size_t(nband) * LPC);
+    L.seeds = align16(L.taubar + sizeof(float) * size_t(nband) * LPC);
+    L.levbot = align16(L.seeds + sizeof(float) * size_t(3 * LPC + 2));
     L.maps = align16(L.levbot + sizeof(double) * 16);
-    L.sfc = align16(L.maps + sizeof(float4) * size_t(NW) * 32 * 2);
+    L.sfc = align16(L.maps + sizeof(float4) * size_t(NWt) * 32 * 2);
     L.recs = align16(L.sfc + sizeof(float) * 32);
-    L.drecs = align16(L.recs + sizeof(Rec) * size_t(NW) * CL * mgb);
-    L.total = align16(L.drecs + sizeof(DRec) * size_t(NW) * CL * mgb);
+    L.drecs = align16(L.recs + sizeof(Rec) * size_t(NWc) * CL * mgb);
+    L.total = align16(L.drecs + sizeof(DRec) * size_t(NWc) * CL * mgb);
     return L;
 }
 
+template <typename Tp>
+__device__ __forceinline__ Tp* remote(cg::cluster_group& cl, Tp* p, int rank)
+{
+    return cl.map_shared_rank(p, rank);
+}
+
+// One column per cluster of CS CTAs (CS = 1: a plain launch).  CTA r of the cluster owns the
+// layers [r LPC, (r + 1) LPC), LPC = NWc CL, as NWc warps of CL layers; chunk maps and the
+// surface source are pushed to every CTA of the cluster through distributed shared memory.
 template <int CL>
 __global__ void __launch_bounds__(512)
-lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjCloud cld, int ncol, int nlay, int idx_o3,
-                  int cd_internal, const float* __restrict__ play, const float* __restrict__ plev,
+lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjCloud cld, int ncol, int nlay, int CS,
+                  int idx_o3, int cd_internal, const float* __restrict__ play, const float* __restrict__ plev,
                   const float* __restrict__ tlay, const float* __restrict__ tlev, const float* __restrict__ tsfc,
                   const float* __restrict__ col_dry_in, const float* __restrict__ sfc_emis,
                   const float* __restrict__ seed_up, const float* __restrict__ seed_dn,
@@ -136,61 +152,83 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
 {
     static_assert(CL == 8 || CL == 16, "chunk length");
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int icol = blockIdx.x;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = CS > 1 ? int(cluster.block_rank()) : 0;
+    const int icol = blockIdx.x / CS;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int NW = blockDim.x >> 5;
+    const int NWc = blockDim.x >> 5;       // warps of this CTA
+    const int NWt = CS * NWc;               // chunks of the column
+    const int LPC = NWc * CL;               // layers per CTA
+    const int Wg = rank * NWc + w;          // this warp's chunk
+    const int j0 = rank * LPC;              // first layer of this CTA
     const int nband = k.nband, nlev = nlay + 1;
     const int mgb = k.max_group_bands;
-    const AdjLayout SL = adj_layout(nlay, k.ngas, nband, NW, CL, mgb);
+    const AdjLayout SL = adj_layout(LPC, k.ngas, nband, NWc, NWt, CL, mgb);
     LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
     float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
     float* sm_cld = reinterpret_cast<float*>(smem_raw + SL.cld);
     float* sm_tb = reinterpret_cast<float*>(smem_raw + SL.taubar);
-    float* sm_a = reinterpret_cast<float*>(smem_raw + SL.seeds);   // pi * seed_up per level (top down)
-    float* sm_b = sm_a + nlev;                                     // pi * seed_dn per level
-    float* sm_h = sm_b + nlev;                                     // h per layer
+    float* sm_a = reinterpret_cast<float*>(smem_raw + SL.seeds);   // pi * seed_up per local level
+    float* sm_b = sm_a + (LPC + 1);                                // pi * seed_dn per local level
+    float* sm_h = sm_b + (LPC + 1);                                // h per local layer
     double* sm_levbot = reinterpret_cast<double*>(smem_raw + SL.levbot);
-    float4* sm_mapA = reinterpret_cast<float4*>(smem_raw + SL.maps);   // (A, Bd, Bu, BUbar)
-    float* sm_mapB = reinterpret_cast<float*>(sm_mapA + NW * 32);      // BIbar
+    float4* sm_mapA = reinterpret_cast<float4*>(smem_raw + SL.maps);   // (A, Bd, Bu, BUbar) per chunk
+    float* sm_mapB = reinterpret_cast<float*>(sm_mapA + NWt * 32);     // BIbar per chunk
     float* sm_sfc = reinterpret_cast<float*>(smem_raw + SL.sfc);
     Rec* recs = reinterpret_cast<Rec*>(smem_raw + SL.recs) + w * CL * mgb;
     DRec* drecs = reinterpret_cast<DRec*>(smem_raw + SL.drecs) + w * CL * mgb;
+    auto at_rank = [&](auto* p, int rr) { return CS > 1 ? remote(cluster, p, rr) : p; };
+    auto csync = [&]() {
+        if (CS > 1)
+            cluster.sync();
+        else
+            __syncthreads();
+    };
 
     const double pi = 3.14159265358979323846;
     const bool top_at_1 = play[icol] < play[icol + size_t(nlay - 1) * ncol];
     const float ts = tsfc[icol];
-    setup_layers(k, gs, ncol, nlay, icol, top_at_1, play, plev, tlay, tlev, col_dry_in, st, sm_cg, threadIdx.x,
-                 blockDim.x);
-    for (int idx = threadIdx.x; idx < nlay * nband; idx += blockDim.x) {
-        const int j = idx % nlay, b = idx / nlay;
+    auto seed_at = [&](const float* sd, int lev) -> float {   // global level (top down) -> pi * seed
+        if (!sd || lev > nlay) return 0.f;
+        return float(pi) * sd[icol + size_t(top_at_1 ? lev : nlay - lev) * ncol];
+    };
+    setup_layer_range(k, gs, ncol, nlay, icol, top_at_1, play, plev, tlay, tlev, col_dry_in, st, sm_cg, LPC, j0, LPC,
+                      threadIdx.x, blockDim.x);
+    for (int idx = threadIdx.x; idx < LPC * nband; idx += blockDim.x) {
+        const int jl = idx % LPC, b = idx / LPC, j = j0 + jl;
         float tau = 0.f, s, g;
-        if (cld.present) {
+        if (cld.present && j < nlay) {
             const int l = top_at_1 ? j : nlay - 1 - j;
             const size_t cl = icol + size_t(l) * ncol;
             const CloudPoint<float> cp = cloud_point(cld.L, cld.lwp[cl], cld.iwp[cl], cld.rel[cl], cld.rei[cl]);
             cloud_band<float, false>(cld.L, cp, b, tau, s, g);
         }
-        sm_cld[b * nlay + j] = tau;
-        sm_tb[b * nlay + j] = 0.f;
+        sm_cld[b * LPC + jl] = tau;
+        sm_tb[b * LPC + jl] = 0.f;
     }
-    for (int l = threadIdx.x; l < nlev; l += blockDim.x) {
-        const int al = top_at_1 ? l : nlay - l;
-        sm_a[l] = seed_up ? float(pi) * seed_up[icol + size_t(al) * ncol] : 0.f;
-        sm_b[l] = seed_dn ? float(pi) * seed_dn[icol + size_t(al) * ncol] : 0.f;
+    for (int ll = threadIdx.x; ll <= LPC; ll += blockDim.x) {
+        sm_a[ll] = seed_at(seed_up, j0 + ll);
+        sm_b[ll] = seed_at(seed_dn, j0 + ll);
     }
     if (threadIdx.x < 16) sm_levbot[threadIdx.x] = 0.0;
     __syncthreads();
-    for (int j = threadIdx.x; j < nlay; j += blockDim.x) {
-        const int l = top_at_1 ? j : nlay - 1 - j;
-        const double g0_cp = 9.80665 / 1004.64;
-        sm_h[j] = seed_hr ? float(g0_cp * 86400.0 * pi * double(seed_hr[icol + size_t(l) * ncol]) / double(st[j].dp))
-                          : 0.f;
+    for (int jl = threadIdx.x; jl < LPC; jl += blockDim.x) {
+        const int j = j0 + jl;
+        float h = 0.f;
+        if (j < nlay && seed_hr) {
+            const int l = top_at_1 ? j : nlay - 1 - j;
+            const double g0_cp = 9.80665 / 1004.64;
+            h = float(g0_cp * 86400.0 * pi * double(seed_hr[icol + size_t(l) * ncol]) / double(st[jl].dp));
+        }
+        sm_h[jl] = h;
     }
     __syncthreads();
 
     const float D = 1.66f;
     const int ngpt = k.ngpt;
-    const int L_end = NW * CL;
+    const int L_end = NWt * CL;
+    const float a_top = seed_at(seed_up, 0);      // pi a_0: U_bar at the top level
+    const float b_bot = seed_at(seed_dn, nlay);   // pi b_N
     constexpr int QPR = 32 / CL;          // quantities per 32-value reduce-scatter
     constexpr int NRS = 4 / QPR;          // reduce-scatters per group for the 4 per-layer quantities
     double acc[NRS];
@@ -211,21 +249,22 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
         const float emis = gv ? __ldg(sfc_emis + gband + size_t(icol) * nband) : 0.f;
 
         for (int r = lane; r < CL * mgb; r += 32) {
-            const int jj = w * CL + (r % CL);
+            const int jl = w * CL + (r % CL);
+            const int jj = j0 + jl;
             const int b = b0 + r / CL;
             if (jj < nlay && b < nband && k.band_lims[2 * b] < 32 * gg + 32) {
                 Rec& R = recs[r];
                 DRec& DR = drecs[r];
-                const LayerState s = st[jj];
-                record_weights(k, R, s, sm_cg + jj, nlay, b);
+                const LayerState s = st[jl];
+                record_weights(k, R, s, sm_cg + jl, LPC, b);
                 const float* tp = k.totplnk + size_t(b) * k.nplanck;
                 const bool bottom = jj == nlay - 1;
                 R.aux = make_float4(interpolate1D(s.t, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp),
                                     interpolate1D(s.t_top, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp),
                                     interpolate1D(s.t_bot, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp),
-                                    sm_cld[b * nlay + jj]);
+                                    sm_cld[b * LPC + jl]);
                 R.aux2 = bottom ? interpolate1D(ts, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp) : 0.f;
-                build_drec(k, DR, s, sm_cg + jj, nlay, b, R.scal, idx_o3, cd_internal);
+                build_drec(k, DR, s, sm_cg + jl, LPC, b, R.scal, idx_o3, cd_internal);
                 DR.dB = make_float4(interpolate1D_slope(s.t, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp),
                                     interpolate1D_slope(s.t_top, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp),
                                     interpolate1D_slope(s.t_bot, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp),
@@ -241,7 +280,8 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
         float pf_bottom = 0.f;
 #pragma unroll
         for (int i = 0; i < CL; ++i) {
-            const int j = w * CL + i;
+            const int jl = w * CL + i;
+            const int j = j0 + jl;
             vtau[i] = 0.f; vpf[i] = 0.f; omt[i] = 0.f; sdn[i] = 0.f; sup[i] = 0.f;
             if (j < nlay && gv) {
                 const Rec& R = recs[slot * CL + i];
@@ -253,11 +293,11 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
                 vpf[i] = pfrac;
                 lw_layer_terms(tau, D, pfrac * R.aux.x, pfrac * R.aux.z, pfrac * R.aux.y, omt[i], sdn[i], sup[i]);
                 if (j == nlay - 1) {
-                    sm_sfc[lane] = pfrac * R.aux2;
+                    for (int rr = 0; rr < CS; ++rr) at_rank(sm_sfc, rr)[lane] = pfrac * R.aux2;
                     pf_bottom = pfrac;
                 }
             } else if (j == nlay - 1) {
-                sm_sfc[lane] = 0.f;
+                for (int rr = 0; rr < CS; ++rr) at_rank(sm_sfc, rr)[lane] = 0.f;
             }
             A = (1.f - omt[i]) * A;
             Bd = (1.f - omt[i]) * Bd + sdn[i];
@@ -269,27 +309,31 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
         float BU = 0.f;   // U_bar: top -> bottom of chunk
 #pragma unroll
         for (int i = 0; i < CL; ++i) {
-            const int j = w * CL + i;
-            const float a_next = (j + 1 < nlev) ? sm_a[j + 1] : 0.f;
-            const float hj = (j < nlay) ? sm_h[j] : 0.f;
+            const int jl = w * CL + i;
+            const int j = j0 + jl;
+            const float a_next = (j + 1 < nlev) ? sm_a[jl + 1] : 0.f;
+            const float hj = (j < nlay) ? sm_h[jl] : 0.f;
             BU = (1.f - omt[i]) * BU + a_next + hj * omt[i];
         }
         float BI = 0.f;   // I_bar: bottom -> top of chunk
 #pragma unroll
         for (int i = CL - 1; i >= 0; --i) {
-            const int j = w * CL + i;
-            const float b_here = (j < nlev) ? sm_b[j] : 0.f;
-            const float hj = (j < nlay) ? sm_h[j] : 0.f;
+            const int jl = w * CL + i;
+            const int j = j0 + jl;
+            const float b_here = (j < nlev) ? sm_b[jl] : 0.f;
+            const float hj = (j < nlay) ? sm_h[jl] : 0.f;
             BI = (1.f - omt[i]) * BI + b_here + hj * omt[i];
         }
-        sm_mapA[w * 32 + lane] = make_float4(A, Bd, Bu, BU);
-        sm_mapB[w * 32 + lane] = BI;
-        __syncthreads();
+        for (int rr = 0; rr < CS; ++rr) {
+            at_rank(sm_mapA, rr)[Wg * 32 + lane] = make_float4(A, Bd, Bu, BU);
+            at_rank(sm_mapB, rr)[Wg * 32 + lane] = BI;
+        }
+        csync();
 
         // ---- exchange ----
-        float x = 0.f, xin = 0.f, u = sm_a[0], uin = 0.f;
-        for (int c = 0; c < NW; ++c) {
-            if (c == w) { xin = x; uin = u; }
+        float x = 0.f, xin = 0.f, u = a_top, uin = 0.f;
+        for (int c = 0; c < NWt; ++c) {
+            if (c == Wg) { xin = x; uin = u; }
             const float4 m = sm_mapA[c * 32 + lane];
             x = m.x * x + m.y;
             u = m.x * u + m.w;
@@ -297,8 +341,8 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
         // x = I at L_end (= I_N), u = U_bar at L_end (= U_bar_N)
         const float Ssrc = sm_sfc[lane];
         float y = x * (1.f - emis) + emis * Ssrc;
-        float ib = (1.f - emis) * u + (L_end == nlay ? sm_b[nlay] : 0.f);
-        for (int c = NW - 1; c > w; --c) {
+        float ib = (1.f - emis) * u + (L_end == nlay ? b_bot : 0.f);
+        for (int c = NWt - 1; c > Wg; --c) {
             const float4 m = sm_mapA[c * 32 + lane];
             y = m.x * y + m.z;
             ib = m.x * ib + sm_mapB[c * 32 + lane];
@@ -320,9 +364,10 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
 #pragma unroll
             for (int i = 0; i < CL; ++i) {
                 vUb[i] = ub;
-                const int j = w * CL + i;
-                const float a_next = (j + 1 < nlev) ? sm_a[j + 1] : 0.f;
-                const float hj = (j < nlay) ? sm_h[j] : 0.f;
+                const int jl = w * CL + i;
+                const int j = j0 + jl;
+                const float a_next = (j + 1 < nlev) ? sm_a[jl + 1] : 0.f;
+                const float hj = (j < nlay) ? sm_h[jl] : 0.f;
                 ub = (1.f - omt[i]) * ub + a_next + hj * omt[i];
             }
         }
@@ -333,11 +378,12 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
         float gTs = 0.f;
 #pragma unroll
         for (int i = CL - 1; i >= 0; --i) {
-            const int j = w * CL + i;
-            const float hj = (j < nlay) ? sm_h[j] : 0.f;
+            const int jl = w * CL + i;
+            const int j = j0 + jl;
+            const float hj = (j < nlay) ? sm_h[jl] : 0.f;
             const float omtb = hj * (vI[i] + vU[i + 1]) - ib * vI[i] - vUb[i] * vU[i + 1];
             const float sdnb = ib - hj, supb = vUb[i] - hj;
-            const float b_here = (j < nlev) ? sm_b[j] : 0.f;
+            const float b_here = (j < nlev) ? sm_b[jl] : 0.f;
             ib = (1.f - omt[i]) * ib + b_here + hj * omt[i];
             gT[i] = 0.f; gH[i] = 0.f; gO[i] = 0.f; gS[i] = 0.f;
             if (j < nlay && gv) {
@@ -404,49 +450,58 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
             const int vi = lane >> SH;
             const int sl = vi / CL, jl = w * CL + (vi % CL);
             const int b = b0 + sl;
-            if ((lane & ((1 << SH) - 1)) == 0 && jl < nlay && b < nband && k.band_lims[2 * b] < 32 * gg + 32)
-                sm_tb[b * nlay + jl] += v[0];
+            if ((lane & ((1 << SH) - 1)) == 0 && j0 + jl < nlay && b < nband && k.band_lims[2 * b] < 32 * gg + 32)
+                sm_tb[b * LPC + jl] += v[0];
         }
         acc_levbot += double(warp_sum(gL[CL]));
-        if (w == (nlay - 1) / CL) acc_tsfc += double(warp_sum(gTs));
-        __syncthreads();
+        if (Wg == (nlay - 1) / CL) acc_tsfc += double(warp_sum(gTs));
+        csync();   // maps and the surface source are rewritten by the next group
     }
 
     // ---- outputs ----
     if (lane == 0) sm_levbot[w] = acc_levbot;
-    __syncthreads();
+    csync();
+    // level gradient of the bottom level of the previous chunk (another CTA's for w = 0)
+    double prev_levbot = 0.0;
+    if (w > 0)
+        prev_levbot = sm_levbot[w - 1];
+    else if (rank > 0)
+        prev_levbot = remote(cluster, sm_levbot, rank - 1)[NWc - 1];
 #pragma unroll
     for (int r = 0; r < NRS; ++r) {
         const int vi = lane;                         // RS<32>: lane L holds value L
         const int q = r * QPR + vi / CL;             // 0 T, 1 H, 2 O, 3 level
         const int jl = w * CL + (vi % CL);
+        const int j = j0 + jl;
         const double val = acc[r];
         if (q < 3) {
-            if (jl < nlay) {
-                const size_t o = icol + size_t(top_at_1 ? jl : nlay - 1 - jl) * ncol;
+            if (j < nlay) {
+                const size_t o = icol + size_t(top_at_1 ? j : nlay - 1 - j) * ncol;
                 float* dst = q == 0 ? out.tlay : (q == 1 ? out.h2o : out.o3);
                 if (dst) dst[o] = float(val);
             }
-        } else if (jl <= nlay && out.tlev) {
+        } else if (j <= nlay && out.tlev) {
             double v = val;
-            if ((vi % CL) == 0 && w > 0) v += sm_levbot[w - 1];
-            out.tlev[icol + size_t(top_at_1 ? jl : nlay - jl) * ncol] = float(v);
+            if ((vi % CL) == 0 && Wg > 0) v += prev_levbot;
+            out.tlev[icol + size_t(top_at_1 ? j : nlay - j) * ncol] = float(v);
         }
     }
-    if (w == NW - 1 && lane == 0) {
+    if (Wg == NWt - 1 && lane == 0) {
         if (L_end == nlay && out.tlev)
-            out.tlev[icol + size_t(top_at_1 ? nlay : 0) * ncol] = float(sm_levbot[NW - 1]);
+            out.tlev[icol + size_t(top_at_1 ? nlay : 0) * ncol] = float(sm_levbot[w]);
     }
-    if (w == (nlay - 1) / CL && lane == 0 && out.tsfc) out.tsfc[icol] = float(acc_tsfc);
+    if (Wg == (nlay - 1) / CL && lane == 0 && out.tsfc) out.tsfc[icol] = float(acc_tsfc);
     // cloud gradients: sum over bands of tau_bar(band) * dtau_cloud(band)/dx
-    for (int j = threadIdx.x; j < nlay; j += blockDim.x) {
+    for (int jl = threadIdx.x; jl < LPC; jl += blockDim.x) {
+        const int j = j0 + jl;
+        if (j >= nlay) break;
         const int l = top_at_1 ? j : nlay - 1 - j;
         const size_t cl = icol + size_t(l) * ncol;
         float4 gsum = make_float4(0.f, 0.f, 0.f, 0.f);
         if (cld.present) {
             const float lw = cld.lwp[cl], iw = cld.iwp[cl], rl = cld.rel[cl], ri = cld.rei[cl];
             for (int b = 0; b < nband; ++b) {
-                const float tb = sm_tb[b * nlay + j];
+                const float tb = sm_tb[b * LPC + jl];
                 const float4 d = cloud_1scl_partials(cld.L, lw, iw, rl, ri, b);
                 gsum.x += tb * d.x;
                 gsum.y += tb * d.y;
@@ -459,8 +514,11 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
         if (out.rel) out.rel[cl] = gsum.z;
         if (out.rei) out.rei[cl] = gsum.w;
     }
+    if (CS > 1) cluster.sync();   // no CTA leaves while its shared memory may still be read remotely
 }
 
+// Up to 128 layers (CL = 8) or 256 (CL = 16, if the records fit) one CTA of ceil(nlay / CL)
+// warps per column; beyond, clusters of CS = ceil(nlay / 128) CTAs of 16 warps (CL = 8).
 template <int CL>
 int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay, int idx_o3, const float* play,
                       const float* plev, const float* tlay, const float* tlev, const float* tsfc, const float* col_dry,
@@ -469,9 +527,17 @@ int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
                       cudaStream_t stream)
 {
     const KdistView<float>& v = k->v32;
-    const int NW = (nlay + CL - 1) / CL;
-    RB_CHECK_ARG(NW <= 16, "adjoint_lw: nlay too large for the fused kernel (at most 16 chunks)");
-    const size_t smem = adj_layout(nlay, v.ngas, v.nband, NW, CL, v.max_group_bands).total;
+    const int NW1 = (nlay + CL - 1) / CL;
+    const size_t smem1 = adj_layout(NW1 * CL, v.ngas, v.nband, NW1, NW1, CL, v.max_group_bands).total;
+    int CS = 1, NWc = NW1;
+    size_t smem = smem1;
+    if (NW1 > 16 || smem1 > 227 * 1024) {
+        RB_CHECK_ARG(CL == 8, "adjoint_lw: columns deeper than one CTA holds need chunk 8");
+        NWc = 16;
+        CS = (nlay + 16 * CL - 1) / (16 * CL);
+        RB_CHECK_ARG(CS <= 8, "adjoint_lw: at most 1024 layers");
+        smem = adj_layout(16 * CL, v.ngas, v.nband, 16, CS * 16, CL, v.max_group_bands).total;
+    }
     if (smem > 227 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_lw: shared memory need exceeds 227 KB");
     static bool attr = false;
     if (!attr) {
@@ -486,9 +552,28 @@ int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
         ca.lwp = lwp; ca.iwp = iwp; ca.rel = rel; ca.rei = rei;
         ca.present = 1;
     }
-    lw_adjoint_kernel<CL><<<ncol, NW * 32, smem, stream>>>(v, gs, ca, ncol, nlay, idx_o3, col_dry ? 0 : 1, play, plev,
-                                                             tlay, tlev, tsfc, col_dry, emis, su, sd, sh, out);
-    RB_LAUNCH("lw_adjoint_kernel");
+    if (CS == 1) {
+        lw_adjoint_kernel<CL><<<ncol, NWc * 32, smem, stream>>>(v, gs, ca, ncol, nlay, 1, idx_o3, col_dry ? 0 : 1,
+                                                                  play, plev, tlay, tlev, tsfc, col_dry, emis, su, sd,
+                                                                  sh, out);
+        RB_LAUNCH("lw_adjoint_kernel");
+        return RRTMGP_B200_OK;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(ncol) * CS);
+    cfg.blockDim = dim3(NWc * 32);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = unsigned(CS);
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    RB_CUDA(cudaLaunchKernelEx(&cfg, lw_adjoint_kernel<CL>, v, gs, ca, ncol, nlay, CS, idx_o3, col_dry ? 0 : 1, play,
+                               plev, tlay, tlev, tsfc, col_dry, emis, su, sd, sh, out),
+            "lw_adjoint_kernel launch");
     return RRTMGP_B200_OK;
 }
 

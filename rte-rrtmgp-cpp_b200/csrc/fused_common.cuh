@@ -168,19 +168,23 @@ struct CtaCtx {
     __device__ __forceinline__ void sync() const { __syncthreads(); }
 };
 
-// Fill the per-layer state of column icol (layers counted from the top) and col_gas; threads
+// Fill the per-layer state and col_gas of layers j0 .. j0 + nloc - 1 (counted from the top,
+// those below nlay) of column icol into st[j - j0] and cg[(gas) * cg_stride + j - j0]; threads
 // tid, tid + nthr, ... of the calling team take one layer each.
-__device__ __forceinline__ void setup_layers(const KdistView<float>& k, const GasSet<float>& gs, int ncol,
-                                             int nlay, int icol, bool top_at_1, const float* __restrict__ play,
-                                             const float* __restrict__ plev, const float* __restrict__ tlay,
-                                             const float* __restrict__ tlev, const float* __restrict__ col_dry,
-                                             LayerState* st, float* cg, int tid, int nthr)
+__device__ __forceinline__ void setup_layer_range(const KdistView<float>& k, const GasSet<float>& gs, int ncol,
+                                                  int nlay, int icol, bool top_at_1, const float* __restrict__ play,
+                                                  const float* __restrict__ plev, const float* __restrict__ tlay,
+                                                  const float* __restrict__ tlev, const float* __restrict__ col_dry,
+                                                  LayerState* st, float* cg, int cg_stride, int j0, int nloc,
+                                                  int tid, int nthr)
 {
-    for (int j = tid; j < nlay; j += nthr) {
+    for (int jl = tid; jl < nloc; jl += nthr) {
+        const int j = j0 + jl;
+        if (j >= nlay) break;
         const int l = top_at_1 ? j : nlay - 1 - j;
         const size_t cl = icol + size_t(l) * ncol;
         const float p = play[cl], t = tlay[cl];
-        fill_col_gas(k, gs, ncol, nlay, icol, l, plev, col_dry, cg + j, nlay);
+        fill_col_gas(k, gs, ncol, nlay, icol, l, plev, col_dry, cg + jl, cg_stride);
         const LayerInterp<float> li = layer_interp(k, p, t);
         const int lt = top_at_1 ? j : nlay - j, lb = top_at_1 ? j + 1 : nlay - 1 - j;
         LayerState s;
@@ -196,8 +200,19 @@ __device__ __forceinline__ void setup_layers(const KdistView<float>& k, const Ga
         s.t_bot = tlev ? tlev[icol + size_t(lb) * ncol] : 0.f;
         s.dp = fabsf(plev[icol + size_t(lb) * ncol] - plev[icol + size_t(lt) * ncol]);
         s.pad2 = 0.f;
-        st[j] = s;
+        st[jl] = s;
     }
+}
+
+// The whole column (layers 0 .. nlay - 1, cg stride nlay).
+__device__ __forceinline__ void setup_layers(const KdistView<float>& k, const GasSet<float>& gs, int ncol,
+                                             int nlay, int icol, bool top_at_1, const float* __restrict__ play,
+                                             const float* __restrict__ plev, const float* __restrict__ tlay,
+                                             const float* __restrict__ tlev, const float* __restrict__ col_dry,
+                                             LayerState* st, float* cg, int tid, int nthr)
+{
+    setup_layer_range(k, gs, ncol, nlay, icol, top_at_1, play, plev, tlay, tlev, col_dry, st, cg, nlay, 0, nlay, tid,
+                      nthr);
 }
 
 // Shared-memory offsets (bytes) of the fused kernels, all 16-byte aligned.

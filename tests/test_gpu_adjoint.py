@@ -121,6 +121,29 @@ def test_lw_adjoint_matches_fd(oracle_mod, tables, gpu, top_at_1, chunk):
         _check("d/drei", got["rei"], _fd(fwd, atm, seeds, "rei"), cloudy_i)
 
 
+def test_lw_adjoint_deep_column_cluster(oracle_mod, tables, gpu):
+    """200 layers: a cluster of two CTAs per column (128 + 72 layers), bottom-up orientation;
+    FD on the rows around the CTA boundary (layers 127/128, levels 127-129) and at both ends."""
+    rng = np.random.default_rng(5)
+    ncol, nlay = 2, 200
+    atm, fwd = _lw_setup(tables, oracle_mod, ncol, nlay, seed=25, clouds=True, top_at_1=False)
+    seeds = _seeds(nlay, ncol, rng)
+    got = _gpu_grads(tables, atm, seeds, True, 8)
+    # rows in the reference's order (top_at_1 False: row l holds layer nlay - 1 - l from the top)
+    lay_rows = sorted({0, 1, nlay - 1 - 127, nlay - 1 - 128, nlay - 2, nlay - 1})
+    lev_rows = sorted({0, nlay - 127, nlay - 128, nlay - 129, nlay})
+    for key, rows in (("tlay", lay_rows), ("h2o", lay_rows), ("o3", lay_rows), ("tlev", lev_rows),
+                      ("tsfc", None)):
+        ref = _fd(fwd, atm, seeds, key, rows)
+        if rows is None:
+            _check(f"d/d{key}", got[key], ref)
+            continue
+        mask = np.zeros_like(ref, dtype=bool)
+        mask[rows] = True
+        mask &= _informative(_get(atm, key))
+        _check(f"d/d{key} rows {rows}", got[key], ref, mask)
+
+
 def test_lw_adjoint_heating_rate_only_clear(oracle_mod, tables, gpu):
     """Seed on heating rates only (the ~0.1 Pa top layers dominate), clear sky, 60 layers."""
     rng = np.random.default_rng(4)

@@ -52,6 +52,10 @@ def parse():
     ap.add_argument("--batched-grids", type=int, default=512,
                     help="uneven-grid batch: grids with ncol U{64..4096}, nlay U{40..200} (0: skip)")
     ap.add_argument("--batched-steps", type=int, default=3)
+    ap.add_argument("--deep-ncol", type=int, default=262144,
+                    help="deep-column forward + adjoint: ncol (0: skip)")
+    ap.add_argument("--deep-nlay", type=int, default=256)
+    ap.add_argument("--deep-steps", type=int, default=2)
     return ap.parse_args()
 
 
@@ -324,6 +328,112 @@ def batched_bench(args, solver, dev, stream, flush, rank, world, dist):
            "max_diff_vs_per_grid": {"flux_w_m2": dflux, "heating_rate_k_day": dhr}}
     bf.close()
     del atms, outs
+    return out
+
+
+def deep_bench(args, solver, fused, dev, stream, flush, rank, world, dist):
+    """Deep columns: args.deep_ncol all-sky columns of args.deep_nlay layers, FP32 forward +
+    adjoint (LW and SW, every output seeded) per step, against the plain FP64 GPU forward of
+    this build run in blocks of 8192 columns (its g-point arrays of the whole grid would not fit)."""
+    import torch
+    from rrtmgp_b200 import shard
+    from rrtmgp_b200 import synthetic as S
+    from rrtmgp_b200.autodiff import adjoint_lw, adjoint_sw
+    from rrtmgp_b200.solver import atm_to_device
+
+    ncol, nlay = args.deep_ncol, args.deep_nlay
+    blk = 16384
+    atm = None
+    for c0 in range(0, ncol, blk):
+        nb = min(blk, ncol - c0)
+        part = atm_to_device(S.make_atmosphere(nb, nlay, seed=shard.rank_seed(args.seed + 5, rank) + c0, clouds=True),
+                             torch.float32, dev)
+        if atm is None:
+            atm = {k: (torch.empty(v.shape[:-1] + (ncol,), dtype=v.dtype, device=dev) if v.dim() and
+                       v.shape[-1] == nb and k not in ("emis_sfc", "sfc_alb_dir", "sfc_alb_dif")
+                       else None) for k, v in part.items() if k != "gases"}
+            for k in ("emis_sfc", "sfc_alb_dir", "sfc_alb_dif"):
+                atm[k] = torch.empty((ncol,) + part[k].shape[1:], dtype=torch.float32, device=dev)
+            atm["gases"] = {k: (torch.empty(v.shape[:-1] + (ncol,), dtype=v.dtype, device=dev) if v.numel() > 1
+                                else v.clone()) for k, v in part["gases"].items()}
+        for k, v in part.items():
+            if k == "gases":
+                for g, t in v.items():
+                    if t.numel() > 1:
+                        atm["gases"][g][..., c0:c0 + nb].copy_(t)
+            elif k in ("emis_sfc", "sfc_alb_dir", "sfc_alb_dif"):
+                atm[k][c0:c0 + nb].copy_(v)
+            elif atm.get(k) is not None:
+                atm[k][..., c0:c0 + nb].copy_(v)
+        del part
+    nlev = nlay + 1
+    gen = torch.Generator(device=dev).manual_seed(args.seed)
+    sd = {k: torch.randn(shape, generator=gen, device=dev) for k, shape in
+          (("up", (nlev, ncol)), ("dn", (nlev, ncol)), ("dir", (nlev, ncol)), ("hr", (nlay, ncol)))}
+
+    def run(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        fused.solve_lw(atm)
+        if ev is not None:
+            ev[1].record(stream)
+        adjoint_lw(fused, atm, sd["up"], sd["dn"], sd["hr"])
+        if ev is not None:
+            ev[2].record(stream)
+        fused.solve_sw(atm)
+        if ev is not None:
+            ev[3].record(stream)
+        adjoint_sw(fused, atm, sd["up"], sd["dn"], sd["dir"], sd["hr"])
+        if ev is not None:
+            ev[4].record(stream)
+
+    run()
+    torch.cuda.synchronize()
+    evs = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(5)) for _ in range(args.deep_steps)]
+    for e in evs:
+        flush.zero_()
+        run(e)
+    torch.cuda.synchronize()
+    parts = [float(np.mean([e[q].elapsed_time(e[q + 1]) for e in evs])) for q in range(4)]
+    tot = shard.max_over_ranks(float(np.sum(parts)), dist if world > 1 else None, dev)
+    # FP64 forward of this build on one 8192-column block of the same atmosphere
+    nb = min(8192, ncol)
+    sub = {k: (v[..., :nb] if k not in ("emis_sfc", "sfc_alb_dir", "sfc_alb_dif") else v[:nb])
+           for k, v in atm.items() if k != "gases" and v is not None}
+    sub = {k: v.double().contiguous() for k, v in sub.items()}
+    sub["gases"] = {k: (v[..., :nb] if v.numel() > 1 else v).double().contiguous() for k, v in atm["gases"].items()}
+    solver.solve_lw(sub)
+    solver.solve_sw(sub)
+    torch.cuda.synchronize()
+    e64 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(2)]
+    for a, b in e64:
+        flush.zero_()
+        a.record(stream)
+        solver.solve_lw(sub)
+        solver.solve_sw(sub)
+        b.record(stream)
+    torch.cuda.synchronize()
+    ms64 = float(np.mean([a.elapsed_time(b) for a, b in e64]))
+    r_lw, r_sw = solver.solve_lw(sub), solver.solve_sw(sub)
+    f_lw, f_sw = fused.solve_lw(atm), fused.solve_sw(atm)
+    ferr = max(float((f[k][:, :nb].double() - r[k]).abs().max()) for f, r in ((f_lw, r_lw), (f_sw, r_sw))
+               for k in ("flux_up", "flux_dn", "flux_net"))
+    herr = max(float((f["heating_rate"][:, :nb].double() - r["heating_rate"]).abs().max())
+               for f, r in ((f_lw, r_lw), (f_sw, r_sw)))
+    solver._bufs = {k: v for k, v in solver._bufs.items() if k[0][2] != torch.float64}
+    fwd_adj = ncol * world / (tot * 1e-3)
+    fp64 = nb / (ms64 * 1e-3)
+    out = {"workload": f"all-sky LW+SW forward + adjoint, ncol={ncol} per GPU, nlay={nlay}",
+           "forward_adjoint": {"value": fwd_adj, "unit": "columns/s", "ms_per_step": tot, "steps": args.deep_steps,
+                               "kernel_ms": {"lw_forward_kernel": round(parts[0], 3),
+                                             "lw_adjoint_kernel": round(parts[1], 3),
+                                             "sw_forward_kernel": round(parts[2], 3),
+                                             "sw_adjoint_kernel": round(parts[3], 3)}},
+           "fp64_forward_blocked": {"value": fp64, "unit": "columns/s", "block_ncol": nb, "ms_per_block": ms64},
+           "ratio_fwd_adj_over_fp64": fwd_adj / (fp64 * world),
+           "fp32_max_flux_err_w_m2": ferr, "fp32_max_heating_rate_err_k_day": herr}
+    del atm, sd, sub
+    torch.cuda.empty_cache()
     return out
 
 
@@ -604,6 +714,10 @@ def main():
         del atm64
         solver._bufs = {k: v for k, v in solver._bufs.items() if k[0][2] != torch.float64}
 
+    deep = None
+    if args.path == "fused" and args.deep_ncol > 0 and not args.no_adjoint:
+        deep = deep_bench(args, solver, fused, dev, stream, flush, rank, world, dist)
+
     batched = None
     if args.path == "fused" and args.batched_grids > 0:
         batched = batched_bench(args, solver, dev, stream, flush, rank, world, dist)
@@ -633,6 +747,7 @@ def main():
             "fp64_forward": fp64,
             "forward_adjoint": fwd_adj,
             "batched": batched,
+            "deep_forward_adjoint": deep,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

@@ -138,10 +138,11 @@ __device__ __forceinline__ Tp* remote(cg::cluster_group& cl, Tp* p, int rank)
     return cl.map_shared_rank(p, rank);
 }
 
-// One column per cluster of CS CTAs (CS = 1: a plain launch).  CTA r of the cluster owns the
-// layers [r LPC, (r + 1) LPC), LPC = NWc CL, as NWc warps of CL layers; chunk maps and the
-// surface source are pushed to every CTA of the cluster through distributed shared memory.
-template <int CL>
+// One column per cluster of CS CTAs (CLUSTER = false: CS = 1, a plain launch compiled without
+// the cluster code).  CTA r of the cluster owns the layers [r LPC, (r + 1) LPC), LPC = NWc CL,
+// as NWc warps of CL layers; chunk maps and the surface source are pushed to every CTA of the
+// cluster through distributed shared memory.
+template <int CL, bool CLUSTER>
 __global__ void __launch_bounds__(512)
 lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjCloud cld, int ncol, int nlay, int CS,
                   int idx_o3, int cd_internal, const float* __restrict__ play, const float* __restrict__ plev,
@@ -153,7 +154,8 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
     static_assert(CL == 8 || CL == 16, "chunk length");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cg::cluster_group cluster = cg::this_cluster();
-    const int rank = CS > 1 ? int(cluster.block_rank()) : 0;
+    if (!CLUSTER) CS = 1;
+    const int rank = CLUSTER ? int(cluster.block_rank()) : 0;
     const int icol = blockIdx.x / CS;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int NWc = blockDim.x >> 5;       // warps of this CTA
@@ -177,9 +179,9 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
     float* sm_sfc = reinterpret_cast<float*>(smem_raw + SL.sfc);
     Rec* recs = reinterpret_cast<Rec*>(smem_raw + SL.recs) + w * CL * mgb;
     DRec* drecs = reinterpret_cast<DRec*>(smem_raw + SL.drecs) + w * CL * mgb;
-    auto at_rank = [&](auto* p, int rr) { return CS > 1 ? remote(cluster, p, rr) : p; };
+    auto at_rank = [&](auto* p, int rr) { return CLUSTER ? remote(cluster, p, rr) : p; };
     auto csync = [&]() {
-        if (CS > 1)
+        if (CLUSTER)
             cluster.sync();
         else
             __syncthreads();
@@ -465,7 +467,7 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
     double prev_levbot = 0.0;
     if (w > 0)
         prev_levbot = sm_levbot[w - 1];
-    else if (rank > 0)
+    else if (CLUSTER && rank > 0)
         prev_levbot = remote(cluster, sm_levbot, rank - 1)[NWc - 1];
 #pragma unroll
     for (int r = 0; r < NRS; ++r) {
@@ -514,7 +516,7 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
         if (out.rel) out.rel[cl] = gsum.z;
         if (out.rei) out.rei[cl] = gsum.w;
     }
-    if (CS > 1) cluster.sync();   // no CTA leaves while its shared memory may still be read remotely
+    if (CLUSTER) cluster.sync();   // no CTA leaves while its shared memory may still be read remotely
 }
 
 // Up to 128 layers (CL = 8) or 256 (CL = 16, if the records fit) one CTA of ceil(nlay / CL)
@@ -541,8 +543,10 @@ int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
     if (smem > 227 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_lw: shared memory need exceeds 227 KB");
     static bool attr = false;
     if (!attr) {
-        RB_CUDA(cudaFuncSetAttribute(lw_adjoint_kernel<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
-                "adjoint_lw attribute");
+        RB_CUDA(cudaFuncSetAttribute(lw_adjoint_kernel<CL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     227 * 1024), "adjoint_lw attribute");
+        RB_CUDA(cudaFuncSetAttribute(lw_adjoint_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     227 * 1024), "adjoint_lw attribute");
         attr = true;
     }
     AdjCloud ca{};
@@ -553,7 +557,7 @@ int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
         ca.present = 1;
     }
     if (CS == 1) {
-        lw_adjoint_kernel<CL><<<ncol, NWc * 32, smem, stream>>>(v, gs, ca, ncol, nlay, 1, idx_o3, col_dry ? 0 : 1,
+        lw_adjoint_kernel<CL, false><<<ncol, NWc * 32, smem, stream>>>(v, gs, ca, ncol, nlay, 1, idx_o3, col_dry ? 0 : 1,
                                                                   play, plev, tlay, tlev, tsfc, col_dry, emis, su, sd,
                                                                   sh, out);
         RB_LAUNCH("lw_adjoint_kernel");
@@ -571,7 +575,7 @@ int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    RB_CUDA(cudaLaunchKernelEx(&cfg, lw_adjoint_kernel<CL>, v, gs, ca, ncol, nlay, CS, idx_o3, col_dry ? 0 : 1, play,
+    RB_CUDA(cudaLaunchKernelEx(&cfg, lw_adjoint_kernel<8, true>, v, gs, ca, ncol, nlay, CS, idx_o3, col_dry ? 0 : 1, play,
                                plev, tlay, tlev, tsfc, col_dry, emis, su, sd, sh, out),
             "lw_adjoint_kernel launch");
     return RRTMGP_B200_OK;

@@ -193,6 +193,94 @@ __device__ __noinline__ LocalAdj sw_local_adjoint(float tau, float w0, float omw
     return r;
 }
 
+
+// Gas-optics adjoint of one (layer, g-point): the absorption tau_bar through the major and
+// minor interpolation (tau_abs_adjoint of adjoint_common.cuh) and the Rayleigh tau_bar
+// through col_rayl * (fm . krayl corners).  Out of line, like the two-stream below: the
+// per-layer loops are unrolled 8 times and, inlined, these bodies made the kernel's code
+// outgrow the instruction cache (10% of the kernel time).
+struct GasGrad { float t, h, o; };
+
+__device__ __noinline__ GasGrad sw_gas_adjoint(const float4* __restrict__ kmaj4, const float2* __restrict__ kmin,
+                                               const float2* __restrict__ krayl2, const Rec* Rc, const DRec* DR,
+                                               int g, int4 mg, int nmax, float tab, float trb)
+{
+    const float4 c0 = __ldg(kmaj4 + (Rc->kb.x + g));
+    const float4 c1 = __ldg(kmaj4 + (Rc->kb.y + g));
+    float dT = dot4(DR->wT0, c0) + dot4(DR->wT1, c1);
+    float dH = dot4(DR->wH0, c0) + dot4(DR->wH1, c1);
+    float dO = dot4(DR->wO0, c0) + dot4(DR->wO1, c1);
+#pragma unroll
+    for (int n = 0; n < 3; ++n) {
+        if (n < nmax) {
+            const int code = n == 0 ? mg.y : (n == 1 ? mg.z : mg.w);
+            const int c = code >> 4, sl = code & 15;
+            const float2 lo = __ldg(kmin + (Rc->kb.z + c));
+            const float2 hi = __ldg(kmin + (Rc->kb.w + c));
+            const float4 cr = make_float4(lo.x, lo.y, hi.x, hi.y);
+            const float M = dot4(Rc->fm, cr);
+            const float sc = Rc->scal[sl];
+            const float tT = DR->dsT[sl] * M + sc * dot4(DR->fmT, cr);
+            const float tH = DR->dsH[sl] * M + sc * dot4(DR->fmH, cr);
+            const float tO = DR->dsO[sl] * M + sc * dot4(DR->fmO, cr);
+            const bool on = n < mg.x;
+            dT += on ? tT : 0.f;
+            dH += on ? tH : 0.f;
+            dO += on ? tO : 0.f;
+        }
+    }
+    GasGrad r{tab * dT, tab * dH, tab * dO};
+    const float2 r0 = __ldg(krayl2 + (Rc->kr[0] + g));
+    const float2 r1 = __ldg(krayl2 + (Rc->kr[1] + g));
+    const float4 kr = make_float4(r0.x, r0.y, r1.x, r1.y);
+    const float colr = Rc->aux.x;
+    r.t += trb * colr * dot4(DR->fmT, kr);
+    r.h += trb * (colr * dot4(DR->fmH, kr) + DR->dB.x * dot4(Rc->fm, kr));
+    r.o += trb * colr * dot4(DR->fmO, kr);
+    return r;
+}
+
+
+// Forward optical properties and two-stream coefficients of one (layer, g-point), as the
+// forward kernel's pass 1 (sw_column.cuh), out of line for the same reason.
+struct LayerFwd { float tau, w0, omw, gasy, R, T, Rdir, Tdir, Tn, adif, adir; };
+
+__device__ __noinline__ LayerFwd sw_layer_forward(const float4* __restrict__ kmaj4, const float2* __restrict__ kmin,
+                                                  const float2* __restrict__ krayl2, const Rec* Rc, int g, int4 mg,
+                                                  int nmax, float mu0, float mu0_inv)
+{
+    const float4 c0 = __ldg(kmaj4 + (Rc->kb.x + g));
+    const float4 c1 = __ldg(kmaj4 + (Rc->kb.y + g));
+    float ta = dot4(Rc->wmaj0, c0) + dot4(Rc->wmaj1, c1);
+#pragma unroll
+    for (int n = 0; n < 3; ++n) {
+        if (n < nmax) {
+            const int code = n == 0 ? mg.y : (n == 1 ? mg.z : mg.w);
+            const int c = code >> 4;
+            const float2 lo = __ldg(kmin + (Rc->kb.z + c));
+            const float2 hi = __ldg(kmin + (Rc->kb.w + c));
+            const float t = Rc->scal[code & 15] * (Rc->fm.x * lo.x + Rc->fm.y * lo.y + Rc->fm.z * hi.x + Rc->fm.w * hi.y);
+            ta += (n < mg.x) ? t : 0.f;
+        }
+    }
+    LayerFwd o;
+    const float2 r0 = __ldg(krayl2 + (Rc->kr[0] + g));
+    const float2 r1 = __ldg(krayl2 + (Rc->kr[1] + g));
+    const float tr = (Rc->fm.x * r0.x + Rc->fm.y * r0.y + Rc->fm.z * r1.x + Rc->fm.w * r1.y) * Rc->aux.x;
+    o.tau = ta + tr + Rc->aux.y;
+    const float ts = tr + Rc->aux.z;
+    o.w0 = 0.f;
+    o.omw = 1.f;
+    if (o.tau > 2.f * FLT_MIN) {
+        const float inv = __fdividef(1.f, o.tau);
+        o.w0 = ts * inv;
+        o.omw = (ta + Rc->aux2) * inv;
+    }
+    o.gasy = __fdividef(Rc->aux.w, fmaxf(ts, 3.f * FLT_MIN));
+    sw_layer_fast(o.tau, o.w0, o.omw, o.gasy, mu0, mu0_inv, o.R, o.T, o.Rdir, o.Tdir, o.Tn, o.adif, o.adir);
+    return o;
+}
+
 // Cloud optics of band b (2str, optionally delta-scaled) as duals over (lwp, iwp, rel, rei):
 // returns tau', tau' ssa', tau' ssa' g' as used by the SW record.
 __device__ __forceinline__ void cloud_sw_dual(const CloudLut<float>& L, int delta, float lwp, float iwp, float rel,
@@ -413,19 +501,10 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
             float tau = 0.f, w0 = 0.f, omw = 1.f, gasy = 0.f;
             if (j < nlay && gv) {
                 const Rec& Rc = recs[slot * CL + i];
-                const float ta = tau_abs(k, Rc, g, Rc.a ? mg1 : mg0, Rc.a ? nm1 : nm0);
-                const float2 r0 = __ldg(k.krayl2 + (Rc.kr[0] + g));
-                const float2 r1 = __ldg(k.krayl2 + (Rc.kr[1] + g));
-                const float tr = (Rc.fm.x * r0.x + Rc.fm.y * r0.y + Rc.fm.z * r1.x + Rc.fm.w * r1.y) * Rc.aux.x;
-                tau = ta + tr + Rc.aux.y;
-                const float ts = tr + Rc.aux.z;
-                if (tau > 2.f * FLT_MIN) {
-                    const float inv = __fdividef(1.f, tau);
-                    w0 = ts * inv;
-                    omw = (ta + Rc.aux2) * inv;
-                }
-                gasy = __fdividef(Rc.aux.w, fmaxf(ts, 3.f * FLT_MIN));
-                sw_layer_fast(tau, w0, omw, gasy, mu0, mu0_inv, R, T, Rdir, Tdir, Tn, adif, adir);
+                const LayerFwd lf = sw_layer_forward(k.kmaj4, k.kmin2[Rc.a], k.krayl2, &Rc, g, Rc.a ? mg1 : mg0,
+                                                     Rc.a ? nm1 : nm0, mu0, mu0_inv);
+                tau = lf.tau; w0 = lf.w0; omw = lf.omw; gasy = lf.gasy;
+                R = lf.R; T = lf.T; Rdir = lf.Rdir; Tdir = lf.Tdir; Tn = lf.Tn; adif = lf.adif; adir = lf.adir;
             }
             vTau[i] = tau; vW0[i] = w0; vOmw[i] = omw; vG[i] = gasy;
             vR[i] = R; vT[i] = T; vRd[i] = Rdir; vTd[i] = Tdir; vTn[i] = Tn; vAf[i] = adif; vAr[i] = adir;
@@ -657,16 +736,9 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
                 const Rec& Rc = recs[slot * CL + i];
                 const DRec& DR = drecs[slot * CL + i];
                 const float tab = la.ta, trb = la.tr, tcb = la.tc, tscb = la.tsc, tsgb = la.tsg;
-                float gt = 0.f, gh = 0.f, go = 0.f;
-                tau_abs_adjoint(k, Rc, DR, g, Rc.a ? mg1 : mg0, Rc.a ? nm1 : nm0, tab, gt, gh, go);
-                // Rayleigh: tr = col_rayl * (fm . krayl corners)
-                const float2 r0 = __ldg(k.krayl2 + (Rc.kr[0] + g));
-                const float2 r1 = __ldg(k.krayl2 + (Rc.kr[1] + g));
-                const float4 kr = make_float4(r0.x, r0.y, r1.x, r1.y);
-                const float colr = Rc.aux.x;
-                gt += trb * colr * dot4(DR.fmT, kr);
-                gh += trb * (colr * dot4(DR.fmH, kr) + DR.dB.x * dot4(Rc.fm, kr));
-                go += trb * colr * dot4(DR.fmO, kr);
+                const GasGrad gg3 = sw_gas_adjoint(k.kmaj4, k.kmin2[Rc.a], k.krayl2, &Rc, &DR, g, Rc.a ? mg1 : mg0,
+                                                   Rc.a ? nm1 : nm0, tab, trb);
+                const float gt = gg3.t, gh = gg3.h, go = gg3.o;
                 gT[i] = gt; gH[i] = gh; gO[i] = go;
                 gC0[i] = tcb; gC1[i] = tscb; gC2[i] = tsgb;
             }

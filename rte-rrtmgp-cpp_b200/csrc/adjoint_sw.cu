@@ -22,8 +22,8 @@
 // flux A_i = F_dir,i adir_i + (fd_i + fu_(i+1)) adif_i as in the forward).  Each recurrence is
 // affine in its adjoint (the albedo/source pair is 2x2 upper triangular), so chunks compose
 // exactly like the forward.  Per layer the adjoints of (R, T, Rdir, Tdir, Tn, adif, adir)
-// go through the two-stream (3-tangent dual numbers on the forward's FP32 formulas; FP64
-// central differences of the reference expressions in the k mu0 = 1 island), the
+// go through the two-stream (reverse mode of the forward's FP32 formulas with its branch
+// selections; FP64 central differences of the reference expressions in the k mu0 = 1 island), the
 // gas/Rayleigh/cloud combination, and the gas-optics interpolation (adjoint_common.cuh).
 #include <cooperative_groups.h>
 
@@ -54,21 +54,7 @@ struct SwAdjOut {
     float* alb_dif;
 };
 
-using D3 = Dual<3>;
 using D4 = Dual<4>;
-
-__device__ __forceinline__ void one_minus_exp_d(const D3& x, D3& E, D3& e)
-{
-    float Ev, ev;
-    one_minus_exp(x.v, Ev, ev);
-    E.v = Ev;
-    e.v = ev;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        E.d[i] = ev * x.d[i];
-        e.d[i] = -ev * x.d[i];
-    }
-}
 
 // FP64 island of the two-stream (|1 - (k mu0)^2| < 0.02, as the forward): Rdir and Tdir from
 // the reference expressions in double and their central differences in (tau, w0, g).  Rare
@@ -90,95 +76,189 @@ __device__ __noinline__ void island_fp64(float tau, float w0, float g, float mu0
     }
 }
 
-// sw_layer_fast (sw_common.cuh) with derivatives w.r.t. (tau, w0, g); omw = 1 - w0 moves with
-// w0.  out: R, T, Rdir, Tdir, Tn, adif, adir.
-__device__ __forceinline__ void sw_layer_dual(float tau, float w0, float omw, float g, float mu0, float mu0_inv,
-                                              D3 out[7])
-{
-    const D3 tw = dvar<3>(tau, 0), W = dvar<3>(w0, 1), G = dvar<3>(g, 2);
-    D3 O = dconst<3>(omw);
-    O.d[1] = -1.f;
-    const D3 g1 = 0.25f * (8.f - W * (5.f + 3.f * G));
-    const D3 g2 = 0.75f * (W * (1.f - G));
-    const D3 g3 = 0.25f * (2.f - (3.f * mu0) * G);
-    const D3 g4 = 1.f - g3;
-    const D3 a1 = g1 * g4 + g2 * g3;
-    const D3 a2 = g1 * g3 + g2 * g4;
-    const D3 kk = (2.f * O) * (2.f - 0.5f * (W * (1.f + 3.f * G)));
-    const D3 kkc = kk.v > 1.e-12f ? kk : dconst<3>(1.e-12f);
-    D3 k;
-    k.v = kkc.v * rsqrtf(kkc.v);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) k.d[i] = kkc.d[i] * 0.5f / k.v;
-    D3 E1, e1, En, Tn;
-    one_minus_exp_d(k * tw, E1, e1);
-    one_minus_exp_d(mu0_inv * tw, En, Tn);
-    const D3 E2 = E1 * (2.f - E1);
-    const D3 e2 = e1 * e1;
-    const D3 rt = ddiv(dconst<3>(1.f), k * (1.f + e2) + g1 * E2, true);
-    const D3 R = rt * g2 * E2;
-    const D3 T = rt * (2.f * k) * e1;
-    const D3 adif = rt * (k * E1 * E1 + (2.f * O) * E2);
-    const D3 km = mu0 * k;
-    const D3 fact = (1.f - km) * (1.f + km);
-    D3 Rdir, Tdir;
-    if (fabsf(fact.v) < 0.02f) {
-        float rd[4], td[4];
-        island_fp64(tau, w0, g, mu0, rd, td);
-        Rdir.v = rd[0];
-        Tdir.v = td[0];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            Rdir.d[i] = rd[1 + i];
-            Tdir.d[i] = td[1 + i];
-        }
-    } else {
-        const D3 rt2 = ddiv(W * rt, fact, true);
-        const D3 br = E2 * (a2 - k * km * g3) + k * (g3 - mu0 * a2) * (E1 * E1 + 2.f * (e1 * En));
-        const D3 bt_thick = (1.f + km) * (a1 + k * g4) * Tn - (1.f - km) * (a1 - k * g4) * e2 * Tn -
-                            2.f * ((k * g4 + a1 * km) * e1);
-        const D3 bt_thin = Tn * E2 * (a1 + k * km * g4) + k * (g4 + mu0 * a1) * (E1 * E1 - (1.f + e2) * En);
-        const D3 bt = (e1.v < .5f && Tn.v < .5f) ? bt_thick : bt_thin;
-        Rdir = rt2 * br;
-        Tdir = -(rt2 * bt);
-    }
-    const D3 tmin = dconst<3>(2.220446049250313e-16f);
-    Rdir = dmax(tmin, dmin(Rdir, En));
-    const D3 rest = En - Rdir;
-    Tdir = dmax(tmin, dmin(Tdir, rest));
-    const D3 adir = dmax(dconst<3>(0.f), rest - Tdir);
-    out[0] = R;
-    out[1] = T;
-    out[2] = Rdir;
-    out[3] = Tdir;
-    out[4] = Tn;
-    out[5] = adif;
-    out[6] = adir;
-}
-
 // Adjoint of one (layer, g-point) from the adjoints of its two-stream outputs (R, T, Rdir,
 // Tdir, Tn, adif, adir) to the optical inputs of the layer: gas absorption tau (x), Rayleigh
 // tau (y), cloud tau (z), cloud tau*ssa (w) and cloud tau*ssa*g (v).  The combination is
-// tau = ta + tr + tc, w0 = (tr + tsc) / tau, g = tsgc / (tr + tsc).  Out of line: the
-// caller's per-layer loop is unrolled, this body is emitted once.
+// tau = ta + tr + tc, w0 = (tr + tsc) / tau, g = tsgc / (tr + tsc).  Reverse mode of
+// sw_layer_fast: the forward is recomputed with the same expressions and branch selections
+// (clamps: the selected argument carries the derivative, as min/max of dual numbers would),
+// then the adjoints run back through it.  Out of line: the caller's per-layer loop is
+// unrolled, this body is emitted once.
 struct LocalAdj {
     float ta, tr, tc, tsc, tsg;
 };
 
-__device__ __noinline__ LocalAdj sw_local_adjoint(float tau, float w0, float omw, float gasy, float mu0, float mu0_inv,
+__device__ __noinline__ LocalAdj sw_local_adjoint(float tau, float w0, float omw, float g, float mu0, float mu0_inv,
                                                   float Rb, float Tb, float Rdb, float Tdb, float Tnb, float Afb,
                                                   float Arb)
 {
-    D3 o[7];
-    sw_layer_dual(tau, w0, omw, gasy, mu0, mu0_inv, o);
-    const float bars[7] = {Rb, Tb, Rdb, Tdb, Tnb, Afb, Arb};
-    float taub = 0.f, w0b = 0.f, gb = 0.f;
-#pragma unroll
-    for (int q = 0; q < 7; ++q) {
-        taub += bars[q] * o[q].d[0];
-        w0b += bars[q] * o[q].d[1];
-        gb += bars[q] * o[q].d[2];
+    // ---- forward, as sw_layer_fast (same expressions, same branch selections) ----
+    const float g1 = (8.f - w0 * (5.f + 3.f * g)) * .25f;
+    const float g2 = 3.f * (w0 * (1.f - g)) * .25f;
+    const float g3 = (2.f - 3.f * mu0 * g) * .25f;
+    const float g4 = 1.f - g3;
+    const float a1 = g1 * g4 + g2 * g3;
+    const float a2 = g1 * g3 + g2 * g4;
+    const float kq = 2.f - .5f * w0 * (1.f + 3.f * g);
+    const float kk = 2.f * omw * kq;
+    const bool kk_on = kk > 1.e-12f;
+    const float kkc = fmaxf(kk, 1.e-12f);
+    const float k = kkc * rsqrtf(kkc);
+    float E1, e1, En, Tn;
+    one_minus_exp(k * tau, E1, e1);
+    one_minus_exp(tau * mu0_inv, En, Tn);
+    const float E2 = E1 * (2.f - E1);
+    const float e2 = e1 * e1;
+    const float den = k * (1.f + e2) + g1 * E2;
+    const float rt = __fdividef(1.f, den);
+    const float km = k * mu0;
+    const float fact = (1.f - km) * (1.f + km);
+    const bool island = fabsf(fact) < 0.02f;
+    float Rdir0, Tdir0, rt2 = 0.f, br = 0.f, bt = 0.f;
+    bool thick = false;
+    float rd[4], td[4];
+    if (island) {
+        island_fp64(tau, w0, g, mu0, rd, td);
+        Rdir0 = rd[0];
+        Tdir0 = td[0];
+    } else {
+        rt2 = __fdividef(w0 * rt, fact);
+        br = E2 * (a2 - k * km * g3) + k * (g3 - mu0 * a2) * (E1 * E1 + 2.f * (e1 * En));
+        thick = e1 < .5f && Tn < .5f;
+        if (thick)
+            bt = (1.f + km) * (a1 + k * g4) * Tn - (1.f - km) * (a1 - k * g4) * e2 * Tn - 2.f * ((k * g4 + a1 * km) * e1);
+        else
+            bt = Tn * E2 * (a1 + k * km * g4) + k * (g4 + mu0 * a1) * (E1 * E1 - (1.f + e2) * En);
+        Rdir0 = rt2 * br;
+        Tdir0 = -(rt2 * bt);
     }
+    const float tmin = 2.220446049250313e-16f;
+    const bool r_lo = Rdir0 <= En;                 // min(Rdir0, En) takes Rdir0
+    const float rm = r_lo ? Rdir0 : En;
+    const bool r_on = !(tmin >= rm);               // max(tmin, .) takes the value
+    const float Rdir = r_on ? rm : tmin;
+    const float rest = En - Rdir;
+    const bool t_lo = Tdir0 <= rest;
+    const float tm = t_lo ? Tdir0 : rest;
+    const bool t_on = !(tmin >= tm);
+    const float Tdir = t_on ? tm : tmin;
+    const bool a_on = !(0.f >= rest - Tdir);
+
+    // ---- reverse ----
+    float rest_b = 0.f, Tdir_b = Tdb, Rdir_b = Rdb, En_b = 0.f, Tn_b = Tnb;
+    if (a_on) { rest_b += Arb; Tdir_b -= Arb; }
+    float Tdir0_b = 0.f;
+    if (t_on) {
+        if (t_lo) Tdir0_b = Tdir_b; else rest_b += Tdir_b;
+    }
+    En_b += rest_b;
+    Rdir_b -= rest_b;
+    float Rdir0_b = 0.f;
+    if (r_on) {
+        if (r_lo) Rdir0_b = Rdir_b; else En_b += Rdir_b;
+    }
+    float tau_b = 0.f, w0_b = 0.f, g_b = 0.f, omw_b = 0.f;
+    float k_b = 0.f, km_b = 0.f, rt_b = 0.f, E1_b = 0.f, e1_b = 0.f, E2_b = 0.f, e2_b = 0.f;
+    float g1_b = 0.f, g2_b = 0.f, g3_b = 0.f, g4_b = 0.f, a1_b = 0.f, a2_b = 0.f;
+    if (island) {
+        tau_b += Rdir0_b * rd[1] + Tdir0_b * td[1];
+        w0_b += Rdir0_b * rd[2] + Tdir0_b * td[2];
+        g_b += Rdir0_b * rd[3] + Tdir0_b * td[3];
+    } else {
+        const float rt2_b = Rdir0_b * br - Tdir0_b * bt;
+        const float br_b = Rdir0_b * rt2;
+        const float bt_b = -Tdir0_b * rt2;
+        // br = E2 X + k Y Z
+        const float X = a2 - k * km * g3, Y = g3 - mu0 * a2, Z = E1 * E1 + 2.f * (e1 * En);
+        E2_b += br_b * X;
+        const float X_b = br_b * E2;
+        a2_b += X_b;
+        k_b -= X_b * km * g3;
+        km_b -= X_b * k * g3;
+        g3_b -= X_b * k * km;
+        k_b += br_b * Y * Z;
+        const float Y_b = br_b * k * Z, Z_b = br_b * k * Y;
+        g3_b += Y_b;
+        a2_b -= Y_b * mu0;
+        E1_b += Z_b * 2.f * E1;
+        e1_b += Z_b * 2.f * En;
+        En_b += Z_b * 2.f * e1;
+        if (thick) {
+            const float P = a1 + k * g4, Q = a1 - k * g4, S = k * g4 + a1 * km;
+            const float P_b = bt_b * (1.f + km) * Tn, Q_b = -bt_b * (1.f - km) * e2 * Tn, S_b = -2.f * bt_b * e1;
+            km_b += bt_b * (P * Tn + Q * e2 * Tn);
+            Tn_b += bt_b * ((1.f + km) * P - (1.f - km) * Q * e2);
+            e2_b -= bt_b * (1.f - km) * Q * Tn;
+            e1_b -= 2.f * bt_b * S;
+            a1_b += P_b + Q_b + S_b * km;
+            k_b += (P_b - Q_b) * g4 + S_b * g4;
+            g4_b += (P_b - Q_b) * k + S_b * k;
+            km_b += S_b * a1;
+        } else {
+            const float U = a1 + k * km * g4, V = g4 + mu0 * a1, W2 = E1 * E1 - (1.f + e2) * En;
+            Tn_b += bt_b * E2 * U;
+            E2_b += bt_b * Tn * U;
+            const float U_b = bt_b * Tn * E2;
+            a1_b += U_b;
+            k_b += U_b * km * g4;
+            km_b += U_b * k * g4;
+            g4_b += U_b * k * km;
+            k_b += bt_b * V * W2;
+            const float V_b = bt_b * k * W2, W2_b = bt_b * k * V;
+            g4_b += V_b;
+            a1_b += V_b * mu0;
+            E1_b += W2_b * 2.f * E1;
+            e2_b -= W2_b * En;
+            En_b -= W2_b * (1.f + e2);
+        }
+        // rt2 = w0 rt / fact, fact = 1 - km^2
+        w0_b += rt2_b * rt / fact;
+        rt_b += rt2_b * w0 / fact;
+        const float fact_b = -rt2_b * rt2 / fact;
+        km_b -= fact_b * 2.f * km;
+    }
+    k_b += km_b * mu0;
+    // R, T, adif
+    const float Aq = k * E1 * E1 + 2.f * omw * E2;
+    rt_b += Rb * g2 * E2 + Tb * 2.f * k * e1 + Afb * Aq;
+    g2_b += Rb * rt * E2;
+    E2_b += Rb * rt * g2 + Afb * rt * 2.f * omw;
+    k_b += Tb * 2.f * rt * e1 + Afb * rt * E1 * E1;
+    e1_b += Tb * 2.f * rt * k;
+    E1_b += Afb * rt * 2.f * k * E1;
+    omw_b += Afb * rt * 2.f * E2;
+    // rt = 1 / den, den = k (1 + e2) + g1 E2
+    const float den_b = -rt_b * rt * rt;
+    k_b += den_b * (1.f + e2);
+    e2_b += den_b * k;
+    g1_b += den_b * E2;
+    E2_b += den_b * g1;
+    // E2 = E1 (2 - E1), e2 = e1^2
+    E1_b += E2_b * (2.f - 2.f * E1);
+    e1_b += e2_b * 2.f * e1;
+    // (E1, e1) = one_minus_exp(k tau): dE1/dx = e1, de1/dx = -e1
+    const float x1_b = e1 * (E1_b - e1_b);
+    k_b += x1_b * tau;
+    tau_b += x1_b * k;
+    const float xn_b = Tn * (En_b - Tn_b);
+    tau_b += xn_b * mu0_inv;
+    // k = sqrt(max(kk, 1e-12)), kk = 2 omw kq
+    const float kk_b = kk_on ? k_b * 0.5f / k : 0.f;
+    omw_b += kk_b * 2.f * kq;
+    w0_b += kk_b * 2.f * omw * (-.5f * (1.f + 3.f * g));
+    g_b += kk_b * 2.f * omw * (-1.5f * w0);
+    // a1, a2, g1..g4
+    g1_b += a1_b * g4 + a2_b * g3;
+    g4_b += a1_b * g1 + a2_b * g2;
+    g2_b += a1_b * g3 + a2_b * g4;
+    g3_b += a1_b * g2 + a2_b * g1;
+    g3_b -= g4_b;
+    g_b += g3_b * (-.75f * mu0);
+    w0_b += g2_b * .75f * (1.f - g) - g1_b * (5.f + 3.f * g) * .25f;
+    g_b += -g2_b * .75f * w0 - g1_b * .75f * w0;
+    // omw = 1 - w0 (formed separately for accuracy): total derivative along w0
+    const float taub = tau_b, w0b = w0_b - omw_b, gb = g_b;
+
     const bool okt = tau > 2.f * FLT_MIN;
     const float ts = w0 * tau;
     const bool oks = ts > 3.f * FLT_MIN;
@@ -186,13 +266,12 @@ __device__ __noinline__ LocalAdj sw_local_adjoint(float tau, float w0, float omw
     const float its = oks ? __fdividef(1.f, ts) : 0.f;
     LocalAdj r;
     r.ta = taub - w0b * w0 * itau;
-    r.tr = taub + w0b * omw * itau - gb * gasy * its;
+    r.tr = taub + w0b * omw * itau - gb * g * its;
     r.tc = taub - w0b * w0 * itau;
-    r.tsc = w0b * itau - gb * gasy * its;
+    r.tsc = w0b * itau - gb * g * its;
     r.tsg = gb * its;
     return r;
 }
-
 
 // Gas-optics adjoint of one (layer, g-point): the absorption tau_bar through the major and
 // minor interpolation (tau_abs_adjoint of adjoint_common.cuh) and the Rayleigh tau_bar

@@ -372,29 +372,25 @@ def deep_bench(args, solver, fused, dev, stream, flush, rank, world, dist):
           (("up", (nlev, ncol)), ("dn", (nlev, ncol)), ("dir", (nlev, ncol)), ("hr", (nlay, ncol)))}
 
     def run(ev=None):
+        # one launch per domain: fluxes and gradients
         if ev is not None:
             ev[0].record(stream)
-        fused.solve_lw(atm)
+        res_lw = adjoint_lw(fused, atm, sd["up"], sd["dn"], sd["hr"], with_fluxes=True)
         if ev is not None:
             ev[1].record(stream)
-        adjoint_lw(fused, atm, sd["up"], sd["dn"], sd["hr"])
+        res_sw = adjoint_sw(fused, atm, sd["up"], sd["dn"], sd["dir"], sd["hr"], with_fluxes=True)
         if ev is not None:
             ev[2].record(stream)
-        fused.solve_sw(atm)
-        if ev is not None:
-            ev[3].record(stream)
-        adjoint_sw(fused, atm, sd["up"], sd["dn"], sd["dir"], sd["hr"])
-        if ev is not None:
-            ev[4].record(stream)
+        return res_lw[0], res_sw[0]
 
     run()
     torch.cuda.synchronize()
-    evs = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(5)) for _ in range(args.deep_steps)]
+    evs = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(3)) for _ in range(args.deep_steps)]
     for e in evs:
         flush.zero_()
-        run(e)
+        f_lw, f_sw = run(e)
     torch.cuda.synchronize()
-    parts = [float(np.mean([e[q].elapsed_time(e[q + 1]) for e in evs])) for q in range(4)]
+    parts = [float(np.mean([e[q].elapsed_time(e[q + 1]) for e in evs])) for q in range(2)]
     tot = shard.max_over_ranks(float(np.sum(parts)), dist if world > 1 else None, dev)
     # FP64 forward of this build on one 8192-column block of the same atmosphere
     nb = min(8192, ncol)
@@ -415,7 +411,6 @@ def deep_bench(args, solver, fused, dev, stream, flush, rank, world, dist):
     torch.cuda.synchronize()
     ms64 = float(np.mean([a.elapsed_time(b) for a, b in e64]))
     r_lw, r_sw = solver.solve_lw(sub), solver.solve_sw(sub)
-    f_lw, f_sw = fused.solve_lw(atm), fused.solve_sw(atm)
     ferr = max(float((f[k][:, :nb].double() - r[k]).abs().max()) for f, r in ((f_lw, r_lw), (f_sw, r_sw))
                for k in ("flux_up", "flux_dn", "flux_net"))
     herr = max(float((f["heating_rate"][:, :nb].double() - r["heating_rate"]).abs().max())
@@ -425,14 +420,12 @@ def deep_bench(args, solver, fused, dev, stream, flush, rank, world, dist):
     fp64 = nb / (ms64 * 1e-3)
     out = {"workload": f"all-sky LW+SW forward + adjoint, ncol={ncol} per GPU, nlay={nlay}",
            "forward_adjoint": {"value": fwd_adj, "unit": "columns/s", "ms_per_step": tot, "steps": args.deep_steps,
-                               "kernel_ms": {"lw_forward_kernel": round(parts[0], 3),
-                                             "lw_adjoint_kernel": round(parts[1], 3),
-                                             "sw_forward_kernel": round(parts[2], 3),
-                                             "sw_adjoint_kernel": round(parts[3], 3)}},
+                               "kernel_ms": {"lw_adjoint_kernel (with fluxes)": round(parts[0], 3),
+                                             "sw_adjoint_kernel (with fluxes)": round(parts[1], 3)}},
            "fp64_forward_blocked": {"value": fp64, "unit": "columns/s", "block_ncol": nb, "ms_per_block": ms64},
            "ratio_fwd_adj_over_fp64": fwd_adj / (fp64 * world),
            "fp32_max_flux_err_w_m2": ferr, "fp32_max_heating_rate_err_k_day": herr}
-    del atm, sd, sub
+    del atm, sd, sub, f_lw, f_sw
     torch.cuda.empty_cache()
     return out
 
@@ -651,20 +644,18 @@ def main():
               (("up", (nlev, args.ncol)), ("dn", (nlev, args.ncol)), ("dir", (nlev, args.ncol)),
                ("hr", (args.nlay, args.ncol)))}
 
-        def fa_step():
-            run_lw(atm)
-            adjoint_lw(fused, atm, sd["up"], sd["dn"], sd["hr"])
-            run_sw(atm)
-            adjoint_sw(fused, atm, sd["up"], sd["dn"], sd["dir"], sd["hr"])
+        def fa_step(e=None):
+            # one launch per domain: fluxes and gradients (rrtmgp_b200_forward_adjoint_*_f32)
+            if e is not None:
+                e[0].record(stream)
+            adjoint_lw(fused, atm, sd["up"], sd["dn"], sd["hr"], with_fluxes=True)
+            if e is not None:
+                e[1].record(stream)
+            adjoint_sw(fused, atm, sd["up"], sd["dn"], sd["dir"], sd["hr"], with_fluxes=True)
+            if e is not None:
+                e[2].record(stream)
 
-        for _ in range(2):
-            fa_step()
-        torch.cuda.synchronize()
-        nrep = max(2, args.steps // 5)
-        ev = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(5)) for _ in range(nrep)]
-        for i in range(nrep):
-            flush.zero_()
-            e = ev[i]
+        def separate_step(e):
             e[0].record(stream)
             run_lw(atm)
             e[1].record(stream)
@@ -674,16 +665,36 @@ def main():
             e[3].record(stream)
             adjoint_sw(fused, atm, sd["up"], sd["dn"], sd["dir"], sd["hr"])
             e[4].record(stream)
+
+        for _ in range(2):
+            fa_step()
         torch.cuda.synchronize()
-        parts = [float(np.mean([e[q].elapsed_time(e[q + 1]) for e in ev])) for q in range(4)]
-        tot = float(np.sum(parts))
-        tot = shard.max_over_ranks(tot, dist if world > 1 else None, dev)
+        nrep = max(2, args.steps // 5)
+        ev = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(3)) for _ in range(nrep)]
+        for i in range(nrep):
+            flush.zero_()
+            fa_step(ev[i])
+        torch.cuda.synchronize()
+        parts = [float(np.mean([e[q].elapsed_time(e[q + 1]) for e in ev])) for q in range(2)]
+        tot = shard.max_over_ranks(float(np.sum(parts)), dist if world > 1 else None, dev)
+        # the same work as separate forward and adjoint launches (breakdown)
+        ev2 = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(5)) for _ in range(2)]
+        for e in ev2:
+            flush.zero_()
+            separate_step(e)
+        torch.cuda.synchronize()
+        sep = [float(np.mean([e[q].elapsed_time(e[q + 1]) for e in ev2])) for q in range(4)]
         fwd_adj = {"value": shard.weak_scaling_rate(args.ncol, world, 1, tot), "unit": "columns/s",
-                   "ms_per_step": tot, "steps": nrep, "gpu_launches_per_step": 4,
-                   "kernel_ms": {"lw_forward_kernel": round(parts[0], 4), "lw_adjoint_kernel": round(parts[1], 4),
-                                 "sw_forward_kernel": round(parts[2], 4), "sw_adjoint_kernel": round(parts[3], 4)},
+                   "ms_per_step": tot, "steps": nrep, "gpu_launches_per_step": 2,
+                   "kernel_ms": {"lw_adjoint_kernel (with fluxes)": round(parts[0], 4),
+                                 "sw_adjoint_kernel (with fluxes)": round(parts[1], 4)},
+                   "separate_launches_ms": {"lw_forward_kernel": round(sep[0], 4),
+                                            "lw_adjoint_kernel": round(sep[1], 4),
+                                            "sw_forward_kernel": round(sep[2], 4),
+                                            "sw_adjoint_kernel": round(sep[3], 4), "total": round(sum(sep), 4)},
                    "gradients": "flux/heating-rate seeds -> tlay, tlev, tsfc, h2o, o3, lwp, iwp, rel, rei (LW); "
-                                "tlay, h2o, o3, lwp, iwp, rel, rei, surface albedos (SW)"}
+                                "tlay, h2o, o3, lwp, iwp, rel, rei, surface albedos (SW); fluxes and heating "
+                                "rates from the same launches"}
 
     # Plain FP64 GPU forward of the same build (the denominator of the FP32 target).
     fp64 = None
@@ -711,6 +722,16 @@ def main():
                    for f, r in ((f_lw, r_lw), (f_sw, r_sw)))
         fp64 = {"value": args.ncol / (ms64 * 1e-3), "unit": "columns/s", "ms_per_step": ms64,
                 "fp32_max_flux_err_w_m2": ferr, "fp32_max_heating_rate_err_k_day": herr}
+        if fwd_adj is not None:
+            # the fluxes of the forward + adjoint launches against the same FP64 forward
+            from rrtmgp_b200.autodiff import adjoint_lw, adjoint_sw
+            a_lw = adjoint_lw(fused, atm, sd["up"], sd["dn"], sd["hr"], with_fluxes=True)[0]
+            a_sw = adjoint_sw(fused, atm, sd["up"], sd["dn"], sd["dir"], sd["hr"], with_fluxes=True)[0]
+            fwd_adj["fp32_max_flux_err_w_m2"] = max(float((f[k].double() - r[k]).abs().max())
+                                                    for f, r in ((a_lw, r_lw), (a_sw, r_sw))
+                                                    for k in ("flux_up", "flux_dn", "flux_net"))
+            fwd_adj["fp32_max_heating_rate_err_k_day"] = max(
+                float((f["heating_rate"].double() - r["heating_rate"]).abs().max()) for f, r in ((a_lw, r_lw), (a_sw, r_sw)))
         del atm64
         solver._bufs = {k: v for k, v in solver._bufs.items() if k[0][2] != torch.float64}
 

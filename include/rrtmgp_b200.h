@@ -417,6 +417,32 @@ int rrtmgp_b200_adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int
         float* grad_lwp, float* grad_iwp, float* grad_rel, float* grad_rei,
         float* grad_sfc_alb_dir, float* grad_sfc_alb_dif, void* stream);
 
+/* Forward + adjoint in one pass per domain (no reference counterpart): the adjoint kernels
+ * above also emit the forward fluxes they recompute, so a caller that needs both (a
+ * variational step, a Jacobian-vector product with its primal) makes one launch per domain
+ * instead of a forward and an adjoint.  Arguments as rrtmgp_b200_adjoint_lw_f32 /
+ * rrtmgp_b200_adjoint_sw_f32, plus the outputs of rrtmgp_b200_forward_lw_f32 /
+ * rrtmgp_b200_forward_sw_f32 (all required; the same values to FP32 rounding). */
+int rrtmgp_b200_forward_adjoint_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int ncol, int nlay,
+        const float* play, const float* plev, const float* tlay, const float* tlev,
+        const float* tsfc, const float* col_dry, const rrtmgp_b200_gas_conc* gases, int ngases,
+        const float* lwp, const float* iwp, const float* rel, const float* rei,
+        const float* sfc_emis, const float* seed_flux_up, const float* seed_flux_dn,
+        const float* seed_heating_rate, float* grad_tlay, float* grad_tlev, float* grad_tsfc,
+        float* grad_h2o, float* grad_o3, float* grad_lwp, float* grad_iwp, float* grad_rel,
+        float* grad_rei, float* flux_up, float* flux_dn, float* flux_net, float* heating_rate,
+        int chunk, void* stream);
+int rrtmgp_b200_forward_adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int ncol, int nlay,
+        const float* play, const float* plev, const float* tlay, const float* col_dry,
+        const rrtmgp_b200_gas_conc* gases, int ngases, const float* lwp, const float* iwp,
+        const float* rel, const float* rei, int delta_cloud, const float* mu0,
+        const float* tsi_scaling, const float* sfc_alb_dir, const float* sfc_alb_dif,
+        const float* seed_flux_up, const float* seed_flux_dn, const float* seed_flux_dn_dir,
+        const float* seed_heating_rate, float* grad_tlay, float* grad_h2o, float* grad_o3,
+        float* grad_lwp, float* grad_iwp, float* grad_rel, float* grad_rei,
+        float* grad_sfc_alb_dir, float* grad_sfc_alb_dif, float* flux_up, float* flux_dn,
+        float* flux_dn_dir, float* flux_net, float* heating_rate, void* stream);
+
 /* ---- Batched forward of many independent column grids ------------------------------------
  * No reference counterpart as one call: the reference's driver runs one grid at a time and
  * splits its columns into blocks of n_col_block (src_test/Radiation_solver.cu:467-615 and

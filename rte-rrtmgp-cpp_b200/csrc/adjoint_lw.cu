@@ -49,6 +49,11 @@ struct AdjOut {
     float* iwp;
     float* rel;
     float* rei;
+    // forward fluxes, written when the kernel is instantiated with FLUX (else unused)
+    float* flux_up;
+    float* flux_dn;
+    float* flux_net;
+    float* heating_rate;
 };
 
 // omt = 1 - exp(-x), fact = omt / x - exp(-x) and their x-derivatives (series below 0.1, as
@@ -142,7 +147,7 @@ __device__ __forceinline__ Tp* remote(cg::cluster_group& cl, Tp* p, int rank)
 // the cluster code).  CTA r of the cluster owns the layers [r LPC, (r + 1) LPC), LPC = NWc CL,
 // as NWc warps of CL layers; chunk maps and the surface source are pushed to every CTA of the
 // cluster through distributed shared memory.
-template <int CL, bool CLUSTER>
+template <int CL, bool CLUSTER, bool FLUX>
 __global__ void __launch_bounds__(512)
 lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjCloud cld, int ncol, int nlay, int CS,
                   int idx_o3, int cd_internal, const float* __restrict__ play, const float* __restrict__ plev,
@@ -237,6 +242,9 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
 #pragma unroll
     for (int r = 0; r < NRS; ++r) acc[r] = 0.0;
     double acc_levbot = 0.0, acc_tsfc = 0.0;
+    // forward fluxes (FLUX), as the forward kernel: level radiances [up | down] and layer
+    // divergences reduce-scattered over the group's g-points, the bottom level separately
+    double acc_flev = 0.0, acc_fdiv = 0.0, acc_fbot_up = 0.0, acc_fbot_dn = 0.0;
 
     for (int gg = 0; gg < k.ngroups; ++gg) {
         const int g = 32 * gg + lane;
@@ -359,6 +367,23 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
         vU[CL] = y;
 #pragma unroll
         for (int i = CL - 1; i >= 0; --i) vU[i] = (1.f - omt[i]) * vU[i + 1] + sup[i];
+        if (FLUX) {
+            float v[2 * CL], dv[CL];
+#pragma unroll
+            for (int i = 0; i < CL; ++i) {
+                v[i] = vU[i];
+                v[CL + i] = vI[i];
+                dv[i] = omt[i] * (vI[i] + vU[i + 1]) - sdn[i] - sup[i];
+            }
+            ReduceScatter<2 * CL, 16>::run(v, lane);
+            ReduceScatter<CL, 16>::run(dv, lane);
+            acc_flev += double(v[0]);
+            acc_fdiv += double(dv[0]);
+            if (Wg == NWt - 1) {
+                acc_fbot_up += double(warp_sum(vU[CL]));
+                acc_fbot_dn += double(warp_sum(vI[CL]));
+            }
+        }
         // ---- reverse: U_bar per level (top down) ----
         float vUb[CL];
         {
@@ -461,6 +486,36 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
     }
 
     // ---- outputs ----
+    if (FLUX) {
+        constexpr int SH_LEV = (CL == 16) ? 0 : 1;   // lane L holds value L >> SH_LEV
+        constexpr int SH_DIV = (CL == 16) ? 1 : 2;
+        const int vidx = lane >> SH_LEV;
+        const double other = __shfl_xor_sync(0xffffffffu, acc_flev, CL << SH_LEV);
+        if ((lane & ((1 << SH_LEV) - 1)) == 0 && vidx < CL) {
+            const int j = j0 + w * CL + vidx;
+            if (j < nlay) {
+                const size_t o = icol + size_t(top_at_1 ? j : nlay - j) * ncol;
+                const double up = pi * acc_flev, dn = pi * other;
+                out.flux_up[o] = float(up);
+                out.flux_dn[o] = float(dn);
+                out.flux_net[o] = float(dn - up);
+            }
+        }
+        if ((lane & ((1 << SH_DIV) - 1)) == 0 && (lane >> SH_DIV) < CL) {
+            const int jl = w * CL + (lane >> SH_DIV), j = j0 + jl;
+            if (j < nlay) {
+                const double g0_cp = 9.80665 / 1004.64;
+                out.heating_rate[icol + size_t(top_at_1 ? j : nlay - 1 - j) * ncol] =
+                    float(g0_cp * 86400.0 * pi * acc_fdiv / double(st[jl].dp));
+            }
+        }
+        if (Wg == NWt - 1 && lane == 0) {
+            const size_t o = icol + size_t(top_at_1 ? nlay : 0) * ncol;
+            out.flux_up[o] = float(pi * acc_fbot_up);
+            out.flux_dn[o] = float(pi * acc_fbot_dn);
+            out.flux_net[o] = float(pi * (acc_fbot_dn - acc_fbot_up));
+        }
+    }
     if (lane == 0) sm_levbot[w] = acc_levbot;
     csync();
     // level gradient of the bottom level of the previous chunk (another CTA's for w = 0)
@@ -521,7 +576,7 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
 
 // Up to 128 layers (CL = 8) or 256 (CL = 16, if the records fit) one CTA of ceil(nlay / CL)
 // warps per column; beyond, clusters of CS = ceil(nlay / 128) CTAs of 16 warps (CL = 8).
-template <int CL>
+template <int CL, bool FLUX>
 int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay, int idx_o3, const float* play,
                       const float* plev, const float* tlay, const float* tlev, const float* tsfc, const float* col_dry,
                       const GasSet<float>& gs, const float* lwp, const float* iwp, const float* rel, const float* rei,
@@ -543,9 +598,9 @@ int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
     if (smem > 227 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_lw: shared memory need exceeds 227 KB");
     static bool attr = false;
     if (!attr) {
-        RB_CUDA(cudaFuncSetAttribute(lw_adjoint_kernel<CL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     227 * 1024), "adjoint_lw attribute");
-        RB_CUDA(cudaFuncSetAttribute(lw_adjoint_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        RB_CUDA(cudaFuncSetAttribute(lw_adjoint_kernel<CL, false, FLUX>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "adjoint_lw attribute");
+        RB_CUDA(cudaFuncSetAttribute(lw_adjoint_kernel<8, true, FLUX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      227 * 1024), "adjoint_lw attribute");
         attr = true;
     }
@@ -557,7 +612,7 @@ int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
         ca.present = 1;
     }
     if (CS == 1) {
-        lw_adjoint_kernel<CL, false><<<ncol, NWc * 32, smem, stream>>>(v, gs, ca, ncol, nlay, 1, idx_o3, col_dry ? 0 : 1,
+        lw_adjoint_kernel<CL, false, FLUX><<<ncol, NWc * 32, smem, stream>>>(v, gs, ca, ncol, nlay, 1, idx_o3, col_dry ? 0 : 1,
                                                                   play, plev, tlay, tlev, tsfc, col_dry, emis, su, sd,
                                                                   sh, out);
         RB_LAUNCH("lw_adjoint_kernel");
@@ -575,7 +630,7 @@ int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    RB_CUDA(cudaLaunchKernelEx(&cfg, lw_adjoint_kernel<8, true>, v, gs, ca, ncol, nlay, CS, idx_o3, col_dry ? 0 : 1, play,
+    RB_CUDA(cudaLaunchKernelEx(&cfg, lw_adjoint_kernel<8, true, FLUX>, v, gs, ca, ncol, nlay, CS, idx_o3, col_dry ? 0 : 1, play,
                                plev, tlay, tlev, tsfc, col_dry, emis, su, sd, sh, out),
             "lw_adjoint_kernel launch");
     return RRTMGP_B200_OK;
@@ -588,9 +643,12 @@ int adjoint_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
                    const rrtmgp_b200_gas_conc* gases, int ngases, const float* lwp, const float* iwp, const float* rel,
                    const float* rei, const float* sfc_emis, const float* seed_up, const float* seed_dn,
                    const float* seed_hr, float* g_tlay, float* g_tlev, float* g_tsfc, float* g_h2o, float* g_o3,
-                   float* g_lwp, float* g_iwp, float* g_rel, float* g_rei, int chunk, void* stream)
+                   float* g_lwp, float* g_iwp, float* g_rel, float* g_rei, float* flux_up, float* flux_dn,
+                   float* flux_net, float* heating_rate, int chunk, void* stream)
 {
     RB_CHECK_ARG(k && k->info.is_longwave, "adjoint_lw: need a longwave k-distribution");
+    const bool with_flux = flux_up != nullptr;
+    RB_CHECK_ARG(!with_flux || (flux_dn && flux_net && heating_rate), "forward_adjoint_lw: null flux array");
     RB_CHECK_ARG(ncol > 0 && nlay > 1, "adjoint_lw: ncol > 0 and nlay > 1 required");
     RB_CHECK_ARG(play && plev && tlay && tlev && tsfc && sfc_emis, "adjoint_lw: null input array");
     RB_CHECK_ARG(!c || (lwp && iwp && rel && rei), "adjoint_lw: cloud arrays required with a cloud handle");
@@ -604,13 +662,15 @@ int adjoint_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     int idx_o3 = 0;
     for (size_t i = 0; i < k->gas_names.size(); ++i)
         if (k->gas_names[i] == "o3") idx_o3 = int(i) + 1;
-    const AdjOut out{g_tlay, g_tlev, g_tsfc, g_h2o, g_o3, g_lwp, g_iwp, g_rel, g_rei};
+    const AdjOut out{g_tlay, g_tlev, g_tsfc, g_h2o, g_o3, g_lwp, g_iwp, g_rel, g_rei,
+                     flux_up, flux_dn, flux_net, heating_rate};
     cudaStream_t s = as_stream(stream);
-    if (chunk == 16)
-        return launch_lw_adjoint<16>(k, c, ncol, nlay, idx_o3, play, plev, tlay, tlev, tsfc, col_dry, gs, lwp, iwp,
-                                     rel, rei, sfc_emis, seed_up, seed_dn, seed_hr, out, s);
-    return launch_lw_adjoint<8>(k, c, ncol, nlay, idx_o3, play, plev, tlay, tlev, tsfc, col_dry, gs, lwp, iwp, rel,
-                                rei, sfc_emis, seed_up, seed_dn, seed_hr, out, s);
+#define RB_LW_ADJ(CLv, F)                                                                                          \
+    launch_lw_adjoint<CLv, F>(k, c, ncol, nlay, idx_o3, play, plev, tlay, tlev, tsfc, col_dry, gs, lwp, iwp, rel, \
+                              rei, sfc_emis, seed_up, seed_dn, seed_hr, out, s)
+    if (chunk == 16) return with_flux ? RB_LW_ADJ(16, true) : RB_LW_ADJ(16, false);
+    return with_flux ? RB_LW_ADJ(8, true) : RB_LW_ADJ(8, false);
+#undef RB_LW_ADJ
 }
 
 }  // namespace rrtmgp_b200
@@ -626,5 +686,21 @@ extern "C" int rrtmgp_b200_adjoint_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud
     return rrtmgp_b200::adjoint_lw_f32(k, c, ncol, nlay, play, plev, tlay, tlev, tsfc, col_dry, gases, ngases, lwp, iwp,
                                        rel, rei, sfc_emis, seed_flux_up, seed_flux_dn, seed_heating_rate, grad_tlay,
                                        grad_tlev, grad_tsfc, grad_h2o, grad_o3, grad_lwp, grad_iwp, grad_rel, grad_rei,
-                                       chunk, stream);
+                                       nullptr, nullptr, nullptr, nullptr, chunk, stream);
+}
+
+extern "C" int rrtmgp_b200_forward_adjoint_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
+        const float* play, const float* plev, const float* tlay, const float* tlev, const float* tsfc,
+        const float* col_dry, const rrtmgp_b200_gas_conc* gases, int ngases, const float* lwp, const float* iwp,
+        const float* rel, const float* rei, const float* sfc_emis, const float* seed_flux_up,
+        const float* seed_flux_dn, const float* seed_heating_rate, float* grad_tlay, float* grad_tlev,
+        float* grad_tsfc, float* grad_h2o, float* grad_o3, float* grad_lwp, float* grad_iwp, float* grad_rel,
+        float* grad_rei, float* flux_up, float* flux_dn, float* flux_net, float* heating_rate, int chunk,
+        void* stream)
+{
+    RB_CHECK_ARG(flux_up, "forward_adjoint_lw: null flux array");
+    return rrtmgp_b200::adjoint_lw_f32(k, c, ncol, nlay, play, plev, tlay, tlev, tsfc, col_dry, gases, ngases, lwp, iwp,
+                                       rel, rei, sfc_emis, seed_flux_up, seed_flux_dn, seed_heating_rate, grad_tlay,
+                                       grad_tlev, grad_tsfc, grad_h2o, grad_o3, grad_lwp, grad_iwp, grad_rel, grad_rei,
+                                       flux_up, flux_dn, flux_net, heating_rate, chunk, stream);
 }

@@ -52,6 +52,12 @@ struct SwAdjOut {
     float* rei;
     float* alb_dir;
     float* alb_dif;
+    // forward fluxes, written when the kernel is instantiated with FLUX (else unused)
+    float* flux_up;
+    float* flux_dn;
+    float* flux_dir;
+    float* flux_net;
+    float* heating_rate;
 };
 
 using D4 = Dual<4>;
@@ -443,6 +449,7 @@ __device__ __forceinline__ Tp* remote(cg::cluster_group& cl, Tp* p, int rank)
     return cl.map_shared_rank(p, rank);
 }
 
+template <bool FLUX>
 __global__ void __launch_bounds__(256, 1)
 sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwCloudArgs cld, int ncol, int nlay, int CS,
                   int idx_o3, int cd_internal, const float* __restrict__ play, const float* __restrict__ plev,
@@ -533,6 +540,11 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
     const float al0 = seed_at(seed_up, 0);
     const float alN = seed_at(seed_up, nlay), beN = seed_at(seed_dn, nlay), gaN = seed_at(seed_dir, nlay);
     double acc_q = 0.0;   // RS<32> accumulator: lane L holds [T | H | O | -][L >> 3], layer L & 7
+    // forward fluxes (FLUX): as the forward kernel, lane L holds value L >> 1 of the chunk's
+    // [levels | layers]: acc_fa direct / direct absorbed, acc_fb up / diffuse absorbed,
+    // acc_fc diffuse down
+    double acc_fa = 0.0, acc_fb = 0.0, acc_fc = 0.0;
+    double acc_sfc_dir = 0.0, acc_sfc_dn = 0.0, acc_sfc_up = 0.0;
     constexpr float m_dry = 0.028964f, m_h2o = 0.018016f;
 
     for (int gg = 0; gg < k.ngroups; ++gg) {
@@ -668,6 +680,38 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
             fd = (vT[i] * fd + vR[i] * s_n + vTd[i] * vDir[i]) * den;
         }
         const float fd_bot = fd;
+        if (FLUX) {
+            float v[2 * CL];
+#pragma unroll
+            for (int i = 0; i < CL; ++i) {
+                v[i] = vDir[i];
+                v[CL + i] = vDir[i] * vAr[i];
+            }
+            ReduceScatter<2 * CL, 16>::run(v, lane);
+            acc_fa += double(v[0]);
+#pragma unroll
+            for (int i = 0; i < CL; ++i) {
+                const float a_n = (i + 1 < CL) ? vA[i + 1] : alb_in;
+                const float s_n = (i + 1 < CL) ? vS[i + 1] : src_in;
+                const float fd_n = (i + 1 < CL) ? vFd[i + 1] : fd_bot;
+                v[i] = fmaf(vFd[i], vA[i], vS[i]);
+                v[CL + i] = (vFd[i] + fmaf(fd_n, a_n, s_n)) * vAf[i];
+            }
+            ReduceScatter<2 * CL, 16>::run(v, lane);
+            acc_fb += double(v[0]);
+#pragma unroll
+            for (int i = 0; i < CL; ++i) {
+                v[i] = vFd[i];
+                v[CL + i] = 0.f;
+            }
+            ReduceScatter<2 * CL, 16>::run(v, lane);
+            acc_fc += double(v[0]);
+            if (Wg == NWt - 1) {
+                acc_sfc_dir += double(warp_sum(dsfc));
+                acc_sfc_dn += double(warp_sum(fd_bot));
+                acc_sfc_up += double(warp_sum(fmaf(fd_bot, alb_in, src_in)));
+            }
+        }
 
         // ---- R3 composite (Fraw bottom -> top of chunk) ----
         {
@@ -861,6 +905,37 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
     }
 
     // ---- outputs ----
+    if (FLUX) {
+        const int v = lane >> 1;
+        const double g0_cp = 9.80665 / 1004.64;
+        if ((lane & 1) == 0) {
+            if (v < CL) {
+                const int j = j0 + w * CL + v;
+                if (j < nlay) {
+                    const size_t o = icol + size_t(top_at_1 ? j : nlay - j) * ncol;
+                    const double dn = acc_fc + acc_fa;
+                    out.flux_up[o] = float(acc_fb);
+                    out.flux_dn[o] = float(dn);
+                    out.flux_dir[o] = float(acc_fa);
+                    out.flux_net[o] = float(dn - acc_fb);
+                }
+            } else {
+                const int jl = w * CL + v - CL, j = j0 + jl;
+                if (j < nlay) {
+                    const size_t o = icol + size_t(top_at_1 ? j : nlay - 1 - j) * ncol;
+                    out.heating_rate[o] = float(g0_cp * 86400.0 * (acc_fa + acc_fb) / double(st[jl].dp));
+                }
+            }
+        }
+        if (Wg == NWt - 1 && lane == 0) {
+            const size_t o = icol + size_t(top_at_1 ? nlay : 0) * ncol;
+            const double dn = acc_sfc_dn + acc_sfc_dir;
+            out.flux_up[o] = float(acc_sfc_up);
+            out.flux_dn[o] = float(dn);
+            out.flux_dir[o] = float(acc_sfc_dir);
+            out.flux_net[o] = float(dn - acc_sfc_up);
+        }
+    }
     {
         const int q = lane >> 3, jl = w * kCL + (lane & 7), j = j0 + jl;
         if (q < 3 && j < nlay) {
@@ -910,9 +985,12 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
                    const float* mu0, const float* tsi_scaling, const float* sfc_alb_dir, const float* sfc_alb_dif,
                    const float* seed_up, const float* seed_dn, const float* seed_dir, const float* seed_hr,
                    float* g_tlay, float* g_h2o, float* g_o3, float* g_lwp, float* g_iwp, float* g_rel, float* g_rei,
-                   float* g_alb_dir, float* g_alb_dif, void* stream)
+                   float* g_alb_dir, float* g_alb_dif, float* flux_up, float* flux_dn, float* flux_dir,
+                   float* flux_net, float* heating_rate, void* stream)
 {
     RB_CHECK_ARG(k && !k->info.is_longwave, "adjoint_sw: need a shortwave k-distribution");
+    const bool with_flux = flux_up != nullptr;
+    RB_CHECK_ARG(!with_flux || (flux_dn && flux_dir && flux_net && heating_rate), "forward_adjoint_sw: null flux array");
     RB_CHECK_ARG(ncol > 0 && nlay > 1, "adjoint_sw: ncol > 0 and nlay > 1 required");
     RB_CHECK_ARG(play && plev && tlay && mu0 && sfc_alb_dir && sfc_alb_dif, "adjoint_sw: null input array");
     RB_CHECK_ARG(!c || (lwp && iwp && rel && rei), "adjoint_sw: cloud arrays required with a cloud handle");
@@ -933,8 +1011,10 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     if (smem > 227 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_sw: shared memory need exceeds 227 KB");
     static bool attr = false;
     if (!attr) {
-        RB_CUDA(cudaFuncSetAttribute(sw_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
-                "adjoint_sw attribute");
+        RB_CUDA(cudaFuncSetAttribute(sw_adjoint_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     227 * 1024), "adjoint_sw attribute");
+        RB_CUDA(cudaFuncSetAttribute(sw_adjoint_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     227 * 1024), "adjoint_sw attribute");
         attr = true;
     }
     SwCloudArgs ca{};
@@ -945,7 +1025,8 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
         ca.present = 1;
         ca.delta = delta_cloud;
     }
-    const SwAdjOut out{g_tlay, g_h2o, g_o3, g_lwp, g_iwp, g_rel, g_rei, g_alb_dir, g_alb_dif};
+    const SwAdjOut out{g_tlay, g_h2o, g_o3, g_lwp, g_iwp, g_rel, g_rei, g_alb_dir, g_alb_dif,
+                       flux_up, flux_dn, flux_dir, flux_net, heating_rate};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(unsigned(ncol) * CS);
     cfg.blockDim = dim3(kWPC * 32);
@@ -958,7 +1039,7 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    RB_CUDA(cudaLaunchKernelEx(&cfg, sw_adjoint_kernel, v, gs, ca, ncol, nlay, CS, idx_o3, col_dry ? 0 : 1, play, plev,
+    RB_CUDA(cudaLaunchKernelEx(&cfg, with_flux ? sw_adjoint_kernel<true> : sw_adjoint_kernel<false>, v, gs, ca, ncol, nlay, CS, idx_o3, col_dry ? 0 : 1, play, plev,
                                tlay, col_dry, mu0, tsi_scaling, sfc_alb_dir, sfc_alb_dif, seed_up, seed_dn, seed_dir,
                                seed_hr, out),
             "sw_adjoint_kernel launch");
@@ -980,5 +1061,22 @@ extern "C" int rrtmgp_b200_adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud
                                        delta_cloud, mu0, tsi_scaling, sfc_alb_dir, sfc_alb_dif, seed_flux_up,
                                        seed_flux_dn, seed_flux_dn_dir, seed_heating_rate, grad_tlay, grad_h2o, grad_o3,
                                        grad_lwp, grad_iwp, grad_rel, grad_rei, grad_sfc_alb_dir, grad_sfc_alb_dif,
-                                       stream);
+                                       nullptr, nullptr, nullptr, nullptr, nullptr, stream);
+}
+
+extern "C" int rrtmgp_b200_forward_adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
+        const float* play, const float* plev, const float* tlay, const float* col_dry,
+        const rrtmgp_b200_gas_conc* gases, int ngases, const float* lwp, const float* iwp, const float* rel,
+        const float* rei, int delta_cloud, const float* mu0, const float* tsi_scaling, const float* sfc_alb_dir,
+        const float* sfc_alb_dif, const float* seed_flux_up, const float* seed_flux_dn, const float* seed_flux_dn_dir,
+        const float* seed_heating_rate, float* grad_tlay, float* grad_h2o, float* grad_o3, float* grad_lwp,
+        float* grad_iwp, float* grad_rel, float* grad_rei, float* grad_sfc_alb_dir, float* grad_sfc_alb_dif,
+        float* flux_up, float* flux_dn, float* flux_dn_dir, float* flux_net, float* heating_rate, void* stream)
+{
+    RB_CHECK_ARG(flux_up, "forward_adjoint_sw: null flux array");
+    return rrtmgp_b200::adjoint_sw_f32(k, c, ncol, nlay, play, plev, tlay, col_dry, gases, ngases, lwp, iwp, rel, rei,
+                                       delta_cloud, mu0, tsi_scaling, sfc_alb_dir, sfc_alb_dif, seed_flux_up,
+                                       seed_flux_dn, seed_flux_dn_dir, seed_heating_rate, grad_tlay, grad_h2o, grad_o3,
+                                       grad_lwp, grad_iwp, grad_rel, grad_rei, grad_sfc_alb_dir, grad_sfc_alb_dif,
+                                       flux_up, flux_dn, flux_dn_dir, flux_net, heating_rate, stream);
 }

@@ -201,6 +201,13 @@ _SIGS = {
     "rrtmgp_b200_forward_sw_f32": (_I, [_P, _P, _I, _I, _P, _P, _P, _P, C.POINTER(GasConc), _I,
                                         _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
     "rrtmgp_b200_fp32_fma_probe": (_I, [_I, _I, _P, _P]),
+    "rrtmgp_b200_forward_adjoint_lw_f32": (_I, [_P, _P, _I, _I, _P, _P, _P, _P, _P, _P, C.POINTER(GasConc), _I,
+                                                _P, _P, _P, _P, _P, _P, _P, _P,
+                                                _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
+    "rrtmgp_b200_forward_adjoint_sw_f32": (_I, [_P, _P, _I, _I, _P, _P, _P, _P, C.POINTER(GasConc), _I,
+                                                _P, _P, _P, _P, _I, _P, _P, _P, _P,
+                                                _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
+                                                _P, _P, _P, _P, _P, _P]),
     "rrtmgp_b200_batch_create": (_I, [_P, _P, _P, _P, _I, _P, _I, C.POINTER(_P)]),
     "rrtmgp_b200_batch_destroy": (_I, [_P]),
     "rrtmgp_b200_batch_run": (_I, [_P, _I, _P]),

@@ -99,9 +99,12 @@ def longwave(fused, atm: dict, with_clouds: bool = True):
     return {"flux_up": up, "flux_dn": dn, "flux_net": net, "heating_rate": hr}
 
 
-def adjoint_lw(fused, atm: dict, seed_up=None, seed_dn=None, seed_hr=None, with_clouds: bool = True, chunk: int = 0):
+def adjoint_lw(fused, atm: dict, seed_up=None, seed_dn=None, seed_hr=None, with_clouds: bool = True, chunk: int = 0,
+               with_fluxes: bool = False):
     """Direct call of the longwave adjoint: dict of gradients of
-    sum(seed_up * flux_up + seed_dn * flux_dn + seed_hr * heating_rate)."""
+    sum(seed_up * flux_up + seed_dn * flux_dn + seed_hr * heating_rate).  with_fluxes: one
+    launch that also returns the forward fluxes (rrtmgp_b200_forward_adjoint_lw_f32), as
+    (fluxes, gradients)."""
     play = atm["play"]
     nlay, ncol = play.shape
     dev = play.device
@@ -113,20 +116,29 @@ def adjoint_lw(fused, atm: dict, seed_up=None, seed_dn=None, seed_hr=None, with_
     P = api._ptr
     arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay)
     cl = (lambda k: P(atm[k])) if c else (lambda k: None)
-    _abi.check(_abi.load().rrtmgp_b200_adjoint_lw_f32(
-        fused.base.klw.handle, c.handle if c else None, ncol, nlay, P(play), P(atm["plev"]), P(atm["tlay"]),
-        P(atm["tlev"]), P(atm["tsfc"]), None, arr, len(atm["gases"]), cl("lwp"), cl("iwp"), cl("rel"), cl("rei"),
-        P(atm["emis_sfc"]), P(seed_up), P(seed_dn), P(seed_hr), P(grads["tlay"]), P(grads["tlev"]),
-        P(grads["tsfc"]), P(grads["h2o"]), P(grads["o3"]), P(grads["lwp"]) if c else None,
-        P(grads["iwp"]) if c else None, P(grads["rel"]) if c else None, P(grads["rei"]) if c else None,
-        int(chunk), api._stream()))
-    return grads
+    args = [fused.base.klw.handle, c.handle if c else None, ncol, nlay, P(play), P(atm["plev"]), P(atm["tlay"]),
+            P(atm["tlev"]), P(atm["tsfc"]), None, arr, len(atm["gases"]), cl("lwp"), cl("iwp"), cl("rel"),
+            cl("rei"), P(atm["emis_sfc"]), P(seed_up), P(seed_dn), P(seed_hr), P(grads["tlay"]), P(grads["tlev"]),
+            P(grads["tsfc"]), P(grads["h2o"]), P(grads["o3"]), P(grads["lwp"]) if c else None,
+            P(grads["iwp"]) if c else None, P(grads["rel"]) if c else None, P(grads["rei"]) if c else None]
+    if not with_fluxes:
+        _abi.check(_abi.load().rrtmgp_b200_adjoint_lw_f32(*args, int(chunk), api._stream()))
+        return grads
+    fl = {k: torch.empty((nlay + 1, ncol), dtype=torch.float32, device=dev) for k in ("flux_up", "flux_dn", "flux_net")}
+    fl["heating_rate"] = torch.empty((nlay, ncol), dtype=torch.float32, device=dev)
+    _abi.check(_abi.load().rrtmgp_b200_forward_adjoint_lw_f32(
+        *args, P(fl["flux_up"]), P(fl["flux_dn"]), P(fl["flux_net"]), P(fl["heating_rate"]), int(chunk),
+        api._stream()))
+    return fl, grads
 
 
-def adjoint_sw(fused, atm: dict, seed_up=None, seed_dn=None, seed_dir=None, seed_hr=None, with_clouds: bool = True):
+def adjoint_sw(fused, atm: dict, seed_up=None, seed_dn=None, seed_dir=None, seed_hr=None, with_clouds: bool = True,
+               with_fluxes: bool = False):
     """Direct call of the shortwave adjoint: dict of gradients of sum(seed_up * flux_up +
     seed_dn * flux_dn + seed_dir * flux_dn_dir + seed_hr * heating_rate) w.r.t. tlay, h2o, o3,
-    lwp, iwp, rel, rei (nlay, ncol) and sfc_alb_dir, sfc_alb_dif (ncol, nband)."""
+    lwp, iwp, rel, rei (nlay, ncol) and sfc_alb_dir, sfc_alb_dif (ncol, nband).  with_fluxes:
+    one launch that also returns the forward fluxes (rrtmgp_b200_forward_adjoint_sw_f32), as
+    (fluxes, gradients)."""
     play = atm["play"]
     nlay, ncol = play.shape
     dev = play.device
@@ -140,14 +152,22 @@ def adjoint_sw(fused, atm: dict, seed_up=None, seed_dn=None, seed_dir=None, seed
     arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay)
     cl = (lambda k: P(atm[k])) if c else (lambda k: None)
     tsi = atm.get("tsi_scaling")
-    _abi.check(_abi.load().rrtmgp_b200_adjoint_sw_f32(
-        fused.base.ksw.handle, c.handle if c else None, ncol, nlay, P(play), P(atm["plev"]), P(atm["tlay"]), None,
-        arr, len(atm["gases"]), cl("lwp"), cl("iwp"), cl("rel"), cl("rei"), int(fused.base.delta_cloud),
-        P(atm["mu0"]), P(tsi) if tsi is not None else None, P(atm["sfc_alb_dir"]), P(atm["sfc_alb_dif"]),
-        P(seed_up), P(seed_dn), P(seed_dir), P(seed_hr), P(grads["tlay"]), P(grads["h2o"]), P(grads["o3"]),
-        P(grads["lwp"]) if c else None, P(grads["iwp"]) if c else None, P(grads["rel"]) if c else None,
-        P(grads["rei"]) if c else None, P(grads["sfc_alb_dir"]), P(grads["sfc_alb_dif"]), api._stream()))
-    return grads
+    args = [fused.base.ksw.handle, c.handle if c else None, ncol, nlay, P(play), P(atm["plev"]), P(atm["tlay"]),
+            None, arr, len(atm["gases"]), cl("lwp"), cl("iwp"), cl("rel"), cl("rei"), int(fused.base.delta_cloud),
+            P(atm["mu0"]), P(tsi) if tsi is not None else None, P(atm["sfc_alb_dir"]), P(atm["sfc_alb_dif"]),
+            P(seed_up), P(seed_dn), P(seed_dir), P(seed_hr), P(grads["tlay"]), P(grads["h2o"]), P(grads["o3"]),
+            P(grads["lwp"]) if c else None, P(grads["iwp"]) if c else None, P(grads["rel"]) if c else None,
+            P(grads["rei"]) if c else None, P(grads["sfc_alb_dir"]), P(grads["sfc_alb_dif"])]
+    if not with_fluxes:
+        _abi.check(_abi.load().rrtmgp_b200_adjoint_sw_f32(*args, api._stream()))
+        return grads
+    fl = {k: torch.empty((nlay + 1, ncol), dtype=torch.float32, device=dev)
+          for k in ("flux_up", "flux_dn", "flux_dn_dir", "flux_net")}
+    fl["heating_rate"] = torch.empty((nlay, ncol), dtype=torch.float32, device=dev)
+    _abi.check(_abi.load().rrtmgp_b200_forward_adjoint_sw_f32(
+        *args, P(fl["flux_up"]), P(fl["flux_dn"]), P(fl["flux_dn_dir"]), P(fl["flux_net"]), P(fl["heating_rate"]),
+        api._stream()))
+    return fl, grads
 
 
 _SW_DIFF = ("tlay", "h2o", "o3", "lwp", "iwp", "rel", "rei", "sfc_alb_dir", "sfc_alb_dif")

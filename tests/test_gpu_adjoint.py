@@ -300,3 +300,37 @@ def test_sw_autograd_directional(oracle_mod, tables, gpu):
     eps = 1e-3
     fd = (shifted(eps) - shifted(-eps)) / (2 * eps)
     assert abs(ad - fd) <= 2e-3 * abs(fd), f"directional derivative: autograd {ad:.6e} vs FD {fd:.6e}"
+
+
+@pytest.mark.parametrize("nlay", [60, 200])
+def test_forward_adjoint_one_launch(tables, gpu, nlay):
+    """rrtmgp_b200_forward_adjoint_{lw,sw}_f32: the fluxes equal the fused forward's and the
+    gradients the adjoint-only launch's, to FP32 rounding (the same arithmetic compiled into
+    another kernel), for one CTA (60 layers) and a cluster of CTAs (200 layers)."""
+    import torch
+    from rrtmgp_b200.autodiff import adjoint_lw, adjoint_sw
+    from rrtmgp_b200.solver import Fused_solver, Radiation_solver, atm_to_device
+    base = Radiation_solver(tables["lw"], tables["sw"], tables["cloud_lw"], tables["cloud_sw"], S.ATM_GASES)
+    fused = Fused_solver(base)
+    ncol = 40
+    atm = atm_to_device(S.make_atmosphere(ncol, nlay, seed=71, clouds=True, top_at_1=nlay < 100), torch.float32, "cuda")
+    g = torch.Generator(device="cuda").manual_seed(3)
+    sd = {k: torch.randn(shape, generator=g, device="cuda") for k, shape in
+          (("up", (nlay + 1, ncol)), ("dn", (nlay + 1, ncol)), ("dir", (nlay + 1, ncol)), ("hr", (nlay, ncol)))}
+    for dom in ("lw", "sw"):
+        if dom == "lw":
+            ref_f = {k: v.clone() for k, v in fused.solve_lw(atm).items()}
+            ref_g = adjoint_lw(fused, atm, sd["up"], sd["dn"], sd["hr"])
+            f, gr = adjoint_lw(fused, atm, sd["up"], sd["dn"], sd["hr"], with_fluxes=True)
+        else:
+            ref_f = {k: v.clone() for k, v in fused.solve_sw(atm).items()}
+            ref_g = adjoint_sw(fused, atm, sd["up"], sd["dn"], sd["dir"], sd["hr"])
+            f, gr = adjoint_sw(fused, atm, sd["up"], sd["dn"], sd["dir"], sd["hr"], with_fluxes=True)
+        torch.cuda.synchronize()
+        for k in ref_f:
+            d = float((f[k] - ref_f[k]).abs().max())
+            assert torch.isfinite(f[k]).all() and d < 2e-3, f"{dom} {k}: {d:.3e}"
+        for k in ref_g:
+            scale = float(ref_g[k].abs().max()) + 1e-30
+            d = float((gr[k] - ref_g[k]).abs().max()) / scale
+            assert d < 1e-4, f"{dom} grad {k}: {d:.3e}"

@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--batched-grids", type=int, default=512,
                     help="uneven-grid batch: grids with ncol U{64..4096}, nlay U{40..200} (0: skip)")
     ap.add_argument("--batched-steps", type=int, default=3)
+    ap.add_argument("--batched-no-autotune", action="store_true",
+                    help="use the built-in tile-shape heuristic instead of the autotuner")
     ap.add_argument("--deep-ncol", type=int, default=262144,
                     help="deep-column forward + adjoint: ncol (0: skip)")
     ap.add_argument("--deep-nlay", type=int, default=256)
@@ -288,7 +290,7 @@ def batched_bench(args, solver, dev, stream, flush, rank, world, dist):
                           torch.float32, dev) for c, l in zip(ncols, nlays)]
     bf = Batched_forward(solver, atms)
     t0 = time.perf_counter()
-    plan = bf.autotune(reps=2)
+    plan = bf.plan() if args.batched_no_autotune else bf.autotune(reps=2)
     tune_s = time.perf_counter() - t0
     res = {}
     outs = {}

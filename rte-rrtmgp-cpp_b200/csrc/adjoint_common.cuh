@@ -61,7 +61,9 @@ __device__ __forceinline__ float interpolate1D_slope(float val, float offset, fl
 
 // Derivative record of band b at layer state s (cg: gas columns of the layer, stride cgs;
 // scal: the forward record's minor scalings).  idx_o3: col_gas index of o3 (0: absent).
-// cd_internal: col_dry was computed from h2o and the level pressures.
+// cd_internal: col_dry was computed from h2o and the level pressures.  PFRAC: also the
+// Planck-fraction weights pT/pH/pO (longwave only).
+template <bool PFRAC = true>
 __device__ __forceinline__ void build_drec(const KdistView<float>& k, DRec& D, const LayerState& s, const float* cg,
                                            int cgs, int b, const float* scal, int idx_o3, int cd_internal)
 {
@@ -122,8 +124,13 @@ __device__ __forceinline__ void build_drec(const KdistView<float>& k, DRec& D, c
         }
         fmT[2 * it] = sg * (1.f - feta) / delta;
         fmT[2 * it + 1] = sg * feta / delta;
-        if (it == 0) { D.wT0 = wT; D.pT0 = pT; D.wH0 = wX[0]; D.wO0 = wX[1]; D.pH0 = pX[0]; D.pO0 = pX[1]; }
-        else         { D.wT1 = wT; D.pT1 = pT; D.wH1 = wX[0]; D.wO1 = wX[1]; D.pH1 = pX[0]; D.pO1 = pX[1]; }
+        if (it == 0) {
+            D.wT0 = wT; D.wH0 = wX[0]; D.wO0 = wX[1];
+            if (PFRAC) { D.pT0 = pT; D.pH0 = pX[0]; D.pO0 = pX[1]; }
+        } else {
+            D.wT1 = wT; D.wH1 = wX[0]; D.wO1 = wX[1];
+            if (PFRAC) { D.pT1 = pT; D.pH1 = pX[0]; D.pO1 = pX[1]; }
+        }
     }
     D.fmT = make_float4(fmT[0], fmT[1], fmT[2], fmT[3]);
     D.fmH = make_float4(fmX[0][0], fmX[0][1], fmX[0][2], fmX[0][3]);

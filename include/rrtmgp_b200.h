@@ -233,6 +233,43 @@ int rrtmgp_b200_cloud_optics_2str_f64(rrtmgp_b200_cloud c, int ncol, int nlay,
         double* tau, double* ssa, double* g, void* stream);
 
 /* ------------------------------------------------------------------------------------ */
+/* Aerosol optics (shortwave, two-stream).  Replaces Aerosol_optics_gpu                  */
+/* (include/Aerosol_optics.h:64-86, src_cuda/Aerosol_optics.cu:188-279) built by          */
+/* load_and_init_aerosol_optics (src_test/Radiation_solver.cu:366-401).  Host tables,     */
+/* double, C order = netCDF dimension order.                                              */
+/* ------------------------------------------------------------------------------------ */
+typedef struct rrtmgp_b200_aerosol_tables {
+    int nband, nhum, nphilic, nphobic;   /* band_sw, relative_humidity, hydrophilic (>= 5),  */
+                                         /* hydrophobic (>= 11)                              */
+    const double* rh_upper;              /* [nhum] "relative_humidity2", increasing          */
+    const double* mext_phobic;           /* (nphobic, nband) "mass_ext_sw_hydrophobic", m2/kg */
+    const double* ssa_phobic;            /* (nphobic, nband)                                 */
+    const double* g_phobic;              /* (nphobic, nband)                                 */
+    const double* mext_philic;           /* (nphilic, nhum, nband)                           */
+    const double* ssa_philic;
+    const double* g_philic;
+} rrtmgp_b200_aerosol_tables;
+
+typedef struct rrtmgp_b200_aerosol_t* rrtmgp_b200_aerosol;
+
+int rrtmgp_b200_aerosol_create(const rrtmgp_b200_aerosol_tables* t, rrtmgp_b200_aerosol* out);
+void rrtmgp_b200_aerosol_destroy(rrtmgp_b200_aerosol a);
+
+/* Aerosol_optics_gpu::aerosol_optics: tau, ssa, g (ncol, nlay, nband) of the 11 species
+ * aermr01 .. aermr11 (mass mixing ratios, kg/kg: sea salt 1-3, dust 1-3, hydrophilic and
+ * hydrophobic organic matter, black carbon 1-2, sulphate), passed as gas_conc entries with
+ * those names and shape (1,1), (1,nlay) or (ncol,nlay); rh (ncol, nlay) relative humidity
+ * as a fraction, plev (ncol, nlay+1).  Layer mass |dp| / 9.81 as the reference GPU kernel.
+ * Divergence: rh above the last rh_upper entry uses the last class (the reference reads
+ * past its table). */
+int rrtmgp_b200_aerosol_optics_f32(rrtmgp_b200_aerosol a, int ncol, int nlay,
+        const rrtmgp_b200_gas_conc* aerosols, int naerosols, const float* rh, const float* plev,
+        float* tau, float* ssa, float* g, void* stream);
+int rrtmgp_b200_aerosol_optics_f64(rrtmgp_b200_aerosol a, int ncol, int nlay,
+        const rrtmgp_b200_gas_conc* aerosols, int naerosols, const double* rh, const double* plev,
+        double* tau, double* ssa, double* g, void* stream);
+
+/* ------------------------------------------------------------------------------------ */
 /* Optical-property arithmetic (src_cuda/Optical_props.cu:93-165)                        */
 /* ------------------------------------------------------------------------------------ */
 /* Optical_props_2str_gpu::delta_scale with f = g^2 (optical_props_kernels.cu:139-160). */

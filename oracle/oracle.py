@@ -174,6 +174,37 @@ class CloudOptics:
         return {"tau": tau, "ssa": ssa, "g": g} if two_stream else {"tau": tau}
 
 
+AEROSOL_NAMES = tuple(f"aermr{i:02d}" for i in range(1, 12))
+
+
+def aerosol_optics(tables: dict, aerosols: dict, rh, plev):
+    """Aerosol optics (rrtmgp_oracle.cpp: oracle_aerosol_optics).  aerosols: aermr01 ..
+    aermr11, each (nlay, ncol), (nlay,) or scalar; rh (nlay, ncol); plev (nlay+1, ncol)."""
+    rh, plev = _f(rh), _f(plev)
+    nlay, ncol = rh.shape
+    ph = _f(tables["mass_ext_sw_hydrophobic"])
+    pl = _f(tables["mass_ext_sw_hydrophilic"])
+    nphobic, nband = ph.shape
+    nphilic, nhum = pl.shape[0], pl.shape[1]
+    fields = []
+    for name in AEROSOL_NAMES:
+        v = np.asarray(aerosols[name], dtype=np.float64)
+        if v.size == 1:
+            v = np.full((nlay, ncol), float(v.reshape(-1)[0]))
+        elif v.ndim == 1 or v.shape[-1] == 1:
+            v = np.repeat(v.reshape(nlay, 1), ncol, axis=1)
+        fields.append(_f(v))
+    ptrs = (_D * 11)(*[_p(f) for f in fields])
+    tau = np.empty((nband, nlay, ncol))
+    ssa, g = np.empty_like(tau), np.empty_like(tau)
+    keep = [_f(tables[k]) for k in ("relative_humidity2", "ssa_sw_hydrophobic", "asymmetry_sw_hydrophobic",
+                                    "ssa_sw_hydrophilic", "asymmetry_sw_hydrophilic")]
+    load().oracle_aerosol_optics(nband, nhum, nphilic, nphobic, _p(keep[0]), _p(ph), _p(keep[1]), _p(keep[2]),
+                                 _p(pl), _p(keep[3]), _p(keep[4]), ncol, nlay, ptrs, _p(rh), _p(plev), _p(tau),
+                                 _p(ssa), _p(g))
+    return {"tau": tau, "ssa": ssa, "g": g}
+
+
 def delta_scale(tau, ssa, g):
     load().oracle_delta_scale(int(tau.size), _p(tau), _p(ssa), _p(g))
 

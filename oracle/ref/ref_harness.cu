@@ -17,6 +17,7 @@
 
 #include "Array.h"
 #include "Cloud_optics.h"
+#include "Aerosol_optics.h"
 #include "Fluxes.h"
 #include "Gas_concs.h"
 #include "Gas_optics_rrtmgp.h"
@@ -341,6 +342,35 @@ int ref_fluxes(int ncol, int nlev, int nband, const int* band_lims, const double
         out(fy.get_bnd_flux_up(), bnd_up);
         out(fy.get_bnd_flux_dn(), bnd_dn);
         out(fy.get_bnd_flux_net(), bnd_net);
+    });
+}
+
+// Aerosol_optics_gpu::aerosol_optics (src_cuda/Aerosol_optics.cu:220-279), tables as
+// load_and_init_aerosol_optics builds them (src_test/Radiation_solver.cu:366-401: netCDF order
+// read into Fortran-order arrays of the reversed dimensions, band_lims_wvn left zero).
+int ref_aerosol_optics(const rrtmgp_b200_aerosol_tables* t, const rrtmgp_b200_gas_conc* aer, int naer, int ncol,
+                       int nlay, const double* rh, const double* plev, double* tau, double* ssa, double* g)
+{
+    return guarded([&] {
+        const int nb = t->nband, nh = t->nhum, npl = t->nphilic, nph = t->nphobic;
+        Array<double, 2> band_lims({2, nb});
+        auto rhu = host<double, 1>(t->rh_upper, {nh});
+        auto mp = host<double, 2>(t->mext_phobic, {nb, nph});
+        auto sp = host<double, 2>(t->ssa_phobic, {nb, nph});
+        auto gp = host<double, 2>(t->g_phobic, {nb, nph});
+        auto ml = host<double, 3>(t->mext_philic, {nb, nh, npl});
+        auto sl = host<double, 3>(t->ssa_philic, {nb, nh, npl});
+        auto gl = host<double, 3>(t->g_philic, {nb, nh, npl});
+        Aerosol_optics_gpu ao(band_lims, rhu, mp, sp, gp, ml, sl, gl);
+        Gas_concs gc = gas_concs(aer, naer, ncol, nlay);
+        Gas_concs_gpu gcg(gc);
+        Optical_props_2str_gpu ops(ncol, nlay, ao);
+        auto r = dev<double, 2>(rh, {ncol, nlay});
+        auto pl = dev<double, 2>(plev, {ncol, nlay + 1});
+        ao.aerosol_optics(gcg, r, pl, ops);
+        out(ops.get_tau(), tau);
+        out(ops.get_ssa(), ssa);
+        out(ops.get_g(), g);
     });
 }
 

@@ -52,6 +52,15 @@ class CloudTables(C.Structure):
     ]
 
 
+class AerosolTables(C.Structure):
+    _fields_ = [
+        ("nband", C.c_int), ("nhum", C.c_int), ("nphilic", C.c_int), ("nphobic", C.c_int),
+        ("rh_upper", c_double_p), ("mext_phobic", c_double_p), ("ssa_phobic", c_double_p),
+        ("g_phobic", c_double_p), ("mext_philic", c_double_p), ("ssa_philic", c_double_p),
+        ("g_philic", c_double_p),
+    ]
+
+
 class GasConc(C.Structure):
     _fields_ = [("name", C.c_char_p), ("vmr", C.c_void_p), ("dim1", C.c_int), ("dim2", C.c_int)]
 
@@ -152,6 +161,25 @@ def kdist_tables(d: dict):
     return t, k
 
 
+def aerosol_tables(d: dict):
+    """ctypes AerosolTables for an aerosol LUT dict in netCDF layout (the variables that
+    load_and_init_aerosol_optics reads); returns (struct, keep)."""
+    k = _Keep()
+    t = AerosolTables()
+    ph = np.asarray(d["mass_ext_sw_hydrophobic"])
+    pl = np.asarray(d["mass_ext_sw_hydrophilic"])
+    t.nphobic, t.nband = ph.shape
+    t.nphilic, t.nhum = pl.shape[0], pl.shape[1]
+    t.rh_upper = k.f64(d["relative_humidity2"])
+    t.mext_phobic = k.f64(ph)
+    t.ssa_phobic = k.f64(d["ssa_sw_hydrophobic"])
+    t.g_phobic = k.f64(d["asymmetry_sw_hydrophobic"])
+    t.mext_philic = k.f64(pl)
+    t.ssa_philic = k.f64(d["ssa_sw_hydrophilic"])
+    t.g_philic = k.f64(d["asymmetry_sw_hydrophilic"])
+    return t, k
+
+
 def cloud_tables(d: dict):
     k = _Keep()
     t = CloudTables()
@@ -201,6 +229,8 @@ _SIGS = {
     "rrtmgp_b200_forward_sw_f32": (_I, [_P, _P, _I, _I, _P, _P, _P, _P, C.POINTER(GasConc), _I,
                                         _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
     "rrtmgp_b200_fp32_fma_probe": (_I, [_I, _I, _P, _P]),
+    "rrtmgp_b200_aerosol_create": (_I, [C.POINTER(AerosolTables), C.POINTER(_P)]),
+    "rrtmgp_b200_aerosol_destroy": (None, [_P]),
     "rrtmgp_b200_forward_adjoint_lw_f32": (_I, [_P, _P, _I, _I, _P, _P, _P, _P, _P, _P, C.POINTER(GasConc), _I,
                                                 _P, _P, _P, _P, _P, _P, _P, _P,
                                                 _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
@@ -239,6 +269,7 @@ _FP_SIGS = {
     "fluxes_broadband": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P],
     "fluxes_byband": [_P, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P],
     "heating_rate": [_I, _I, _P, _P, _P, _P, _P],
+    "aerosol_optics": [_P, _I, _I, C.POINTER(GasConc), _I, _P, _P, _P, _P, _P, _P],
 }
 
 

@@ -210,6 +210,37 @@ class Cloud_optics:
         return {"tau": tau}
 
 
+AEROSOL_NAMES = tuple(f"aermr{i:02d}" for i in range(1, 12))
+
+
+class Aerosol_optics:
+    """Aerosol_optics_gpu band LUT aerosol optics (include/Aerosol_optics.h:64-86)."""
+
+    def __init__(self, tables: dict):
+        lib = _abi.load()
+        t, keep = _abi.aerosol_tables(tables)
+        h = C.c_void_p()
+        check(lib.rrtmgp_b200_aerosol_create(C.byref(t), C.byref(h)))
+        self.handle = h
+        self.nband = t.nband
+
+    def __del__(self, _release=_release):
+        if getattr(self, "handle", None) is not None:
+            _release("rrtmgp_b200_aerosol_destroy", self.handle)
+            self.handle = None
+
+    def aerosol_optics(self, aerosols: dict, rh, plev):
+        """aerosols: {aermr01 .. aermr11: tensor (nlay, ncol), (nlay,) or scalar}; rh (nlay,
+        ncol); plev (nlay+1, ncol).  Returns tau, ssa, g (nband, nlay, ncol)."""
+        nlay, ncol = rh.shape
+        arr, keep = Gas_optics_rrtmgp._gases(aerosols, ncol, nlay)
+        tau = _empty((self.nband, nlay, ncol), rh)
+        ssa, g = _empty(tau.shape, rh), _empty(tau.shape, rh)
+        _call("aerosol_optics", rh, self.handle, ncol, nlay, arr, len(aerosols), _ptr(rh), _ptr(plev), _ptr(tau),
+              _ptr(ssa), _ptr(g), _stream())
+        return {"tau": tau, "ssa": ssa, "g": g}
+
+
 def delta_scale(tau, ssa, g):
     """Optical_props_2str_gpu::delta_scale, in place."""
     ngpt, nlay, ncol = tau.shape

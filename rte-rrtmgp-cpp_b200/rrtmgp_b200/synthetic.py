@@ -292,6 +292,38 @@ def make_cloud_luts(kind: str, seed: int = 7):
     )
 
 
+def make_aerosol_luts(seed: int = 11, nband: int = 14, nhum: int = 12, nphilic: int = 5, nphobic: int = 14):
+    """Aerosol optics tables with the variables and dimension order that
+    load_and_init_aerosol_optics reads (src_test/Radiation_solver.cu:366-401):
+    relative_humidity2 (nhum, increasing, last 1), mass_ext/ssa/asymmetry_sw_hydrophobic
+    (hydrophobic, band_sw) and _hydrophilic (hydrophilic, relative_humidity, band_sw).
+    Hydrophilic extinction grows with humidity; mass extinction is in m2/kg."""
+    rng = np.random.default_rng(seed)
+    rh2 = np.concatenate([np.linspace(0.1, 0.9, nhum - 3), [0.95, 0.98, 1.0]])
+    growth = (1.0 + 2.0 * rh2 ** 4)[None, :, None]
+    return {
+        "relative_humidity2": rh2,
+        "mass_ext_sw_hydrophobic": rng.uniform(2.0e2, 6.0e3, (nphobic, nband)),
+        "ssa_sw_hydrophobic": rng.uniform(0.6, 0.99, (nphobic, nband)),
+        "asymmetry_sw_hydrophobic": rng.uniform(0.5, 0.8, (nphobic, nband)),
+        "mass_ext_sw_hydrophilic": rng.uniform(1.0e3, 8.0e3, (nphilic, 1, nband)) * growth,
+        "ssa_sw_hydrophilic": np.minimum(rng.uniform(0.85, 0.99, (nphilic, nhum, nband)), 1.0),
+        "asymmetry_sw_hydrophilic": rng.uniform(0.6, 0.8, (nphilic, nhum, nband)),
+    }
+
+
+def make_aerosols(play: np.ndarray, seed: int = 12):
+    """Mass mixing ratios aermr01 .. aermr11 (kg/kg, (nlay, ncol)) decaying with height, and a
+    relative humidity field in [0, 1] (higher near the surface), for the layers of play."""
+    rng = np.random.default_rng(seed)
+    z = 7.0 * np.log(1.0e5 / play)   # km
+    shape = np.exp(-z / 2.0)
+    base = [2e-9, 8e-9, 1e-9, 5e-9, 1e-8, 4e-9, 3e-9, 2e-9, 5e-10, 5e-10, 6e-9]
+    aer = {f"aermr{i + 1:02d}": base[i] * shape * rng.lognormal(0.0, 0.5, play.shape) for i in range(11)}
+    rh = np.clip(0.2 + 0.7 * shape + rng.normal(0.0, 0.1, play.shape), 0.0, 1.0)
+    return aer, rh
+
+
 def make_atmosphere(ncol: int, nlay: int, seed: int = 42, clouds: bool = True,
                     nband_lw: int = 16, nband_sw: int = 14, top_at_1: bool = True):
     """Synthetic atmosphere in the reference layouts (column fastest; numpy (nlay, ncol)).

@@ -64,6 +64,13 @@ def flux_inputs():
     return tuple(rng.uniform(0, 20, (224, NLAY + 1, NCOL)) for _ in range(3))
 
 
+def aerosol_inputs(atm):
+    """Mixing ratios aermr01 .. aermr11 and relative humidity of the aerosol case."""
+    aer, rh = S.make_aerosols(atm["play"], seed=108)
+    aer["aermr05"] = np.array([3e-9])
+    return aer, rh
+
+
 def D(a):
     return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
 
@@ -177,6 +184,17 @@ def main(outdir: Path):
                            P(up), P(dn), P(dr)))
         np.savez_compressed(outdir / f"{name}.npz", alb_dir=alb, alb_dif=albf, mu0=mu0, flux_up=up, flux_dn=dn,
                             flux_dir=dr)
+
+    # Aerosol optics (shortwave) on seeded synthetic tables and mixing ratios, bottom-up
+    # column order, one species given as a scalar.
+    aer_tab, keep_aer = _abi.aerosol_tables(S.make_aerosol_luts())
+    atm = S.make_atmosphere(NCOL, NLAY, seed=107, clouds=False, top_at_1=False)
+    aer, rh = aerosol_inputs(atm)
+    arr, keep = gas_array(aer)
+    o = {k: np.empty((14, NLAY, NCOL)) for k in ("tau", "ssa", "g")}
+    chk(lib.ref_aerosol_optics(C.byref(aer_tab), arr, len(aer), NCOL, NLAY, P(D(rh)), P(D(atm["plev"])),
+                               P(o["tau"]), P(o["ssa"]), P(o["g"])))
+    np.savez_compressed(outdir / "aerosol_sw.npz", **o)
 
     # Flux reductions.
     gu, gd, gr = flux_inputs()

@@ -1,0 +1,108 @@
+"""Aerosol optics (Aerosol_optics_gpu, src_cuda/Aerosol_optics.cu): oracle checks on the CPU and
+GPU parity of the FP64 and FP32 kernels against the oracle."""
+import numpy as np
+import pytest
+
+from rrtmgp_b200 import synthetic as S
+
+
+def _case(ncol=7, nlay=9, top_at_1=True, seed=3):
+    atm = S.make_atmosphere(ncol, nlay, seed=seed, clouds=False, top_at_1=top_at_1)
+    aer, rh = S.make_aerosols(atm["play"], seed=seed + 1)
+    return atm, aer, rh
+
+
+def test_oracle_aerosol_by_hand(oracle_mod):
+    """One species at a time against a direct numpy evaluation of the table look-up."""
+    t = S.make_aerosol_luts()
+    atm, aer, rh = _case()
+    plev = atm["plev"]
+    dpg = np.abs(plev[:-1] - plev[1:]) / 9.81
+    ihum = np.minimum(np.searchsorted(t["relative_humidity2"], rh, side="left"), len(t["relative_humidity2"]) - 1)
+    # name -> (hydrophilic?, 0-based type), as in the reference kernel
+    spec = {"aermr01": (1, 0), "aermr02": (1, 1), "aermr03": (1, 2), "aermr04": (0, 0), "aermr05": (0, 7),
+            "aermr06": (0, 5), "aermr07": (1, 3), "aermr08": (0, 9), "aermr09": (0, 10), "aermr10": (0, 10),
+            "aermr11": (1, 4)}
+    zero = {k: np.zeros_like(v) for k, v in aer.items()}
+    for name, (phil, typ) in spec.items():
+        one = dict(zero)
+        one[name] = aer[name]
+        out = oracle_mod.aerosol_optics(t, one, rh, plev)
+        for b in (0, 5, 13):
+            if phil:
+                me = t["mass_ext_sw_hydrophilic"][typ][ihum, b]
+                sa = t["ssa_sw_hydrophilic"][typ][ihum, b]
+                ga = t["asymmetry_sw_hydrophilic"][typ][ihum, b]
+            else:
+                me = t["mass_ext_sw_hydrophobic"][typ, b]
+                sa = t["ssa_sw_hydrophobic"][typ, b]
+                ga = t["asymmetry_sw_hydrophobic"][typ, b]
+            tau = aer[name] * dpg * me
+            eps = np.finfo(np.float64).eps
+            ts = tau * sa
+            np.testing.assert_allclose(out["tau"][b], tau, rtol=1e-13)
+            np.testing.assert_allclose(out["ssa"][b], ts / np.maximum(tau, eps), rtol=1e-12)
+            np.testing.assert_allclose(out["g"][b], ts * ga / np.maximum(ts, eps), rtol=1e-12)
+
+
+def test_oracle_aerosol_zero_and_clamp(oracle_mod):
+    t = S.make_aerosol_luts()
+    atm, aer, rh = _case()
+    zero = {k: np.zeros_like(v) for k, v in aer.items()}
+    out = oracle_mod.aerosol_optics(t, zero, rh, atm["plev"])
+    assert not out["tau"].any() and not out["ssa"].any() and not out["g"].any()
+    # rh above the table's last class uses the last class
+    hi = oracle_mod.aerosol_optics(t, aer, np.full_like(rh, 1.5), atm["plev"])
+    top = oracle_mod.aerosol_optics(t, aer, np.full_like(rh, 1.0), atm["plev"])
+    np.testing.assert_array_equal(hi["tau"], top["tau"])
+    # orientation: |dp| gives the same optics for a flipped column
+    atm2, aer2, rh2 = _case(top_at_1=False)
+    a = oracle_mod.aerosol_optics(t, aer, rh, atm["plev"])
+    b = oracle_mod.aerosol_optics(t, {k: v[::-1].copy() for k, v in aer.items()}, rh[::-1].copy(),
+                                  atm["plev"][::-1].copy())
+    np.testing.assert_allclose(a["tau"], b["tau"][:, ::-1], rtol=1e-14)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+@pytest.mark.parametrize("profile", [False, True])
+def test_aerosol_gpu_matches_oracle(oracle_mod, gpu, dtype, profile):
+    import torch
+    from rrtmgp_b200 import api
+    t = S.make_aerosol_luts()
+    atm, aer, rh = _case(ncol=33, nlay=20)
+    if profile:   # (nlay,) profiles and one scalar broadcast over the columns
+        aer = {k: (v[:, 0].copy() if i % 2 else v) for i, (k, v) in enumerate(aer.items())}
+        aer["aermr05"] = np.array([3e-9])
+    ref = oracle_mod.aerosol_optics(t, aer, rh, atm["plev"])
+    dt = getattr(torch, dtype)
+    ao = api.Aerosol_optics(t)
+    d = {k: torch.as_tensor(np.ascontiguousarray(v), dtype=dt, device=gpu) for k, v in aer.items()}
+    got = ao.aerosol_optics(d, torch.as_tensor(rh, dtype=dt, device=gpu),
+                            torch.as_tensor(atm["plev"], dtype=dt, device=gpu))
+    torch.cuda.synchronize()
+    rtol = 1e-13 if dtype == "float64" else 2e-6
+    # ssa and g divide by max(tau, eps) and max(tau ssa, eps) with the precision's epsilon
+    # (as the reference builds): FP32 is compared where those do not bind
+    feps = np.finfo(np.float32).eps
+    masks = {"tau": np.ones(ref["tau"].shape, bool), "ssa": ref["tau"] > 2 * feps,
+             "g": ref["tau"] * ref["ssa"] > 2 * feps}
+    for k in ("tau", "ssa", "g"):
+        g = got[k].double().cpu().numpy()
+        m = masks[k] if dtype == "float32" else masks["tau"]
+        assert m.any()
+        np.testing.assert_allclose(g[m], ref[k][m], rtol=rtol, atol=1e-30, err_msg=k)
+
+
+@pytest.mark.gpu
+def test_aerosol_missing_species(gpu):
+    import torch
+    from rrtmgp_b200 import _abi, api
+    t = S.make_aerosol_luts()
+    atm, aer, rh = _case()
+    aer.pop("aermr07")
+    ao = api.Aerosol_optics(t)
+    d = {k: torch.as_tensor(v, device=gpu) for k, v in aer.items()}
+    with pytest.raises(_abi.RrtmgpError) as e:
+        ao.aerosol_optics(d, torch.as_tensor(rh, device=gpu), torch.as_tensor(atm["plev"], device=gpu))
+    assert e.value.status == _abi.ERR_MISSING_GAS

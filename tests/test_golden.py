@@ -118,3 +118,12 @@ def test_flux_reductions_match_reference(oracle_mod, tables):
     first = bl[:, 0] - 1
     np.testing.assert_allclose(by["bnd_flux_up"] - up[first], ref["bnd_flux_up"], rtol=1e-12, atol=1e-12)
     np.testing.assert_allclose(by["bnd_flux_dn"] - dn[first], ref["bnd_flux_dn"], rtol=1e-12, atol=1e-12)
+
+
+def test_aerosol_optics_matches_reference(oracle_mod):
+    ref = load("aerosol_sw")
+    atm = S.make_atmosphere(NCOL, NLAY, seed=107, clouds=False, top_at_1=False)
+    aer, rh = G.aerosol_inputs(atm)
+    out = oracle_mod.aerosol_optics(S.make_aerosol_luts(), aer, rh, atm["plev"])
+    for k in ("tau", "ssa", "g"):
+        assert relerr(out[k], ref[k], 1e-12) < 1e-13, k

@@ -72,6 +72,16 @@ inline int cloud_1scl(rrtmgp_b200_cloud c, int ncol, int nlay, const float* lwp,
 inline int cloud_1scl(rrtmgp_b200_cloud c, int ncol, int nlay, const double* lwp, const double* iwp, const double* rl,
                       const double* ri, double* tau)
 { return rrtmgp_b200_cloud_optics_1scl_f64(c, ncol, nlay, lwp, iwp, rl, ri, tau, stream()); }
+inline int aerosol_optics(rrtmgp_b200_aerosol a, int ncol, int nlay, const rrtmgp_b200_gas_conc* aer, int naer,
+                          const float* rh, const float* plev, float* tau, float* ssa, float* g)
+{
+    return rrtmgp_b200_aerosol_optics_f32(a, ncol, nlay, aer, naer, rh, plev, tau, ssa, g, stream());
+}
+inline int aerosol_optics(rrtmgp_b200_aerosol a, int ncol, int nlay, const rrtmgp_b200_gas_conc* aer, int naer,
+                          const double* rh, const double* plev, double* tau, double* ssa, double* g)
+{
+    return rrtmgp_b200_aerosol_optics_f64(a, ncol, nlay, aer, naer, rh, plev, tau, ssa, g, stream());
+}
 inline int cloud_2str(rrtmgp_b200_cloud c, int ncol, int nlay, const float* lwp, const float* iwp, const float* rl,
                       const float* ri, float* tau, float* ssa, float* g)
 { return rrtmgp_b200_cloud_optics_2str_f32(c, ncol, nlay, lwp, iwp, rl, ri, tau, ssa, g, stream()); }

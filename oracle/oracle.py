@@ -299,10 +299,13 @@ def forward_lw(kd: GasOptics, cloud: CloudOptics | None, atm: dict, col_dry=None
     return fl
 
 
-def forward_sw(kd: GasOptics, cloud: CloudOptics | None, atm: dict, col_dry=None, delta_cloud=True):
+def forward_sw(kd: GasOptics, cloud: CloudOptics | None, atm: dict, col_dry=None, delta_cloud=True,
+               aerosol_tables: dict | None = None, delta_aerosol=False):
     """Reference SW sequence of Radiation_solver_shortwave::solve_gpu
     (src_test/Radiation_solver.cu:683-950): gas optics, toa_src x tsi_scaling, cloud 2str +
-    delta-scale added by band, rte_sw, broadband reduce, plus heating rates."""
+    delta-scale added by band, aerosol optics (+ delta-scale) added by band when
+    aerosol_tables is given (atm["aerosols"], atm["rh"]), rte_sw, broadband reduce, plus
+    heating rates."""
     go = kd.gas_optics_sw(atm["play"], atm["plev"], atm["tlay"], atm["gases"], col_dry)
     toa = go["toa_src"] * _f(atm["tsi_scaling"])[None, :]
     if cloud is not None:
@@ -310,6 +313,11 @@ def forward_sw(kd: GasOptics, cloud: CloudOptics | None, atm: dict, col_dry=None
         if delta_cloud:
             delta_scale(c["tau"], c["ssa"], c["g"])
         add_to(kd.band_lims, go, c)
+    if aerosol_tables is not None:
+        a = aerosol_optics(aerosol_tables, atm["aerosols"], atm["rh"], atm["plev"])
+        if delta_aerosol:
+            delta_scale(a["tau"], a["ssa"], a["g"])
+        add_to(kd.band_lims, go, a)
     up, dn, dr = rte_sw(kd.band_lims, go["tau"], go["ssa"], go["g"], atm["top_at_1"], atm["mu0"], toa,
                         atm["sfc_alb_dir"], atm["sfc_alb_dif"])
     fl = fluxes_broadband(up, dn, dr)

@@ -17,12 +17,16 @@ ATM_KEYS_2D = ("play", "plev", "tlay", "tlev", "lwp", "iwp", "rel", "rei")
 
 class Radiation_solver:
     def __init__(self, kdist_lw: dict, kdist_sw: dict, cloud_lw: dict | None, cloud_sw: dict | None,
-                 available_gases, delta_cloud: bool = True):
+                 available_gases, delta_cloud: bool = True, aerosol_sw: dict | None = None,
+                 delta_aerosol: bool = False):
         self.klw = api.Gas_optics_rrtmgp(kdist_lw, available_gases)
         self.ksw = api.Gas_optics_rrtmgp(kdist_sw, available_gases)
         self.clw = api.Cloud_optics(cloud_lw) if cloud_lw is not None else None
         self.csw = api.Cloud_optics(cloud_sw) if cloud_sw is not None else None
         self.delta_cloud = delta_cloud
+        # Aerosol_optics_gpu of Radiation_solver_shortwave (src_test/Radiation_solver.cu:664-680)
+        self.aer = api.Aerosol_optics(aerosol_sw) if aerosol_sw is not None else None
+        self.delta_aerosol = delta_aerosol
         self._bufs = {}
 
     def _buffers(self, key, like, ncol, nlay, kind):
@@ -89,9 +93,11 @@ class Radiation_solver:
             ncol, nlay, P(b["flux_up"]), P(b["flux_dn"]), P(atm["plev"]), P(b["heating_rate"]), s))
         return {k: b[k] for k in ("flux_up", "flux_dn", "flux_net", "heating_rate")}
 
-    def solve_sw(self, atm: dict, with_clouds: bool = True, top_at_1: bool = True):
+    def solve_sw(self, atm: dict, with_clouds: bool = True, top_at_1: bool = True, with_aerosols: bool = False):
         """atm additionally needs mu0 (ncol), sfc_alb_dir / sfc_alb_dif (ncol, nband) and
-        optionally tsi_scaling (ncol)."""
+        optionally tsi_scaling (ncol); with_aerosols: aerosols {aermr01 .. aermr11} and rh
+        (nlay, ncol), their optics (delta-scaled if delta_aerosol) added by band after the
+        clouds (switch_aerosol_optics, src_test/Radiation_solver.cu:794-807)."""
         from . import _abi
         play = atm["play"]
         nlay, ncol = play.shape
@@ -118,6 +124,14 @@ class Radiation_solver:
             _abi.check(getattr(lib, "rrtmgp_b200_add_to_2str" + sfx)(
                 self.ksw.bands.handle, ncol, nlay, P(b["tau"]), P(b["ssa"]), P(b["g"]), P(b["c_tau"]),
                 P(b["c_ssa"]), P(b["c_g"]), nb, s))
+        if with_aerosols:
+            assert self.aer is not None, "solver built without aerosol tables"
+            a = self.aer.aerosol_optics(atm["aerosols"], atm["rh"], atm["plev"])
+            if self.delta_aerosol:
+                api.delta_scale(a["tau"], a["ssa"], a["g"])
+            _abi.check(getattr(lib, "rrtmgp_b200_add_to_2str" + sfx)(
+                self.ksw.bands.handle, ncol, nlay, P(b["tau"]), P(b["ssa"]), P(b["g"]), P(a["tau"]),
+                P(a["ssa"]), P(a["g"]), nb, s))
         import ctypes as C
         _abi.check(getattr(lib, "rrtmgp_b200_rte_sw" + sfx)(
             self.ksw.bands.handle, ncol, nlay, int(top_at_1), P(b["tau"]), P(b["ssa"]), P(b["g"]), P(atm["mu0"]),

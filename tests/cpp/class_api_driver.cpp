@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "Aerosol_optics.h"
 #include "Cloud_optics.h"
 #include "Fluxes.h"
 #include "Gas_optics_rrtmgp.h"
@@ -131,6 +132,12 @@ Gas_concs make_gases(int ngas, const char* const* names, const double* const* vm
 void out2(const Array_gpu<Float, 2>& a, double* o)
 {
     const Array<Float, 2> h(a);
+    for (int i = 0; i < h.size(); ++i) o[i] = double(h.v()[i]);
+}
+
+void out3(const Array_gpu<Float, 3>& a, double* o)
+{
+    const Array<Float, 3> h(a);
     for (int i = 0; i < h.size(); ++i) o[i] = double(h.v()[i]);
 }
 
@@ -284,6 +291,33 @@ int class_api_missing_gas_throws(const rrtmgp_b200_kdist_tables* tk, char* err, 
     } catch (const std::runtime_error& e) {
         fail(e, err, errlen);
         return 0;
+    }
+}
+
+// Aerosol optics through Aerosol_optics_gpu, tables as load_and_init_aerosol_optics builds them
+// (src_test/Radiation_solver.cu:366-401); the species are Aerosol_concs entries aermr01 ..
+// aermr11.  tau, ssa, g (ncol, nlay, nband).
+int class_api_aerosol_optics(const rrtmgp_b200_aerosol_tables* ta, int ncol, int nlay, const double* rh_in,
+                             const double* plev_in, int naer, const char* const* names, const double* const* mmr,
+                             const int* dims, double* tau, double* ssa, double* g, char* err, int errlen)
+{
+    try {
+        const int nb = ta->nband, nh = ta->nhum, npl = ta->nphilic, nph = ta->nphobic;
+        Aerosol_optics_gpu aerosol(Array<Float, 2>({2, nb}), farr<1>(ta->rh_upper, {nh}),
+                                   farr<2>(ta->mext_phobic, {nb, nph}), farr<2>(ta->ssa_phobic, {nb, nph}),
+                                   farr<2>(ta->g_phobic, {nb, nph}), farr<3>(ta->mext_philic, {nb, nh, npl}),
+                                   farr<3>(ta->ssa_philic, {nb, nh, npl}), farr<3>(ta->g_philic, {nb, nh, npl}));
+        const Aerosol_concs concs = make_gases(naer, names, mmr, dims);
+        Aerosol_concs_gpu concs_gpu(concs);
+        Optical_props_2str_gpu props(ncol, nlay, aerosol);
+        aerosol.aerosol_optics(concs_gpu, Array_gpu<Float, 2>(farr<2>(rh_in, {ncol, nlay})),
+                               Array_gpu<Float, 2>(farr<2>(plev_in, {ncol, nlay + 1})), props);
+        out3(props.get_tau(), tau);
+        out3(props.get_ssa(), ssa);
+        out3(props.get_g(), g);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e, err, errlen);
     }
 }
 

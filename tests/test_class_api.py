@@ -34,8 +34,9 @@ def _driver(fbytes):
 
 def test_headers_compile_both_precisions(tmp_path):
     src = tmp_path / "t.cpp"
-    src.write_text("".join(f'#include "{h}"\n' for h in ("Gas_optics_rrtmgp.h", "Cloud_optics.h", "Rte_lw.h",
-                                                          "Rte_sw.h", "Fluxes.h")) + "int main() { return 0; }\n")
+    src.write_text("".join(f'#include "{h}"\n' for h in ("Gas_optics_rrtmgp.h", "Cloud_optics.h", "Aerosol_optics.h",
+                                                          "Rte_lw.h", "Rte_sw.h", "Fluxes.h")) +
+                   "int main() { return 0; }\n")
     for flag in ([], ["-DRTE_USE_SP"]):
         subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", *flag,
                         f"-I{REPO / 'include' / 'cpp'}", "-I/usr/local/cuda/include", str(src)], check=True)
@@ -142,3 +143,32 @@ def test_class_api_missing_key_species_throws(tables, gpu):
     err = C.create_string_buffer(512)
     assert lib.class_api_missing_gas_throws(C.byref(kt), err, 512) == 0
     assert "missing" in err.value.decode().lower()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fbytes", [8, 4])
+def test_aerosol_optics_class(oracle_mod, gpu, fbytes):
+    """Aerosol_optics_gpu::aerosol_optics (Aerosol_concs with profile and field species)
+    against the oracle."""
+    lib = _driver(fbytes)
+    tab = S.make_aerosol_luts()
+    ta, keep_t = _abi.aerosol_tables(tab)
+    ncol, nlay = 6, 15
+    atm = S.make_atmosphere(ncol, nlay, seed=61, clouds=False)
+    aer, rh = S.make_aerosols(atm["play"], seed=62)
+    aer["aermr03"] = aer["aermr03"][:, 0].copy()   # a profile, broadcast over the columns
+    ref = oracle_mod.aerosol_optics(tab, aer, rh, atm["plev"])
+    args, keep = _gas_args({"gases": {k: (v[:, None] if v.ndim == 1 else v) for k, v in aer.items()}})
+    out = {k: np.empty((14, nlay, ncol)) for k in ("tau", "ssa", "g")}
+    err = C.create_string_buffer(256)
+    P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    rh_c = np.ascontiguousarray(rh)
+    pl_c = np.ascontiguousarray(atm["plev"])
+    st = lib.class_api_aerosol_optics(C.byref(ta), ncol, nlay, P(rh_c), P(pl_c), *args, P(out["tau"]),
+                                      P(out["ssa"]), P(out["g"]), err, 256)
+    assert st == 0, err.value.decode()
+    feps = np.finfo(np.float32 if fbytes == 4 else np.float64).eps
+    rtol = 1e-12 if fbytes == 8 else 2e-6
+    m = {"tau": np.ones(out["tau"].shape, bool), "ssa": ref["tau"] > 2 * feps, "g": ref["tau"] * ref["ssa"] > 2 * feps}
+    for k in out:
+        np.testing.assert_allclose(out[k][m[k]], ref[k][m[k]], rtol=rtol, atol=1e-30, err_msg=k)

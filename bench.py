@@ -737,6 +737,35 @@ def main():
         del atm64
         solver._bufs = {k: v for k, v in solver._bufs.items() if k[0][2] != torch.float64}
 
+    # Aerosol optics (the SW band LUT by relative humidity): one launch over the bench columns;
+    # HBM-bound streaming (13 (ncol, nlay) fields in, tau/ssa/g per band out).
+    aer_line = None
+    if args.path == "fused":
+        from rrtmgp_b200 import api
+        aer_np, rh_np = S.make_aerosols(atm_np["play"], seed=args.seed + 9)
+        ao = api.Aerosol_optics(S.make_aerosol_luts())
+        aer_t = {k: torch.as_tensor(v, dtype=torch.float32, device=dev) for k, v in aer_np.items()}
+        rh_t = torch.as_tensor(rh_np, dtype=torch.float32, device=dev)
+        for _ in range(3):
+            ao.aerosol_optics(aer_t, rh_t, atm["plev"])
+        torch.cuda.synchronize()
+        ev = [evpair() for _ in range(5)]
+        for a, b in ev:
+            flush.zero_()
+            a.record(stream)
+            ao.aerosol_optics(aer_t, rh_t, atm["plev"])
+            b.record(stream)
+        torch.cuda.synchronize()
+        ms = float(np.median([a.elapsed_time(b) for a, b in ev]))
+        nb = ao.nband
+        nbytes = 4 * args.ncol * (13 * args.nlay + 1 + 3 * nb * args.nlay)
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        aer_line = {"workload": f"aerosol optics, 11 species, ncol={args.ncol}, nlay={args.nlay}, {nb} bands",
+                    "ms": ms, "columns_per_s": args.ncol / (ms * 1e-3),
+                    "roofline": {"bound": "hbm", "algorithmic_bytes": nbytes, "achieved": gbs, "peak": hbm_peak,
+                                 "unit": "GB/s", "frac": gbs / hbm_peak, "peak_source": peak_kind}}
+        del aer_t, rh_t
+
     deep = None
     if args.path == "fused" and args.deep_ncol > 0 and not args.no_adjoint:
         deep = deep_bench(args, solver, fused, dev, stream, flush, rank, world, dist)
@@ -771,6 +800,7 @@ def main():
             "forward_adjoint": fwd_adj,
             "batched": batched,
             "deep_forward_adjoint": deep,
+            "aerosol_optics": aer_line,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

@@ -260,7 +260,7 @@ size_t team_smem_bytes(const rrtmgp_b200_batch_t* b, int domain, int nlay, int c
 {
     const KdistView<float>& v = b->k[domain]->v32;
     const int W = ceil_div_i(nlay, cl);
-    const SmemLayout L = domain == 0 ? smem_layout(nlay, v.ngas, v.nband, 1, W, 1, cl, v.max_group_bands)
+    const SmemLayout L = domain == 0 ? smem_layout(nlay, v.ngas, v.nband, 1, W, 2, cl, v.max_group_bands)
                                      : smem_layout(nlay, v.ngas, v.nband, 0, W, 3, cl, v.max_group_bands);
     return align16(L.total);
 }

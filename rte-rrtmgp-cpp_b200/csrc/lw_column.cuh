@@ -100,13 +100,15 @@ __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<
     static_assert(CL == 8 || CL == 16, "chunk length");
     const int lane = threadIdx.x & 31;
     const int nband = k.nband;
-    const SmemLayout SL = smem_layout(io.nlay(), k.ngas, nband, 1, cx.nwarps(), 1, CL, k.max_group_bands);
+    const SmemLayout SL = smem_layout(io.nlay(), k.ngas, nband, 1, cx.nwarps(), 2, CL, k.max_group_bands);
     unsigned char* const smem_raw = cx.smem();
     LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
     float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
     float* sm_cld = reinterpret_cast<float*>(smem_raw + SL.cloud);
-    float4* sm_maps = reinterpret_cast<float4*>(smem_raw + SL.maps);
-    float* sm_sfc = reinterpret_cast<float*>(smem_raw + SL.sfc);
+    // chunk maps and surface source are double-buffered by group parity, so a warp can
+    // start the next group while others still read this group's (one barrier per group)
+    float4* const sm_maps0 = reinterpret_cast<float4*>(smem_raw + SL.maps);
+    float* const sm_sfc0 = reinterpret_cast<float*>(smem_raw + SL.sfc);
     Rec* recs = reinterpret_cast<Rec*>(smem_raw + SL.recs) + cx.warp() * CL * k.max_group_bands;
 
     bool top_at_1;
@@ -139,6 +141,8 @@ __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<
 
     for (int gg = 0; gg < k.ngroups; ++gg) {
         const int nlay = io.nlay();
+        float4* const sm_maps = sm_maps0 + (gg & 1) * cx.nwarps() * 32;
+        float* const sm_sfc = sm_sfc0 + (gg & 1) * 32;
         const int g = 32 * gg + lane;
         const bool gv = g < ngpt;
         const int b0 = k.group_band0[gg];
@@ -230,7 +234,6 @@ __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<
             acc_bot_up += double(warp_sum(S));
             acc_bot_dn += double(warp_sum(rd));
         }
-        cx.sync();
     }
 
     // Outputs.  Fluxes = 2 pi w * (sum of radiances) with w = 0.5.

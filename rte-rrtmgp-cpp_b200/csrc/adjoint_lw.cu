@@ -143,12 +143,14 @@ __device__ __forceinline__ Tp* remote(cg::cluster_group& cl, Tp* p, int rank)
     return cl.map_shared_rank(p, rank);
 }
 
+// CL = 16: at most 8 warps (128 layers) with up to 255 registers per thread; CL = 8: up to 16
+// warps per CTA at 128 registers.
 // One column per cluster of CS CTAs (CLUSTER = false: CS = 1, a plain launch compiled without
 // the cluster code).  CTA r of the cluster owns the layers [r LPC, (r + 1) LPC), LPC = NWc CL,
 // as NWc warps of CL layers; chunk maps and the surface source are pushed to every CTA of the
 // cluster through distributed shared memory.
 template <int CL, bool CLUSTER, bool FLUX>
-__global__ void __launch_bounds__(512)
+__global__ void __launch_bounds__(CL == 16 ? 256 : 512, 1)
 lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjCloud cld, int ncol, int nlay, int CS,
                   int idx_o3, int cd_internal, const float* __restrict__ play, const float* __restrict__ plev,
                   const float* __restrict__ tlay, const float* __restrict__ tlev, const float* __restrict__ tsfc,
@@ -586,6 +588,7 @@ int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
     const KdistView<float>& v = k->v32;
     const int NW1 = (nlay + CL - 1) / CL;
     const size_t smem1 = adj_layout(NW1 * CL, v.ngas, v.nband, NW1, NW1, CL, v.max_group_bands).total;
+    RB_CHECK_ARG(CL == 8 || NW1 <= 8, "adjoint_lw: chunk 16 covers at most 128 layers");
     int CS = 1, NWc = NW1;
     size_t smem = smem1;
     if (NW1 > 16 || smem1 > 227 * 1024) {

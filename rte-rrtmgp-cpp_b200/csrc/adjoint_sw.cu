@@ -38,9 +38,11 @@ namespace {
 
 using namespace fused;
 
-constexpr int kWPC = 8;            // warps per CTA
-constexpr int kCL = 8;             // layers per warp
-constexpr int kLPC = kWPC * kCL;   // layers per CTA
+constexpr int kLPC = 64;           // layers per CTA: 8 warps of 8 layers, or 16 warps of 4
+// Layers per warp of the launched kernel.  CL = 4 (16 warps per SM at 128 registers, 456 bytes
+// of spills) measured the same as CL = 8 (8 warps at 255 registers) at 8192 x 128: 33.9 vs
+// 33.4 ms; the occupancy it gains goes into spills and twice the chunk compositions.
+constexpr int kSwAdjointChunk = 8;
 
 struct SwAdjOut {
     float* tlay;
@@ -422,7 +424,7 @@ struct SwAdjLayout {
     size_t state, cg, seeds, clsum, albacc, x1, x2, x3, x4, x5, recs, drecs, total;
 };
 
-__host__ __device__ __forceinline__ SwAdjLayout sw_adj_layout(int ngas, int nband, int mgb, int CS)
+__host__ __device__ __forceinline__ SwAdjLayout sw_adj_layout(int ngas, int nband, int mgb, int CS, int WPC)
 {
     SwAdjLayout L;
     L.state = 0;
@@ -432,14 +434,14 @@ __host__ __device__ __forceinline__ SwAdjLayout sw_adj_layout(int ngas, int nban
     L.albacc = align16(L.clsum + sizeof(float) * size_t(nband) * kLPC * 3);
     L.x1 = align16(L.albacc + sizeof(double) * size_t(nband) * 2);
     // chunk maps of every chunk of the cluster (each warp pushes its map to all CTAs)
-    const size_t nw = size_t(kWPC) * CS * 32;
+    const size_t nw = size_t(WPC) * CS * 32;
     L.x2 = align16(L.x1 + sizeof(float) * nw);
     L.x3 = align16(L.x2 + (sizeof(float4) + sizeof(float)) * nw);
     L.x4 = align16(L.x3 + sizeof(float2) * nw);
     L.x5 = align16(L.x4 + (sizeof(float4) + sizeof(float)) * nw);
     L.recs = align16(L.x5 + sizeof(float2) * nw);
-    L.drecs = align16(L.recs + sizeof(Rec) * size_t(kWPC) * kCL * mgb);
-    L.total = align16(L.drecs + sizeof(DRec) * size_t(kWPC) * kCL * mgb);
+    L.drecs = align16(L.recs + sizeof(Rec) * size_t(kLPC) * mgb);
+    L.total = align16(L.drecs + sizeof(DRec) * size_t(kLPC) * mgb);
     return L;
 }
 
@@ -449,8 +451,10 @@ __device__ __forceinline__ Tp* remote(cg::cluster_group& cl, Tp* p, int rank)
     return cl.map_shared_rank(p, rank);
 }
 
-template <bool FLUX>
-__global__ void __launch_bounds__(256, 1)
+// CL layers per warp, kLPC / CL warps per CTA: CL = 8 gives 8 warps with up to 255 registers,
+// CL = 4 gives 16 warps at 128 registers (half the per-layer values per thread).
+template <int CL, bool FLUX>
+__global__ void __launch_bounds__(kLPC / CL * 32, 1)
 sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwCloudArgs cld, int ncol, int nlay, int CS,
                   int idx_o3, int cd_internal, const float* __restrict__ play, const float* __restrict__ plev,
                   const float* __restrict__ tlay, const float* __restrict__ col_dry_in,
@@ -459,18 +463,18 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
                   const float* __restrict__ seed_up, const float* __restrict__ seed_dn,
                   const float* __restrict__ seed_dir, const float* __restrict__ seed_hr, const SwAdjOut out)
 {
-    constexpr int CL = kCL;
+    constexpr int WPC = kLPC / CL;   // warps per CTA
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = int(cluster.block_rank());
     const int icol = blockIdx.x / CS;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int Wg = rank * kWPC + w;
-    const int NWt = CS * kWPC;
+    const int Wg = rank * WPC + w;
+    const int NWt = CS * WPC;
     const int L_end = NWt * CL;
     const int j0 = rank * kLPC;          // first global layer of this CTA
     const int nband = k.nband, mgb = k.max_group_bands;
-    const SwAdjLayout SL = sw_adj_layout(k.ngas, nband, mgb, CS);
+    const SwAdjLayout SL = sw_adj_layout(k.ngas, nband, mgb, CS, WPC);
     LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
     float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
     float* sm_al = reinterpret_cast<float*>(smem_raw + SL.seeds);   // seed F_up per local level (0..64)
@@ -539,7 +543,7 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
     // top / bottom boundary seeds (every thread walks the whole column)
     const float al0 = seed_at(seed_up, 0);
     const float alN = seed_at(seed_up, nlay), beN = seed_at(seed_dn, nlay), gaN = seed_at(seed_dir, nlay);
-    double acc_q = 0.0;   // RS<32> accumulator: lane L holds [T | H | O | -][L >> 3], layer L & 7
+    double acc_q = 0.0;   // reduce-scatter of [T | H | O | -] x CL: see the output section
     // forward fluxes (FLUX): as the forward kernel, lane L holds value L >> 1 of the chunk's
     // [levels | layers]: acc_fa direct / direct absorbed, acc_fb up / diffuse absorbed,
     // acc_fc diffuse down
@@ -869,35 +873,40 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
 
         // ---- sums over the 32 g-points ----
         {
-            float v[32];
+            float v[4 * CL];   // [T | H | O | -] x CL
 #pragma unroll
-            for (int i = 0; i < CL; ++i) { v[i] = gT[i]; v[8 + i] = gH[i]; v[16 + i] = gO[i]; v[24 + i] = 0.f; }
-            ReduceScatter<32, 16>::run(v, lane);
+            for (int i = 0; i < CL; ++i) { v[i] = gT[i]; v[CL + i] = gH[i]; v[2 * CL + i] = gO[i]; v[3 * CL + i] = 0.f; }
+            ReduceScatter<4 * CL, 16>::run(v, lane);
             acc_q += double(v[0]);
         }
         {
-            // cloud: [tc s0 | tc s1 | tsc s0 | tsc s1] then [tsg s0 | tsg s1]
-            float v[32];
+            // cloud: [tc s0 | tc s1 | tsc s0 | tsc s1] then [tsg s0 | tsg s1], CL layers each
+            constexpr int SH4 = (4 * CL == 32) ? 0 : 1;   // lane L holds value L >> SH4 of 4 CL
+            constexpr int SH2 = SH4 + 1;                  // ... and value L >> SH2 of 2 CL
+            float v[4 * CL];
 #pragma unroll
             for (int i = 0; i < CL; ++i) {
                 v[i] = slot == 0 ? gC0[i] : 0.f;
-                v[8 + i] = slot == 1 ? gC0[i] : 0.f;
-                v[16 + i] = slot == 0 ? gC1[i] : 0.f;
-                v[24 + i] = slot == 1 ? gC1[i] : 0.f;
+                v[CL + i] = slot == 1 ? gC0[i] : 0.f;
+                v[2 * CL + i] = slot == 0 ? gC1[i] : 0.f;
+                v[3 * CL + i] = slot == 1 ? gC1[i] : 0.f;
             }
-            ReduceScatter<32, 16>::run(v, lane);
+            ReduceScatter<4 * CL, 16>::run(v, lane);
             {
-                const int q = lane >> 4, sl = (lane >> 3) & 1, jl = w * CL + (lane & 7), b = b0 + sl;
-                if (j0 + jl < nlay && b < nband && k.band_lims[2 * b] < 32 * gg + 32)
+                const int vi = lane >> SH4;
+                const int q = vi / (2 * CL), sl = (vi / CL) & 1, jl = w * CL + (vi % CL), b = b0 + sl;
+                if ((lane & ((1 << SH4) - 1)) == 0 && j0 + jl < nlay && b < nband &&
+                    k.band_lims[2 * b] < 32 * gg + 32)
                     sm_cl[(b * kLPC + jl) * 3 + q] += v[0];
             }
-            float u[16];
+            float u[2 * CL];
 #pragma unroll
-            for (int i = 0; i < CL; ++i) { u[i] = slot == 0 ? gC2[i] : 0.f; u[8 + i] = slot == 1 ? gC2[i] : 0.f; }
-            ReduceScatter<16, 16>::run(u, lane);
+            for (int i = 0; i < CL; ++i) { u[i] = slot == 0 ? gC2[i] : 0.f; u[CL + i] = slot == 1 ? gC2[i] : 0.f; }
+            ReduceScatter<2 * CL, 16>::run(u, lane);
             {
-                const int vi = lane >> 1, sl = vi >> 3, jl = w * CL + (vi & 7), b = b0 + sl;
-                if ((lane & 1) == 0 && j0 + jl < nlay && b < nband && k.band_lims[2 * b] < 32 * gg + 32)
+                const int vi = lane >> SH2, sl = vi / CL, jl = w * CL + (vi % CL), b = b0 + sl;
+                if ((lane & ((1 << SH2) - 1)) == 0 && j0 + jl < nlay && b < nband &&
+                    k.band_lims[2 * b] < 32 * gg + 32)
                     sm_cl[(b * kLPC + jl) * 3 + 2] += u[0];
             }
         }
@@ -910,9 +919,10 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
 
     // ---- outputs ----
     if (FLUX) {
-        const int v = lane >> 1;
+        constexpr int SHF = (2 * CL == 16) ? 1 : 2;   // lane L holds value L >> SHF of 2 CL
+        const int v = lane >> SHF;
         const double g0_cp = 9.80665 / 1004.64;
-        if ((lane & 1) == 0) {
+        if ((lane & ((1 << SHF) - 1)) == 0) {
             if (v < CL) {
                 const int j = j0 + w * CL + v;
                 if (j < nlay) {
@@ -941,8 +951,10 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
         }
     }
     {
-        const int q = lane >> 3, jl = w * kCL + (lane & 7), j = j0 + jl;
-        if (q < 3 && j < nlay) {
+        constexpr int SHQ = (4 * CL == 32) ? 0 : 1;   // lane L holds value L >> SHQ of 4 CL
+        const int vi = lane >> SHQ;
+        const int q = vi / CL, jl = w * CL + (vi % CL), j = j0 + jl;
+        if ((lane & ((1 << SHQ) - 1)) == 0 && q < 3 && j < nlay) {
             const size_t o = icol + size_t(top_at_1 ? j : nlay - 1 - j) * ncol;
             float* dst = q == 0 ? out.tlay : (q == 1 ? out.h2o : out.o3);
             if (dst) dst[o] = float(acc_q);
@@ -1011,13 +1023,14 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     int idx_o3 = 0;
     for (size_t i = 0; i < k->gas_names.size(); ++i)
         if (k->gas_names[i] == "o3") idx_o3 = int(i) + 1;
-    const size_t smem = sw_adj_layout(v.ngas, v.nband, v.max_group_bands, CS).total;
+    constexpr int CL = kSwAdjointChunk;
+    const size_t smem = sw_adj_layout(v.ngas, v.nband, v.max_group_bands, CS, kLPC / CL).total;
     if (smem > 227 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_sw: shared memory need exceeds 227 KB");
     static bool attr = false;
     if (!attr) {
-        RB_CUDA(cudaFuncSetAttribute(sw_adjoint_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        RB_CUDA(cudaFuncSetAttribute(sw_adjoint_kernel<CL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      227 * 1024), "adjoint_sw attribute");
-        RB_CUDA(cudaFuncSetAttribute(sw_adjoint_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        RB_CUDA(cudaFuncSetAttribute(sw_adjoint_kernel<CL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      227 * 1024), "adjoint_sw attribute");
         attr = true;
     }
@@ -1033,7 +1046,7 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
                        flux_up, flux_dn, flux_dir, flux_net, heating_rate};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(unsigned(ncol) * CS);
-    cfg.blockDim = dim3(kWPC * 32);
+    cfg.blockDim = dim3(kLPC / CL * 32);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = as_stream(stream);
     cudaLaunchAttribute at[1];
@@ -1043,7 +1056,7 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    RB_CUDA(cudaLaunchKernelEx(&cfg, with_flux ? sw_adjoint_kernel<true> : sw_adjoint_kernel<false>, v, gs, ca, ncol, nlay, CS, idx_o3, col_dry ? 0 : 1, play, plev,
+    RB_CUDA(cudaLaunchKernelEx(&cfg, with_flux ? sw_adjoint_kernel<CL, true> : sw_adjoint_kernel<CL, false>, v, gs, ca, ncol, nlay, CS, idx_o3, col_dry ? 0 : 1, play, plev,
                                tlay, col_dry, mu0, tsi_scaling, sfc_alb_dir, sfc_alb_dif, seed_up, seed_dn, seed_dir,
                                seed_hr, out),
             "sw_adjoint_kernel launch");

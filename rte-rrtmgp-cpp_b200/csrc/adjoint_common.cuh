@@ -42,7 +42,8 @@ struct __align__(16) DRec {
     float4 fmT, fmH, fmO;   // d fminor / dx on the minor corners (lo.x, lo.y, hi.x, hi.y)
     float4 dB;              // LW: dB/dT of the band Planck function at T_lay, T_top, T_bot, T_sfc
                             // SW: d col_rayl / d vmr_h2o in x
-    float dsT[kMaxMinor], dsH[kMaxMinor], dsO[kMaxMinor];   // d scaling_n / dx
+    float dsT[kMaxMinor];   // d ln(scaling_n) / dT (scaling_n: the forward record's scal[n])
+    float dsH[kMaxMinor], dsO[kMaxMinor];   // d scaling_n / d vmr
 };
 
 __device__ __forceinline__ float dot4(const float4& a, const float4& b)
@@ -59,13 +60,14 @@ __device__ __forceinline__ float interpolate1D_slope(float val, float offset, fl
     return (table[idx] - table[idx - 1]) / delta;
 }
 
-// Derivative record of band b at layer state s (cg: gas columns of the layer, stride cgs;
-// scal: the forward record's minor scalings).  idx_o3: col_gas index of o3 (0: absent).
+// Derivative record of band b at layer state s (cg: gas columns of the layer, stride cgs).
+// It does not read the forward record, so both can be built at once.  idx_o3: col_gas
+// index of o3 (0: absent).
 // cd_internal: col_dry was computed from h2o and the level pressures.  PFRAC: also the
 // Planck-fraction weights pT/pH/pO (longwave only).
 template <bool PFRAC = true>
 __device__ __forceinline__ void build_drec(const KdistView<float>& k, DRec& D, const LayerState& s, const float* cg,
-                                           int cgs, int b, const float* scal, int idx_o3, int cd_internal)
+                                           int cgs, int b, int idx_o3, int cd_internal)
 {
     const float delta = k.temp_ref_delta;
     const int a = s.itropo;
@@ -146,7 +148,7 @@ __device__ __forceinline__ void build_drec(const KdistView<float>& k, DRec& D, c
         float dsT = 0.f;
         if (flags & 1) {
             Dd = 0.01f * s.p / s.t;
-            dsT = -scal[n] / s.t;
+            dsT = -1.f / s.t;   // d ln(scaling_n) / dT
             const int sgi = k.minor_sgas[a][im];
             if (sgi > 0) {
                 const float vs = cg[sgi * cgs] / cd;
@@ -187,7 +189,7 @@ __device__ __forceinline__ void tau_abs_adjoint(const KdistView<float>& k, const
             const float4 cr = make_float4(lo.x, lo.y, hi.x, hi.y);
             const float M = dot4(R.fm, cr);
             const float sc = R.scal[sl];
-            const float tT = D.dsT[sl] * M + sc * dot4(D.fmT, cr);
+            const float tT = sc * (D.dsT[sl] * M + dot4(D.fmT, cr));
             const float tH = D.dsH[sl] * M + sc * dot4(D.fmH, cr);
             const float tO = D.dsO[sl] * M + sc * dot4(D.fmO, cr);
             const bool on = n < mg.x;

@@ -276,7 +276,7 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
                                     interpolate1D(s.t_bot, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp),
                                     sm_cld[b * LPC + jl]);
                 R.aux2 = bottom ? interpolate1D(ts, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp) : 0.f;
-                build_drec(k, DR, s, sm_cg + jl, LPC, b, R.scal, idx_o3, cd_internal);
+                build_drec(k, DR, s, sm_cg + jl, LPC, b, idx_o3, cd_internal);
                 DR.dB = make_float4(interpolate1D_slope(s.t, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp),
                                     interpolate1D_slope(s.t_top, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp),
                                     interpolate1D_slope(s.t_bot, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp),

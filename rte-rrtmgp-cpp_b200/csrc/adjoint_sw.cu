@@ -23,7 +23,7 @@
 // affine in its adjoint (the albedo/source pair is 2x2 upper triangular), so chunks compose
 // exactly like the forward.  Per layer the adjoints of (R, T, Rdir, Tdir, Tn, adif, adir)
 // go through the two-stream (reverse mode of the forward's FP32 formulas with its branch
-// selections; FP64 central differences of the reference expressions in the k mu0 = 1 island), the
+// selections; FP64 forward-mode derivatives of the reference expressions in the k mu0 = 1 island), the
 // gas/Rayleigh/cloud combination, and the gas-optics interpolation (adjoint_common.cuh).
 #include <cooperative_groups.h>
 
@@ -64,24 +64,88 @@ struct SwAdjOut {
 
 using D4 = Dual<4>;
 
-// FP64 island of the two-stream (|1 - (k mu0)^2| < 0.02, as the forward): Rdir and Tdir from
-// the reference expressions in double and their central differences in (tau, w0, g).  Rare
-// (strongly absorbing g-points at mu0 near 1/k), so kept out of line: one copy of the code.
-__device__ __noinline__ void island_fp64(float tau, float w0, float g, float mu0, float* rd, float* td)
+// Minor-interval code n (contributor << 4 | slot) of a g-point's list (minor_entry).
+__device__ __forceinline__ int minor_code(const int4& mg, int n)
 {
-    double Rd, Td, Rr, Tr, Tn64;
-    sw_two_stream<double>(double(tau), double(w0), double(g), double(mu0), Rd, Td, Rr, Tr, Tn64);
-    rd[0] = float(Rr);
-    td[0] = float(Tr);
-    const double steps[3] = {1e-6 * fmax(double(tau), 1e-12), 1e-6, 1e-6};
-    for (int i = 0; i < 3; ++i) {
-        double Rp, Tp, Rm, Tm, x0, x1, x2;
-        const double dt = i == 0 ? steps[0] : 0.0, dw = i == 1 ? steps[1] : 0.0, dg = i == 2 ? steps[2] : 0.0;
-        sw_two_stream<double>(double(tau) + dt, double(w0) + dw, double(g) + dg, double(mu0), x0, x1, Rp, Tp, x2);
-        sw_two_stream<double>(double(tau) - dt, double(w0) - dw, double(g) - dg, double(mu0), x0, x1, Rm, Tm, x2);
-        rd[1 + i] = float((Rp - Rm) / (2.0 * steps[i]));
-        td[1 + i] = float((Tp - Tm) / (2.0 * steps[i]));
+    return n == 0 ? mg.y : (n == 1 ? mg.z : mg.w);
+}
+
+// FP64 value with its derivatives with respect to (tau, w0, g): forward-mode arithmetic for
+// the island below.
+struct DD3 {
+    double v, t, w, g;
+};
+__device__ __forceinline__ DD3 dd(double v) { return DD3{v, 0.0, 0.0, 0.0}; }
+__device__ __forceinline__ DD3 operator+(const DD3& a, const DD3& b) { return DD3{a.v + b.v, a.t + b.t, a.w + b.w, a.g + b.g}; }
+__device__ __forceinline__ DD3 operator-(const DD3& a, const DD3& b) { return DD3{a.v - b.v, a.t - b.t, a.w - b.w, a.g - b.g}; }
+__device__ __forceinline__ DD3 operator*(const DD3& a, const DD3& b)
+{
+    return DD3{a.v * b.v, a.t * b.v + a.v * b.t, a.w * b.v + a.v * b.w, a.g * b.v + a.v * b.g};
+}
+__device__ __forceinline__ DD3 operator*(double s, const DD3& a) { return DD3{s * a.v, s * a.t, s * a.w, s * a.g}; }
+__device__ __forceinline__ DD3 operator+(double s, const DD3& a) { return DD3{s + a.v, a.t, a.w, a.g}; }
+__device__ __forceinline__ DD3 operator-(double s, const DD3& a) { return DD3{s - a.v, -a.t, -a.w, -a.g}; }
+__device__ __forceinline__ DD3 recip(const DD3& a)
+{
+    const double r = 1.0 / a.v, d = -r * r;
+    return DD3{r, d * a.t, d * a.w, d * a.g};
+}
+__device__ __forceinline__ DD3 exp_neg(const DD3& a)   // exp(-a)
+{
+    const double e = exp(-a.v);
+    return DD3{e, -e * a.t, -e * a.w, -e * a.g};
+}
+
+// FP64 island of the two-stream (|1 - (k mu0)^2| < 0.02, as the forward): the unclamped Rdir
+// and Tdir of the reference expressions (sw_two_stream, rte_device.cuh) in double, and their
+// derivatives with respect to (tau, w0, g) by forward-mode differentiation of the same
+// expressions.  rd = [Rdir, dRdir/dtau, dRdir/dw0, dRdir/dg], td likewise.  Out of line: one
+// copy of the code.
+__device__ __noinline__ void island_fp64(float tau_f, float w0_f, float g_f, float mu0_f, float* rd, float* td)
+{
+    const double mu0 = double(mu0_f);
+    const DD3 tau{double(tau_f), 1.0, 0.0, 0.0};
+    const DD3 w0{double(w0_f), 0.0, 1.0, 0.0};
+    const DD3 g{double(g_f), 0.0, 0.0, 1.0};
+    const DD3 gamma1 = 0.25 * (8.0 - w0 * (5.0 + 3.0 * g));
+    const DD3 gamma2 = 0.75 * (w0 * (1.0 - g));
+    const DD3 gamma3 = 0.25 * (2.0 - (3.0 * mu0) * g);
+    const DD3 gamma4 = 1.0 - gamma3;
+    const DD3 alpha1 = gamma1 * gamma4 + gamma2 * gamma3;
+    const DD3 alpha2 = gamma1 * gamma3 + gamma2 * gamma4;
+    const DD3 kk = (gamma1 - gamma2) * (gamma1 + gamma2);
+    DD3 k = dd(sqrt(1.e-12));
+    if (kk.v > 1.e-12) {
+        const double kv = sqrt(kk.v), h = 0.5 / kv;
+        k = DD3{kv, h * kk.t, h * kk.w, h * kk.g};
     }
+    const DD3 e1 = exp_neg(tau * k);
+    const DD3 e2 = e1 * e1;
+    const DD3 rt = recip(k * (1.0 + e2) + gamma1 * (1.0 - e2));
+    const DD3 Tn = exp_neg((1.0 / mu0) * tau);
+    const DD3 k_mu = mu0 * k;
+    const DD3 k_gamma3 = k * gamma3;
+    const DD3 k_gamma4 = k * gamma4;
+    const double tmin = 2.220446049250313e-16;
+    DD3 fact = 1.0 - k_mu * k_mu;
+    if (!(fabs(fact.v) > tmin)) fact = dd(tmin);
+    const DD3 rt2 = w0 * rt * recip(fact);
+    const DD3 Rdir = rt2 * ((1.0 - k_mu) * (alpha2 + k_gamma3) - (1.0 + k_mu) * (alpha2 - k_gamma3) * e2 -
+                            2.0 * ((k_gamma3 - alpha2 * k_mu) * e1 * Tn));
+    const DD3 Tdir = rt2 * (2.0 * ((k_gamma4 + alpha1 * k_mu) * e1) - (1.0 + k_mu) * (alpha1 + k_gamma4) * Tn +
+                            (1.0 - k_mu) * (alpha1 - k_gamma4) * e2 * Tn);
+    rd[0] = float(Rdir.v); rd[1] = float(Rdir.t); rd[2] = float(Rdir.w); rd[3] = float(Rdir.g);
+    td[0] = float(Tdir.v); td[1] = float(Tdir.t); td[2] = float(Tdir.w); td[3] = float(Tdir.g);
+}
+
+// Whether the two-stream of (tau, w0 = 1 - omw, g) takes the FP64 island (the expressions of
+// sw_layer_fast; independent of tau).
+__device__ __forceinline__ bool island_flag(float w0, float omw, float g, float mu0)
+{
+    const float kk = 2.f * omw * (2.f - .5f * w0 * (1.f + 3.f * g));
+    const float kkc = fmaxf(kk, 1.e-12f);
+    const float km = kkc * rsqrtf(kkc) * mu0;
+    return fabsf((1.f - km) * (1.f + km)) < 0.02f;
 }
 
 // Adjoint of one (layer, g-point) from the adjoints of its two-stream outputs (R, T, Rdir,
@@ -90,15 +154,16 @@ __device__ __noinline__ void island_fp64(float tau, float w0, float g, float mu0
 // tau = ta + tr + tc, w0 = (tr + tsc) / tau, g = tsgc / (tr + tsc).  Reverse mode of
 // sw_layer_fast: the forward is recomputed with the same expressions and branch selections
 // (clamps: the selected argument carries the derivative, as min/max of dual numbers would),
-// then the adjoints run back through it.  Out of line: the caller's per-layer loop is
-// unrolled, this body is emitted once.
+// then the adjoints run back through it.  island: the (layer, g-point) takes the FP64 island
+// (decided once per group, island_flag); isl: its island_fp64 results [Rdir, dRdir/d(tau, w0,
+// g), Tdir, dTdir/d(...)] when the warp computed them already, else null.
 struct LocalAdj {
     float ta, tr, tc, tsc, tsg;
 };
 
-__device__ __noinline__ LocalAdj sw_local_adjoint(float tau, float w0, float omw, float g, float mu0, float mu0_inv,
-                                                  float Rb, float Tb, float Rdb, float Tdb, float Tnb, float Afb,
-                                                  float Arb)
+__device__ __forceinline__ LocalAdj sw_local_adjoint(float tau, float w0, float omw, float g, float mu0, float mu0_inv,
+                                                     float Rb, float Tb, float Rdb, float Tdb, float Tnb, float Afb,
+                                                     float Arb, bool island, const float* isl)
 {
     // ---- forward, as sw_layer_fast (same expressions, same branch selections) ----
     const float g1 = (8.f - w0 * (5.f + 3.f * g)) * .25f;
@@ -121,12 +186,16 @@ __device__ __noinline__ LocalAdj sw_local_adjoint(float tau, float w0, float omw
     const float rt = __fdividef(1.f, den);
     const float km = k * mu0;
     const float fact = (1.f - km) * (1.f + km);
-    const bool island = fabsf(fact) < 0.02f;
     float Rdir0, Tdir0, rt2 = 0.f, br = 0.f, bt = 0.f;
     bool thick = false;
     float rd[4], td[4];
     if (island) {
-        island_fp64(tau, w0, g, mu0, rd, td);
+        if (isl) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) { rd[q] = isl[q]; td[q] = isl[4 + q]; }
+        } else {
+            island_fp64(tau, w0, g, mu0, rd, td);
+        }
         Rdir0 = rd[0];
         Tdir0 = td[0];
     } else {
@@ -281,44 +350,61 @@ __device__ __noinline__ LocalAdj sw_local_adjoint(float tau, float w0, float omw
     return r;
 }
 
-// Gas-optics adjoint of one (layer, g-point): the absorption tau_bar through the major and
-// minor interpolation (tau_abs_adjoint of adjoint_common.cuh) and the Rayleigh tau_bar
-// through col_rayl * (fm . krayl corners).  Out of line, like the two-stream below: the
-// per-layer loops are unrolled 8 times and, inlined, these bodies made the kernel's code
-// outgrow the instruction cache (10% of the kernel time).
-struct GasGrad { float t, h, o; };
+// Adjoint of one (layer, g-point) through the two-stream (sw_local_adjoint) and the gas optics:
+// the absorption tau_bar through the major and minor interpolation (as tau_abs_adjoint of
+// adjoint_common.cuh) and the Rayleigh tau_bar through col_rayl * (fm . krayl corners).  The
+// table corners are read first, so their latency overlaps the two-stream adjoint.  Out of
+// line: the caller's per-layer loops are unrolled 8 times and, inlined, these bodies made the
+// kernel's code outgrow the instruction cache (10% of the kernel time).
+struct LayerAdj {
+    float t, h, o;          // d/dT, d/d vmr_h2o, d/d vmr_o3
+    float tc, tsc, tsg;     // adjoints of the cloud tau, tau*ssa, tau*ssa*g
+};
 
-__device__ __noinline__ GasGrad sw_gas_adjoint(const float4* __restrict__ kmaj4, const float2* __restrict__ kmin,
-                                               const float2* __restrict__ krayl2, const Rec* Rc, const DRec* DR,
-                                               int g, int4 mg, int nmax, float tab, float trb)
+__device__ __noinline__ LayerAdj sw_layer_adjoint(const float4* __restrict__ kmaj4, const float2* __restrict__ kmin,
+                                                  const float2* __restrict__ krayl2, const Rec* Rc, const DRec* DR,
+                                                  int g, int4 mg, int nmax, float tau, float w0, float omw, float gasy,
+                                                  float mu0, float mu0_inv, float Rb, float Tb, float Rdb, float Tdb,
+                                                  float Tnb, float Afb, float Arb, bool island, const float* isl)
 {
     const float4 c0 = __ldg(kmaj4 + (Rc->kb.x + g));
     const float4 c1 = __ldg(kmaj4 + (Rc->kb.y + g));
+    float4 cr[3];
+#pragma unroll
+    for (int n = 0; n < 3; ++n) {
+        cr[n] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (n < nmax) {
+            const int c = minor_code(mg, n) >> 4;
+            const float2 lo = __ldg(kmin + (Rc->kb.z + c));
+            const float2 hi = __ldg(kmin + (Rc->kb.w + c));
+            cr[n] = make_float4(lo.x, lo.y, hi.x, hi.y);
+        }
+    }
+    const float2 r0 = __ldg(krayl2 + (Rc->kr[0] + g));
+    const float2 r1 = __ldg(krayl2 + (Rc->kr[1] + g));
+
+    const LocalAdj la = sw_local_adjoint(tau, w0, omw, gasy, mu0, mu0_inv, Rb, Tb, Rdb, Tdb, Tnb, Afb, Arb, island, isl);
+
     float dT = dot4(DR->wT0, c0) + dot4(DR->wT1, c1);
     float dH = dot4(DR->wH0, c0) + dot4(DR->wH1, c1);
     float dO = dot4(DR->wO0, c0) + dot4(DR->wO1, c1);
 #pragma unroll
     for (int n = 0; n < 3; ++n) {
         if (n < nmax) {
-            const int code = n == 0 ? mg.y : (n == 1 ? mg.z : mg.w);
-            const int c = code >> 4, sl = code & 15;
-            const float2 lo = __ldg(kmin + (Rc->kb.z + c));
-            const float2 hi = __ldg(kmin + (Rc->kb.w + c));
-            const float4 cr = make_float4(lo.x, lo.y, hi.x, hi.y);
-            const float M = dot4(Rc->fm, cr);
+            const int sl = minor_code(mg, n) & 15;
+            const float M = dot4(Rc->fm, cr[n]);
             const float sc = Rc->scal[sl];
-            const float tT = DR->dsT[sl] * M + sc * dot4(DR->fmT, cr);
-            const float tH = DR->dsH[sl] * M + sc * dot4(DR->fmH, cr);
-            const float tO = DR->dsO[sl] * M + sc * dot4(DR->fmO, cr);
+            const float tT = sc * (DR->dsT[sl] * M + dot4(DR->fmT, cr[n]));
+            const float tH = DR->dsH[sl] * M + sc * dot4(DR->fmH, cr[n]);
+            const float tO = DR->dsO[sl] * M + sc * dot4(DR->fmO, cr[n]);
             const bool on = n < mg.x;
             dT += on ? tT : 0.f;
             dH += on ? tH : 0.f;
             dO += on ? tO : 0.f;
         }
     }
-    GasGrad r{tab * dT, tab * dH, tab * dO};
-    const float2 r0 = __ldg(krayl2 + (Rc->kr[0] + g));
-    const float2 r1 = __ldg(krayl2 + (Rc->kr[1] + g));
+    const float tab = la.ta, trb = la.tr;
+    LayerAdj r{tab * dT, tab * dH, tab * dO, la.tc, la.tsc, la.tsg};
     const float4 kr = make_float4(r0.x, r0.y, r1.x, r1.y);
     const float colr = Rc->aux.x;
     r.t += trb * colr * dot4(DR->fmT, kr);
@@ -326,7 +412,6 @@ __device__ __noinline__ GasGrad sw_gas_adjoint(const float4* __restrict__ kmaj4,
     r.o += trb * colr * dot4(DR->fmO, kr);
     return r;
 }
-
 
 // Forward optical properties and two-stream coefficients of one (layer, g-point), as the
 // forward kernel's pass 1 (sw_column.cuh), out of line for the same reason.
@@ -420,8 +505,12 @@ __device__ __forceinline__ void cloud_sw_dual(const CloudLut<float>& L, int delt
     tsg = ts * g;
 }
 
+// FP64 island tasks of a warp per group (one per lane): inputs tau, w0, g, (pad), then the
+// island_fp64 results [Rdir, dRdir/d(tau, w0, g), Tdir, dTdir/d(tau, w0, g)].
+constexpr int kIslTask = 12;
+
 struct SwAdjLayout {
-    size_t state, cg, seeds, clsum, albacc, x1, x2, x3, x4, x5, recs, drecs, total;
+    size_t state, cg, seeds, clsum, albacc, x1, x2, x3, x4, x5, recs, drecs, isl, total;
 };
 
 __host__ __device__ __forceinline__ SwAdjLayout sw_adj_layout(int ngas, int nband, int mgb, int CS, int WPC)
@@ -441,7 +530,8 @@ __host__ __device__ __forceinline__ SwAdjLayout sw_adj_layout(int ngas, int nban
     L.x5 = align16(L.x4 + (sizeof(float4) + sizeof(float)) * nw);
     L.recs = align16(L.x5 + sizeof(float2) * nw);
     L.drecs = align16(L.recs + sizeof(Rec) * size_t(kLPC) * mgb);
-    L.total = align16(L.drecs + sizeof(DRec) * size_t(kLPC) * mgb);
+    L.isl = align16(L.drecs + sizeof(DRec) * size_t(kLPC) * mgb);
+    L.total = align16(L.isl + sizeof(float) * kIslTask * 32 * WPC);
     return L;
 }
 
@@ -492,6 +582,7 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
     float2* sm_x5 = reinterpret_cast<float2*>(smem_raw + SL.x5);
     Rec* recs = reinterpret_cast<Rec*>(smem_raw + SL.recs) + w * CL * mgb;
     DRec* drecs = reinterpret_cast<DRec*>(smem_raw + SL.drecs) + w * CL * mgb;
+    float* sm_isl = reinterpret_cast<float*>(smem_raw + SL.isl) + w * 32 * kIslTask;
 
     const bool top_at_1 = play[icol] < play[icol + size_t(nlay - 1) * ncol];
     const float mu0 = mu0_in[icol];
@@ -564,21 +655,26 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
         const float ad = gv ? __ldg(alb_dir + gband + size_t(icol) * nband) : 0.f;
         const float af = gv ? __ldg(alb_dif + gband + size_t(icol) * nband) : 0.f;
 
-        for (int r = lane; r < CL * mgb; r += 32) {
+        // forward records on one half of the tasks, derivative records on the other (they are
+        // independent): with 8 layers and 2 bands every lane builds one
+        for (int t = lane; t < 2 * CL * mgb; t += 32) {
+            const int r = t % (CL * mgb);
             const int jl = w * CL + (r % CL);
             const int jj = j0 + jl;
             const int b = b0 + r / CL;
             if (jj < nlay && b < nband && k.band_lims[2 * b] < 32 * gg + 32) {
-                const int l = top_at_1 ? jj : nlay - 1 - jj;
-                Rec& R = recs[r];
-                DRec& DR = drecs[r];
                 const LayerState s = st[jl];
-                build_sw_record(k, R, s, sm_cg + jl, kLPC, b, cld, icol + size_t(l) * ncol);
-                build_drec<false>(k, DR, s, sm_cg + jl, kLPC, b, R.scal, idx_o3, cd_internal);
-                const float cd = sm_cg[jl];
-                const float vh = sm_cg[k.idx_h2o * kLPC + jl] / cd;
-                const float dcd_h = cd_internal ? -cd * m_h2o / (m_dry + m_h2o * vh) : 0.f;
-                DR.dB = make_float4(dcd_h * (1.f + vh) + cd, 0.f, 0.f, 0.f);   // d col_rayl / d vmr_h2o
+                if (t < CL * mgb) {
+                    const int l = top_at_1 ? jj : nlay - 1 - jj;
+                    build_sw_record(k, recs[r], s, sm_cg + jl, kLPC, b, cld, icol + size_t(l) * ncol);
+                } else {
+                    DRec& DR = drecs[r];
+                    build_drec<false>(k, DR, s, sm_cg + jl, kLPC, b, idx_o3, cd_internal);
+                    const float cd = sm_cg[jl];
+                    const float vh = sm_cg[k.idx_h2o * kLPC + jl] / cd;
+                    const float dcd_h = cd_internal ? -cd * m_h2o / (m_dry + m_h2o * vh) : 0.f;
+                    DR.dB = make_float4(dcd_h * (1.f + vh) + cd, 0.f, 0.f, 0.f);   // d col_rayl / d vmr_h2o
+                }
             }
         }
         __syncwarp();
@@ -847,27 +943,60 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
             Db = m.x * Db + m.y;
         }
 
+        // ---- FP64 island tasks of the chunk, compacted over the lanes ----
+        // A (layer, g-point) near k mu0 = 1 needs island_fp64 (an FP64 two-stream with three
+        // tangents).  Such pairs are sparse and scattered over the lanes, so instead of every
+        // layer's call running it for the lanes that need it (the warp waiting each time), the
+        // first 32 tasks of the chunk (layer by layer, lane by lane) are run at once, one per
+        // lane; a task beyond the first 32 is run by its own lane in the layer call.
+        unsigned isl_bits = 0;
+        int ntask = 0;
+#pragma unroll
+        for (int i = 0; i < CL; ++i) {
+            const bool f = (j0 + w * CL + i < nlay) && gv && island_flag(vW0[i], vOmw[i], vG[i], mu0);
+            const unsigned m = __ballot_sync(0xffffffffu, f);
+            const int idx = ntask + __popc(m & ((1u << lane) - 1u));
+            if (f) {
+                isl_bits |= 1u << i;
+                if (idx < 32) {
+                    float* t = sm_isl + idx * kIslTask;
+                    t[0] = vTau[i];
+                    t[1] = vW0[i];
+                    t[2] = vG[i];
+                }
+            }
+            ntask += __popc(m);
+        }
+        __syncwarp();
+        if (lane < ntask) {
+            float* t = sm_isl + lane * kIslTask;
+            island_fp64(t[0], t[1], t[2], mu0, t + 4, t + 8);
+        }
+        __syncwarp();
+
         // ---- R1 resweep + local adjoints per layer ----
         float gT[CL], gH[CL], gO[CL], gC0[CL], gC1[CL], gC2[CL];
+        int rem = ntask;   // island tasks of layers < i
 #pragma unroll
         for (int i = CL - 1; i >= 0; --i) {
             const int jl = w * CL + i;
             const int j = j0 + jl;
+            const bool isl = (isl_bits >> i) & 1u;
+            const unsigned m = __ballot_sync(0xffffffffu, isl);
+            rem -= __popc(m);
+            const int idx = rem + __popc(m & ((1u << lane) - 1u));
             const float dir = vDir[i];
             const float Tnb = Db * dir, Rdb = vSub[i] * dir, Tdb = vSdb[i] * dir, Arb = sm_hh[jl] * dir;
             Db = sm_be[jl] + sm_ga[jl] + sm_hh[jl] * vAr[i] + vSub[i] * vRd[i] + vSdb[i] * vTd[i] + vTn[i] * Db;
             gT[i] = 0.f; gH[i] = 0.f; gO[i] = 0.f; gC0[i] = 0.f; gC1[i] = 0.f; gC2[i] = 0.f;
             if (j < nlay && gv) {
-                const LocalAdj la = sw_local_adjoint(vTau[i], vW0[i], vOmw[i], vG[i], mu0, mu0_inv, vRb[i], vTb[i],
-                                                     Rdb, Tdb, Tnb, vAfb[i], Arb);
                 const Rec& Rc = recs[slot * CL + i];
-                const DRec& DR = drecs[slot * CL + i];
-                const float tab = la.ta, trb = la.tr, tcb = la.tc, tscb = la.tsc, tsgb = la.tsg;
-                const GasGrad gg3 = sw_gas_adjoint(k.kmaj4, k.kmin2[Rc.a], k.krayl2, &Rc, &DR, g, Rc.a ? mg1 : mg0,
-                                                   Rc.a ? nm1 : nm0, tab, trb);
-                const float gt = gg3.t, gh = gg3.h, go = gg3.o;
-                gT[i] = gt; gH[i] = gh; gO[i] = go;
-                gC0[i] = tcb; gC1[i] = tscb; gC2[i] = tsgb;
+                const LayerAdj la = sw_layer_adjoint(k.kmaj4, k.kmin2[Rc.a], k.krayl2, &Rc, &drecs[slot * CL + i], g,
+                                                     Rc.a ? mg1 : mg0, Rc.a ? nm1 : nm0, vTau[i], vW0[i], vOmw[i],
+                                                     vG[i], mu0, mu0_inv, vRb[i], vTb[i], Rdb, Tdb, Tnb, vAfb[i], Arb,
+                                                     isl, (isl && idx < 32) ? sm_isl + idx * kIslTask + 4 : nullptr);
+                gT[i] = la.t; gH[i] = la.h; gO[i] = la.o;
+                gC0[i] = la.tc; gC1[i] = la.tsc; gC2[i] = la.tsg;
             }
         }
 

@@ -269,6 +269,25 @@ def test_sw_adjoint_matches_fd(oracle_mod, tables, gpu, nlay, top_at_1):
         _check("sw d/drei", got["rei"], _fd(fwd, atm, seeds, "rei"), cloudy_i)
 
 
+@pytest.mark.parametrize("nlay", [24, 80])
+def test_sw_adjoint_fp64_island_columns(oracle_mod, tables, gpu, nlay):
+    """Columns with mu0 near 1/k of the strongly absorbing g-points (k ~ 2): 13% of the (layer,
+    g-point) pairs at mu0 = 0.5 take the FP64 island (|1 - (k mu0)^2| < 0.02), more than the 32
+    per chunk of 8 layers that a warp runs at once, so both the compacted and the per-layer
+    island paths run.  Checked per column against FP64 central differences."""
+    rng = np.random.default_rng(8)
+    ncol = 4
+    atm, fwd = _sw_setup(tables, oracle_mod, ncol, nlay, seed=57 + nlay, clouds=True)
+    atm["mu0"] = np.array([0.4995, 0.501, 0.51, 0.55])
+    seeds = _sw_seeds(nlay, ncol, rng)
+    got = _gpu_grads_sw(tables, atm, seeds, True)
+    for key in ("tlay", "h2o", "o3"):
+        ref = _fd(fwd, atm, seeds, key)
+        inf = _informative(_get(atm, key))
+        for c in range(ncol):
+            _check(f"sw d/d{key} column {c}", got[key][:, c], ref[:, c], inf[:, c])
+
+
 def test_sw_autograd_directional(oracle_mod, tables, gpu):
     import torch
     from rrtmgp_b200.autodiff import shortwave

@@ -594,6 +594,17 @@ def main():
                     "algorithmic_bytes": bpc[dom] * args.ncol,
                     "kernel_ms": {k: round(v, 4) for k, v in breakdown.items()}}
 
+    # Per-stage kernels of the class API (FP32), each against its HBM roofline.
+    staged_kernels = None
+    if args.path == "fused" and rank == 0:
+        sk = staged_breakdown(3)
+        bpc_s = bytes_per_column(args.nlay)
+        staged_kernels = {}
+        for k, ms in sk.items():
+            gbs = bpc_s[k] * args.ncol / (ms * 1e-3) / 1e9
+            staged_kernels[k] = {"ms": round(ms, 4), "algorithmic_bytes": bpc_s[k] * args.ncol,
+                                 "achieved_gbs": round(gbs, 1), "frac": round(gbs / hbm_peak, 4)}
+
     # End to end through the public API with host buffers (pinned), copies in the timed region.
     in_keys = ["play", "plev", "tlay", "tlev", "tsfc", "lwp", "iwp", "rel", "rei", "mu0", "emis_sfc",
                "sfc_alb_dir", "sfc_alb_dif"]
@@ -801,6 +812,7 @@ def main():
             "batched": batched,
             "deep_forward_adjoint": deep,
             "aerosol_optics": aer_line,
+            "staged_kernels": staged_kernels,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

@@ -138,16 +138,6 @@ __device__ __noinline__ void island_fp64(float tau_f, float w0_f, float g_f, flo
     td[0] = float(Tdir.v); td[1] = float(Tdir.t); td[2] = float(Tdir.w); td[3] = float(Tdir.g);
 }
 
-// Whether the two-stream of (tau, w0 = 1 - omw, g) takes the FP64 island (the expressions of
-// sw_layer_fast; independent of tau).
-__device__ __forceinline__ bool island_flag(float w0, float omw, float g, float mu0)
-{
-    const float kk = 2.f * omw * (2.f - .5f * w0 * (1.f + 3.f * g));
-    const float kkc = fmaxf(kk, 1.e-12f);
-    const float km = kkc * rsqrtf(kkc) * mu0;
-    return fabsf((1.f - km) * (1.f + km)) < 0.02f;
-}
-
 // Adjoint of one (layer, g-point) from the adjoints of its two-stream outputs (R, T, Rdir,
 // Tdir, Tn, adif, adir) to the optical inputs of the layer: gas absorption tau (x), Rayleigh
 // tau (y), cloud tau (z), cloud tau*ssa (w) and cloud tau*ssa*g (v).  The combination is
@@ -155,7 +145,7 @@ __device__ __forceinline__ bool island_flag(float w0, float omw, float g, float 
 // sw_layer_fast: the forward is recomputed with the same expressions and branch selections
 // (clamps: the selected argument carries the derivative, as min/max of dual numbers would),
 // then the adjoints run back through it.  island: the (layer, g-point) takes the FP64 island
-// (decided once per group, island_flag); isl: its island_fp64 results [Rdir, dRdir/d(tau, w0,
+// (decided once per group, sw_island); isl: its island_fp64 results [Rdir, dRdir/d(tau, w0,
 // g), Tdir, dTdir/d(...)] when the warp computed them already, else null.
 struct LocalAdj {
     float ta, tr, tc, tsc, tsg;
@@ -953,7 +943,7 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
         int ntask = 0;
 #pragma unroll
         for (int i = 0; i < CL; ++i) {
-            const bool f = (j0 + w * CL + i < nlay) && gv && island_flag(vW0[i], vOmw[i], vG[i], mu0);
+            const bool f = (j0 + w * CL + i < nlay) && gv && sw_island(vW0[i], vOmw[i], vG[i], mu0);
             const unsigned m = __ballot_sync(0xffffffffu, f);
             const int idx = ntask + __popc(m & ((1u << lane) - 1u));
             if (f) {

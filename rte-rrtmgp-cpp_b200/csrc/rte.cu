@@ -1,15 +1,22 @@
 // Per-stage RTE solvers: longwave no-scattering (Gauss quadrature) and shortwave two-stream
-// with adding.  One thread per (column, g-point); a block is a run of consecutive columns at
-// one g-point, so every layer read and level write is a coalesced row of the column-fastest
-// (ncol, nlay|nlev, ngpt) arrays.  No temporaries are allocated: the longwave up-sweep
-// inputs are kept in shared memory (or recomputed when nlay is too large), and the
-// shortwave adding recurrences use a caller workspace plus the output arrays themselves.
+// with adding, over the reference's column-fastest (ncol, nlay|nlev, ngpt) arrays.
+//   * Up to 256 layers (one angle for the longwave; FP64 shortwave up to 128): the chunked
+//     kernels below -- a warp is 32 consecutive columns x a chunk of layers at one g-point,
+//     the chunks of a column are the warps of a block and exchange affine maps through shared
+//     memory -- read every input once and write every level once (no workspace, no stash).
+//   * Otherwise one thread per (column, g-point), a block being a run of consecutive columns
+//     at one g-point: the longwave up-sweep inputs are kept in shared memory (or recomputed
+//     when nlay is too large), and the shortwave adding recurrences use the caller workspace
+//     plus the output arrays themselves.
+// Every layer read and level write is a coalesced row either way.  The shortwave workspace is
+// required by the C ABI whichever kernel runs.
 #include <algorithm>
 #include <cfloat>
 #include <mutex>
 
 #include "common.cuh"
 #include "rte_device.cuh"
+#include "sw_common.cuh"
 
 namespace rrtmgp_b200 {
 namespace {
@@ -169,6 +176,299 @@ __global__ void sw_solver_kernel(int ncol, int nlay, int ngpt, int nband, int to
     }
 }
 
+// ---- Chunked solvers (nlay <= 16 CL) ----
+// A warp is 32 consecutive columns x one chunk of CL layers at one g-point, and the chunks of a
+// column are the warps of one block (blockDim = 32 ceil(nlay / CL)).  Each thread reads its
+// layers once (coalesced 128-byte rows, all loads of the chunk in flight together), composes
+// the chunk's affine maps in registers, the chunks exchange the maps through shared memory,
+// and a re-sweep of the registers writes every level once: the HBM traffic is the algorithmic
+// one (inputs read once, outputs written once), with no shared-memory stash or workspace.
+template <typename T, int CL, int MAXT>
+__global__ void __launch_bounds__(MAXT) lw_solver_chunked(int ncol, int nlay, int nband, int top_at_1,
+                                                          const int* __restrict__ gpt2band, const T* __restrict__ tau,
+                                                          const T* __restrict__ lay_src, const T* __restrict__ lev_inc,
+                                                          const T* __restrict__ lev_dec, const T* __restrict__ sfc_src,
+                                                          const T* __restrict__ sfc_emis, const T* __restrict__ inc_flux,
+                                                          T* __restrict__ flux_up, T* __restrict__ flux_dn)
+{
+    __shared__ T sm_a[16 * 32], sm_bd[16 * 32], sm_bu[16 * 32];   // chunk maps [chunk][lane]
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int icol = blockIdx.x * 32 + lane;
+    const bool cv = icol < ncol;
+    const int ic = cv ? icol : 0;
+    const int g = blockIdx.y;
+    const size_t ncl = size_t(ncol) * nlay, ncv = size_t(ncol) * (nlay + 1);
+    const T* lev_dn = top_at_1 ? lev_inc : lev_dec;
+    const T* lev_up = top_at_1 ? lev_dec : lev_inc;
+    const int j0 = w * CL;
+    // one angle (D = 1.66, weight 0.5: Rte_lw.cpp:101-113)
+    const T D = T(1.66);
+    const T two_pi_w = pi_value<T>();
+
+    // every input of the chunk is read before any is used (the layer terms branch, and loads
+    // are not moved above a branch: read in the loop, one layer's rows would be in flight)
+    T tr[CL], sdn[CL], sup[CL], lay[CL];
+#pragma unroll
+    for (int i = 0; i < CL; ++i) {
+        const int j = j0 + i;
+        tr[i] = T(0); lay[i] = T(0); sdn[i] = T(0); sup[i] = T(0);
+        if (cv && j < nlay) {
+            const size_t x = ic + size_t(g) * ncl + size_t(top_at_1 ? j : nlay - 1 - j) * ncol;
+            tr[i] = tau[x];
+            lay[i] = lay_src[x];
+            sdn[i] = lev_dn[x];
+            sup[i] = lev_up[x];
+        }
+    }
+    T A = T(1), Bd = T(0), Bu = T(0);
+#pragma unroll
+    for (int i = 0; i < CL; ++i) {
+        lw_layer(tr[i], D, lay[i], sdn[i], sup[i], tr[i], sdn[i], sup[i]);   // tau -> trans (1 for padding)
+        A *= tr[i];
+        Bd = tr[i] * Bd + sdn[i];
+    }
+#pragma unroll
+    for (int i = CL - 1; i >= 0; --i) Bu = tr[i] * Bu + sup[i];
+    sm_a[w * 32 + lane] = A;
+    sm_bd[w * 32 + lane] = Bd;
+    sm_bu[w * 32 + lane] = Bu;
+    __syncthreads();
+    if (!cv) return;
+    // radiance entering the chunk at its top, then at the surface
+    T radn = (inc_flux ? inc_flux[ic + size_t(g) * ncol] : T(0)) / two_pi_w;
+    for (int c = 0; c < w; ++c) radn = sm_a[c * 32 + lane] * radn + sm_bd[c * 32 + lane];
+    T rs = radn;
+    for (int c = w; c < nw; ++c) rs = sm_a[c * 32 + lane] * rs + sm_bd[c * 32 + lane];
+    const T emis = sfc_emis[gpt2band[g] + size_t(ic) * nband];
+    const T rsfc = rs * (T(1) - emis) + emis * sfc_src[ic + size_t(g) * ncol];   // leaving the surface
+    T rup = rsfc;
+    for (int c = nw - 1; c > w; --c) rup = sm_a[c * 32 + lane] * rup + sm_bu[c * 32 + lane];
+    // re-sweeps: level j0 + i is the top of layer j0 + i
+    T* const dn = flux_dn + ic + size_t(g) * ncv;
+    T* const up = flux_up + ic + size_t(g) * ncv;
+    const ptrdiff_t step = top_at_1 ? ptrdiff_t(ncol) : -ptrdiff_t(ncol);
+    const ptrdiff_t o0 = top_at_1 ? ptrdiff_t(j0) * ncol : ptrdiff_t(nlay - j0) * ncol;   // level j0
+    if (w == 0) dn[o0] = two_pi_w * radn;
+#pragma unroll
+    for (int i = 0; i < CL; ++i) {
+        radn = tr[i] * radn + sdn[i];
+        if (j0 + i < nlay) dn[o0 + (i + 1) * step] = two_pi_w * radn;
+    }
+    if (j0 <= nlay - 1 && nlay - 1 < j0 + CL) up[o0 + (nlay - j0) * step] = two_pi_w * rsfc;
+#pragma unroll
+    for (int i = CL - 1; i >= 0; --i) {
+        rup = tr[i] * rup + sup[i];
+        if (j0 + i < nlay) up[o0 + i * step] = two_pi_w * rup;
+    }
+}
+
+// Rdir and Tdir of the FP64 island of the FP32 two-stream (sw_layer_fast), out of line.
+__device__ __noinline__ float2 island_dir(float tau, float w0, float g, float mu0)
+{
+    return fused::sw_island_dir_inl(tau, w0, g, mu0);
+}
+
+template <typename T>
+__device__ __forceinline__ T adding_den(T R, T a) { return T(1) / (T(1) - R * a); }
+template <>
+__device__ __forceinline__ float adding_den<float>(float R, float a) { return __fdividef(1.f, fmaf(-R, a, 1.f)); }
+
+template <typename T, int CL, int MAXT, int MINB = 1>
+__global__ void __launch_bounds__(MAXT, MINB) sw_solver_chunked(int ncol, int nlay, int nband, int top_at_1,
+                                                         const int* __restrict__ gpt2band, const T* __restrict__ tau,
+                                                         const T* __restrict__ ssa, const T* __restrict__ gasy,
+                                                         const T* __restrict__ mu0, const T* __restrict__ inc_dir,
+                                                         const T* __restrict__ alb_dir, const T* __restrict__ alb_dif,
+                                                         const T* __restrict__ inc_dif, T* __restrict__ flux_up,
+                                                         T* __restrict__ flux_dn, T* __restrict__ flux_dir)
+{
+    __shared__ T sm_p[16 * 32];                                      // direct-beam product per chunk
+    __shared__ float4 sm_isl[sizeof(T) == 4 ? 16 * 32 : 1];          // FP64 island tasks (FP32)
+    __shared__ T sm_ru[16 * 32], sm_rd[16 * 32], sm_t[16 * 32], sm_u[16 * 32], sm_d[16 * 32];   // composites
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int icol = blockIdx.x * 32 + lane;
+    const bool cv = icol < ncol;
+    const int ic = cv ? icol : 0;
+    const int g = blockIdx.y;
+    const size_t ncl = size_t(ncol) * nlay, ncv = size_t(ncol) * (nlay + 1);
+    const size_t base = ic + size_t(g) * ncl;
+    const int band = gpt2band[g];
+    const T m0 = mu0[ic], m0_inv = T(1) / m0;
+    const T ad = alb_dir[band + size_t(ic) * nband], af = alb_dif[band + size_t(ic) * nband];
+    const T dir_toa = inc_dir[ic + size_t(g) * ncol] * m0;
+    const T fd_toa = inc_dif ? inc_dif[ic + size_t(g) * ncol] : T(0);
+    const int j0 = w * CL;
+
+    // 1. layer coefficients; direct beam relative to the chunk top; adding composite of the chunk
+    T vR[CL], vT[CL], vSu[CL], vSd[CL], vP[CL];
+    T P = T(1), cRu = T(0), cRd = T(0), cT = T(1), cU = T(0), cD = T(0);
+    auto add_layer = [&](int i, T R, T Tt, T Rdir, T Tdir, T Tn) {
+        vR[i] = R;
+        vT[i] = Tt;
+        vP[i] = P;
+        vSu[i] = Rdir * P;
+        vSd[i] = Tdir * P;
+        const T den = adding_den(cRd, R);
+        const T nRu = cRu + cT * cT * R * den;
+        const T nRd = R + Tt * Tt * cRd * den;
+        const T nU = cU + cT * (vSu[i] + R * cD) * den;
+        const T nD = vSd[i] + Tt * (cD + cRd * vSu[i]) * den;
+        cT = cT * Tt * den;
+        cRu = nRu;
+        cRd = nRd;
+        cU = nU;
+        cD = nD;
+        P *= Tn;
+    };
+    if constexpr (sizeof(T) == 4) {
+        // FP32 two-stream (sw_layer_fast) with its FP64 island run once per warp: the (layer,
+        // column) pairs near k mu0 = 1 are sparse and scattered over the lanes, so the first
+        // 32 of the chunk are computed together, one per lane; any beyond run in place.
+        float vTau[CL], vW0[CL], vG[CL];
+        float4* const isl_buf = sm_isl + w * 32;
+        unsigned isl = 0;
+        int ntask = 0;
+#pragma unroll
+        for (int i = 0; i < CL; ++i) {
+            const int j = j0 + i;
+            const bool valid = cv && j < nlay;
+            vTau[i] = 0.f; vW0[i] = 0.f; vG[i] = 0.f;
+            if (valid) {
+                const size_t x = base + size_t(top_at_1 ? j : nlay - 1 - j) * ncol;
+                vTau[i] = tau[x];
+                vW0[i] = ssa[x];
+                vG[i] = gasy[x];
+            }
+            const bool f = valid && fused::sw_island(vW0[i], 1.f - vW0[i], vG[i], m0);
+            const unsigned m = __ballot_sync(0xffffffffu, f);
+            const int idx = ntask + __popc(m & ((1u << lane) - 1u));
+            if (f) {
+                isl |= 1u << i;
+                if (idx < 32) isl_buf[idx] = make_float4(vTau[i], vW0[i], vG[i], m0);
+            }
+            ntask += __popc(m);
+        }
+        __syncwarp();
+        if (lane < ntask) {
+            const float4 q = isl_buf[lane];
+            const float2 d = island_dir(q.x, q.y, q.z, q.w);
+            isl_buf[lane] = make_float4(d.x, d.y, 0.f, 0.f);
+        }
+        __syncwarp();
+        int first = 0;
+#pragma unroll
+        for (int i = 0; i < CL; ++i) {
+            const bool f = (isl >> i) & 1u;
+            const unsigned m = __ballot_sync(0xffffffffu, f);
+            const int idx = first + __popc(m & ((1u << lane) - 1u));
+            first += __popc(m);
+            fused::SwLayerPre pre;
+            fused::sw_layer_fast_pre(vTau[i], vW0[i], 1.f - vW0[i], vG[i], m0, m0_inv, f, pre);
+            float Rd = pre.Rdir0, Td = pre.Tdir0;
+            if (f) {
+                const float2 d = idx < 32 ? make_float2(isl_buf[idx].x, isl_buf[idx].y)
+                                          : island_dir(vTau[i], vW0[i], vG[i], m0);
+                Rd = d.x;
+                Td = d.y;
+            }
+            float Rdir, Tdir, adir;
+            fused::sw_layer_clamp(pre, Rd, Td, Rdir, Tdir, adir);
+            add_layer(i, pre.R, pre.T, Rdir, Tdir, pre.Tn);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < CL; ++i) {
+            const int j = j0 + i;
+            T R = T(0), Tt = T(1), Rdir = T(0), Tdir = T(0), Tn = T(1);
+            if (cv && j < nlay) {
+                const size_t x = base + size_t(top_at_1 ? j : nlay - 1 - j) * ncol;
+                sw_two_stream<T>(tau[x], ssa[x], gasy[x], m0, R, Tt, Rdir, Tdir, Tn);
+            }
+            add_layer(i, R, Tt, Rdir, Tdir, Tn);
+        }
+    }
+    sm_p[w * 32 + lane] = P;
+    __syncthreads();
+    // 2. direct beam at the chunk top and at the surface
+    T dtop = dir_toa;
+    for (int c = 0; c < w; ++c) dtop *= sm_p[c * 32 + lane];
+    T dsfc = dtop;
+    for (int c = w; c < nw; ++c) dsfc *= sm_p[c * 32 + lane];
+    sm_ru[w * 32 + lane] = cRu;
+    sm_rd[w * 32 + lane] = cRd;
+    sm_t[w * 32 + lane] = cT;
+    sm_u[w * 32 + lane] = cU * dtop;
+    sm_d[w * 32 + lane] = cD * dtop;
+    __syncthreads();
+    // 3. albedo and source at the chunk bottom (from the surface up), and the diffuse flux at
+    //    the chunk top as fa * (TOA diffuse) + fb
+    T alb = af, src = dsfc * ad, alb_in = af, src_in = dsfc * ad, fa = T(1), fb = T(0);
+    for (int c = nw - 1; c >= 0; --c) {
+        if (c == w) {
+            alb_in = alb;
+            src_in = src;
+            if (w == 0) break;
+        }
+        const T mRu = sm_ru[c * 32 + lane], mRd = sm_rd[c * 32 + lane], mT = sm_t[c * 32 + lane];
+        const T mU = sm_u[c * 32 + lane], mD = sm_d[c * 32 + lane];
+        const T den = adding_den(mRd, alb);
+        if (c < w) {
+            const T F = mT * den, G = (mRd * src + mD) * den;
+            fb = fa * G + fb;
+            fa *= F;
+        }
+        const T nalb = mRu + mT * mT * alb * den;
+        src = mU + mT * (alb * mD + src) * den;
+        alb = nalb;
+    }
+    // 4. albedo and upward source at the top of every layer (bottom-up)
+    T vA[CL];
+    {
+        T a = alb_in, s = src_in;
+#pragma unroll
+        for (int i = CL - 1; i >= 0; --i) {
+            const T su = vSu[i] * dtop, sd = vSd[i] * dtop;
+            const T den = adding_den(vR[i], a);
+            const T na = vR[i] + vT[i] * vT[i] * a * den;
+            const T ns = su + vT[i] * (a * sd + s) * den;
+            vSd[i] = sd;
+            vSu[i] = ns;
+            vA[i] = na;
+            a = na;
+            s = ns;
+        }
+    }
+    // 5. diffuse fluxes (top-down) and the level outputs
+    if (!cv) return;
+    const size_t off = ic + size_t(g) * ncv;
+    const ptrdiff_t step = top_at_1 ? ptrdiff_t(ncol) : -ptrdiff_t(ncol);
+    const ptrdiff_t o0 = top_at_1 ? ptrdiff_t(j0) * ncol : ptrdiff_t(nlay - j0) * ncol;   // level j0
+    T* const up = flux_up + off;
+    T* const dn = flux_dn + off;
+    T* const dr = flux_dir + off;
+    T fd = fa * fd_toa + fb;
+#pragma unroll
+    for (int i = 0; i < CL; ++i) {
+        const T a_n = (i + 1 < CL) ? vA[i + 1] : alb_in;
+        const T s_n = (i + 1 < CL) ? vSu[i + 1] : src_in;
+        if (j0 + i < nlay) {
+            const T dir = dtop * vP[i];
+            up[o0 + i * step] = fd * vA[i] + vSu[i];
+            dn[o0 + i * step] = fd + dir;
+            dr[o0 + i * step] = dir;
+        }
+        const T den = adding_den(vR[i], a_n);
+        fd = (vT[i] * fd + vR[i] * s_n + vSd[i]) * den;
+    }
+    if (j0 <= nlay - 1 && nlay - 1 < j0 + CL) {
+        // fd is now at the chunk bottom (padding layers are the identity): the surface level
+        const ptrdiff_t o = o0 + (nlay - j0) * step;
+        up[o] = fd * alb_in + src_in;
+        dn[o] = fd + dsfc;
+        dr[o] = dsfc;
+    }
+}
+
 template <typename T>
 int lw_smem_block(int nlay, size_t* smem)
 {
@@ -190,6 +490,21 @@ int rte_lw(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const T* tau, 
     RB_CHECK_ARG(nmus >= 1 && nmus <= 4, "rte_lw: n_gauss_angles must be 1..4");
     RB_CHECK_ARG(tau && lay_src && lev_inc && lev_dec && sfc_src && sfc_emis && flux_up && flux_dn,
                  "rte_lw: null array");
+    if (nmus == 1 && nlay <= 16 * 16) {
+        const dim3 grid(ceil_div(ncol, 32), b->ngpt);
+        // FP32 up to 128 layers: 8-layer chunks (more warps with fewer rows in flight each
+        // measured faster than 16 at 8192 x 128); FP64 and deeper columns: 16-layer chunks
+        if (sizeof(T) == 4 && nlay <= 8 * 16)
+            lw_solver_chunked<T, 8, 512><<<grid, 32 * ceil_div(nlay, 8), 0, as_stream(stream)>>>(
+                ncol, nlay, b->nband, top_at_1, b->d_gpt2band, tau, lay_src, lev_inc, lev_dec, sfc_src, sfc_emis,
+                inc_flux, flux_up, flux_dn);
+        else
+            lw_solver_chunked<T, 16, 512><<<grid, 32 * ceil_div(nlay, 16), 0, as_stream(stream)>>>(
+                ncol, nlay, b->nband, top_at_1, b->d_gpt2band, tau, lay_src, lev_inc, lev_dec, sfc_src, sfc_emis,
+                inc_flux, flux_up, flux_dn);
+        RB_LAUNCH("lw_solver_chunked");
+        return RRTMGP_B200_OK;
+    }
     size_t smem = 0;
     const int bs = lw_smem_block<T>(nlay, &smem);
     if (bs > 0) {
@@ -230,6 +545,26 @@ int rte_sw(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const T* tau, 
     const size_t need = sw_ws_bytes(ncol, nlay, b->ngpt, sizeof(T) == 8);
     if (!ws || ws_bytes < need)
         return fail(RRTMGP_B200_ERR_WORKSPACE, "rte_sw: workspace of " + std::to_string(need) + " bytes required");
+    // Chunked solver up to 256 layers (FP64: 128; its deeper columns would spill registers).
+    constexpr bool fp64 = sizeof(T) == 8;
+    if (nlay <= (fp64 ? 128 : 256)) {
+        const dim3 grid(ceil_div(ncol, 32), b->ngpt);
+        if constexpr (fp64) {
+            sw_solver_chunked<T, 16, 256><<<grid, 32 * ceil_div(nlay, 16), 0, as_stream(stream)>>>(
+                ncol, nlay, b->nband, top_at_1, b->d_gpt2band, tau, ssa, g, mu0, inc_dir, alb_dir, alb_dif, inc_dif,
+                flux_up, flux_dn, flux_dir);
+        } else if (nlay <= 128) {
+            sw_solver_chunked<T, 8, 512, 2><<<grid, 32 * ceil_div(nlay, 8), 0, as_stream(stream)>>>(
+                ncol, nlay, b->nband, top_at_1, b->d_gpt2band, tau, ssa, g, mu0, inc_dir, alb_dir, alb_dif, inc_dif,
+                flux_up, flux_dn, flux_dir);
+        } else {
+            sw_solver_chunked<T, 16, 512><<<grid, 32 * ceil_div(nlay, 16), 0, as_stream(stream)>>>(
+                ncol, nlay, b->nband, top_at_1, b->d_gpt2band, tau, ssa, g, mu0, inc_dir, alb_dir, alb_dif, inc_dif,
+                flux_up, flux_dn, flux_dir);
+        }
+        RB_LAUNCH("sw_solver_chunked");
+        return RRTMGP_B200_OK;
+    }
     const dim3 grid(ceil_div(ncol, 64), b->ngpt);
     sw_solver_kernel<T, double><<<grid, 64, 0, as_stream(stream)>>>(
         ncol, nlay, b->ngpt, b->nband, top_at_1, b->d_gpt2band, tau, ssa, g, mu0, inc_dir, alb_dir, alb_dif,

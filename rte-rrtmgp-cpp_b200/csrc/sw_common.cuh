@@ -46,9 +46,23 @@ __device__ __forceinline__ void one_minus_exp(float x, float& E, float& e)
 // from absorption optical depths, so it keeps its accuracy for w0 -> 1.  Clamps and k_min are
 // those of the FP64 reference (DBL_EPSILON, 1e-12).  Divisions and the square root use the
 // approximate intrinsics (a few ulp; the operands are normal numbers).
-__device__ __forceinline__ void sw_layer_fast(float tau, float w0, float omw, float g, float mu0, float mu0_inv,
-                                              float& R, float& T, float& Rdir, float& Tdir, float& Tn,
-                                              float& adif, float& adir)
+struct SwLayerPre {
+    float R, T, adif, Tn, En, Rdir0, Tdir0;   // Rdir0, Tdir0: before the clamps (FP32 values)
+};
+
+// The island test of sw_layer_fast (independent of tau): |1 - (k mu0)^2| < 0.02.
+__device__ __forceinline__ bool sw_island(float w0, float omw, float g, float mu0)
+{
+    const float kk = 2.f * omw * (2.f - .5f * w0 * (1.f + 3.f * g));
+    const float kkc = fmaxf(kk, 1.e-12f);
+    const float km = kkc * rsqrtf(kkc) * mu0;
+    return fabsf((1.f - km) * (1.f + km)) < 0.02f;
+}
+
+// FP32 part of sw_layer_fast.  island: the layer takes the FP64 island (sw_island), where
+// Rdir0 and Tdir0 are meaningless and sw_island_dir_inl supplies them.
+__device__ __forceinline__ void sw_layer_fast_pre(float tau, float w0, float omw, float g, float mu0, float mu0_inv,
+                                                  bool island, SwLayerPre& p)
 {
     const float g1 = (8.f - w0 * (5.f + 3.f * g)) * .25f;
     const float g2 = 3.f * (w0 * (1.f - g)) * .25f;
@@ -59,37 +73,66 @@ __device__ __forceinline__ void sw_layer_fast(float tau, float w0, float omw, fl
     const float kk = 2.f * omw * (2.f - .5f * w0 * (1.f + 3.f * g));
     const float kkc = fmaxf(kk, 1.e-12f);
     const float k = kkc * rsqrtf(kkc);
-    float E1, e1, En;
+    float E1, e1, En, Tn;
     one_minus_exp(k * tau, E1, e1);
     one_minus_exp(tau * mu0_inv, En, Tn);
     const float E2 = E1 * (2.f - E1);
     const float e2 = e1 * e1;
     const float rt = __fdividef(1.f, k * (1.f + e2) + g1 * E2);
-    R = rt * g2 * E2;
-    T = rt * 2.f * k * e1;
-    adif = rt * (k * E1 * E1 + 2.f * omw * E2);
+    p.R = rt * g2 * E2;
+    p.T = rt * 2.f * k * e1;
+    p.adif = rt * (k * E1 * E1 + 2.f * omw * E2);
+    p.Tn = Tn;
+    p.En = En;
     const float km = k * mu0;
     const float fact = (1.f - km) * (1.f + km);
-    if (fabsf(fact) < 0.02f) {
-        double Rd, Td, Rr, Tr, Tn64;
-        sw_two_stream<double>(double(tau), double(w0), double(g), double(mu0), Rd, Td, Rr, Tr, Tn64);
-        Rdir = float(Rr);
-        Tdir = float(Tr);
-    } else {
-        const float rt2 = __fdividef(w0 * rt, fact);
-        const float br = E2 * (a2 - k * km * g3) + k * (g3 - mu0 * a2) * (E1 * E1 + 2.f * e1 * En);
-        const float bt_thick =
-            (1.f + km) * (a1 + k * g4) * Tn - (1.f - km) * (a1 - k * g4) * e2 * Tn - 2.f * (k * g4 + a1 * km) * e1;
-        const float bt_thin = Tn * E2 * (a1 + k * km * g4) + k * (g4 + mu0 * a1) * (E1 * E1 - (1.f + e2) * En);
-        const float bt = (e1 < .5f && Tn < .5f) ? bt_thick : bt_thin;
-        Rdir = rt2 * br;
-        Tdir = -rt2 * bt;
-    }
+    const float rt2 = __fdividef(w0 * rt, island ? 1.f : fact);
+    const float br = E2 * (a2 - k * km * g3) + k * (g3 - mu0 * a2) * (E1 * E1 + 2.f * e1 * En);
+    const float bt_thick =
+        (1.f + km) * (a1 + k * g4) * Tn - (1.f - km) * (a1 - k * g4) * e2 * Tn - 2.f * (k * g4 + a1 * km) * e1;
+    const float bt_thin = Tn * E2 * (a1 + k * km * g4) + k * (g4 + mu0 * a1) * (E1 * E1 - (1.f + e2) * En);
+    const float bt = (e1 < .5f && Tn < .5f) ? bt_thick : bt_thin;
+    p.Rdir0 = rt2 * br;
+    p.Tdir0 = -rt2 * bt;
+}
+
+// Rdir and Tdir of the FP64 island: the reference expressions in double.
+__device__ __forceinline__ float2 sw_island_dir_inl(float tau, float w0, float g, float mu0)
+{
+    double Rd, Td, Rr, Tr, Tn64;
+    sw_two_stream<double>(double(tau), double(w0), double(g), double(mu0), Rd, Td, Rr, Tr, Tn64);
+    return make_float2(float(Rr), float(Tr));
+}
+
+// The clamps of the reference (rte_solver_kernels.cu:582-583) and the direct absorptance.
+__device__ __forceinline__ void sw_layer_clamp(const SwLayerPre& p, float Rdir0, float Tdir0, float& Rdir, float& Tdir,
+                                               float& adir)
+{
     const float tmin = 2.220446049250313e-16f;
-    Rdir = fmaxf(tmin, fminf(Rdir, En));
-    const float rest = En - Rdir;
-    Tdir = fmaxf(tmin, fminf(Tdir, rest));
+    Rdir = fmaxf(tmin, fminf(Rdir0, p.En));
+    const float rest = p.En - Rdir;
+    Tdir = fmaxf(tmin, fminf(Tdir0, rest));
     adir = fmaxf(0.f, rest - Tdir);
+}
+
+__device__ __forceinline__ void sw_layer_fast(float tau, float w0, float omw, float g, float mu0, float mu0_inv,
+                                              float& R, float& T, float& Rdir, float& Tdir, float& Tn,
+                                              float& adif, float& adir)
+{
+    SwLayerPre p;
+    const bool island = sw_island(w0, omw, g, mu0);
+    sw_layer_fast_pre(tau, w0, omw, g, mu0, mu0_inv, island, p);
+    float Rd = p.Rdir0, Td = p.Tdir0;
+    if (island) {
+        const float2 d = sw_island_dir_inl(tau, w0, g, mu0);
+        Rd = d.x;
+        Td = d.y;
+    }
+    R = p.R;
+    T = p.T;
+    Tn = p.Tn;
+    adif = p.adif;
+    sw_layer_clamp(p, Rd, Td, Rdir, Tdir, adir);
 }
 
 __device__ __forceinline__ void build_sw_record(const KdistView<float>& k, Rec& R, const LayerState& s,

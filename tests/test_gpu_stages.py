@@ -249,6 +249,47 @@ def test_rte_sw(api, oracle_mod, tables, gpu, prec, top_at_1, with_dif):
     cmp_flux("flux_up", N(gu), up, prec)
 
 
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+@pytest.mark.parametrize("nlay", [129, 200, 257])
+@pytest.mark.parametrize("top_at_1", [True, False])
+def test_rte_deep_columns(api, oracle_mod, tables, gpu, prec, nlay, top_at_1):
+    """Layer counts around the solvers' kernel switches: the chunked kernels take 16-layer
+    chunks above 128 layers (the FP64 shortwave switches to one thread per column and g-point
+    there) and both solvers switch to one thread per column and g-point above 256."""
+    dt = dtypes()[prec]
+    ncol = 33
+    atm = S.make_atmosphere(ncol, nlay, seed=nlay, clouds=True, top_at_1=top_at_1)
+    kd_lw = api.Gas_optics_rrtmgp(tables["lw"], S.ATM_GASES)
+    go = oracle_mod.GasOptics(tables["lw"], S.ATM_GASES).gas_optics_lw(
+        atm["play"], atm["plev"], atm["tlay"], atm["tsfc"], atm["gases"], atm["tlev"])
+    emis = np.random.default_rng(nlay).uniform(0.8, 1.0, (ncol, 16))
+    up, dn = oracle_mod.rte_lw(tables["lw"]["bnd_limits_gpt"], go["tau"], top_at_1, go, emis)
+    src = {k: T(v, dt, gpu) for k, v in go.items()}
+    gu, gd = api.Rte_lw.rte_lw(kd_lw.bands, src["tau"], top_at_1, src, T(emis, dt, gpu))
+    cmp_flux("lw flux_up", N(gu), up, prec)
+    cmp_flux("lw flux_dn", N(gd), dn, prec)
+
+    ko = oracle_mod.GasOptics(tables["sw"], S.ATM_GASES)
+    gs = ko.gas_optics_sw(atm["play"], atm["plev"], atm["tlay"], atm["gases"])
+    c = oracle_mod.CloudOptics(tables["cloud_sw"]).cloud_optics(atm["lwp"], atm["iwp"], atm["rel"], atm["rei"], True)
+    oracle_mod.delta_scale(c["tau"], c["ssa"], c["g"])
+    bl = tables["sw"]["bnd_limits_gpt"]
+    oracle_mod.add_to(bl, gs, c)
+    rng = np.random.default_rng(nlay + 1)
+    alb_dir = rng.uniform(0.05, 0.3, (ncol, 14))
+    alb_dif = rng.uniform(0.05, 0.3, (ncol, 14))
+    inc_dif = rng.uniform(0, 1, (224, ncol))
+    up, dn, dr = oracle_mod.rte_sw(bl, gs["tau"], gs["ssa"], gs["g"], top_at_1, atm["mu0"], gs["toa_src"],
+                                   alb_dir, alb_dif, inc_dif)
+    kd_sw = api.Gas_optics_rrtmgp(tables["sw"], S.ATM_GASES)
+    gu, gd, gr = api.Rte_sw.rte_sw(kd_sw.bands, T(gs["tau"], dt, gpu), T(gs["ssa"], dt, gpu), T(gs["g"], dt, gpu),
+                                   top_at_1, T(atm["mu0"], dt, gpu), T(gs["toa_src"], dt, gpu),
+                                   T(alb_dir, dt, gpu), T(alb_dif, dt, gpu), T(inc_dif, dt, gpu))
+    cmp_flux("sw flux_dir", N(gr), dr, prec)
+    cmp_flux("sw flux_dn", N(gd), dn, prec)
+    cmp_flux("sw flux_up", N(gu), up, prec)
+
+
 def test_rte_sw_workspace_required(api, tables, gpu):
     import torch
     from rrtmgp_b200._abi import RrtmgpError, ERR_WORKSPACE

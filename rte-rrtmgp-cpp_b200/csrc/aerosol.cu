@@ -30,11 +30,22 @@ AerosolLut<double> lut_view<double>(const rrtmgp_b200_aerosol_t* a)
     return AerosolLut<double>{a->nband, a->nhum, a->nphilic, a->nphobic, a->lut64};
 }
 
+// One thread per (column, layer).  The block first copies the tables (a few thousand values)
+// into shared memory: the per-band lookups of the 11 species then cost shared-memory loads
+// (same address across the warp for the hydrophobic species, distinct banks for the
+// hydrophilic ones, whose rows differ by nband per humidity class) instead of L1 gathers.
 template <typename T>
-__global__ void aerosol_optics_kernel(const AerosolLut<T> L, const AerosolSet<T> as, int ncol, int nlay,
-                                      const T* __restrict__ rh, const T* __restrict__ plev, T* __restrict__ tau,
-                                      T* __restrict__ ssa, T* __restrict__ g)
+__global__ void __launch_bounds__(512) aerosol_optics_kernel(const AerosolLut<T> Lg, const AerosolSet<T> as, int ncol,
+                                                             int nlay, const T* __restrict__ rh,
+                                                             const T* __restrict__ plev, T* __restrict__ tau,
+                                                             T* __restrict__ ssa, T* __restrict__ g)
 {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* tab = reinterpret_cast<T*>(smem_raw);
+    const int n = Lg.nhum + 3 * Lg.nphobic * Lg.nband + 3 * Lg.nphilic * Lg.nhum * Lg.nband;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) tab[i] = Lg.tab[i];
+    __syncthreads();
+    const AerosolLut<T> L{Lg.nband, Lg.nhum, Lg.nphilic, Lg.nphobic, tab};
     const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     const size_t ncl = size_t(ncol) * nlay;
     if (i >= ncl) return;
@@ -53,6 +64,12 @@ __global__ void aerosol_optics_kernel(const AerosolLut<T> L, const AerosolSet<T>
         ssa[o] = ts / (t > eps ? t : eps);
         g[o] = tsg / (ts > eps ? ts : eps);
     }
+}
+
+template <typename T>
+size_t aerosol_smem(const rrtmgp_b200_aerosol_t* a)
+{
+    return sizeof(T) * (size_t(a->nhum) + 3 * size_t(a->nphobic) * a->nband + 3 * size_t(a->nphilic) * a->nhum * a->nband);
 }
 
 }  // namespace
@@ -100,8 +117,13 @@ int aerosol_optics(rrtmgp_b200_aerosol a, int ncol, int nlay, const rrtmgp_b200_
     int st = make_aerosol_set<T>(ncol, nlay, aer, naer, as);
     if (st) return st;
     const size_t n = size_t(ncol) * nlay;
-    const int threads = 128;
-    aerosol_optics_kernel<T><<<unsigned((n + threads - 1) / threads), threads, 0, as_stream(stream)>>>(
+    const int threads = 512;
+    const size_t smem = aerosol_smem<T>(a);
+    RB_CHECK_ARG(smem <= 227 * 1024, "aerosol_optics: tables exceed shared memory");
+    if (smem > 48 * 1024)
+        RB_CUDA(cudaFuncSetAttribute(aerosol_optics_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+                "aerosol_optics attribute");
+    aerosol_optics_kernel<T><<<unsigned((n + threads - 1) / threads), threads, smem, as_stream(stream)>>>(
         lut_view<T>(a), as, ncol, nlay, rh, plev, tau, ssa, g);
     RB_LAUNCH("aerosol_optics_kernel");
     return RRTMGP_B200_OK;

@@ -503,7 +503,8 @@ struct SwAdjLayout {
     size_t state, cg, seeds, clsum, albacc, x1, x2, x3, x4, x5, recs, drecs, isl, total;
 };
 
-__host__ __device__ __forceinline__ SwAdjLayout sw_adj_layout(int ngas, int nband, int mgb, int CS, int WPC)
+__host__ __device__ __forceinline__ SwAdjLayout sw_adj_layout(int ngas, int nband, int mgb, int CS, int WPC,
+                                                              int nbuf)
 {
     SwAdjLayout L;
     L.state = 0;
@@ -519,8 +520,8 @@ __host__ __device__ __forceinline__ SwAdjLayout sw_adj_layout(int ngas, int nban
     L.x4 = align16(L.x3 + sizeof(float2) * nw);
     L.x5 = align16(L.x4 + (sizeof(float4) + sizeof(float)) * nw);
     L.recs = align16(L.x5 + sizeof(float2) * nw);
-    L.drecs = align16(L.recs + sizeof(Rec) * size_t(kLPC) * mgb);
-    L.isl = align16(L.drecs + sizeof(DRec) * size_t(kLPC) * mgb);
+    L.drecs = align16(L.recs + sizeof(Rec) * size_t(kLPC) * mgb * nbuf);
+    L.isl = align16(L.drecs + sizeof(DRec) * size_t(kLPC) * mgb * nbuf);
     L.total = align16(L.isl + sizeof(float) * kIslTask * 32 * WPC);
     return L;
 }
@@ -533,7 +534,7 @@ __device__ __forceinline__ Tp* remote(cg::cluster_group& cl, Tp* p, int rank)
 
 // CL layers per warp, kLPC / CL warps per CTA: CL = 8 gives 8 warps with up to 255 registers,
 // CL = 4 gives 16 warps at 128 registers (half the per-layer values per thread).
-template <int CL, bool FLUX>
+template <int CL, bool FLUX, bool PAIR>
 __global__ void __launch_bounds__(kLPC / CL * 32, 1)
 sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwCloudArgs cld, int ncol, int nlay, int CS,
                   int idx_o3, int cd_internal, const float* __restrict__ play, const float* __restrict__ plev,
@@ -554,7 +555,7 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
     const int L_end = NWt * CL;
     const int j0 = rank * kLPC;          // first global layer of this CTA
     const int nband = k.nband, mgb = k.max_group_bands;
-    const SwAdjLayout SL = sw_adj_layout(k.ngas, nband, mgb, CS, WPC);
+    const SwAdjLayout SL = sw_adj_layout(k.ngas, nband, mgb, CS, WPC, PAIR ? 2 : 1);
     LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
     float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
     float* sm_al = reinterpret_cast<float*>(smem_raw + SL.seeds);   // seed F_up per local level (0..64)
@@ -570,8 +571,8 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
     float4* sm_x4a = reinterpret_cast<float4*>(smem_raw + SL.x4);
     float* sm_x4b = reinterpret_cast<float*>(sm_x4a + NWt * 32);
     float2* sm_x5 = reinterpret_cast<float2*>(smem_raw + SL.x5);
-    Rec* recs = reinterpret_cast<Rec*>(smem_raw + SL.recs) + w * CL * mgb;
-    DRec* drecs = reinterpret_cast<DRec*>(smem_raw + SL.drecs) + w * CL * mgb;
+    Rec* const recs0 = reinterpret_cast<Rec*>(smem_raw + SL.recs) + w * CL * mgb;
+    DRec* const drecs0 = reinterpret_cast<DRec*>(smem_raw + SL.drecs) + w * CL * mgb;
     float* sm_isl = reinterpret_cast<float*>(smem_raw + SL.isl) + w * 32 * kIslTask;
 
     const bool top_at_1 = play[icol] < play[icol + size_t(nlay - 1) * ncol];
@@ -645,20 +646,26 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
         const float ad = gv ? __ldg(alb_dir + gband + size_t(icol) * nband) : 0.f;
         const float af = gv ? __ldg(alb_dif + gband + size_t(icol) * nband) : 0.f;
 
-        // forward records on one half of the tasks, derivative records on the other (they are
-        // independent): with 8 layers and 2 bands every lane builds one
-        for (int t = lane; t < 2 * CL * mgb; t += 32) {
-            const int r = t % (CL * mgb);
-            const int jl = w * CL + (r % CL);
-            const int jj = j0 + jl;
-            const int b = b0 + r / CL;
-            if (jj < nlay && b < nband && k.band_lims[2 * b] < 32 * gg + 32) {
-                const LayerState s = st[jl];
-                if (t < CL * mgb) {
+        // Records (forward and derivative) of every (layer, band) of the group.  With PAIR, the
+        // records of groups gg and gg + 1 are built together at even gg into two buffers: with
+        // 8 layers and 2 bands a group has 16 records per warp, so one group alone leaves half
+        // the lanes idle.
+        Rec* const recs = recs0 + (PAIR ? (gg & 1) : 0) * kLPC * mgb;
+        DRec* const drecs = drecs0 + (PAIR ? (gg & 1) : 0) * kLPC * mgb;
+        if (!PAIR || (gg & 1) == 0) {
+            const int nrec = CL * mgb;
+            for (int t = lane; t < (PAIR ? 2 : 1) * nrec; t += 32) {
+                const int gq = gg + t / nrec, r = t % nrec;
+                if (gq >= k.ngroups) continue;
+                const int jl = w * CL + (r % CL);
+                const int jj = j0 + jl;
+                const int b = k.group_band0[gq] + r / CL;
+                if (jj < nlay && b < nband && k.band_lims[2 * b] < 32 * gq + 32) {
+                    const int qb = PAIR ? (gq & 1) : 0;
                     const int l = top_at_1 ? jj : nlay - 1 - jj;
-                    build_sw_record(k, recs[r], s, sm_cg + jl, kLPC, b, cld, icol + size_t(l) * ncol);
-                } else {
-                    DRec& DR = drecs[r];
+                    const LayerState s = st[jl];
+                    build_sw_record(k, recs0[qb * kLPC * mgb + r], s, sm_cg + jl, kLPC, b, cld, icol + size_t(l) * ncol);
+                    DRec& DR = drecs0[qb * kLPC * mgb + r];
                     build_drec<false>(k, DR, s, sm_cg + jl, kLPC, b, idx_o3, cd_internal);
                     const float cd = sm_cg[jl];
                     const float vh = sm_cg[k.idx_h2o * kLPC + jl] / cd;
@@ -1143,14 +1150,17 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     for (size_t i = 0; i < k->gas_names.size(); ++i)
         if (k->gas_names[i] == "o3") idx_o3 = int(i) + 1;
     constexpr int CL = kSwAdjointChunk;
-    const size_t smem = sw_adj_layout(v.ngas, v.nband, v.max_group_bands, CS, kLPC / CL).total;
+    // two record buffers (records of two groups built at once) when they fit
+    const size_t smem2 = sw_adj_layout(v.ngas, v.nband, v.max_group_bands, CS, kLPC / CL, 2).total;
+    const bool pair = smem2 <= 227 * 1024;
+    const size_t smem = pair ? smem2 : sw_adj_layout(v.ngas, v.nband, v.max_group_bands, CS, kLPC / CL, 1).total;
     if (smem > 227 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_sw: shared memory need exceeds 227 KB");
     static bool attr = false;
     if (!attr) {
-        RB_CUDA(cudaFuncSetAttribute(sw_adjoint_kernel<CL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     227 * 1024), "adjoint_sw attribute");
-        RB_CUDA(cudaFuncSetAttribute(sw_adjoint_kernel<CL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     227 * 1024), "adjoint_sw attribute");
+        for (auto fn : {sw_adjoint_kernel<CL, false, false>, sw_adjoint_kernel<CL, true, false>,
+                        sw_adjoint_kernel<CL, false, true>, sw_adjoint_kernel<CL, true, true>})
+            RB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
+                    "adjoint_sw attribute");
         attr = true;
     }
     SwCloudArgs ca{};
@@ -1175,7 +1185,9 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    RB_CUDA(cudaLaunchKernelEx(&cfg, with_flux ? sw_adjoint_kernel<CL, true> : sw_adjoint_kernel<CL, false>, v, gs, ca, ncol, nlay, CS, idx_o3, col_dry ? 0 : 1, play, plev,
+    const auto kernel = with_flux ? (pair ? sw_adjoint_kernel<CL, true, true> : sw_adjoint_kernel<CL, true, false>)
+                                  : (pair ? sw_adjoint_kernel<CL, false, true> : sw_adjoint_kernel<CL, false, false>);
+    RB_CUDA(cudaLaunchKernelEx(&cfg, kernel, v, gs, ca, ncol, nlay, CS, idx_o3, col_dry ? 0 : 1, play, plev,
                                tlay, col_dry, mu0, tsi_scaling, sfc_alb_dir, sfc_alb_dif, seed_up, seed_dn, seed_dir,
                                seed_hr, out),
             "sw_adjoint_kernel launch");

@@ -1,5 +1,6 @@
 // Cloud optics LUT, delta scaling and add_to (optical-property arithmetic).
 #include <cfloat>
+#include <cstdint>
 
 #include "common.cuh"
 #include "optics_device.cuh"
@@ -48,33 +49,67 @@ __global__ void delta_scale_kernel(size_t n, T* __restrict__ tau, T* __restrict_
 
 // increment_1scalar_by_1scalar / inc_1scalar_by_1scalar_bybnd (optical_props_kernels.cu:30-98);
 // bybnd uses gpt2band instead of scanning all bands per element.
+// add_to kernels: grid (column-layer blocks, g-point), so no thread divides its flat index;
+// 16 bytes per array and thread (4 FP32 / 2 FP64 values) when ncl and the pointers allow.
 template <typename T>
-__global__ void add_1scl_kernel(size_t ncl, int ngpt, T* __restrict__ tau1, const T* __restrict__ tau2,
+struct alignas(16) Vec16 {
+    T v[16 / sizeof(T)];
+};
+
+// increment_1scalar_by_1scalar / inc_1scalar_by_1scalar_bybnd (optical_props_kernels.cu:30-43).
+template <typename T, bool VEC>
+__global__ void add_1scl_kernel(size_t ncl, T* __restrict__ tau1, const T* __restrict__ tau2,
                                 const int* __restrict__ gpt2band)
 {
-    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= ncl * ngpt) return;
-    const size_t cl = i % ncl;
-    const int gpt = int(i / ncl);
-    const int src = gpt2band ? gpt2band[gpt] : gpt;
-    tau1[i] = tau1[i] + tau2[cl + size_t(src) * ncl];
+    constexpr int V = VEC ? 16 / sizeof(T) : 1;
+    const int gpt = blockIdx.y;
+    const size_t src = size_t(gpt2band ? gpt2band[gpt] : gpt);
+    const size_t i = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) * V;
+    if (i >= ncl) return;
+    T* const t1 = tau1 + size_t(gpt) * ncl + i;
+    const T* const t2 = tau2 + src * ncl + i;
+    if constexpr (VEC) {
+        Vec16<T> a = *reinterpret_cast<const Vec16<T>*>(t1);
+        const Vec16<T> b = *reinterpret_cast<const Vec16<T>*>(t2);
+#pragma unroll
+        for (int q = 0; q < V; ++q) a.v[q] = a.v[q] + b.v[q];
+        *reinterpret_cast<Vec16<T>*>(t1) = a;
+    } else {
+        t1[0] = t1[0] + t2[0];
+    }
 }
 
 // increment_2stream_by_2stream / inc_2stream_by_2stream_bybnd (:44-136).
-template <typename T>
-__global__ void add_2str_kernel(size_t ncl, int ngpt, T* __restrict__ tau1, T* __restrict__ ssa1,
-                                T* __restrict__ g1, const T* __restrict__ tau2, const T* __restrict__ ssa2,
-                                const T* __restrict__ g2, const int* __restrict__ gpt2band)
+template <typename T, bool VEC>
+__global__ void add_2str_kernel(size_t ncl, T* __restrict__ tau1, T* __restrict__ ssa1, T* __restrict__ g1,
+                                const T* __restrict__ tau2, const T* __restrict__ ssa2, const T* __restrict__ g2,
+                                const int* __restrict__ gpt2band)
 {
-    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= ncl * ngpt) return;
-    const size_t cl = i % ncl;
-    const int gpt = int(i / ncl);
-    const size_t j = cl + size_t(gpt2band ? gpt2band[gpt] : gpt) * ncl;
-    T t = tau1[i], s = ssa1[i], a = g1[i];
-    add_2str_point(t, s, a, tau2[j], ssa2[j], g2[j]);
-    tau1[i] = t; ssa1[i] = s; g1[i] = a;
+    constexpr int V = VEC ? 16 / sizeof(T) : 1;
+    const int gpt = blockIdx.y;
+    const size_t src = size_t(gpt2band ? gpt2band[gpt] : gpt);
+    const size_t i = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) * V;
+    if (i >= ncl) return;
+    const size_t o1 = size_t(gpt) * ncl + i, o2 = src * ncl + i;
+    if constexpr (VEC) {
+        using W = Vec16<T>;
+        W t = *reinterpret_cast<const W*>(tau1 + o1), s = *reinterpret_cast<const W*>(ssa1 + o1),
+          a = *reinterpret_cast<const W*>(g1 + o1);
+        const W t2 = *reinterpret_cast<const W*>(tau2 + o2), s2 = *reinterpret_cast<const W*>(ssa2 + o2),
+                a2 = *reinterpret_cast<const W*>(g2 + o2);
+#pragma unroll
+        for (int q = 0; q < V; ++q) add_2str_point(t.v[q], s.v[q], a.v[q], t2.v[q], s2.v[q], a2.v[q]);
+        *reinterpret_cast<W*>(tau1 + o1) = t;
+        *reinterpret_cast<W*>(ssa1 + o1) = s;
+        *reinterpret_cast<W*>(g1 + o1) = a;
+    } else {
+        T t = tau1[o1], s = ssa1[o1], a = g1[o1];
+        add_2str_point(t, s, a, tau2[o2], ssa2[o2], g2[o2]);
+        tau1[o1] = t; ssa1[o1] = s; g1[o1] = a;
+    }
 }
+
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
 template <typename T>
 int cloud_optics(rrtmgp_b200_cloud c, int ncol, int nlay, const T* clwp, const T* ciwp, const T* reliq,
@@ -111,6 +146,7 @@ int delta_scale(int ncol, int nlay, int ngpt, T* tau, T* ssa, T* g, void* stream
 inline int resolve_add(rrtmgp_b200_bands b, int ngpt_in, const int** g2b)
 {
     RB_CHECK_ARG(b, "add_to: null bands");
+    RB_CHECK_ARG(b->ngpt <= 65535, "add_to: more than 65535 g-points");
     if (ngpt_in == b->ngpt) { *g2b = nullptr; return RRTMGP_B200_OK; }
     if (ngpt_in == b->nband) { *g2b = b->d_gpt2band; return RRTMGP_B200_OK; }
     return fail(RRTMGP_B200_ERR_ARG, "Cannot add optical properties with incompatible band - gpoint combination");
@@ -124,7 +160,13 @@ int add_to_1scl(rrtmgp_b200_bands b, int ncol, int nlay, T* tau1, const T* tau2,
     if (st) return st;
     RB_CHECK_ARG(ncol > 0 && nlay > 0 && tau1 && tau2, "add_to_1scl: bad argument");
     const size_t ncl = size_t(ncol) * nlay;
-    add_1scl_kernel<T><<<ceil_div(long(ncl * b->ngpt), 256), 256, 0, as_stream(stream)>>>(ncl, b->ngpt, tau1, tau2, g2b);
+    constexpr size_t V = 16 / sizeof(T);
+    if (ncl % V == 0 && aligned16(tau1) && aligned16(tau2))
+        add_1scl_kernel<T, true><<<dim3(unsigned(ceil_div(long(ncl / V), 256)), b->ngpt), 256, 0, as_stream(stream)>>>(
+            ncl, tau1, tau2, g2b);
+    else
+        add_1scl_kernel<T, false><<<dim3(unsigned(ceil_div(long(ncl), 256)), b->ngpt), 256, 0, as_stream(stream)>>>(
+            ncl, tau1, tau2, g2b);
     RB_LAUNCH("add_1scl_kernel");
     return RRTMGP_B200_OK;
 }
@@ -138,8 +180,14 @@ int add_to_2str(rrtmgp_b200_bands b, int ncol, int nlay, T* tau1, T* ssa1, T* g1
     if (st) return st;
     RB_CHECK_ARG(ncol > 0 && nlay > 0 && tau1 && ssa1 && g1 && tau2 && ssa2 && g2, "add_to_2str: bad argument");
     const size_t ncl = size_t(ncol) * nlay;
-    add_2str_kernel<T><<<ceil_div(long(ncl * b->ngpt), 256), 256, 0, as_stream(stream)>>>(
-        ncl, b->ngpt, tau1, ssa1, g1, tau2, ssa2, g2, g2b);
+    constexpr size_t V = 16 / sizeof(T);
+    if (ncl % V == 0 && aligned16(tau1) && aligned16(ssa1) && aligned16(g1) && aligned16(tau2) && aligned16(ssa2) &&
+        aligned16(g2))
+        add_2str_kernel<T, true><<<dim3(unsigned(ceil_div(long(ncl / V), 256)), b->ngpt), 256, 0, as_stream(stream)>>>(
+            ncl, tau1, ssa1, g1, tau2, ssa2, g2, g2b);
+    else
+        add_2str_kernel<T, false><<<dim3(unsigned(ceil_div(long(ncl), 256)), b->ngpt), 256, 0, as_stream(stream)>>>(
+            ncl, tau1, ssa1, g1, tau2, ssa2, g2, g2b);
     RB_LAUNCH("add_2str_kernel");
     return RRTMGP_B200_OK;
 }

@@ -135,35 +135,54 @@ def test_cloud_optics(api, oracle_mod, tables, gpu, prec, kind):
         cmp(k, N(got[k]), ref[k], prec)
 
 
+def _offset_tensor(x, dt, dev):
+    """x on the device one element past a 16-byte boundary (a view into a larger buffer)."""
+    import torch
+    flat = torch.empty(x.size + 1, dtype=dt, device=dev)
+    t = flat[1:].view(x.shape)
+    t.copy_(torch.as_tensor(x, dtype=dt))
+    return t
+
+
 @pytest.mark.parametrize("prec", ["f32", "f64"])
-def test_delta_scale_and_add_to(api, oracle_mod, tables, gpu, prec):
+@pytest.mark.parametrize("layout", ["ragged", "aligned", "offset"])
+def test_delta_scale_and_add_to(api, oracle_mod, tables, gpu, prec, layout):
+    """add_to takes 16-byte vector loads when ncol*nlay and the pointers allow ("aligned"),
+    one value per thread otherwise (odd ncol*nlay: "ragged"; views off a 16-byte boundary)."""
     dt = dtypes()[prec]
     rng = np.random.default_rng(3)
     kd = api.Gas_optics_rrtmgp(tables["sw"], S.ATM_GASES)
     nb, ng = 14, 224
-    gas = {"tau": rng.uniform(0, 2, (ng, NLAY, NCOL)), "ssa": rng.uniform(0, 1, (ng, NLAY, NCOL)),
-           "g": rng.uniform(0, 0.9, (ng, NLAY, NCOL))}
-    cld = {"tau": rng.uniform(0, 5, (nb, NLAY, NCOL)), "ssa": rng.uniform(0.5, 1, (nb, NLAY, NCOL)),
-           "g": rng.uniform(0.7, 0.9, (nb, NLAY, NCOL))}
+    nlay, ncol = (NLAY, NCOL) if layout == "ragged" else (24, 32)
+    T_ = _offset_tensor if layout == "offset" else T
+    gas = {"tau": rng.uniform(0, 2, (ng, nlay, ncol)), "ssa": rng.uniform(0, 1, (ng, nlay, ncol)),
+           "g": rng.uniform(0, 0.9, (ng, nlay, ncol))}
+    cld = {"tau": rng.uniform(0, 5, (nb, nlay, ncol)), "ssa": rng.uniform(0.5, 1, (nb, nlay, ncol)),
+           "g": rng.uniform(0.7, 0.9, (nb, nlay, ncol))}
     cld["tau"][:, ::3] = 0.0
     ref_c = {k: v.copy() for k, v in cld.items()}
     oracle_mod.delta_scale(ref_c["tau"], ref_c["ssa"], ref_c["g"])
-    got_c = {k: T(v, dt, gpu) for k, v in cld.items()}
+    got_c = {k: T_(v, dt, gpu) for k, v in cld.items()}
     api.delta_scale(got_c["tau"], got_c["ssa"], got_c["g"])
     for k in cld:
         cmp("delta_" + k, N(got_c[k]), ref_c[k], prec)
     ref_g = {k: v.copy() for k, v in gas.items()}
     oracle_mod.add_to(tables["sw"]["bnd_limits_gpt"], ref_g, ref_c)
-    got_g = {k: T(v, dt, gpu) for k, v in gas.items()}
+    got_g = {k: T_(v, dt, gpu) for k, v in gas.items()}
     api.add_to(kd.bands, got_g, got_c)
     for k in gas:
         cmp("add_" + k, N(got_g[k]), ref_g[k], prec)
-    # g-point by g-point, 1scl
+    # g-point by g-point, 1scl; and by band, 1scl
     ref1 = {"tau": gas["tau"].copy()}
     oracle_mod.add_to(None, ref1, {"tau": gas["tau"]})
-    got1 = {"tau": T(gas["tau"], dt, gpu)}
-    api.add_to(kd.bands, got1, {"tau": T(gas["tau"], dt, gpu)})
+    got1 = {"tau": T_(gas["tau"], dt, gpu)}
+    api.add_to(kd.bands, got1, {"tau": T_(gas["tau"], dt, gpu)})
     cmp("add_1scl", N(got1["tau"]), ref1["tau"], prec)
+    ref2 = {"tau": gas["tau"].copy()}
+    oracle_mod.add_to(tables["sw"]["bnd_limits_gpt"], ref2, {"tau": cld["tau"]})
+    got2 = {"tau": T_(gas["tau"], dt, gpu)}
+    api.add_to(kd.bands, got2, {"tau": T_(cld["tau"], dt, gpu)})
+    cmp("add_1scl_bybnd", N(got2["tau"]), ref2["tau"], prec)
 
 
 def test_add_to_rejects_incompatible_shapes(api, tables, gpu):

@@ -262,10 +262,24 @@ __global__ void __launch_bounds__(MAXT) lw_solver_chunked(int ncol, int nlay, in
     }
 }
 
-// Rdir and Tdir of the FP64 island of the FP32 two-stream (sw_layer_fast), out of line.
-__device__ __noinline__ float2 island_dir(float tau, float w0, float g, float mu0)
+// Two-stream layer coefficients of the chunked shortwave solver: FP32 uses the fused kernels'
+// rearranged FP32 expressions (sw_layer_fast; 1 - ssa is exact in FP32 for ssa >= 1/2), FP64
+// the reference expressions.
+template <typename T>
+__device__ __forceinline__ void sw_layer_coeffs(T tau, T ssa, T g, T mu0, T mu0_inv, T& R, T& Tt, T& Rdir, T& Tdir,
+                                                T& Tn);
+template <>
+__device__ __forceinline__ void sw_layer_coeffs<float>(float tau, float ssa, float g, float mu0, float mu0_inv,
+                                                       float& R, float& Tt, float& Rdir, float& Tdir, float& Tn)
 {
-    return fused::sw_island_dir_inl(tau, w0, g, mu0);
+    float adif, adir;
+    fused::sw_layer_fast(tau, ssa, 1.f - ssa, g, mu0, mu0_inv, R, Tt, Rdir, Tdir, Tn, adif, adir);
+}
+template <>
+__device__ __forceinline__ void sw_layer_coeffs<double>(double tau, double ssa, double g, double mu0, double,
+                                                        double& R, double& Tt, double& Rdir, double& Tdir, double& Tn)
+{
+    sw_two_stream<double>(tau, ssa, g, mu0, R, Tt, Rdir, Tdir, Tn);
 }
 
 template <typename T>
@@ -283,7 +297,6 @@ __global__ void __launch_bounds__(MAXT, MINB) sw_solver_chunked(int ncol, int nl
                                                          T* __restrict__ flux_dn, T* __restrict__ flux_dir)
 {
     __shared__ T sm_p[16 * 32];                                      // direct-beam product per chunk
-    __shared__ float4 sm_isl[sizeof(T) == 4 ? 16 * 32 : 1];          // FP64 island tasks (FP32)
     __shared__ T sm_ru[16 * 32], sm_rd[16 * 32], sm_t[16 * 32], sm_u[16 * 32], sm_d[16 * 32];   // composites
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int icol = blockIdx.x * 32 + lane;
@@ -320,72 +333,15 @@ __global__ void __launch_bounds__(MAXT, MINB) sw_solver_chunked(int ncol, int nl
         cD = nD;
         P *= Tn;
     };
-    if constexpr (sizeof(T) == 4) {
-        // FP32 two-stream (sw_layer_fast) with its FP64 island run once per warp: the (layer,
-        // column) pairs near k mu0 = 1 are sparse and scattered over the lanes, so the first
-        // 32 of the chunk are computed together, one per lane; any beyond run in place.
-        float vTau[CL], vW0[CL], vG[CL];
-        float4* const isl_buf = sm_isl + w * 32;
-        unsigned isl = 0;
-        int ntask = 0;
 #pragma unroll
-        for (int i = 0; i < CL; ++i) {
-            const int j = j0 + i;
-            const bool valid = cv && j < nlay;
-            vTau[i] = 0.f; vW0[i] = 0.f; vG[i] = 0.f;
-            if (valid) {
-                const size_t x = base + size_t(top_at_1 ? j : nlay - 1 - j) * ncol;
-                vTau[i] = tau[x];
-                vW0[i] = ssa[x];
-                vG[i] = gasy[x];
-            }
-            const bool f = valid && fused::sw_island(vW0[i], 1.f - vW0[i], vG[i], m0);
-            const unsigned m = __ballot_sync(0xffffffffu, f);
-            const int idx = ntask + __popc(m & ((1u << lane) - 1u));
-            if (f) {
-                isl |= 1u << i;
-                if (idx < 32) isl_buf[idx] = make_float4(vTau[i], vW0[i], vG[i], m0);
-            }
-            ntask += __popc(m);
+    for (int i = 0; i < CL; ++i) {
+        const int j = j0 + i;
+        T R = T(0), Tt = T(1), Rdir = T(0), Tdir = T(0), Tn = T(1);
+        if (cv && j < nlay) {
+            const size_t x = base + size_t(top_at_1 ? j : nlay - 1 - j) * ncol;
+            sw_layer_coeffs<T>(tau[x], ssa[x], gasy[x], m0, m0_inv, R, Tt, Rdir, Tdir, Tn);
         }
-        __syncwarp();
-        if (lane < ntask) {
-            const float4 q = isl_buf[lane];
-            const float2 d = island_dir(q.x, q.y, q.z, q.w);
-            isl_buf[lane] = make_float4(d.x, d.y, 0.f, 0.f);
-        }
-        __syncwarp();
-        int first = 0;
-#pragma unroll
-        for (int i = 0; i < CL; ++i) {
-            const bool f = (isl >> i) & 1u;
-            const unsigned m = __ballot_sync(0xffffffffu, f);
-            const int idx = first + __popc(m & ((1u << lane) - 1u));
-            first += __popc(m);
-            fused::SwLayerPre pre;
-            fused::sw_layer_fast_pre(vTau[i], vW0[i], 1.f - vW0[i], vG[i], m0, m0_inv, f, pre);
-            float Rd = pre.Rdir0, Td = pre.Tdir0;
-            if (f) {
-                const float2 d = idx < 32 ? make_float2(isl_buf[idx].x, isl_buf[idx].y)
-                                          : island_dir(vTau[i], vW0[i], vG[i], m0);
-                Rd = d.x;
-                Td = d.y;
-            }
-            float Rdir, Tdir, adir;
-            fused::sw_layer_clamp(pre, Rd, Td, Rdir, Tdir, adir);
-            add_layer(i, pre.R, pre.T, Rdir, Tdir, pre.Tn);
-        }
-    } else {
-#pragma unroll
-        for (int i = 0; i < CL; ++i) {
-            const int j = j0 + i;
-            T R = T(0), Tt = T(1), Rdir = T(0), Tdir = T(0), Tn = T(1);
-            if (cv && j < nlay) {
-                const size_t x = base + size_t(top_at_1 ? j : nlay - 1 - j) * ncol;
-                sw_two_stream<T>(tau[x], ssa[x], gasy[x], m0, R, Tt, Rdir, Tdir, Tn);
-            }
-            add_layer(i, R, Tt, Rdir, Tdir, Tn);
-        }
+        add_layer(i, R, Tt, Rdir, Tdir, Tn);
     }
     sm_p[w * 32 + lane] = P;
     __syncthreads();

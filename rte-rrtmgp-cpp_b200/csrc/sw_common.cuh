@@ -41,28 +41,23 @@ __device__ __forceinline__ void one_minus_exp(float x, float& E, float& e)
 //   Rdir bracket = E2 (alpha2 - k^2 mu0 gamma3) + k (gamma3 - mu0 alpha2) (E1^2 + 2 e1 En),
 //   Tdir bracket = Tn E2 (alpha1 + k^2 mu0 gamma4) + k (gamma4 + mu0 alpha1) (E1^2 - (1 + e2) En),
 // the Tdir bracket taking the reference form when both exponentials are small (thick layers).
-// Near the removable singularity k mu0 = 1 (|1 - (k mu0)^2| < 0.02) Rdir and Tdir come from
-// the reference expressions in FP64 (FP64 island).  omw = 1 - w0 is passed separately, formed
-// from absorption optical depths, so it keeps its accuracy for w0 -> 1.  Clamps and k_min are
-// those of the FP64 reference (DBL_EPSILON, 1e-12).  Divisions and the square root use the
-// approximate intrinsics (a few ulp; the operands are normal numbers).
-struct SwLayerPre {
-    float R, T, adif, Tn, En, Rdir0, Tdir0;   // Rdir0, Tdir0: before the clamps (FP32 values)
-};
-
-// The island test of sw_layer_fast (independent of tau): |1 - (k mu0)^2| < 0.02.
-__device__ __forceinline__ bool sw_island(float w0, float omw, float g, float mu0)
-{
-    const float kk = 2.f * omw * (2.f - .5f * w0 * (1.f + 3.f * g));
-    const float kkc = fmaxf(kk, 1.e-12f);
-    const float km = kkc * rsqrtf(kkc) * mu0;
-    return fabsf((1.f - km) * (1.f + km)) < 0.02f;
-}
-
-// FP32 part of sw_layer_fast.  island: the layer takes the FP64 island (sw_island), where
-// Rdir0 and Tdir0 are meaningless and sw_island_dir_inl supplies them.
-__device__ __forceinline__ void sw_layer_fast_pre(float tau, float w0, float omw, float g, float mu0, float mu0_inv,
-                                                  bool island, SwLayerPre& p)
+// omw = 1 - w0 is passed separately, formed from absorption optical depths, so it keeps its
+// accuracy for w0 -> 1.  Clamps and k_min are those of the FP64 reference (DBL_EPSILON,
+// 1e-12).  Divisions and the square root use the approximate intrinsics (a few ulp; the
+// operands are normal numbers).
+//
+// Near the removable singularity k mu0 = 1 (|1 - (k mu0)^2| < 0.02) both brackets vanish with
+// 1 - (k mu0)^2.  With d = 1 - k mu0 and x = tau d / mu0 they factor exactly as
+//   Rdir bracket = d [ (alpha2 + k gamma3) Z - 2 X e1^2 (tau/mu0) phi(x) ],
+//   Tdir bracket = -d [ 2 U e1 (tau/mu0) phi(x) + (alpha1 - k gamma4) W ],
+// Z = E1^2 + 2 e1 En, X = alpha2 - k^2 mu0 gamma3, U = alpha1 + k^2 mu0 gamma4,
+// W = E1^2 - (1 + e2) En = Tn (1 + e2) - 2 e1, phi(x) = (1 - exp(-x)) / x (so that
+// e1 phi(x) = (e1 - Tn) / x, a series below |x| = 1/2), and the factor d cancels against
+// 1 - (k mu0)^2 = d (1 + k mu0): no FP64.  An FP32 emulation over 10^6 (tau, w0, g, mu0) with
+// k mu0 within 1.5% of 1 keeps Rdir and Tdir within 1.6e-4 of (1 - Tn) of the FP64 reference.
+__device__ __forceinline__ void sw_layer_fast(float tau, float w0, float omw, float g, float mu0, float mu0_inv,
+                                              float& R, float& T, float& Rdir, float& Tdir, float& Tn,
+                                              float& adif, float& adir)
 {
     const float g1 = (8.f - w0 * (5.f + 3.f * g)) * .25f;
     const float g2 = 3.f * (w0 * (1.f - g)) * .25f;
@@ -73,66 +68,52 @@ __device__ __forceinline__ void sw_layer_fast_pre(float tau, float w0, float omw
     const float kk = 2.f * omw * (2.f - .5f * w0 * (1.f + 3.f * g));
     const float kkc = fmaxf(kk, 1.e-12f);
     const float k = kkc * rsqrtf(kkc);
-    float E1, e1, En, Tn;
+    float E1, e1, En;
     one_minus_exp(k * tau, E1, e1);
     one_minus_exp(tau * mu0_inv, En, Tn);
     const float E2 = E1 * (2.f - E1);
     const float e2 = e1 * e1;
     const float rt = __fdividef(1.f, k * (1.f + e2) + g1 * E2);
-    p.R = rt * g2 * E2;
-    p.T = rt * 2.f * k * e1;
-    p.adif = rt * (k * E1 * E1 + 2.f * omw * E2);
-    p.Tn = Tn;
-    p.En = En;
+    R = rt * g2 * E2;
+    T = rt * 2.f * k * e1;
+    adif = rt * (k * E1 * E1 + 2.f * omw * E2);
     const float km = k * mu0;
     const float fact = (1.f - km) * (1.f + km);
-    const float rt2 = __fdividef(w0 * rt, island ? 1.f : fact);
-    const float br = E2 * (a2 - k * km * g3) + k * (g3 - mu0 * a2) * (E1 * E1 + 2.f * e1 * En);
-    const float bt_thick =
-        (1.f + km) * (a1 + k * g4) * Tn - (1.f - km) * (a1 - k * g4) * e2 * Tn - 2.f * (k * g4 + a1 * km) * e1;
-    const float bt_thin = Tn * E2 * (a1 + k * km * g4) + k * (g4 + mu0 * a1) * (E1 * E1 - (1.f + e2) * En);
-    const float bt = (e1 < .5f && Tn < .5f) ? bt_thick : bt_thin;
-    p.Rdir0 = rt2 * br;
-    p.Tdir0 = -rt2 * bt;
-}
-
-// Rdir and Tdir of the FP64 island: the reference expressions in double.
-__device__ __forceinline__ float2 sw_island_dir_inl(float tau, float w0, float g, float mu0)
-{
-    double Rd, Td, Rr, Tr, Tn64;
-    sw_two_stream<double>(double(tau), double(w0), double(g), double(mu0), Rd, Td, Rr, Tr, Tn64);
-    return make_float2(float(Rr), float(Tr));
-}
-
-// The clamps of the reference (rte_solver_kernels.cu:582-583) and the direct absorptance.
-__device__ __forceinline__ void sw_layer_clamp(const SwLayerPre& p, float Rdir0, float Tdir0, float& Rdir, float& Tdir,
-                                               float& adir)
-{
+    const bool thick = e1 < .5f && Tn < .5f;
+    float Rdir0, Tdir0;
+    if (fabsf(fact) < 0.02f) {
+        const float tm = tau * mu0_inv;
+        const float x = tm * (1.f - km);
+        const float ser = 1.f - x * (.5f - x * (1.f / 6.f - x * (1.f / 24.f - x * (1.f / 120.f))));
+        const float e1phi = fabsf(x) < .5f ? e1 * ser : __fdividef(e1 - Tn, x);
+        const float c = __fdividef(w0 * rt, 1.f + km);
+        const float W = thick ? Tn * (1.f + e2) - 2.f * e1 : E1 * E1 - (1.f + e2) * En;
+        Rdir0 = c * ((a2 + k * g3) * (E1 * E1 + 2.f * e1 * En) - 2.f * (a2 - k * km * g3) * e1 * e1phi * tm);
+        Tdir0 = c * (2.f * (a1 + k * km * g4) * e1phi * tm + (a1 - k * g4) * W);
+    } else {
+        const float rt2 = __fdividef(w0 * rt, fact);
+        const float br = E2 * (a2 - k * km * g3) + k * (g3 - mu0 * a2) * (E1 * E1 + 2.f * e1 * En);
+        const float bt_thick =
+            (1.f + km) * (a1 + k * g4) * Tn - (1.f - km) * (a1 - k * g4) * e2 * Tn - 2.f * (k * g4 + a1 * km) * e1;
+        const float bt_thin = Tn * E2 * (a1 + k * km * g4) + k * (g4 + mu0 * a1) * (E1 * E1 - (1.f + e2) * En);
+        Rdir0 = rt2 * br;
+        Tdir0 = -rt2 * (thick ? bt_thick : bt_thin);
+    }
     const float tmin = 2.220446049250313e-16f;
-    Rdir = fmaxf(tmin, fminf(Rdir0, p.En));
-    const float rest = p.En - Rdir;
+    Rdir = fmaxf(tmin, fminf(Rdir0, En));
+    const float rest = En - Rdir;
     Tdir = fmaxf(tmin, fminf(Tdir0, rest));
     adir = fmaxf(0.f, rest - Tdir);
 }
 
-__device__ __forceinline__ void sw_layer_fast(float tau, float w0, float omw, float g, float mu0, float mu0_inv,
-                                              float& R, float& T, float& Rdir, float& Tdir, float& Tn,
-                                              float& adif, float& adir)
+// The island test of sw_layer_fast (independent of tau): |1 - (k mu0)^2| < 0.02.  The adjoint
+// takes its FP64 derivatives there.
+__device__ __forceinline__ bool sw_island(float w0, float omw, float g, float mu0)
 {
-    SwLayerPre p;
-    const bool island = sw_island(w0, omw, g, mu0);
-    sw_layer_fast_pre(tau, w0, omw, g, mu0, mu0_inv, island, p);
-    float Rd = p.Rdir0, Td = p.Tdir0;
-    if (island) {
-        const float2 d = sw_island_dir_inl(tau, w0, g, mu0);
-        Rd = d.x;
-        Td = d.y;
-    }
-    R = p.R;
-    T = p.T;
-    Tn = p.Tn;
-    adif = p.adif;
-    sw_layer_clamp(p, Rd, Td, Rdir, Tdir, adir);
+    const float kk = 2.f * omw * (2.f - .5f * w0 * (1.f + 3.f * g));
+    const float kkc = fmaxf(kk, 1.e-12f);
+    const float km = kkc * rsqrtf(kkc) * mu0;
+    return fabsf((1.f - km) * (1.f + km)) < 0.02f;
 }
 
 __device__ __forceinline__ void build_sw_record(const KdistView<float>& k, Rec& R, const LayerState& s,

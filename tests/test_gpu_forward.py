@@ -99,7 +99,9 @@ def test_fused_sw_matches_oracle(oracle_mod, tables, gpu, nlay, clouds, top_at_1
 
 def test_fused_sw_low_sun_and_resonance(oracle_mod, tables, gpu):
     """mu0 over [0.02, 1] including values where k mu0 = 1 for purely absorbing g-points
-    (k = 2 at w0 = 0, i.e. mu0 = 0.5): exercises the FP64 island and the thick-layer branch."""
+    (k = 2 at w0 = 0, i.e. mu0 = 0.5): exercises the factored k mu0 = 1 expressions of the FP32
+    two-stream and its thick-layer branch, in the fused kernel and in the per-stage FP32 solver
+    (fluxes; its heating rates come from FP32 level-flux differences)."""
     import torch
     from rrtmgp_b200.solver import atm_to_device
     base, fused = _solvers(tables)
@@ -110,6 +112,11 @@ def test_fused_sw_low_sun_and_resonance(oracle_mod, tables, gpu):
     got = fused.solve_sw(atm_to_device(atm, torch.float32, gpu))
     torch.cuda.synchronize()
     _check_sw(got, ref, "sw low sun / resonance")
+    staged = base.solve_sw(atm_to_device(atm, torch.float32, gpu))
+    torch.cuda.synchronize()
+    for k in ("flux_up", "flux_dn", "flux_dn_dir", "flux_net"):
+        e = np.max(np.abs(staged[k].double().cpu().numpy() - ref[k]))
+        assert e < 5e-3, f"staged sw low sun / resonance {k}: {e:.3e} W/m2"
 
 
 def test_fused_sw_matches_staged_fp32(tables, gpu):

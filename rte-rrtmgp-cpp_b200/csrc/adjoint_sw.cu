@@ -23,7 +23,7 @@
 // affine in its adjoint (the albedo/source pair is 2x2 upper triangular), so chunks compose
 // exactly like the forward.  Per layer the adjoints of (R, T, Rdir, Tdir, Tn, adif, adir)
 // go through the two-stream (reverse mode of the forward's FP32 formulas with its branch
-// selections; FP64 forward-mode derivatives of the reference expressions in the k mu0 = 1 island), the
+// selections, the k mu0 = 1 form of sw_common.cuh included), the
 // gas/Rayleigh/cloud combination, and the gas-optics interpolation (adjoint_common.cuh).
 #include <cooperative_groups.h>
 
@@ -70,90 +70,20 @@ __device__ __forceinline__ int minor_code(const int4& mg, int n)
     return n == 0 ? mg.y : (n == 1 ? mg.z : mg.w);
 }
 
-// FP64 value with its derivatives with respect to (tau, w0, g): forward-mode arithmetic for
-// the island below.
-struct DD3 {
-    double v, t, w, g;
-};
-__device__ __forceinline__ DD3 dd(double v) { return DD3{v, 0.0, 0.0, 0.0}; }
-__device__ __forceinline__ DD3 operator+(const DD3& a, const DD3& b) { return DD3{a.v + b.v, a.t + b.t, a.w + b.w, a.g + b.g}; }
-__device__ __forceinline__ DD3 operator-(const DD3& a, const DD3& b) { return DD3{a.v - b.v, a.t - b.t, a.w - b.w, a.g - b.g}; }
-__device__ __forceinline__ DD3 operator*(const DD3& a, const DD3& b)
-{
-    return DD3{a.v * b.v, a.t * b.v + a.v * b.t, a.w * b.v + a.v * b.w, a.g * b.v + a.v * b.g};
-}
-__device__ __forceinline__ DD3 operator*(double s, const DD3& a) { return DD3{s * a.v, s * a.t, s * a.w, s * a.g}; }
-__device__ __forceinline__ DD3 operator+(double s, const DD3& a) { return DD3{s + a.v, a.t, a.w, a.g}; }
-__device__ __forceinline__ DD3 operator-(double s, const DD3& a) { return DD3{s - a.v, -a.t, -a.w, -a.g}; }
-__device__ __forceinline__ DD3 recip(const DD3& a)
-{
-    const double r = 1.0 / a.v, d = -r * r;
-    return DD3{r, d * a.t, d * a.w, d * a.g};
-}
-__device__ __forceinline__ DD3 exp_neg(const DD3& a)   // exp(-a)
-{
-    const double e = exp(-a.v);
-    return DD3{e, -e * a.t, -e * a.w, -e * a.g};
-}
-
-// FP64 island of the two-stream (|1 - (k mu0)^2| < 0.02, as the forward): the unclamped Rdir
-// and Tdir of the reference expressions (sw_two_stream, rte_device.cuh) in double, and their
-// derivatives with respect to (tau, w0, g) by forward-mode differentiation of the same
-// expressions.  rd = [Rdir, dRdir/dtau, dRdir/dw0, dRdir/dg], td likewise.  Out of line: one
-// copy of the code.
-__device__ __noinline__ void island_fp64(float tau_f, float w0_f, float g_f, float mu0_f, float* rd, float* td)
-{
-    const double mu0 = double(mu0_f);
-    const DD3 tau{double(tau_f), 1.0, 0.0, 0.0};
-    const DD3 w0{double(w0_f), 0.0, 1.0, 0.0};
-    const DD3 g{double(g_f), 0.0, 0.0, 1.0};
-    const DD3 gamma1 = 0.25 * (8.0 - w0 * (5.0 + 3.0 * g));
-    const DD3 gamma2 = 0.75 * (w0 * (1.0 - g));
-    const DD3 gamma3 = 0.25 * (2.0 - (3.0 * mu0) * g);
-    const DD3 gamma4 = 1.0 - gamma3;
-    const DD3 alpha1 = gamma1 * gamma4 + gamma2 * gamma3;
-    const DD3 alpha2 = gamma1 * gamma3 + gamma2 * gamma4;
-    const DD3 kk = (gamma1 - gamma2) * (gamma1 + gamma2);
-    DD3 k = dd(sqrt(1.e-12));
-    if (kk.v > 1.e-12) {
-        const double kv = sqrt(kk.v), h = 0.5 / kv;
-        k = DD3{kv, h * kk.t, h * kk.w, h * kk.g};
-    }
-    const DD3 e1 = exp_neg(tau * k);
-    const DD3 e2 = e1 * e1;
-    const DD3 rt = recip(k * (1.0 + e2) + gamma1 * (1.0 - e2));
-    const DD3 Tn = exp_neg((1.0 / mu0) * tau);
-    const DD3 k_mu = mu0 * k;
-    const DD3 k_gamma3 = k * gamma3;
-    const DD3 k_gamma4 = k * gamma4;
-    const double tmin = 2.220446049250313e-16;
-    DD3 fact = 1.0 - k_mu * k_mu;
-    if (!(fabs(fact.v) > tmin)) fact = dd(tmin);
-    const DD3 rt2 = w0 * rt * recip(fact);
-    const DD3 Rdir = rt2 * ((1.0 - k_mu) * (alpha2 + k_gamma3) - (1.0 + k_mu) * (alpha2 - k_gamma3) * e2 -
-                            2.0 * ((k_gamma3 - alpha2 * k_mu) * e1 * Tn));
-    const DD3 Tdir = rt2 * (2.0 * ((k_gamma4 + alpha1 * k_mu) * e1) - (1.0 + k_mu) * (alpha1 + k_gamma4) * Tn +
-                            (1.0 - k_mu) * (alpha1 - k_gamma4) * e2 * Tn);
-    rd[0] = float(Rdir.v); rd[1] = float(Rdir.t); rd[2] = float(Rdir.w); rd[3] = float(Rdir.g);
-    td[0] = float(Tdir.v); td[1] = float(Tdir.t); td[2] = float(Tdir.w); td[3] = float(Tdir.g);
-}
-
 // Adjoint of one (layer, g-point) from the adjoints of its two-stream outputs (R, T, Rdir,
 // Tdir, Tn, adif, adir) to the optical inputs of the layer: gas absorption tau (x), Rayleigh
 // tau (y), cloud tau (z), cloud tau*ssa (w) and cloud tau*ssa*g (v).  The combination is
 // tau = ta + tr + tc, w0 = (tr + tsc) / tau, g = tsgc / (tr + tsc).  Reverse mode of
 // sw_layer_fast: the forward is recomputed with the same expressions and branch selections
 // (clamps: the selected argument carries the derivative, as min/max of dual numbers would),
-// then the adjoints run back through it.  island: the (layer, g-point) takes the FP64 island
-// (decided once per group, sw_island); isl: its island_fp64 results [Rdir, dRdir/d(tau, w0,
-// g), Tdir, dTdir/d(...)] when the warp computed them already, else null.
+// then the adjoints run back through it, in the k mu0 = 1 region through its factored form.
 struct LocalAdj {
     float ta, tr, tc, tsc, tsg;
 };
 
 __device__ __forceinline__ LocalAdj sw_local_adjoint(float tau, float w0, float omw, float g, float mu0, float mu0_inv,
                                                      float Rb, float Tb, float Rdb, float Tdb, float Tnb, float Afb,
-                                                     float Arb, bool island, const float* isl)
+                                                     float Arb)
 {
     // ---- forward, as sw_layer_fast (same expressions, same branch selections) ----
     const float g1 = (8.f - w0 * (5.f + 3.f * g)) * .25f;
@@ -176,22 +106,26 @@ __device__ __forceinline__ LocalAdj sw_local_adjoint(float tau, float w0, float 
     const float rt = __fdividef(1.f, den);
     const float km = k * mu0;
     const float fact = (1.f - km) * (1.f + km);
+    const bool island = fabsf(fact) < 0.02f;
     float Rdir0, Tdir0, rt2 = 0.f, br = 0.f, bt = 0.f;
-    bool thick = false;
-    float rd[4], td[4];
+    const bool thick = e1 < .5f && Tn < .5f;
+    // k mu0 = 1 form (sw_layer_fast): d = 1 - k mu0 factored out of both brackets
+    const float tmu = tau * mu0_inv, xi = tmu * (1.f - km);
+    const bool xs = fabsf(xi) < .5f;
+    const float ser = 1.f - xi * (.5f - xi * (1.f / 6.f - xi * (1.f / 24.f - xi * (1.f / 120.f))));
+    float e1phi = 0.f, cI = 0.f, WI = 0.f, BR = 0.f, BT = 0.f;
+    const float XI = a2 - k * km * g3, UI = a1 + k * km * g4, ZI = E1 * E1 + 2.f * e1 * En;
     if (island) {
-        if (isl) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) { rd[q] = isl[q]; td[q] = isl[4 + q]; }
-        } else {
-            island_fp64(tau, w0, g, mu0, rd, td);
-        }
-        Rdir0 = rd[0];
-        Tdir0 = td[0];
+        e1phi = xs ? e1 * ser : __fdividef(e1 - Tn, xi);
+        cI = __fdividef(w0 * rt, 1.f + km);
+        WI = thick ? Tn * (1.f + e2) - 2.f * e1 : E1 * E1 - (1.f + e2) * En;
+        BR = (a2 + k * g3) * ZI - 2.f * XI * e1 * e1phi * tmu;
+        BT = 2.f * UI * e1phi * tmu + (a1 - k * g4) * WI;
+        Rdir0 = cI * BR;
+        Tdir0 = cI * BT;
     } else {
         rt2 = __fdividef(w0 * rt, fact);
         br = E2 * (a2 - k * km * g3) + k * (g3 - mu0 * a2) * (E1 * E1 + 2.f * (e1 * En));
-        thick = e1 < .5f && Tn < .5f;
         if (thick)
             bt = (1.f + km) * (a1 + k * g4) * Tn - (1.f - km) * (a1 - k * g4) * e2 * Tn - 2.f * ((k * g4 + a1 * km) * e1);
         else
@@ -228,9 +162,62 @@ __device__ __forceinline__ LocalAdj sw_local_adjoint(float tau, float w0, float 
     float k_b = 0.f, km_b = 0.f, rt_b = 0.f, E1_b = 0.f, e1_b = 0.f, E2_b = 0.f, e2_b = 0.f;
     float g1_b = 0.f, g2_b = 0.f, g3_b = 0.f, g4_b = 0.f, a1_b = 0.f, a2_b = 0.f;
     if (island) {
-        tau_b += Rdir0_b * rd[1] + Tdir0_b * td[1];
-        w0_b += Rdir0_b * rd[2] + Tdir0_b * td[2];
-        g_b += Rdir0_b * rd[3] + Tdir0_b * td[3];
+        // reverse of Rdir0 = c BR, Tdir0 = c BT (the k mu0 = 1 form above)
+        const float c_b = Rdir0_b * BR + Tdir0_b * BT;
+        const float BR_b = Rdir0_b * cI, BT_b = Tdir0_b * cI;
+        a2_b += BR_b * ZI;
+        k_b += BR_b * g3 * ZI;
+        g3_b += BR_b * k * ZI;
+        const float Z_b = BR_b * (a2 + k * g3);
+        const float P_b = -2.f * BR_b;                 // P = X e1 e1phi tm
+        const float X_b = P_b * e1 * e1phi * tmu;
+        e1_b += P_b * XI * e1phi * tmu;
+        float e1phi_b = P_b * XI * e1 * tmu;
+        float tm_b = P_b * XI * e1 * e1phi;
+        const float Q_b = 2.f * BT_b;                  // Q = U e1phi tm
+        const float U_b = Q_b * e1phi * tmu;
+        e1phi_b += Q_b * UI * tmu;
+        tm_b += Q_b * UI * e1phi;
+        a1_b += BT_b * WI;
+        k_b -= BT_b * g4 * WI;
+        g4_b -= BT_b * k * WI;
+        const float W_b = BT_b * (a1 - k * g4);
+        E1_b += Z_b * 2.f * E1;
+        e1_b += Z_b * 2.f * En;
+        En_b += Z_b * 2.f * e1;
+        a2_b += X_b;
+        k_b -= X_b * km * g3;
+        km_b -= X_b * k * g3;
+        g3_b -= X_b * k * km;
+        a1_b += U_b;
+        k_b += U_b * km * g4;
+        km_b += U_b * k * g4;
+        g4_b += U_b * k * km;
+        if (thick) {
+            Tn_b += W_b * (1.f + e2);
+            e2_b += W_b * Tn;
+            e1_b -= 2.f * W_b;
+        } else {
+            E1_b += W_b * 2.f * E1;
+            e2_b -= W_b * En;
+            En_b -= W_b * (1.f + e2);
+        }
+        w0_b += c_b * rt / (1.f + km);
+        rt_b += c_b * w0 / (1.f + km);
+        km_b -= c_b * cI / (1.f + km);
+        float x_b;
+        if (xs) {
+            const float dser = -.5f + xi * (1.f / 3.f - xi * (1.f / 8.f - xi * (1.f / 30.f)));
+            e1_b += e1phi_b * ser;
+            x_b = e1phi_b * e1 * dser;
+        } else {
+            e1_b += e1phi_b / xi;
+            Tn_b -= e1phi_b / xi;
+            x_b = -e1phi_b * e1phi / xi;
+        }
+        tm_b += x_b * (1.f - km);
+        km_b -= x_b * tmu;
+        tau_b += tm_b * mu0_inv;
     } else {
         const float rt2_b = Rdir0_b * br - Tdir0_b * bt;
         const float br_b = Rdir0_b * rt2;
@@ -355,7 +342,7 @@ __device__ __noinline__ LayerAdj sw_layer_adjoint(const float4* __restrict__ kma
                                                   const float2* __restrict__ krayl2, const Rec* Rc, const DRec* DR,
                                                   int g, int4 mg, int nmax, float tau, float w0, float omw, float gasy,
                                                   float mu0, float mu0_inv, float Rb, float Tb, float Rdb, float Tdb,
-                                                  float Tnb, float Afb, float Arb, bool island, const float* isl)
+                                                  float Tnb, float Afb, float Arb)
 {
     const float4 c0 = __ldg(kmaj4 + (Rc->kb.x + g));
     const float4 c1 = __ldg(kmaj4 + (Rc->kb.y + g));
@@ -373,7 +360,7 @@ __device__ __noinline__ LayerAdj sw_layer_adjoint(const float4* __restrict__ kma
     const float2 r0 = __ldg(krayl2 + (Rc->kr[0] + g));
     const float2 r1 = __ldg(krayl2 + (Rc->kr[1] + g));
 
-    const LocalAdj la = sw_local_adjoint(tau, w0, omw, gasy, mu0, mu0_inv, Rb, Tb, Rdb, Tdb, Tnb, Afb, Arb, island, isl);
+    const LocalAdj la = sw_local_adjoint(tau, w0, omw, gasy, mu0, mu0_inv, Rb, Tb, Rdb, Tdb, Tnb, Afb, Arb);
 
     float dT = dot4(DR->wT0, c0) + dot4(DR->wT1, c1);
     float dH = dot4(DR->wH0, c0) + dot4(DR->wH1, c1);
@@ -495,12 +482,8 @@ __device__ __forceinline__ void cloud_sw_dual(const CloudLut<float>& L, int delt
     tsg = ts * g;
 }
 
-// FP64 island tasks of a warp per group (one per lane): inputs tau, w0, g, (pad), then the
-// island_fp64 results [Rdir, dRdir/d(tau, w0, g), Tdir, dTdir/d(tau, w0, g)].
-constexpr int kIslTask = 12;
-
 struct SwAdjLayout {
-    size_t state, cg, seeds, clsum, albacc, x1, x2, x3, x4, x5, recs, drecs, isl, total;
+    size_t state, cg, seeds, clsum, albacc, x1, x2, x3, x4, x5, recs, drecs, total;
 };
 
 __host__ __device__ __forceinline__ SwAdjLayout sw_adj_layout(int ngas, int nband, int mgb, int CS, int WPC,
@@ -521,8 +504,7 @@ __host__ __device__ __forceinline__ SwAdjLayout sw_adj_layout(int ngas, int nban
     L.x5 = align16(L.x4 + (sizeof(float4) + sizeof(float)) * nw);
     L.recs = align16(L.x5 + sizeof(float2) * nw);
     L.drecs = align16(L.recs + sizeof(Rec) * size_t(kLPC) * mgb * nbuf);
-    L.isl = align16(L.drecs + sizeof(DRec) * size_t(kLPC) * mgb * nbuf);
-    L.total = align16(L.isl + sizeof(float) * kIslTask * 32 * WPC);
+    L.total = align16(L.drecs + sizeof(DRec) * size_t(kLPC) * mgb * nbuf);
     return L;
 }
 
@@ -573,7 +555,6 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
     float2* sm_x5 = reinterpret_cast<float2*>(smem_raw + SL.x5);
     Rec* const recs0 = reinterpret_cast<Rec*>(smem_raw + SL.recs) + w * CL * mgb;
     DRec* const drecs0 = reinterpret_cast<DRec*>(smem_raw + SL.drecs) + w * CL * mgb;
-    float* sm_isl = reinterpret_cast<float*>(smem_raw + SL.isl) + w * 32 * kIslTask;
 
     const bool top_at_1 = play[icol] < play[icol + size_t(nlay - 1) * ncol];
     const float mu0 = mu0_in[icol];
@@ -940,48 +921,12 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
             Db = m.x * Db + m.y;
         }
 
-        // ---- FP64 island tasks of the chunk, compacted over the lanes ----
-        // A (layer, g-point) near k mu0 = 1 needs island_fp64 (an FP64 two-stream with three
-        // tangents).  Such pairs are sparse and scattered over the lanes, so instead of every
-        // layer's call running it for the lanes that need it (the warp waiting each time), the
-        // first 32 tasks of the chunk (layer by layer, lane by lane) are run at once, one per
-        // lane; a task beyond the first 32 is run by its own lane in the layer call.
-        unsigned isl_bits = 0;
-        int ntask = 0;
-#pragma unroll
-        for (int i = 0; i < CL; ++i) {
-            const bool f = (j0 + w * CL + i < nlay) && gv && sw_island(vW0[i], vOmw[i], vG[i], mu0);
-            const unsigned m = __ballot_sync(0xffffffffu, f);
-            const int idx = ntask + __popc(m & ((1u << lane) - 1u));
-            if (f) {
-                isl_bits |= 1u << i;
-                if (idx < 32) {
-                    float* t = sm_isl + idx * kIslTask;
-                    t[0] = vTau[i];
-                    t[1] = vW0[i];
-                    t[2] = vG[i];
-                }
-            }
-            ntask += __popc(m);
-        }
-        __syncwarp();
-        if (lane < ntask) {
-            float* t = sm_isl + lane * kIslTask;
-            island_fp64(t[0], t[1], t[2], mu0, t + 4, t + 8);
-        }
-        __syncwarp();
-
         // ---- R1 resweep + local adjoints per layer ----
         float gT[CL], gH[CL], gO[CL], gC0[CL], gC1[CL], gC2[CL];
-        int rem = ntask;   // island tasks of layers < i
 #pragma unroll
         for (int i = CL - 1; i >= 0; --i) {
             const int jl = w * CL + i;
             const int j = j0 + jl;
-            const bool isl = (isl_bits >> i) & 1u;
-            const unsigned m = __ballot_sync(0xffffffffu, isl);
-            rem -= __popc(m);
-            const int idx = rem + __popc(m & ((1u << lane) - 1u));
             const float dir = vDir[i];
             const float Tnb = Db * dir, Rdb = vSub[i] * dir, Tdb = vSdb[i] * dir, Arb = sm_hh[jl] * dir;
             Db = sm_be[jl] + sm_ga[jl] + sm_hh[jl] * vAr[i] + vSub[i] * vRd[i] + vSdb[i] * vTd[i] + vTn[i] * Db;
@@ -990,8 +935,7 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
                 const Rec& Rc = recs[slot * CL + i];
                 const LayerAdj la = sw_layer_adjoint(k.kmaj4, k.kmin2[Rc.a], k.krayl2, &Rc, &drecs[slot * CL + i], g,
                                                      Rc.a ? mg1 : mg0, Rc.a ? nm1 : nm0, vTau[i], vW0[i], vOmw[i],
-                                                     vG[i], mu0, mu0_inv, vRb[i], vTb[i], Rdb, Tdb, Tnb, vAfb[i], Arb,
-                                                     isl, (isl && idx < 32) ? sm_isl + idx * kIslTask + 4 : nullptr);
+                                                     vG[i], mu0, mu0_inv, vRb[i], vTb[i], Rdb, Tdb, Tnb, vAfb[i], Arb);
                 gT[i] = la.t; gH[i] = la.h; gO[i] = la.o;
                 gC0[i] = la.tc; gC1[i] = la.tsc; gC2[i] = la.tsg;
             }

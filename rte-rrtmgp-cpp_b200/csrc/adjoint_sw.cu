@@ -106,7 +106,7 @@ __device__ __forceinline__ LocalAdj sw_local_adjoint(float tau, float w0, float 
     const float rt = __fdividef(1.f, den);
     const float km = k * mu0;
     const float fact = (1.f - km) * (1.f + km);
-    const bool island = fabsf(fact) < 0.02f;
+    const bool near1 = fabsf(fact) < 0.02f;   // k mu0 = 1 form (sw_layer_fast)
     float Rdir0, Tdir0, rt2 = 0.f, br = 0.f, bt = 0.f;
     const bool thick = e1 < .5f && Tn < .5f;
     // k mu0 = 1 form (sw_layer_fast): d = 1 - k mu0 factored out of both brackets
@@ -115,7 +115,7 @@ __device__ __forceinline__ LocalAdj sw_local_adjoint(float tau, float w0, float 
     const float ser = 1.f - xi * (.5f - xi * (1.f / 6.f - xi * (1.f / 24.f - xi * (1.f / 120.f))));
     float e1phi = 0.f, cI = 0.f, WI = 0.f, BR = 0.f, BT = 0.f;
     const float XI = a2 - k * km * g3, UI = a1 + k * km * g4, ZI = E1 * E1 + 2.f * e1 * En;
-    if (island) {
+    if (near1) {
         e1phi = xs ? e1 * ser : __fdividef(e1 - Tn, xi);
         cI = __fdividef(w0 * rt, 1.f + km);
         WI = thick ? Tn * (1.f + e2) - 2.f * e1 : E1 * E1 - (1.f + e2) * En;
@@ -161,7 +161,7 @@ __device__ __forceinline__ LocalAdj sw_local_adjoint(float tau, float w0, float 
     float tau_b = 0.f, w0_b = 0.f, g_b = 0.f, omw_b = 0.f;
     float k_b = 0.f, km_b = 0.f, rt_b = 0.f, E1_b = 0.f, e1_b = 0.f, E2_b = 0.f, e2_b = 0.f;
     float g1_b = 0.f, g2_b = 0.f, g3_b = 0.f, g4_b = 0.f, a1_b = 0.f, a2_b = 0.f;
-    if (island) {
+    if (near1) {
         // reverse of Rdir0 = c BR, Tdir0 = c BT (the k mu0 = 1 form above)
         const float c_b = Rdir0_b * BR + Tdir0_b * BT;
         const float BR_b = Rdir0_b * cI, BT_b = Tdir0_b * cI;

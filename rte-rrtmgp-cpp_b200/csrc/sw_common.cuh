@@ -106,16 +106,6 @@ __device__ __forceinline__ void sw_layer_fast(float tau, float w0, float omw, fl
     adir = fmaxf(0.f, rest - Tdir);
 }
 
-// The island test of sw_layer_fast (independent of tau): |1 - (k mu0)^2| < 0.02.  The adjoint
-// takes its FP64 derivatives there.
-__device__ __forceinline__ bool sw_island(float w0, float omw, float g, float mu0)
-{
-    const float kk = 2.f * omw * (2.f - .5f * w0 * (1.f + 3.f * g));
-    const float kkc = fmaxf(kk, 1.e-12f);
-    const float km = kkc * rsqrtf(kkc) * mu0;
-    return fabsf((1.f - km) * (1.f + km)) < 0.02f;
-}
-
 __device__ __forceinline__ void build_sw_record(const KdistView<float>& k, Rec& R, const LayerState& s,
                                                 const float* cg, int nlay, int b, const SwCloudArgs& cld,
                                                 size_t cl)

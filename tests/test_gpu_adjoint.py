@@ -270,11 +270,11 @@ def test_sw_adjoint_matches_fd(oracle_mod, tables, gpu, nlay, top_at_1):
 
 
 @pytest.mark.parametrize("nlay", [24, 80])
-def test_sw_adjoint_fp64_island_columns(oracle_mod, tables, gpu, nlay):
+def test_sw_adjoint_resonance_columns(oracle_mod, tables, gpu, nlay):
     """Columns with mu0 near 1/k of the strongly absorbing g-points (k ~ 2): 13% of the (layer,
-    g-point) pairs at mu0 = 0.5 take the FP64 island (|1 - (k mu0)^2| < 0.02), more than the 32
-    per chunk of 8 layers that a warp runs at once, so both the compacted and the per-layer
-    island paths run.  Checked per column against FP64 central differences."""
+    g-point) pairs at mu0 = 0.5 take the factored k mu0 = 1 form of the two-stream
+    (|1 - (k mu0)^2| < 0.02) and its hand-written reverse mode.  Checked per column against
+    FP64 central differences."""
     rng = np.random.default_rng(8)
     ncol = 4
     atm, fwd = _sw_setup(tables, oracle_mod, ncol, nlay, seed=57 + nlay, clouds=True)

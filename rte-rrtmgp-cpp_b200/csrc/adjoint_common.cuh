@@ -169,12 +169,12 @@ __device__ __forceinline__ void build_drec(const KdistView<float>& k, DRec& D, c
     }
 }
 
-// Adjoint of tau_abs for g-point g: accumulates tau_bar * dtau/dx into gT, gH, gO.
+// Adjoint of tau_abs for g-point g: accumulates tau_bar * dtau/dx into gT, gH, gO.  c0, c1:
+// the g-point's kmaj4 corners of the record's two rows (loaded by the caller, early).
 __device__ __forceinline__ void tau_abs_adjoint(const KdistView<float>& k, const Rec& R, const DRec& D, int g,
-                                                int4 mg, int nmax, float tb, float& gT, float& gH, float& gO)
+                                                int4 mg, int nmax, float tb, const float4& c0, const float4& c1,
+                                                float& gT, float& gH, float& gO)
 {
-    const float4 c0 = __ldg(k.kmaj4 + (R.kb.x + g));
-    const float4 c1 = __ldg(k.kmaj4 + (R.kb.y + g));
     float dT = dot4(D.wT0, c0) + dot4(D.wT1, c1);
     float dH = dot4(D.wH0, c0) + dot4(D.wH1, c1);
     float dO = dot4(D.wO0, c0) + dot4(D.wO1, c1);

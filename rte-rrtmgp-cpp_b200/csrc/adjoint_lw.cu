@@ -418,6 +418,11 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
             if (j < nlay && gv) {
                 const Rec& R = recs[slot * CL + i];
                 const DRec& DR = drecs[slot * CL + i];
+                // table corners first: their latency overlaps the layer terms below
+                const float4 c0 = __ldg(k.kmaj4 + (R.kb.x + g));
+                const float4 c1 = __ldg(k.kmaj4 + (R.kb.y + g));
+                const float4 p0 = __ldg(k.pfrac4 + (R.kb.x + g));
+                const float4 p1 = __ldg(k.pfrac4 + (R.kb.y + g));
                 const float pf = vpf[i];
                 const float lay = pf * R.aux.x, ldn = pf * R.aux.z, lup = pf * R.aux.y;
                 float om, fact, domt, dfact;
@@ -437,9 +442,7 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
                     gTs += Sbar * pf_bottom * DR.dB.w;
                 }
                 float gh = 0.f, go = 0.f;
-                tau_abs_adjoint(k, R, DR, g, R.a ? mg1 : mg0, R.a ? nm1 : nm0, tb, gt, gh, go);
-                const float4 p0 = __ldg(k.pfrac4 + (R.kb.x + g));
-                const float4 p1 = __ldg(k.pfrac4 + (R.kb.y + g));
+                tau_abs_adjoint(k, R, DR, g, R.a ? mg1 : mg0, R.a ? nm1 : nm0, tb, c0, c1, gt, gh, go);
                 gt += pfb * (dot4(DR.pT0, p0) + dot4(DR.pT1, p1));
                 gh += pfb * (dot4(DR.pH0, p0) + dot4(DR.pH1, p1));
                 go += pfb * (dot4(DR.pO0, p0) + dot4(DR.pO1, p1));

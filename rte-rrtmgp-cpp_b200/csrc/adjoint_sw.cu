@@ -980,14 +980,17 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
                     sm_cl[(b * kLPC + jl) * 3 + 2] += u[0];
             }
         }
-        // The exchange buffers would be safe without this barrier (each is rewritten only after
-        // the next group's previous cluster barrier), but keeping the warps in phase keeps
-        // them in the same code: without it the kernel ran 22% slower at 60 layers
-        // (instruction-cache misses).
-        cluster.sync();
+        // No barrier closes the group: each exchange buffer is rewritten in the next group only
+        // after a cluster barrier that every reader of this group's values has passed (a warp
+        // reads buffer k between barriers k and k + 1, and the next group writes it after that
+        // group's barrier k - 1 at the earliest); records and cloud sums are per warp.  (With
+        // the FP64 code in the kernel, a closing barrier measured faster at 60 layers by
+        // keeping the warps in the same code; without it the kernel is 2-4% faster at 60, 128
+        // and 256 layers.)
     }
 
     // ---- outputs ----
+    __syncthreads();   // the cloud sums of the last group are read below by other warps
     if (FLUX) {
         constexpr int SHF = (2 * CL == 16) ? 1 : 2;   // lane L holds value L >> SHF of 2 CL
         const int v = lane >> SHF;

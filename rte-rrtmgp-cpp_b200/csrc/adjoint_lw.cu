@@ -120,7 +120,7 @@ struct AdjLayout {
 // Shared memory of one CTA: LPC local layers (LPC + 1 local levels), maps of all NWt chunks of
 // the column, records of its NWc warps.
 __host__ __device__ __forceinline__ AdjLayout adj_layout(int LPC, int ngas, int nband, int NWc, int NWt, int CL,
-                                                         int mgb)
+                                                         int mgb, int nbuf)
 {
     AdjLayout L;
     L.state = 0;
@@ -130,8 +130,8 @@ __host__ __device__ __forceinline__ AdjLayout adj_layout(int LPC, int ngas, int 
     L.seeds = align16(L.taubar + sizeof(float) * size_t(nband) * LPC);
     L.levbot = align16(L.seeds + sizeof(float) * size_t(3 * LPC + 2));
     L.maps = align16(L.levbot + sizeof(double) * 16);
-    L.sfc = align16(L.maps + sizeof(float4) * size_t(NWt) * 32 * 2);
-    L.recs = align16(L.sfc + sizeof(float) * 32);
+    L.sfc = align16(L.maps + sizeof(float4) * size_t(NWt) * 32 * 2 * nbuf);
+    L.recs = align16(L.sfc + sizeof(float) * 32 * nbuf);
     L.drecs = align16(L.recs + sizeof(Rec) * size_t(NWc) * CL * mgb);
     L.total = align16(L.drecs + sizeof(DRec) * size_t(NWc) * CL * mgb);
     return L;
@@ -172,7 +172,10 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
     const int j0 = rank * LPC;              // first layer of this CTA
     const int nband = k.nband, nlev = nlay + 1;
     const int mgb = k.max_group_bands;
-    const AdjLayout SL = adj_layout(LPC, k.ngas, nband, NWc, NWt, CL, mgb);
+    // One-CTA columns double-buffer the chunk maps and the surface source by group parity, so
+    // no barrier is needed at the end of a group; clusters (maps of every chunk in every CTA)
+    // keep one buffer and that barrier.
+    const AdjLayout SL = adj_layout(LPC, k.ngas, nband, NWc, NWt, CL, mgb, CLUSTER ? 1 : 2);
     LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
     float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
     float* sm_cld = reinterpret_cast<float*>(smem_raw + SL.cld);
@@ -181,9 +184,8 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
     float* sm_b = sm_a + (LPC + 1);                                // pi * seed_dn per local level
     float* sm_h = sm_b + (LPC + 1);                                // h per local layer
     double* sm_levbot = reinterpret_cast<double*>(smem_raw + SL.levbot);
-    float4* sm_mapA = reinterpret_cast<float4*>(smem_raw + SL.maps);   // (A, Bd, Bu, BUbar) per chunk
-    float* sm_mapB = reinterpret_cast<float*>(sm_mapA + NWt * 32);     // BIbar per chunk
-    float* sm_sfc = reinterpret_cast<float*>(smem_raw + SL.sfc);
+    float4* const sm_map0 = reinterpret_cast<float4*>(smem_raw + SL.maps);
+    float* const sm_sfc0 = reinterpret_cast<float*>(smem_raw + SL.sfc);
     Rec* recs = reinterpret_cast<Rec*>(smem_raw + SL.recs) + w * CL * mgb;
     DRec* drecs = reinterpret_cast<DRec*>(smem_raw + SL.drecs) + w * CL * mgb;
     auto at_rank = [&](auto* p, int rr) { return CLUSTER ? remote(cluster, p, rr) : p; };
@@ -249,6 +251,10 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
     double acc_flev = 0.0, acc_fdiv = 0.0, acc_fbot_up = 0.0, acc_fbot_dn = 0.0;
 
     for (int gg = 0; gg < k.ngroups; ++gg) {
+        const int pb = CLUSTER ? 0 : (gg & 1);
+        float4* const sm_mapA = sm_map0 + pb * NWt * 32 * 2;                 // (A, Bd, Bu, BUbar) per chunk
+        float* const sm_mapB = reinterpret_cast<float*>(sm_mapA + NWt * 32);  // BIbar per chunk
+        float* const sm_sfc = sm_sfc0 + pb * 32;
         const int g = 32 * gg + lane;
         const bool gv = g < ngpt;
         const int b0 = k.group_band0[gg];
@@ -487,7 +493,7 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
         }
         acc_levbot += double(warp_sum(gL[CL]));
         if (Wg == (nlay - 1) / CL) acc_tsfc += double(warp_sum(gTs));
-        csync();   // maps and the surface source are rewritten by the next group
+        if (CLUSTER) csync();   // maps and the surface source are rewritten by the next group
     }
 
     // ---- outputs ----
@@ -590,7 +596,7 @@ int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
 {
     const KdistView<float>& v = k->v32;
     const int NW1 = (nlay + CL - 1) / CL;
-    const size_t smem1 = adj_layout(NW1 * CL, v.ngas, v.nband, NW1, NW1, CL, v.max_group_bands).total;
+    const size_t smem1 = adj_layout(NW1 * CL, v.ngas, v.nband, NW1, NW1, CL, v.max_group_bands, 2).total;
     RB_CHECK_ARG(CL == 8 || NW1 <= 8, "adjoint_lw: chunk 16 covers at most 128 layers");
     int CS = 1, NWc = NW1;
     size_t smem = smem1;
@@ -599,7 +605,7 @@ int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
         NWc = 16;
         CS = (nlay + 16 * CL - 1) / (16 * CL);
         RB_CHECK_ARG(CS <= 8, "adjoint_lw: at most 1024 layers");
-        smem = adj_layout(16 * CL, v.ngas, v.nband, 16, CS * 16, CL, v.max_group_bands).total;
+        smem = adj_layout(16 * CL, v.ngas, v.nband, 16, CS * 16, CL, v.max_group_bands, 1).total;
     }
     if (smem > 227 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_lw: shared memory need exceeds 227 KB");
     static bool attr = false;

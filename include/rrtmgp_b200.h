@@ -315,7 +315,9 @@ int rrtmgp_b200_rte_lw_f64(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1
  * adding (rte_solver_kernels.cu:188-278,535-647; F90 :512-606,996-1228).  mu0 (ncol);
  * inc_flux_dir (ncol, ngpt); sfc_alb_dir/dif (nband, ncol); inc_flux_dif (ncol, ngpt) or
  * NULL.  Outputs gpt_flux_up, gpt_flux_dn (total = diffuse + direct), gpt_flux_dir
- * (ncol, nlay+1, ngpt).  workspace: device scratch of rrtmgp_b200_rte_sw_workspace_bytes().*/
+ * (ncol, nlay+1, ngpt).  workspace: device scratch of rrtmgp_b200_rte_sw_workspace_bytes(),
+ * always required; only columns deeper than 256 layers (FP32) or 128 layers (FP64) use it,
+ * shallower ones run a kernel that keeps the adding recurrences on chip. */
 size_t rrtmgp_b200_rte_sw_workspace_bytes(int ncol, int nlay, int ngpt, int fp64);
 int rrtmgp_b200_rte_sw_f32(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1,
         const float* tau, const float* ssa, const float* g, const float* mu0,

@@ -10,7 +10,7 @@ using namespace fused;
 template <int CL>
 __global__ void __launch_bounds__(512) sw_forward_kernel(const KdistView<float> k, const SwGridIo io)
 {
-    sw_forward_column<CL>(CtaCtx{}, k, io);
+    sw_forward_column<CL, true>(CtaCtx{}, k, io);
 }
 
 template <int CL>
@@ -23,7 +23,7 @@ int launch_sw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
     const KdistView<float>& v = k->v32;
     const int NW = (nlay + CL - 1) / CL;
     RB_CHECK_ARG(NW <= 16, "forward_sw: nlay too large for the fused kernel (at most 16 chunks)");
-    const size_t smem = smem_layout(nlay, v.ngas, v.nband, 0, NW, 3, CL, v.max_group_bands).total;
+    const size_t smem = smem_layout(nlay, v.ngas, v.nband, 0, NW, 3, CL, v.max_group_bands * (CL == 8 ? 2 : 1)).total;
     if (smem > 220 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "forward_sw: shared memory need exceeds 220 KB");
     static bool attr = false;
     if (!attr) {

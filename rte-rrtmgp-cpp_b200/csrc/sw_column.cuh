@@ -59,20 +59,25 @@ struct SwGridIo {
 // One column by the warps that context cx names (cx.nwarps() warps of CL layers each,
 // nlay <= cx.nwarps() * CL; chunks past nlay are identity layers).  Context and arguments are
 // read through accessors at every use, as in lw_forward_column.
-template <int CL, class Cx, class Io>
+// PAIR (8-layer chunks): the records of groups gg and gg + 1 are built together at even gg
+// into two buffers (one group's 16 records per warp leave half the lanes idle).
+template <int CL, bool PAIR = false, class Cx, class Io>
 __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<float>& k, const Io& io)
 {
     static_assert(CL == 8 || CL == 16, "chunk length");
+    constexpr bool P2 = PAIR && CL == 8;
     const int lane = threadIdx.x & 31;
     const int nband = k.nband;
-    const SmemLayout SL = smem_layout(io.nlay(), k.ngas, nband, 0, cx.nwarps(), 3, CL, k.max_group_bands);
+    const SmemLayout SL = smem_layout(io.nlay(), k.ngas, nband, 0, cx.nwarps(), 3, CL,
+                                      k.max_group_bands * (P2 ? 2 : 1));
     unsigned char* const smem_raw = cx.smem();
     LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
     float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
     float* sm_pt = reinterpret_cast<float*>(smem_raw + SL.maps);                            // [NW][32]
     float4* sm_comp = reinterpret_cast<float4*>(smem_raw + SL.maps) + cx.nwarps() * 32;     // [NW][32]
     float* sm_compd = reinterpret_cast<float*>(sm_comp + cx.nwarps() * 32);                 // [NW][32]
-    Rec* recs = reinterpret_cast<Rec*>(smem_raw + SL.recs) + cx.warp() * CL * k.max_group_bands;
+    Rec* const recs0 = reinterpret_cast<Rec*>(smem_raw + SL.recs) + cx.warp() * CL * k.max_group_bands;
+    const int rbuf = cx.nwarps() * CL * k.max_group_bands;   // records per buffer
 
     bool top_at_1;
     float mu0, tsi;
@@ -105,13 +110,19 @@ __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<
         const int nm0 = __reduce_max_sync(0xffffffffu, mg0.x);
         const int nm1 = __reduce_max_sync(0xffffffffu, mg1.x);
 
-        for (int r = lane; r < CL * k.max_group_bands; r += 32) {
-            const int jj = cx.warp() * CL + (r % CL);
-            const int b = b0 + r / CL;
-            if (jj < nlay && b < nband && k.band_lims[2 * b] < 32 * gg + 32) {
-                const int l = top_at_1 ? jj : nlay - 1 - jj;
-                build_sw_record(k, recs[r], st[jj], sm_cg + jj, nlay, b, io.cloud(),
-                                cx.icol() + size_t(l) * io.ncol());
+        Rec* const recs = recs0 + (P2 ? (gg & 1) : 0) * rbuf;
+        if (!P2 || (gg & 1) == 0) {
+            const int nrec = CL * k.max_group_bands;
+            for (int t = lane; t < (P2 ? 2 : 1) * nrec; t += 32) {
+                const int gq = gg + t / nrec, r = t % nrec;
+                if (gq >= k.ngroups) continue;
+                const int jj = cx.warp() * CL + (r % CL);
+                const int b = k.group_band0[gq] + r / CL;
+                if (jj < nlay && b < nband && k.band_lims[2 * b] < 32 * gq + 32) {
+                    const int l = top_at_1 ? jj : nlay - 1 - jj;
+                    build_sw_record(k, recs0[(P2 ? (gq & 1) : 0) * rbuf + r], st[jj], sm_cg + jj, nlay, b,
+                                    io.cloud(), cx.icol() + size_t(l) * io.ncol());
+                }
             }
         }
         __syncwarp();

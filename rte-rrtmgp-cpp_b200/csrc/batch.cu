@@ -175,7 +175,7 @@ batch_forward_kernel(const KdistView<float> klw, const KdistView<float> ksw, con
             } else {
                 const SwItemIo io{{nc, nl}};
                 if (cl == 8)
-                    sw_forward_column<8>(cx, ksw, io);
+                    sw_forward_column<8, true>(cx, ksw, io);
                 else
                     sw_forward_column<16>(cx, ksw, io);
             }
@@ -261,7 +261,8 @@ size_t team_smem_bytes(const rrtmgp_b200_batch_t* b, int domain, int nlay, int c
     const KdistView<float>& v = b->k[domain]->v32;
     const int W = ceil_div_i(nlay, cl);
     const SmemLayout L = domain == 0 ? smem_layout(nlay, v.ngas, v.nband, 1, W, 2, cl, v.max_group_bands)
-                                     : smem_layout(nlay, v.ngas, v.nband, 0, W, 3, cl, v.max_group_bands);
+                                     : smem_layout(nlay, v.ngas, v.nband, 0, W, 3, cl,
+                                                   v.max_group_bands * (cl == 8 ? 2 : 1));
     return align16(L.total);
 }
 

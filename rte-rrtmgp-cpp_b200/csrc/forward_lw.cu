@@ -10,7 +10,7 @@ using namespace fused;
 template <int CL>
 __global__ void __launch_bounds__(512) lw_forward_kernel(const KdistView<float> k, const LwGridIo io)
 {
-    lw_forward_column<CL>(CtaCtx{}, k, io);
+    lw_forward_column<CL, true>(CtaCtx{}, k, io);
 }
 
 template <int CL>
@@ -22,7 +22,7 @@ int launch_lw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
     const KdistView<float>& v = k->v32;
     const int NW = (nlay + CL - 1) / CL;
     RB_CHECK_ARG(NW <= 16, "forward_lw: nlay too large for the fused kernel (at most 16 chunks)");
-    const size_t smem = smem_layout(nlay, v.ngas, v.nband, 1, NW, 2, CL, v.max_group_bands).total;
+    const size_t smem = smem_layout(nlay, v.ngas, v.nband, 1, NW, 2, CL, v.max_group_bands * (CL == 8 ? 2 : 1)).total;
     if (smem > 220 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "forward_lw: shared memory need exceeds 220 KB");
     static bool attr = false;
     if (!attr) {

@@ -94,13 +94,17 @@ __device__ __forceinline__ void build_lw_record(const KdistView<float>& k, Rec& 
 // sizes, arrays, gas set, cloud arrays) so that the batched kernel, which keeps them in shared
 // memory, holds no register for them across the column (see LwGridIo / CtaCtx for the per-grid
 // kernel, where they are launch constants).
-template <int CL, class Cx, class Io>
+// PAIR (8-layer chunks): the records of groups gg and gg + 1 are built together at even gg
+// into two buffers (one group's 16 records per warp leave half the lanes idle).
+template <int CL, bool PAIR = false, class Cx, class Io>
 __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<float>& k, const Io& io)
 {
     static_assert(CL == 8 || CL == 16, "chunk length");
+    constexpr bool P2 = PAIR && CL == 8;
     const int lane = threadIdx.x & 31;
     const int nband = k.nband;
-    const SmemLayout SL = smem_layout(io.nlay(), k.ngas, nband, 1, cx.nwarps(), 2, CL, k.max_group_bands);
+    const SmemLayout SL = smem_layout(io.nlay(), k.ngas, nband, 1, cx.nwarps(), 2, CL,
+                                      k.max_group_bands * (P2 ? 2 : 1));
     unsigned char* const smem_raw = cx.smem();
     LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
     float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
@@ -109,7 +113,8 @@ __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<
     // start the next group while others still read this group's (one barrier per group)
     float4* const sm_maps0 = reinterpret_cast<float4*>(smem_raw + SL.maps);
     float* const sm_sfc0 = reinterpret_cast<float*>(smem_raw + SL.sfc);
-    Rec* recs = reinterpret_cast<Rec*>(smem_raw + SL.recs) + cx.warp() * CL * k.max_group_bands;
+    Rec* const recs0 = reinterpret_cast<Rec*>(smem_raw + SL.recs) + cx.warp() * CL * k.max_group_bands;
+    const int rbuf = cx.nwarps() * CL * k.max_group_bands;   // records per buffer
 
     bool top_at_1;
     float ts;
@@ -154,11 +159,18 @@ __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<
         const int nm1 = __reduce_max_sync(0xffffffffu, mg1.x);
 
         // 1. records of this warp's chunk
-        for (int r = lane; r < CL * k.max_group_bands; r += 32) {
-            const int jj = cx.warp() * CL + (r % CL);
-            const int b = b0 + r / CL;
-            if (jj < nlay && b < nband && k.band_lims[2 * b] < 32 * gg + 32)
-                build_lw_record(k, recs[r], st[jj], sm_cg + jj, nlay, b, sm_cld[b * nlay + jj], jj == nlay - 1, ts);
+        Rec* const recs = recs0 + (P2 ? (gg & 1) : 0) * rbuf;
+        if (!P2 || (gg & 1) == 0) {
+            const int nrec = CL * k.max_group_bands;
+            for (int t = lane; t < (P2 ? 2 : 1) * nrec; t += 32) {
+                const int gq = gg + t / nrec, r = t % nrec;
+                if (gq >= k.ngroups) continue;
+                const int jj = cx.warp() * CL + (r % CL);
+                const int b = k.group_band0[gq] + r / CL;
+                if (jj < nlay && b < nband && k.band_lims[2 * b] < 32 * gq + 32)
+                    build_lw_record(k, recs0[(P2 ? (gq & 1) : 0) * rbuf + r], st[jj], sm_cg + jj, nlay, b,
+                                    sm_cld[b * nlay + jj], jj == nlay - 1, ts);
+            }
         }
         __syncwarp();
 

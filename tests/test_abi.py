@@ -46,6 +46,32 @@ def test_null_arguments_are_rejected_without_gpu():
     assert b"null" in lib.rrtmgp_b200_last_error()
 
 
+def test_every_entry_point_rejects_null_arguments():
+    """Every compute and handle entry point validates its arguments before any CUDA call:
+    with null handles and pointers and zero sizes each returns RRTMGP_B200_ERR_ARG and
+    leaves a message naming itself, on a machine with or without a GPU."""
+    lib = _abi.load()
+    no_status = {"rrtmgp_b200_abi_version", "rrtmgp_b200_last_error",
+                 "rrtmgp_b200_rte_sw_workspace_bytes", "rrtmgp_b200_kdist_bands"}
+    checked = 0
+    for name in sorted(_abi.declared_symbols()):
+        if name in no_status or name.endswith("_destroy"):
+            continue
+        f = getattr(lib, name)
+        args = [0 if a in (ctypes.c_int, ctypes.c_long, ctypes.c_ulong)
+                else 0.0 if a in (ctypes.c_float, ctypes.c_double) else None
+                for a in f.argtypes]
+        assert f(*args) == _abi.ERR_ARG, name
+        msg = lib.rrtmgp_b200_last_error().decode()
+        stem = name[len("rrtmgp_b200_"):].removesuffix("_f32").removesuffix("_f64")
+        assert msg.split(":")[0] in stem, (name, msg)
+        checked += 1
+    assert checked >= 50
+    for name in ("kdist", "cloud", "aerosol", "bands"):
+        getattr(lib, f"rrtmgp_b200_{name}_destroy")(None)      # destroying NULL is a no-op
+    assert lib.rrtmgp_b200_batch_destroy(None) in (0, _abi.ERR_ARG)
+
+
 def test_table_struct_dimensions(tables):
     t, keep = _abi.kdist_tables(tables["lw"])
     assert (t.nband, t.ngpt, t.ntemp, t.npres, t.neta) == (16, 256, 14, 59, 9)

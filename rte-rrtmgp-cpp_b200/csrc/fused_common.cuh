@@ -81,9 +81,16 @@ __device__ __forceinline__ float warp_sum(float x)
 }
 
 // Interpolation part of a record (interpolation_kernel, gas_optics_rrtmgp_kernels.cu:256-291)
-// for band b at layer state s.
+// for band b at layer state s; the minor scaling of interval n of the band's list goes to
+// scal_out(n, value) (R.scal[n] by default).
+struct RecScal {
+    Rec& R;
+    __device__ __forceinline__ void operator()(int n, float v) const { R.scal[n] = v; }
+};
+
+template <class ScalOut>
 __device__ __forceinline__ void record_weights(const KdistView<float>& k, Rec& R, const LayerState& s,
-                                               const float* cg, int cgs, int b)
+                                               const float* cg, int cgs, int b, const ScalOut& scal_out)
 {
     LayerInterp<float> li;
     li.jt = s.jt;
@@ -113,7 +120,13 @@ __device__ __forceinline__ void record_weights(const KdistView<float>& k, Rec& R
     R.kr[1] = ((a * k.ntemp + li.jt) * ne1 + (fw.j1 - 1)) * k.ngpt;
     int n = 0;
     for (int ii = k.band_minor_begin[a][b]; ii < k.band_minor_begin[a][b + 1] && n < kMaxMinor; ++ii, ++n)
-        R.scal[n] = minor_scaling(k, a, k.band_minor_list[a][ii], cg, cgs, s.p, s.t);
+        scal_out(n, minor_scaling(k, a, k.band_minor_list[a][ii], cg, cgs, s.p, s.t));
+}
+
+__device__ __forceinline__ void record_weights(const KdistView<float>& k, Rec& R, const LayerState& s,
+                                               const float* cg, int cgs, int b)
+{
+    record_weights(k, R, s, cg, cgs, b, RecScal{R});
 }
 
 // Absorption optical depth of g-point g from a record: major (8 corners via two float4 loads)

@@ -11,6 +11,7 @@
 #include <cmath>
 
 #include "common.cuh"
+#include "fused_common.cuh"
 #include "gas_optics_device.cuh"
 
 namespace rrtmgp_b200 {
@@ -131,6 +132,187 @@ gas_optics_sw_kernel(const KdistView<T> k, const GasSet<T> gases, int ncol, int 
     }
 }
 
+// FP32 variants on the corner-packed tables of the fused kernels (KdistView::kmaj4, pfrac4,
+// kmin2, krayl2, minor_g).  Same thread mapping and outputs; per (column, layer, g-point) the
+// major interpolation is two 16-byte loads instead of eight 4-byte ones (the Planck fraction
+// likewise), each minor interval one 8-byte pair per eta corner, and the sum over minor
+// intervals stays in registers instead of a shared-memory accumulator.  The per-band weights
+// are the records of the fused kernels (fused::record_weights) held in registers, except the
+// minor scalings, which are indexed per g-point and so sit in shared memory, one column of
+// kMaxMinor values per thread (stride kThreads: no bank conflicts).
+// Usable when the tables satisfy the fused kernels' layout conditions (packed_tables_ok).
+__host__ __device__ inline size_t packed_smem_bytes(int ngas)
+{
+    return sizeof(float) * size_t(ngas + 1 + fused::kMaxMinor) * kThreads;
+}
+
+struct ScalColumn {
+    float* p;
+    __device__ __forceinline__ void operator()(int n, float v) const { p[n * kThreads] = v; }
+};
+
+inline bool packed_tables_ok(const KdistView<float>& v, bool lw)
+{
+    return v.minor_in_band && v.max_band_minor <= fused::kMaxMinor && v.max_minor_per_g <= 3 && v.kmaj4 &&
+           v.minor_g[0] && v.minor_g[1] && (lw ? v.pfrac4 != nullptr : v.krayl2 != nullptr);
+}
+
+// Absorption optical depth of g-point g (major + minor intervals of g), as fused::tau_abs with
+// the minor scalings read from the thread's shared column scal[n * kThreads].
+// g is the same for every thread of a warp, so nmax = max(mg0.x, mg1.x) is warp-uniform.
+__device__ __forceinline__ float tau_abs_packed(const KdistView<float>& k, const fused::Rec& R,
+                                                const float* scal, int g, int4 mg, int nmax)
+{
+    const float4 c0 = __ldg(k.kmaj4 + (R.kb.x + g));
+    const float4 c1 = __ldg(k.kmaj4 + (R.kb.y + g));
+    float tau = R.wmaj0.x * c0.x + R.wmaj0.y * c0.y + R.wmaj0.z * c0.z + R.wmaj0.w * c0.w +
+                R.wmaj1.x * c1.x + R.wmaj1.y * c1.y + R.wmaj1.z * c1.z + R.wmaj1.w * c1.w;
+    const float2* kn = k.kmin2[R.a];
+#pragma unroll
+    for (int n = 0; n < 3; ++n) {
+        if (n < nmax) {
+            const int code = n == 0 ? mg.y : (n == 1 ? mg.z : mg.w);
+            const int c = code >> 4;
+            const float2 lo = __ldg(kn + (R.kb.z + c));
+            const float2 hi = __ldg(kn + (R.kb.w + c));
+            const float t = scal[(code & 15) * kThreads] *
+                            (R.fm.x * lo.x + R.fm.y * lo.y + R.fm.z * hi.x + R.fm.w * hi.y);
+            tau += (n < mg.x) ? t : 0.f;
+        }
+    }
+    return tau;
+}
+
+__device__ __forceinline__ fused::LayerState thread_layer_state(const LayerInterp<float>& li, float p, float t)
+{
+    fused::LayerState s;
+    s.jt = li.jt;
+    s.jp = li.jp;
+    s.itropo = li.itropo;
+    s.pad = 0;
+    s.ftemp = li.ftemp;
+    s.fpress = li.fpress;
+    s.p = p;
+    s.t = t;
+    s.t_top = s.t_bot = s.dp = s.pad2 = 0.f;
+    return s;
+}
+
+__global__ void __launch_bounds__(kThreads, 7)
+gas_optics_lw_packed_kernel(const KdistView<float> k, const GasSet<float> gases, int ncol, int nlay,
+                            const float* __restrict__ play, const float* __restrict__ plev,
+                            const float* __restrict__ tlay, const float* __restrict__ tsfc,
+                            const float* __restrict__ tlev, const float* __restrict__ col_dry_in,
+                            float* __restrict__ tau, float* __restrict__ lay_src, float* __restrict__ lev_inc,
+                            float* __restrict__ lev_dec, float* __restrict__ sfc_src, float* __restrict__ sfc_jac)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int tid = threadIdx.x + threadIdx.y * kBX;
+    float* cg = reinterpret_cast<float*>(smem_raw) + tid;                       // [ngas + 1]
+    float* scal = reinterpret_cast<float*>(smem_raw) + (k.ngas + 1) * kThreads + tid;   // [kMaxMinor]
+
+    const int icol = blockIdx.x * kBX + threadIdx.x;
+    const int ilay = blockIdx.y * kBY + threadIdx.y;
+    if (icol >= ncol || ilay >= nlay) return;
+    const size_t cl = size_t(icol) + size_t(ilay) * ncol;
+    const size_t ncl = size_t(ncol) * nlay;
+
+    const float p = play[cl], t = tlay[cl];
+    fill_col_gas(k, gases, ncol, nlay, icol, ilay, plev, col_dry_in, cg, kThreads);
+    const fused::LayerState s = thread_layer_state(layer_interp(k, p, t), p, t);
+
+    const int sfc_lay = play[icol] > play[icol + size_t(nlay - 1) * ncol] ? 0 : nlay - 1;
+    const bool at_sfc = ilay == sfc_lay;
+    const float tl_up = tlev[icol + size_t(ilay + 1) * ncol];
+    const float tl_dn = tlev[cl];
+    const float ts = tsfc[icol];
+
+    // minor_g entries of the next g-point are loaded one iteration ahead, so that the kminor
+    // loads of an iteration do not wait on a dependent table load
+    int4 nx0 = fused::minor_entry(k.minor_g[0], 0, true), nx1 = fused::minor_entry(k.minor_g[1], 0, true);
+    for (int b = 0; b < k.nband; ++b) {
+        const int g0 = k.band_lims[2 * b], g1 = k.band_lims[2 * b + 1];
+        fused::Rec R;
+        fused::record_weights(k, R, s, cg, kThreads, b, ScalColumn{scal});
+        const float4 wp0 = R.wpl0, wp1 = R.wpl1;
+
+        const float* tp = k.totplnk + size_t(b) * k.nplanck;
+        const float pl = interpolate1D(t, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp);
+        const float pinc = interpolate1D(tl_up, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp);
+        const float pdec = interpolate1D(tl_dn, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp);
+        float ps = 0.f, ps2 = 0.f;
+        if (at_sfc) {
+            ps = interpolate1D(ts, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp);
+            ps2 = interpolate1D(ts + 1.f, k.temp_ref_min, k.totplnk_delta, k.nplanck, tp);
+        }
+        for (int g = g0; g < g1; ++g) {
+            const int4 mg0 = nx0, mg1 = nx1;
+            nx0 = fused::minor_entry(k.minor_g[0], g + 1, g + 1 < k.ngpt);
+            nx1 = fused::minor_entry(k.minor_g[1], g + 1, g + 1 < k.ngpt);
+            const float ta = tau_abs_packed(k, R, scal, g, R.a ? mg1 : mg0, max(mg0.x, mg1.x));
+            const float4 p0 = __ldg(k.pfrac4 + (R.kb.x + g));
+            const float4 p1 = __ldg(k.pfrac4 + (R.kb.y + g));
+            const float pfrac = (wp0.x * p0.x + wp0.y * p0.y + wp0.z * p0.z + wp0.w * p0.w) +
+                                (wp1.x * p1.x + wp1.y * p1.y + wp1.z * p1.z + wp1.w * p1.w);
+            const size_t o = cl + size_t(g) * ncl;
+            tau[o] = ta;
+            lay_src[o] = pfrac * pl;
+            lev_inc[o] = pfrac * pinc;
+            lev_dec[o] = pfrac * pdec;
+            if (at_sfc) {
+                sfc_src[icol + size_t(g) * ncol] = pfrac * ps;
+                sfc_jac[icol + size_t(g) * ncol] = pfrac * (ps2 - ps);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 8)
+gas_optics_sw_packed_kernel(const KdistView<float> k, const GasSet<float> gases, int ncol, int nlay,
+                            const float* __restrict__ play, const float* __restrict__ plev,
+                            const float* __restrict__ tlay, const float* __restrict__ col_dry_in,
+                            float* __restrict__ tau, float* __restrict__ ssa, float* __restrict__ gasy)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int tid = threadIdx.x + threadIdx.y * kBX;
+    float* cg = reinterpret_cast<float*>(smem_raw) + tid;                       // [ngas + 1]
+    float* scal = reinterpret_cast<float*>(smem_raw) + (k.ngas + 1) * kThreads + tid;   // [kMaxMinor]
+
+    const int icol = blockIdx.x * kBX + threadIdx.x;
+    const int ilay = blockIdx.y * kBY + threadIdx.y;
+    if (icol >= ncol || ilay >= nlay) return;
+    const size_t cl = size_t(icol) + size_t(ilay) * ncol;
+    const size_t ncl = size_t(ncol) * nlay;
+
+    const float p = play[cl], t = tlay[cl];
+    fill_col_gas(k, gases, ncol, nlay, icol, ilay, plev, col_dry_in, cg, kThreads);
+    const fused::LayerState s = thread_layer_state(layer_interp(k, p, t), p, t);
+    const float col_rayl = cg[k.idx_h2o * kThreads] + cg[0];
+    const float two_tmin = 2.f * FLT_MIN;
+
+    int4 nx0 = fused::minor_entry(k.minor_g[0], 0, true), nx1 = fused::minor_entry(k.minor_g[1], 0, true);
+    for (int b = 0; b < k.nband; ++b) {
+        const int g0 = k.band_lims[2 * b], g1 = k.band_lims[2 * b + 1];
+        fused::Rec R;
+        fused::record_weights(k, R, s, cg, kThreads, b, ScalColumn{scal});
+        const int kr0 = R.kr[0], kr1 = R.kr[1];
+        for (int g = g0; g < g1; ++g) {
+            const int4 mg0 = nx0, mg1 = nx1;
+            nx0 = fused::minor_entry(k.minor_g[0], g + 1, g + 1 < k.ngpt);
+            nx1 = fused::minor_entry(k.minor_g[1], g + 1, g + 1 < k.ngpt);
+            const float ta = tau_abs_packed(k, R, scal, g, R.a ? mg1 : mg0, max(mg0.x, mg1.x));
+            const float2 r0 = __ldg(k.krayl2 + (kr0 + g));
+            const float2 r1 = __ldg(k.krayl2 + (kr1 + g));
+            const float tr = (R.fm.x * r0.x + R.fm.y * r0.y + R.fm.z * r1.x + R.fm.w * r1.y) * col_rayl;
+            const float tt = ta + tr;
+            const size_t o = cl + size_t(g) * ncl;
+            tau[o] = tt;
+            ssa[o] = tt > two_tmin ? tr / tt : 0.f;
+            gasy[o] = 0.f;
+        }
+    }
+}
+
 template <typename T>
 __global__ void spread_solar_kernel(int ncol, int ngpt, const T* __restrict__ src, T* __restrict__ toa)
 {
@@ -174,6 +356,15 @@ int gas_optics_lw(rrtmgp_b200_kdist k, int ncol, int nlay, const T* play, const 
     int st = make_gas_set<T>(k, ncol, nlay, gases, ngases, gs);
     if (st) return st;
     const dim3 block(kBX, kBY), grid(ceil_div(ncol, kBX), ceil_div(nlay, kBY));
+    if constexpr (std::is_same<T, float>::value) {
+        if (packed_tables_ok(k->v32, true)) {
+            gas_optics_lw_packed_kernel<<<grid, block, packed_smem_bytes(k->info.ngas), as_stream(stream)>>>(
+                k->v32, gs, ncol, nlay, play, plev, tlay, tsfc, tlev, col_dry, tau, lay_src, lev_inc, lev_dec,
+                sfc_src, sfc_jac);
+            RB_LAUNCH("gas_optics_lw_packed_kernel");
+            return RRTMGP_B200_OK;
+        }
+    }
     const size_t smem = size_t(k->info.ngas + 1 + kMaxBandGpt) * kThreads * sizeof(T);
     gas_optics_lw_kernel<T><<<grid, block, smem, as_stream(stream)>>>(
         view<T>(k), gs, ncol, nlay, play, plev, tlay, tsfc, tlev, col_dry, tau, lay_src, lev_inc,
@@ -196,10 +387,21 @@ int gas_optics_sw(rrtmgp_b200_kdist k, int ncol, int nlay, const T* play, const 
     int st = make_gas_set<T>(k, ncol, nlay, gases, ngases, gs);
     if (st) return st;
     const dim3 block(kBX, kBY), grid(ceil_div(ncol, kBX), ceil_div(nlay, kBY));
-    const size_t smem = size_t(k->info.ngas + 1 + kMaxBandGpt) * kThreads * sizeof(T);
-    gas_optics_sw_kernel<T><<<grid, block, smem, as_stream(stream)>>>(
-        view<T>(k), gs, ncol, nlay, play, plev, tlay, col_dry, tau, ssa, g);
-    RB_LAUNCH("gas_optics_sw_kernel");
+    bool packed = false;
+    if constexpr (std::is_same<T, float>::value) {
+        if (packed_tables_ok(k->v32, false)) {
+            gas_optics_sw_packed_kernel<<<grid, block, packed_smem_bytes(k->info.ngas), as_stream(stream)>>>(
+                k->v32, gs, ncol, nlay, play, plev, tlay, col_dry, tau, ssa, g);
+            RB_LAUNCH("gas_optics_sw_packed_kernel");
+            packed = true;
+        }
+    }
+    if (!packed) {
+        const size_t smem = size_t(k->info.ngas + 1 + kMaxBandGpt) * kThreads * sizeof(T);
+        gas_optics_sw_kernel<T><<<grid, block, smem, as_stream(stream)>>>(
+            view<T>(k), gs, ncol, nlay, play, plev, tlay, col_dry, tau, ssa, g);
+        RB_LAUNCH("gas_optics_sw_kernel");
+    }
     const size_t n = size_t(ncol) * k->info.ngpt;
     spread_solar_kernel<T><<<ceil_div(long(n), 256), 256, 0, as_stream(stream)>>>(
         ncol, k->info.ngpt, view<T>(k).solar_source, toa_src);

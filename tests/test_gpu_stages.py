@@ -100,6 +100,48 @@ def test_gas_optics_sw(api, oracle_mod, tables, gpu, prec, top_at_1):
     assert float(got["g"].abs().max()) == 0.0
 
 
+def _tables_with_band_crossing_minor(t):
+    """Copy of an LW table set whose h2o_frgn interval [22, 30] (band 17-32, 1-based g) is
+    moved to [28, 36], across the boundary with band 33-48: same contributor count, so the
+    kminor columns stay valid.  Such a layout is outside the corner-packed tables."""
+    t = dict(t)
+    lims = np.array(t["minor_limits_gpt_lower"], copy=True)
+    i = [n for n, (m, l) in enumerate(zip(t["minor_gases_lower"], lims))
+         if m.strip() == "h2o_frgn" and tuple(l) == (22, 30)]
+    assert i, "synthetic table layout changed"
+    lims[i[0]] = (28, 36)
+    t["minor_limits_gpt_lower"] = lims
+    return t
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_gas_optics_lw_band_crossing_minor(api, oracle_mod, tables, gpu, prec):
+    """A minor interval that spans two bands: the FP32 gas optics then runs the scalar-table
+    kernel (the packed one needs intervals inside one band) and matches the oracle, and the
+    fused forward, which needs the packed layout, refuses the table set."""
+    import torch
+    from rrtmgp_b200._abi import RrtmgpError, ERR_UNSUPPORTED
+    from rrtmgp_b200.solver import Fused_solver, Radiation_solver, atm_to_device
+    dt = dtypes()[prec]
+    t = _tables_with_band_crossing_minor(tables["lw"])
+    atm = S.make_atmosphere(NCOL, NLAY, seed=15, clouds=False)
+    ref = oracle_mod.GasOptics(t, S.ATM_GASES).gas_optics_lw(
+        atm["play"], atm["plev"], atm["tlay"], atm["tsfc"], atm["gases"], atm["tlev"], None)
+    base_ref = oracle_mod.GasOptics(tables["lw"], S.ATM_GASES).gas_optics_lw(
+        atm["play"], atm["plev"], atm["tlay"], atm["tsfc"], atm["gases"], atm["tlev"], None)
+    assert not np.allclose(ref["tau"], base_ref["tau"], rtol=1e-6)   # the move changes tau
+    kd = api.Gas_optics_rrtmgp(t, S.ATM_GASES)
+    got = kd.gas_optics_lw(T(atm["play"], dt, gpu), T(atm["plev"], dt, gpu), T(atm["tlay"], dt, gpu),
+                           T(atm["tsfc"], dt, gpu), gas_dict(atm, dt, gpu), T(atm["tlev"], dt, gpu), None)
+    for k in ("tau", "lay_src", "lev_src_inc", "lev_src_dec", "sfc_src", "sfc_src_jac"):
+        cmp(k, N(got[k]), ref[k], prec)
+    if prec == "f32":
+        base = Radiation_solver(t, tables["sw"], tables["cloud_lw"], tables["cloud_sw"], S.ATM_GASES)
+        with pytest.raises(RrtmgpError) as e:
+            Fused_solver(base).solve_lw(atm_to_device(atm, torch.float32, gpu), with_clouds=False)
+        assert e.value.status == ERR_UNSUPPORTED
+
+
 def test_gas_profile_and_scalar_inputs(api, oracle_mod, tables, gpu):
     """Gas_concs accepts scalars, (1, nlay) profiles and (ncol, nlay) fields."""
     import torch

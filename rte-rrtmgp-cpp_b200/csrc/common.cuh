@@ -77,7 +77,8 @@ struct KdistView {
     //   kmin2[a]     [t][eta][c], eta < neta-1: (k(e), k(e+1))
     //   krayl2       [a][t][eta][g], eta < neta-1: (k(e), k(e+1))
     //   minor_g[a]   [g]: x = number of intervals covering g (<= 3), y/z/w = (c << 4) | slot,
-    //                slot = position of the interval in its band's list, c = contributor.
+    //                slot = position of the interval in its band's list, c = contributor;
+    //                unused slots repeat y (0 when no interval covers g).
     const float4* kmaj4;
     const float4* pfrac4;
     const float2* kmin2[2];

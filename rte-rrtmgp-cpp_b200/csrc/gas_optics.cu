@@ -183,6 +183,12 @@ __device__ __forceinline__ float tau_abs_packed(const KdistView<float>& k, const
     return tau;
 }
 
+// minor_g row of g-point g (unused slots already repeat the first one), zeros past the end.
+__device__ __forceinline__ int4 next_minor_row(const int4* mgt, int g, int ngpt)
+{
+    return g < ngpt ? __ldg(mgt + g) : make_int4(0, 0, 0, 0);
+}
+
 __device__ __forceinline__ fused::LayerState thread_layer_state(const LayerInterp<float>& li, float p, float t)
 {
     fused::LayerState s;
@@ -229,7 +235,7 @@ gas_optics_lw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
 
     // minor_g entries of the next g-point are loaded one iteration ahead, so that the kminor
     // loads of an iteration do not wait on a dependent table load
-    int4 nx0 = fused::minor_entry(k.minor_g[0], 0, true), nx1 = fused::minor_entry(k.minor_g[1], 0, true);
+    int4 nx0 = __ldg(k.minor_g[0]), nx1 = __ldg(k.minor_g[1]);
     for (int b = 0; b < k.nband; ++b) {
         const int g0 = k.band_lims[2 * b], g1 = k.band_lims[2 * b + 1];
         fused::Rec R;
@@ -247,8 +253,8 @@ gas_optics_lw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
         }
         for (int g = g0; g < g1; ++g) {
             const int4 mg0 = nx0, mg1 = nx1;
-            nx0 = fused::minor_entry(k.minor_g[0], g + 1, g + 1 < k.ngpt);
-            nx1 = fused::minor_entry(k.minor_g[1], g + 1, g + 1 < k.ngpt);
+            nx0 = next_minor_row(k.minor_g[0], g + 1, k.ngpt);
+            nx1 = next_minor_row(k.minor_g[1], g + 1, k.ngpt);
             const float ta = tau_abs_packed(k, R, scal, g, R.a ? mg1 : mg0, max(mg0.x, mg1.x));
             const float4 p0 = __ldg(k.pfrac4 + (R.kb.x + g));
             const float4 p1 = __ldg(k.pfrac4 + (R.kb.y + g));
@@ -290,7 +296,7 @@ gas_optics_sw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
     const float col_rayl = cg[k.idx_h2o * kThreads] + cg[0];
     const float two_tmin = 2.f * FLT_MIN;
 
-    int4 nx0 = fused::minor_entry(k.minor_g[0], 0, true), nx1 = fused::minor_entry(k.minor_g[1], 0, true);
+    int4 nx0 = __ldg(k.minor_g[0]), nx1 = __ldg(k.minor_g[1]);
     for (int b = 0; b < k.nband; ++b) {
         const int g0 = k.band_lims[2 * b], g1 = k.band_lims[2 * b + 1];
         fused::Rec R;
@@ -298,8 +304,8 @@ gas_optics_sw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
         const int kr0 = R.kr[0], kr1 = R.kr[1];
         for (int g = g0; g < g1; ++g) {
             const int4 mg0 = nx0, mg1 = nx1;
-            nx0 = fused::minor_entry(k.minor_g[0], g + 1, g + 1 < k.ngpt);
-            nx1 = fused::minor_entry(k.minor_g[1], g + 1, g + 1 < k.ngpt);
+            nx0 = next_minor_row(k.minor_g[0], g + 1, k.ngpt);
+            nx1 = next_minor_row(k.minor_g[1], g + 1, k.ngpt);
             const float ta = tau_abs_packed(k, R, scal, g, R.a ? mg1 : mg0, max(mg0.x, mg1.x));
             const float2 r0 = __ldg(k.krayl2 + (kr0 + g));
             const float2 r1 = __ldg(k.krayl2 + (kr1 + g));

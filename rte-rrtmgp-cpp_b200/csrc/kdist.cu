@@ -257,6 +257,12 @@ int fill_view(rrtmgp_b200_kdist_t* k, KdistView<T>& v, const rrtmgp_b200_kdist_t
                         v.max_minor_per_g = std::max(v.max_minor_per_g, e.x);
                     }
                 }
+            // unused slots repeat the first one, so a kernel may read every slot below a
+            // warp-wide maximum count and discard the extra terms
+            for (int4& e : mg[atm]) {
+                if (e.x < 2) e.z = e.y;
+                if (e.x < 3) e.w = e.y;
+            }
         }
         if (info.has_rayleigh) {
             kr2.resize(size_t(2) * nt * (ne - 1) * ng);
@@ -333,9 +339,17 @@ int rrtmgp_b200_kdist_create(const rrtmgp_b200_kdist_tables* t, const char* cons
     const bool sw = t->solar_source_quiet && t->solar_source_facular && t->solar_source_sunspot;
     RB_CHECK_ARG(lw != sw, "kdist_create: need either (totplnk, planck_frac) or the solar source tables");
     RB_CHECK_ARG(t->nband <= kMaxBands, "kdist_create: too many bands");
-    for (int b = 0; b < t->nband; ++b)
+    RB_CHECK_ARG(t->nband > 0 && t->ngpt > 0, "kdist_create: nband and ngpt must be > 0");
+    for (int b = 0; b < t->nband; ++b) {
         RB_CHECK_ARG(t->band_lims_gpt[2 * b + 1] - t->band_lims_gpt[2 * b] + 1 <= kMaxBandGpt,
                      "kdist_create: more than 32 g-points in a band");
+        // the kernels walk the bands in order and take g-point g + 1 to follow g
+        RB_CHECK_ARG(t->band_lims_gpt[2 * b] == (b == 0 ? 1 : t->band_lims_gpt[2 * b - 1] + 1) &&
+                     t->band_lims_gpt[2 * b + 1] >= t->band_lims_gpt[2 * b],
+                     "kdist_create: band limits must cover g-points 1..ngpt in order, without gaps");
+    }
+    RB_CHECK_ARG(t->band_lims_gpt[2 * t->nband - 1] == t->ngpt,
+                 "kdist_create: band limits must cover g-points 1..ngpt in order, without gaps");
 
     *out = nullptr;
     auto* k = new rrtmgp_b200_kdist_t();

@@ -5,6 +5,7 @@ import re
 from pathlib import Path
 
 import numpy as np
+import pytest
 
 from rrtmgp_b200 import _abi, synthetic as S
 
@@ -70,6 +71,31 @@ def test_every_entry_point_rejects_null_arguments():
     for name in ("kdist", "cloud", "aerosol", "bands"):
         getattr(lib, f"rrtmgp_b200_{name}_destroy")(None)      # destroying NULL is a no-op
     assert lib.rrtmgp_b200_batch_destroy(None) in (0, _abi.ERR_ARG)
+
+
+@pytest.mark.parametrize("case", ["gap", "overlap", "short", "reversed"])
+def test_kdist_create_rejects_band_limits_with_gaps(tables, case):
+    """Band limits must cover g-points 1..ngpt in order (the kernels walk the g-points band
+    after band); kdist_create refuses other layouts before any device allocation."""
+    import ctypes as C
+    d = dict(tables["lw"])
+    lims = np.array(d["bnd_limits_gpt"], copy=True)
+    if case == "gap":
+        lims[3, 0] += 1
+    elif case == "overlap":
+        lims[3, 0] -= 1
+    elif case == "short":
+        lims[-1, 1] -= 1
+    else:
+        lims[[2, 3]] = lims[[3, 2]]
+    d["bnd_limits_gpt"] = lims
+    lib = _abi.load()
+    t, keep = _abi.kdist_tables(d)
+    names, keep2 = _abi.string_array(list(S.ATM_GASES))
+    h = C.c_void_p()
+    assert lib.rrtmgp_b200_kdist_create(C.byref(t), names, len(S.ATM_GASES), C.byref(h)) == _abi.ERR_ARG
+    assert b"band limits" in lib.rrtmgp_b200_last_error()
+    assert not h.value
 
 
 def test_table_struct_dimensions(tables):

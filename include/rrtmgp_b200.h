@@ -66,7 +66,8 @@ typedef struct rrtmgp_b200_kdist_tables {
 
     const char* const* gas_names;          /* [ngas]                                     */
     const int* key_species;                /* (nband, 2 atmos_layer, 2 pair), 1-based    */
-    const int* band_lims_gpt;              /* (nband, 2), 1-based inclusive              */
+    const int* band_lims_gpt;              /* (nband, 2), 1-based inclusive, covering    */
+                                           /* 1..ngpt in order without gaps              */
     const double* band_lims_wvn;           /* (nband, 2)                                 */
     const double* press_ref;               /* [npres], Pa, decreasing                    */
     double press_ref_trop;
@@ -110,7 +111,9 @@ typedef struct rrtmgp_b200_bands_t* rrtmgp_b200_bands;
  * src_cuda/Gas_optics_rrtmgp.cu:427-803): keeps the gases also listed in available_gases,
  * drops absent minor absorbers, builds flavors/gpoint_flavor, re-lays the tables out
  * g-point fastest in FP32 and FP64 on the current device.  Errors: MISSING_GAS when a key
- * species is not available ("Gas optics: required gas X is missing", :241-243). */
+ * species is not available ("Gas optics: required gas X is missing", :241-243); ARG for
+ * missing tables, more than 32 g-points in a band, or band limits that do not cover
+ * 1..ngpt in order without gaps (checked before any device allocation). */
 int rrtmgp_b200_kdist_create(const rrtmgp_b200_kdist_tables* tables,
                              const char* const* available_gases, int n_available,
                              rrtmgp_b200_kdist* out);

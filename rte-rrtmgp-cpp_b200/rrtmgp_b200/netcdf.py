@@ -20,7 +20,8 @@ table (v1 B-tree + local heap) or with links, compact or dense (fractal heap + v
 link names); datasets of fixed-point, floating-point and fixed-length string type (netCDF's
 NC_CHAR) with compact, contiguous or chunked storage (data layout version 3, v1 B-tree chunk
 index, deflate / shuffle / fletcher32 filters).  Anything else (layout version 4 chunk indexes,
-variable-length types, external storage) raises NetcdfError naming what it met.
+variable-length types, external storage) raises NetcdfError naming what it met.  netCDF
+classic (CDF-1) and 64-bit-offset (CDF-2) files are read too (ClassicFile); CDF-5 is not.
 """
 from __future__ import annotations
 
@@ -474,9 +475,129 @@ class _FractalHeap:
         raise NetcdfError(f"{self.f.path}: fractal heap offset {off} outside every block")
 
 
+# netCDF classic (CDF-1) and 64-bit-offset (CDF-2) format: a big-endian header listing the
+# dimensions, attributes and variables, then the variables' data at the offsets the header
+# gives; variables whose first dimension is the record (unlimited) dimension are interleaved
+# record by record.  Tags and type codes of the published format specification.
+_NC_DIMENSION, _NC_VARIABLE, _NC_ATTRIBUTE = 0x0A, 0x0B, 0x0C
+_NC_TYPES = {1: np.dtype(">i1"), 2: np.dtype("S1"), 3: np.dtype(">i2"), 4: np.dtype(">i4"),
+             5: np.dtype(">f4"), 6: np.dtype(">f8")}
+
+
+class ClassicFile:
+    """A netCDF classic or 64-bit-offset file in memory, with the interface of H5File."""
+
+    def __init__(self, path):
+        self.path = str(path)
+        self.b = Path(path).read_bytes()
+        if self.b[:3] != b"CDF" or len(self.b) < 8:
+            raise NetcdfError(f"{self.path}: not a netCDF classic file")
+        version = self.b[3]
+        if version not in (1, 2):
+            raise NetcdfError(f"{self.path}: netCDF classic version {version} not supported (CDF-1 and CDF-2 are)")
+        self.offset_size = 4 if version == 1 else 8
+        self.pos = 4
+        numrecs = self._int(4)
+        if numrecs == 0xFFFFFFFF:
+            raise NetcdfError(f"{self.path}: record count not set (file still being written)")
+        self.numrecs = numrecs
+        self.dims = self._list(_NC_DIMENSION, self._dim)
+        self._list(_NC_ATTRIBUTE, self._attr)
+        vars_ = self._list(_NC_VARIABLE, self._var)
+        self._vars = {v["name"]: v for v in vars_}
+        rec = [v for v in vars_ if v["record"]]
+        # one record variable: its records are not padded to 4 bytes
+        self.recsize = (rec[0]["slab"] if len(rec) == 1 else sum(v["vsize"] for v in rec))
+
+    def _int(self, n):
+        if self.pos + n > len(self.b):
+            raise NetcdfError(f"{self.path}: header truncated")
+        v = int.from_bytes(self.b[self.pos:self.pos + n], "big")
+        self.pos += n
+        return v
+
+    def _name(self):
+        n = self._int(4)
+        raw = self.b[self.pos:self.pos + n]
+        self.pos += (n + 3) & ~3
+        return raw.decode("utf-8", "replace")
+
+    def _list(self, tag, item):
+        t, n = self._int(4), self._int(4)
+        if t == 0 and n == 0:
+            return []
+        if t != tag:
+            raise NetcdfError(f"{self.path}: header tag {t:#x} where {tag:#x} was expected")
+        return [item() for _ in range(n)]
+
+    def _dim(self):
+        return (self._name(), self._int(4))
+
+    def _type(self):
+        t = self._int(4)
+        if t not in _NC_TYPES:
+            raise NetcdfError(f"{self.path}: netCDF type {t} not supported")
+        return _NC_TYPES[t]
+
+    def _attr(self):
+        name = self._name()
+        dt = self._type()
+        n = self._int(4)
+        self.pos += (n * dt.itemsize + 3) & ~3
+        return name
+
+    def _var(self):
+        name = self._name()
+        dimids = [self._int(4) for _ in range(self._int(4))]
+        self._list(_NC_ATTRIBUTE, self._attr)
+        dt = self._type()
+        vsize = self._int(4)
+        begin = self._int(self.offset_size)
+        for d in dimids:
+            if d >= len(self.dims):
+                raise NetcdfError(f"{self.path}: variable {name} names dimension {d} of {len(self.dims)}")
+        record = bool(dimids) and self.dims[dimids[0]][1] == 0
+        inner = [self.dims[d][1] for d in dimids[1 if record else 0:]]
+        slab = int(np.prod(inner, dtype=np.int64)) * dt.itemsize
+        return {"name": name, "dimids": dimids, "dtype": dt, "vsize": vsize, "begin": begin,
+                "record": record, "inner": inner, "slab": slab}
+
+    def variables(self):
+        return list(self._vars)
+
+    def read(self, name):
+        v = self._vars.get(name)
+        if v is None:
+            raise NetcdfError(f"{self.path}: no variable {name}")
+        dt, n_inner = v["dtype"], v["slab"] // v["dtype"].itemsize
+        if v["record"]:
+            parts = []
+            for r in range(self.numrecs):
+                off = v["begin"] + r * self.recsize
+                parts.append(self._slab(name, off, dt, n_inner))
+            a = (np.concatenate(parts) if parts else np.zeros(0, dt)).reshape([self.numrecs] + v["inner"])
+        else:
+            a = self._slab(name, v["begin"], dt, n_inner).reshape(v["inner"])
+        return a if dt.kind == "S" else a.astype(dt.newbyteorder("="))
+
+    def _slab(self, name, off, dt, count):
+        if off + count * dt.itemsize > len(self.b):
+            raise NetcdfError(f"{self.path}: data of {name} past the end of the file")
+        return np.frombuffer(self.b, dt, count, off)
+
+
+def open_netcdf(path):
+    """H5File for netCDF-4 (HDF5) files, ClassicFile for netCDF classic / 64-bit offset."""
+    head = Path(path).open("rb").read(8)
+    if head[:3] == b"CDF":
+        return ClassicFile(path)
+    return H5File(path)
+
+
 def read_netcdf(path) -> dict:
-    """Every variable of a netCDF-4 file as numpy arrays (char arrays as bytes)."""
-    f = H5File(path)
+    """Every variable of a netCDF file (netCDF-4 or classic) as numpy arrays (char arrays as
+    bytes)."""
+    f = open_netcdf(path)
     return {name: f.read(name) for name in f.variables()}
 
 

@@ -4,7 +4,9 @@ The reference ships one netCDF-4 file, data/aerosol_optics.nc (read by its
 load_and_init_aerosol_optics, src_test/Radiation_solver.cu:366-401); where the reference
 checkout is present it is decoded here and run through the aerosol optics of the oracle.  The
 k-distribution and cloud files (rrtmgp-data) are not in the checkout, so their loaders are
-exercised through the same reader only when such files are supplied (RRTMGP_DATA_DIR).
+exercised through the same reader only when such files are supplied (RRTMGP_DATA_DIR); the
+table loaders themselves are checked on netCDF classic and 64-bit-offset files that scipy's
+writer makes from the synthetic tables (the same variable names and layouts).
 """
 import os
 from pathlib import Path
@@ -77,3 +79,117 @@ def test_loads_supplied_rrtmgp_files():
         if (d / name).exists():
             c = N.load_cloud_optics(d / name)
             assert c["lut_extice"].ndim == 3
+
+
+def _write_classic(path, tables, version):
+    """Write a table dict (netCDF variable names, C order, strings as lists) as a netCDF
+    classic (version 1) or 64-bit-offset (version 2) file with scipy's writer."""
+    from scipy.io import netcdf_file
+    f = netcdf_file(str(path), "w", version=version)
+    for k, v in tables.items():
+        if k == "kind" or v is None:
+            continue
+        if isinstance(v, list):
+            width = max([1] + [len(x) for x in v])
+            a = np.zeros((len(v), width), "S1")
+            for i, x in enumerate(v):
+                a[i, :len(x)] = [bytes([c]) for c in x.encode()]
+            f.createDimension(f"{k}_n", a.shape[0])
+            f.createDimension(f"{k}_len", width)
+            f.createVariable(k, "c", (f"{k}_n", f"{k}_len"))[:] = a
+        elif np.ndim(v) == 0:
+            f.createVariable(k, "d", ())[...] = float(v)
+        else:
+            a = np.asarray(v)
+            dims = []
+            for i, n in enumerate(a.shape):
+                f.createDimension(f"{k}_{i}", n)
+                dims.append(f"{k}_{i}")
+            f.createVariable(k, "i" if a.dtype.kind == "i" else "d", tuple(dims))[:] = a
+    f.close()
+
+
+def _same_tables(got, want):
+    for k, v in want.items():
+        if k == "kind":
+            continue
+        if v is None:
+            assert got[k] is None, k
+        elif isinstance(v, list):
+            assert got[k] == v, k
+        else:
+            g = np.asarray(got[k])
+            assert g.shape == np.shape(v), (k, g.shape, np.shape(v))
+            assert np.array_equal(g, np.asarray(v)), k
+
+
+@pytest.mark.parametrize("version", [1, 2])
+@pytest.mark.parametrize("kind", ["lw", "sw"])
+def test_gas_optics_tables_round_trip_classic(tmp_path, kind, version):
+    """load_gas_optics on a classic / 64-bit-offset file written by scipy from the synthetic
+    k-distribution returns the same tables, strings and scalars included."""
+    t = S.make_kdist(kind)
+    p = tmp_path / f"gas_{kind}.nc"
+    _write_classic(p, t, version)
+    got = N.load_gas_optics(p)
+    assert got["kind"] == kind
+    _same_tables(got, t)
+    assert got["kmajor"].dtype == np.float64 and got["bnd_limits_gpt"].dtype == np.int32
+
+
+@pytest.mark.parametrize("kind", ["lw", "sw"])
+def test_cloud_and_aerosol_tables_round_trip_classic(tmp_path, kind):
+    c = S.make_cloud_luts(kind)
+    p = tmp_path / "cloud.nc"
+    _write_classic(p, c, 2)
+    got = N.load_cloud_optics(p, kind)
+    assert got["kind"] == kind
+    for k in ("lut_extliq", "lut_ssaliq", "lut_asyliq", "lut_extice", "lut_ssaice", "lut_asyice",
+              "bnd_limits_wavenumber"):
+        assert np.array_equal(got[k], c[k]), k
+    for k in ("radliq_lwr", "radliq_upr", "radice_lwr", "radice_upr", "radliq_fac", "radice_fac"):
+        assert float(got[k]) == float(np.asarray(c[k]).reshape(-1)[0]), k
+    a = S.make_aerosol_luts()
+    pa = tmp_path / "aerosol.nc"
+    _write_classic(pa, {k: a[k] for k in N._AEROSOL_VARS}, 1)
+    ga = N.load_aerosol_optics(pa)
+    for k in N._AEROSOL_VARS:
+        assert np.array_equal(ga[k], a[k]), k
+
+
+def test_classic_reader_types_records_and_errors(tmp_path):
+    """Every classic type, a record variable interleaved with another one, and the errors."""
+    from scipy.io import netcdf_file
+    p = tmp_path / "types.nc"
+    f = netcdf_file(str(p), "w", version=2)
+    f.createDimension("t", None)
+    f.createDimension("x", 3)
+    vals = {"b": ("b", np.array([-1, 2, 3], np.int8)), "h": ("h", np.array([-300, 2, 7], np.int16)),
+            "i": ("i", np.array([-70000, 1, 2], np.int32)), "f": ("f", np.array([1.5, -2.25, 3e10], np.float32)),
+            "d": ("d", np.array([1e-300, 2.0, -3.5]))}
+    for k, (code, a) in vals.items():
+        f.createVariable(k, code, ("x",))[:] = a
+    r1 = f.createVariable("r1", "d", ("t", "x"))
+    r2 = f.createVariable("r2", "h", ("t",))
+    for r in range(4):
+        r1[r] = np.arange(3) + 10.0 * r
+        r2[r] = r - 2
+    f.close()
+    c = N.ClassicFile(p)
+    assert sorted(c.variables()) == sorted(list(vals) + ["r1", "r2"])
+    for k, (_, a) in vals.items():
+        got = c.read(k)
+        assert got.dtype == a.dtype.newbyteorder("=") and np.array_equal(got, a), k
+    assert np.array_equal(c.read("r1"), np.arange(3)[None, :] + 10.0 * np.arange(4)[:, None])
+    assert np.array_equal(c.read("r2"), np.arange(4) - 2)
+    assert N.read_netcdf(p).keys() == set(c.variables())
+    with pytest.raises(N.NetcdfError, match="no variable"):
+        c.read("zz")
+    bad = tmp_path / "v5.nc"
+    bad.write_bytes(b"CDF\x05" + bytes(60))
+    with pytest.raises(N.NetcdfError, match="version 5"):
+        N.read_netcdf(bad)
+    short = tmp_path / "short.nc"
+    short.write_bytes(p.read_bytes()[:40])
+    with pytest.raises(N.NetcdfError):
+        N.read_netcdf(short)

@@ -193,3 +193,60 @@ def test_classic_reader_types_records_and_errors(tmp_path):
     short.write_bytes(p.read_bytes()[:40])
     with pytest.raises(N.NetcdfError):
         N.read_netcdf(short)
+
+
+def test_hdf5_symbol_table_v1_headers_and_chunked_filters(tmp_path):
+    """The reader's superblock-0 / v1-header / symbol-table path and every storage layout it
+    decodes, on a file written by tests/h5_writer.py: compact, contiguous, unallocated (read as
+    zeros), chunked with partial edge chunks under a one- and a two-level chunk B-tree, filter
+    pipelines of version 1 (shuffle + deflate) and 2 (deflate + fletcher32, one chunk stored with
+    deflate skipped), big- and little-endian numbers, NC_CHAR strings and a nested group."""
+    from h5_writer import H5Writer, Dataset, SHUFFLE, DEFLATE, FLETCHER32
+    rng = np.random.default_rng(4)
+    k3 = rng.standard_normal((5, 7, 9)).astype(np.float32)
+    i2 = rng.integers(-3000, 3000, (11, 6)).astype(np.int16)
+    names = np.array([[bytes([c]) for c in f"{s:<4}".encode()] for s in ("h2o", "co2", "o3")], "S1")
+    members = {
+        "kmajor": Dataset(k3, "chunked", chunks=(2, 4, 9), filters=[SHUFFLE, DEFLATE], leaf=3),
+        "counts": Dataset(i2, "chunked", chunks=(4, 6), filters=[DEFLATE, FLETCHER32], pipeline_version=2,
+                          skip={(4, 0): 1}),
+        "press_ref": Dataset(np.linspace(1.0, 1e5, 13), "contiguous"),
+        "big_endian": Dataset(np.arange(6, dtype=">i4").reshape(2, 3), "contiguous"),
+        "key_species": Dataset(np.arange(8, dtype=np.int32), "compact"),
+        "tsi_default": Dataset(np.array(1360.9), "contiguous"),
+        "gas_names": Dataset(names, "contiguous"),
+        "never_written": Dataset(np.zeros((3, 2)), "unallocated"),
+        "sub": {"inner": Dataset(np.array([1.5, 2.5], np.float64), "chunked", chunks=(1,), filters=[DEFLATE])},
+    }
+    p = tmp_path / "v0.nc"
+    H5Writer().write(p, members)
+    f = N.H5File(p)
+    assert f.variables() == sorted(["kmajor", "counts", "press_ref", "big_endian", "key_species", "tsi_default",
+                                    "gas_names", "never_written", "sub/inner"])
+    assert np.array_equal(f.read("kmajor"), k3) and f.read("kmajor").dtype == np.float32
+    assert np.array_equal(f.read("counts"), i2)
+    assert np.array_equal(f.read("press_ref"), members["press_ref"].data)
+    got = f.read("big_endian")
+    assert got.dtype == np.dtype("=i4") and np.array_equal(got, np.arange(6).reshape(2, 3))
+    assert np.array_equal(f.read("key_species"), np.arange(8))
+    assert float(f.read("tsi_default")) == 1360.9
+    assert N._strings(f.read("gas_names")) == ["h2o", "co2", "o3"]
+    assert np.array_equal(f.read("never_written"), np.zeros((3, 2)))
+    assert np.array_equal(f.read("sub/inner"), [1.5, 2.5])
+    assert set(N.read_netcdf(p)) == set(f.variables())
+
+
+def test_hdf5_aerosol_tables_round_trip(tmp_path):
+    """load_aerosol_optics on an HDF5 file of the synthetic aerosol tables (chunked and
+    deflated, as netCDF-4 writes compressed variables)."""
+    from h5_writer import H5Writer, Dataset, SHUFFLE, DEFLATE
+    a = S.make_aerosol_luts()
+    members = {}
+    for k in N._AEROSOL_VARS:
+        v = np.asarray(a[k])
+        members[k] = Dataset(v, "chunked", chunks=tuple(max(1, n // 2) for n in v.shape), filters=[SHUFFLE, DEFLATE])
+    p = tmp_path / "aerosol_h5.nc"
+    H5Writer().write(p, members)
+    got = N.load_aerosol_optics(p)
+    for k in N._AEROSOL_VARS:
+        assert np.array_equal(got[k], a[k]), k

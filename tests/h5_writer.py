@@ -1,9 +1,10 @@
 """A small HDF5 writer for tests of rrtmgp_b200.netcdf.
 
-It writes the file-format structures that the reader's symbol-table path decodes: superblock
-version 0, version-1 object headers, groups as a symbol table (v1 B-tree of group nodes + local
-heap + symbol-table nodes), datasets with a version-1 dataspace, fixed-point / floating-point /
-fixed-length string datatypes, and data layout version 3 (compact, contiguous, chunked with a
+It writes the file-format structures that the reader decodes, in two styles: superblock
+version 0 with version-1 object headers and groups as symbol tables (v1 B-tree of group nodes
++ local heap + symbol-table nodes), or superblock version 2 with version-2 object headers and
+groups as link messages.  Datasets carry a version-1 dataspace, a fixed-point / floating-point /
+fixed-length string datatype, and data layout version 3 (compact, contiguous, chunked with a
 v1 B-tree chunk index of one or two levels) behind a filter pipeline of version 1 or 2
 (shuffle, deflate, fletcher32).  The structures follow the HDF5 file-format specification;
 checksums are written as zeros (the reader does not verify them).
@@ -36,8 +37,14 @@ class Dataset:
 
 
 class H5Writer:
-    def __init__(self):
-        self.b = bytearray(96)       # superblock version 0 with the root symbol-table entry
+    """version 0: superblock 0, version-1 object headers, groups as symbol tables;
+    version 2: superblock 2, version-2 object headers ("OHDR"), groups as link messages (a link
+    info message with no dense storage plus one hard-link message per member)."""
+
+    def __init__(self, version=0):
+        assert version in (0, 2)
+        self.version = version
+        self.b = bytearray(96 if version == 0 else 48)
 
     def _alloc(self, data):
         while len(self.b) % 8:
@@ -47,6 +54,14 @@ class H5Writer:
         return addr
 
     def _header(self, msgs):
+        if self.version == 2:
+            body = bytearray()
+            for mtype, d in msgs:
+                body += struct.pack("<BHB", mtype, len(d), 0) + d
+            wide = len(body) > 255                            # flags bits 0-1: chunk-size width 1 or 2 bytes
+            head = b"OHDR" + bytes([2, 0x01 if wide else 0x00])
+            head += struct.pack("<H" if wide else "<B", len(body))
+            return self._alloc(head + body + bytes(4))       # checksum (not verified by the reader)
         body = bytearray()
         for mtype, d in msgs:
             pad = (-len(d)) % 8
@@ -157,6 +172,12 @@ class H5Writer:
         for name in sorted(members):
             m = members[name]
             addrs[name] = self.group(m) if isinstance(m, dict) else self.dataset(m)
+        if self.version == 2:
+            msgs = [(0x02, bytes([0, 0]) + struct.pack("<QQ", UNDEF, UNDEF))]    # link info, no dense links
+            for name, addr in addrs.items():
+                raw = name.encode()
+                msgs.append((0x06, bytes([1, 0x08]) + bytes([0]) + bytes([len(raw)]) + raw + struct.pack("<Q", addr)))
+            return self._header(msgs)
         heap = bytearray(8)                         # offset 0: the empty name
         offs = {}
         for name in sorted(addrs):
@@ -177,6 +198,13 @@ class H5Writer:
 
     def write(self, path, members):
         root = self.group(members)
+        if self.version == 2:
+            sb = SIG + bytes([2, 8, 8, 0]) + struct.pack("<QQQQ", 0, UNDEF, len(self.b), root) + bytes(4)
+            assert len(sb) == 48
+            self.b[:48] = sb
+            with open(path, "wb") as f:
+                f.write(bytes(self.b))
+            return
         sb = (SIG + bytes([0, 0, 0, 0, 0, 8, 8, 0]) + struct.pack("<HHI", 4, 16, 0) +
               struct.pack("<QQQQ", 0, UNDEF, len(self.b), UNDEF) + struct.pack("<QQII", 0, root, 0, 0) + bytes(16))
         assert len(sb) == 96

@@ -195,12 +195,14 @@ def test_classic_reader_types_records_and_errors(tmp_path):
         N.read_netcdf(short)
 
 
-def test_hdf5_symbol_table_v1_headers_and_chunked_filters(tmp_path):
+@pytest.mark.parametrize("style", [0, 2])
+def test_hdf5_symbol_table_v1_headers_and_chunked_filters(tmp_path, style):
     """The reader's superblock-0 / v1-header / symbol-table path and every storage layout it
     decodes, on a file written by tests/h5_writer.py: compact, contiguous, unallocated (read as
     zeros), chunked with partial edge chunks under a one- and a two-level chunk B-tree, filter
     pipelines of version 1 (shuffle + deflate) and 2 (deflate + fletcher32, one chunk stored with
-    deflate skipped), big- and little-endian numbers, NC_CHAR strings and a nested group."""
+    deflate skipped), big- and little-endian numbers, NC_CHAR strings and a nested group.  Style
+    2 writes the same datasets under superblock 2 with version-2 headers and link messages."""
     from h5_writer import H5Writer, Dataset, SHUFFLE, DEFLATE, FLETCHER32
     rng = np.random.default_rng(4)
     k3 = rng.standard_normal((5, 7, 9)).astype(np.float32)
@@ -213,16 +215,18 @@ def test_hdf5_symbol_table_v1_headers_and_chunked_filters(tmp_path):
         "press_ref": Dataset(np.linspace(1.0, 1e5, 13), "contiguous"),
         "big_endian": Dataset(np.arange(6, dtype=">i4").reshape(2, 3), "contiguous"),
         "key_species": Dataset(np.arange(8, dtype=np.int32), "compact"),
+        "compact_big": Dataset(np.arange(100, dtype=np.float64), "compact"),   # header over 255 bytes
         "tsi_default": Dataset(np.array(1360.9), "contiguous"),
         "gas_names": Dataset(names, "contiguous"),
         "never_written": Dataset(np.zeros((3, 2)), "unallocated"),
         "sub": {"inner": Dataset(np.array([1.5, 2.5], np.float64), "chunked", chunks=(1,), filters=[DEFLATE])},
     }
-    p = tmp_path / "v0.nc"
-    H5Writer().write(p, members)
+    p = tmp_path / f"v{style}.nc"
+    H5Writer(style).write(p, members)
     f = N.H5File(p)
-    assert f.variables() == sorted(["kmajor", "counts", "press_ref", "big_endian", "key_species", "tsi_default",
-                                    "gas_names", "never_written", "sub/inner"])
+    assert f.variables() == sorted(["kmajor", "counts", "press_ref", "big_endian", "key_species", "compact_big",
+                                    "tsi_default", "gas_names", "never_written", "sub/inner"])
+    assert np.array_equal(f.read("compact_big"), np.arange(100.0))
     assert np.array_equal(f.read("kmajor"), k3) and f.read("kmajor").dtype == np.float32
     assert np.array_equal(f.read("counts"), i2)
     assert np.array_equal(f.read("press_ref"), members["press_ref"].data)

@@ -128,3 +128,27 @@ def test_fused_sw_matches_staged_fp32(tables, gpu):
     b = base.solve_sw(atm)
     for k in ("flux_up", "flux_dn", "flux_dn_dir"):
         assert float((a[k] - b[k]).abs().max()) < 5e-3
+
+
+@pytest.mark.parametrize("ncol,nlay", [(1, 2), (2, 3), (1, 9), (5, 17)])
+@pytest.mark.parametrize("top_at_1", [True, False])
+def test_fused_small_domains_match_oracle(oracle_mod, tables, gpu, ncol, nlay, top_at_1):
+    """Domains far below one warp of columns and one chunk of layers (a single CTA with one
+    warp, most lanes and chunk layers idle) for both fused kernels at both chunk lengths."""
+    import torch
+    from rrtmgp_b200.solver import atm_to_device
+    base, fused = _solvers(tables)
+    atm = _vary_surface(S.make_atmosphere(ncol, nlay, seed=90 + nlay, clouds=True, top_at_1=top_at_1), nlay)
+    ref_lw = oracle_mod.forward_lw(oracle_mod.GasOptics(tables["lw"], S.ATM_GASES),
+                                   oracle_mod.CloudOptics(tables["cloud_lw"]), atm)
+    ref_sw = oracle_mod.forward_sw(oracle_mod.GasOptics(tables["sw"], S.ATM_GASES),
+                                   oracle_mod.CloudOptics(tables["cloud_sw"]), atm)
+    dev = atm_to_device(atm, torch.float32, gpu)
+    for chunk in (8, 16):
+        fused.chunk = chunk
+        got = fused.solve_lw(dev, with_clouds=True)
+        torch.cuda.synchronize()
+        _check(got, ref_lw, atm, f"lw ncol={ncol} nlay={nlay} chunk={chunk}")
+        got = fused.solve_sw(dev, with_clouds=True)
+        torch.cuda.synchronize()
+        _check_sw(got, ref_sw, f"sw ncol={ncol} nlay={nlay} chunk={chunk}")

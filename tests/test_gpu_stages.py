@@ -317,12 +317,28 @@ def test_rte_deep_columns(api, oracle_mod, tables, gpu, prec, nlay, top_at_1):
     """Layer counts around the solvers' kernel switches: the chunked kernels take 16-layer
     chunks above 128 layers (the FP64 shortwave switches to one thread per column and g-point
     there) and both solvers switch to one thread per column and g-point above 256."""
+    _gas_optics_and_rte(api, oracle_mod, tables, gpu, prec, 33, nlay, top_at_1)
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+@pytest.mark.parametrize("ncol,nlay", [(1, 2), (2, 3), (1, 9)])
+@pytest.mark.parametrize("top_at_1", [True, False])
+def test_rte_small_domains(api, oracle_mod, tables, gpu, prec, ncol, nlay, top_at_1):
+    """Domains of one or two columns and a few layers: gas optics and both solvers with most
+    lanes of every warp and most layers of every chunk idle."""
+    _gas_optics_and_rte(api, oracle_mod, tables, gpu, prec, ncol, nlay, top_at_1)
+
+
+def _gas_optics_and_rte(api, oracle_mod, tables, gpu, prec, ncol, nlay, top_at_1):
     dt = dtypes()[prec]
-    ncol = 33
     atm = S.make_atmosphere(ncol, nlay, seed=nlay, clouds=True, top_at_1=top_at_1)
     kd_lw = api.Gas_optics_rrtmgp(tables["lw"], S.ATM_GASES)
     go = oracle_mod.GasOptics(tables["lw"], S.ATM_GASES).gas_optics_lw(
         atm["play"], atm["plev"], atm["tlay"], atm["tsfc"], atm["gases"], atm["tlev"])
+    g_lw = kd_lw.gas_optics_lw(T(atm["play"], dt, gpu), T(atm["plev"], dt, gpu), T(atm["tlay"], dt, gpu),
+                               T(atm["tsfc"], dt, gpu), gas_dict(atm, dt, gpu), T(atm["tlev"], dt, gpu), None)
+    for k in ("tau", "lay_src", "lev_src_inc", "lev_src_dec", "sfc_src", "sfc_src_jac"):
+        cmp("gas lw " + k, N(g_lw[k]), go[k], prec)
     emis = np.random.default_rng(nlay).uniform(0.8, 1.0, (ncol, 16))
     up, dn = oracle_mod.rte_lw(tables["lw"]["bnd_limits_gpt"], go["tau"], top_at_1, go, emis)
     src = {k: T(v, dt, gpu) for k, v in go.items()}
@@ -332,6 +348,11 @@ def test_rte_deep_columns(api, oracle_mod, tables, gpu, prec, nlay, top_at_1):
 
     ko = oracle_mod.GasOptics(tables["sw"], S.ATM_GASES)
     gs = ko.gas_optics_sw(atm["play"], atm["plev"], atm["tlay"], atm["gases"])
+    kd_sw = api.Gas_optics_rrtmgp(tables["sw"], S.ATM_GASES)
+    g_sw = kd_sw.gas_optics_sw(T(atm["play"], dt, gpu), T(atm["plev"], dt, gpu), T(atm["tlay"], dt, gpu),
+                               gas_dict(atm, dt, gpu))
+    for k in ("tau", "ssa", "toa_src"):
+        cmp("gas sw " + k, N(g_sw[k]), gs[k], prec)
     c = oracle_mod.CloudOptics(tables["cloud_sw"]).cloud_optics(atm["lwp"], atm["iwp"], atm["rel"], atm["rei"], True)
     oracle_mod.delta_scale(c["tau"], c["ssa"], c["g"])
     bl = tables["sw"]["bnd_limits_gpt"]
@@ -342,7 +363,6 @@ def test_rte_deep_columns(api, oracle_mod, tables, gpu, prec, nlay, top_at_1):
     inc_dif = rng.uniform(0, 1, (224, ncol))
     up, dn, dr = oracle_mod.rte_sw(bl, gs["tau"], gs["ssa"], gs["g"], top_at_1, atm["mu0"], gs["toa_src"],
                                    alb_dir, alb_dif, inc_dif)
-    kd_sw = api.Gas_optics_rrtmgp(tables["sw"], S.ATM_GASES)
     gu, gd, gr = api.Rte_sw.rte_sw(kd_sw.bands, T(gs["tau"], dt, gpu), T(gs["ssa"], dt, gpu), T(gs["g"], dt, gpu),
                                    top_at_1, T(atm["mu0"], dt, gpu), T(gs["toa_src"], dt, gpu),
                                    T(alb_dir, dt, gpu), T(alb_dif, dt, gpu), T(inc_dif, dt, gpu))

@@ -491,7 +491,7 @@ def main():
         ncol, nlay = args.ncol, args.nlay
         P = api._ptr
         s = api._stream()
-        arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay)
+        arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay, atm["play"])
 
         def t_gas_lw():
             lib.rrtmgp_b200_gas_optics_lw_f32(solver.klw.handle, ncol, nlay, P(atm["play"]), P(atm["plev"]),

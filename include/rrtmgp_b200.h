@@ -318,9 +318,10 @@ int rrtmgp_b200_rte_lw_f64(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1
  * adding (rte_solver_kernels.cu:188-278,535-647; F90 :512-606,996-1228).  mu0 (ncol);
  * inc_flux_dir (ncol, ngpt); sfc_alb_dir/dif (nband, ncol); inc_flux_dif (ncol, ngpt) or
  * NULL.  Outputs gpt_flux_up, gpt_flux_dn (total = diffuse + direct), gpt_flux_dir
- * (ncol, nlay+1, ngpt).  workspace: device scratch of rrtmgp_b200_rte_sw_workspace_bytes(),
- * always required; only columns deeper than 256 layers (FP32) or 128 layers (FP64) use it,
- * shallower ones run a kernel that keeps the adding recurrences on chip. */
+ * (ncol, nlay+1, ngpt).  workspace: device scratch of rrtmgp_b200_rte_sw_workspace_bytes()
+ * bytes.  Only columns deeper than 256 layers (FP32) or 128 layers (FP64) use it; for
+ * shallower ones the kernel keeps the adding recurrences on chip, the query returns 0 and
+ * workspace may be NULL. */
 size_t rrtmgp_b200_rte_sw_workspace_bytes(int ncol, int nlay, int ngpt, int fp64);
 int rrtmgp_b200_rte_sw_f32(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1,
         const float* tau, const float* ssa, const float* g, const float* mu0,
@@ -343,7 +344,11 @@ int rrtmgp_b200_rte_sw_f64(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1
  * Limit: ncol * nlay * ngpt <= RRTMGP_B200_SW_STATIC_SCRATCH_MAX_ELEMS, else
  * RRTMGP_B200_ERR_WORKSPACE and nothing is launched (split the columns into smaller calls).
  * The first call on a device looks up the array's device address (cudaGetSymbolAddress) with
- * that device current; make that first call before any stream capture.  All calls share the
+ * that device current; make that first call before any stream capture.  The address is kept
+ * per device ordinal for the life of the process and belongs to the context that was current
+ * at that first call (normally the device's primary context, which the CUDA runtime uses):
+ * it does not survive cudaDeviceReset, and a caller that makes another context current must
+ * not use this entry point.  All calls share the
  * one array, so calls that overlap on the GPU (concurrent streams, or several host threads)
  * race and must be serialised by the caller.  No slot of the scratch needs to start at zero:
  * each call writes every slot it reads. */

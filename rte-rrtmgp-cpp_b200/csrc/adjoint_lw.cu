@@ -608,14 +608,15 @@ int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
         smem = adj_layout(16 * CL, v.ngas, v.nband, 16, CS * 16, CL, v.max_group_bands, 1).total;
     }
     if (smem > 227 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_lw: shared memory need exceeds 227 KB");
-    static bool attr = false;
-    if (!attr) {
-        RB_CUDA(cudaFuncSetAttribute(lw_adjoint_kernel<CL, false, FLUX>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "adjoint_lw attribute");
-        RB_CUDA(cudaFuncSetAttribute(lw_adjoint_kernel<8, true, FLUX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     227 * 1024), "adjoint_lw attribute");
-        attr = true;
-    }
+    static PerDeviceOnce attr;
+    const int ast = attr.run([] {
+        const cudaError_t e = cudaFuncSetAttribute(lw_adjoint_kernel<CL, false, FLUX>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        if (e != cudaSuccess) return e;
+        return cudaFuncSetAttribute(lw_adjoint_kernel<8, true, FLUX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    227 * 1024);
+    }, "adjoint_lw attribute");
+    if (ast) return ast;
     AdjCloud ca{};
     if (c) {
         ca.L = CloudLut<float>{c->nband, c->nsize_liq, c->nsize_ice, float(c->radliq_lwr), float(c->liq_step),
@@ -659,6 +660,7 @@ int adjoint_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
                    float* flux_net, float* heating_rate, int chunk, void* stream)
 {
     RB_CHECK_ARG(k && k->info.is_longwave, "adjoint_lw: need a longwave k-distribution");
+    if (const int dst = check_device(k->device, "adjoint_lw")) return dst;
     const bool with_flux = flux_up != nullptr;
     RB_CHECK_ARG(!with_flux || (flux_dn && flux_net && heating_rate), "forward_adjoint_lw: null flux array");
     RB_CHECK_ARG(ncol > 0 && nlay > 1, "adjoint_lw: ncol > 0 and nlay > 1 required");

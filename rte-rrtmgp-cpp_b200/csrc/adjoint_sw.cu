@@ -1078,6 +1078,7 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
                    float* flux_net, float* heating_rate, void* stream)
 {
     RB_CHECK_ARG(k && !k->info.is_longwave, "adjoint_sw: need a shortwave k-distribution");
+    if (const int dst = check_device(k->device, "adjoint_sw")) return dst;
     const bool with_flux = flux_up != nullptr;
     RB_CHECK_ARG(!with_flux || (flux_dn && flux_dir && flux_net && heating_rate), "forward_adjoint_sw: null flux array");
     RB_CHECK_ARG(ncol > 0 && nlay > 1, "adjoint_sw: ncol > 0 and nlay > 1 required");
@@ -1102,14 +1103,16 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     const bool pair = smem2 <= 227 * 1024;
     const size_t smem = pair ? smem2 : sw_adj_layout(v.ngas, v.nband, v.max_group_bands, CS, kLPC / CL, 1).total;
     if (smem > 227 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_sw: shared memory need exceeds 227 KB");
-    static bool attr = false;
-    if (!attr) {
+    static PerDeviceOnce attr;
+    const int ast = attr.run([] {
         for (auto fn : {sw_adjoint_kernel<CL, false, false>, sw_adjoint_kernel<CL, true, false>,
-                        sw_adjoint_kernel<CL, false, true>, sw_adjoint_kernel<CL, true, true>})
-            RB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
-                    "adjoint_sw attribute");
-        attr = true;
-    }
+                        sw_adjoint_kernel<CL, false, true>, sw_adjoint_kernel<CL, true, true>}) {
+            const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }, "adjoint_sw attribute");
+    if (ast) return ast;
     SwCloudArgs ca{};
     if (c) {
         ca.L = CloudLut<float>{c->nband, c->nsize_liq, c->nsize_ice, float(c->radliq_lwr), float(c->liq_step),

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -26,6 +27,42 @@ int cuda_status(cudaError_t err, const char* where);
     do { cudaError_t e_ = cudaGetLastError(); if (e_ != cudaSuccess) return ::rrtmgp_b200::cuda_status(e_, (where)); } while (0)
 
 inline int ceil_div(long a, long b) { return int((a + b - 1) / b); }
+
+// Per-device one-time set-up (cudaFuncSetAttribute and the like act on the current device's
+// context only).  run(f) calls f once for every device that is current when run is called,
+// from any host thread; a failed f is retried on the next call.
+class PerDeviceOnce {
+public:
+    template <class F>
+    int run(F&& f, const char* where)
+    {
+        int dev = 0;
+        RB_CUDA(cudaGetDevice(&dev), where);
+        if (dev < 0 || dev >= 64) return fail(RRTMGP_B200_ERR_UNSUPPORTED, std::string(where) + ": device ordinal >= 64");
+        std::lock_guard<std::mutex> lock(mu_);
+        if ((done_ >> dev) & 1ull) return RRTMGP_B200_OK;
+        RB_CUDA(f(), where);
+        done_ |= 1ull << dev;
+        return RRTMGP_B200_OK;
+    }
+
+private:
+    std::mutex mu_;
+    unsigned long long done_ = 0;
+};
+
+// Handles hold device pointers of the device they were created on: a call made while another
+// device is current is refused.
+inline int check_device(int handle_device, const char* where)
+{
+    int dev = 0;
+    RB_CUDA(cudaGetDevice(&dev), where);
+    if (dev != handle_device)
+        return fail(RRTMGP_B200_ERR_ARG, std::string(where) + ": the handle's tables live on device " +
+                                             std::to_string(handle_device) + ", the current device is " +
+                                             std::to_string(dev));
+    return RRTMGP_B200_OK;
+}
 
 constexpr int kMaxGases = 24;          // gases in one k-distribution after reduction
 constexpr int kMaxBandGpt = 32;        // g-points per band handled in registers/shared mem

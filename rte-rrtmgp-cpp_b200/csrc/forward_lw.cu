@@ -24,12 +24,10 @@ int launch_lw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
     RB_CHECK_ARG(NW <= 16, "forward_lw: nlay too large for the fused kernel (at most 16 chunks)");
     const size_t smem = smem_layout(nlay, v.ngas, v.nband, 1, NW, 2, CL, v.max_group_bands * (CL == 8 ? 2 : 1)).total;
     if (smem > 220 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "forward_lw: shared memory need exceeds 220 KB");
-    static bool attr = false;
-    if (!attr) {
-        RB_CUDA(cudaFuncSetAttribute(lw_forward_kernel<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024),
-                "forward_lw attribute");
-        attr = true;
-    }
+    static PerDeviceOnce attr;
+    int st = attr.run([] { return cudaFuncSetAttribute(lw_forward_kernel<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       220 * 1024); }, "forward_lw attribute");
+    if (st) return st;
     CloudArgs ca{};
     if (c) {
         ca.L = CloudLut<float>{c->nband, c->nsize_liq, c->nsize_ice, float(c->radliq_lwr), float(c->liq_step),
@@ -52,6 +50,7 @@ int forward_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
                    float* flux_net, float* heating_rate, int chunk, void* stream)
 {
     RB_CHECK_ARG(k && k->info.is_longwave, "forward_lw: need a longwave k-distribution");
+    if (const int dst = check_device(k->device, "forward_lw")) return dst;
     RB_CHECK_ARG(ncol > 0 && nlay > 1, "forward_lw: ncol > 0 and nlay > 1 required");
     RB_CHECK_ARG(play && plev && tlay && tlev && tsfc && sfc_emis && flux_up && flux_dn && flux_net && heating_rate,
                  "forward_lw: null array");

@@ -25,12 +25,10 @@ int launch_sw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
     RB_CHECK_ARG(NW <= 16, "forward_sw: nlay too large for the fused kernel (at most 16 chunks)");
     const size_t smem = smem_layout(nlay, v.ngas, v.nband, 0, NW, 3, CL, v.max_group_bands * (CL == 8 ? 2 : 1)).total;
     if (smem > 220 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "forward_sw: shared memory need exceeds 220 KB");
-    static bool attr = false;
-    if (!attr) {
-        RB_CUDA(cudaFuncSetAttribute(sw_forward_kernel<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024),
-                "forward_sw attribute");
-        attr = true;
-    }
+    static PerDeviceOnce attr;
+    int st = attr.run([] { return cudaFuncSetAttribute(sw_forward_kernel<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       220 * 1024); }, "forward_sw attribute");
+    if (st) return st;
     SwCloudArgs ca{};
     if (c) {
         ca.L = CloudLut<float>{c->nband, c->nsize_liq, c->nsize_ice, float(c->radliq_lwr), float(c->liq_step),
@@ -55,6 +53,7 @@ int forward_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
                    float* heating_rate, int chunk, void* stream)
 {
     RB_CHECK_ARG(k && !k->info.is_longwave, "forward_sw: need a shortwave k-distribution");
+    if (const int dst = check_device(k->device, "forward_sw")) return dst;
     RB_CHECK_ARG(ncol > 0 && nlay > 1, "forward_sw: ncol > 0 and nlay > 1 required");
     RB_CHECK_ARG(play && plev && tlay && mu0 && sfc_alb_dir && sfc_alb_dif && flux_up && flux_dn && flux_dn_dir &&
                  flux_net && heating_rate, "forward_sw: null array");

@@ -358,6 +358,7 @@ int gas_optics_lw(rrtmgp_b200_kdist k, int ncol, int nlay, const T* play, const 
     RB_CHECK_ARG(ncol > 0 && nlay > 0, "gas_optics_lw: ncol and nlay must be > 0");
     RB_CHECK_ARG(play && plev && tlay && tsfc && tlev && tau && lay_src && lev_inc && lev_dec && sfc_src &&
                  sfc_jac, "gas_optics_lw: null array");
+    if (const int dst = check_device(k->device, "gas_optics_lw")) return dst;
     GasSet<T> gs;
     int st = make_gas_set<T>(k, ncol, nlay, gases, ngases, gs);
     if (st) return st;
@@ -389,6 +390,7 @@ int gas_optics_sw(rrtmgp_b200_kdist k, int ncol, int nlay, const T* play, const 
     RB_CHECK_ARG(ncol > 0 && nlay > 0, "gas_optics_sw: ncol and nlay must be > 0");
     RB_CHECK_ARG(play && plev && tlay && tau && ssa && g && toa_src, "gas_optics_sw: null array");
     RB_CHECK_ARG(k->info.has_rayleigh, "gas_optics_sw: Rayleigh tables required");
+    if (const int dst = check_device(k->device, "gas_optics_sw")) return dst;
     GasSet<T> gs;
     int st = make_gas_set<T>(k, ncol, nlay, gases, ngases, gs);
     if (st) return st;

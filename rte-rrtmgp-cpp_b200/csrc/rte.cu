@@ -464,12 +464,11 @@ int rte_lw(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const T* tau, 
     size_t smem = 0;
     const int bs = lw_smem_block<T>(nlay, &smem);
     if (bs > 0) {
-        static bool attr_set = false;
-        if (!attr_set) {
-            RB_CUDA(cudaFuncSetAttribute(lw_solver_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         96 * 1024), "rte_lw attribute");
-            attr_set = true;
-        }
+        static PerDeviceOnce attr;
+        const int ast = attr.run([] { return cudaFuncSetAttribute(lw_solver_kernel<T, true>,
+                                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                                  96 * 1024); }, "rte_lw attribute");
+        if (ast) return ast;
         const dim3 grid(ceil_div(ncol, bs), b->ngpt);
         lw_solver_kernel<T, true><<<grid, bs, smem, as_stream(stream)>>>(
             ncol, nlay, b->nband, top_at_1, nmus, b->d_gpt2band, tau, lay_src, lev_inc, lev_dec, sfc_src, sfc_emis,
@@ -484,8 +483,12 @@ int rte_lw(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const T* tau, 
     return RRTMGP_B200_OK;
 }
 
+// Columns up to this depth run the chunked shortwave solver, which needs no workspace.
+constexpr int sw_chunked_max_nlay(bool fp64) { return fp64 ? 128 : 256; }
+
 size_t sw_ws_bytes(int ncol, int nlay, int ngpt, int fp64)
 {
+    if (ncol <= 0 || nlay <= 0 || ngpt <= 0 || nlay <= sw_chunked_max_nlay(fp64 != 0)) return 0;
     return size_t(4) * ncol * nlay * ngpt * (fp64 ? sizeof(double) : sizeof(float));
 }
 
@@ -498,12 +501,9 @@ int rte_sw(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const T* tau, 
     RB_CHECK_ARG(ncol > 0 && nlay > 0, "rte_sw: ncol and nlay must be > 0");
     RB_CHECK_ARG(tau && ssa && g && mu0 && inc_dir && alb_dir && alb_dif && flux_up && flux_dn && flux_dir,
                  "rte_sw: null array");
-    const size_t need = sw_ws_bytes(ncol, nlay, b->ngpt, sizeof(T) == 8);
-    if (!ws || ws_bytes < need)
-        return fail(RRTMGP_B200_ERR_WORKSPACE, "rte_sw: workspace of " + std::to_string(need) + " bytes required");
     // Chunked solver up to 256 layers (FP64: 128; its deeper columns would spill registers).
     constexpr bool fp64 = sizeof(T) == 8;
-    if (nlay <= (fp64 ? 128 : 256)) {
+    if (nlay <= sw_chunked_max_nlay(fp64)) {
         const dim3 grid(ceil_div(ncol, 32), b->ngpt);
         if constexpr (fp64) {
             sw_solver_chunked<T, 16, 256><<<grid, 32 * ceil_div(nlay, 16), 0, as_stream(stream)>>>(
@@ -521,6 +521,9 @@ int rte_sw(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const T* tau, 
         RB_LAUNCH("sw_solver_chunked");
         return RRTMGP_B200_OK;
     }
+    const size_t need = sw_ws_bytes(ncol, nlay, b->ngpt, fp64);
+    if (!ws || ws_bytes < need)
+        return fail(RRTMGP_B200_ERR_WORKSPACE, "rte_sw: workspace of " + std::to_string(need) + " bytes required");
     const dim3 grid(ceil_div(ncol, 64), b->ngpt);
     sw_solver_kernel<T, double><<<grid, 64, 0, as_stream(stream)>>>(
         ncol, nlay, b->ngpt, b->nband, top_at_1, b->d_gpt2band, tau, ssa, g, mu0, inc_dir, alb_dir, alb_dif,

@@ -127,16 +127,29 @@ class Gas_optics_rrtmgp:
         self.info = info
 
     @staticmethod
-    def _gases(gases: dict, ncol, nlay):
+    def _gases(gases: dict, ncol, nlay, like):
+        """GasConc array of the C ABI for {name: vmr}.  Every vmr must be a CUDA tensor on the
+        device of `like` with its dtype (the kernel reads it as that type), shaped as a scalar,
+        a profile (nlay,) / (nlay, 1) or a field (nlay, ncol); anything else raises before a
+        pointer is taken."""
         arr = (_abi.GasConc * max(len(gases), 1))()
         keep = []
         for i, (name, v) in enumerate(gases.items()):
+            if not isinstance(v, torch.Tensor):
+                raise ValueError(f"gas '{name}': vmr must be a torch tensor")
+            if v.dtype != like.dtype:
+                raise ValueError(f"gas '{name}': vmr dtype {v.dtype} differs from the call's {like.dtype}")
             if v.dim() == 0 or v.numel() == 1:
                 d1, d2 = 1, 1
-            elif v.dim() == 1 or (v.dim() == 2 and v.shape[1] == 1):
+            elif (v.dim() == 1 and v.shape[0] == nlay) or (v.dim() == 2 and v.shape == (nlay, 1)):
                 d1, d2 = 1, nlay
-            else:
+            elif v.dim() == 2 and v.shape == (nlay, ncol):
                 d1, d2 = ncol, nlay
+            else:
+                raise ValueError(f"gas '{name}': vmr shape {tuple(v.shape)} is none of (), ({nlay},), "
+                                 f"({nlay}, 1), ({nlay}, {ncol})")
+            if not v.is_cuda or v.device != like.device:
+                raise ValueError(f"gas '{name}': vmr must be a CUDA tensor on {like.device}")
             v = v.contiguous()
             keep.append(v)
             arr[i].name = name.encode()
@@ -154,7 +167,7 @@ class Gas_optics_rrtmgp:
     def gas_optics_lw(self, play, plev, tlay, tsfc, gases: dict, tlev, col_dry=None):
         nlay, ncol = play.shape
         ng = self.info.ngpt
-        arr, keep = self._gases(gases, ncol, nlay)
+        arr, keep = self._gases(gases, ncol, nlay, play)
         out = {k: _empty((ng, nlay, ncol), play) for k in ("tau", "lay_src", "lev_src_inc", "lev_src_dec")}
         out["sfc_src"] = _empty((ng, ncol), play)
         out["sfc_src_jac"] = _empty((ng, ncol), play)
@@ -167,7 +180,7 @@ class Gas_optics_rrtmgp:
     def gas_optics_sw(self, play, plev, tlay, gases: dict, col_dry=None):
         nlay, ncol = play.shape
         ng = self.info.ngpt
-        arr, keep = self._gases(gases, ncol, nlay)
+        arr, keep = self._gases(gases, ncol, nlay, play)
         out = {k: _empty((ng, nlay, ncol), play) for k in ("tau", "ssa", "g")}
         out["toa_src"] = _empty((ng, ncol), play)
         _call("gas_optics_sw", play, self.handle, ncol, nlay, _ptr(play), _ptr(plev), _ptr(tlay), _ptr(col_dry),
@@ -233,7 +246,7 @@ class Aerosol_optics:
         """aerosols: {aermr01 .. aermr11: tensor (nlay, ncol), (nlay,) or scalar}; rh (nlay,
         ncol); plev (nlay+1, ncol).  Returns tau, ssa, g (nband, nlay, ncol)."""
         nlay, ncol = rh.shape
-        arr, keep = Gas_optics_rrtmgp._gases(aerosols, ncol, nlay)
+        arr, keep = Gas_optics_rrtmgp._gases(aerosols, ncol, nlay, rh)
         tau = _empty((self.nband, nlay, ncol), rh)
         ssa, g = _empty(tau.shape, rh), _empty(tau.shape, rh)
         _call("aerosol_optics", rh, self.handle, ncol, nlay, arr, len(aerosols), _ptr(rh), _ptr(plev), _ptr(tau),
@@ -298,7 +311,8 @@ class Rte_sw:
         ws = workspace if workspace is not None else cls.workspace(ncol, nlay, ngpt, tau)
         _call("rte_sw", tau, bands.handle, ncol, nlay, int(bool(top_at_1)), _ptr(tau), _ptr(ssa), _ptr(g),
               _ptr(mu0), _ptr(inc_flux_dir), _ptr(sfc_alb_dir), _ptr(sfc_alb_dif), _ptr(inc_flux_dif),
-              _ptr(up), _ptr(dn), _ptr(dr), C.c_void_p(ws.data_ptr()), C.c_size_t(ws.numel()), _stream())
+              _ptr(up), _ptr(dn), _ptr(dr), C.c_void_p(ws.data_ptr()) if ws.numel() else None,
+              C.c_size_t(ws.numel()), _stream())
         return up, dn, dr
 
 

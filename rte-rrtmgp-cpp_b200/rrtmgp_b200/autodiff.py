@@ -69,7 +69,7 @@ class _LongwaveFn(torch.autograd.Function):
         grads["tlev"] = torch.empty((nlay + 1, ncol), dtype=torch.float32, device=dev)
         grads["tsfc"] = torch.empty((ncol,), dtype=torch.float32, device=dev)
         P = api._ptr
-        arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay)
+        arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay, atm["play"])
         c = fused.base.clw if ctx.clouds else None
         cl = (lambda k: P(atm[k])) if c else (lambda k: None)
         _abi.check(_abi.load().rrtmgp_b200_adjoint_lw_f32(
@@ -114,7 +114,7 @@ def adjoint_lw(fused, atm: dict, seed_up=None, seed_dn=None, seed_hr=None, with_
     grads["tlev"] = torch.empty((nlay + 1, ncol), dtype=torch.float32, device=dev)
     grads["tsfc"] = torch.empty((ncol,), dtype=torch.float32, device=dev)
     P = api._ptr
-    arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay)
+    arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay, atm["play"])
     cl = (lambda k: P(atm[k])) if c else (lambda k: None)
     args = [fused.base.klw.handle, c.handle if c else None, ncol, nlay, P(play), P(atm["plev"]), P(atm["tlay"]),
             P(atm["tlev"]), P(atm["tsfc"]), None, arr, len(atm["gases"]), cl("lwp"), cl("iwp"), cl("rel"),
@@ -149,7 +149,7 @@ def adjoint_sw(fused, atm: dict, seed_up=None, seed_dn=None, seed_dir=None, seed
     grads["sfc_alb_dir"] = torch.empty((ncol, nb), dtype=torch.float32, device=dev)
     grads["sfc_alb_dif"] = torch.empty((ncol, nb), dtype=torch.float32, device=dev)
     P = api._ptr
-    arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay)
+    arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay, atm["play"])
     cl = (lambda k: P(atm[k])) if c else (lambda k: None)
     tsi = atm.get("tsi_scaling")
     args = [fused.base.ksw.handle, c.handle if c else None, ncol, nlay, P(play), P(atm["plev"]), P(atm["tlay"]),

@@ -103,7 +103,7 @@ class Batched_forward:
             g.play, g.plev, g.tlay = _ptr(play), _ptr(atm["plev"]), _ptr(atm["tlay"])
             g.tlev, g.tsfc = _ptr(atm.get("tlev")), _ptr(atm.get("tsfc"))
             g.col_dry = _ptr(atm.get("col_dry"))
-            arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay)
+            arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay, atm["play"])
             self._keep += [arr, keep]
             g.gases = C.cast(arr, C.POINTER(_abi.GasConc))
             g.ngases = len(atm["gases"])

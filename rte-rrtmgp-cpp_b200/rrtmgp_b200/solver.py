@@ -72,7 +72,7 @@ class Radiation_solver:
         sfx = api._sfx(play)
         s = api._stream()
         P = api._ptr
-        arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay)
+        arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay, atm["play"])
         _abi.check(getattr(lib, "rrtmgp_b200_gas_optics_lw" + sfx)(
             self.klw.handle, ncol, nlay, P(play), P(atm["plev"]), P(atm["tlay"]), P(atm["tsfc"]), P(atm["tlev"]),
             None, arr, len(atm["gases"]), P(b["tau"]), P(b["lay_src"]), P(b["lev_src_inc"]), P(b["lev_src_dec"]),
@@ -107,7 +107,7 @@ class Radiation_solver:
         sfx = api._sfx(play)
         s = api._stream()
         P = api._ptr
-        arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay)
+        arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay, atm["play"])
         _abi.check(getattr(lib, "rrtmgp_b200_gas_optics_sw" + sfx)(
             self.ksw.handle, ncol, nlay, P(play), P(atm["plev"]), P(atm["tlay"]), None, arr, len(atm["gases"]),
             P(b["tau"]), P(b["ssa"]), P(b["g"]), P(b["toa_src"]), s))
@@ -171,7 +171,7 @@ class Fused_solver:
         nlay, ncol = play.shape
         o = self._outputs("lw", play, ncol, nlay)
         P = api._ptr
-        arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay)
+        arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay, atm["play"])
         c = self.base.clw if (with_clouds and self.base.clw is not None) else None
         _abi.check(_abi.load().rrtmgp_b200_forward_lw_f32(
             self.base.klw.handle, c.handle if c else None, ncol, nlay, P(play), P(atm["plev"]), P(atm["tlay"]),
@@ -189,7 +189,7 @@ class Fused_solver:
         nlay, ncol = play.shape
         o = self._outputs("sw", play, ncol, nlay)
         P = api._ptr
-        arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay)
+        arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay, atm["play"])
         c = self.base.csw if (with_clouds and self.base.csw is not None) else None
         tsi = atm.get("tsi_scaling")
         _abi.check(_abi.load().rrtmgp_b200_forward_sw_f32(

@@ -208,4 +208,6 @@ def main(outdir: Path):
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else REPO / "gpurun_out" / "golden")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_ref_golden.py OUTPUT_DIR")
+    main(Path(sys.argv[1]))

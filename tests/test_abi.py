@@ -36,8 +36,11 @@ def test_binding_signatures_load():
 
 def test_workspace_query_needs_no_gpu():
     lib = _abi.load()
-    assert lib.rrtmgp_b200_rte_sw_workspace_bytes(10, 20, 30, 0) == 4 * 10 * 20 * 30 * 4
-    assert lib.rrtmgp_b200_rte_sw_workspace_bytes(10, 20, 30, 1) == 4 * 10 * 20 * 30 * 8
+    # on-chip solver up to 256 layers (FP32) / 128 (FP64): no workspace
+    assert lib.rrtmgp_b200_rte_sw_workspace_bytes(10, 20, 30, 0) == 0
+    assert lib.rrtmgp_b200_rte_sw_workspace_bytes(10, 256, 30, 0) == 0
+    assert lib.rrtmgp_b200_rte_sw_workspace_bytes(10, 129, 30, 1) == 4 * 10 * 129 * 30 * 8
+    assert lib.rrtmgp_b200_rte_sw_workspace_bytes(10, 257, 30, 0) == 4 * 10 * 257 * 30 * 4
 
 
 def test_null_arguments_are_rejected_without_gpu():
@@ -115,3 +118,20 @@ def test_synthetic_atmosphere_layout():
     assert atm["plev"][0, 0] >= S.PRESS_REF_MIN
     flip = S.make_atmosphere(7, 9, seed=1, top_at_1=False)
     assert np.all(np.diff(flip["plev"][:, 0]) < 0)
+
+
+def test_gas_concentrations_are_validated_before_any_pointer_is_taken():
+    """Gas_concs entries reach the kernels as raw pointers read in the call's precision, so a
+    host tensor, another dtype or an unknown shape is refused on the host (no GPU needed)."""
+    import torch
+    from rrtmgp_b200 import api
+    nlay, ncol = 6, 5
+    play = torch.ones((nlay, ncol), dtype=torch.float32)
+    with pytest.raises(ValueError, match="dtype"):
+        api.Gas_optics_rrtmgp._gases({"h2o": torch.ones((nlay, ncol), dtype=torch.float64)}, ncol, nlay, play)
+    with pytest.raises(ValueError, match="CUDA"):
+        api.Gas_optics_rrtmgp._gases({"h2o": torch.ones((nlay, ncol), dtype=torch.float32)}, ncol, nlay, play)
+    with pytest.raises(ValueError, match="shape"):
+        api.Gas_optics_rrtmgp._gases({"o3": torch.ones((ncol, nlay), dtype=torch.float32)}, ncol, nlay, play)
+    with pytest.raises(ValueError, match="torch tensor"):
+        api.Gas_optics_rrtmgp._gases({"co2": np.ones(1, np.float32)}, ncol, nlay, play)

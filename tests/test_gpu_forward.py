@@ -152,3 +152,46 @@ def test_fused_small_domains_match_oracle(oracle_mod, tables, gpu, ncol, nlay, t
         got = fused.solve_sw(dev, with_clouds=True)
         torch.cuda.synchronize()
         _check_sw(got, ref_sw, f"sw ncol={ncol} nlay={nlay} chunk={chunk}")
+
+
+def test_fused_forward_from_two_host_threads(tables, gpu):
+    """The fused entry points are called from two host threads at once, each on its own
+    stream with its own output buffers and the same k-distribution handles (handles are
+    immutable after creation; the launchers' one-time per-device set-up is locked).  Every
+    result equals the single-thread result bit for bit."""
+    import threading
+
+    import torch
+    from rrtmgp_b200.solver import Fused_solver, atm_to_device
+    base, fused = _solvers(tables)
+    atms = [atm_to_device(S.make_atmosphere(64, 60 + 30 * i, seed=70 + i, clouds=True), torch.float32, gpu)
+            for i in range(2)]
+    want = []
+    for a in atms:
+        lw, sw = fused.solve_lw(a), fused.solve_sw(a)
+        want.append({**{"lw_" + k: v.clone() for k, v in lw.items()}, **{"sw_" + k: v.clone() for k, v in sw.items()}})
+    torch.cuda.synchronize()
+    got, errors = [None, None], []
+
+    def run(i):
+        try:
+            f = Fused_solver(base)
+            s = torch.cuda.Stream(device=gpu)
+            with torch.cuda.stream(s):
+                for _ in range(20):
+                    lw, sw = f.solve_lw(atms[i]), f.solve_sw(atms[i])
+                got[i] = {**{"lw_" + k: v.clone() for k, v in lw.items()},
+                          **{"sw_" + k: v.clone() for k, v in sw.items()}}
+            s.synchronize()
+        except Exception as e:   # reported in the main thread
+            errors.append(e)
+
+    threads = [threading.Thread(target=run, args=(i,)) for i in range(2)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=120)
+    assert not errors, errors
+    for i in range(2):
+        for k, v in want[i].items():
+            assert torch.equal(got[i][k], v), f"thread {i} {k}"

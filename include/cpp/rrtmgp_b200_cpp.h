@@ -113,6 +113,14 @@ inline int rte_lw(rrtmgp_b200_bands b, int ncol, int nlay, int top, const double
                   const double* inc, const double* dec, const double* sfc, const double* emis, const double* incf,
                   int nmu, double* up, double* dn)
 { return rrtmgp_b200_rte_lw_f64(b, ncol, nlay, top, tau, lay, inc, dec, sfc, emis, incf, nmu, up, dn, stream()); }
+inline int rte_lw_jac(rrtmgp_b200_bands b, int ncol, int nlay, int top, const float* tau, const float* lay,
+                      const float* inc, const float* dec, const float* sfc, const float* sfc_jac, const float* emis,
+                      const float* incf, int nmu, float* up, float* dn, float* up_jac)
+{ return rrtmgp_b200_rte_lw_jac_f32(b, ncol, nlay, top, tau, lay, inc, dec, sfc, sfc_jac, emis, incf, nmu, up, dn, up_jac, stream()); }
+inline int rte_lw_jac(rrtmgp_b200_bands b, int ncol, int nlay, int top, const double* tau, const double* lay,
+                      const double* inc, const double* dec, const double* sfc, const double* sfc_jac,
+                      const double* emis, const double* incf, int nmu, double* up, double* dn, double* up_jac)
+{ return rrtmgp_b200_rte_lw_jac_f64(b, ncol, nlay, top, tau, lay, inc, dec, sfc, sfc_jac, emis, incf, nmu, up, dn, up_jac, stream()); }
 
 inline int rte_sw(rrtmgp_b200_bands b, int ncol, int nlay, int top, const float* tau, const float* ssa,
                   const float* g, const float* mu0, const float* idir, const float* ad, const float* af,

@@ -313,6 +313,23 @@ int rrtmgp_b200_rte_lw_f64(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1
         const double* lev_src_dec, const double* sfc_src, const double* sfc_emis,
         const double* inc_flux, int n_gauss_angles, double* gpt_flux_up, double* gpt_flux_dn,
         void* stream);
+/* The same solve with the surface-temperature Jacobian: the reference's do_jacobians path of
+ * lw_solver_noscat (rte_solver_kernels.cu:56,65,82,91 and the step-3 scaling; wired through
+ * src_cuda/Rte_lw.cu:125-148, where the reference disables it).  sfc_src_jac (ncol, ngpt) is
+ * the gas optics' sfc_source_jac (Planck source at Tsfc + 1 K minus at Tsfc);
+ * gpt_flux_up_jac (ncol, nlay+1, ngpt) receives 2 pi w sum over angles of the upward
+ * radiance that the surface term sfc_emis * sfc_src_jac alone produces at every level, i.e.
+ * d gpt_flux_up / d Tsfc in the reference's finite-difference form. */
+int rrtmgp_b200_rte_lw_jac_f32(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1,
+        const float* tau, const float* lay_src, const float* lev_src_inc,
+        const float* lev_src_dec, const float* sfc_src, const float* sfc_src_jac,
+        const float* sfc_emis, const float* inc_flux, int n_gauss_angles, float* gpt_flux_up,
+        float* gpt_flux_dn, float* gpt_flux_up_jac, void* stream);
+int rrtmgp_b200_rte_lw_jac_f64(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1,
+        const double* tau, const double* lay_src, const double* lev_src_inc,
+        const double* lev_src_dec, const double* sfc_src, const double* sfc_src_jac,
+        const double* sfc_emis, const double* inc_flux, int n_gauss_angles, double* gpt_flux_up,
+        double* gpt_flux_dn, double* gpt_flux_up_jac, void* stream);
 
 /* Rte_sw_gpu::rte_sw (include/Rte_sw.h:65-75; src_cuda/Rte_sw.cu:116-161), two-stream +
  * adding (rte_solver_kernels.cu:188-278,535-647; F90 :512-606,996-1228).  mu0 (ncol);

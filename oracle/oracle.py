@@ -224,18 +224,22 @@ def add_to(band_lims, inout: dict, inp: dict):
                          _p(_f(inp["g"])) if two else None, nband, None if bl is None else bl.ctypes.data_as(_I))
 
 
-def rte_lw(band_lims, tau, top_at_1, sources, sfc_emis, inc_flux=None, n_gauss_angles=1):
+def rte_lw(band_lims, tau, top_at_1, sources, sfc_emis, inc_flux=None, n_gauss_angles=1, flux_up_jac=False):
+    """(up, dn), or (up, dn, up_jac) with flux_up_jac (surface-temperature Jacobian from
+    sources["sfc_src_jac"])."""
     bl = np.ascontiguousarray(np.asarray(band_lims, np.int32))
     tau = _f(tau)
     ngpt, nlay, ncol = tau.shape
     up = np.empty((ngpt, nlay + 1, ncol))
     dn = np.empty_like(up)
-    s = {k: _f(v) for k, v in sources.items()}
+    jac = np.empty_like(up) if flux_up_jac else None
+    s = {k: _f(v) for k, v in sources.items() if v is not None}
     _check(load().oracle_rte_lw(ncol, nlay, ngpt, len(bl), bl.ctypes.data_as(_I), int(bool(top_at_1)), _p(tau),
                                 _p(s["lay_src"]), _p(s["lev_src_inc"]), _p(s["lev_src_dec"]), _p(s["sfc_src"]),
                                 _p(_f(sfc_emis)), None if inc_flux is None else _p(_f(inc_flux)),
-                                int(n_gauss_angles), _p(up), _p(dn)))
-    return up, dn
+                                int(n_gauss_angles), _p(up), _p(dn), _p(s["sfc_src_jac"]) if flux_up_jac else None,
+                                _p(jac)))
+    return (up, dn, jac) if flux_up_jac else (up, dn)
 
 
 def rte_sw(band_lims, tau, ssa, g, top_at_1, mu0, inc_flux_dir, sfc_alb_dir, sfc_alb_dif, inc_flux_dif=None):

@@ -42,9 +42,7 @@ struct __align__(16) DRec {
     float4 fmT, fmH, fmO;   // d fminor / dx on the minor corners (lo.x, lo.y, hi.x, hi.y)
     float4 dB;              // LW: dB/dT of the band Planck function at T_lay, T_top, T_bot, T_sfc
                             // SW: d col_rayl / d vmr_h2o in x
-    float dsT[kMaxMinor];   // d ln(scaling_n) / dT (scaling_n: the forward record's scal[n])
-    float dsH[kMaxMinor], dsO[kMaxMinor];   // d scaling_n / d vmr
-};
+};                          // (minor scalings and their derivatives: layer_minor_scalings_d)
 
 __device__ __forceinline__ float dot4(const float4& a, const float4& b)
 {
@@ -137,19 +135,46 @@ __device__ __forceinline__ void build_drec(const KdistView<float>& k, DRec& D, c
     D.fmT = make_float4(fmT[0], fmT[1], fmT[2], fmT[3]);
     D.fmH = make_float4(fmX[0][0], fmX[0][1], fmX[0][2], fmX[0][3]);
     D.fmO = make_float4(fmX[1][0], fmX[1][1], fmX[1][2], fmX[1][3]);
-    // Minor scalings.
-    int n = 0;
-    for (int ii = k.band_minor_begin[a][b]; ii < k.band_minor_begin[a][b + 1] && n < kMaxMinor; ++ii, ++n) {
-        const int im = k.band_minor_list[a][ii];
-        const int flags = k.minor_flags[a][im];
-        const int mg = k.minor_gas[a][im];
+}
+
+// Minor scalings of every scaling kind of layers 0 .. nloc - 1 with their derivatives:
+// sc4[jl * k.max_nscal + sid] = (scaling, d ln(scaling) / dT, d scaling / d vmr_h2o,
+// d scaling / d vmr_o3) (kind_scaling; zero past the layer's atmosphere's kind count).  Threads
+// tid, tid + nthr, ... of the calling team take one (layer, kind) each.
+__device__ __forceinline__ void layer_minor_scalings_d(const KdistView<float>& k, const LayerState* st,
+                                                       const float* cg_all, int cgs, float4* sc4, int nloc,
+                                                       int idx_o3, int cd_internal, int tid, int nthr)
+{
+    const int ns = k.max_nscal;
+    constexpr float m_dry = 0.028964f, m_h2o = 0.018016f;
+    for (int idx = tid; idx < nloc * ns; idx += nthr) {
+        const int jl = idx / ns, sid = idx - jl * ns;
+        const LayerState& s = st[jl];
+        const int a = s.itropo;
+        if (sid >= k.nscal[a]) {
+            sc4[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+            continue;
+        }
+        const float* cg = cg_all + jl;
+        const float cd = cg[0];
+        const float vh = cg[k.idx_h2o * cgs] / cd;
+        const float dcd_h = cd_internal ? -cd * m_h2o / (m_dry + m_h2o * vh) : 0.f;
+        // d col_gas[gi] / d vmr of col_gas index xi (as build_drec)
+        auto dcol = [&](int gi, int xi) -> float {
+            if (xi <= 0) return 0.f;
+            float d = 0.f;
+            if (xi == k.idx_h2o) d = (gi == 0 ? 1.f : cg[gi * cgs] / cd) * dcd_h;
+            if (gi == xi) d += cd;
+            return d;
+        };
+        const int flags = k.scal_flags[a][sid];
+        const int mg = k.scal_gas[a][sid];
         const float colm = cg[mg * cgs];
-        float Dd = 1.f, Q = 1.f, dQh = 0.f, dQo = 0.f;
-        float dsT = 0.f;
+        float Dd = 1.f, Q = 1.f, dQh = 0.f, dQo = 0.f, dsT = 0.f;
         if (flags & 1) {
             Dd = 0.01f * s.p / s.t;
-            dsT = -1.f / s.t;   // d ln(scaling_n) / dT
-            const int sgi = k.minor_sgas[a][im];
+            dsT = -1.f / s.t;
+            const int sgi = k.scal_sgas[a][sid];
             if (sgi > 0) {
                 const float vs = cg[sgi * cgs] / cd;
                 const float q0 = vs / (1.f + vh);
@@ -163,41 +188,40 @@ __device__ __forceinline__ void build_drec(const KdistView<float>& k, DRec& D, c
                 dQo = sign * dqo;
             }
         }
-        D.dsT[n] = dsT;
-        D.dsH[n] = Dd * (Q * dcol(mg, k.idx_h2o) + colm * dQh);
-        D.dsO[n] = Dd * (Q * dcol(mg, idx_o3) + colm * dQo);
+        sc4[idx] = make_float4(kind_scaling(k, a, sid, cg, cgs, s.p, s.t), dsT,
+                               Dd * (Q * dcol(mg, k.idx_h2o) + colm * dQh), Dd * (Q * dcol(mg, idx_o3) + colm * dQo));
     }
 }
 
 // Adjoint of tau_abs for g-point g: accumulates tau_bar * dtau/dx into gT, gH, gO.  c0, c1:
-// the g-point's kmaj4 corners of the record's two rows (loaded by the caller, early).
+// the g-point's kmaj4 corners of the record's two rows (loaded by the caller, early); sc4:
+// the layer's scaling table (layer_minor_scalings_d).
 __device__ __forceinline__ void tau_abs_adjoint(const KdistView<float>& k, const Rec& R, const DRec& D, int g,
                                                 int4 mg, int nmax, float tb, const float4& c0, const float4& c1,
-                                                float& gT, float& gH, float& gO)
+                                                const float4* sc4, float& gT, float& gH, float& gO)
 {
     float dT = dot4(D.wT0, c0) + dot4(D.wT1, c1);
     float dH = dot4(D.wH0, c0) + dot4(D.wH1, c1);
     float dO = dot4(D.wO0, c0) + dot4(D.wO1, c1);
     const float2* kn = k.kmin2[R.a];
+    auto term = [&](int code, bool on) {
+        const int c = code >> kScalBits;
+        const float2 lo = __ldg(kn + (R.kb.z + c));
+        const float2 hi = __ldg(kn + (R.kb.w + c));
+        const float4 cr = make_float4(lo.x, lo.y, hi.x, hi.y);
+        const float M = dot4(R.fm, cr);
+        const float4 S = sc4[code & (kMaxScal - 1)];
+        const float tT = S.x * (S.y * M + dot4(D.fmT, cr));
+        const float tH = S.z * M + S.x * dot4(D.fmH, cr);
+        const float tO = S.w * M + S.x * dot4(D.fmO, cr);
+        dT += on ? tT : 0.f;
+        dH += on ? tH : 0.f;
+        dO += on ? tO : 0.f;
+    };
 #pragma unroll
-    for (int n = 0; n < 3; ++n) {
-        if (n < nmax) {
-            const int code = n == 0 ? mg.y : (n == 1 ? mg.z : mg.w);
-            const int c = code >> 4, sl = code & 15;
-            const float2 lo = __ldg(kn + (R.kb.z + c));
-            const float2 hi = __ldg(kn + (R.kb.w + c));
-            const float4 cr = make_float4(lo.x, lo.y, hi.x, hi.y);
-            const float M = dot4(R.fm, cr);
-            const float sc = R.scal[sl];
-            const float tT = sc * (D.dsT[sl] * M + dot4(D.fmT, cr));
-            const float tH = D.dsH[sl] * M + sc * dot4(D.fmH, cr);
-            const float tO = D.dsO[sl] * M + sc * dot4(D.fmO, cr);
-            const bool on = n < mg.x;
-            dT += on ? tT : 0.f;
-            dH += on ? tH : 0.f;
-            dO += on ? tO : 0.f;
-        }
-    }
+    for (int n = 0; n < 3; ++n)
+        if (n < nmax) term(n == 0 ? mg.y : (n == 1 ? mg.z : mg.w), n < mg.x);
+    for (int n = 3; n < nmax; ++n) term(minor_code_at(k, R.a, mg, g, n), n < mg.x);   // dense layouts
     gT += tb * dT;
     gH += tb * dH;
     gO += tb * dO;

@@ -114,18 +114,19 @@ __device__ __forceinline__ float4 cloud_1scl_partials(const CloudLut<float>& L, 
 }
 
 struct AdjLayout {
-    size_t state, cg, cld, taubar, seeds, levbot, maps, sfc, recs, drecs, total;
+    size_t state, cg, scal, cld, taubar, seeds, levbot, maps, sfc, recs, drecs, total;
 };
 
 // Shared memory of one CTA: LPC local layers (LPC + 1 local levels), maps of all NWt chunks of
 // the column, records of its NWc warps.
 __host__ __device__ __forceinline__ AdjLayout adj_layout(int LPC, int ngas, int nband, int NWc, int NWt, int CL,
-                                                         int mgb, int nbuf)
+                                                         int mgb, int nbuf, int nscal)
 {
     AdjLayout L;
     L.state = 0;
     L.cg = align16(L.state + sizeof(LayerState) * size_t(LPC));
-    L.cld = align16(L.cg + sizeof(float) * size_t(ngas + 1) * LPC);
+    L.scal = align16(L.cg + sizeof(float) * size_t(ngas + 1) * LPC);
+    L.cld = align16(L.scal + sizeof(float4) * size_t(nscal) * LPC);
     L.taubar = align16(L.cld + sizeof(float) * size_t(nband) * LPC);
     L.seeds = align16(L.taubar + sizeof(float) * size_t(nband) * LPC);
     L.levbot = align16(L.seeds + sizeof(float) * size_t(3 * LPC + 2));
@@ -175,9 +176,10 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
     // One-CTA columns double-buffer the chunk maps and the surface source by group parity, so
     // no barrier is needed at the end of a group; clusters (maps of every chunk in every CTA)
     // keep one buffer and that barrier.
-    const AdjLayout SL = adj_layout(LPC, k.ngas, nband, NWc, NWt, CL, mgb, CLUSTER ? 1 : 2);
+    const AdjLayout SL = adj_layout(LPC, k.ngas, nband, NWc, NWt, CL, mgb, CLUSTER ? 1 : 2, k.max_nscal);
     LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
     float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
+    float4* sm_sc4 = reinterpret_cast<float4*>(smem_raw + SL.scal);   // [local layer][scaling kind]
     float* sm_cld = reinterpret_cast<float*>(smem_raw + SL.cld);
     float* sm_tb = reinterpret_cast<float*>(smem_raw + SL.taubar);
     float* sm_a = reinterpret_cast<float*>(smem_raw + SL.seeds);   // pi * seed_up per local level
@@ -223,6 +225,8 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
     }
     if (threadIdx.x < 16) sm_levbot[threadIdx.x] = 0.0;
     __syncthreads();
+    layer_minor_scalings_d(k, st, sm_cg, LPC, sm_sc4, max(0, min(LPC, nlay - j0)), idx_o3, cd_internal, threadIdx.x,
+                           blockDim.x);
     for (int jl = threadIdx.x; jl < LPC; jl += blockDim.x) {
         const int j = j0 + jl;
         float h = 0.f;
@@ -303,7 +307,8 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
             vtau[i] = 0.f; vpf[i] = 0.f; omt[i] = 0.f; sdn[i] = 0.f; sup[i] = 0.f;
             if (j < nlay && gv) {
                 const Rec& R = recs[slot * CL + i];
-                const float tau = tau_abs(k, R, g, R.a ? mg1 : mg0, R.a ? nm1 : nm0) + R.aux.w;
+                const float tau = tau_abs(k, R, g, R.a ? mg1 : mg0, R.a ? nm1 : nm0,
+                                          &sm_sc4[jl * k.max_nscal].x, 4) + R.aux.w;
                 const float4 p0 = __ldg(k.pfrac4 + (R.kb.x + g));
                 const float4 p1 = __ldg(k.pfrac4 + (R.kb.y + g));
                 const float pfrac = dot4(R.wpl0, p0) + dot4(R.wpl1, p1);
@@ -448,7 +453,8 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
                     gTs += Sbar * pf_bottom * DR.dB.w;
                 }
                 float gh = 0.f, go = 0.f;
-                tau_abs_adjoint(k, R, DR, g, R.a ? mg1 : mg0, R.a ? nm1 : nm0, tb, c0, c1, gt, gh, go);
+                tau_abs_adjoint(k, R, DR, g, R.a ? mg1 : mg0, R.a ? nm1 : nm0, tb, c0, c1, sm_sc4 + jl * k.max_nscal,
+                                gt, gh, go);
                 gt += pfb * (dot4(DR.pT0, p0) + dot4(DR.pT1, p1));
                 gh += pfb * (dot4(DR.pH0, p0) + dot4(DR.pH1, p1));
                 go += pfb * (dot4(DR.pO0, p0) + dot4(DR.pO1, p1));
@@ -596,7 +602,7 @@ int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
 {
     const KdistView<float>& v = k->v32;
     const int NW1 = (nlay + CL - 1) / CL;
-    const size_t smem1 = adj_layout(NW1 * CL, v.ngas, v.nband, NW1, NW1, CL, v.max_group_bands, 2).total;
+    const size_t smem1 = adj_layout(NW1 * CL, v.ngas, v.nband, NW1, NW1, CL, v.max_group_bands, 2, v.max_nscal).total;
     RB_CHECK_ARG(CL == 8 || NW1 <= 8, "adjoint_lw: chunk 16 covers at most 128 layers");
     int CS = 1, NWc = NW1;
     size_t smem = smem1;
@@ -605,7 +611,7 @@ int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
         NWc = 16;
         CS = (nlay + 16 * CL - 1) / (16 * CL);
         RB_CHECK_ARG(CS <= 8, "adjoint_lw: at most 1024 layers");
-        smem = adj_layout(16 * CL, v.ngas, v.nband, 16, CS * 16, CL, v.max_group_bands, 1).total;
+        smem = adj_layout(16 * CL, v.ngas, v.nband, 16, CS * 16, CL, v.max_group_bands, 1, v.max_nscal).total;
     }
     if (smem > 227 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_lw: shared memory need exceeds 227 KB");
     static PerDeviceOnce attr;
@@ -668,7 +674,7 @@ int adjoint_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     RB_CHECK_ARG(!c || (lwp && iwp && rel && rei), "adjoint_lw: cloud arrays required with a cloud handle");
     RB_CHECK_ARG(!c || c->nband == k->info.nband, "adjoint_lw: cloud and gas band counts differ");
     const KdistView<float>& v = k->v32;
-    if (!v.minor_in_band || v.max_band_minor > kMaxMinor || v.max_minor_per_g > 3 || v.max_group_bands > 2)
+    if (!fused_layout_ok(v, false, 2))
         return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_lw: k-distribution layout not supported by the adjoint kernel");
     GasSet<float> gs;
     int st = make_gas_set<float>(k, ncol, nlay, gases, ngases, gs);

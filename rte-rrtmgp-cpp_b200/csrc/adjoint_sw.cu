@@ -64,7 +64,8 @@ struct SwAdjOut {
 
 using D4 = Dual<4>;
 
-// Minor-interval code n (contributor << 4 | slot) of a g-point's list (minor_entry).
+// Minor-interval code n < 3 (contributor << kScalBits | scaling kind) of a g-point's list
+// (minor_entry); codes 4, 5, ... come from gx = minor_gx[a] + g * minor_gx_stride.
 __device__ __forceinline__ int minor_code(const int4& mg, int n)
 {
     return n == 0 ? mg.y : (n == 1 ? mg.z : mg.w);
@@ -340,9 +341,10 @@ struct LayerAdj {
 
 __device__ __noinline__ LayerAdj sw_layer_adjoint(const float4* __restrict__ kmaj4, const float2* __restrict__ kmin,
                                                   const float2* __restrict__ krayl2, const Rec* Rc, const DRec* DR,
-                                                  int g, int4 mg, int nmax, float tau, float w0, float omw, float gasy,
-                                                  float mu0, float mu0_inv, float Rb, float Tb, float Rdb, float Tdb,
-                                                  float Tnb, float Afb, float Arb)
+                                                  const float4* sc4, const int* gx, int g, int4 mg, int nmax,
+                                                  float tau, float w0, float omw, float gasy, float mu0, float mu0_inv,
+                                                  float Rb, float Tb, float Rdb, float Tdb, float Tnb, float Afb,
+                                                  float Arb)
 {
     const float4 c0 = __ldg(kmaj4 + (Rc->kb.x + g));
     const float4 c1 = __ldg(kmaj4 + (Rc->kb.y + g));
@@ -351,7 +353,7 @@ __device__ __noinline__ LayerAdj sw_layer_adjoint(const float4* __restrict__ kma
     for (int n = 0; n < 3; ++n) {
         cr[n] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (n < nmax) {
-            const int c = minor_code(mg, n) >> 4;
+            const int c = minor_code(mg, n) >> kScalBits;
             const float2 lo = __ldg(kmin + (Rc->kb.z + c));
             const float2 hi = __ldg(kmin + (Rc->kb.w + c));
             cr[n] = make_float4(lo.x, lo.y, hi.x, hi.y);
@@ -365,20 +367,25 @@ __device__ __noinline__ LayerAdj sw_layer_adjoint(const float4* __restrict__ kma
     float dT = dot4(DR->wT0, c0) + dot4(DR->wT1, c1);
     float dH = dot4(DR->wH0, c0) + dot4(DR->wH1, c1);
     float dO = dot4(DR->wO0, c0) + dot4(DR->wO1, c1);
+    auto minor_term = [&](int code, const float4& crn, bool on) {
+        const float M = dot4(Rc->fm, crn);
+        const float4 S = sc4[code & (kMaxScal - 1)];   // scaling, d ln / dT, d / d h2o, d / d o3
+        const float tT = S.x * (S.y * M + dot4(DR->fmT, crn));
+        const float tH = S.z * M + S.x * dot4(DR->fmH, crn);
+        const float tO = S.w * M + S.x * dot4(DR->fmO, crn);
+        dT += on ? tT : 0.f;
+        dH += on ? tH : 0.f;
+        dO += on ? tO : 0.f;
+    };
 #pragma unroll
-    for (int n = 0; n < 3; ++n) {
-        if (n < nmax) {
-            const int sl = minor_code(mg, n) & 15;
-            const float M = dot4(Rc->fm, cr[n]);
-            const float sc = Rc->scal[sl];
-            const float tT = sc * (DR->dsT[sl] * M + dot4(DR->fmT, cr[n]));
-            const float tH = DR->dsH[sl] * M + sc * dot4(DR->fmH, cr[n]);
-            const float tO = DR->dsO[sl] * M + sc * dot4(DR->fmO, cr[n]);
-            const bool on = n < mg.x;
-            dT += on ? tT : 0.f;
-            dH += on ? tH : 0.f;
-            dO += on ? tO : 0.f;
-        }
+    for (int n = 0; n < 3; ++n)
+        if (n < nmax) minor_term(minor_code(mg, n), cr[n], n < mg.x);
+    for (int n = 3; n < nmax; ++n) {   // dense layouts: more than three intervals over g
+        const int code = n < mg.x ? gx[n - 3] : mg.y;
+        const int c = code >> kScalBits;
+        const float2 lo = __ldg(kmin + (Rc->kb.z + c));
+        const float2 hi = __ldg(kmin + (Rc->kb.w + c));
+        minor_term(code, make_float4(lo.x, lo.y, hi.x, hi.y), n < mg.x);
     }
     const float tab = la.ta, trb = la.tr;
     LayerAdj r{tab * dT, tab * dH, tab * dO, la.tc, la.tsc, la.tsg};
@@ -395,23 +402,24 @@ __device__ __noinline__ LayerAdj sw_layer_adjoint(const float4* __restrict__ kma
 struct LayerFwd { float tau, w0, omw, gasy, R, T, Rdir, Tdir, Tn, adif, adir; };
 
 __device__ __noinline__ LayerFwd sw_layer_forward(const float4* __restrict__ kmaj4, const float2* __restrict__ kmin,
-                                                  const float2* __restrict__ krayl2, const Rec* Rc, int g, int4 mg,
-                                                  int nmax, float mu0, float mu0_inv)
+                                                  const float2* __restrict__ krayl2, const Rec* Rc, const float4* sc4,
+                                                  const int* gx, int g, int4 mg, int nmax, float mu0, float mu0_inv)
 {
     const float4 c0 = __ldg(kmaj4 + (Rc->kb.x + g));
     const float4 c1 = __ldg(kmaj4 + (Rc->kb.y + g));
     float ta = dot4(Rc->wmaj0, c0) + dot4(Rc->wmaj1, c1);
+    auto minor_term = [&](int code, bool on) {
+        const int c = code >> kScalBits;
+        const float2 lo = __ldg(kmin + (Rc->kb.z + c));
+        const float2 hi = __ldg(kmin + (Rc->kb.w + c));
+        const float t = sc4[code & (kMaxScal - 1)].x *
+                        (Rc->fm.x * lo.x + Rc->fm.y * lo.y + Rc->fm.z * hi.x + Rc->fm.w * hi.y);
+        ta += on ? t : 0.f;
+    };
 #pragma unroll
-    for (int n = 0; n < 3; ++n) {
-        if (n < nmax) {
-            const int code = n == 0 ? mg.y : (n == 1 ? mg.z : mg.w);
-            const int c = code >> 4;
-            const float2 lo = __ldg(kmin + (Rc->kb.z + c));
-            const float2 hi = __ldg(kmin + (Rc->kb.w + c));
-            const float t = Rc->scal[code & 15] * (Rc->fm.x * lo.x + Rc->fm.y * lo.y + Rc->fm.z * hi.x + Rc->fm.w * hi.y);
-            ta += (n < mg.x) ? t : 0.f;
-        }
-    }
+    for (int n = 0; n < 3; ++n)
+        if (n < nmax) minor_term(minor_code(mg, n), n < mg.x);
+    for (int n = 3; n < nmax; ++n) minor_term(n < mg.x ? gx[n - 3] : mg.y, n < mg.x);   // dense layouts
     LayerFwd o;
     const float2 r0 = __ldg(krayl2 + (Rc->kr[0] + g));
     const float2 r1 = __ldg(krayl2 + (Rc->kr[1] + g));
@@ -483,16 +491,17 @@ __device__ __forceinline__ void cloud_sw_dual(const CloudLut<float>& L, int delt
 }
 
 struct SwAdjLayout {
-    size_t state, cg, seeds, clsum, albacc, x1, x2, x3, x4, x5, recs, drecs, total;
+    size_t state, cg, scal, seeds, clsum, albacc, x1, x2, x3, x4, x5, recs, drecs, total;
 };
 
 __host__ __device__ __forceinline__ SwAdjLayout sw_adj_layout(int ngas, int nband, int mgb, int CS, int WPC,
-                                                              int nbuf)
+                                                              int nbuf, int nscal)
 {
     SwAdjLayout L;
     L.state = 0;
     L.cg = align16(L.state + sizeof(LayerState) * kLPC);
-    L.seeds = align16(L.cg + sizeof(float) * size_t(ngas + 1) * kLPC);
+    L.scal = align16(L.cg + sizeof(float) * size_t(ngas + 1) * kLPC);
+    L.seeds = align16(L.scal + sizeof(float4) * size_t(nscal) * kLPC);
     L.clsum = align16(L.seeds + sizeof(float) * (4 * (kLPC + 1)));
     L.albacc = align16(L.clsum + sizeof(float) * size_t(nband) * kLPC * 3);
     L.x1 = align16(L.albacc + sizeof(double) * size_t(nband) * 2);
@@ -537,9 +546,10 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
     const int L_end = NWt * CL;
     const int j0 = rank * kLPC;          // first global layer of this CTA
     const int nband = k.nband, mgb = k.max_group_bands;
-    const SwAdjLayout SL = sw_adj_layout(k.ngas, nband, mgb, CS, WPC, PAIR ? 2 : 1);
+    const SwAdjLayout SL = sw_adj_layout(k.ngas, nband, mgb, CS, WPC, PAIR ? 2 : 1, k.max_nscal);
     LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
     float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
+    float4* sm_sc4 = reinterpret_cast<float4*>(smem_raw + SL.scal);   // [local layer][scaling kind]
     float* sm_al = reinterpret_cast<float*>(smem_raw + SL.seeds);   // seed F_up per local level (0..64)
     float* sm_be = sm_al + (kLPC + 1);                                // seed F_dn
     float* sm_ga = sm_be + (kLPC + 1);                                // seed F_dir
@@ -591,6 +601,8 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
     for (int i = threadIdx.x; i < nband * kLPC * 3; i += blockDim.x) sm_cl[i] = 0.f;
     for (int i = threadIdx.x; i < nband * 2; i += blockDim.x) sm_alb[i] = 0.0;
     __syncthreads();
+    layer_minor_scalings_d(k, st, sm_cg, kLPC, sm_sc4, max(0, min(kLPC, nlay - j0)), idx_o3, cd_internal, threadIdx.x,
+                           blockDim.x);
     for (int jl = threadIdx.x; jl < kLPC; jl += blockDim.x) {
         const int j = j0 + jl;
         float h = 0.f;
@@ -670,8 +682,9 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
             float tau = 0.f, w0 = 0.f, omw = 1.f, gasy = 0.f;
             if (j < nlay && gv) {
                 const Rec& Rc = recs[slot * CL + i];
-                const LayerFwd lf = sw_layer_forward(k.kmaj4, k.kmin2[Rc.a], k.krayl2, &Rc, g, Rc.a ? mg1 : mg0,
-                                                     Rc.a ? nm1 : nm0, mu0, mu0_inv);
+                const LayerFwd lf = sw_layer_forward(k.kmaj4, k.kmin2[Rc.a], k.krayl2, &Rc, sm_sc4 + jl * k.max_nscal,
+                                                     k.minor_gx[Rc.a] + size_t(g) * k.minor_gx_stride, g,
+                                                     Rc.a ? mg1 : mg0, Rc.a ? nm1 : nm0, mu0, mu0_inv);
                 tau = lf.tau; w0 = lf.w0; omw = lf.omw; gasy = lf.gasy;
                 R = lf.R; T = lf.T; Rdir = lf.Rdir; Tdir = lf.Tdir; Tn = lf.Tn; adif = lf.adif; adir = lf.adir;
             }
@@ -933,7 +946,9 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
             gT[i] = 0.f; gH[i] = 0.f; gO[i] = 0.f; gC0[i] = 0.f; gC1[i] = 0.f; gC2[i] = 0.f;
             if (j < nlay && gv) {
                 const Rec& Rc = recs[slot * CL + i];
-                const LayerAdj la = sw_layer_adjoint(k.kmaj4, k.kmin2[Rc.a], k.krayl2, &Rc, &drecs[slot * CL + i], g,
+                const LayerAdj la = sw_layer_adjoint(k.kmaj4, k.kmin2[Rc.a], k.krayl2, &Rc, &drecs[slot * CL + i],
+                                                     sm_sc4 + jl * k.max_nscal,
+                                                     k.minor_gx[Rc.a] + size_t(g) * k.minor_gx_stride, g,
                                                      Rc.a ? mg1 : mg0, Rc.a ? nm1 : nm0, vTau[i], vW0[i], vOmw[i],
                                                      vG[i], mu0, mu0_inv, vRb[i], vTb[i], Rdb, Tdb, Tnb, vAfb[i], Arb);
                 gT[i] = la.t; gH[i] = la.h; gO[i] = la.o;
@@ -1086,8 +1101,7 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     RB_CHECK_ARG(!c || (lwp && iwp && rel && rei), "adjoint_sw: cloud arrays required with a cloud handle");
     RB_CHECK_ARG(!c || c->nband == k->info.nband, "adjoint_sw: cloud and gas band counts differ");
     const KdistView<float>& v = k->v32;
-    if (!v.minor_in_band || v.max_band_minor > kMaxMinor || v.max_minor_per_g > 3 || v.max_group_bands > 2 ||
-        !v.krayl2)
+    if (!fused_layout_ok(v, true, 2))
         return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_sw: k-distribution layout not supported by the adjoint kernel");
     const int CS = (nlay + kLPC - 1) / kLPC;
     RB_CHECK_ARG(CS <= 8, "adjoint_sw: nlay too large (at most 512 layers)");
@@ -1099,9 +1113,10 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
         if (k->gas_names[i] == "o3") idx_o3 = int(i) + 1;
     constexpr int CL = kSwAdjointChunk;
     // two record buffers (records of two groups built at once) when they fit
-    const size_t smem2 = sw_adj_layout(v.ngas, v.nband, v.max_group_bands, CS, kLPC / CL, 2).total;
+    const size_t smem2 = sw_adj_layout(v.ngas, v.nband, v.max_group_bands, CS, kLPC / CL, 2, v.max_nscal).total;
     const bool pair = smem2 <= 227 * 1024;
-    const size_t smem = pair ? smem2 : sw_adj_layout(v.ngas, v.nband, v.max_group_bands, CS, kLPC / CL, 1).total;
+    const size_t smem =
+        pair ? smem2 : sw_adj_layout(v.ngas, v.nband, v.max_group_bands, CS, kLPC / CL, 1, v.max_nscal).total;
     if (smem > 227 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_sw: shared memory need exceeds 227 KB");
     static PerDeviceOnce attr;
     const int ast = attr.run([] {

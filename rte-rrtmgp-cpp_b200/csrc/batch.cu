@@ -215,11 +215,7 @@ int forward_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
 
 namespace {
 
-bool fused_layout_ok(const KdistView<float>& v, bool sw)
-{
-    return v.minor_in_band && v.max_band_minor <= kMaxMinor && v.max_minor_per_g <= 3 && v.max_group_bands <= 8 &&
-           (!sw || v.krayl2);
-}
+bool batch_layout_ok(const KdistView<float>& v, bool sw) { return fused_layout_ok(v, sw, 8); }
 
 }  // namespace
 }  // namespace rrtmgp_b200
@@ -260,9 +256,9 @@ size_t team_smem_bytes(const rrtmgp_b200_batch_t* b, int domain, int nlay, int c
 {
     const KdistView<float>& v = b->k[domain]->v32;
     const int W = ceil_div_i(nlay, cl);
-    const SmemLayout L = domain == 0 ? smem_layout(nlay, v.ngas, v.nband, 1, W, 2, cl, v.max_group_bands)
+    const SmemLayout L = domain == 0 ? smem_layout(nlay, v.ngas, v.nband, 1, W, 2, cl, v.max_group_bands, v.max_nscal)
                                      : smem_layout(nlay, v.ngas, v.nband, 0, W, 3, cl,
-                                                   v.max_group_bands * (cl == 8 ? 2 : 1));
+                                                   v.max_group_bands * (cl == 8 ? 2 : 1), v.max_nscal);
     return align16(L.total);
 }
 
@@ -428,7 +424,7 @@ int batch_create(rrtmgp_b200_kdist klw, rrtmgp_b200_cloud clw, rrtmgp_b200_kdist
     RB_CHECK_ARG(!ksw || !ksw->info.is_longwave, "batch_create: k_sw is not a shortwave k-distribution");
     RB_CHECK_ARG(!clw || (klw && clw->nband == klw->info.nband), "batch_create: longwave cloud bands differ");
     RB_CHECK_ARG(!csw || (ksw && csw->nband == ksw->info.nband), "batch_create: shortwave cloud bands differ");
-    if ((klw && !fused_layout_ok(klw->v32, false)) || (ksw && !fused_layout_ok(ksw->v32, true)))
+    if ((klw && !batch_layout_ok(klw->v32, false)) || (ksw && !batch_layout_ok(ksw->v32, true)))
         return fail(RRTMGP_B200_ERR_UNSUPPORTED, "batch_create: k-distribution layout not supported");
     std::unique_ptr<rrtmgp_b200_batch_t> b(new rrtmgp_b200_batch_t);
     b->k[0] = klw;

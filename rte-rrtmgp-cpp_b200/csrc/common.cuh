@@ -113,16 +113,33 @@ struct KdistView {
     //   kmaj4/pfrac4 [t][p][eta][g], p < npres, eta < neta-1: (k(e,p), k(e+1,p), k(e,p+1), k(e+1,p+1))
     //   kmin2[a]     [t][eta][c], eta < neta-1: (k(e), k(e+1))
     //   krayl2       [a][t][eta][g], eta < neta-1: (k(e), k(e+1))
-    //   minor_g[a]   [g]: x = number of intervals covering g (<= 3), y/z/w = (c << 4) | slot,
-    //                slot = position of the interval in its band's list, c = contributor;
-    //                unused slots repeat y (0 when no interval covers g).
+    //   minor_g[a]   [g]: x = number of intervals covering g, y/z/w = the first three codes
+    //                (c << kScalBits) | sid, c = contributor, sid = scaling kind of the
+    //                interval (below); unused slots repeat y (0 when no interval covers g).
+    //   minor_gx[a]  [g][minor_gx_stride]: codes 4, 5, ... of g (NULL when no g-point has
+    //                more than three intervals).
     const float4* kmaj4;
     const float4* pfrac4;
     const float2* kmin2[2];
     const float2* krayl2;
     const int4* minor_g[2];
-    int max_minor_per_g;            // most intervals covering one g-point (fused kernels: <= 3)
+    const int* minor_gx[2];
+    int minor_gx_stride;
+    int max_minor_per_g;            // most intervals covering one g-point
+    // Scaling kinds: intervals whose scaling (gas_optical_depths_minor_kernel,
+    // gas_optics_rrtmgp_kernels.cu:396-417) is the same function of the layer -- same minor
+    // gas, and with density scaling the same scaling gas and complement flag -- share one
+    // kind, so the fused kernels evaluate each kind once per layer instead of once per
+    // (layer, interval).  scal_gas/sgas/flags [a][sid] as minor_gas/sgas/flags.
+    int nscal[2];
+    int max_nscal;                  // max(nscal[0], nscal[1], 1)
+    const int* scal_gas[2];
+    const int* scal_sgas[2];
+    const int* scal_flags[2];
 };
+
+constexpr int kScalBits = 6;                    // bits of a scaling kind in a minor code
+constexpr int kMaxScal = 1 << kScalBits;        // scaling kinds per atmosphere (fused kernels)
 
 }  // namespace rrtmgp_b200
 

@@ -22,7 +22,8 @@ int launch_lw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
     const KdistView<float>& v = k->v32;
     const int NW = (nlay + CL - 1) / CL;
     RB_CHECK_ARG(NW <= 16, "forward_lw: nlay too large for the fused kernel (at most 16 chunks)");
-    const size_t smem = smem_layout(nlay, v.ngas, v.nband, 1, NW, 2, CL, v.max_group_bands * (CL == 8 ? 2 : 1)).total;
+    const size_t smem =
+        smem_layout(nlay, v.ngas, v.nband, 1, NW, 2, CL, v.max_group_bands * (CL == 8 ? 2 : 1), v.max_nscal).total;
     if (smem > 220 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "forward_lw: shared memory need exceeds 220 KB");
     static PerDeviceOnce attr;
     int st = attr.run([] { return cudaFuncSetAttribute(lw_forward_kernel<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -57,7 +58,7 @@ int forward_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     RB_CHECK_ARG(!c || (lwp && iwp && rel && rei), "forward_lw: cloud arrays required with a cloud handle");
     RB_CHECK_ARG(!c || c->nband == k->info.nband, "forward_lw: cloud and gas band counts differ");
     const KdistView<float>& v = k->v32;
-    if (!v.minor_in_band || v.max_band_minor > kMaxMinor || v.max_minor_per_g > 3 || v.max_group_bands > 8)
+    if (!fused_layout_ok(v, false, 8))
         return fail(RRTMGP_B200_ERR_UNSUPPORTED, "forward_lw: k-distribution layout not supported by the fused kernel");
     GasSet<float> gs;
     int st = make_gas_set<float>(k, ncol, nlay, gases, ngases, gs);

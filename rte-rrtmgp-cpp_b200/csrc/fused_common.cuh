@@ -18,8 +18,6 @@
 namespace rrtmgp_b200 {
 namespace fused {
 
-constexpr int kMaxMinor = 8;   // minor intervals per (band, atmosphere) held in a record
-
 // Per-layer state kept in shared memory for the whole kernel (layers counted from the top).
 struct __align__(16) LayerState {
     int jt, jp, itropo, pad;
@@ -36,7 +34,6 @@ struct __align__(16) Rec {
     float4 fm;             // fminor (minor and Rayleigh weights)
     float4 aux;            // LW: pl_lay, pl_top, pl_bot, tau_cloud
                            // SW: col_dry + col_h2o (Rayleigh), cloud tau, ssa, g
-    float scal[kMaxMinor]; // minor scaling of each interval in the band's list
     float aux2;            // LW: surface Planck function (bottom layer only)
                            // SW: cloud absorption optical depth tau_c * (1 - ssa_c)
     int a;                 // 0 lower / 1 upper atmosphere
@@ -81,16 +78,10 @@ __device__ __forceinline__ float warp_sum(float x)
 }
 
 // Interpolation part of a record (interpolation_kernel, gas_optics_rrtmgp_kernels.cu:256-291)
-// for band b at layer state s; the minor scaling of interval n of the band's list goes to
-// scal_out(n, value) (R.scal[n] by default).
-struct RecScal {
-    Rec& R;
-    __device__ __forceinline__ void operator()(int n, float v) const { R.scal[n] = v; }
-};
-
-template <class ScalOut>
+// for band b at layer state s.  The minor scalings are per layer, not per record
+// (layer_minor_scalings).
 __device__ __forceinline__ void record_weights(const KdistView<float>& k, Rec& R, const LayerState& s,
-                                               const float* cg, int cgs, int b, const ScalOut& scal_out)
+                                               const float* cg, int cgs, int b)
 {
     LayerInterp<float> li;
     li.jt = s.jt;
@@ -118,22 +109,57 @@ __device__ __forceinline__ void record_weights(const KdistView<float>& k, Rec& R
     R.a = a;
     R.kr[0] = ((a * k.ntemp + li.jt - 1) * ne1 + (fw.j0 - 1)) * k.ngpt;
     R.kr[1] = ((a * k.ntemp + li.jt) * ne1 + (fw.j1 - 1)) * k.ngpt;
-    int n = 0;
-    for (int ii = k.band_minor_begin[a][b]; ii < k.band_minor_begin[a][b + 1] && n < kMaxMinor; ++ii, ++n)
-        scal_out(n, minor_scaling(k, a, k.band_minor_list[a][ii], cg, cgs, s.p, s.t));
 }
 
-__device__ __forceinline__ void record_weights(const KdistView<float>& k, Rec& R, const LayerState& s,
-                                               const float* cg, int cgs, int b)
+// Minor scaling of scaling kind sid of atmosphere a at a layer (minor_scaling: the same
+// arithmetic, gas_optical_depths_minor_kernel :396-417).
+__device__ __forceinline__ float kind_scaling(const KdistView<float>& k, int a, int sid, const float* cg, int cgs,
+                                              float p, float t)
 {
-    record_weights(k, R, s, cg, cgs, b, RecScal{R});
+    const int flags = k.scal_flags[a][sid];
+    float scaling = cg[k.scal_gas[a][sid] * cgs];
+    if (flags & 1) {
+        scaling *= 0.01f * p / t;
+        const int sg = k.scal_sgas[a][sid];
+        if (sg > 0) {
+            const float vmr_fact = 1.f / cg[0];
+            const float dry_fact = 1.f / (1.f + cg[k.idx_h2o * cgs] * vmr_fact);
+            if (flags & 2) scaling *= (1.f - cg[sg * cgs] * vmr_fact * dry_fact);
+            else scaling *= cg[sg * cgs] * vmr_fact * dry_fact;
+        }
+    }
+    return scaling;
+}
+
+// Scalings of every kind of layers 0 .. nloc - 1 (layer state st[], gas columns cg with
+// stride cgs) into sc[jl * k.max_nscal + sid]; threads tid, tid + nthr, ... of the calling
+// team take one (layer, kind) each.  Kinds past the layer's atmosphere's count are set to 0.
+__device__ __forceinline__ void layer_minor_scalings(const KdistView<float>& k, const LayerState* st, const float* cg,
+                                                     int cgs, float* sc, int nloc, int tid, int nthr)
+{
+    const int ns = k.max_nscal;
+    for (int idx = tid; idx < nloc * ns; idx += nthr) {
+        const int jl = idx / ns, sid = idx - jl * ns;
+        const LayerState& s = st[jl];
+        sc[idx] = sid < k.nscal[s.itropo] ? kind_scaling(k, s.itropo, sid, cg + jl, cgs, s.p, s.t) : 0.f;
+    }
+}
+
+// Code n of g-point g's minor-interval list (minor_g / minor_gx; n < count, or a code that
+// repeats the first one for n < 3).
+__device__ __forceinline__ int minor_code_at(const KdistView<float>& k, int a, const int4& mg, int g, int n)
+{
+    if (n < 3) return n == 0 ? mg.y : (n == 1 ? mg.z : mg.w);
+    return n < mg.x ? __ldg(k.minor_gx[a] + size_t(g) * k.minor_gx_stride + (n - 3)) : mg.y;
 }
 
 // Absorption optical depth of g-point g from a record: major (8 corners via two float4 loads)
 // plus the minor intervals covering g (minor_g list), as gas_optical_depths_major/minor.
 // nmax = most intervals over the warp's lanes (warp-uniform loop bound); lanes with fewer
 // intervals read a valid entry and discard it with a select, so the loop does not diverge.
-__device__ __forceinline__ float tau_abs(const KdistView<float>& k, const Rec& R, int g, int4 mg, int nmax)
+// sc: the layer's scalings, kind sid at sc[sid * sst].
+__device__ __forceinline__ float tau_abs(const KdistView<float>& k, const Rec& R, int g, int4 mg, int nmax,
+                                         const float* sc, int sst = 1)
 {
     const float4 c0 = __ldg(k.kmaj4 + (R.kb.x + g));
     const float4 c1 = __ldg(k.kmaj4 + (R.kb.y + g));
@@ -144,12 +170,22 @@ __device__ __forceinline__ float tau_abs(const KdistView<float>& k, const Rec& R
     for (int n = 0; n < 3; ++n) {
         if (n < nmax) {
             const int code = n == 0 ? mg.y : (n == 1 ? mg.z : mg.w);
-            const int c = code >> 4;
+            const int c = code >> kScalBits;
             const float2 lo = __ldg(kn + (R.kb.z + c));
             const float2 hi = __ldg(kn + (R.kb.w + c));
-            const float t = R.scal[code & 15] * (R.fm.x * lo.x + R.fm.y * lo.y + R.fm.z * hi.x + R.fm.w * hi.y);
+            const float t = sc[(code & (kMaxScal - 1)) * sst] *
+                            (R.fm.x * lo.x + R.fm.y * lo.y + R.fm.z * hi.x + R.fm.w * hi.y);
             tau += (n < mg.x) ? t : 0.f;
         }
+    }
+    for (int n = 3; n < nmax; ++n) {   // dense layouts: more than three intervals over g
+        const int code = minor_code_at(k, R.a, mg, g, n);
+        const int c = code >> kScalBits;
+        const float2 lo = __ldg(kn + (R.kb.z + c));
+        const float2 hi = __ldg(kn + (R.kb.w + c));
+        const float t = sc[(code & (kMaxScal - 1)) * sst] *
+                        (R.fm.x * lo.x + R.fm.y * lo.y + R.fm.z * hi.x + R.fm.w * hi.y);
+        tau += (n < mg.x) ? t : 0.f;
     }
     return tau;
 }
@@ -228,20 +264,31 @@ __device__ __forceinline__ void setup_layers(const KdistView<float>& k, const Ga
                       nthr);
 }
 
+// Table layouts the corner-packed FP32 kernels take: minor intervals inside one band (their
+// interpolation weights are the band's), at most kMaxScal scaling kinds per atmosphere, and
+// a group of 32 g-points touching at most max_bands bands.  Any number of minor intervals per
+// band or per g-point is accepted.
+inline bool fused_layout_ok(const KdistView<float>& v, bool sw, int max_bands)
+{
+    return v.kmaj4 && v.minor_in_band && v.nscal[0] <= kMaxScal && v.nscal[1] <= kMaxScal &&
+           v.max_group_bands <= max_bands && (sw ? v.krayl2 != nullptr : v.pfrac4 != nullptr);
+}
+
 // Shared-memory offsets (bytes) of the fused kernels, all 16-byte aligned.
 struct SmemLayout {
-    size_t state, cg, cloud, maps, sfc, recs, total;
+    size_t state, cg, scal, cloud, maps, sfc, recs, total;
 };
 
 __host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
 __host__ __device__ __forceinline__ SmemLayout smem_layout(int nlay, int ngas, int nband, int ncloud_vals, int NW,
-                                                           int nmaps, int CL, int nbands_per_group)
+                                                           int nmaps, int CL, int nbands_per_group, int nscal)
 {
     SmemLayout L;
     L.state = 0;
     L.cg = align16(L.state + sizeof(LayerState) * size_t(nlay));
-    L.cloud = align16(L.cg + sizeof(float) * size_t(ngas + 1) * nlay);
+    L.scal = align16(L.cg + sizeof(float) * size_t(ngas + 1) * nlay);
+    L.cloud = align16(L.scal + sizeof(float) * size_t(nscal) * nlay);
     L.maps = align16(L.cloud + sizeof(float) * size_t(ncloud_vals) * nband * nlay);
     L.sfc = align16(L.maps + sizeof(float4) * size_t(NW) * 32 * nmaps);
     L.recs = align16(L.sfc + sizeof(float) * 64);

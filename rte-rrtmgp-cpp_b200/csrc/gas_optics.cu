@@ -137,50 +137,19 @@ gas_optics_sw_kernel(const KdistView<T> k, const GasSet<T> gases, int ncol, int 
 // major interpolation is two 16-byte loads instead of eight 4-byte ones (the Planck fraction
 // likewise), each minor interval one 8-byte pair per eta corner, and the sum over minor
 // intervals stays in registers instead of a shared-memory accumulator.  The per-band weights
-// are the records of the fused kernels (fused::record_weights) held in registers, except the
-// minor scalings, which are indexed per g-point and so sit in shared memory, one column of
-// kMaxMinor values per thread (stride kThreads: no bank conflicts).
+// are the records of the fused kernels (fused::record_weights) held in registers.  The minor
+// scalings are computed once per (column, layer) for every scaling kind (not per band) and
+// are indexed per g-point, so they sit in shared memory, one column of max_nscal values per
+// thread (stride kThreads: no bank conflicts).
 // Usable when the tables satisfy the fused kernels' layout conditions (packed_tables_ok).
-__host__ __device__ inline size_t packed_smem_bytes(int ngas)
+__host__ __device__ inline size_t packed_smem_bytes(int ngas, int nscal)
 {
-    return sizeof(float) * size_t(ngas + 1 + fused::kMaxMinor) * kThreads;
+    return sizeof(float) * size_t(ngas + 1 + nscal) * kThreads;
 }
-
-struct ScalColumn {
-    float* p;
-    __device__ __forceinline__ void operator()(int n, float v) const { p[n * kThreads] = v; }
-};
 
 inline bool packed_tables_ok(const KdistView<float>& v, bool lw)
 {
-    return v.minor_in_band && v.max_band_minor <= fused::kMaxMinor && v.max_minor_per_g <= 3 && v.kmaj4 &&
-           v.minor_g[0] && v.minor_g[1] && (lw ? v.pfrac4 != nullptr : v.krayl2 != nullptr);
-}
-
-// Absorption optical depth of g-point g (major + minor intervals of g), as fused::tau_abs with
-// the minor scalings read from the thread's shared column scal[n * kThreads].
-// g is the same for every thread of a warp, so nmax = max(mg0.x, mg1.x) is warp-uniform.
-__device__ __forceinline__ float tau_abs_packed(const KdistView<float>& k, const fused::Rec& R,
-                                                const float* scal, int g, int4 mg, int nmax)
-{
-    const float4 c0 = __ldg(k.kmaj4 + (R.kb.x + g));
-    const float4 c1 = __ldg(k.kmaj4 + (R.kb.y + g));
-    float tau = R.wmaj0.x * c0.x + R.wmaj0.y * c0.y + R.wmaj0.z * c0.z + R.wmaj0.w * c0.w +
-                R.wmaj1.x * c1.x + R.wmaj1.y * c1.y + R.wmaj1.z * c1.z + R.wmaj1.w * c1.w;
-    const float2* kn = k.kmin2[R.a];
-#pragma unroll
-    for (int n = 0; n < 3; ++n) {
-        if (n < nmax) {
-            const int code = n == 0 ? mg.y : (n == 1 ? mg.z : mg.w);
-            const int c = code >> 4;
-            const float2 lo = __ldg(kn + (R.kb.z + c));
-            const float2 hi = __ldg(kn + (R.kb.w + c));
-            const float t = scal[(code & 15) * kThreads] *
-                            (R.fm.x * lo.x + R.fm.y * lo.y + R.fm.z * hi.x + R.fm.w * hi.y);
-            tau += (n < mg.x) ? t : 0.f;
-        }
-    }
-    return tau;
+    return fused::fused_layout_ok(v, !lw, 1 << 30) && v.minor_g[0] && v.minor_g[1];
 }
 
 // minor_g row of g-point g (unused slots already repeat the first one), zeros past the end.
@@ -215,7 +184,7 @@ gas_optics_lw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int tid = threadIdx.x + threadIdx.y * kBX;
     float* cg = reinterpret_cast<float*>(smem_raw) + tid;                       // [ngas + 1]
-    float* scal = reinterpret_cast<float*>(smem_raw) + (k.ngas + 1) * kThreads + tid;   // [kMaxMinor]
+    float* scal = reinterpret_cast<float*>(smem_raw) + (k.ngas + 1) * kThreads + tid;   // [max_nscal]
 
     const int icol = blockIdx.x * kBX + threadIdx.x;
     const int ilay = blockIdx.y * kBY + threadIdx.y;
@@ -226,6 +195,8 @@ gas_optics_lw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
     const float p = play[cl], t = tlay[cl];
     fill_col_gas(k, gases, ncol, nlay, icol, ilay, plev, col_dry_in, cg, kThreads);
     const fused::LayerState s = thread_layer_state(layer_interp(k, p, t), p, t);
+    for (int sid = 0; sid < k.nscal[s.itropo]; ++sid)
+        scal[sid * kThreads] = fused::kind_scaling(k, s.itropo, sid, cg, kThreads, p, t);
 
     const int sfc_lay = play[icol] > play[icol + size_t(nlay - 1) * ncol] ? 0 : nlay - 1;
     const bool at_sfc = ilay == sfc_lay;
@@ -239,7 +210,7 @@ gas_optics_lw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
     for (int b = 0; b < k.nband; ++b) {
         const int g0 = k.band_lims[2 * b], g1 = k.band_lims[2 * b + 1];
         fused::Rec R;
-        fused::record_weights(k, R, s, cg, kThreads, b, ScalColumn{scal});
+        fused::record_weights(k, R, s, cg, kThreads, b);
         const float4 wp0 = R.wpl0, wp1 = R.wpl1;
 
         const float* tp = k.totplnk + size_t(b) * k.nplanck;
@@ -255,7 +226,7 @@ gas_optics_lw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
             const int4 mg0 = nx0, mg1 = nx1;
             nx0 = next_minor_row(k.minor_g[0], g + 1, k.ngpt);
             nx1 = next_minor_row(k.minor_g[1], g + 1, k.ngpt);
-            const float ta = tau_abs_packed(k, R, scal, g, R.a ? mg1 : mg0, max(mg0.x, mg1.x));
+            const float ta = fused::tau_abs(k, R, g, R.a ? mg1 : mg0, max(mg0.x, mg1.x), scal, kThreads);
             const float4 p0 = __ldg(k.pfrac4 + (R.kb.x + g));
             const float4 p1 = __ldg(k.pfrac4 + (R.kb.y + g));
             const float pfrac = (wp0.x * p0.x + wp0.y * p0.y + wp0.z * p0.z + wp0.w * p0.w) +
@@ -282,7 +253,7 @@ gas_optics_sw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int tid = threadIdx.x + threadIdx.y * kBX;
     float* cg = reinterpret_cast<float*>(smem_raw) + tid;                       // [ngas + 1]
-    float* scal = reinterpret_cast<float*>(smem_raw) + (k.ngas + 1) * kThreads + tid;   // [kMaxMinor]
+    float* scal = reinterpret_cast<float*>(smem_raw) + (k.ngas + 1) * kThreads + tid;   // [max_nscal]
 
     const int icol = blockIdx.x * kBX + threadIdx.x;
     const int ilay = blockIdx.y * kBY + threadIdx.y;
@@ -293,6 +264,8 @@ gas_optics_sw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
     const float p = play[cl], t = tlay[cl];
     fill_col_gas(k, gases, ncol, nlay, icol, ilay, plev, col_dry_in, cg, kThreads);
     const fused::LayerState s = thread_layer_state(layer_interp(k, p, t), p, t);
+    for (int sid = 0; sid < k.nscal[s.itropo]; ++sid)
+        scal[sid * kThreads] = fused::kind_scaling(k, s.itropo, sid, cg, kThreads, p, t);
     const float col_rayl = cg[k.idx_h2o * kThreads] + cg[0];
     const float two_tmin = 2.f * FLT_MIN;
 
@@ -300,13 +273,13 @@ gas_optics_sw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
     for (int b = 0; b < k.nband; ++b) {
         const int g0 = k.band_lims[2 * b], g1 = k.band_lims[2 * b + 1];
         fused::Rec R;
-        fused::record_weights(k, R, s, cg, kThreads, b, ScalColumn{scal});
+        fused::record_weights(k, R, s, cg, kThreads, b);
         const int kr0 = R.kr[0], kr1 = R.kr[1];
         for (int g = g0; g < g1; ++g) {
             const int4 mg0 = nx0, mg1 = nx1;
             nx0 = next_minor_row(k.minor_g[0], g + 1, k.ngpt);
             nx1 = next_minor_row(k.minor_g[1], g + 1, k.ngpt);
-            const float ta = tau_abs_packed(k, R, scal, g, R.a ? mg1 : mg0, max(mg0.x, mg1.x));
+            const float ta = fused::tau_abs(k, R, g, R.a ? mg1 : mg0, max(mg0.x, mg1.x), scal, kThreads);
             const float2 r0 = __ldg(k.krayl2 + (kr0 + g));
             const float2 r1 = __ldg(k.krayl2 + (kr1 + g));
             const float tr = (R.fm.x * r0.x + R.fm.y * r0.y + R.fm.z * r1.x + R.fm.w * r1.y) * col_rayl;
@@ -365,7 +338,7 @@ int gas_optics_lw(rrtmgp_b200_kdist k, int ncol, int nlay, const T* play, const 
     const dim3 block(kBX, kBY), grid(ceil_div(ncol, kBX), ceil_div(nlay, kBY));
     if constexpr (std::is_same<T, float>::value) {
         if (packed_tables_ok(k->v32, true)) {
-            gas_optics_lw_packed_kernel<<<grid, block, packed_smem_bytes(k->info.ngas), as_stream(stream)>>>(
+            gas_optics_lw_packed_kernel<<<grid, block, packed_smem_bytes(k->info.ngas, k->v32.max_nscal), as_stream(stream)>>>(
                 k->v32, gs, ncol, nlay, play, plev, tlay, tsfc, tlev, col_dry, tau, lay_src, lev_inc, lev_dec,
                 sfc_src, sfc_jac);
             RB_LAUNCH("gas_optics_lw_packed_kernel");
@@ -373,6 +346,13 @@ int gas_optics_lw(rrtmgp_b200_kdist k, int ncol, int nlay, const T* play, const 
         }
     }
     const size_t smem = size_t(k->info.ngas + 1 + kMaxBandGpt) * kThreads * sizeof(T);
+    if (smem > 48 * 1024) {   // many gases in FP64: opt in to more than the default 48 KB
+        static PerDeviceOnce attr;
+        const int ast = attr.run([] { return cudaFuncSetAttribute(gas_optics_lw_kernel<T>,
+                                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                                  227 * 1024); }, "gas_optics_lw attribute");
+        if (ast) return ast;
+    }
     gas_optics_lw_kernel<T><<<grid, block, smem, as_stream(stream)>>>(
         view<T>(k), gs, ncol, nlay, play, plev, tlay, tsfc, tlev, col_dry, tau, lay_src, lev_inc,
         lev_dec, sfc_src, sfc_jac);
@@ -398,7 +378,7 @@ int gas_optics_sw(rrtmgp_b200_kdist k, int ncol, int nlay, const T* play, const 
     bool packed = false;
     if constexpr (std::is_same<T, float>::value) {
         if (packed_tables_ok(k->v32, false)) {
-            gas_optics_sw_packed_kernel<<<grid, block, packed_smem_bytes(k->info.ngas), as_stream(stream)>>>(
+            gas_optics_sw_packed_kernel<<<grid, block, packed_smem_bytes(k->info.ngas, k->v32.max_nscal), as_stream(stream)>>>(
                 k->v32, gs, ncol, nlay, play, plev, tlay, col_dry, tau, ssa, g);
             RB_LAUNCH("gas_optics_sw_packed_kernel");
             packed = true;
@@ -406,6 +386,13 @@ int gas_optics_sw(rrtmgp_b200_kdist k, int ncol, int nlay, const T* play, const 
     }
     if (!packed) {
         const size_t smem = size_t(k->info.ngas + 1 + kMaxBandGpt) * kThreads * sizeof(T);
+        if (smem > 48 * 1024) {
+            static PerDeviceOnce attr;
+            const int ast = attr.run([] { return cudaFuncSetAttribute(gas_optics_sw_kernel<T>,
+                                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                                      227 * 1024); }, "gas_optics_sw attribute");
+            if (ast) return ast;
+        }
         gas_optics_sw_kernel<T><<<grid, block, smem, as_stream(stream)>>>(
             view<T>(k), gs, ncol, nlay, play, plev, tlay, col_dry, tau, ssa, g);
         RB_LAUNCH("gas_optics_sw_kernel");

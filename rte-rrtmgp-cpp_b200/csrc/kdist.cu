@@ -200,6 +200,33 @@ int fill_view(rrtmgp_b200_kdist_t* k, KdistView<T>& v, const rrtmgp_b200_kdist_t
     }
     v.minor_in_band = in_band;
     v.max_band_minor = max_minor;
+    // Scaling kinds (see KdistView): one per distinct (minor gas, scaling gas, complement
+    // flag) among the density-scaled intervals and per minor gas among the others.
+    std::vector<int> sid[2], sgas_k[2], ssg_k[2], sfl_k[2];
+    v.max_nscal = 1;
+    for (int atm = 0; atm < 2; ++atm) {
+        const MinorHost& m = mh[atm];
+        sid[atm].resize(m.gstart.size());
+        for (size_t i = 0; i < m.gstart.size(); ++i) {
+            const int fl = m.flags[i] & 3;
+            const int gas = m.gas[i], sg = (fl & 1) ? m.sgas[i] : 0, f = (fl & 1) ? fl : 0;
+            int found = -1;
+            for (size_t q = 0; q < sgas_k[atm].size(); ++q)
+                if (sgas_k[atm][q] == gas && ssg_k[atm][q] == sg && sfl_k[atm][q] == f) found = int(q);
+            if (found < 0) {
+                found = int(sgas_k[atm].size());
+                sgas_k[atm].push_back(gas);
+                ssg_k[atm].push_back(sg);
+                sfl_k[atm].push_back(f);
+            }
+            sid[atm][i] = found;
+        }
+        v.nscal[atm] = int(sgas_k[atm].size());
+        v.max_nscal = std::max(v.max_nscal, v.nscal[atm]);
+        a.add(sgas_k[atm], &v.scal_gas[atm]);
+        a.add(ssg_k[atm], &v.scal_sgas[atm]);
+        a.add(sfl_k[atm], &v.scal_flags[atm]);
+    }
     v.ngroups = (t->ngpt + 31) / 32;
     std::vector<int> gb0(v.ngroups);
     int max_gb = 0;
@@ -213,9 +240,11 @@ int fill_view(rrtmgp_b200_kdist_t* k, KdistView<T>& v, const rrtmgp_b200_kdist_t
 
     // Corner-packed tables for the fused FP32 kernels.
     v.max_minor_per_g = 0;
+    v.minor_gx_stride = 0;
     std::vector<float4> km4, pf4;
     std::vector<float2> kn2[2], kr2;
     std::vector<int4> mg[2];
+    std::vector<int> mgx[2];
     if (std::is_same<T, float>::value) {
         const int nt = t->ntemp, np = t->npres, np1 = t->npres + 1, ne = t->neta, ng = t->ngpt;
         auto pack4 = [&](const double* src, std::vector<float4>& dst) {
@@ -241,27 +270,32 @@ int fill_view(rrtmgp_b200_kdist_t* k, KdistView<T>& v, const rrtmgp_b200_kdist_t
                         kn2[atm][(size_t(it) * (ne - 1) + ie) * nc + c] =
                             make_float2(float(m.kminor[(size_t(it) * ne + ie) * nc + c]),
                                         float(m.kminor[(size_t(it) * ne + ie + 1) * nc + c]));
-            // Intervals covering each g-point, as (contributor, slot in the band's list).
+        }
+        // Intervals covering each g-point, as codes (contributor << kScalBits) | scaling kind,
+        // in the file order of the intervals.
+        std::vector<std::vector<int>> codes[2];
+        for (int atm = 0; atm < 2; ++atm) {
+            const MinorHost& m = mh[atm];
+            codes[atm].assign(ng, {});
+            for (size_t im = 0; im < m.gstart.size(); ++im)
+                for (int g = m.gstart[im]; g < m.gend[im]; ++g)
+                    codes[atm][g].push_back(((m.kstart[im] + g - m.gstart[im]) << kScalBits) | sid[atm][im]);
+            for (int g = 0; g < ng; ++g) v.max_minor_per_g = std::max(v.max_minor_per_g, int(codes[atm][g].size()));
+        }
+        v.minor_gx_stride = std::max(v.max_minor_per_g - 3, 0);
+        for (int atm = 0; atm < 2; ++atm) {
             mg[atm].assign(ng, make_int4(0, 0, 0, 0));
-            for (int b = 0; b < t->nband; ++b)
-                for (int s = m.band_begin[b]; s < m.band_begin[b + 1]; ++s) {
-                    const int im = m.band_list[s];
-                    const int slot = s - m.band_begin[b];
-                    for (int g = m.gstart[im]; g < m.gend[im]; ++g) {
-                        int4& e = mg[atm][g];
-                        const int code = ((m.kstart[im] + g - m.gstart[im]) << 4) | slot;
-                        if (e.x == 0) e.y = code;
-                        else if (e.x == 1) e.z = code;
-                        else if (e.x == 2) e.w = code;
-                        e.x = std::min(e.x + 1, 4);  // 4 marks "more than 3": fused kernels refuse
-                        v.max_minor_per_g = std::max(v.max_minor_per_g, e.x);
-                    }
-                }
-            // unused slots repeat the first one, so a kernel may read every slot below a
-            // warp-wide maximum count and discard the extra terms
-            for (int4& e : mg[atm]) {
-                if (e.x < 2) e.z = e.y;
-                if (e.x < 3) e.w = e.y;
+            if (v.minor_gx_stride) mgx[atm].assign(size_t(ng) * v.minor_gx_stride, 0);
+            for (int g = 0; g < ng; ++g) {
+                const std::vector<int>& c = codes[atm][g];
+                int4& e = mg[atm][g];
+                e.x = int(c.size());
+                // unused slots repeat the first one, so a kernel may read every slot below a
+                // warp-wide maximum count and discard the extra terms
+                e.y = c.empty() ? 0 : c[0];
+                e.z = c.size() > 1 ? c[1] : e.y;
+                e.w = c.size() > 2 ? c[2] : e.y;
+                for (size_t n = 3; n < c.size(); ++n) mgx[atm][size_t(g) * v.minor_gx_stride + n - 3] = c[n];
             }
         }
         if (info.has_rayleigh) {
@@ -284,6 +318,8 @@ int fill_view(rrtmgp_b200_kdist_t* k, KdistView<T>& v, const rrtmgp_b200_kdist_t
     a.add(kr2, &v.krayl2);
     a.add(mg[0], &v.minor_g[0]);
     a.add(mg[1], &v.minor_g[1]);
+    a.add(mgx[0], &v.minor_gx[0]);
+    a.add(mgx[1], &v.minor_gx[1]);
     return a.upload(k->allocations);
 }
 

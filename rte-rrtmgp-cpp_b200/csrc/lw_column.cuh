@@ -104,10 +104,11 @@ __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<
     const int lane = threadIdx.x & 31;
     const int nband = k.nband;
     const SmemLayout SL = smem_layout(io.nlay(), k.ngas, nband, 1, cx.nwarps(), 2, CL,
-                                      k.max_group_bands * (P2 ? 2 : 1));
+                                      k.max_group_bands * (P2 ? 2 : 1), k.max_nscal);
     unsigned char* const smem_raw = cx.smem();
     LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
     float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
+    float* sm_sc = reinterpret_cast<float*>(smem_raw + SL.scal);   // [layer][scaling kind]
     float* sm_cld = reinterpret_cast<float*>(smem_raw + SL.cloud);
     // chunk maps and surface source are double-buffered by group parity, so a warp can
     // start the next group while others still read this group's (one barrier per group)
@@ -138,6 +139,8 @@ __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<
             sm_cld[b * nlay + j] = tau;
         }
     }
+    cx.sync();
+    layer_minor_scalings(k, st, sm_cg, io.nlay(), sm_sc, io.nlay(), cx.tid(), cx.nthreads());
     cx.sync();
 
     const float D = 1.66f;                 // single-angle secant (Rte_lw.cpp:101-113)
@@ -184,7 +187,8 @@ __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<
             omt[i] = 0.f; sdn[i] = 0.f; sup[i] = 0.f;
             if (j < nlay && gv) {
                 const Rec& R = recs[slot * CL + i];
-                const float tau = tau_abs(k, R, g, R.a ? mg1 : mg0, R.a ? nm1 : nm0) + R.aux.w;
+                const float tau =
+                    tau_abs(k, R, g, R.a ? mg1 : mg0, R.a ? nm1 : nm0, sm_sc + j * k.max_nscal) + R.aux.w;
                 const float4 p0 = __ldg(k.pfrac4 + (R.kb.x + g));
                 const float4 p1 = __ldg(k.pfrac4 + (R.kb.y + g));
                 const float pfrac = (R.wpl0.x * p0.x + R.wpl0.y * p0.y + R.wpl0.z * p0.z + R.wpl0.w * p0.w) +

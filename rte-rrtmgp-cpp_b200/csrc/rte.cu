@@ -24,13 +24,19 @@ namespace {
 // Longwave no-scattering solver (lw_solver_noscat steps 1-3 + lw_transport_noscat_kernel,
 // rte_solver_kernels.cu:35-185; F90 lw_solver_noscat / _GaussQuad :58-380).  Stash: trans
 // and source_up of the down sweep kept in shared memory [nlay][blockDim] for the up sweep.
+// Surface-temperature Jacobian (the reference's do_jacobians path of
+// lw_transport_noscat_kernel, rte_solver_kernels.cu:56,65,82,91 and step 3): when flux_up_jac
+// is not NULL, flux_up_jac = 2 pi w sum over angles of the upward radiance a surface source
+// sfc_emis * sfc_src_jac produces with no other source, i.e. that source attenuated by the
+// transmissivities of the layers between the surface and the level.
 template <typename T, bool Stash>
 __global__ void lw_solver_kernel(int ncol, int nlay, int nband, int top_at_1, int nmus,
                                  const int* __restrict__ gpt2band, const T* __restrict__ tau,
                                  const T* __restrict__ lay_src, const T* __restrict__ lev_inc,
                                  const T* __restrict__ lev_dec, const T* __restrict__ sfc_src,
                                  const T* __restrict__ sfc_emis, const T* __restrict__ inc_flux,
-                                 T* __restrict__ flux_up, T* __restrict__ flux_dn)
+                                 T* __restrict__ flux_up, T* __restrict__ flux_dn,
+                                 const T* __restrict__ sfc_src_jac, T* __restrict__ flux_up_jac)
 {
     extern __shared__ unsigned char smem_raw[];
     T* st_tr = reinterpret_cast<T*>(smem_raw);
@@ -75,6 +81,11 @@ __global__ void lw_solver_kernel(int ncol, int nlay, int nband, int top_at_1, in
         T rup = radn * (T(1) - emis) + emis * ssrc;
         if (imu == 0) flux_up[fbase + size_t(sfc) * ncol] = two_pi_w * rup;
         else flux_up[fbase + size_t(sfc) * ncol] += two_pi_w * rup;
+        T rjac = flux_up_jac ? emis * sfc_src_jac[icol + size_t(g) * ncol] : T(0);
+        if (flux_up_jac) {
+            if (imu == 0) flux_up_jac[fbase + size_t(sfc) * ncol] = two_pi_w * rjac;
+            else flux_up_jac[fbase + size_t(sfc) * ncol] += two_pi_w * rjac;
+        }
         // Upward sweep.
 #pragma unroll 4
         for (int j = nlay - 1; j >= 0; --j) {
@@ -92,6 +103,11 @@ __global__ void lw_solver_kernel(int ncol, int nlay, int nband, int top_at_1, in
             const size_t o = fbase + size_t(top_at_1 ? l : l + 1) * ncol;
             if (imu == 0) flux_up[o] = two_pi_w * rup;
             else flux_up[o] += two_pi_w * rup;
+            if (flux_up_jac) {
+                rjac *= tr;
+                if (imu == 0) flux_up_jac[o] = two_pi_w * rjac;
+                else flux_up_jac[o] += two_pi_w * rjac;
+            }
         }
     }
 }
@@ -189,7 +205,8 @@ __global__ void __launch_bounds__(MAXT) lw_solver_chunked(int ncol, int nlay, in
                                                           const T* __restrict__ lay_src, const T* __restrict__ lev_inc,
                                                           const T* __restrict__ lev_dec, const T* __restrict__ sfc_src,
                                                           const T* __restrict__ sfc_emis, const T* __restrict__ inc_flux,
-                                                          T* __restrict__ flux_up, T* __restrict__ flux_dn)
+                                                          T* __restrict__ flux_up, T* __restrict__ flux_dn,
+                                                          const T* __restrict__ sfc_src_jac, T* __restrict__ flux_up_jac)
 {
     __shared__ T sm_a[16 * 32], sm_bd[16 * 32], sm_bu[16 * 32];   // chunk maps [chunk][lane]
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -243,6 +260,11 @@ __global__ void __launch_bounds__(MAXT) lw_solver_chunked(int ncol, int nlay, in
     const T rsfc = rs * (T(1) - emis) + emis * sfc_src[ic + size_t(g) * ncol];   // leaving the surface
     T rup = rsfc;
     for (int c = nw - 1; c > w; --c) rup = sm_a[c * 32 + lane] * rup + sm_bu[c * 32 + lane];
+    // surface-temperature Jacobian: the surface term alone, attenuated by the chunks below
+    const T jsfc = flux_up_jac ? emis * sfc_src_jac[ic + size_t(g) * ncol] : T(0);
+    T rjac = jsfc;
+    if (flux_up_jac)
+        for (int c = nw - 1; c > w; --c) rjac *= sm_a[c * 32 + lane];
     // re-sweeps: level j0 + i is the top of layer j0 + i
     T* const dn = flux_dn + ic + size_t(g) * ncv;
     T* const up = flux_up + ic + size_t(g) * ncv;
@@ -259,6 +281,15 @@ __global__ void __launch_bounds__(MAXT) lw_solver_chunked(int ncol, int nlay, in
     for (int i = CL - 1; i >= 0; --i) {
         rup = tr[i] * rup + sup[i];
         if (j0 + i < nlay) up[o0 + i * step] = two_pi_w * rup;
+    }
+    if (flux_up_jac) {
+        T* const uj = flux_up_jac + ic + size_t(g) * ncv;
+        if (j0 <= nlay - 1 && nlay - 1 < j0 + CL) uj[o0 + (nlay - j0) * step] = two_pi_w * jsfc;
+#pragma unroll
+        for (int i = CL - 1; i >= 0; --i) {
+            rjac *= tr[i];
+            if (j0 + i < nlay) uj[o0 + i * step] = two_pi_w * rjac;
+        }
     }
 }
 
@@ -439,7 +470,7 @@ int lw_smem_block(int nlay, size_t* smem)
 template <typename T>
 int rte_lw(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const T* tau, const T* lay_src,
            const T* lev_inc, const T* lev_dec, const T* sfc_src, const T* sfc_emis, const T* inc_flux,
-           int nmus, T* flux_up, T* flux_dn, void* stream)
+           int nmus, T* flux_up, T* flux_dn, void* stream, const T* sfc_src_jac = nullptr, T* flux_up_jac = nullptr)
 {
     RB_CHECK_ARG(b, "rte_lw: null bands");
     RB_CHECK_ARG(ncol > 0 && nlay > 0, "rte_lw: ncol and nlay must be > 0");
@@ -453,11 +484,11 @@ int rte_lw(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const T* tau, 
         if (sizeof(T) == 4 && nlay <= 8 * 16)
             lw_solver_chunked<T, 8, 512><<<grid, 32 * ceil_div(nlay, 8), 0, as_stream(stream)>>>(
                 ncol, nlay, b->nband, top_at_1, b->d_gpt2band, tau, lay_src, lev_inc, lev_dec, sfc_src, sfc_emis,
-                inc_flux, flux_up, flux_dn);
+                inc_flux, flux_up, flux_dn, sfc_src_jac, flux_up_jac);
         else
             lw_solver_chunked<T, 16, 512><<<grid, 32 * ceil_div(nlay, 16), 0, as_stream(stream)>>>(
                 ncol, nlay, b->nband, top_at_1, b->d_gpt2band, tau, lay_src, lev_inc, lev_dec, sfc_src, sfc_emis,
-                inc_flux, flux_up, flux_dn);
+                inc_flux, flux_up, flux_dn, sfc_src_jac, flux_up_jac);
         RB_LAUNCH("lw_solver_chunked");
         return RRTMGP_B200_OK;
     }
@@ -472,12 +503,12 @@ int rte_lw(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const T* tau, 
         const dim3 grid(ceil_div(ncol, bs), b->ngpt);
         lw_solver_kernel<T, true><<<grid, bs, smem, as_stream(stream)>>>(
             ncol, nlay, b->nband, top_at_1, nmus, b->d_gpt2band, tau, lay_src, lev_inc, lev_dec, sfc_src, sfc_emis,
-            inc_flux, flux_up, flux_dn);
+            inc_flux, flux_up, flux_dn, sfc_src_jac, flux_up_jac);
     } else {
         const dim3 grid(ceil_div(ncol, 64), b->ngpt);
         lw_solver_kernel<T, false><<<grid, 64, 0, as_stream(stream)>>>(
             ncol, nlay, b->nband, top_at_1, nmus, b->d_gpt2band, tau, lay_src, lev_inc, lev_dec, sfc_src, sfc_emis,
-            inc_flux, flux_up, flux_dn);
+            inc_flux, flux_up, flux_dn, sfc_src_jac, flux_up_jac);
     }
     RB_LAUNCH("lw_solver_kernel");
     return RRTMGP_B200_OK;
@@ -603,6 +634,25 @@ int rrtmgp_b200_rte_lw_f64(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1
         const double* lay_src, const double* lev_src_inc, const double* lev_src_dec, const double* sfc_src,
         const double* sfc_emis, const double* inc_flux, int n_gauss_angles, double* up, double* dn, void* s)
 { return rte_lw<double>(b, ncol, nlay, top_at_1, tau, lay_src, lev_src_inc, lev_src_dec, sfc_src, sfc_emis, inc_flux, n_gauss_angles, up, dn, s); }
+
+int rrtmgp_b200_rte_lw_jac_f32(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const float* tau,
+        const float* lay_src, const float* lev_src_inc, const float* lev_src_dec, const float* sfc_src,
+        const float* sfc_src_jac, const float* sfc_emis, const float* inc_flux, int n_gauss_angles, float* up,
+        float* dn, float* up_jac, void* s)
+{
+    RB_CHECK_ARG(sfc_src_jac && up_jac, "rte_lw_jac: null Jacobian array");
+    return rte_lw<float>(b, ncol, nlay, top_at_1, tau, lay_src, lev_src_inc, lev_src_dec, sfc_src, sfc_emis, inc_flux,
+                         n_gauss_angles, up, dn, s, sfc_src_jac, up_jac);
+}
+int rrtmgp_b200_rte_lw_jac_f64(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const double* tau,
+        const double* lay_src, const double* lev_src_inc, const double* lev_src_dec, const double* sfc_src,
+        const double* sfc_src_jac, const double* sfc_emis, const double* inc_flux, int n_gauss_angles, double* up,
+        double* dn, double* up_jac, void* s)
+{
+    RB_CHECK_ARG(sfc_src_jac && up_jac, "rte_lw_jac: null Jacobian array");
+    return rte_lw<double>(b, ncol, nlay, top_at_1, tau, lay_src, lev_src_inc, lev_src_dec, sfc_src, sfc_emis,
+                          inc_flux, n_gauss_angles, up, dn, s, sfc_src_jac, up_jac);
+}
 
 size_t rrtmgp_b200_rte_sw_workspace_bytes(int ncol, int nlay, int ngpt, int fp64)
 { return sw_ws_bytes(ncol, nlay, ngpt, fp64); }

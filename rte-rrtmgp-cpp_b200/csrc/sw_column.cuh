@@ -69,10 +69,11 @@ __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<
     const int lane = threadIdx.x & 31;
     const int nband = k.nband;
     const SmemLayout SL = smem_layout(io.nlay(), k.ngas, nband, 0, cx.nwarps(), 3, CL,
-                                      k.max_group_bands * (P2 ? 2 : 1));
+                                      k.max_group_bands * (P2 ? 2 : 1), k.max_nscal);
     unsigned char* const smem_raw = cx.smem();
     LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
     float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
+    float* sm_sc = reinterpret_cast<float*>(smem_raw + SL.scal);   // [layer][scaling kind]
     float* sm_pt = reinterpret_cast<float*>(smem_raw + SL.maps);                            // [NW][32]
     float4* sm_comp = reinterpret_cast<float4*>(smem_raw + SL.maps) + cx.nwarps() * 32;     // [NW][32]
     float* sm_compd = reinterpret_cast<float*>(sm_comp + cx.nwarps() * 32);                 // [NW][32]
@@ -91,6 +92,8 @@ __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<
                      sm_cg, cx.tid(), cx.nthreads());
     }
     const float mu0_inv = 1.f / mu0;
+    cx.sync();
+    layer_minor_scalings(k, st, sm_cg, io.nlay(), sm_sc, io.nlay(), cx.tid(), cx.nthreads());
     cx.sync();
 
     const int ngpt = k.ngpt;
@@ -138,7 +141,7 @@ __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<
             float R = 0.f, T = 1.f, Rdir = 0.f, Tdir = 0.f, Tn = 1.f, adif = 0.f, adir = 0.f;
             if (j < nlay && gv) {
                 const Rec& Rc = recs[slot * CL + i];
-                const float ta = tau_abs(k, Rc, g, Rc.a ? mg1 : mg0, Rc.a ? nm1 : nm0);
+                const float ta = tau_abs(k, Rc, g, Rc.a ? mg1 : mg0, Rc.a ? nm1 : nm0, sm_sc + j * k.max_nscal);
                 const float2 r0 = __ldg(k.krayl2 + (Rc.kr[0] + g));
                 const float2 r1 = __ldg(k.krayl2 + (Rc.kr[1] + g));
                 const float tr = (Rc.fm.x * r0.x + Rc.fm.y * r0.y + Rc.fm.z * r1.x + Rc.fm.w * r1.y) * Rc.aux.x;

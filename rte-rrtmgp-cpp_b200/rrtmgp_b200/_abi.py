@@ -265,6 +265,7 @@ _FP_SIGS = {
     "add_to_1scl": [_P, _I, _I, _P, _P, _I, _P],
     "add_to_2str": [_P, _I, _I, _P, _P, _P, _P, _P, _P, _I, _P],
     "rte_lw": [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P],
+    "rte_lw_jac": [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P],
     "rte_sw": [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _SZ, _P],
     "fluxes_broadband": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P],
     "fluxes_byband": [_P, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P],

@@ -275,10 +275,21 @@ class Rte_lw:
     """Rte_lw_gpu::rte_lw (include/Rte_lw.h:65-73)."""
 
     @staticmethod
-    def rte_lw(bands: Bands, tau, top_at_1, sources: dict, sfc_emis, inc_flux=None, n_gauss_angles=1):
+    def rte_lw(bands: Bands, tau, top_at_1, sources: dict, sfc_emis, inc_flux=None, n_gauss_angles=1,
+               flux_up_jac=False):
+        """Returns (up, dn), or (up, dn, up_jac) with flux_up_jac: the surface-temperature
+        Jacobian of the upward g-point fluxes from sources["sfc_src_jac"] (the reference's
+        do_jacobians output of lw_solver_noscat)."""
         ngpt, nlay, ncol = tau.shape
         up = _empty((ngpt, nlay + 1, ncol), tau)
         dn = _empty((ngpt, nlay + 1, ncol), tau)
+        if flux_up_jac:
+            jac = _empty((ngpt, nlay + 1, ncol), tau)
+            _call("rte_lw_jac", tau, bands.handle, ncol, nlay, int(bool(top_at_1)), _ptr(tau),
+                  _ptr(sources["lay_src"]), _ptr(sources["lev_src_inc"]), _ptr(sources["lev_src_dec"]),
+                  _ptr(sources["sfc_src"]), _ptr(sources["sfc_src_jac"]), _ptr(sfc_emis), _ptr(inc_flux),
+                  int(n_gauss_angles), _ptr(up), _ptr(dn), _ptr(jac), _stream())
+            return up, dn, jac
         _call("rte_lw", tau, bands.handle, ncol, nlay, int(bool(top_at_1)), _ptr(tau), _ptr(sources["lay_src"]),
               _ptr(sources["lev_src_inc"]), _ptr(sources["lev_src_dec"]), _ptr(sources["sfc_src"]),
               _ptr(sfc_emis), _ptr(inc_flux), int(n_gauss_angles), _ptr(up), _ptr(dn), _stream())

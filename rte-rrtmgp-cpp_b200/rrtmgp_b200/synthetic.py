@@ -31,6 +31,15 @@ GAS_NAMES = ["h2o", "co2", "o3", "n2o", "co", "ch4", "o2", "n2", "cfc11", "cfc12
 # Gases present in the synthetic atmospheres (co, cfc11, cfc12 are absent on purpose so the
 # k-distribution constructor's gas/minor-absorber reduction is exercised).
 ATM_GASES = ["h2o", "co2", "o3", "n2o", "ch4", "o2", "n2"]
+# The dense tables (make_kdist(..., dense=True)) list every gas of the public LW g256 file,
+# halocarbons included, and the trace-gas atmospheres (make_atmosphere(..., trace_gases=True))
+# carry all of them.
+TRACE_GASES = ["ccl4", "cfc22", "hfc143a", "hfc125", "hfc23", "hfc32", "hfc134a", "cf4", "no2"]
+GAS_NAMES_DENSE = GAS_NAMES + TRACE_GASES
+ATM_GASES_DENSE = ATM_GASES + ["co", "cfc11", "cfc12"] + TRACE_GASES
+_TRACE_VMR = {"co": 1.2e-7, "cfc11": 2.3e-10, "cfc12": 5.2e-10, "ccl4": 8.0e-11, "cfc22": 2.5e-10,
+              "hfc143a": 2.0e-11, "hfc125": 2.5e-11, "hfc23": 3.0e-11, "hfc32": 1.5e-11,
+              "hfc134a": 1.0e-10, "cf4": 8.0e-11, "no2": 1.0e-9}
 
 LW_BAND_WVN = [(10, 250), (250, 500), (500, 630), (630, 700), (700, 820), (820, 980),
                (980, 1080), (1080, 1180), (1180, 1390), (1390, 1480), (1480, 1800),
@@ -65,6 +74,8 @@ _MINOR_IDS = ["h2o_frgn", "h2o_self", "co2", "o3", "n2o", "co", "ch4", "o2", "n2
               "cfc12", "o2_n2"]
 _MINOR_GAS = ["h2o", "h2o", "co2", "o3", "n2o", "co", "ch4", "o2", "n2", "cfc11", "cfc12",
               "o2"]
+_MINOR_IDS_DENSE = _MINOR_IDS + ["co2_n2", "n2_o2"] + TRACE_GASES
+_MINOR_GAS_DENSE = _MINOR_GAS + ["co2", "n2"] + TRACE_GASES
 
 _H = 6.62607015e-34
 _C = 2.99792458e8
@@ -112,10 +123,45 @@ def _minor_intervals(rng, band_lims, atm):
     return out
 
 
-def make_kdist(kind: str, seed: int = 1):
-    """Return a dict with the reference netCDF variables for an LW or SW k-distribution."""
+def _minor_intervals_dense(rng, band_lims, atm):
+    """Minor-absorber intervals of the dense tables: 2-5 per band, 13 in band 0, and in bands 3
+    and 9 seven intervals that all cover the whole band (seven on the same g-points), drawn
+    over every minor absorber including the halocarbons, as the public LW g256 file lists many
+    absorbers over the same g-points."""
+    out = []
+    for ib, (g0, g1) in enumerate(band_lims):
+        nint = 13 if ib == 0 else (7 if ib in (3, 9) else int(rng.integers(2, 6)))
+        for _ in range(nint):
+            mid = int(rng.integers(0, len(_MINOR_IDS_DENSE)))
+            ident = _MINOR_IDS_DENSE[mid]
+            if ib in (3, 9):
+                start, ng = g0, g1 - g0 + 1
+            else:
+                ng = int(rng.integers(2, g1 - g0 + 2))
+                start = int(rng.integers(g0, g1 - ng + 2))
+            if ident in ("h2o_frgn", "h2o_self"):
+                dens, sgas, comp = 1, "h2o", 1 if ident == "h2o_frgn" else 0
+            elif ident in ("o2_n2", "co2_n2"):
+                dens, sgas, comp = 1, "n2", 0
+            elif ident == "n2_o2":
+                dens, sgas, comp = 1, "o2", 0
+            else:
+                dens = int(rng.integers(0, 2))
+                sgas = "" if (atm == 1 or rng.random() < 0.5) else "h2o"
+                comp = int(rng.integers(0, 2)) if sgas else 0
+            out.append(dict(id=ident, lims=(start, start + ng - 1), dens=dens, sgas=sgas, comp=comp))
+    return out
+
+
+def make_kdist(kind: str, seed: int = 1, dense: bool = False):
+    """Return a dict with the reference netCDF variables for an LW or SW k-distribution.
+
+    dense=True: the gas list of the public LW g256 file (halocarbons included) and a dense
+    minor-absorber layout (_minor_intervals_dense); the default tables keep 1-3 intervals per
+    band."""
     assert kind in ("lw", "sw")
     rng = np.random.default_rng(seed + (0 if kind == "lw" else 1000))
+    gas_names = GAS_NAMES_DENSE if dense else GAS_NAMES
     wvn = LW_BAND_WVN if kind == "lw" else SW_BAND_WVN
     keys = _LW_KEY if kind == "lw" else _SW_KEY
     nband = len(wvn)
@@ -123,7 +169,7 @@ def make_kdist(kind: str, seed: int = 1):
     ngpt = nband * ngpb
     band_lims_gpt = np.array([[1 + b * ngpb, (b + 1) * ngpb] for b in range(nband)], np.int32)
     press_ref, temp_ref = _ref_grids()
-    ngas = len(GAS_NAMES)
+    ngas = len(gas_names)
 
     key_species = np.zeros((nband, 2, 2), np.int32)
     for b, (lo, up) in enumerate(keys):
@@ -133,9 +179,10 @@ def make_kdist(kind: str, seed: int = 1):
     # vmr_ref (ntemp, ngas+1, 2): reference volume mixing ratios; index 0 is dry air.
     base_vmr = {"h2o": 3e-3, "co2": 4e-4, "o3": 5e-7, "n2o": 3e-7, "co": 1e-7, "ch4": 1.8e-6,
                 "o2": 0.2095, "n2": 0.7808, "cfc11": 2e-10, "cfc12": 5e-10}
+    base_vmr.update({g: _TRACE_VMR[g] for g in TRACE_GASES})
     vmr_ref = np.zeros((NTEMP, ngas + 1, 2))
     vmr_ref[:, 0, :] = 1.0
-    for i, gname in enumerate(GAS_NAMES):
+    for i, gname in enumerate(gas_names):
         for atm in range(2):
             fac = (1.0 if atm == 0 else (0.002 if gname == "h2o" else (8.0 if gname == "o3" else 1.0)))
             vmr_ref[:, i + 1, atm] = base_vmr[gname] * fac * (1.0 + 0.02 * np.linspace(-1, 1, NTEMP))
@@ -165,7 +212,7 @@ def make_kdist(kind: str, seed: int = 1):
 
     # Minor absorbers.
     def minor_block(atm):
-        ints = _minor_intervals(rng, band_lims_gpt.tolist(), atm)
+        ints = (_minor_intervals_dense if dense else _minor_intervals)(rng, band_lims_gpt.tolist(), atm)
         ncontrib = sum(iv["lims"][1] - iv["lims"][0] + 1 for iv in ints)
         kmin = np.empty((NTEMP, NETA, ncontrib))
         start = []
@@ -197,14 +244,15 @@ def make_kdist(kind: str, seed: int = 1):
     lo, up = pack(ints_lo), pack(ints_up)
 
     d = dict(
-        kind=kind, gas_names=list(GAS_NAMES), key_species=key_species,
+        kind=kind, gas_names=list(gas_names), key_species=key_species,
         bnd_limits_gpt=band_lims_gpt,
         bnd_limits_wavenumber=np.array(wvn, np.float64),
         press_ref=press_ref, press_ref_trop=PRESS_REF_TROP, temp_ref=temp_ref,
         absorption_coefficient_ref_P=1013.25, absorption_coefficient_ref_T=273.15,
         vmr_ref=vmr_ref, kmajor=kmajor,
         kminor_lower=kminor_lower, kminor_upper=kminor_upper,
-        gas_minor=list(_MINOR_GAS), identifier_minor=list(_MINOR_IDS),
+        gas_minor=list(_MINOR_GAS_DENSE if dense else _MINOR_GAS),
+        identifier_minor=list(_MINOR_IDS_DENSE if dense else _MINOR_IDS),
         minor_gases_lower=lo["gases"], minor_gases_upper=up["gases"],
         minor_limits_gpt_lower=lo["lims"], minor_limits_gpt_upper=up["lims"],
         minor_scales_with_density_lower=lo["dens"], minor_scales_with_density_upper=up["dens"],
@@ -325,7 +373,7 @@ def make_aerosols(play: np.ndarray, seed: int = 12):
 
 
 def make_atmosphere(ncol: int, nlay: int, seed: int = 42, clouds: bool = True,
-                    nband_lw: int = 16, nband_sw: int = 14, top_at_1: bool = True):
+                    nband_lw: int = 16, nband_sw: int = 14, top_at_1: bool = True, trace_gases: bool = False):
     """Synthetic atmosphere in the reference layouts (column fastest; numpy (nlay, ncol)).
 
     Pressure levels are log spaced from 1e5 Pa to the top (clamped to the table minimum);
@@ -356,6 +404,8 @@ def make_atmosphere(ncol: int, nlay: int, seed: int = 42, clouds: bool = True,
     o3 = 8.0e-6 * np.exp(-((z - 25.0) / 5.0) ** 2)
     gases = {"h2o": h2o, "o3": o3, "co2": np.array([[4.0e-4]]), "ch4": np.array([[1.8e-6]]),
              "n2o": np.array([[3.2e-7]]), "o2": np.array([[0.2095]]), "n2": np.array([[0.7808]])}
+    if trace_gases:   # scalar halocarbons, co and no2 (ATM_GASES_DENSE), drawn after every other field
+        gases.update({g: np.array([[v]]) for g, v in _TRACE_VMR.items()})
     atm = dict(ncol=ncol, nlay=nlay, top_at_1=top_at_1, play=play, plev=plev, tlay=tlay,
                tlev=tlev, tsfc=tsfc, gases=gases,
                emis_sfc=np.full((ncol, nband_lw), 0.98),

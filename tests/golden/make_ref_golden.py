@@ -4,7 +4,10 @@ Runs the reference's own FP64 GPU classes (rte-rrtmgp-cpp src_cuda/ + src_kernel
 compiled by oracle/ref/Makefile into oracle/_ref/libref_rrtmgp_f64.so) on small seeded
 synthetic cases and stores inputs and outputs as compressed npz files:
 
-    python tests/golden/make_ref_golden.py OUTDIR      # on a machine with a GPU
+    python tests/golden/make_ref_golden.py OUTDIR [--only dense]   # on a machine with a GPU
+
+--only dense writes only the gas-optics fixtures of the dense tables (make_kdist(dense=True):
+every halocarbon, up to 13 minor intervals in a band and 11 over one g-point).
 
 The reference's runtime tuner would otherwise time many block shapes on first use; its cache
 file (rte_rrtmgp_kernel_tuning.txt, read from the working directory, include/tuner.h:50-61)
@@ -94,7 +97,34 @@ def gas_array(gases):
     return arr, keep
 
 
-def main(outdir: Path):
+def dense_gas_cases(lib, chk, outdir: Path):
+    """Gas optics of the dense tables (LW top-at-1 and bottom-at-1, SW top-at-1) on a
+    trace-gas atmosphere."""
+    lw, sw = S.make_kdist("lw", dense=True), S.make_kdist("sw", dense=True)
+    tlw, k1 = _abi.kdist_tables(lw)
+    tsw, k2 = _abi.kdist_tables(sw)
+    for name, top in (("gas_lw_dense_top1", True), ("gas_lw_dense_bot1", False)):
+        atm = S.make_atmosphere(NCOL, NLAY, seed=111, clouds=False, top_at_1=top, trace_gases=True)
+        arr, keep = gas_array(atm["gases"])
+        o = {k: np.empty((256, NLAY, NCOL)) for k in ("tau", "lay_src", "lev_src_inc", "lev_src_dec")}
+        o["sfc_src"] = np.empty((256, NCOL))
+        o["sfc_src_jac"] = np.empty((256, NCOL))
+        chk(lib.ref_gas_optics_lw(C.byref(tlw), arr, len(atm["gases"]), NCOL, NLAY, P(D(atm["play"])),
+                                  P(D(atm["plev"])), P(D(atm["tlay"])), P(D(atm["tsfc"])), P(D(atm["tlev"])), None,
+                                  P(o["tau"]), P(o["lay_src"]), P(o["lev_src_inc"]), P(o["lev_src_dec"]),
+                                  P(o["sfc_src"]), P(o["sfc_src_jac"])))
+        np.savez_compressed(outdir / f"{name}.npz", seed=111, top_at_1=top, **o)
+    atm = S.make_atmosphere(NCOL, NLAY, seed=112, clouds=False, top_at_1=True, trace_gases=True)
+    arr, keep = gas_array(atm["gases"])
+    o = {k: np.empty((224, NLAY, NCOL)) for k in ("tau", "ssa", "g")}
+    o["toa_src"] = np.empty((224, NCOL))
+    chk(lib.ref_gas_optics_sw(C.byref(tsw), arr, len(atm["gases"]), NCOL, NLAY, P(D(atm["play"])),
+                              P(D(atm["plev"])), P(D(atm["tlay"])), None, P(o["tau"]), P(o["ssa"]), P(o["g"]),
+                              P(o["toa_src"])))
+    np.savez_compressed(outdir / "gas_sw_dense_top1.npz", seed=112, top_at_1=True, **o)
+
+
+def main(outdir: Path, only: str = ""):
     outdir = outdir.resolve()
     outdir.mkdir(parents=True, exist_ok=True)
     workdir = outdir / "_tuner_cwd"
@@ -110,6 +140,10 @@ def main(outdir: Path):
         if st != 0:
             raise RuntimeError(lib.ref_last_error().decode())
 
+    if only == "dense":
+        dense_gas_cases(lib, chk, outdir)
+        print("golden fixtures written to", outdir)
+        return
     lw, sw = S.make_kdist("lw"), S.make_kdist("sw")
     clw, csw = S.make_cloud_luts("lw"), S.make_cloud_luts("sw")
     tlw, k1 = _abi.kdist_tables(lw)
@@ -208,6 +242,6 @@ def main(outdir: Path):
 
 
 if __name__ == "__main__":
-    if len(sys.argv) != 2:
-        sys.exit("usage: python tests/golden/make_ref_golden.py OUTPUT_DIR")
-    main(Path(sys.argv[1]))
+    if len(sys.argv) not in (2, 4) or (len(sys.argv) == 4 and sys.argv[2:] != ["--only", "dense"]):
+        sys.exit("usage: python tests/golden/make_ref_golden.py OUTPUT_DIR [--only dense]")
+    main(Path(sys.argv[1]), sys.argv[3] if len(sys.argv) == 4 else "")

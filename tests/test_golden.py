@@ -127,3 +127,38 @@ def test_aerosol_optics_matches_reference(oracle_mod):
     out = oracle_mod.aerosol_optics(S.make_aerosol_luts(), aer, rh, atm["plev"])
     for k in ("tau", "ssa", "g"):
         assert relerr(out[k], ref[k], 1e-12) < 1e-13, k
+
+
+# Dense minor-absorber layouts: the reference's gas optics on the dense tables (every
+# halocarbon, up to 13 minor intervals in a band and 11 over one g-point), trace-gas
+# atmospheres; make_ref_golden.py OUTDIR --only dense.
+@pytest.mark.parametrize("name,kind,top,seed", [("gas_lw_dense_top1", "lw", True, 111),
+                                                ("gas_lw_dense_bot1", "lw", False, 111),
+                                                ("gas_sw_dense_top1", "sw", True, 112)])
+def test_gas_optics_dense_matches_reference(oracle_mod, name, kind, top, seed):
+    ref = load(name)
+    atm = S.make_atmosphere(NCOL, NLAY, seed=seed, clouds=False, top_at_1=top, trace_gases=True)
+    go = oracle_mod.GasOptics(S.make_kdist(kind, dense=True), S.ATM_GASES_DENSE)
+    if kind == "lw":
+        out = go.gas_optics_lw(atm["play"], atm["plev"], atm["tlay"], atm["tsfc"], atm["gases"], atm["tlev"])
+        keys = ("tau", "lay_src", "lev_src_inc", "lev_src_dec", "sfc_src", "sfc_src_jac")
+    else:
+        out = go.gas_optics_sw(atm["play"], atm["plev"], atm["tlay"], atm["gases"])
+        keys = ("tau", "ssa", "g", "toa_src")
+    for k in keys:
+        assert relerr(out[k], ref[k], 1e-9) < 1e-12, k
+
+
+def test_dense_tables_layout():
+    """The dense tables carry what the fused kernels must accept: 13 intervals in one band,
+    seven over the same g-points, intervals of every halocarbon."""
+    for kind in ("lw", "sw"):
+        d = S.make_kdist(kind, dense=True)
+        lims = d["minor_limits_gpt_lower"]
+        per_band = np.bincount((lims[:, 0] - 1) // 16, minlength=len(d["bnd_limits_gpt"]))
+        assert per_band.max() >= 12
+        cover = np.zeros(d["kmajor"].shape[-1], int)
+        for a, b in lims:
+            cover[a - 1:b] += 1
+        assert cover.max() >= 6
+        assert set(S.TRACE_GASES) <= set(d["gas_names"])

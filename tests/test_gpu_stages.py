@@ -284,6 +284,36 @@ def test_rte_lw_large_nlay_without_smem_stash(api, oracle_mod, tables, gpu):
 
 @pytest.mark.parametrize("prec", ["f32", "f64"])
 @pytest.mark.parametrize("top_at_1", [True, False])
+@pytest.mark.parametrize("nmu,nlay", [(1, NLAY), (3, NLAY), (1, 300)])
+def test_rte_lw_surface_temperature_jacobian(api, oracle_mod, tables, gpu, prec, top_at_1, nmu, nlay):
+    """gpt_flux_up_jac (the reference's do_jacobians output) against the oracle's, and against
+    the finite difference it stands for: gpt_flux_up at Tsfc + 1 K minus at Tsfc (the fluxes
+    depend on Tsfc only through the surface source, linearly).  One angle runs the chunked
+    kernel up to 256 layers; three angles and 300 layers the per-(column, g-point) kernel."""
+    import torch
+    dt = dtypes()[prec]
+    atm = S.make_atmosphere(NCOL, nlay, seed=23, clouds=False, top_at_1=top_at_1)
+    ko = oracle_mod.GasOptics(tables["lw"], S.ATM_GASES)
+    go = ko.gas_optics_lw(atm["play"], atm["plev"], atm["tlay"], atm["tsfc"], atm["gases"], atm["tlev"])
+    emis = np.random.default_rng(6).uniform(0.8, 1.0, (NCOL, 16))
+    bl = tables["lw"]["bnd_limits_gpt"]
+    up, dn, jac = oracle_mod.rte_lw(bl, go["tau"], top_at_1, go, emis, None, nmu, flux_up_jac=True)
+    go1 = ko.gas_optics_lw(atm["play"], atm["plev"], atm["tlay"], atm["tsfc"] + 1.0, atm["gases"], atm["tlev"])
+    up1, _ = oracle_mod.rte_lw(bl, go1["tau"], top_at_1, go1, emis, None, nmu)
+    np.testing.assert_allclose(jac, up1 - up, rtol=1e-9, atol=1e-9 * np.max(np.abs(jac)))
+    kd = api.Gas_optics_rrtmgp(tables["lw"], S.ATM_GASES)
+    src = {k: T(v, dt, gpu) for k, v in go.items()}
+    gu, gd, gj = api.Rte_lw.rte_lw(kd.bands, src["tau"], top_at_1, src, T(emis, dt, gpu), None, nmu,
+                                   flux_up_jac=True)
+    torch.cuda.synchronize()
+    cmp_flux("flux_up", N(gu), up, prec)
+    cmp_flux("flux_dn", N(gd), dn, prec)
+    cmp_flux("flux_up_jac", N(gj), jac, prec)
+    assert np.max(jac) > 0
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+@pytest.mark.parametrize("top_at_1", [True, False])
 @pytest.mark.parametrize("with_dif", [False, True])
 def test_rte_sw(api, oracle_mod, tables, gpu, prec, top_at_1, with_dif):
     dt = dtypes()[prec]
@@ -372,17 +402,24 @@ def _gas_optics_and_rte(api, oracle_mod, tables, gpu, prec, ncol, nlay, top_at_1
 
 
 def test_rte_sw_workspace_required(api, tables, gpu):
+    """Columns deeper than the on-chip solver's limit (256 layers in FP32) need the caller's
+    workspace and are refused without one; shallower columns need none."""
     import torch
     from rrtmgp_b200._abi import RrtmgpError, ERR_WORKSPACE
     kd = api.Gas_optics_rrtmgp(tables["sw"], S.ATM_GASES)
-    z = torch.zeros((224, 3, 2), dtype=torch.float32, device=gpu)
     m = torch.ones(2, dtype=torch.float32, device=gpu)
     a = torch.zeros((2, 14), dtype=torch.float32, device=gpu)
     s = torch.ones((224, 2), dtype=torch.float32, device=gpu)
     small = torch.empty(16, dtype=torch.uint8, device=gpu)
+    deep = torch.zeros((224, 257, 2), dtype=torch.float32, device=gpu)
     with pytest.raises(RrtmgpError) as e:
-        api.Rte_sw.rte_sw(kd.bands, z, z, z, True, m, s, a, a, workspace=small)
+        api.Rte_sw.rte_sw(kd.bands, deep, deep, deep, True, m, s, a, a, workspace=small)
     assert e.value.status == ERR_WORKSPACE
+    none = torch.empty(0, dtype=torch.uint8, device=gpu)
+    z = torch.zeros((224, 3, 2), dtype=torch.float32, device=gpu)
+    up, dn, dr = api.Rte_sw.rte_sw(kd.bands, z, z, z, True, m, s, a, a, workspace=none)
+    torch.cuda.synchronize()
+    assert torch.allclose(dr[:, -1, :], s)   # tau = 0: the direct beam reaches the surface unchanged
 
 
 @pytest.mark.parametrize("prec", ["f32", "f64"])

@@ -407,6 +407,30 @@ int rrtmgp_b200_heating_rate_f32(int ncol, int nlay, const float* flux_up, const
         const float* plev, float* heating_rate, void* stream);
 int rrtmgp_b200_heating_rate_f64(int ncol, int nlay, const double* flux_up,
         const double* flux_dn, const double* plev, double* heating_rate, void* stream);
+/* Heating rates from per-layer absorbed flux (no reference counterpart; the reference leaves
+ * heating rates to the caller): the per-stage solvers' layer terms are recomputed from their
+ * inputs and the absorbed flux sum_g A_g is accumulated in FP64, so FP32 inputs keep their
+ * accuracy in layers of ~0.1 Pa where a difference of FP32 level fluxes loses ~1 K/day.
+ * Longwave (one angle, as rte_lw with n_gauss_angles = 1): A_g = (1 - T)(F_dn(top) +
+ * F_up(bottom)) - pi (S_dn + S_up) from tau and the Planck sources; shortwave: A_g =
+ * F_dir(top)(1 - Tn - Rdir - Tdir) + (F_dn(top) - F_dir(top) + F_up(bottom))(1 - R - T) from
+ * tau, ssa, g and mu0.  g-point arrays as rte_lw / rte_sw; heating_rate (ncol, nlay) K/day. */
+int rrtmgp_b200_heating_rate_lw_layers_f32(int ncol, int nlay, int ngpt, int top_at_1,
+        const float* tau, const float* lay_src, const float* lev_src_inc, const float* lev_src_dec,
+        const float* gpt_flux_up, const float* gpt_flux_dn, const float* plev, float* heating_rate,
+        void* stream);
+int rrtmgp_b200_heating_rate_lw_layers_f64(int ncol, int nlay, int ngpt, int top_at_1,
+        const double* tau, const double* lay_src, const double* lev_src_inc,
+        const double* lev_src_dec, const double* gpt_flux_up, const double* gpt_flux_dn,
+        const double* plev, double* heating_rate, void* stream);
+int rrtmgp_b200_heating_rate_sw_layers_f32(int ncol, int nlay, int ngpt, int top_at_1,
+        const float* tau, const float* ssa, const float* g, const float* mu0, const float* gpt_flux_up,
+        const float* gpt_flux_dn, const float* gpt_flux_dir, const float* plev, float* heating_rate,
+        void* stream);
+int rrtmgp_b200_heating_rate_sw_layers_f64(int ncol, int nlay, int ngpt, int top_at_1,
+        const double* tau, const double* ssa, const double* g, const double* mu0,
+        const double* gpt_flux_up, const double* gpt_flux_dn, const double* gpt_flux_dir,
+        const double* plev, double* heating_rate, void* stream);
 
 /* ------------------------------------------------------------------------------------ */
 /* Fused column forward (FP32 product path)                                              */

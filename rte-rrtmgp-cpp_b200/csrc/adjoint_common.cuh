@@ -42,7 +42,10 @@ struct __align__(16) DRec {
     float4 fmT, fmH, fmO;   // d fminor / dx on the minor corners (lo.x, lo.y, hi.x, hi.y)
     float4 dB;              // LW: dB/dT of the band Planck function at T_lay, T_top, T_bot, T_sfc
                             // SW: d col_rayl / d vmr_h2o in x
+    float4 pad;             // 272 bytes: an odd number of 16-byte units (bank-conflict-free stores
+                            // of consecutive records, as Rec)
 };                          // (minor scalings and their derivatives: layer_minor_scalings_d)
+static_assert(sizeof(DRec) == 272, "DRec stride");
 
 __device__ __forceinline__ float dot4(const float4& a, const float4& b)
 {
@@ -195,7 +198,8 @@ __device__ __forceinline__ void layer_minor_scalings_d(const KdistView<float>& k
 
 // Adjoint of tau_abs for g-point g: accumulates tau_bar * dtau/dx into gT, gH, gO.  c0, c1:
 // the g-point's kmaj4 corners of the record's two rows (loaded by the caller, early); sc4:
-// the layer's scaling table (layer_minor_scalings_d).
+// the layer's scaling table (layer_minor_scalings_d).  DENSE as tau_abs.
+template <bool DENSE = false>
 __device__ __forceinline__ void tau_abs_adjoint(const KdistView<float>& k, const Rec& R, const DRec& D, int g,
                                                 int4 mg, int nmax, float tb, const float4& c0, const float4& c1,
                                                 const float4* sc4, float& gT, float& gH, float& gO)
@@ -221,7 +225,8 @@ __device__ __forceinline__ void tau_abs_adjoint(const KdistView<float>& k, const
 #pragma unroll
     for (int n = 0; n < 3; ++n)
         if (n < nmax) term(n == 0 ? mg.y : (n == 1 ? mg.z : mg.w), n < mg.x);
-    for (int n = 3; n < nmax; ++n) term(minor_code_at(k, R.a, mg, g, n), n < mg.x);   // dense layouts
+    if constexpr (DENSE)
+        for (int n = 3; n < nmax; ++n) term(minor_code_at(k, R.a, mg, g, n), n < mg.x);
     gT += tb * dT;
     gH += tb * dH;
     gO += tb * dO;

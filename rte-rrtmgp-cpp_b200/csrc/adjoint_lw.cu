@@ -150,7 +150,8 @@ __device__ __forceinline__ Tp* remote(cg::cluster_group& cl, Tp* p, int rank)
 // the cluster code).  CTA r of the cluster owns the layers [r LPC, (r + 1) LPC), LPC = NWc CL,
 // as NWc warps of CL layers; chunk maps and the surface source are pushed to every CTA of the
 // cluster through distributed shared memory.
-template <int CL, bool CLUSTER, bool FLUX>
+// DENSE: more than three minor intervals over some g-point (tau_abs).
+template <int CL, bool CLUSTER, bool FLUX, bool DENSE>
 __global__ void __launch_bounds__(CL == 16 ? 256 : 512, 1)
 lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjCloud cld, int ncol, int nlay, int CS,
                   int idx_o3, int cd_internal, const float* __restrict__ play, const float* __restrict__ plev,
@@ -307,7 +308,7 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
             vtau[i] = 0.f; vpf[i] = 0.f; omt[i] = 0.f; sdn[i] = 0.f; sup[i] = 0.f;
             if (j < nlay && gv) {
                 const Rec& R = recs[slot * CL + i];
-                const float tau = tau_abs(k, R, g, R.a ? mg1 : mg0, R.a ? nm1 : nm0,
+                const float tau = tau_abs<DENSE>(k, R, g, R.a ? mg1 : mg0, R.a ? nm1 : nm0,
                                           &sm_sc4[jl * k.max_nscal].x, 4) + R.aux.w;
                 const float4 p0 = __ldg(k.pfrac4 + (R.kb.x + g));
                 const float4 p1 = __ldg(k.pfrac4 + (R.kb.y + g));
@@ -453,7 +454,7 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
                     gTs += Sbar * pf_bottom * DR.dB.w;
                 }
                 float gh = 0.f, go = 0.f;
-                tau_abs_adjoint(k, R, DR, g, R.a ? mg1 : mg0, R.a ? nm1 : nm0, tb, c0, c1, sm_sc4 + jl * k.max_nscal,
+                tau_abs_adjoint<DENSE>(k, R, DR, g, R.a ? mg1 : mg0, R.a ? nm1 : nm0, tb, c0, c1, sm_sc4 + jl * k.max_nscal,
                                 gt, gh, go);
                 gt += pfb * (dot4(DR.pT0, p0) + dot4(DR.pT1, p1));
                 gh += pfb * (dot4(DR.pH0, p0) + dot4(DR.pH1, p1));
@@ -593,7 +594,7 @@ lw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const AdjClo
 
 // Up to 128 layers (CL = 8) or 256 (CL = 16, if the records fit) one CTA of ceil(nlay / CL)
 // warps per column; beyond, clusters of CS = ceil(nlay / 128) CTAs of 16 warps (CL = 8).
-template <int CL, bool FLUX>
+template <int CL, bool FLUX, bool DENSE>
 int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay, int idx_o3, const float* play,
                       const float* plev, const float* tlay, const float* tlev, const float* tsfc, const float* col_dry,
                       const GasSet<float>& gs, const float* lwp, const float* iwp, const float* rel, const float* rei,
@@ -616,10 +617,10 @@ int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
     if (smem > 227 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_lw: shared memory need exceeds 227 KB");
     static PerDeviceOnce attr;
     const int ast = attr.run([] {
-        const cudaError_t e = cudaFuncSetAttribute(lw_adjoint_kernel<CL, false, FLUX>,
+        const cudaError_t e = cudaFuncSetAttribute(lw_adjoint_kernel<CL, false, FLUX, DENSE>,
                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         if (e != cudaSuccess) return e;
-        return cudaFuncSetAttribute(lw_adjoint_kernel<8, true, FLUX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        return cudaFuncSetAttribute(lw_adjoint_kernel<8, true, FLUX, DENSE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     227 * 1024);
     }, "adjoint_lw attribute");
     if (ast) return ast;
@@ -631,7 +632,7 @@ int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
         ca.present = 1;
     }
     if (CS == 1) {
-        lw_adjoint_kernel<CL, false, FLUX><<<ncol, NWc * 32, smem, stream>>>(v, gs, ca, ncol, nlay, 1, idx_o3, col_dry ? 0 : 1,
+        lw_adjoint_kernel<CL, false, FLUX, DENSE><<<ncol, NWc * 32, smem, stream>>>(v, gs, ca, ncol, nlay, 1, idx_o3, col_dry ? 0 : 1,
                                                                   play, plev, tlay, tlev, tsfc, col_dry, emis, su, sd,
                                                                   sh, out);
         RB_LAUNCH("lw_adjoint_kernel");
@@ -649,7 +650,7 @@ int launch_lw_adjoint(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    RB_CUDA(cudaLaunchKernelEx(&cfg, lw_adjoint_kernel<8, true, FLUX>, v, gs, ca, ncol, nlay, CS, idx_o3, col_dry ? 0 : 1, play,
+    RB_CUDA(cudaLaunchKernelEx(&cfg, lw_adjoint_kernel<8, true, FLUX, DENSE>, v, gs, ca, ncol, nlay, CS, idx_o3, col_dry ? 0 : 1, play,
                                plev, tlay, tlev, tsfc, col_dry, emis, su, sd, sh, out),
             "lw_adjoint_kernel launch");
     return RRTMGP_B200_OK;
@@ -685,11 +686,16 @@ int adjoint_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     const AdjOut out{g_tlay, g_tlev, g_tsfc, g_h2o, g_o3, g_lwp, g_iwp, g_rel, g_rei,
                      flux_up, flux_dn, flux_net, heating_rate};
     cudaStream_t s = as_stream(stream);
-#define RB_LW_ADJ(CLv, F)                                                                                          \
-    launch_lw_adjoint<CLv, F>(k, c, ncol, nlay, idx_o3, play, plev, tlay, tlev, tsfc, col_dry, gs, lwp, iwp, rel, \
-                              rei, sfc_emis, seed_up, seed_dn, seed_hr, out, s)
-    if (chunk == 16) return with_flux ? RB_LW_ADJ(16, true) : RB_LW_ADJ(16, false);
-    return with_flux ? RB_LW_ADJ(8, true) : RB_LW_ADJ(8, false);
+    const bool dense = v.max_minor_per_g > 3;
+#define RB_LW_ADJ(CLv, F, D)                                                                                        \
+    launch_lw_adjoint<CLv, F, D>(k, c, ncol, nlay, idx_o3, play, plev, tlay, tlev, tsfc, col_dry, gs, lwp, iwp, rel, \
+                                 rei, sfc_emis, seed_up, seed_dn, seed_hr, out, s)
+    if (dense) {
+        if (chunk == 16) return with_flux ? RB_LW_ADJ(16, true, true) : RB_LW_ADJ(16, false, true);
+        return with_flux ? RB_LW_ADJ(8, true, true) : RB_LW_ADJ(8, false, true);
+    }
+    if (chunk == 16) return with_flux ? RB_LW_ADJ(16, true, false) : RB_LW_ADJ(16, false, false);
+    return with_flux ? RB_LW_ADJ(8, true, false) : RB_LW_ADJ(8, false, false);
 #undef RB_LW_ADJ
 }
 

@@ -339,6 +339,7 @@ struct LayerAdj {
     float tc, tsc, tsg;     // adjoints of the cloud tau, tau*ssa, tau*ssa*g
 };
 
+template <bool DENSE>
 __device__ __noinline__ LayerAdj sw_layer_adjoint(const float4* __restrict__ kmaj4, const float2* __restrict__ kmin,
                                                   const float2* __restrict__ krayl2, const Rec* Rc, const DRec* DR,
                                                   const float4* sc4, const int* gx, int g, int4 mg, int nmax,
@@ -380,12 +381,14 @@ __device__ __noinline__ LayerAdj sw_layer_adjoint(const float4* __restrict__ kma
 #pragma unroll
     for (int n = 0; n < 3; ++n)
         if (n < nmax) minor_term(minor_code(mg, n), cr[n], n < mg.x);
-    for (int n = 3; n < nmax; ++n) {   // dense layouts: more than three intervals over g
-        const int code = n < mg.x ? gx[n - 3] : mg.y;
-        const int c = code >> kScalBits;
-        const float2 lo = __ldg(kmin + (Rc->kb.z + c));
-        const float2 hi = __ldg(kmin + (Rc->kb.w + c));
-        minor_term(code, make_float4(lo.x, lo.y, hi.x, hi.y), n < mg.x);
+    if constexpr (DENSE) {   // more than three intervals over some g-point
+        for (int n = 3; n < nmax; ++n) {
+            const int code = n < mg.x ? gx[n - 3] : mg.y;
+            const int c = code >> kScalBits;
+            const float2 lo = __ldg(kmin + (Rc->kb.z + c));
+            const float2 hi = __ldg(kmin + (Rc->kb.w + c));
+            minor_term(code, make_float4(lo.x, lo.y, hi.x, hi.y), n < mg.x);
+        }
     }
     const float tab = la.ta, trb = la.tr;
     LayerAdj r{tab * dT, tab * dH, tab * dO, la.tc, la.tsc, la.tsg};
@@ -401,6 +404,7 @@ __device__ __noinline__ LayerAdj sw_layer_adjoint(const float4* __restrict__ kma
 // forward kernel's pass 1 (sw_column.cuh), out of line for the same reason.
 struct LayerFwd { float tau, w0, omw, gasy, R, T, Rdir, Tdir, Tn, adif, adir; };
 
+template <bool DENSE>
 __device__ __noinline__ LayerFwd sw_layer_forward(const float4* __restrict__ kmaj4, const float2* __restrict__ kmin,
                                                   const float2* __restrict__ krayl2, const Rec* Rc, const float4* sc4,
                                                   const int* gx, int g, int4 mg, int nmax, float mu0, float mu0_inv)
@@ -419,7 +423,8 @@ __device__ __noinline__ LayerFwd sw_layer_forward(const float4* __restrict__ kma
 #pragma unroll
     for (int n = 0; n < 3; ++n)
         if (n < nmax) minor_term(minor_code(mg, n), n < mg.x);
-    for (int n = 3; n < nmax; ++n) minor_term(n < mg.x ? gx[n - 3] : mg.y, n < mg.x);   // dense layouts
+    if constexpr (DENSE)
+        for (int n = 3; n < nmax; ++n) minor_term(n < mg.x ? gx[n - 3] : mg.y, n < mg.x);
     LayerFwd o;
     const float2 r0 = __ldg(krayl2 + (Rc->kr[0] + g));
     const float2 r1 = __ldg(krayl2 + (Rc->kr[1] + g));
@@ -525,7 +530,8 @@ __device__ __forceinline__ Tp* remote(cg::cluster_group& cl, Tp* p, int rank)
 
 // CL layers per warp, kLPC / CL warps per CTA: CL = 8 gives 8 warps with up to 255 registers,
 // CL = 4 gives 16 warps at 128 registers (half the per-layer values per thread).
-template <int CL, bool FLUX, bool PAIR>
+// DENSE: more than three minor intervals over some g-point (sw_layer_forward/adjoint).
+template <int CL, bool FLUX, bool PAIR, bool DENSE>
 __global__ void __launch_bounds__(kLPC / CL * 32, 1)
 sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwCloudArgs cld, int ncol, int nlay, int CS,
                   int idx_o3, int cd_internal, const float* __restrict__ play, const float* __restrict__ plev,
@@ -682,7 +688,7 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
             float tau = 0.f, w0 = 0.f, omw = 1.f, gasy = 0.f;
             if (j < nlay && gv) {
                 const Rec& Rc = recs[slot * CL + i];
-                const LayerFwd lf = sw_layer_forward(k.kmaj4, k.kmin2[Rc.a], k.krayl2, &Rc, sm_sc4 + jl * k.max_nscal,
+                const LayerFwd lf = sw_layer_forward<DENSE>(k.kmaj4, k.kmin2[Rc.a], k.krayl2, &Rc, sm_sc4 + jl * k.max_nscal,
                                                      k.minor_gx[Rc.a] + size_t(g) * k.minor_gx_stride, g,
                                                      Rc.a ? mg1 : mg0, Rc.a ? nm1 : nm0, mu0, mu0_inv);
                 tau = lf.tau; w0 = lf.w0; omw = lf.omw; gasy = lf.gasy;
@@ -946,7 +952,7 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
             gT[i] = 0.f; gH[i] = 0.f; gO[i] = 0.f; gC0[i] = 0.f; gC1[i] = 0.f; gC2[i] = 0.f;
             if (j < nlay && gv) {
                 const Rec& Rc = recs[slot * CL + i];
-                const LayerAdj la = sw_layer_adjoint(k.kmaj4, k.kmin2[Rc.a], k.krayl2, &Rc, &drecs[slot * CL + i],
+                const LayerAdj la = sw_layer_adjoint<DENSE>(k.kmaj4, k.kmin2[Rc.a], k.krayl2, &Rc, &drecs[slot * CL + i],
                                                      sm_sc4 + jl * k.max_nscal,
                                                      k.minor_gx[Rc.a] + size_t(g) * k.minor_gx_stride, g,
                                                      Rc.a ? mg1 : mg0, Rc.a ? nm1 : nm0, vTau[i], vW0[i], vOmw[i],
@@ -1120,8 +1126,10 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     if (smem > 227 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_sw: shared memory need exceeds 227 KB");
     static PerDeviceOnce attr;
     const int ast = attr.run([] {
-        for (auto fn : {sw_adjoint_kernel<CL, false, false>, sw_adjoint_kernel<CL, true, false>,
-                        sw_adjoint_kernel<CL, false, true>, sw_adjoint_kernel<CL, true, true>}) {
+        for (auto fn : {sw_adjoint_kernel<CL, false, false, false>, sw_adjoint_kernel<CL, true, false, false>,
+                        sw_adjoint_kernel<CL, false, true, false>, sw_adjoint_kernel<CL, true, true, false>,
+                        sw_adjoint_kernel<CL, false, false, true>, sw_adjoint_kernel<CL, true, false, true>,
+                        sw_adjoint_kernel<CL, false, true, true>, sw_adjoint_kernel<CL, true, true, true>}) {
             const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
             if (e != cudaSuccess) return e;
         }
@@ -1150,8 +1158,13 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    const auto kernel = with_flux ? (pair ? sw_adjoint_kernel<CL, true, true> : sw_adjoint_kernel<CL, true, false>)
-                                  : (pair ? sw_adjoint_kernel<CL, false, true> : sw_adjoint_kernel<CL, false, false>);
+    const bool dense = v.max_minor_per_g > 3;
+    const auto kernel =
+        dense ? (with_flux ? (pair ? sw_adjoint_kernel<CL, true, true, true> : sw_adjoint_kernel<CL, true, false, true>)
+                           : (pair ? sw_adjoint_kernel<CL, false, true, true> : sw_adjoint_kernel<CL, false, false, true>))
+              : (with_flux ? (pair ? sw_adjoint_kernel<CL, true, true, false> : sw_adjoint_kernel<CL, true, false, false>)
+                           : (pair ? sw_adjoint_kernel<CL, false, true, false>
+                                   : sw_adjoint_kernel<CL, false, false, false>));
     RB_CUDA(cudaLaunchKernelEx(&cfg, kernel, v, gs, ca, ncol, nlay, CS, idx_o3, col_dry ? 0 : 1, play, plev,
                                tlay, col_dry, mu0, tsi_scaling, sfc_alb_dir, sfc_alb_dif, seed_up, seed_dn, seed_dir,
                                seed_hr, out),

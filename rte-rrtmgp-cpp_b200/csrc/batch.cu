@@ -117,6 +117,8 @@ struct SwItemIo : ItemIo {
     }
 };
 
+// DENSE: a k-distribution with more than three minor intervals over some g-point (tau_abs).
+template <bool DENSE>
 __global__ void __launch_bounds__(kBatchThreads, 1)
 batch_forward_kernel(const KdistView<float> klw, const KdistView<float> ksw, const BatchItem* __restrict__ items,
                      const long long* __restrict__ tile_start, int nitems, unsigned long long* __restrict__ counter)
@@ -169,15 +171,15 @@ batch_forward_kernel(const KdistView<float> klw, const KdistView<float> ksw, con
             if (domain == 0) {
                 const ItemIo io{nc, nl};
                 if (cl == 8)
-                    lw_forward_column<8>(cx, klw, io);
+                    lw_forward_column<8, false, DENSE>(cx, klw, io);
                 else
-                    lw_forward_column<16>(cx, klw, io);
+                    lw_forward_column<16, false, DENSE>(cx, klw, io);
             } else {
                 const SwItemIo io{{nc, nl}};
                 if (cl == 8)
-                    sw_forward_column<8, true>(cx, ksw, io);
+                    sw_forward_column<8, true, DENSE>(cx, ksw, io);
                 else
-                    sw_forward_column<16>(cx, ksw, io);
+                    sw_forward_column<16, false, DENSE>(cx, ksw, io);
             }
         }
         __syncthreads();
@@ -232,6 +234,7 @@ struct rrtmgp_b200_batch_t {
     std::vector<BatchItem> items;      // unplanned items (cl, W, P, team_smem set by plan())
     TileShape shape[2][kMaxBins + 1];  // [domain][bin]
     int nsm = 0, device = 0;
+    bool dense = false;                // a k-distribution needs the DENSE kernel
     int max_smem = 0;                  // dynamic shared memory per CTA the kernel may use
     // planned state
     bool dirty = true;
@@ -387,7 +390,10 @@ int launch_persistent(rrtmgp_b200_batch_t* b, const BatchItem* d_items, const lo
     const int ctas = int(std::min<long long>(b->nsm, std::max<long long>(ntiles, 1)));
     const KdistView<float> klw = b->k[0] ? b->k[0]->v32 : KdistView<float>{};
     const KdistView<float> ksw = b->k[1] ? b->k[1]->v32 : KdistView<float>{};
-    batch_forward_kernel<<<ctas, kBatchThreads, smem, s>>>(klw, ksw, d_items, d_starts, nitems, b->d_counter);
+    if (b->dense)
+        batch_forward_kernel<true><<<ctas, kBatchThreads, smem, s>>>(klw, ksw, d_items, d_starts, nitems, b->d_counter);
+    else
+        batch_forward_kernel<false><<<ctas, kBatchThreads, smem, s>>>(klw, ksw, d_items, d_starts, nitems, b->d_counter);
     RB_LAUNCH("batch_forward_kernel");
     return RRTMGP_B200_OK;
 }
@@ -507,10 +513,12 @@ int batch_create(rrtmgp_b200_kdist klw, rrtmgp_b200_cloud clw, rrtmgp_b200_kdist
     RB_CUDA(cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->device), "batch_create");
     int optin = 0;
     RB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device), "batch_create");
+    b->dense = (klw && klw->v32.max_minor_per_g > 3) || (ksw && ksw->v32.max_minor_per_g > 3);
+    const auto kernel = b->dense ? batch_forward_kernel<true> : batch_forward_kernel<false>;
     cudaFuncAttributes fa{};
-    RB_CUDA(cudaFuncGetAttributes(&fa, batch_forward_kernel), "batch_create");
+    RB_CUDA(cudaFuncGetAttributes(&fa, kernel), "batch_create");
     b->max_smem = optin - int(fa.sharedSizeBytes);
-    RB_CUDA(cudaFuncSetAttribute(batch_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, b->max_smem),
+    RB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, b->max_smem),
             "batch_create: kernel attribute");
     for (const BatchItem& it : b->items)
         if (!shape_for(b.get(), it.domain, it.nlay).cl)

@@ -7,13 +7,14 @@ namespace {
 
 using namespace fused;
 
-template <int CL>
+// DENSE: tables with more than three minor intervals over some g-point (tau_abs).
+template <int CL, bool DENSE>
 __global__ void __launch_bounds__(512) lw_forward_kernel(const KdistView<float> k, const LwGridIo io)
 {
-    lw_forward_column<CL, true>(CtaCtx{}, k, io);
+    lw_forward_column<CL, true, DENSE>(CtaCtx{}, k, io);
 }
 
-template <int CL>
+template <int CL, bool DENSE>
 int launch_lw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay, const float* play,
                       const float* plev, const float* tlay, const float* tlev, const float* tsfc, const float* col_dry,
                       const GasSet<float>& gs, const float* lwp, const float* iwp, const float* rel, const float* rei,
@@ -26,7 +27,7 @@ int launch_lw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
         smem_layout(nlay, v.ngas, v.nband, 1, NW, 2, CL, v.max_group_bands * (CL == 8 ? 2 : 1), v.max_nscal).total;
     if (smem > 220 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "forward_lw: shared memory need exceeds 220 KB");
     static PerDeviceOnce attr;
-    int st = attr.run([] { return cudaFuncSetAttribute(lw_forward_kernel<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    int st = attr.run([] { return cudaFuncSetAttribute(lw_forward_kernel<CL, DENSE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                        220 * 1024); }, "forward_lw attribute");
     if (st) return st;
     CloudArgs ca{};
@@ -37,7 +38,7 @@ int launch_lw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
         ca.present = 1;
     }
     LwGridIo io{ncol, nlay, play, plev, tlay, tlev, tsfc, col_dry, emis, up, dn, net, hr, gs, ca};
-    lw_forward_kernel<CL><<<ncol, NW * 32, smem, stream>>>(v, io);
+    lw_forward_kernel<CL, DENSE><<<ncol, NW * 32, smem, stream>>>(v, io);
     RB_LAUNCH("lw_forward_kernel");
     return RRTMGP_B200_OK;
 }
@@ -64,11 +65,13 @@ int forward_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     int st = make_gas_set<float>(k, ncol, nlay, gases, ngases, gs);
     if (st) return st;
     cudaStream_t s = as_stream(stream);
-    if (chunk == 8)
-        return launch_lw_forward<8>(k, c, ncol, nlay, play, plev, tlay, tlev, tsfc, col_dry, gs, lwp, iwp, rel, rei,
-                                    sfc_emis, flux_up, flux_dn, flux_net, heating_rate, s);
-    return launch_lw_forward<16>(k, c, ncol, nlay, play, plev, tlay, tlev, tsfc, col_dry, gs, lwp, iwp, rel, rei,
-                                 sfc_emis, flux_up, flux_dn, flux_net, heating_rate, s);
+    const bool dense = v.max_minor_per_g > 3;
+#define RB_LW_FWD(CLv, D)                                                                                          \
+    launch_lw_forward<CLv, D>(k, c, ncol, nlay, play, plev, tlay, tlev, tsfc, col_dry, gs, lwp, iwp, rel, rei, \
+                              sfc_emis, flux_up, flux_dn, flux_net, heating_rate, s)
+    if (chunk == 8) return dense ? RB_LW_FWD(8, true) : RB_LW_FWD(8, false);
+    return dense ? RB_LW_FWD(16, true) : RB_LW_FWD(16, false);
+#undef RB_LW_FWD
 }
 
 }  // namespace rrtmgp_b200

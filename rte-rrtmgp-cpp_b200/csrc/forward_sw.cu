@@ -7,13 +7,14 @@ namespace {
 
 using namespace fused;
 
-template <int CL>
+// DENSE: tables with more than three minor intervals over some g-point (tau_abs).
+template <int CL, bool DENSE>
 __global__ void __launch_bounds__(512) sw_forward_kernel(const KdistView<float> k, const SwGridIo io)
 {
-    sw_forward_column<CL, true>(CtaCtx{}, k, io);
+    sw_forward_column<CL, true, DENSE>(CtaCtx{}, k, io);
 }
 
-template <int CL>
+template <int CL, bool DENSE>
 int launch_sw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay, const float* play,
                       const float* plev, const float* tlay, const float* col_dry, const GasSet<float>& gs,
                       const float* lwp, const float* iwp, const float* rel, const float* rei, int delta,
@@ -27,7 +28,7 @@ int launch_sw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
         smem_layout(nlay, v.ngas, v.nband, 0, NW, 3, CL, v.max_group_bands * (CL == 8 ? 2 : 1), v.max_nscal).total;
     if (smem > 220 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "forward_sw: shared memory need exceeds 220 KB");
     static PerDeviceOnce attr;
-    int st = attr.run([] { return cudaFuncSetAttribute(sw_forward_kernel<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    int st = attr.run([] { return cudaFuncSetAttribute(sw_forward_kernel<CL, DENSE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                        220 * 1024); }, "forward_sw attribute");
     if (st) return st;
     SwCloudArgs ca{};
@@ -39,7 +40,7 @@ int launch_sw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
         ca.delta = delta;
     }
     SwGridIo io{ncol, nlay, play, plev, tlay, col_dry, mu0, tsi, alb_dir, alb_dif, up, dn, dir, net, hr, gs, ca};
-    sw_forward_kernel<CL><<<ncol, NW * 32, smem, stream>>>(v, io);
+    sw_forward_kernel<CL, DENSE><<<ncol, NW * 32, smem, stream>>>(v, io);
     RB_LAUNCH("sw_forward_kernel");
     return RRTMGP_B200_OK;
 }
@@ -68,13 +69,14 @@ int forward_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     if (st) return st;
     cudaStream_t s = as_stream(stream);
     const int cl = chunk ? chunk : (nlay > 128 ? 16 : 8);
-    if (cl == 16)
-        return launch_sw_forward<16>(k, c, ncol, nlay, play, plev, tlay, col_dry, gs, lwp, iwp, rel, rei, delta_cloud,
-                                     mu0, tsi_scaling, sfc_alb_dir, sfc_alb_dif, flux_up, flux_dn, flux_dn_dir,
-                                     flux_net, heating_rate, s);
-    return launch_sw_forward<8>(k, c, ncol, nlay, play, plev, tlay, col_dry, gs, lwp, iwp, rel, rei, delta_cloud, mu0,
-                                tsi_scaling, sfc_alb_dir, sfc_alb_dif, flux_up, flux_dn, flux_dn_dir, flux_net,
-                                heating_rate, s);
+    const bool dense = v.max_minor_per_g > 3;
+#define RB_SW_FWD(CLv, D)                                                                                           \
+    launch_sw_forward<CLv, D>(k, c, ncol, nlay, play, plev, tlay, col_dry, gs, lwp, iwp, rel, rei, delta_cloud, mu0, \
+                              tsi_scaling, sfc_alb_dir, sfc_alb_dif, flux_up, flux_dn, flux_dn_dir, flux_net,         \
+                              heating_rate, s)
+    if (cl == 16) return dense ? RB_SW_FWD(16, true) : RB_SW_FWD(16, false);
+    return dense ? RB_SW_FWD(8, true) : RB_SW_FWD(8, false);
+#undef RB_SW_FWD
 }
 
 }  // namespace rrtmgp_b200

@@ -38,7 +38,10 @@ struct __align__(16) Rec {
                            // SW: cloud absorption optical depth tau_c * (1 - ssa_c)
     int a;                 // 0 lower / 1 upper atmosphere
     int kr[2];             // element offsets (row * ngpt) of the krayl2 rows of (a, t0, e0), (a, t1, e1)
+    int4 pad;              // 144 bytes: an odd number of 16-byte units, so that the 128-bit stores of
+                           // 32 lanes building consecutive records spread over all 32 banks
 };
+static_assert(sizeof(Rec) == 144, "Rec stride");
 
 // Reduce-scatter of N per-lane values over 32 lanes: afterwards lane L holds in v[0] the warp
 // total of value L >> log2(32 / N) (N <= 32, a power of two).
@@ -157,7 +160,11 @@ __device__ __forceinline__ int minor_code_at(const KdistView<float>& k, int a, c
 // plus the minor intervals covering g (minor_g list), as gas_optical_depths_major/minor.
 // nmax = most intervals over the warp's lanes (warp-uniform loop bound); lanes with fewer
 // intervals read a valid entry and discard it with a select, so the loop does not diverge.
-// sc: the layer's scalings, kind sid at sc[sid * sst].
+// sc: the layer's scalings, kind sid at sc[sid * sst].  DENSE: tables with more than three
+// intervals over some g-point (KdistView::max_minor_per_g > 3); the loop over the further
+// intervals is compiled only then, so that for the usual layouts the whole function stays
+// straight-line code whose table loads the caller's unrolled layer loop can overlap.
+template <bool DENSE = false>
 __device__ __forceinline__ float tau_abs(const KdistView<float>& k, const Rec& R, int g, int4 mg, int nmax,
                                          const float* sc, int sst = 1)
 {
@@ -178,14 +185,16 @@ __device__ __forceinline__ float tau_abs(const KdistView<float>& k, const Rec& R
             tau += (n < mg.x) ? t : 0.f;
         }
     }
-    for (int n = 3; n < nmax; ++n) {   // dense layouts: more than three intervals over g
-        const int code = minor_code_at(k, R.a, mg, g, n);
-        const int c = code >> kScalBits;
-        const float2 lo = __ldg(kn + (R.kb.z + c));
-        const float2 hi = __ldg(kn + (R.kb.w + c));
-        const float t = sc[(code & (kMaxScal - 1)) * sst] *
-                        (R.fm.x * lo.x + R.fm.y * lo.y + R.fm.z * hi.x + R.fm.w * hi.y);
-        tau += (n < mg.x) ? t : 0.f;
+    if constexpr (DENSE) {
+        for (int n = 3; n < nmax; ++n) {
+            const int code = minor_code_at(k, R.a, mg, g, n);
+            const int c = code >> kScalBits;
+            const float2 lo = __ldg(kn + (R.kb.z + c));
+            const float2 hi = __ldg(kn + (R.kb.w + c));
+            const float t = sc[(code & (kMaxScal - 1)) * sst] *
+                            (R.fm.x * lo.x + R.fm.y * lo.y + R.fm.z * hi.x + R.fm.w * hi.y);
+            tau += (n < mg.x) ? t : 0.f;
+        }
     }
     return tau;
 }

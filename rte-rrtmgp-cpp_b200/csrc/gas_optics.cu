@@ -173,6 +173,7 @@ __device__ __forceinline__ fused::LayerState thread_layer_state(const LayerInter
     return s;
 }
 
+template <bool DENSE>
 __global__ void __launch_bounds__(kThreads, 7)
 gas_optics_lw_packed_kernel(const KdistView<float> k, const GasSet<float> gases, int ncol, int nlay,
                             const float* __restrict__ play, const float* __restrict__ plev,
@@ -226,7 +227,7 @@ gas_optics_lw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
             const int4 mg0 = nx0, mg1 = nx1;
             nx0 = next_minor_row(k.minor_g[0], g + 1, k.ngpt);
             nx1 = next_minor_row(k.minor_g[1], g + 1, k.ngpt);
-            const float ta = fused::tau_abs(k, R, g, R.a ? mg1 : mg0, max(mg0.x, mg1.x), scal, kThreads);
+            const float ta = fused::tau_abs<DENSE>(k, R, g, R.a ? mg1 : mg0, max(mg0.x, mg1.x), scal, kThreads);
             const float4 p0 = __ldg(k.pfrac4 + (R.kb.x + g));
             const float4 p1 = __ldg(k.pfrac4 + (R.kb.y + g));
             const float pfrac = (wp0.x * p0.x + wp0.y * p0.y + wp0.z * p0.z + wp0.w * p0.w) +
@@ -244,6 +245,7 @@ gas_optics_lw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
     }
 }
 
+template <bool DENSE>
 __global__ void __launch_bounds__(kThreads, 8)
 gas_optics_sw_packed_kernel(const KdistView<float> k, const GasSet<float> gases, int ncol, int nlay,
                             const float* __restrict__ play, const float* __restrict__ plev,
@@ -279,7 +281,7 @@ gas_optics_sw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
             const int4 mg0 = nx0, mg1 = nx1;
             nx0 = next_minor_row(k.minor_g[0], g + 1, k.ngpt);
             nx1 = next_minor_row(k.minor_g[1], g + 1, k.ngpt);
-            const float ta = fused::tau_abs(k, R, g, R.a ? mg1 : mg0, max(mg0.x, mg1.x), scal, kThreads);
+            const float ta = fused::tau_abs<DENSE>(k, R, g, R.a ? mg1 : mg0, max(mg0.x, mg1.x), scal, kThreads);
             const float2 r0 = __ldg(k.krayl2 + (kr0 + g));
             const float2 r1 = __ldg(k.krayl2 + (kr1 + g));
             const float tr = (R.fm.x * r0.x + R.fm.y * r0.y + R.fm.z * r1.x + R.fm.w * r1.y) * col_rayl;
@@ -338,9 +340,11 @@ int gas_optics_lw(rrtmgp_b200_kdist k, int ncol, int nlay, const T* play, const 
     const dim3 block(kBX, kBY), grid(ceil_div(ncol, kBX), ceil_div(nlay, kBY));
     if constexpr (std::is_same<T, float>::value) {
         if (packed_tables_ok(k->v32, true)) {
-            gas_optics_lw_packed_kernel<<<grid, block, packed_smem_bytes(k->info.ngas, k->v32.max_nscal), as_stream(stream)>>>(
-                k->v32, gs, ncol, nlay, play, plev, tlay, tsfc, tlev, col_dry, tau, lay_src, lev_inc, lev_dec,
-                sfc_src, sfc_jac);
+            const size_t psm = packed_smem_bytes(k->info.ngas, k->v32.max_nscal);
+            const auto kernel = k->v32.max_minor_per_g > 3 ? gas_optics_lw_packed_kernel<true>
+                                                           : gas_optics_lw_packed_kernel<false>;
+            kernel<<<grid, block, psm, as_stream(stream)>>>(k->v32, gs, ncol, nlay, play, plev, tlay, tsfc, tlev,
+                                                            col_dry, tau, lay_src, lev_inc, lev_dec, sfc_src, sfc_jac);
             RB_LAUNCH("gas_optics_lw_packed_kernel");
             return RRTMGP_B200_OK;
         }
@@ -378,8 +382,11 @@ int gas_optics_sw(rrtmgp_b200_kdist k, int ncol, int nlay, const T* play, const 
     bool packed = false;
     if constexpr (std::is_same<T, float>::value) {
         if (packed_tables_ok(k->v32, false)) {
-            gas_optics_sw_packed_kernel<<<grid, block, packed_smem_bytes(k->info.ngas, k->v32.max_nscal), as_stream(stream)>>>(
-                k->v32, gs, ncol, nlay, play, plev, tlay, col_dry, tau, ssa, g);
+            const size_t psm = packed_smem_bytes(k->info.ngas, k->v32.max_nscal);
+            const auto kernel = k->v32.max_minor_per_g > 3 ? gas_optics_sw_packed_kernel<true>
+                                                           : gas_optics_sw_packed_kernel<false>;
+            kernel<<<grid, block, psm, as_stream(stream)>>>(k->v32, gs, ncol, nlay, play, plev, tlay, col_dry, tau,
+                                                            ssa, g);
             RB_LAUNCH("gas_optics_sw_packed_kernel");
             packed = true;
         }

@@ -1,0 +1,160 @@
+// Heating rates of the per-stage (class-API) path from per-layer absorbed flux.
+//
+// The reference has no heating-rate routine; a caller differences its broadband level fluxes.
+// In the top layers of a model atmosphere (Delta p ~ 0.1 Pa) one FP32 rounding of a
+// ~1000 W/m2 level flux is worth ~1 K/day, so a difference of FP32 level fluxes cannot give
+// 0.01 K/day there.  These kernels form the heating rate of layer l from the flux the layer
+// absorbs, summed over g-points in FP64:
+//   longwave  A_g = (1 - T) (F_dn,g(top) + F_up,g(bottom)) - pi (S_dn + S_up)   (one angle,
+//             D = 1.66, weight 0.5: the per-stage solver's transmissivity and linear-in-tau
+//             sources recomputed from tau and the Planck sources);
+//   shortwave A_g = F_dir,g(top) (1 - Tn - Rdir - Tdir) + (F_dif,g(top) + F_up,g(bottom)) (1 - R - T)
+//             (the per-stage solver's two-stream coefficients recomputed from tau, ssa, g, mu0;
+//             F_dif = F_dn - F_dir).
+// These equal the net-flux divergence of the solvers' recurrences exactly, but every FP32
+// rounding of a level flux enters multiplied by the layer's absorptance, which is small
+// exactly where the layers are thin.  HR = g/cp 86400 sum_g A_g / |Delta p| as
+// heating_rate_kernel.  One thread per (column, layer), lanes over consecutive columns.
+#include <cfloat>
+
+#include "common.cuh"
+#include "rte_device.cuh"
+#include "sw_common.cuh"
+
+namespace rrtmgp_b200 {
+namespace {
+
+constexpr double kG0OverCp = 9.80665 / 1004.64;
+
+template <typename T> __device__ __forceinline__ T one_minus_exp_neg(T x);
+template <> __device__ __forceinline__ float one_minus_exp_neg<float>(float x) { return -expm1f(-x); }
+template <> __device__ __forceinline__ double one_minus_exp_neg<double>(double x) { return -expm1(-x); }
+
+template <typename T>
+__global__ void heating_rate_lw_layers_kernel(int ncol, int nlay, int ngpt, int top_at_1, const T* __restrict__ tau,
+                                              const T* __restrict__ lay_src, const T* __restrict__ lev_inc,
+                                              const T* __restrict__ lev_dec, const T* __restrict__ up,
+                                              const T* __restrict__ dn, const T* __restrict__ plev,
+                                              T* __restrict__ hr)
+{
+    const int icol = blockIdx.x * blockDim.x + threadIdx.x;
+    const int l = blockIdx.y;
+    if (icol >= ncol) return;
+    const size_t ncl = size_t(ncol) * nlay, ncv = size_t(ncol) * (nlay + 1);
+    const size_t cl = icol + size_t(l) * ncol;
+    const int lt = top_at_1 ? l : l + 1, lb = top_at_1 ? l + 1 : l;
+    const T* lev_dn = top_at_1 ? lev_inc : lev_dec;
+    const T* lev_up = top_at_1 ? lev_dec : lev_inc;
+    const T D = T(1.66), pi = pi_value<T>();
+    double acc = 0.0;
+    for (int g = 0; g < ngpt; ++g) {
+        const size_t i = cl + size_t(g) * ncl;
+        T trans, sdn, sup;
+        lw_layer(tau[i], D, lay_src[i], lev_dn[i], lev_up[i], trans, sdn, sup);
+        const T omt = one_minus_exp_neg(tau[i] * D);
+        const size_t ot = icol + size_t(lt) * ncol + size_t(g) * ncv, ob = icol + size_t(lb) * ncol + size_t(g) * ncv;
+        acc += double(omt * (dn[ot] + up[ob]) - pi * (sdn + sup));
+    }
+    const double dp = fabs(double(plev[icol + size_t(lb) * ncol]) - double(plev[icol + size_t(lt) * ncol]));
+    hr[cl] = T(kG0OverCp * 86400.0 * acc / dp);
+}
+
+// Two-stream coefficients and the layer's direct and diffuse absorptances, as the per-stage
+// shortwave solver computes them.
+template <typename T>
+__device__ __forceinline__ void sw_absorptances(T tau, T ssa, T g, T mu0, T& adir, T& adif);
+template <>
+__device__ __forceinline__ void sw_absorptances<float>(float tau, float ssa, float g, float mu0, float& adir,
+                                                       float& adif)
+{
+    float R, Tt, Rdir, Tdir, Tn;
+    fused::sw_layer_fast(tau, ssa, 1.f - ssa, g, mu0, 1.f / mu0, R, Tt, Rdir, Tdir, Tn, adif, adir);
+}
+template <>
+__device__ __forceinline__ void sw_absorptances<double>(double tau, double ssa, double g, double mu0, double& adir,
+                                                        double& adif)
+{
+    double R, Tt, Rdir, Tdir, Tn;
+    sw_two_stream<double>(tau, ssa, g, mu0, R, Tt, Rdir, Tdir, Tn);
+    adif = 1. - R - Tt;
+    adir = 1. - Tn - Rdir - Tdir;
+}
+
+template <typename T>
+__global__ void heating_rate_sw_layers_kernel(int ncol, int nlay, int ngpt, int top_at_1, const T* __restrict__ tau,
+                                              const T* __restrict__ ssa, const T* __restrict__ gasy,
+                                              const T* __restrict__ mu0, const T* __restrict__ up,
+                                              const T* __restrict__ dn, const T* __restrict__ dir,
+                                              const T* __restrict__ plev, T* __restrict__ hr)
+{
+    const int icol = blockIdx.x * blockDim.x + threadIdx.x;
+    const int l = blockIdx.y;
+    if (icol >= ncol) return;
+    const size_t ncl = size_t(ncol) * nlay, ncv = size_t(ncol) * (nlay + 1);
+    const size_t cl = icol + size_t(l) * ncol;
+    const int lt = top_at_1 ? l : l + 1, lb = top_at_1 ? l + 1 : l;
+    const T m0 = mu0[icol];
+    double acc = 0.0;
+    for (int g = 0; g < ngpt; ++g) {
+        const size_t i = cl + size_t(g) * ncl;
+        T adir, adif;
+        sw_absorptances<T>(tau[i], ssa[i], gasy[i], m0, adir, adif);
+        const size_t ot = icol + size_t(lt) * ncol + size_t(g) * ncv, ob = icol + size_t(lb) * ncol + size_t(g) * ncv;
+        const T fdir = dir[ot];
+        acc += double(fdir * adir + ((dn[ot] - fdir) + up[ob]) * adif);
+    }
+    const double dp = fabs(double(plev[icol + size_t(lb) * ncol]) - double(plev[icol + size_t(lt) * ncol]));
+    hr[cl] = T(kG0OverCp * 86400.0 * acc / dp);
+}
+
+template <typename T>
+int hr_lw_layers(int ncol, int nlay, int ngpt, int top_at_1, const T* tau, const T* lay, const T* inc, const T* dec,
+                 const T* up, const T* dn, const T* plev, T* hr, void* stream)
+{
+    RB_CHECK_ARG(ncol > 0 && nlay > 0 && ngpt > 0, "heating_rate_lw_layers: ncol, nlay and ngpt must be > 0");
+    RB_CHECK_ARG(tau && lay && inc && dec && up && dn && plev && hr, "heating_rate_lw_layers: null array");
+    const dim3 grid(ceil_div(ncol, 128), nlay);
+    heating_rate_lw_layers_kernel<T><<<grid, 128, 0, as_stream(stream)>>>(ncol, nlay, ngpt, top_at_1, tau, lay, inc,
+                                                                          dec, up, dn, plev, hr);
+    RB_LAUNCH("heating_rate_lw_layers_kernel");
+    return RRTMGP_B200_OK;
+}
+
+template <typename T>
+int hr_sw_layers(int ncol, int nlay, int ngpt, int top_at_1, const T* tau, const T* ssa, const T* g, const T* mu0,
+                 const T* up, const T* dn, const T* dir, const T* plev, T* hr, void* stream)
+{
+    RB_CHECK_ARG(ncol > 0 && nlay > 0 && ngpt > 0, "heating_rate_sw_layers: ncol, nlay and ngpt must be > 0");
+    RB_CHECK_ARG(tau && ssa && g && mu0 && up && dn && dir && plev && hr, "heating_rate_sw_layers: null array");
+    const dim3 grid(ceil_div(ncol, 128), nlay);
+    heating_rate_sw_layers_kernel<T><<<grid, 128, 0, as_stream(stream)>>>(ncol, nlay, ngpt, top_at_1, tau, ssa, g,
+                                                                          mu0, up, dn, dir, plev, hr);
+    RB_LAUNCH("heating_rate_sw_layers_kernel");
+    return RRTMGP_B200_OK;
+}
+
+}  // namespace
+}  // namespace rrtmgp_b200
+
+using namespace rrtmgp_b200;
+
+extern "C" {
+
+int rrtmgp_b200_heating_rate_lw_layers_f32(int ncol, int nlay, int ngpt, int top_at_1, const float* tau,
+        const float* lay_src, const float* lev_src_inc, const float* lev_src_dec, const float* gpt_flux_up,
+        const float* gpt_flux_dn, const float* plev, float* heating_rate, void* s)
+{ return hr_lw_layers<float>(ncol, nlay, ngpt, top_at_1, tau, lay_src, lev_src_inc, lev_src_dec, gpt_flux_up, gpt_flux_dn, plev, heating_rate, s); }
+int rrtmgp_b200_heating_rate_lw_layers_f64(int ncol, int nlay, int ngpt, int top_at_1, const double* tau,
+        const double* lay_src, const double* lev_src_inc, const double* lev_src_dec, const double* gpt_flux_up,
+        const double* gpt_flux_dn, const double* plev, double* heating_rate, void* s)
+{ return hr_lw_layers<double>(ncol, nlay, ngpt, top_at_1, tau, lay_src, lev_src_inc, lev_src_dec, gpt_flux_up, gpt_flux_dn, plev, heating_rate, s); }
+int rrtmgp_b200_heating_rate_sw_layers_f32(int ncol, int nlay, int ngpt, int top_at_1, const float* tau,
+        const float* ssa, const float* g, const float* mu0, const float* gpt_flux_up, const float* gpt_flux_dn,
+        const float* gpt_flux_dir, const float* plev, float* heating_rate, void* s)
+{ return hr_sw_layers<float>(ncol, nlay, ngpt, top_at_1, tau, ssa, g, mu0, gpt_flux_up, gpt_flux_dn, gpt_flux_dir, plev, heating_rate, s); }
+int rrtmgp_b200_heating_rate_sw_layers_f64(int ncol, int nlay, int ngpt, int top_at_1, const double* tau,
+        const double* ssa, const double* g, const double* mu0, const double* gpt_flux_up, const double* gpt_flux_dn,
+        const double* gpt_flux_dir, const double* plev, double* heating_rate, void* s)
+{ return hr_sw_layers<double>(ncol, nlay, ngpt, top_at_1, tau, ssa, g, mu0, gpt_flux_up, gpt_flux_dn, gpt_flux_dir, plev, heating_rate, s); }
+
+}  // extern "C"

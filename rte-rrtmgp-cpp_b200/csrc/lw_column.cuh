@@ -96,7 +96,7 @@ __device__ __forceinline__ void build_lw_record(const KdistView<float>& k, Rec& 
 // kernel, where they are launch constants).
 // PAIR (8-layer chunks): the records of groups gg and gg + 1 are built together at even gg
 // into two buffers (one group's 16 records per warp leave half the lanes idle).
-template <int CL, bool PAIR = false, class Cx, class Io>
+template <int CL, bool PAIR = false, bool DENSE = false, class Cx, class Io>
 __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<float>& k, const Io& io)
 {
     static_assert(CL == 8 || CL == 16, "chunk length");
@@ -188,7 +188,7 @@ __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<
             if (j < nlay && gv) {
                 const Rec& R = recs[slot * CL + i];
                 const float tau =
-                    tau_abs(k, R, g, R.a ? mg1 : mg0, R.a ? nm1 : nm0, sm_sc + j * k.max_nscal) + R.aux.w;
+                    tau_abs<DENSE>(k, R, g, R.a ? mg1 : mg0, R.a ? nm1 : nm0, sm_sc + j * k.max_nscal) + R.aux.w;
                 const float4 p0 = __ldg(k.pfrac4 + (R.kb.x + g));
                 const float4 p1 = __ldg(k.pfrac4 + (R.kb.y + g));
                 const float pfrac = (R.wpl0.x * p0.x + R.wpl0.y * p0.y + R.wpl0.z * p0.z + R.wpl0.w * p0.w) +

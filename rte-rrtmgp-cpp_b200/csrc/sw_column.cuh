@@ -61,7 +61,7 @@ struct SwGridIo {
 // read through accessors at every use, as in lw_forward_column.
 // PAIR (8-layer chunks): the records of groups gg and gg + 1 are built together at even gg
 // into two buffers (one group's 16 records per warp leave half the lanes idle).
-template <int CL, bool PAIR = false, class Cx, class Io>
+template <int CL, bool PAIR = false, bool DENSE = false, class Cx, class Io>
 __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<float>& k, const Io& io)
 {
     static_assert(CL == 8 || CL == 16, "chunk length");
@@ -141,7 +141,8 @@ __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<
             float R = 0.f, T = 1.f, Rdir = 0.f, Tdir = 0.f, Tn = 1.f, adif = 0.f, adir = 0.f;
             if (j < nlay && gv) {
                 const Rec& Rc = recs[slot * CL + i];
-                const float ta = tau_abs(k, Rc, g, Rc.a ? mg1 : mg0, Rc.a ? nm1 : nm0, sm_sc + j * k.max_nscal);
+                const float ta =
+                    tau_abs<DENSE>(k, Rc, g, Rc.a ? mg1 : mg0, Rc.a ? nm1 : nm0, sm_sc + j * k.max_nscal);
                 const float2 r0 = __ldg(k.krayl2 + (Rc.kr[0] + g));
                 const float2 r1 = __ldg(k.krayl2 + (Rc.kr[1] + g));
                 const float tr = (Rc.fm.x * r0.x + Rc.fm.y * r0.y + Rc.fm.z * r1.x + Rc.fm.w * r1.y) * Rc.aux.x;

@@ -270,6 +270,8 @@ _FP_SIGS = {
     "fluxes_broadband": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P],
     "fluxes_byband": [_P, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P],
     "heating_rate": [_I, _I, _P, _P, _P, _P, _P],
+    "heating_rate_lw_layers": [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P],
+    "heating_rate_sw_layers": [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "aerosol_optics": [_P, _I, _I, C.POINTER(GasConc), _I, _P, _P, _P, _P, _P, _P],
 }
 

@@ -89,8 +89,15 @@ class Radiation_solver:
         _abi.check(getattr(lib, "rrtmgp_b200_fluxes_broadband" + sfx)(
             ncol, nlay + 1, self.klw.get_ngpt(), P(b["gpt_up"]), P(b["gpt_dn"]), None, P(b["flux_up"]),
             P(b["flux_dn"]), None, P(b["flux_net"]), s))
-        _abi.check(getattr(lib, "rrtmgp_b200_heating_rate" + sfx)(
-            ncol, nlay, P(b["flux_up"]), P(b["flux_dn"]), P(atm["plev"]), P(b["heating_rate"]), s))
+        if play.dtype == torch.float32:
+            # FP32: from per-layer absorbed flux (a difference of FP32 level fluxes loses ~1 K/day
+            # in ~0.1 Pa top layers); FP64: the level-flux difference, exact to ~1e-9 K/day
+            _abi.check(lib.rrtmgp_b200_heating_rate_lw_layers_f32(
+                ncol, nlay, self.klw.get_ngpt(), int(top_at_1), P(b["tau"]), P(b["lay_src"]), P(b["lev_src_inc"]),
+                P(b["lev_src_dec"]), P(b["gpt_up"]), P(b["gpt_dn"]), P(atm["plev"]), P(b["heating_rate"]), s))
+        else:
+            _abi.check(getattr(lib, "rrtmgp_b200_heating_rate" + sfx)(
+                ncol, nlay, P(b["flux_up"]), P(b["flux_dn"]), P(atm["plev"]), P(b["heating_rate"]), s))
         return {k: b[k] for k in ("flux_up", "flux_dn", "flux_net", "heating_rate")}
 
     def solve_sw(self, atm: dict, with_clouds: bool = True, top_at_1: bool = True, with_aerosols: bool = False):
@@ -140,8 +147,13 @@ class Radiation_solver:
         _abi.check(getattr(lib, "rrtmgp_b200_fluxes_broadband" + sfx)(
             ncol, nlay + 1, self.ksw.get_ngpt(), P(b["gpt_up"]), P(b["gpt_dn"]), P(b["gpt_dir"]), P(b["flux_up"]),
             P(b["flux_dn"]), P(b["flux_dn_dir"]), P(b["flux_net"]), s))
-        _abi.check(getattr(lib, "rrtmgp_b200_heating_rate" + sfx)(
-            ncol, nlay, P(b["flux_up"]), P(b["flux_dn"]), P(atm["plev"]), P(b["heating_rate"]), s))
+        if play.dtype == torch.float32:   # as solve_lw
+            _abi.check(lib.rrtmgp_b200_heating_rate_sw_layers_f32(
+                ncol, nlay, self.ksw.get_ngpt(), int(top_at_1), P(b["tau"]), P(b["ssa"]), P(b["g"]), P(atm["mu0"]),
+                P(b["gpt_up"]), P(b["gpt_dn"]), P(b["gpt_dir"]), P(atm["plev"]), P(b["heating_rate"]), s))
+        else:
+            _abi.check(getattr(lib, "rrtmgp_b200_heating_rate" + sfx)(
+                ncol, nlay, P(b["flux_up"]), P(b["flux_dn"]), P(atm["plev"]), P(b["heating_rate"]), s))
         return {k: b[k] for k in ("flux_up", "flux_dn", "flux_dn_dir", "flux_net", "heating_rate")}
 
 

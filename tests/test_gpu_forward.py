@@ -195,3 +195,24 @@ def test_fused_forward_from_two_host_threads(tables, gpu):
     for i in range(2):
         for k, v in want[i].items():
             assert torch.equal(got[i][k], v), f"thread {i} {k}"
+
+
+@pytest.mark.parametrize("top_at_1", [True, False])
+def test_staged_fp32_heating_rates_match_oracle(oracle_mod, tables, gpu, top_at_1):
+    """The per-stage FP32 path (class API sequence) forms heating rates from per-layer absorbed
+    flux (rrtmgp_b200_heating_rate_{lw,sw}_layers_f32): within 0.01 K/day of FP64 at every
+    layer, the ~0.1 Pa top layers included, where differences of its FP32 level fluxes are off
+    by ~1 K/day."""
+    import torch
+    from rrtmgp_b200.solver import atm_to_device
+    base, _ = _solvers(tables)
+    atm = _vary_surface(S.make_atmosphere(37, 128, seed=61, clouds=True, top_at_1=top_at_1), 62)
+    d = atm_to_device(atm, torch.float32, gpu)
+    lw, sw = base.solve_lw(d, top_at_1=top_at_1), base.solve_sw(d, top_at_1=top_at_1)
+    torch.cuda.synchronize()
+    rlw = oracle_mod.forward_lw(oracle_mod.GasOptics(tables["lw"], S.ATM_GASES),
+                                oracle_mod.CloudOptics(tables["cloud_lw"]), atm)
+    rsw = oracle_mod.forward_sw(oracle_mod.GasOptics(tables["sw"], S.ATM_GASES),
+                                oracle_mod.CloudOptics(tables["cloud_sw"]), atm)
+    _check(lw, rlw, atm, f"staged fp32 lw top_at_1={top_at_1}")
+    _check_sw(sw, rsw, f"staged fp32 sw top_at_1={top_at_1}")

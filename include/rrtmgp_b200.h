@@ -463,6 +463,20 @@ int rrtmgp_b200_forward_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int
         const float* tsi_scaling, const float* sfc_alb_dir, const float* sfc_alb_dif,
         float* flux_up, float* flux_dn, float* flux_dn_dir, float* flux_net,
         float* heating_rate, int chunk, void* stream);
+/* The same shortwave column forward with aerosols, the reference's switch_aerosol_optics
+ * step (src_test/Radiation_solver.cu:794-807): Aerosol_optics_gpu::aerosol_optics of the
+ * tables a (rrtmgp_b200_aerosol_create) for the mass mixing ratios aermr01 .. aermr11
+ * (aerosols, naer; scalars, profiles or fields as gases) and relative humidity rh
+ * (ncol, nlay), delta-scaled when delta_aerosol != 0, added by band after the clouds -- all
+ * inside the kernel, per (layer, band).  a must not be NULL. */
+int rrtmgp_b200_forward_sw_aer_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, rrtmgp_b200_aerosol a,
+        int ncol, int nlay, const float* play, const float* plev, const float* tlay,
+        const float* col_dry, const rrtmgp_b200_gas_conc* gases, int ngases, const float* lwp,
+        const float* iwp, const float* rel, const float* rei, int delta_cloud,
+        const rrtmgp_b200_gas_conc* aerosols, int naer, const float* rh, int delta_aerosol,
+        const float* mu0, const float* tsi_scaling, const float* sfc_alb_dir,
+        const float* sfc_alb_dif, float* flux_up, float* flux_dn, float* flux_dn_dir,
+        float* flux_net, float* heating_rate, int chunk, void* stream);
 
 /* Longwave adjoint of rrtmgp_b200_forward_lw_f32 (no reference counterpart; the reference
  * has only the disabled surface Jacobian of lw_transport_noscat_kernel,
@@ -530,6 +544,21 @@ int rrtmgp_b200_forward_adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cl
         float* grad_lwp, float* grad_iwp, float* grad_rel, float* grad_rei,
         float* grad_sfc_alb_dir, float* grad_sfc_alb_dif, float* flux_up, float* flux_dn,
         float* flux_dn_dir, float* flux_net, float* heating_rate, void* stream);
+/* Shortwave forward + adjoint with aerosols: rrtmgp_b200_forward_adjoint_sw_f32 with the
+ * aerosol arguments of rrtmgp_b200_forward_sw_aer_f32 (a not NULL).  The aerosol optics enter
+ * the recomputed forward; they depend on none of the differentiated inputs (rh is an input of
+ * its own), so no aerosol gradient is formed.  The flux outputs may all be NULL (adjoint only). */
+int rrtmgp_b200_forward_adjoint_sw_aer_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud,
+        rrtmgp_b200_aerosol a, int ncol, int nlay, const float* play, const float* plev,
+        const float* tlay, const float* col_dry, const rrtmgp_b200_gas_conc* gases, int ngases,
+        const float* lwp, const float* iwp, const float* rel, const float* rei, int delta_cloud,
+        const rrtmgp_b200_gas_conc* aerosols, int naer, const float* rh, int delta_aerosol,
+        const float* mu0, const float* tsi_scaling, const float* sfc_alb_dir,
+        const float* sfc_alb_dif, const float* seed_flux_up, const float* seed_flux_dn,
+        const float* seed_flux_dn_dir, const float* seed_heating_rate, float* grad_tlay,
+        float* grad_h2o, float* grad_o3, float* grad_lwp, float* grad_iwp, float* grad_rel,
+        float* grad_rei, float* grad_sfc_alb_dir, float* grad_sfc_alb_dif, float* flux_up,
+        float* flux_dn, float* flux_dn_dir, float* flux_net, float* heating_rate, void* stream);
 
 /* ---- Batched forward of many independent column grids ------------------------------------
  * No reference counterpart as one call: the reference's driver runs one grid at a time and

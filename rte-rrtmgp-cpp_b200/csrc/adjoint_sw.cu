@@ -496,17 +496,19 @@ __device__ __forceinline__ void cloud_sw_dual(const CloudLut<float>& L, int delt
 }
 
 struct SwAdjLayout {
-    size_t state, cg, scal, seeds, clsum, albacc, x1, x2, x3, x4, x5, recs, drecs, total;
+    size_t state, cg, scal, aer, seeds, clsum, albacc, x1, x2, x3, x4, x5, recs, drecs, total;
 };
 
+// aer: aerosol values per (band, local layer) when aerosols are present (aerosol_point).
 __host__ __device__ __forceinline__ SwAdjLayout sw_adj_layout(int ngas, int nband, int mgb, int CS, int WPC,
-                                                              int nbuf, int nscal)
+                                                              int nbuf, int nscal, bool aer)
 {
     SwAdjLayout L;
     L.state = 0;
     L.cg = align16(L.state + sizeof(LayerState) * kLPC);
     L.scal = align16(L.cg + sizeof(float) * size_t(ngas + 1) * kLPC);
-    L.seeds = align16(L.scal + sizeof(float4) * size_t(nscal) * kLPC);
+    L.aer = align16(L.scal + sizeof(float4) * size_t(nscal) * kLPC);
+    L.seeds = align16(L.aer + (aer ? sizeof(float4) * size_t(nband) * kLPC : 0));
     L.clsum = align16(L.seeds + sizeof(float) * (4 * (kLPC + 1)));
     L.albacc = align16(L.clsum + sizeof(float) * size_t(nband) * kLPC * 3);
     L.x1 = align16(L.albacc + sizeof(double) * size_t(nband) * 2);
@@ -539,7 +541,8 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
                   const float* __restrict__ mu0_in, const float* __restrict__ tsi_scaling,
                   const float* __restrict__ alb_dir, const float* __restrict__ alb_dif,
                   const float* __restrict__ seed_up, const float* __restrict__ seed_dn,
-                  const float* __restrict__ seed_dir, const float* __restrict__ seed_hr, const SwAdjOut out)
+                  const float* __restrict__ seed_dir, const float* __restrict__ seed_hr, const SwAdjOut out,
+                  const SwAerosolArgs aer)
 {
     constexpr int WPC = kLPC / CL;   // warps per CTA
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -552,10 +555,11 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
     const int L_end = NWt * CL;
     const int j0 = rank * kLPC;          // first global layer of this CTA
     const int nband = k.nband, mgb = k.max_group_bands;
-    const SwAdjLayout SL = sw_adj_layout(k.ngas, nband, mgb, CS, WPC, PAIR ? 2 : 1, k.max_nscal);
+    const SwAdjLayout SL = sw_adj_layout(k.ngas, nband, mgb, CS, WPC, PAIR ? 2 : 1, k.max_nscal, aer.present != 0);
     LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
     float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
     float4* sm_sc4 = reinterpret_cast<float4*>(smem_raw + SL.scal);   // [local layer][scaling kind]
+    float4* sm_aer = reinterpret_cast<float4*>(smem_raw + SL.aer);    // [band][local layer] (aerosols)
     float* sm_al = reinterpret_cast<float*>(smem_raw + SL.seeds);   // seed F_up per local level (0..64)
     float* sm_be = sm_al + (kLPC + 1);                                // seed F_dn
     float* sm_ga = sm_be + (kLPC + 1);                                // seed F_dir
@@ -609,6 +613,13 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
     __syncthreads();
     layer_minor_scalings_d(k, st, sm_cg, kLPC, sm_sc4, max(0, min(kLPC, nlay - j0)), idx_o3, cd_internal, threadIdx.x,
                            blockDim.x);
+    if (aer.present) {
+        const int nloc = max(0, min(kLPC, nlay - j0));
+        for (int idx = threadIdx.x; idx < nloc * nband; idx += blockDim.x) {
+            const int jl = idx % nloc, b = idx / nloc, j = j0 + jl;
+            sm_aer[b * kLPC + jl] = aerosol_point(aer, ncol, icol, top_at_1 ? j : nlay - 1 - j, st[jl].dp, b);
+        }
+    }
     for (int jl = threadIdx.x; jl < kLPC; jl += blockDim.x) {
         const int j = j0 + jl;
         float h = 0.f;
@@ -663,7 +674,8 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
                     const int qb = PAIR ? (gq & 1) : 0;
                     const int l = top_at_1 ? jj : nlay - 1 - jj;
                     const LayerState s = st[jl];
-                    build_sw_record(k, recs0[qb * kLPC * mgb + r], s, sm_cg + jl, kLPC, b, cld, icol + size_t(l) * ncol);
+                    build_sw_record(k, recs0[qb * kLPC * mgb + r], s, sm_cg + jl, kLPC, b, cld, icol + size_t(l) * ncol,
+                                    aer.present ? sm_aer + b * kLPC + jl : nullptr);
                     DRec& DR = drecs0[qb * kLPC * mgb + r];
                     build_drec<false>(k, DR, s, sm_cg + jl, kLPC, b, idx_o3, cd_internal);
                     const float cd = sm_cg[jl];
@@ -1089,6 +1101,9 @@ sw_adjoint_kernel(const KdistView<float> k, const GasSet<float> gs, const SwClou
 
 }  // namespace
 
+// a: aerosol tables or NULL (no aerosols); aerosols, naer, rh, delta_aerosol as
+// rrtmgp_b200_forward_sw_aer_f32.  The aerosol optics enter the recomputed forward; they depend
+// on none of the differentiated inputs, so no aerosol gradient is formed.
 int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay, const float* play, const float* plev,
                    const float* tlay, const float* col_dry, const rrtmgp_b200_gas_conc* gases, int ngases,
                    const float* lwp, const float* iwp, const float* rel, const float* rei, int delta_cloud,
@@ -1096,7 +1111,9 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
                    const float* seed_up, const float* seed_dn, const float* seed_dir, const float* seed_hr,
                    float* g_tlay, float* g_h2o, float* g_o3, float* g_lwp, float* g_iwp, float* g_rel, float* g_rei,
                    float* g_alb_dir, float* g_alb_dif, float* flux_up, float* flux_dn, float* flux_dir,
-                   float* flux_net, float* heating_rate, void* stream)
+                   float* flux_net, float* heating_rate, void* stream, rrtmgp_b200_aerosol a = nullptr,
+                   const rrtmgp_b200_gas_conc* aerosols = nullptr, int naer = 0, const float* rh = nullptr,
+                   int delta_aerosol = 0)
 {
     RB_CHECK_ARG(k && !k->info.is_longwave, "adjoint_sw: need a shortwave k-distribution");
     if (const int dst = check_device(k->device, "adjoint_sw")) return dst;
@@ -1117,12 +1134,24 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     int idx_o3 = 0;
     for (size_t i = 0; i < k->gas_names.size(); ++i)
         if (k->gas_names[i] == "o3") idx_o3 = int(i) + 1;
+    SwAerosolArgs aer{};
+    if (a) {
+        RB_CHECK_ARG(rh, "adjoint_sw: rh required with aerosol tables");
+        aer.L = aerosol_lut32(a);
+        RB_CHECK_ARG(aer.L.nband == k->info.nband, "adjoint_sw: aerosol and gas band counts differ");
+        st = make_aerosol_set<float>(ncol, nlay, aerosols, naer, aer.s);
+        if (st) return st;
+        aer.rh = rh;
+        aer.present = 1;
+        aer.delta = delta_aerosol;
+    }
     constexpr int CL = kSwAdjointChunk;
     // two record buffers (records of two groups built at once) when they fit
-    const size_t smem2 = sw_adj_layout(v.ngas, v.nband, v.max_group_bands, CS, kLPC / CL, 2, v.max_nscal).total;
+    const bool wa = aer.present != 0;
+    const size_t smem2 = sw_adj_layout(v.ngas, v.nband, v.max_group_bands, CS, kLPC / CL, 2, v.max_nscal, wa).total;
     const bool pair = smem2 <= 227 * 1024;
     const size_t smem =
-        pair ? smem2 : sw_adj_layout(v.ngas, v.nband, v.max_group_bands, CS, kLPC / CL, 1, v.max_nscal).total;
+        pair ? smem2 : sw_adj_layout(v.ngas, v.nband, v.max_group_bands, CS, kLPC / CL, 1, v.max_nscal, wa).total;
     if (smem > 227 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "adjoint_sw: shared memory need exceeds 227 KB");
     static PerDeviceOnce attr;
     const int ast = attr.run([] {
@@ -1167,7 +1196,7 @@ int adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
                                    : sw_adjoint_kernel<CL, false, false, false>));
     RB_CUDA(cudaLaunchKernelEx(&cfg, kernel, v, gs, ca, ncol, nlay, CS, idx_o3, col_dry ? 0 : 1, play, plev,
                                tlay, col_dry, mu0, tsi_scaling, sfc_alb_dir, sfc_alb_dif, seed_up, seed_dn, seed_dir,
-                               seed_hr, out),
+                               seed_hr, out, aer),
             "sw_adjoint_kernel launch");
     return RRTMGP_B200_OK;
 }
@@ -1205,4 +1234,23 @@ extern "C" int rrtmgp_b200_forward_adjoint_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b2
                                        seed_flux_dn, seed_flux_dn_dir, seed_heating_rate, grad_tlay, grad_h2o, grad_o3,
                                        grad_lwp, grad_iwp, grad_rel, grad_rei, grad_sfc_alb_dir, grad_sfc_alb_dif,
                                        flux_up, flux_dn, flux_dn_dir, flux_net, heating_rate, stream);
+}
+
+extern "C" int rrtmgp_b200_forward_adjoint_sw_aer_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c,
+        rrtmgp_b200_aerosol a, int ncol, int nlay, const float* play, const float* plev, const float* tlay,
+        const float* col_dry, const rrtmgp_b200_gas_conc* gases, int ngases, const float* lwp, const float* iwp,
+        const float* rel, const float* rei, int delta_cloud, const rrtmgp_b200_gas_conc* aerosols, int naer,
+        const float* rh, int delta_aerosol, const float* mu0, const float* tsi_scaling, const float* sfc_alb_dir,
+        const float* sfc_alb_dif, const float* seed_flux_up, const float* seed_flux_dn, const float* seed_flux_dn_dir,
+        const float* seed_heating_rate, float* grad_tlay, float* grad_h2o, float* grad_o3, float* grad_lwp,
+        float* grad_iwp, float* grad_rel, float* grad_rei, float* grad_sfc_alb_dir, float* grad_sfc_alb_dif,
+        float* flux_up, float* flux_dn, float* flux_dn_dir, float* flux_net, float* heating_rate, void* stream)
+{
+    RB_CHECK_ARG(a, "forward_adjoint_sw_aer: null aerosol handle");
+    return rrtmgp_b200::adjoint_sw_f32(k, c, ncol, nlay, play, plev, tlay, col_dry, gases, ngases, lwp, iwp, rel, rei,
+                                       delta_cloud, mu0, tsi_scaling, sfc_alb_dir, sfc_alb_dif, seed_flux_up,
+                                       seed_flux_dn, seed_flux_dn_dir, seed_heating_rate, grad_tlay, grad_h2o, grad_o3,
+                                       grad_lwp, grad_iwp, grad_rel, grad_rei, grad_sfc_alb_dir, grad_sfc_alb_dif,
+                                       flux_up, flux_dn, flux_dn_dir, flux_net, heating_rate, stream, a, aerosols,
+                                       naer, rh, delta_aerosol);
 }

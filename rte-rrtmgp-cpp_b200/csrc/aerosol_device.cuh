@@ -89,4 +89,39 @@ __device__ __forceinline__ void aerosol_band(const AerosolLut<T>& L, const T mmr
     }
 }
 
+// The same sums plus the absorption optical depth sum_s od_s (1 - ssa_s) of band b, formed per
+// species (the fused shortwave kernels carry 1 - ssa as absorption over extinction, which a
+// difference tau - tau*ssa would lose for nearly conservative scattering).
+template <typename T>
+__device__ __forceinline__ void aerosol_band_abs(const AerosolLut<T>& L, const T mmr[kNAerosol], int ihum, T dpg,
+                                                 int b, T& tau, T& taussa, T& taussag, T& tauabs)
+{
+    constexpr int kMmr[kNAerosol] = {3, 4, 5, 8, 9, 0, 1, 2, 10, 7, 6};
+    constexpr int kPhilic[kNAerosol] = {0, 0, 0, 0, 0, 1, 1, 1, 1, 0, 1};
+    constexpr int kType[kNAerosol] = {0, 7, 5, 10, 10, 0, 1, 2, 4, 9, 3};
+    tau = T(0);
+    taussa = T(0);
+    taussag = T(0);
+    tauabs = T(0);
+#pragma unroll
+    for (int s = 0; s < kNAerosol; ++s) {
+        const size_t idx = kPhilic[s] ? b + size_t(ihum) * L.nband + size_t(kType[s]) * L.nband * L.nhum
+                                      : b + size_t(kType[s]) * L.nband;
+        const T* me = kPhilic[s] ? L.philic(0) : L.phobic(0);
+        const T* ss = kPhilic[s] ? L.philic(1) : L.phobic(1);
+        const T* gg = kPhilic[s] ? L.philic(2) : L.phobic(2);
+        const T od = mmr[kMmr[s]] * dpg * me[idx];
+        const T w = ss[idx];
+        tau += od;
+        taussa += od * w;
+        taussag += od * w * gg[idx];
+        tauabs += od * (T(1) - w);
+    }
+}
+
+// Host-side helpers of aerosol.cu used by the fused shortwave launchers.
+template <typename T>
+int make_aerosol_set(int ncol, int nlay, const rrtmgp_b200_gas_conc* aer, int naer, AerosolSet<T>& out);
+AerosolLut<float> aerosol_lut32(const rrtmgp_b200_aerosol_t* a);
+
 }  // namespace rrtmgp_b200

@@ -111,6 +111,7 @@ struct ItemIo {
 };
 
 struct SwItemIo : ItemIo {
+    __device__ __forceinline__ SwAerosolArgs aerosol() const { return SwAerosolArgs{}; }   // no aerosols
     __device__ __forceinline__ SwCloudArgs cloud() const
     {
         return SwCloudArgs{g_item.lut, g_item.lwp, g_item.iwp, g_item.rel, g_item.rei, g_item.cloudy, g_item.delta};

@@ -19,13 +19,13 @@ int launch_sw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
                       const float* plev, const float* tlay, const float* col_dry, const GasSet<float>& gs,
                       const float* lwp, const float* iwp, const float* rel, const float* rei, int delta,
                       const float* mu0, const float* tsi, const float* alb_dir, const float* alb_dif, float* up,
-                      float* dn, float* dir, float* net, float* hr, cudaStream_t stream)
+                      float* dn, float* dir, float* net, float* hr, const SwAerosolArgs& aer, cudaStream_t stream)
 {
     const KdistView<float>& v = k->v32;
     const int NW = (nlay + CL - 1) / CL;
     RB_CHECK_ARG(NW <= 16, "forward_sw: nlay too large for the fused kernel (at most 16 chunks)");
-    const size_t smem =
-        smem_layout(nlay, v.ngas, v.nband, 0, NW, 3, CL, v.max_group_bands * (CL == 8 ? 2 : 1), v.max_nscal).total;
+    const size_t smem = smem_layout(nlay, v.ngas, v.nband, aer.present ? 4 : 0, NW, 3, CL,
+                                    v.max_group_bands * (CL == 8 ? 2 : 1), v.max_nscal).total;
     if (smem > 220 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "forward_sw: shared memory need exceeds 220 KB");
     static PerDeviceOnce attr;
     int st = attr.run([] { return cudaFuncSetAttribute(sw_forward_kernel<CL, DENSE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -39,7 +39,7 @@ int launch_sw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
         ca.present = 1;
         ca.delta = delta;
     }
-    SwGridIo io{ncol, nlay, play, plev, tlay, col_dry, mu0, tsi, alb_dir, alb_dif, up, dn, dir, net, hr, gs, ca};
+    SwGridIo io{ncol, nlay, play, plev, tlay, col_dry, mu0, tsi, alb_dir, alb_dif, up, dn, dir, net, hr, gs, ca, aer};
     sw_forward_kernel<CL, DENSE><<<ncol, NW * 32, smem, stream>>>(v, io);
     RB_LAUNCH("sw_forward_kernel");
     return RRTMGP_B200_OK;
@@ -47,12 +47,14 @@ int launch_sw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
 
 }  // namespace
 
-int forward_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay, const float* play,
-                   const float* plev, const float* tlay, const float* col_dry, const rrtmgp_b200_gas_conc* gases,
-                   int ngases, const float* lwp, const float* iwp, const float* rel, const float* rei,
-                   int delta_cloud, const float* mu0, const float* tsi_scaling, const float* sfc_alb_dir,
-                   const float* sfc_alb_dif, float* flux_up, float* flux_dn, float* flux_dn_dir, float* flux_net,
-                   float* heating_rate, int chunk, void* stream)
+// a: aerosol tables (NULL: no aerosols); aerosols/naer: aermr01 .. aermr11; rh (ncol, nlay).
+int forward_sw_aer_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, rrtmgp_b200_aerosol a, int ncol, int nlay,
+                       const float* play, const float* plev, const float* tlay, const float* col_dry,
+                       const rrtmgp_b200_gas_conc* gases, int ngases, const float* lwp, const float* iwp,
+                       const float* rel, const float* rei, int delta_cloud, const rrtmgp_b200_gas_conc* aerosols,
+                       int naer, const float* rh, int delta_aerosol, const float* mu0, const float* tsi_scaling,
+                       const float* sfc_alb_dir, const float* sfc_alb_dif, float* flux_up, float* flux_dn,
+                       float* flux_dn_dir, float* flux_net, float* heating_rate, int chunk, void* stream)
 {
     RB_CHECK_ARG(k && !k->info.is_longwave, "forward_sw: need a shortwave k-distribution");
     if (const int dst = check_device(k->device, "forward_sw")) return dst;
@@ -67,16 +69,39 @@ int forward_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay,
     GasSet<float> gs;
     int st = make_gas_set<float>(k, ncol, nlay, gases, ngases, gs);
     if (st) return st;
+    SwAerosolArgs aer{};
+    if (a) {
+        RB_CHECK_ARG(rh, "forward_sw: rh required with aerosol tables");
+        aer.L = aerosol_lut32(a);
+        RB_CHECK_ARG(aer.L.nband == k->info.nband, "forward_sw: aerosol and gas band counts differ");
+        st = make_aerosol_set<float>(ncol, nlay, aerosols, naer, aer.s);
+        if (st) return st;
+        aer.rh = rh;
+        aer.present = 1;
+        aer.delta = delta_aerosol;
+    }
     cudaStream_t s = as_stream(stream);
     const int cl = chunk ? chunk : (nlay > 128 ? 16 : 8);
     const bool dense = v.max_minor_per_g > 3;
 #define RB_SW_FWD(CLv, D)                                                                                           \
     launch_sw_forward<CLv, D>(k, c, ncol, nlay, play, plev, tlay, col_dry, gs, lwp, iwp, rel, rei, delta_cloud, mu0, \
                               tsi_scaling, sfc_alb_dir, sfc_alb_dif, flux_up, flux_dn, flux_dn_dir, flux_net,         \
-                              heating_rate, s)
+                              heating_rate, aer, s)
     if (cl == 16) return dense ? RB_SW_FWD(16, true) : RB_SW_FWD(16, false);
     return dense ? RB_SW_FWD(8, true) : RB_SW_FWD(8, false);
 #undef RB_SW_FWD
+}
+
+int forward_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay, const float* play,
+                   const float* plev, const float* tlay, const float* col_dry, const rrtmgp_b200_gas_conc* gases,
+                   int ngases, const float* lwp, const float* iwp, const float* rel, const float* rei,
+                   int delta_cloud, const float* mu0, const float* tsi_scaling, const float* sfc_alb_dir,
+                   const float* sfc_alb_dif, float* flux_up, float* flux_dn, float* flux_dn_dir, float* flux_net,
+                   float* heating_rate, int chunk, void* stream)
+{
+    return forward_sw_aer_f32(k, c, nullptr, ncol, nlay, play, plev, tlay, col_dry, gases, ngases, lwp, iwp, rel, rei,
+                              delta_cloud, nullptr, 0, nullptr, 0, mu0, tsi_scaling, sfc_alb_dir, sfc_alb_dif, flux_up,
+                              flux_dn, flux_dn_dir, flux_net, heating_rate, chunk, stream);
 }
 
 }  // namespace rrtmgp_b200
@@ -91,4 +116,19 @@ extern "C" int rrtmgp_b200_forward_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud
     return rrtmgp_b200::forward_sw_f32(k, c, ncol, nlay, play, plev, tlay, col_dry, gases, ngases, lwp, iwp, rel, rei,
                                        delta_cloud, mu0, tsi_scaling, sfc_alb_dir, sfc_alb_dif, flux_up, flux_dn,
                                        flux_dn_dir, flux_net, heating_rate, chunk, stream);
+}
+
+extern "C" int rrtmgp_b200_forward_sw_aer_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, rrtmgp_b200_aerosol a,
+        int ncol, int nlay, const float* play, const float* plev, const float* tlay, const float* col_dry,
+        const rrtmgp_b200_gas_conc* gases, int ngases, const float* lwp, const float* iwp, const float* rel,
+        const float* rei, int delta_cloud, const rrtmgp_b200_gas_conc* aerosols, int naer, const float* rh,
+        int delta_aerosol, const float* mu0, const float* tsi_scaling, const float* sfc_alb_dir,
+        const float* sfc_alb_dif, float* flux_up, float* flux_dn, float* flux_dn_dir, float* flux_net,
+        float* heating_rate, int chunk, void* stream)
+{
+    RB_CHECK_ARG(a, "forward_sw_aer: null aerosol handle (use rrtmgp_b200_forward_sw_f32 without aerosols)");
+    return rrtmgp_b200::forward_sw_aer_f32(k, c, a, ncol, nlay, play, plev, tlay, col_dry, gases, ngases, lwp, iwp,
+                                           rel, rei, delta_cloud, aerosols, naer, rh, delta_aerosol, mu0, tsi_scaling,
+                                           sfc_alb_dir, sfc_alb_dif, flux_up, flux_dn, flux_dn_dir, flux_net,
+                                           heating_rate, chunk, stream);
 }

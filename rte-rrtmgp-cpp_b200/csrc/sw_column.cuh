@@ -37,6 +37,7 @@ struct SwGridIo {
     float *up_, *dn_, *dir_, *net_, *hr_;
     GasSet<float> gs_;
     SwCloudArgs cld_;
+    SwAerosolArgs aer_;
     __device__ __forceinline__ int ncol() const { return ncol_; }
     __device__ __forceinline__ int nlay() const { return nlay_; }
     __device__ __forceinline__ const float* play() const { return play_; }
@@ -54,6 +55,7 @@ struct SwGridIo {
     __device__ __forceinline__ float* hr() const { return hr_; }
     __device__ __forceinline__ const GasSet<float>& gs() const { return gs_; }
     __device__ __forceinline__ const SwCloudArgs& cloud() const { return cld_; }
+    __device__ __forceinline__ const SwAerosolArgs& aerosol() const { return aer_; }
 };
 
 // One column by the warps that context cx names (cx.nwarps() warps of CL layers each,
@@ -68,7 +70,9 @@ __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<
     constexpr bool P2 = PAIR && CL == 8;
     const int lane = threadIdx.x & 31;
     const int nband = k.nband;
-    const SmemLayout SL = smem_layout(io.nlay(), k.ngas, nband, 0, cx.nwarps(), 3, CL,
+    const bool with_aer = io.aerosol().present != 0;
+    // the "cloud" region holds the aerosol (tau, tau ssa, tau ssa g, tau (1 - ssa)) per (band, layer)
+    const SmemLayout SL = smem_layout(io.nlay(), k.ngas, nband, with_aer ? 4 : 0, cx.nwarps(), 3, CL,
                                       k.max_group_bands * (P2 ? 2 : 1), k.max_nscal);
     unsigned char* const smem_raw = cx.smem();
     LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
@@ -94,6 +98,14 @@ __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<
     const float mu0_inv = 1.f / mu0;
     cx.sync();
     layer_minor_scalings(k, st, sm_cg, io.nlay(), sm_sc, io.nlay(), cx.tid(), cx.nthreads());
+    float4* const sm_aer = reinterpret_cast<float4*>(smem_raw + SL.cloud);   // [band][layer]
+    if (with_aer) {
+        const int nlay = io.nlay();
+        for (int idx = cx.tid(); idx < nlay * nband; idx += cx.nthreads()) {
+            const int j = idx % nlay, b = idx / nlay;
+            sm_aer[idx] = aerosol_point(io.aerosol(), io.ncol(), cx.icol(), top_at_1 ? j : nlay - 1 - j, st[j].dp, b);
+        }
+    }
     cx.sync();
 
     const int ngpt = k.ngpt;
@@ -124,7 +136,8 @@ __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<
                 if (jj < nlay && b < nband && k.band_lims[2 * b] < 32 * gq + 32) {
                     const int l = top_at_1 ? jj : nlay - 1 - jj;
                     build_sw_record(k, recs0[(P2 ? (gq & 1) : 0) * rbuf + r], st[jj], sm_cg + jj, nlay, b,
-                                    io.cloud(), cx.icol() + size_t(l) * io.ncol());
+                                    io.cloud(), cx.icol() + size_t(l) * io.ncol(),
+                                    with_aer ? sm_aer + b * nlay + jj : nullptr);
                 }
             }
         }

@@ -3,6 +3,7 @@
 // coefficients and the per-(layer, band) record.
 #pragma once
 
+#include "aerosol_device.cuh"
 #include "fused_common.cuh"
 #include "optics_device.cuh"
 
@@ -18,6 +19,43 @@ struct SwCloudArgs {
     int present;
     int delta;
 };
+
+// Aerosol optics of the fused shortwave kernels (the reference's switch_aerosol_optics step,
+// src_test/Radiation_solver.cu:794-807: aerosol optics, optionally delta-scaled, added by band
+// after the clouds).  present == 0: no aerosols.
+struct SwAerosolArgs {
+    AerosolLut<float> L;
+    AerosolSet<float> s;
+    const float* rh;     // (ncol, nlay)
+    int present;
+    int delta;
+};
+
+// Aerosol (tau, tau*ssa, tau*ssa*g, tau*(1 - ssa)) of band b at reference-layout layer l of
+// column icol, delta-scaled when a.delta (Optical_props_2str_gpu::delta_scale,
+// optical_props_kernels.cu:139-160); dp = |p_bottom - p_top| of the layer.  ssa and g are
+// formed with the epsilon clamps of combine_and_store_kernel (src_cuda/Aerosol_optics.cu:
+// 170-186) at the FP64 build's epsilon, as the other clamps of the FP32 kernels: with the
+// FP32 epsilon (1.2e-7) g of the thin upper-layer aerosol would collapse to ~0 and its delta
+// scaling differ from the FP64 result.
+__device__ __forceinline__ float4 aerosol_point(const SwAerosolArgs& a, int ncol, int icol, int l, float dp, int b)
+{
+    const size_t cl = icol + size_t(l) * ncol;
+    const int ihum = aerosol_rh_class(a.L, a.rh[cl]);
+    float mmr[kNAerosol];
+#pragma unroll
+    for (int s = 0; s < kNAerosol; ++s) mmr[s] = aerosol_mmr(a.s, s, ncol, icol, l);
+    float t, ts, tsg, tabs;
+    aerosol_band_abs(a.L, mmr, ihum, dp / 9.81f, b, t, ts, tsg, tabs);
+    if (a.delta) {
+        const float eps = 2.220446049250313e-16f;   // DBL_EPSILON
+        float ssa = ts / fmaxf(t, eps), g = tsg / fmaxf(ts, eps);
+        delta_scale_point(t, ssa, g);
+        ts = t * ssa;
+        tsg = ts * g;
+    }
+    return make_float4(t, ts, tsg, tabs);
+}
 
 // 1 - exp(-x) and exp(-x) for x >= 0, each with a small relative error: Taylor series of
 // 1 - exp(-x) through x^8 below 0.5 (truncation < 1.4e-8 relative), the exp intrinsic above.
@@ -106,9 +144,10 @@ __device__ __forceinline__ void sw_layer_fast(float tau, float w0, float omw, fl
     adir = fmaxf(0.f, rest - Tdir);
 }
 
+// aer: the (layer, band) aerosol values of aerosol_point, or NULL without aerosols.
 __device__ __forceinline__ void build_sw_record(const KdistView<float>& k, Rec& R, const LayerState& s,
                                                 const float* cg, int nlay, int b, const SwCloudArgs& cld,
-                                                size_t cl)
+                                                size_t cl, const float4* aer = nullptr)
 {
     record_weights(k, R, s, cg, nlay, b);
     float tau = 0.f, ssa = 0.f, g = 0.f;
@@ -121,8 +160,15 @@ __device__ __forceinline__ void build_sw_record(const KdistView<float>& k, Rec& 
     } else {
         R.aux2 = 0.f;
     }
-    const float ts = tau * ssa;
-    R.aux = make_float4(cg[0] + cg[k.idx_h2o * nlay], tau, ts, ts * g);
+    float ts = tau * ssa, tsg = ts * g;
+    if (aer) {
+        const float4 a = *aer;
+        tau += a.x;
+        ts += a.y;
+        tsg += a.z;
+        R.aux2 += a.w;
+    }
+    R.aux = make_float4(cg[0] + cg[k.idx_h2o * nlay], tau, ts, tsg);
 }
 
 }  // namespace fused

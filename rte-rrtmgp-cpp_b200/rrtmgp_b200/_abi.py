@@ -228,6 +228,9 @@ _SIGS = {
                                         _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
     "rrtmgp_b200_forward_sw_f32": (_I, [_P, _P, _I, _I, _P, _P, _P, _P, C.POINTER(GasConc), _I,
                                         _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
+    "rrtmgp_b200_forward_sw_aer_f32": (_I, [_P, _P, _P, _I, _I, _P, _P, _P, _P, C.POINTER(GasConc), _I,
+                                            _P, _P, _P, _P, _I, C.POINTER(GasConc), _I, _P, _I,
+                                            _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
     "rrtmgp_b200_fp32_fma_probe": (_I, [_I, _I, _P, _P]),
     "rrtmgp_b200_aerosol_create": (_I, [C.POINTER(AerosolTables), C.POINTER(_P)]),
     "rrtmgp_b200_aerosol_destroy": (None, [_P]),
@@ -238,6 +241,11 @@ _SIGS = {
                                                 _P, _P, _P, _P, _I, _P, _P, _P, _P,
                                                 _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
                                                 _P, _P, _P, _P, _P, _P]),
+    "rrtmgp_b200_forward_adjoint_sw_aer_f32": (_I, [_P, _P, _P, _I, _I, _P, _P, _P, _P, C.POINTER(GasConc), _I,
+                                                    _P, _P, _P, _P, _I, C.POINTER(GasConc), _I, _P, _I,
+                                                    _P, _P, _P, _P,
+                                                    _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
+                                                    _P, _P, _P, _P, _P, _P]),
     "rrtmgp_b200_batch_create": (_I, [_P, _P, _P, _P, _I, _P, _I, C.POINTER(_P)]),
     "rrtmgp_b200_batch_destroy": (_I, [_P]),
     "rrtmgp_b200_batch_run": (_I, [_P, _I, _P]),

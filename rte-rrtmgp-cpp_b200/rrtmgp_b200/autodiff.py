@@ -133,12 +133,13 @@ def adjoint_lw(fused, atm: dict, seed_up=None, seed_dn=None, seed_hr=None, with_
 
 
 def adjoint_sw(fused, atm: dict, seed_up=None, seed_dn=None, seed_dir=None, seed_hr=None, with_clouds: bool = True,
-               with_fluxes: bool = False):
+               with_fluxes: bool = False, with_aerosols: bool = False):
     """Direct call of the shortwave adjoint: dict of gradients of sum(seed_up * flux_up +
     seed_dn * flux_dn + seed_dir * flux_dn_dir + seed_hr * heating_rate) w.r.t. tlay, h2o, o3,
     lwp, iwp, rel, rei (nlay, ncol) and sfc_alb_dir, sfc_alb_dif (ncol, nband).  with_fluxes:
     one launch that also returns the forward fluxes (rrtmgp_b200_forward_adjoint_sw_f32), as
-    (fluxes, gradients)."""
+    (fluxes, gradients).  with_aerosols: atm["aerosols"] and atm["rh"] through the base
+    solver's aerosol tables in the recomputed forward (rrtmgp_b200_forward_adjoint_sw_aer_f32)."""
     play = atm["play"]
     nlay, ncol = play.shape
     dev = play.device
@@ -158,15 +159,24 @@ def adjoint_sw(fused, atm: dict, seed_up=None, seed_dn=None, seed_dir=None, seed
             P(seed_up), P(seed_dn), P(seed_dir), P(seed_hr), P(grads["tlay"]), P(grads["h2o"]), P(grads["o3"]),
             P(grads["lwp"]) if c else None, P(grads["iwp"]) if c else None, P(grads["rel"]) if c else None,
             P(grads["rei"]) if c else None, P(grads["sfc_alb_dir"]), P(grads["sfc_alb_dif"])]
+    fl = None
+    if with_fluxes:
+        fl = {k: torch.empty((nlay + 1, ncol), dtype=torch.float32, device=dev)
+              for k in ("flux_up", "flux_dn", "flux_dn_dir", "flux_net")}
+        fl["heating_rate"] = torch.empty((nlay, ncol), dtype=torch.float32, device=dev)
+    fargs = ([P(fl[k]) for k in ("flux_up", "flux_dn", "flux_dn_dir", "flux_net", "heating_rate")] if with_fluxes
+             else [None] * 5)
+    if with_aerosols:
+        assert fused.base.aer is not None, "solver built without aerosol tables"
+        aer, keep_a = api.Gas_optics_rrtmgp._gases(atm["aerosols"], ncol, nlay, atm["play"])
+        aargs = args[:2] + [fused.base.aer.handle] + args[2:15] + [aer, len(atm["aerosols"]), P(atm["rh"]),
+                                                                  int(fused.base.delta_aerosol)] + args[15:]
+        _abi.check(_abi.load().rrtmgp_b200_forward_adjoint_sw_aer_f32(*aargs, *fargs, api._stream()))
+        return (fl, grads) if with_fluxes else grads
     if not with_fluxes:
         _abi.check(_abi.load().rrtmgp_b200_adjoint_sw_f32(*args, api._stream()))
         return grads
-    fl = {k: torch.empty((nlay + 1, ncol), dtype=torch.float32, device=dev)
-          for k in ("flux_up", "flux_dn", "flux_dn_dir", "flux_net")}
-    fl["heating_rate"] = torch.empty((nlay, ncol), dtype=torch.float32, device=dev)
-    _abi.check(_abi.load().rrtmgp_b200_forward_adjoint_sw_f32(
-        *args, P(fl["flux_up"]), P(fl["flux_dn"]), P(fl["flux_dn_dir"]), P(fl["flux_net"]), P(fl["heating_rate"]),
-        api._stream()))
+    _abi.check(_abi.load().rrtmgp_b200_forward_adjoint_sw_f32(*args, *fargs, api._stream()))
     return fl, grads
 
 

@@ -194,7 +194,9 @@ class Fused_solver:
         return {k: o[k] for k in ("flux_up", "flux_dn", "flux_net", "heating_rate")}
 
 
-    def solve_sw(self, atm: dict, with_clouds: bool = True):
+    def solve_sw(self, atm: dict, with_clouds: bool = True, with_aerosols: bool = False):
+        """with_aerosols: atm["aerosols"] {aermr01 .. aermr11} and atm["rh"] (nlay, ncol) through
+        the base solver's aerosol tables, inside the fused kernel (rrtmgp_b200_forward_sw_aer_f32)."""
         from . import _abi
         play = atm["play"]
         assert play.dtype == torch.float32, "the fused path is FP32"
@@ -204,6 +206,18 @@ class Fused_solver:
         arr, keep = api.Gas_optics_rrtmgp._gases(atm["gases"], ncol, nlay, atm["play"])
         c = self.base.csw if (with_clouds and self.base.csw is not None) else None
         tsi = atm.get("tsi_scaling")
+        if with_aerosols:
+            assert self.base.aer is not None, "solver built without aerosol tables"
+            aer, keep_a = api.Gas_optics_rrtmgp._gases(atm["aerosols"], ncol, nlay, atm["play"])
+            _abi.check(_abi.load().rrtmgp_b200_forward_sw_aer_f32(
+                self.base.ksw.handle, c.handle if c else None, self.base.aer.handle, ncol, nlay, P(play),
+                P(atm["plev"]), P(atm["tlay"]), None, arr, len(atm["gases"]), P(atm["lwp"]) if c else None,
+                P(atm["iwp"]) if c else None, P(atm["rel"]) if c else None, P(atm["rei"]) if c else None,
+                int(self.base.delta_cloud), aer, len(atm["aerosols"]), P(atm["rh"]), int(self.base.delta_aerosol),
+                P(atm["mu0"]), P(tsi) if tsi is not None else None, P(atm["sfc_alb_dir"]), P(atm["sfc_alb_dif"]),
+                P(o["flux_up"]), P(o["flux_dn"]), P(o["flux_dn_dir"]), P(o["flux_net"]), P(o["heating_rate"]),
+                int(self.chunk), api._stream()))
+            return {k: o[k] for k in ("flux_up", "flux_dn", "flux_dn_dir", "flux_net", "heating_rate")}
         _abi.check(_abi.load().rrtmgp_b200_forward_sw_f32(
             self.base.ksw.handle, c.handle if c else None, ncol, nlay, P(play), P(atm["plev"]), P(atm["tlay"]),
             None, arr, len(atm["gases"]), P(atm["lwp"]) if c else None, P(atm["iwp"]) if c else None,

@@ -135,3 +135,77 @@ def test_solve_sw_with_aerosols(oracle_mod, tables, gpu, delta_aerosol):
         np.testing.assert_allclose(g, ref[k], rtol=1e-8, atol=1e-6 if k == "heating_rate" else 1e-8, err_msg=k)
     # the aerosols change the fluxes
     assert float((plain["flux_dn_dir"] - got["flux_dn_dir"]).abs().max()) > 1e-3
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("delta_aerosol", [False, True])
+@pytest.mark.parametrize("top_at_1,nlay", [(True, 60), (False, 128), (True, 200)])
+def test_fused_sw_with_aerosols(oracle_mod, tables, gpu, delta_aerosol, top_at_1, nlay):
+    """The fused FP32 shortwave kernel with aerosols (rrtmgp_b200_forward_sw_aer_f32): aerosol
+    optics per (layer, band) inside the kernel, delta-scaled or not, added after the clouds;
+    against the oracle's solve_gpu sequence with the fused kernels' bounds (5e-3 W/m2,
+    0.01 K/day), profiles and a scalar among the species."""
+    import torch
+    from rrtmgp_b200.solver import Fused_solver, Radiation_solver, atm_to_device
+    tab = S.make_aerosol_luts()
+    base = Radiation_solver(tables["lw"], tables["sw"], tables["cloud_lw"], tables["cloud_sw"], S.ATM_GASES,
+                            aerosol_sw=tab, delta_aerosol=delta_aerosol)
+    atm = S.make_atmosphere(37, nlay, seed=83 + nlay, clouds=True, top_at_1=top_at_1)
+    aer, rh = S.make_aerosols(atm["play"], seed=84)
+    aer["aermr02"] = aer["aermr02"][:, 0].copy()   # a profile
+    aer["aermr07"] = np.array([2e-9])               # a scalar
+    atm["aerosols"], atm["rh"] = aer, rh
+    d = atm_to_device(atm, torch.float32, gpu)
+    d["aerosols"] = {k: torch.as_tensor(v, dtype=torch.float32, device=gpu).contiguous() for k, v in aer.items()}
+    d["rh"] = torch.as_tensor(rh, dtype=torch.float32, device=gpu).contiguous()
+    fused = Fused_solver(base)
+    got = {k: v.clone() for k, v in fused.solve_sw(d, with_aerosols=True).items()}
+    plain = {k: v.clone() for k, v in fused.solve_sw(d).items()}
+    torch.cuda.synchronize()
+    ref = oracle_mod.forward_sw(oracle_mod.GasOptics(tables["sw"], S.ATM_GASES),
+                                oracle_mod.CloudOptics(tables["cloud_sw"]), atm, aerosol_tables=tab,
+                                delta_aerosol=delta_aerosol)
+    for k in ("flux_up", "flux_dn", "flux_dn_dir", "flux_net", "heating_rate"):
+        e = float(np.max(np.abs(got[k].double().cpu().numpy() - ref[k])))
+        assert e < (0.01 if k == "heating_rate" else 5e-3), f"{k}: {e:.3e}"
+    assert float((plain["flux_dn_dir"] - got["flux_dn_dir"]).abs().max()) > 1e-3
+
+
+@pytest.mark.gpu
+def test_sw_adjoint_with_aerosols_matches_fd(oracle_mod, tables, gpu):
+    """SW forward + adjoint with aerosols in the recomputed forward
+    (rrtmgp_b200_forward_adjoint_sw_aer_f32): gradients against FP64 central differences of the
+    oracle's sequence with the same aerosols (bounds of the other adjoint tests), fluxes against
+    its forward."""
+    import torch
+    from test_gpu_adjoint import _check, _fd, _fd_bands, _get, _informative, _sw_seeds
+    from rrtmgp_b200.autodiff import adjoint_sw
+    from rrtmgp_b200.solver import Fused_solver, Radiation_solver, atm_to_device
+    tab = S.make_aerosol_luts()
+    base = Radiation_solver(tables["lw"], tables["sw"], tables["cloud_lw"], tables["cloud_sw"], S.ATM_GASES,
+                            aerosol_sw=tab, delta_aerosol=True)
+    ncol, nlay = 3, 24
+    atm = S.make_atmosphere(ncol, nlay, seed=85, clouds=True)
+    atm["mu0"] = np.array([0.3, 0.6, 0.9])
+    atm["aerosols"], atm["rh"] = S.make_aerosols(atm["play"], seed=86)
+    kd, cl = oracle_mod.GasOptics(tables["sw"], S.ATM_GASES), oracle_mod.CloudOptics(tables["cloud_sw"])
+    fwd = lambda a: oracle_mod.forward_sw(kd, cl, a, aerosol_tables=tab, delta_aerosol=True)  # noqa: E731
+    seeds = _sw_seeds(nlay, ncol, np.random.default_rng(87))
+    d = atm_to_device(atm, torch.float32, gpu)
+    d["aerosols"] = {k: torch.as_tensor(v, dtype=torch.float32, device=gpu).contiguous()
+                     for k, v in atm["aerosols"].items()}
+    d["rh"] = torch.as_tensor(atm["rh"], dtype=torch.float32, device=gpu).contiguous()
+    t = {k: torch.as_tensor(v, dtype=torch.float32, device=gpu).contiguous() for k, v in seeds.items()}
+    fl, g = adjoint_sw(Fused_solver(base), d, t["flux_up"], t["flux_dn"], t["flux_dn_dir"], t["heating_rate"],
+                       with_fluxes=True, with_aerosols=True)
+    torch.cuda.synchronize()
+    ref = fwd(atm)
+    for k in ("flux_up", "flux_dn", "flux_dn_dir", "heating_rate"):
+        e = float(np.max(np.abs(fl[k].double().cpu().numpy() - ref[k])))
+        assert e < (0.01 if k == "heating_rate" else 5e-3), f"{k}: {e:.3e}"
+    got = {k: v.double().cpu().numpy() for k, v in g.items()}
+    for key in ("tlay", "h2o", "o3"):
+        _check(f"sw+aerosol d/d{key}", got[key], _fd(fwd, atm, seeds, key), _informative(_get(atm, key)))
+    _check("sw+aerosol d/dsfc_alb_dif", got["sfc_alb_dif"], _fd_bands(fwd, atm, seeds, "sfc_alb_dif"))
+    if (atm["lwp"] > 0).any():
+        _check("sw+aerosol d/dlwp", got["lwp"], _fd(fwd, atm, seeds, "lwp"), atm["lwp"] > 0)

@@ -40,7 +40,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference", "reference-gpu-child"])
     ap.add_argument("--path", default="fused", choices=["staged", "fused"])
     ap.add_argument("--ncol", type=int, default=8192)
     ap.add_argument("--nlay", type=int, default=128)
@@ -231,6 +231,67 @@ def cpu_baseline(args, tables, seconds):
                       f"OpenMP over columns"}
 
 
+def run_reference_gpu_child(args):
+    """Child process of the reference arm: the reference's own FP64 CUDA classes
+    (oracle/_ref, built from the reference sources) timed on the all-sky forward of this
+    workload as its test driver runs it (solve_gpu, columns in blocks of 1024), and checked
+    on 64 sampled columns against the CPU port.  Prints one JSON object.  Runs in its own
+    working directory because the reference's tuner reads and rewrites a cache file there."""
+    from oracle import oracle as O
+    from oracle import ref_gpu
+    from rrtmgp_b200 import synthetic as S
+    tables = {"lw": S.make_kdist("lw"), "sw": S.make_kdist("sw"),
+              "cloud_lw": S.make_cloud_luts("lw"), "cloud_sw": S.make_cloud_luts("sw")}
+    atm = S.make_atmosphere(args.ncol, args.nlay, seed=args.seed, clouds=True)
+    ref_gpu.write_tuning(Path.cwd())
+    lib = ref_gpu.load()
+    ms_lw, ms_sw, out = ref_gpu.time_forward(lib, tables, atm, nsteps=max(3, args.steps // 5 + 1))
+    cols = np.linspace(0, args.ncol - 1, 64).astype(int)
+    sub = {k: (v[:, cols] if getattr(v, "ndim", 0) == 2 and v.shape[1] == args.ncol and
+               k not in ("emis_sfc", "sfc_alb_dir", "sfc_alb_dif") else
+               (v[cols] if getattr(v, "ndim", 0) >= 1 and v.shape[0] == args.ncol else v))
+           for k, v in atm.items() if k != "gases"}
+    sub["gases"] = {k: (v[:, cols] if v.size > 1 else v) for k, v in atm["gases"].items()}
+    sub["ncol"] = len(cols)
+    rlw = O.forward_lw(O.GasOptics(tables["lw"], S.ATM_GASES), O.CloudOptics(tables["cloud_lw"]), sub)
+    rsw = O.forward_sw(O.GasOptics(tables["sw"], S.ATM_GASES), O.CloudOptics(tables["cloud_sw"]), sub)
+    err = max(float(np.max(np.abs(out[d + "_" + k][:, cols] - r["flux_" + k])))
+              for d, r in (("lw", rlw), ("sw", rsw)) for k in ("up", "dn"))
+    ms = ms_lw + ms_sw
+    print(json.dumps({"value": args.ncol / (ms * 1e-3), "unit": "columns/s", "ms_per_step": ms,
+                      "kernel_ms": {"lw": round(ms_lw, 3), "sw": round(ms_sw, 3)}, "dtype": "f64",
+                      "max_flux_diff_vs_cpu_port_w_m2": err,
+                      "how": "the reference's Gas_optics_rrtmgp_gpu, Cloud_optics_gpu, Rte_lw_gpu, Rte_sw_gpu and "
+                             "Fluxes_broadband_gpu built from its sources (FP64), columns in blocks of 1024 as its "
+                             "solve_gpu, tuner cache pre-seeded (no tuning)"}), flush=True)
+    return 0
+
+
+def reference_gpu(args):
+    """Secondary measurement of the reference arm: the reference's GPU forward (FP64), run in a
+    child process; an {"unavailable": ...} object when it cannot run here."""
+    lib = REPO / "oracle" / "_ref" / "libref_rrtmgp_f64.so"
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no GPU"}
+    except Exception as e:   # noqa: BLE001
+        return {"unavailable": f"torch: {e}"}
+    if not lib.exists():
+        return {"unavailable": "oracle/_ref/libref_rrtmgp_f64.so not built (the reference sources are needed)"}
+    with tempfile.TemporaryDirectory() as tmp:
+        cmd = [sys.executable, str(REPO / "bench.py"), "--impl", "reference-gpu-child", "--ncol", str(args.ncol),
+               "--nlay", str(args.nlay), "--seed", str(args.seed), "--steps", str(args.steps)]
+        try:
+            r = subprocess.run(cmd, cwd=tmp, capture_output=True, text=True, timeout=900)
+        except subprocess.TimeoutExpired:
+            return {"unavailable": "reference GPU run exceeded 900 s"}
+        if r.returncode != 0:
+            return {"unavailable": "reference GPU run failed: " + (r.stderr.strip().splitlines() or ["?"])[-1][:200]}
+        lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+        return json.loads(lines[-1]) if lines else {"unavailable": "no output from the reference GPU run"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -268,6 +329,7 @@ def run_reference(args):
                                    f"(FP64 C++ restatement of the reference path; the reference's own CPU "
                                    f"build needs the absent rte-rrtmgp Fortran, gfortran, netCDF and Boost)"},
         "e2e": {"value": value, "unit": "columns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu": reference_gpu(args),
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -436,6 +498,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.impl == "reference-gpu-child":
+        return run_reference_gpu_child(args)
 
     import torch
     import torch.distributed as dist

@@ -9,6 +9,7 @@
 // (src_test/Radiation_solver.cpp:70-284).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -140,6 +141,19 @@ int guarded(F&& f)
         g_err = "reference threw a non-std exception";
         return 1;
     }
+}
+
+Cloud_optics_gpu make_cloud(const rrtmgp_b200_cloud_tables* c)
+{
+    const int nb = c->nband;
+    return Cloud_optics_gpu(host<double, 2>(c->band_lims_wvn, {2, nb}), c->radliq_lwr, c->radliq_upr, c->radliq_fac,
+                            c->radice_lwr, c->radice_upr, c->radice_fac,
+                            host<double, 2>(c->lut_extliq, {c->nsize_liq, nb}),
+                            host<double, 2>(c->lut_ssaliq, {c->nsize_liq, nb}),
+                            host<double, 2>(c->lut_asyliq, {c->nsize_liq, nb}),
+                            host<double, 3>(c->lut_extice, {c->nsize_ice, nb, c->nrghice}),
+                            host<double, 3>(c->lut_ssaice, {c->nsize_ice, nb, c->nrghice}),
+                            host<double, 3>(c->lut_asyice, {c->nsize_ice, nb, c->nrghice}));
 }
 
 }  // namespace
@@ -371,6 +385,134 @@ int ref_aerosol_optics(const rrtmgp_b200_aerosol_tables* t, const rrtmgp_b200_ga
         out(ops.get_tau(), tau);
         out(ops.get_ssa(), ssa);
         out(ops.get_g(), g);
+    });
+}
+
+
+// Times the reference's all-sky forward on the GPU the way its test driver runs it
+// (Radiation_solver_longwave/shortwave::solve_gpu, src_test/Radiation_solver.cu:419-950):
+// columns in blocks of ncol_block; per block the column subsets of the inputs, get_col_dry,
+// gas_optics, cloud_optics (LW 1scl; SW 2str + delta_scale) added by band, rte_lw / rte_sw
+// and Fluxes_broadband::reduce.  The k-distributions, cloud tables and input arrays are
+// built once, outside the timing (the driver keeps them in its solver objects).  One
+// untimed warm-up step, then nsteps timed with CUDA events per domain; ms_lw, ms_sw are the
+// mean times per step.  The broadband fluxes of the last step go to the (ncol, nlev) outputs
+// (NULL to skip).  tsi scaling is 1.
+int ref_time_forward(const rrtmgp_b200_kdist_tables* tlw, const rrtmgp_b200_kdist_tables* tsw,
+                     const rrtmgp_b200_cloud_tables* clw, const rrtmgp_b200_cloud_tables* csw,
+                     const rrtmgp_b200_gas_conc* gases, int ngases, int ncol, int nlay, int ncol_block,
+                     const double* play, const double* plev, const double* tlay, const double* tlev,
+                     const double* tsfc, const double* emis, const double* mu0, const double* alb_dir,
+                     const double* alb_dif, const double* lwp, const double* iwp, const double* rel,
+                     const double* rei, int nsteps, double* ms_lw, double* ms_sw, double* lw_up, double* lw_dn,
+                     double* sw_up, double* sw_dn)
+{
+    return guarded([&] {
+        const int nlev = nlay + 1;
+        Gas_concs gc = gas_concs(gases, ngases, ncol, nlay);
+        Gas_concs_gpu gcg(gc);
+        auto klw = make_kdist(tlw, gcg);
+        auto ksw = make_kdist(tsw, gcg);
+        Cloud_optics_gpu colw = make_cloud(clw), cosw = make_cloud(csw);
+        const int nblw = klw->get_nband(), nbsw = ksw->get_nband();
+        const auto P = dev<double, 2>(play, {ncol, nlay});
+        const auto PL = dev<double, 2>(plev, {ncol, nlev});
+        const auto TL = dev<double, 2>(tlay, {ncol, nlay});
+        const auto TV = dev<double, 2>(tlev, {ncol, nlev});
+        const auto TS = dev<double, 1>(tsfc, {ncol});
+        const auto EM = dev<double, 2>(emis, {nblw, ncol});
+        const auto M0 = dev<double, 1>(mu0, {ncol});
+        const auto AD = dev<double, 2>(alb_dir, {nbsw, ncol});
+        const auto AF = dev<double, 2>(alb_dif, {nbsw, ncol});
+        const auto LW = dev<double, 2>(lwp, {ncol, nlay});
+        const auto IW = dev<double, 2>(iwp, {ncol, nlay});
+        const auto RL = dev<double, 2>(rel, {ncol, nlay});
+        const auto RI = dev<double, 2>(rei, {ncol, nlay});
+        const Bool top_at_1 = play[0] < play[size_t(nlay - 1) * ncol];
+        Rte_lw_gpu rte_lw;
+        Rte_sw_gpu rte_sw;
+        cudaEvent_t e0, e1, e2;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventCreate(&e2);
+        double tot_lw = 0., tot_sw = 0.;
+        for (int step = 0; step <= nsteps; ++step) {
+            const bool last = step == nsteps;
+            cudaEventRecord(e0);
+            for (int c0 = 0; c0 < ncol; c0 += ncol_block) {
+                const int nb = std::min(ncol_block, ncol - c0), cs = c0 + 1, ce = c0 + nb;
+                Gas_concs_gpu gsub(gcg, cs, nb);
+                auto pl = PL.subset({{{cs, ce}, {1, nlev}}});
+                Array_gpu<double, 2> cd({nb, nlay});
+                Gas_optics_rrtmgp_gpu::get_col_dry(cd, gsub.get_vmr("h2o"), pl);
+                std::unique_ptr<Optical_props_arry_gpu> ops = std::make_unique<Optical_props_1scl_gpu>(nb, nlay, *klw);
+                Source_func_lw_gpu src(nb, nlay, *klw);
+                klw->gas_optics(P.subset({{{cs, ce}, {1, nlay}}}), pl, TL.subset({{{cs, ce}, {1, nlay}}}),
+                                TS.subset({{{cs, ce}}}), gsub, ops, src, cd, TV.subset({{{cs, ce}, {1, nlev}}}));
+                Optical_props_1scl_gpu cop(nb, nlay, colw);
+                colw.cloud_optics(LW.subset({{{cs, ce}, {1, nlay}}}), IW.subset({{{cs, ce}, {1, nlay}}}),
+                                  RL.subset({{{cs, ce}, {1, nlay}}}), RI.subset({{{cs, ce}, {1, nlay}}}), cop);
+                add_to(dynamic_cast<Optical_props_1scl_gpu&>(*ops), cop);
+                Array_gpu<double, 3> up({nb, nlev, klw->get_ngpt()}), dn({nb, nlev, klw->get_ngpt()});
+                rte_lw.rte_lw(ops, top_at_1, src, EM.subset({{{1, nblw}, {cs, ce}}}), Array_gpu<double, 2>(), up, dn, 1);
+                Fluxes_broadband_gpu fl(nb, nlev);
+                fl.reduce(up, dn, ops, top_at_1);
+                if (last && lw_up && lw_dn) {
+                    cudaDeviceSynchronize();
+                    for (int l = 0; l < nlev; ++l) {
+                        cudaMemcpy(lw_up + size_t(l) * ncol + c0, fl.get_flux_up().ptr() + size_t(l) * nb, nb * 8,
+                                   cudaMemcpyDeviceToHost);
+                        cudaMemcpy(lw_dn + size_t(l) * ncol + c0, fl.get_flux_dn().ptr() + size_t(l) * nb, nb * 8,
+                                   cudaMemcpyDeviceToHost);
+                    }
+                }
+            }
+            cudaEventRecord(e1);
+            for (int c0 = 0; c0 < ncol; c0 += ncol_block) {
+                const int nb = std::min(ncol_block, ncol - c0), cs = c0 + 1, ce = c0 + nb;
+                Gas_concs_gpu gsub(gcg, cs, nb);
+                auto pl = PL.subset({{{cs, ce}, {1, nlev}}});
+                Array_gpu<double, 2> cd({nb, nlay});
+                Gas_optics_rrtmgp_gpu::get_col_dry(cd, gsub.get_vmr("h2o"), pl);
+                std::unique_ptr<Optical_props_arry_gpu> ops = std::make_unique<Optical_props_2str_gpu>(nb, nlay, *ksw);
+                Array_gpu<double, 2> toa({nb, ksw->get_ngpt()});
+                ksw->gas_optics(P.subset({{{cs, ce}, {1, nlay}}}), pl, TL.subset({{{cs, ce}, {1, nlay}}}), gsub, ops,
+                                toa, cd);
+                Optical_props_2str_gpu cop(nb, nlay, cosw);
+                cosw.cloud_optics(LW.subset({{{cs, ce}, {1, nlay}}}), IW.subset({{{cs, ce}, {1, nlay}}}),
+                                  RL.subset({{{cs, ce}, {1, nlay}}}), RI.subset({{{cs, ce}, {1, nlay}}}), cop);
+                cop.delta_scale();
+                add_to(dynamic_cast<Optical_props_2str_gpu&>(*ops), cop);
+                const int ng = ksw->get_ngpt();
+                Array_gpu<double, 3> up({nb, nlev, ng}), dn({nb, nlev, ng}), dr({nb, nlev, ng});
+                rte_sw.rte_sw(ops, top_at_1, M0.subset({{{cs, ce}}}), toa, AD.subset({{{1, nbsw}, {cs, ce}}}),
+                              AF.subset({{{1, nbsw}, {cs, ce}}}), Array_gpu<double, 2>(), up, dn, dr);
+                Fluxes_broadband_gpu fl(nb, nlev);
+                fl.reduce(up, dn, dr, ops, top_at_1);
+                if (last && sw_up && sw_dn) {
+                    cudaDeviceSynchronize();
+                    for (int l = 0; l < nlev; ++l) {
+                        cudaMemcpy(sw_up + size_t(l) * ncol + c0, fl.get_flux_up().ptr() + size_t(l) * nb, nb * 8,
+                                   cudaMemcpyDeviceToHost);
+                        cudaMemcpy(sw_dn + size_t(l) * ncol + c0, fl.get_flux_dn().ptr() + size_t(l) * nb, nb * 8,
+                                   cudaMemcpyDeviceToHost);
+                    }
+                }
+            }
+            cudaEventRecord(e2);
+            cudaEventSynchronize(e2);
+            float a = 0.f, b = 0.f;
+            cudaEventElapsedTime(&a, e0, e1);
+            cudaEventElapsedTime(&b, e1, e2);
+            if (step > 0 && !last) { tot_lw += a; tot_sw += b; }
+            if (step == 0 && nsteps == 0) { tot_lw = a; tot_sw = b; }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaEventDestroy(e2);
+        const int n = std::max(nsteps - 1, 1);
+        *ms_lw = tot_lw / n;
+        *ms_sw = tot_sw / n;
     });
 }
 

@@ -32,21 +32,7 @@ from rrtmgp_b200 import _abi, synthetic as S  # noqa: E402
 
 LIB = REPO / "oracle" / "_ref" / "libref_rrtmgp_f64.so"
 
-TUNING = {
-    "gas_optical_depths_major_kernel": (16, 1, 8),
-    "gas_optical_depths_minor_kernel_lower": (16, 1, 1),
-    "gas_optical_depths_minor_kernel_upper": (16, 1, 1),
-    "Planck_source_kernel": (32, 4, 1),
-    "compute_tau_rayleigh_kernel": (32, 4, 1),
-    "combine_abs_and_rayleigh_kernel": (32, 4, 1),
-    "reorder123x321_kernel": (32, 4, 1),
-    "inc_2stream_by_2stream_bybnd_kernel": (16, 4, 1),
-    "lw_step_1": (32, 4, 1),
-    "lw_step_2": (64, 1, 1),
-    "lw_step_3": (32, 4, 1),
-    "sw_source_2stream_kernel": (32, 4, 1),
-    "sw_adding": (32, 4, 1),
-}
+from oracle.ref_gpu import REF_KERNEL_TUNING as TUNING, D, P, gas_array  # noqa: E402
 
 NCOL, NLAY = 5, 10
 
@@ -72,29 +58,6 @@ def aerosol_inputs(atm):
     aer, rh = S.make_aerosols(atm["play"], seed=108)
     aer["aermr05"] = np.array([3e-9])
     return aer, rh
-
-
-def D(a):
-    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
-
-
-def P(a):
-    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
-
-
-def gas_array(gases):
-    arr = (_abi.GasConc * len(gases))()
-    keep = []
-    for i, (k, v) in enumerate(gases.items()):
-        v = D(v)
-        keep.append(v)
-        arr[i].name = k.encode()
-        arr[i].vmr = v.ctypes.data
-        if v.size == 1:
-            arr[i].dim1, arr[i].dim2 = 1, 1
-        else:
-            arr[i].dim1, arr[i].dim2 = v.shape[1], v.shape[0]
-    return arr, keep
 
 
 def dense_gas_cases(lib, chk, outdir: Path):

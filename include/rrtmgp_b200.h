@@ -441,7 +441,8 @@ int rrtmgp_b200_heating_rate_sw_layers_f64(int ncol, int nlay, int ngpt, int top
  * rates, in one kernel that keeps every (layer, g-point) quantity on chip.  Outputs
  * flux_up, flux_dn, flux_net (ncol, nlay+1) and heating_rate (ncol, nlay) [K/day].  The
  * vertical orientation is taken per column from play.  chunk: layers per warp (8 or 16;
- * 0 picks the tuned default).  nlay <= 16 * chunk. */
+ * 0 picks the tuned default).  Up to 16 chunks (16 * chunk layers) a column is one CTA; deeper
+ * columns run on a thread-block cluster of ceil(chunks / 16) CTAs, nlay <= 128 * chunk. */
 int rrtmgp_b200_forward_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int ncol, int nlay,
         const float* play, const float* plev, const float* tlay, const float* tlev,
         const float* tsfc, const float* col_dry, const rrtmgp_b200_gas_conc* gases, int ngases,
@@ -455,7 +456,8 @@ int rrtmgp_b200_forward_lw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int
  * Fluxes_broadband::reduce -- plus heating rates, in one kernel.  mu0 (ncol) > 0; surface
  * albedos (nband, ncol) in the reference's column-fastest order.  Outputs flux_up, flux_dn
  * (direct included), flux_dn_dir, flux_net (ncol, nlay+1) and heating_rate (ncol, nlay).
- * chunk: layers per warp (8 or 16; 0: 8 up to 128 layers, else 16).  nlay <= 16 * chunk. */
+ * chunk: layers per warp (8 or 16; 0: 8 up to 128 layers, else 16).  Columns of more than 16
+ * chunks run on a thread-block cluster of ceil(chunks / 16) CTAs; nlay <= 128 * chunk. */
 int rrtmgp_b200_forward_sw_f32(rrtmgp_b200_kdist k, rrtmgp_b200_cloud cloud, int ncol, int nlay,
         const float* play, const float* plev, const float* tlay, const float* col_dry,
         const rrtmgp_b200_gas_conc* gases, int ngases, const float* lwp, const float* iwp,

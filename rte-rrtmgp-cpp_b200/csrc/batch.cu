@@ -68,8 +68,13 @@ struct TeamCtx {
     __device__ __forceinline__ int icol() const { return ic; }
     __device__ __forceinline__ int warp() const { return int(threadIdx.x >> 5) - fw; }
     __device__ __forceinline__ int nwarps() const { return nw; }
+    __device__ __forceinline__ int lwarp() const { return int(threadIdx.x >> 5) - fw; }
     __device__ __forceinline__ int tid() const { return int(threadIdx.x) - 32 * fw; }
     __device__ __forceinline__ int nthreads() const { return 32 * nw; }
+    __device__ __forceinline__ int layer0() const { return 0; }
+    __device__ __forceinline__ int nloc(int nlay) const { return nlay; }
+    template <class T>
+    __device__ __forceinline__ void put(T* p, const T& v) const { *p = v; }
     __device__ __forceinline__ unsigned char* smem() const
     {
         extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -260,8 +265,9 @@ size_t team_smem_bytes(const rrtmgp_b200_batch_t* b, int domain, int nlay, int c
 {
     const KdistView<float>& v = b->k[domain]->v32;
     const int W = ceil_div_i(nlay, cl);
-    const SmemLayout L = domain == 0 ? smem_layout(nlay, v.ngas, v.nband, 1, W, 2, cl, v.max_group_bands, v.max_nscal)
-                                     : smem_layout(nlay, v.ngas, v.nband, 0, W, 3, cl,
+    // as the column code lays it out: by capacity, W cl layers
+    const SmemLayout L = domain == 0 ? smem_layout(W * cl, v.ngas, v.nband, 1, W, 2, cl, v.max_group_bands, v.max_nscal)
+                                     : smem_layout(W * cl, v.ngas, v.nband, 0, W, 3, cl,
                                                    v.max_group_bands * (cl == 8 ? 2 : 1), v.max_nscal);
     return align16(L.total);
 }

@@ -14,6 +14,14 @@ __global__ void __launch_bounds__(512) sw_forward_kernel(const KdistView<float> 
     sw_forward_column<CL, true, DENSE>(CtaCtx{}, k, io);
 }
 
+// Columns of more than 16 chunks: one thread-block cluster of cs CTAs per column (ClusterCtx).
+template <int CL, bool DENSE>
+__global__ void __launch_bounds__(512) sw_forward_cluster_kernel(const KdistView<float> k, const SwGridIo io, int cs)
+{
+    sw_forward_column<CL, true, DENSE>(ClusterCtx<CL>{cs}, k, io);
+    cooperative_groups::this_cluster().sync();   // no CTA leaves while another may store into its shared memory
+}
+
 template <int CL, bool DENSE>
 int launch_sw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nlay, const float* play,
                       const float* plev, const float* tlay, const float* col_dry, const GasSet<float>& gs,
@@ -23,13 +31,20 @@ int launch_sw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
 {
     const KdistView<float>& v = k->v32;
     const int NW = (nlay + CL - 1) / CL;
-    RB_CHECK_ARG(NW <= 16, "forward_sw: nlay too large for the fused kernel (at most 16 chunks)");
-    const size_t smem = smem_layout(nlay, v.ngas, v.nband, aer.present ? 4 : 0, NW, 3, CL,
-                                    v.max_group_bands * (CL == 8 ? 2 : 1), v.max_nscal).total;
+    // more than 16 chunks: a cluster of CS CTAs of NWc warps per column
+    const int CS = (NW + 15) / 16, NWc = (NW + CS - 1) / CS;
+    RB_CHECK_ARG(CS <= 8, "forward_sw: nlay too large for the fused kernel (at most 128 chunks)");
+    const size_t smem = smem_layout(NWc * CL, v.ngas, v.nband, aer.present ? 4 : 0, CS * NWc, 3, CL,
+                                    v.max_group_bands * (CL == 8 ? 2 : 1), v.max_nscal, NWc).total;
     if (smem > 220 * 1024) return fail(RRTMGP_B200_ERR_UNSUPPORTED, "forward_sw: shared memory need exceeds 220 KB");
     static PerDeviceOnce attr;
-    int st = attr.run([] { return cudaFuncSetAttribute(sw_forward_kernel<CL, DENSE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       220 * 1024); }, "forward_sw attribute");
+    int st = attr.run([] {
+        const cudaError_t e = cudaFuncSetAttribute(sw_forward_kernel<CL, DENSE>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+        if (e != cudaSuccess) return e;
+        return cudaFuncSetAttribute(sw_forward_cluster_kernel<CL, DENSE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    220 * 1024);
+    }, "forward_sw attribute");
     if (st) return st;
     SwCloudArgs ca{};
     if (c) {
@@ -40,8 +55,24 @@ int launch_sw_forward(rrtmgp_b200_kdist k, rrtmgp_b200_cloud c, int ncol, int nl
         ca.delta = delta;
     }
     SwGridIo io{ncol, nlay, play, plev, tlay, col_dry, mu0, tsi, alb_dir, alb_dif, up, dn, dir, net, hr, gs, ca, aer};
-    sw_forward_kernel<CL, DENSE><<<ncol, NW * 32, smem, stream>>>(v, io);
-    RB_LAUNCH("sw_forward_kernel");
+    if (CS == 1) {
+        sw_forward_kernel<CL, DENSE><<<ncol, NW * 32, smem, stream>>>(v, io);
+        RB_LAUNCH("sw_forward_kernel");
+        return RRTMGP_B200_OK;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(ncol) * CS);
+    cfg.blockDim = dim3(NWc * 32);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = unsigned(CS);
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    RB_CUDA(cudaLaunchKernelEx(&cfg, sw_forward_cluster_kernel<CL, DENSE>, v, io, CS), "sw_forward_cluster_kernel");
     return RRTMGP_B200_OK;
 }
 

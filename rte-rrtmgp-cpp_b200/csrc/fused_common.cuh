@@ -9,6 +9,8 @@
 // 128-bit corner-packed global loads (KdistView::kmaj4 & co.).
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include <cfloat>
 #include <cmath>
 
@@ -209,21 +211,65 @@ __device__ __forceinline__ int4 minor_entry(const int4* mgt, int g, bool valid)
     return m;
 }
 
-// Context of a fused column computation when the whole CTA computes column blockIdx.x: every
-// value is a special register or a launch constant, so none occupies a register across the
-// column.  The batched kernel supplies its own context type with the same members.
+// Context of a fused column computation.  Members: icol(); warp() = the chunk this warp owns
+// and nwarps() = the chunks of the column; lwarp() = the warp within the CTA (or team) that
+// holds its shared memory; tid() / nthreads() of that CTA (team); smem(); sync() = the barrier
+// of every warp of the column; layer0() / nloc(nlay) = the layers whose state that shared
+// memory holds; put(p, v) stores v at p in the shared memory of every CTA that reads it.
+// CtaCtx: the whole CTA computes column blockIdx.x; every value is a special register or a
+// launch constant, so none occupies a register across the column.  The batched kernel
+// supplies its own context type with the same members.
 struct CtaCtx {
     __device__ __forceinline__ int icol() const { return blockIdx.x; }
     __device__ __forceinline__ int warp() const { return threadIdx.x >> 5; }
     __device__ __forceinline__ int nwarps() const { return blockDim.x >> 5; }
+    __device__ __forceinline__ int lwarp() const { return threadIdx.x >> 5; }
     __device__ __forceinline__ int tid() const { return threadIdx.x; }
     __device__ __forceinline__ int nthreads() const { return blockDim.x; }
+    __device__ __forceinline__ int layer0() const { return 0; }
+    __device__ __forceinline__ int nloc(int nlay) const { return nlay; }
     __device__ __forceinline__ unsigned char* smem() const
     {
         extern __shared__ __align__(16) unsigned char smem_raw[];
         return smem_raw;
     }
     __device__ __forceinline__ void sync() const { __syncthreads(); }
+    template <class T>
+    __device__ __forceinline__ void put(T* p, const T& v) const { *p = v; }
+};
+
+// One column on a thread-block cluster of cs CTAs (columns deeper than one CTA holds): CTA r
+// of the cluster owns the chunks [r W, (r + 1) W) (W = its warps) and the state of their
+// layers [r W CL, (r + 1) W CL); the chunk quantities every warp reads are stored into the
+// shared memory of all CTAs of the cluster (distributed shared memory) and the barrier is the
+// cluster's.
+template <int CL>
+struct ClusterCtx {
+    int cs;
+    __device__ __forceinline__ int rank() const { return int(cooperative_groups::this_cluster().block_rank()); }
+    __device__ __forceinline__ int icol() const { return blockIdx.x / cs; }
+    __device__ __forceinline__ int warp() const { return rank() * int(blockDim.x >> 5) + int(threadIdx.x >> 5); }
+    __device__ __forceinline__ int nwarps() const { return cs * int(blockDim.x >> 5); }
+    __device__ __forceinline__ int lwarp() const { return threadIdx.x >> 5; }
+    __device__ __forceinline__ int tid() const { return threadIdx.x; }
+    __device__ __forceinline__ int nthreads() const { return blockDim.x; }
+    __device__ __forceinline__ int layer0() const { return rank() * int(blockDim.x >> 5) * CL; }
+    __device__ __forceinline__ int nloc(int nlay) const
+    {
+        return max(0, min(int(blockDim.x >> 5) * CL, nlay - layer0()));
+    }
+    __device__ __forceinline__ unsigned char* smem() const
+    {
+        extern __shared__ __align__(16) unsigned char smem_raw[];
+        return smem_raw;
+    }
+    __device__ __forceinline__ void sync() const { cooperative_groups::this_cluster().sync(); }
+    template <class T>
+    __device__ __forceinline__ void put(T* p, const T& v) const
+    {
+        cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+        for (int r = 0; r < cs; ++r) *cl.map_shared_rank(p, r) = v;
+    }
 };
 
 // Fill the per-layer state and col_gas of layers j0 .. j0 + nloc - 1 (counted from the top,
@@ -290,9 +336,13 @@ struct SmemLayout {
 
 __host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
+// nlay: layers whose state the CTA holds; NW: chunks of the column (maps); NWloc: warps of
+// the CTA (records).
 __host__ __device__ __forceinline__ SmemLayout smem_layout(int nlay, int ngas, int nband, int ncloud_vals, int NW,
-                                                           int nmaps, int CL, int nbands_per_group, int nscal)
+                                                           int nmaps, int CL, int nbands_per_group, int nscal,
+                                                           int NWloc = -1)
 {
+    if (NWloc < 0) NWloc = NW;
     SmemLayout L;
     L.state = 0;
     L.cg = align16(L.state + sizeof(LayerState) * size_t(nlay));
@@ -301,7 +351,7 @@ __host__ __device__ __forceinline__ SmemLayout smem_layout(int nlay, int ngas, i
     L.maps = align16(L.cloud + sizeof(float) * size_t(ncloud_vals) * nband * nlay);
     L.sfc = align16(L.maps + sizeof(float4) * size_t(NW) * 32 * nmaps);
     L.recs = align16(L.sfc + sizeof(float) * 64);
-    L.total = align16(L.recs + sizeof(Rec) * size_t(NW) * CL * nbands_per_group);
+    L.total = align16(L.recs + sizeof(Rec) * size_t(NWloc) * CL * nbands_per_group);
     return L;
 }
 

@@ -103,8 +103,13 @@ __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<
     constexpr bool P2 = PAIR && CL == 8;
     const int lane = threadIdx.x & 31;
     const int nband = k.nband;
-    const SmemLayout SL = smem_layout(io.nlay(), k.ngas, nband, 1, cx.nwarps(), 2, CL,
-                                      k.max_group_bands * (P2 ? 2 : 1), k.max_nscal);
+    // layer state of the layers [L0, L0 + NL) in this CTA's shared memory, indexed j - L0
+    const int L0 = cx.layer0(), NL = cx.nloc(io.nlay());
+    const int NWloc = cx.nthreads() >> 5;
+    // sized by capacity (NWloc CL layers), the same in every CTA of a cluster: the chunk maps
+    // stored into another CTA's shared memory land at the offset this CTA uses
+    const SmemLayout SL = smem_layout(NWloc * CL, k.ngas, nband, 1, cx.nwarps(), 2, CL,
+                                      k.max_group_bands * (P2 ? 2 : 1), k.max_nscal, NWloc);
     unsigned char* const smem_raw = cx.smem();
     LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
     float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
@@ -114,8 +119,8 @@ __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<
     // start the next group while others still read this group's (one barrier per group)
     float4* const sm_maps0 = reinterpret_cast<float4*>(smem_raw + SL.maps);
     float* const sm_sfc0 = reinterpret_cast<float*>(smem_raw + SL.sfc);
-    Rec* const recs0 = reinterpret_cast<Rec*>(smem_raw + SL.recs) + cx.warp() * CL * k.max_group_bands;
-    const int rbuf = cx.nwarps() * CL * k.max_group_bands;   // records per buffer
+    Rec* const recs0 = reinterpret_cast<Rec*>(smem_raw + SL.recs) + cx.lwarp() * CL * k.max_group_bands;
+    const int rbuf = NWloc * CL * k.max_group_bands;   // records per buffer
 
     bool top_at_1;
     float ts;
@@ -124,11 +129,11 @@ __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<
         const float* play = io.play();
         top_at_1 = play[icol] < play[icol + size_t(nlay - 1) * ncol];
         ts = io.tsfc()[icol];
-        setup_layers(k, io.gs(), ncol, nlay, icol, top_at_1, play, io.plev(), io.tlay(), io.tlev(), io.col_dry(), st,
-                     sm_cg, cx.tid(), cx.nthreads());
+        setup_layer_range(k, io.gs(), ncol, nlay, icol, top_at_1, play, io.plev(), io.tlay(), io.tlev(), io.col_dry(),
+                          st, sm_cg, NL, L0, NL, cx.tid(), cx.nthreads());
         const CloudArgs cld = io.cloud();
-        for (int idx = cx.tid(); idx < nlay * nband; idx += cx.nthreads()) {
-            const int j = idx % nlay, b = idx / nlay;
+        for (int idx = cx.tid(); idx < NL * nband; idx += cx.nthreads()) {
+            const int jl = idx % NL, b = idx / NL, j = L0 + jl;
             float tau = 0.f, s, g;
             if (cld.present) {
                 const int l = top_at_1 ? j : nlay - 1 - j;
@@ -136,11 +141,11 @@ __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<
                 const CloudPoint<float> cp = cloud_point(cld.L, cld.lwp[cl], cld.iwp[cl], cld.rel[cl], cld.rei[cl]);
                 cloud_band<float, false>(cld.L, cp, b, tau, s, g);
             }
-            sm_cld[b * nlay + j] = tau;
+            sm_cld[b * NL + jl] = tau;
         }
     }
     cx.sync();
-    layer_minor_scalings(k, st, sm_cg, io.nlay(), sm_sc, io.nlay(), cx.tid(), cx.nthreads());
+    layer_minor_scalings(k, st, sm_cg, NL, sm_sc, NL, cx.tid(), cx.nthreads());
     cx.sync();
 
     const float D = 1.66f;                 // single-angle secant (Rte_lw.cpp:101-113)
@@ -168,11 +173,11 @@ __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<
             for (int t = lane; t < (P2 ? 2 : 1) * nrec; t += 32) {
                 const int gq = gg + t / nrec, r = t % nrec;
                 if (gq >= k.ngroups) continue;
-                const int jj = cx.warp() * CL + (r % CL);
+                const int jj = cx.warp() * CL + (r % CL), jl = jj - L0;
                 const int b = k.group_band0[gq] + r / CL;
                 if (jj < nlay && b < nband && k.band_lims[2 * b] < 32 * gq + 32)
-                    build_lw_record(k, recs0[(P2 ? (gq & 1) : 0) * rbuf + r], st[jj], sm_cg + jj, nlay, b,
-                                    sm_cld[b * nlay + jj], jj == nlay - 1, ts);
+                    build_lw_record(k, recs0[(P2 ? (gq & 1) : 0) * rbuf + r], st[jl], sm_cg + jl, NL, b,
+                                    sm_cld[b * NL + jl], jj == nlay - 1, ts);
             }
         }
         __syncwarp();
@@ -188,15 +193,16 @@ __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<
             if (j < nlay && gv) {
                 const Rec& R = recs[slot * CL + i];
                 const float tau =
-                    tau_abs<DENSE>(k, R, g, R.a ? mg1 : mg0, R.a ? nm1 : nm0, sm_sc + j * k.max_nscal) + R.aux.w;
+                    tau_abs<DENSE>(k, R, g, R.a ? mg1 : mg0, R.a ? nm1 : nm0, sm_sc + (j - L0) * k.max_nscal) +
+                    R.aux.w;
                 const float4 p0 = __ldg(k.pfrac4 + (R.kb.x + g));
                 const float4 p1 = __ldg(k.pfrac4 + (R.kb.y + g));
                 const float pfrac = (R.wpl0.x * p0.x + R.wpl0.y * p0.y + R.wpl0.z * p0.z + R.wpl0.w * p0.w) +
                                     (R.wpl1.x * p1.x + R.wpl1.y * p1.y + R.wpl1.z * p1.z + R.wpl1.w * p1.w);
                 lw_layer_fast(tau, D, pfrac * R.aux.x, pfrac * R.aux.z, pfrac * R.aux.y, omt[i], sdn[i], sup[i]);
-                if (j == nlay - 1) sm_sfc[lane] = pfrac * R.aux2;
+                if (j == nlay - 1) cx.put(&sm_sfc[lane], pfrac * R.aux2);
             } else if (j == nlay - 1) {
-                sm_sfc[lane] = 0.f;
+                cx.put(&sm_sfc[lane], 0.f);
             }
             Ad = (1.f - omt[i]) * Ad;
             Bd = (1.f - omt[i]) * Bd + sdn[i];
@@ -207,7 +213,7 @@ __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<
             Au = (1.f - omt[i]) * Au;
             Bu = (1.f - omt[i]) * Bu + sup[i];
         }
-        sm_maps[cx.warp() * 32 + lane] = make_float4(Ad, Bd, Au, Bu);
+        cx.put(&sm_maps[cx.warp() * 32 + lane], make_float4(Ad, Bd, Au, Bu));
         cx.sync();
 
         // 3. incoming radiances of the chunk (no incident longwave flux at the top)
@@ -279,7 +285,7 @@ __device__ __forceinline__ void lw_forward_column(const Cx& cx, const KdistView<
         if (jl < nlay && (lane >> SH_DIV) < CL) {
             const int l = top_at_1 ? jl : nlay - 1 - jl;
             const double g0_cp = 9.80665 / 1004.64;
-            heating_rate[icol + size_t(l) * ncol] = float(g0_cp * 86400.0 * pi * acc_div / double(st[jl].dp));
+            heating_rate[icol + size_t(l) * ncol] = float(g0_cp * 86400.0 * pi * acc_div / double(st[jl - L0].dp));
         }
     }
     if (w == NW - 1 && lane == 0) {

@@ -72,8 +72,12 @@ __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<
     const int nband = k.nband;
     const bool with_aer = io.aerosol().present != 0;
     // the "cloud" region holds the aerosol (tau, tau ssa, tau ssa g, tau (1 - ssa)) per (band, layer)
-    const SmemLayout SL = smem_layout(io.nlay(), k.ngas, nband, with_aer ? 4 : 0, cx.nwarps(), 3, CL,
-                                      k.max_group_bands * (P2 ? 2 : 1), k.max_nscal);
+    // layer state of the layers [L0, L0 + NL) in this CTA's shared memory, indexed j - L0
+    const int L0 = cx.layer0(), NL = cx.nloc(io.nlay());
+    const int NWloc = cx.nthreads() >> 5;
+    // sized by capacity (NWloc CL layers), the same in every CTA of a cluster (as lw_forward_column)
+    const SmemLayout SL = smem_layout(NWloc * CL, k.ngas, nband, with_aer ? 4 : 0, cx.nwarps(), 3, CL,
+                                      k.max_group_bands * (P2 ? 2 : 1), k.max_nscal, NWloc);
     unsigned char* const smem_raw = cx.smem();
     LayerState* st = reinterpret_cast<LayerState*>(smem_raw + SL.state);
     float* sm_cg = reinterpret_cast<float*>(smem_raw + SL.cg);
@@ -81,8 +85,8 @@ __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<
     float* sm_pt = reinterpret_cast<float*>(smem_raw + SL.maps);                            // [NW][32]
     float4* sm_comp = reinterpret_cast<float4*>(smem_raw + SL.maps) + cx.nwarps() * 32;     // [NW][32]
     float* sm_compd = reinterpret_cast<float*>(sm_comp + cx.nwarps() * 32);                 // [NW][32]
-    Rec* const recs0 = reinterpret_cast<Rec*>(smem_raw + SL.recs) + cx.warp() * CL * k.max_group_bands;
-    const int rbuf = cx.nwarps() * CL * k.max_group_bands;   // records per buffer
+    Rec* const recs0 = reinterpret_cast<Rec*>(smem_raw + SL.recs) + cx.lwarp() * CL * k.max_group_bands;
+    const int rbuf = NWloc * CL * k.max_group_bands;   // records per buffer
 
     bool top_at_1;
     float mu0, tsi;
@@ -92,18 +96,18 @@ __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<
         top_at_1 = play[icol] < play[icol + size_t(nlay - 1) * ncol];
         mu0 = io.mu0()[icol];
         tsi = io.tsi() ? io.tsi()[icol] : 1.f;
-        setup_layers(k, io.gs(), ncol, nlay, icol, top_at_1, play, io.plev(), io.tlay(), nullptr, io.col_dry(), st,
-                     sm_cg, cx.tid(), cx.nthreads());
+        setup_layer_range(k, io.gs(), ncol, nlay, icol, top_at_1, play, io.plev(), io.tlay(), nullptr, io.col_dry(),
+                          st, sm_cg, NL, L0, NL, cx.tid(), cx.nthreads());
     }
     const float mu0_inv = 1.f / mu0;
     cx.sync();
-    layer_minor_scalings(k, st, sm_cg, io.nlay(), sm_sc, io.nlay(), cx.tid(), cx.nthreads());
-    float4* const sm_aer = reinterpret_cast<float4*>(smem_raw + SL.cloud);   // [band][layer]
+    layer_minor_scalings(k, st, sm_cg, NL, sm_sc, NL, cx.tid(), cx.nthreads());
+    float4* const sm_aer = reinterpret_cast<float4*>(smem_raw + SL.cloud);   // [band][local layer]
     if (with_aer) {
         const int nlay = io.nlay();
-        for (int idx = cx.tid(); idx < nlay * nband; idx += cx.nthreads()) {
-            const int j = idx % nlay, b = idx / nlay;
-            sm_aer[idx] = aerosol_point(io.aerosol(), io.ncol(), cx.icol(), top_at_1 ? j : nlay - 1 - j, st[j].dp, b);
+        for (int idx = cx.tid(); idx < NL * nband; idx += cx.nthreads()) {
+            const int jl = idx % NL, b = idx / NL, j = L0 + jl;
+            sm_aer[idx] = aerosol_point(io.aerosol(), io.ncol(), cx.icol(), top_at_1 ? j : nlay - 1 - j, st[jl].dp, b);
         }
     }
     cx.sync();
@@ -135,9 +139,9 @@ __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<
                 const int b = k.group_band0[gq] + r / CL;
                 if (jj < nlay && b < nband && k.band_lims[2 * b] < 32 * gq + 32) {
                     const int l = top_at_1 ? jj : nlay - 1 - jj;
-                    build_sw_record(k, recs0[(P2 ? (gq & 1) : 0) * rbuf + r], st[jj], sm_cg + jj, nlay, b,
+                    build_sw_record(k, recs0[(P2 ? (gq & 1) : 0) * rbuf + r], st[jj - L0], sm_cg + (jj - L0), NL, b,
                                     io.cloud(), cx.icol() + size_t(l) * io.ncol(),
-                                    with_aer ? sm_aer + b * nlay + jj : nullptr);
+                                    with_aer ? sm_aer + b * NL + (jj - L0) : nullptr);
                 }
             }
         }
@@ -155,7 +159,7 @@ __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<
             if (j < nlay && gv) {
                 const Rec& Rc = recs[slot * CL + i];
                 const float ta =
-                    tau_abs<DENSE>(k, Rc, g, Rc.a ? mg1 : mg0, Rc.a ? nm1 : nm0, sm_sc + j * k.max_nscal);
+                    tau_abs<DENSE>(k, Rc, g, Rc.a ? mg1 : mg0, Rc.a ? nm1 : nm0, sm_sc + (j - L0) * k.max_nscal);
                 const float2 r0 = __ldg(k.krayl2 + (Rc.kr[0] + g));
                 const float2 r1 = __ldg(k.krayl2 + (Rc.kr[1] + g));
                 const float tr = (Rc.fm.x * r0.x + Rc.fm.y * r0.y + Rc.fm.z * r1.x + Rc.fm.w * r1.y) * Rc.aux.x;
@@ -190,7 +194,7 @@ __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<
             cD = nD;
             P *= Tn;
         }
-        sm_pt[cx.warp() * 32 + lane] = P;
+        cx.put(&sm_pt[cx.warp() * 32 + lane], P);
         cx.sync();
 
         // 2. direct flux at the chunk top and at the surface
@@ -210,8 +214,8 @@ __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<
             ReduceScatter<2 * CL, 16>::run(v, lane);
             acc_a += double(v[0]);
         }
-        sm_comp[w * 32 + lane] = make_float4(cRu, cRd, cT, cU * dtop);
-        sm_compd[w * 32 + lane] = cD * dtop;
+        cx.put(&sm_comp[w * 32 + lane], make_float4(cRu, cRd, cT, cU * dtop));
+        cx.put(&sm_compd[w * 32 + lane], cD * dtop);
         cx.sync();
 
         // 3. albedo and source at this chunk's bottom; incident diffuse flux at its top
@@ -311,7 +315,8 @@ __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<
             if (jl < nlay) {
                 const int l = top_at_1 ? jl : nlay - 1 - jl;
                 const double g0_cp = 9.80665 / 1004.64;
-                heating_rate[icol + size_t(l) * ncol] = float(g0_cp * 86400.0 * (acc_a + acc_b) / double(st[jl].dp));
+                heating_rate[icol + size_t(l) * ncol] =
+                    float(g0_cp * 86400.0 * (acc_a + acc_b) / double(st[jl - L0].dp));
             }
         }
     }

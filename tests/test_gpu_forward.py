@@ -216,3 +216,23 @@ def test_staged_fp32_heating_rates_match_oracle(oracle_mod, tables, gpu, top_at_
                                 oracle_mod.CloudOptics(tables["cloud_sw"]), atm)
     _check(lw, rlw, atm, f"staged fp32 lw top_at_1={top_at_1}")
     _check_sw(sw, rsw, f"staged fp32 sw top_at_1={top_at_1}")
+
+
+@pytest.mark.parametrize("nlay,top_at_1", [(300, True), (520, False), (1000, True)])
+def test_fused_deep_columns_on_clusters(oracle_mod, tables, gpu, nlay, top_at_1):
+    """Columns of more than 16 chunks (here 19 to 63 chunks of 16 layers) run on a thread-block
+    cluster of 2 to 4 CTAs per column, the chunk maps in distributed shared memory; LW and SW
+    against the oracle with the bounds of the other fused tests."""
+    import torch
+    from rrtmgp_b200.solver import atm_to_device
+    base, fused = _solvers(tables)
+    atm = _vary_surface(S.make_atmosphere(9, nlay, seed=nlay, clouds=True, top_at_1=top_at_1), nlay + 1)
+    d = atm_to_device(atm, torch.float32, gpu)
+    lw, sw = fused.solve_lw(d), fused.solve_sw(d)
+    torch.cuda.synchronize()
+    rlw = oracle_mod.forward_lw(oracle_mod.GasOptics(tables["lw"], S.ATM_GASES),
+                                oracle_mod.CloudOptics(tables["cloud_lw"]), atm)
+    rsw = oracle_mod.forward_sw(oracle_mod.GasOptics(tables["sw"], S.ATM_GASES),
+                                oracle_mod.CloudOptics(tables["cloud_sw"]), atm)
+    _check(lw, rlw, atm, f"deep lw nlay={nlay}")
+    _check_sw(sw, rsw, f"deep sw nlay={nlay}")

@@ -331,6 +331,12 @@ int rrtmgp_b200_rte_lw_jac_f64(rrtmgp_b200_bands b, int ncol, int nlay, int top_
         const double* sfc_emis, const double* inc_flux, int n_gauss_angles, double* gpt_flux_up,
         double* gpt_flux_dn, double* gpt_flux_up_jac, void* stream);
 
+/* No reference counterpart.  Kernels that copy their inputs with TMA tile loads wait for each
+ * copy for at most 2 s; a copy that has not landed by then ends the kernel early (its outputs
+ * are then incomplete) and is counted on the current device.  *count receives that count
+ * since the library was loaded (0 in normal operation); the call synchronises the device. */
+int rrtmgp_b200_device_wait_timeouts(unsigned int* count);
+
 /* Rte_sw_gpu::rte_sw (include/Rte_sw.h:65-75; src_cuda/Rte_sw.cu:116-161), two-stream +
  * adding (rte_solver_kernels.cu:188-278,535-647; F90 :512-606,996-1228).  mu0 (ncol);
  * inc_flux_dir (ncol, ngpt); sfc_alb_dir/dif (nband, ncol); inc_flux_dif (ncol, ngpt) or

@@ -9,7 +9,8 @@
 //     when nlay is too large), and the shortwave adding recurrences use the caller workspace
 //     plus the output arrays themselves.
 // Every layer read and level write is a coalesced row either way.  The shortwave workspace is
-// required by the C ABI whichever kernel runs.
+// needed only by the second kind.  The FP32 longwave solver up to 192 layers stages its layer
+// inputs through shared memory with TMA tile copies (lw_solver_tma).
 #include <algorithm>
 #include <cfloat>
 #include <mutex>
@@ -17,6 +18,7 @@
 #include "common.cuh"
 #include "rte_device.cuh"
 #include "sw_common.cuh"
+#include "tma.cuh"
 
 namespace rrtmgp_b200 {
 namespace {
@@ -199,44 +201,25 @@ __global__ void sw_solver_kernel(int ncol, int nlay, int ngpt, int nband, int to
 // the chunk's affine maps in registers, the chunks exchange the maps through shared memory,
 // and a re-sweep of the registers writes every level once: the HBM traffic is the algorithmic
 // one (inputs read once, outputs written once), with no shared-memory stash or workspace.
-template <typename T, int CL, int MAXT>
-__global__ void __launch_bounds__(MAXT) lw_solver_chunked(int ncol, int nlay, int nband, int top_at_1,
-                                                          const int* __restrict__ gpt2band, const T* __restrict__ tau,
-                                                          const T* __restrict__ lay_src, const T* __restrict__ lev_inc,
-                                                          const T* __restrict__ lev_dec, const T* __restrict__ sfc_src,
-                                                          const T* __restrict__ sfc_emis, const T* __restrict__ inc_flux,
-                                                          T* __restrict__ flux_up, T* __restrict__ flux_dn,
-                                                          const T* __restrict__ sfc_src_jac, T* __restrict__ flux_up_jac)
-{
-    __shared__ T sm_a[16 * 32], sm_bd[16 * 32], sm_bu[16 * 32];   // chunk maps [chunk][lane]
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int icol = blockIdx.x * 32 + lane;
-    const bool cv = icol < ncol;
-    const int ic = cv ? icol : 0;
-    const int g = blockIdx.y;
-    const size_t ncl = size_t(ncol) * nlay, ncv = size_t(ncol) * (nlay + 1);
-    const T* lev_dn = top_at_1 ? lev_inc : lev_dec;
-    const T* lev_up = top_at_1 ? lev_dec : lev_inc;
-    const int j0 = w * CL;
-    // one angle (D = 1.66, weight 0.5: Rte_lw.cpp:101-113)
-    const T D = T(1.66);
-    const T two_pi_w = pi_value<T>();
 
-    // every input of the chunk is read before any is used (the layer terms branch, and loads
-    // are not moved above a branch: read in the loop, one layer's rows would be in flight)
-    T tr[CL], sdn[CL], sup[CL], lay[CL];
-#pragma unroll
-    for (int i = 0; i < CL; ++i) {
-        const int j = j0 + i;
-        tr[i] = T(0); lay[i] = T(0); sdn[i] = T(0); sup[i] = T(0);
-        if (cv && j < nlay) {
-            const size_t x = ic + size_t(g) * ncl + size_t(top_at_1 ? j : nlay - 1 - j) * ncol;
-            tr[i] = tau[x];
-            lay[i] = lay_src[x];
-            sdn[i] = lev_dn[x];
-            sup[i] = lev_up[x];
-        }
-    }
+// Arguments of the chunked longwave solvers other than the layer inputs.
+template <typename T>
+struct LwChunkArgs {
+    int ncol, nlay, nband, top_at_1;
+    const int* gpt2band;
+    const T *sfc_src, *sfc_emis, *inc_flux, *sfc_src_jac;
+    T *flux_up, *flux_dn, *flux_up_jac;
+};
+
+// Layer inputs (tau, Planck sources; tr/sdn/sup are overwritten with the transmissivity and
+// the layer sources) -> the chunk's maps: the down sweep x -> A x + Bd and the up sweep
+// x -> A x + Bu, stored at [w][lane] of sm_a, sm_bd, sm_bu.  One angle (D = 1.66, weight 0.5:
+// Rte_lw.cpp:101-113).
+template <typename T, int CL>
+__device__ __forceinline__ void lw_chunk_maps(T (&tr)[CL], const T (&lay)[CL], T (&sdn)[CL], T (&sup)[CL], T* sm_a,
+                                              T* sm_bd, T* sm_bu, int w, int lane)
+{
+    const T D = T(1.66);
     T A = T(1), Bd = T(0), Bu = T(0);
 #pragma unroll
     for (int i = 0; i < CL; ++i) {
@@ -249,27 +232,38 @@ __global__ void __launch_bounds__(MAXT) lw_solver_chunked(int ncol, int nlay, in
     sm_a[w * 32 + lane] = A;
     sm_bd[w * 32 + lane] = Bd;
     sm_bu[w * 32 + lane] = Bu;
-    __syncthreads();
-    if (!cv) return;
+}
+
+// After the maps of all nw chunks are visible: the radiances entering the chunk (scan over the
+// chunks above, then below through the surface), and re-sweeps writing every level of the
+// chunk (column ic, g-point g; level j0 + i is the top of layer j0 + i).
+template <typename T, int CL>
+__device__ __forceinline__ void lw_chunk_levels(const LwChunkArgs<T>& a, const T (&tr)[CL], const T (&sdn)[CL],
+                                                const T (&sup)[CL], const T* sm_a, const T* sm_bd, const T* sm_bu,
+                                                int w, int nw, int lane, int ic, int g)
+{
+    const int ncol = a.ncol, nlay = a.nlay;
+    const size_t ncv = size_t(ncol) * (nlay + 1);
+    const T two_pi_w = pi_value<T>();
+    const int j0 = w * CL;
     // radiance entering the chunk at its top, then at the surface
-    T radn = (inc_flux ? inc_flux[ic + size_t(g) * ncol] : T(0)) / two_pi_w;
+    T radn = (a.inc_flux ? a.inc_flux[ic + size_t(g) * ncol] : T(0)) / two_pi_w;
     for (int c = 0; c < w; ++c) radn = sm_a[c * 32 + lane] * radn + sm_bd[c * 32 + lane];
     T rs = radn;
     for (int c = w; c < nw; ++c) rs = sm_a[c * 32 + lane] * rs + sm_bd[c * 32 + lane];
-    const T emis = sfc_emis[gpt2band[g] + size_t(ic) * nband];
-    const T rsfc = rs * (T(1) - emis) + emis * sfc_src[ic + size_t(g) * ncol];   // leaving the surface
+    const T emis = a.sfc_emis[a.gpt2band[g] + size_t(ic) * a.nband];
+    const T rsfc = rs * (T(1) - emis) + emis * a.sfc_src[ic + size_t(g) * ncol];   // leaving the surface
     T rup = rsfc;
     for (int c = nw - 1; c > w; --c) rup = sm_a[c * 32 + lane] * rup + sm_bu[c * 32 + lane];
     // surface-temperature Jacobian: the surface term alone, attenuated by the chunks below
-    const T jsfc = flux_up_jac ? emis * sfc_src_jac[ic + size_t(g) * ncol] : T(0);
+    const T jsfc = a.flux_up_jac ? emis * a.sfc_src_jac[ic + size_t(g) * ncol] : T(0);
     T rjac = jsfc;
-    if (flux_up_jac)
+    if (a.flux_up_jac)
         for (int c = nw - 1; c > w; --c) rjac *= sm_a[c * 32 + lane];
-    // re-sweeps: level j0 + i is the top of layer j0 + i
-    T* const dn = flux_dn + ic + size_t(g) * ncv;
-    T* const up = flux_up + ic + size_t(g) * ncv;
-    const ptrdiff_t step = top_at_1 ? ptrdiff_t(ncol) : -ptrdiff_t(ncol);
-    const ptrdiff_t o0 = top_at_1 ? ptrdiff_t(j0) * ncol : ptrdiff_t(nlay - j0) * ncol;   // level j0
+    T* const dn = a.flux_dn + ic + size_t(g) * ncv;
+    T* const up = a.flux_up + ic + size_t(g) * ncv;
+    const ptrdiff_t step = a.top_at_1 ? ptrdiff_t(ncol) : -ptrdiff_t(ncol);
+    const ptrdiff_t o0 = a.top_at_1 ? ptrdiff_t(j0) * ncol : ptrdiff_t(nlay - j0) * ncol;   // level j0
     if (w == 0) dn[o0] = two_pi_w * radn;
 #pragma unroll
     for (int i = 0; i < CL; ++i) {
@@ -282,14 +276,153 @@ __global__ void __launch_bounds__(MAXT) lw_solver_chunked(int ncol, int nlay, in
         rup = tr[i] * rup + sup[i];
         if (j0 + i < nlay) up[o0 + i * step] = two_pi_w * rup;
     }
-    if (flux_up_jac) {
-        T* const uj = flux_up_jac + ic + size_t(g) * ncv;
+    if (a.flux_up_jac) {
+        T* const uj = a.flux_up_jac + ic + size_t(g) * ncv;
         if (j0 <= nlay - 1 && nlay - 1 < j0 + CL) uj[o0 + (nlay - j0) * step] = two_pi_w * jsfc;
 #pragma unroll
         for (int i = CL - 1; i >= 0; --i) {
             rjac *= tr[i];
             if (j0 + i < nlay) uj[o0 + i * step] = two_pi_w * rjac;
         }
+    }
+}
+
+template <typename T, int CL, int MAXT>
+__global__ void __launch_bounds__(MAXT) lw_solver_chunked(const LwChunkArgs<T> a, const T* __restrict__ tau,
+                                                          const T* __restrict__ lay_src, const T* __restrict__ lev_inc,
+                                                          const T* __restrict__ lev_dec)
+{
+    __shared__ T sm_a[16 * 32], sm_bd[16 * 32], sm_bu[16 * 32];   // chunk maps [chunk][lane]
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int ncol = a.ncol, nlay = a.nlay;
+    const int icol = blockIdx.x * 32 + lane;
+    const bool cv = icol < ncol;
+    const int ic = cv ? icol : 0;
+    const int g = blockIdx.y;
+    const size_t ncl = size_t(ncol) * nlay;
+    const T* lev_dn = a.top_at_1 ? lev_inc : lev_dec;
+    const T* lev_up = a.top_at_1 ? lev_dec : lev_inc;
+    const int j0 = w * CL;
+
+    // every input of the chunk is read before any is used (the layer terms branch, and loads
+    // are not moved above a branch: read in the loop, one layer's rows would be in flight)
+    T tr[CL], sdn[CL], sup[CL], lay[CL];
+#pragma unroll
+    for (int i = 0; i < CL; ++i) {
+        const int j = j0 + i;
+        tr[i] = T(0); lay[i] = T(0); sdn[i] = T(0); sup[i] = T(0);
+        if (cv && j < nlay) {
+            const size_t x = ic + size_t(g) * ncl + size_t(a.top_at_1 ? j : nlay - 1 - j) * ncol;
+            tr[i] = tau[x];
+            lay[i] = lay_src[x];
+            sdn[i] = lev_dn[x];
+            sup[i] = lev_up[x];
+        }
+    }
+    lw_chunk_maps<T, CL>(tr, lay, sdn, sup, sm_a, sm_bd, sm_bu, w, lane);
+    __syncthreads();
+    if (!cv) return;
+    lw_chunk_levels<T, CL>(a, tr, sdn, sup, sm_a, sm_bd, sm_bu, w, nw, lane, ic, g);
+}
+
+// TMA-staged FP32 variant (nlay <= kLwTmaMaxLay).  A tile is the (32 columns x nlay layers)
+// block of the four layer inputs at one g-point; tiles are numbered g-point by g-point, column
+// tile fastest, and a persistent block takes every gridDim.x-th tile.  One shared-memory stage
+// per block, several blocks per SM: the block copies its layers of tile k from the stage into
+// registers, frees the stage, and thread 0 has the TMA unit copy tile k + 1 into it while the
+// block computes tile k (as lw_solver_chunked), so HBM reads continue through the compute and
+// store phases (the one-tile-per-block kernel above has its loads in flight only between its
+// start and its first use).  Lane = column: the stage reads are conflict-free rows.  Three
+// barriers per tile: after thread 0's wait (hands out its outcome), after the stage reads
+// (frees the stage), after the maps (publishes them).
+// Shared memory: [array 4][layer nlay][32] floats, maps [3][nw][32], one mbarrier.
+constexpr int kLwTmaMaxLay = 192;
+
+__device__ unsigned int g_tma_wait_timeouts;   // tiles whose copy did not complete in time
+
+inline size_t lw_tma_smem_bytes(int nlay, int nw)
+{
+    return 128 /* alignment slack */ + size_t(4) * 32 * nlay * sizeof(float) + size_t(3) * nw * 32 * sizeof(float) +
+           sizeof(uint64_t);
+}
+
+template <int CL>
+__global__ void __launch_bounds__(512, CL == 8 ? 2 : 1) lw_solver_tma(const __grid_constant__ CUtensorMap m_tau,
+                                                     const __grid_constant__ CUtensorMap m_lay,
+                                                     const __grid_constant__ CUtensorMap m_dn,
+                                                     const __grid_constant__ CUtensorMap m_up,
+                                                     const LwChunkArgs<float> a, int ngpt)
+{
+    extern __shared__ unsigned char smem_dyn[];
+    __shared__ int s_ok;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int ncol = a.ncol, nlay = a.nlay;
+    const int tile_floats = 32 * nlay;
+    float* const stage = reinterpret_cast<float*>(
+        (reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));   // 128-byte aligned tiles
+    float* const sm_a = stage + 4 * tile_floats;
+    float* const sm_bd = sm_a + nw * 32;
+    float* const sm_bu = sm_bd + nw * 32;
+    uint64_t* const bar = reinterpret_cast<uint64_t*>(sm_bu + nw * 32);   // 8-byte aligned: nw * 32 floats
+    const int nct = (ncol + 31) >> 5;
+    const long long ntiles = (long long)nct * ngpt;
+    const long long t0 = blockIdx.x, dt = gridDim.x;
+    const unsigned tx_bytes = 4u * unsigned(tile_floats) * 4u;
+
+    auto issue = [&](long long t) {
+        const int g = int(t / nct), x = int(t % nct) * 32;
+        tma::mbar_arrive_expect_tx(bar, tx_bytes);
+        tma::load_3d(stage, &m_tau, x, 0, g, bar);
+        tma::load_3d(stage + tile_floats, &m_lay, x, 0, g, bar);
+        tma::load_3d(stage + 2 * tile_floats, &m_dn, x, 0, g, bar);
+        tma::load_3d(stage + 3 * tile_floats, &m_up, x, 0, g, bar);
+    };
+    if (threadIdx.x == 0) {
+        tma::prefetch_map(&m_tau);
+        tma::prefetch_map(&m_lay);
+        tma::prefetch_map(&m_dn);
+        tma::prefetch_map(&m_up);
+        tma::mbar_init(bar, 1);
+        tma::fence_mbar_init();
+        if (t0 < ntiles) issue(t0);
+    }
+    int k = 0;
+    for (long long t = t0; t < ntiles; t += dt, ++k) {
+        if (threadIdx.x == 0) s_ok = tma::mbar_wait(bar, k & 1);
+        __syncthreads();
+        if (!s_ok) {
+            // the copy of tile k did not complete: count it, let it land (bounded) before the
+            // block's shared memory is released, and stop
+            if (threadIdx.x == 0) {
+                atomicAdd(&g_tma_wait_timeouts, 1u);
+                tma::mbar_wait(bar, k & 1);
+            }
+            return;
+        }
+        const int j0 = w * CL;
+        float tr[CL], sdn[CL], sup[CL], lay[CL];
+#pragma unroll
+        for (int i = 0; i < CL; ++i) {
+            const int j = j0 + i;
+            tr[i] = 0.f; lay[i] = 0.f; sdn[i] = 0.f; sup[i] = 0.f;
+            if (j < nlay) {
+                const int x = (a.top_at_1 ? j : nlay - 1 - j) * 32 + lane;
+                tr[i] = stage[x];
+                lay[i] = stage[tile_floats + x];
+                sdn[i] = stage[2 * tile_floats + x];
+                sup[i] = stage[3 * tile_floats + x];
+            }
+        }
+        __syncthreads();   // every read of the stage done
+        if (threadIdx.x == 0 && t + dt < ntiles) {
+            tma::fence_proxy_async_smem();
+            issue(t + dt);
+        }
+        const int g = int(t / nct);
+        const int icol = int(t % nct) * 32 + lane;
+        lw_chunk_maps<float, CL>(tr, lay, sdn, sup, sm_a, sm_bd, sm_bu, w, lane);
+        __syncthreads();   // maps visible
+        if (icol < ncol) lw_chunk_levels<float, CL>(a, tr, sdn, sup, sm_a, sm_bd, sm_bu, w, nw, lane, icol, g);
     }
 }
 
@@ -318,35 +451,25 @@ __device__ __forceinline__ T adding_den(T R, T a) { return T(1) / (T(1) - R * a)
 template <>
 __device__ __forceinline__ float adding_den<float>(float R, float a) { return __fdividef(1.f, fmaf(-R, a, 1.f)); }
 
-template <typename T, int CL, int MAXT, int MINB = 1>
-__global__ void __launch_bounds__(MAXT, MINB) sw_solver_chunked(int ncol, int nlay, int nband, int top_at_1,
-                                                         const int* __restrict__ gpt2band, const T* __restrict__ tau,
-                                                         const T* __restrict__ ssa, const T* __restrict__ gasy,
-                                                         const T* __restrict__ mu0, const T* __restrict__ inc_dir,
-                                                         const T* __restrict__ alb_dir, const T* __restrict__ alb_dif,
-                                                         const T* __restrict__ inc_dif, T* __restrict__ flux_up,
-                                                         T* __restrict__ flux_dn, T* __restrict__ flux_dir)
-{
-    __shared__ T sm_p[16 * 32];                                      // direct-beam product per chunk
-    __shared__ T sm_ru[16 * 32], sm_rd[16 * 32], sm_t[16 * 32], sm_u[16 * 32], sm_d[16 * 32];   // composites
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int icol = blockIdx.x * 32 + lane;
-    const bool cv = icol < ncol;
-    const int ic = cv ? icol : 0;
-    const int g = blockIdx.y;
-    const size_t ncl = size_t(ncol) * nlay, ncv = size_t(ncol) * (nlay + 1);
-    const size_t base = ic + size_t(g) * ncl;
-    const int band = gpt2band[g];
-    const T m0 = mu0[ic], m0_inv = T(1) / m0;
-    const T ad = alb_dir[band + size_t(ic) * nband], af = alb_dif[band + size_t(ic) * nband];
-    const T dir_toa = inc_dir[ic + size_t(g) * ncol] * m0;
-    const T fd_toa = inc_dif ? inc_dif[ic + size_t(g) * ncol] : T(0);
-    const int j0 = w * CL;
+// Arguments of the chunked shortwave solvers other than the layer optical properties.
+template <typename T>
+struct SwChunkArgs {
+    int ncol, nlay, nband, top_at_1;
+    const int* gpt2band;
+    const T *mu0, *inc_dir, *alb_dir, *alb_dif, *inc_dif;
+    T *flux_up, *flux_dn, *flux_dir;
+};
 
-    // 1. layer coefficients; direct beam relative to the chunk top; adding composite of the chunk
+// Per-thread state of one chunk: its layers' diffuse reflectance and transmittance, direct
+// sources relative to the chunk top, direct-beam product above each layer, and the adding
+// composite of the chunk (R_up, R_dn, T, U, D) with its direct-beam product P.
+template <typename T, int CL>
+struct SwChunk {
     T vR[CL], vT[CL], vSu[CL], vSd[CL], vP[CL];
     T P = T(1), cRu = T(0), cRd = T(0), cT = T(1), cU = T(0), cD = T(0);
-    auto add_layer = [&](int i, T R, T Tt, T Rdir, T Tdir, T Tn) {
+
+    __device__ __forceinline__ void add_layer(int i, T R, T Tt, T Rdir, T Tdir, T Tn)
+    {
         vR[i] = R;
         vT[i] = Tt;
         vP[i] = P;
@@ -363,43 +486,52 @@ __global__ void __launch_bounds__(MAXT, MINB) sw_solver_chunked(int ncol, int nl
         cU = nU;
         cD = nD;
         P *= Tn;
-    };
-#pragma unroll
-    for (int i = 0; i < CL; ++i) {
-        const int j = j0 + i;
-        T R = T(0), Tt = T(1), Rdir = T(0), Tdir = T(0), Tn = T(1);
-        if (cv && j < nlay) {
-            const size_t x = base + size_t(top_at_1 ? j : nlay - 1 - j) * ncol;
-            sw_layer_coeffs<T>(tau[x], ssa[x], gasy[x], m0, m0_inv, R, Tt, Rdir, Tdir, Tn);
-        }
-        add_layer(i, R, Tt, Rdir, Tdir, Tn);
     }
-    sm_p[w * 32 + lane] = P;
+};
+
+// Shared-memory arrays of the chunk exchange, [chunk][lane] each.
+template <typename T>
+struct SwChunkSmem {
+    T *p, *ru, *rd, *t, *u, *d;
+};
+
+// After every layer of the chunk is added (column ic, g-point g): the direct beam and the
+// adding composites exchanged between the chunks (two barriers), albedo and source at the
+// chunk bottom, and the level outputs.  Threads of columns past ncol take part in the
+// barriers and write nothing.
+template <typename T, int CL>
+__device__ __forceinline__ void sw_chunk_finish(const SwChunkArgs<T>& a, SwChunk<T, CL>& c, const SwChunkSmem<T>& sm,
+                                                int w, int nw, int lane, bool cv, int ic, int g, T dir_toa, T fd_toa,
+                                                T ad, T af)
+{
+    const int ncol = a.ncol, nlay = a.nlay;
+    const int j0 = w * CL;
+    sm.p[w * 32 + lane] = c.P;
     __syncthreads();
     // 2. direct beam at the chunk top and at the surface
     T dtop = dir_toa;
-    for (int c = 0; c < w; ++c) dtop *= sm_p[c * 32 + lane];
+    for (int q = 0; q < w; ++q) dtop *= sm.p[q * 32 + lane];
     T dsfc = dtop;
-    for (int c = w; c < nw; ++c) dsfc *= sm_p[c * 32 + lane];
-    sm_ru[w * 32 + lane] = cRu;
-    sm_rd[w * 32 + lane] = cRd;
-    sm_t[w * 32 + lane] = cT;
-    sm_u[w * 32 + lane] = cU * dtop;
-    sm_d[w * 32 + lane] = cD * dtop;
+    for (int q = w; q < nw; ++q) dsfc *= sm.p[q * 32 + lane];
+    sm.ru[w * 32 + lane] = c.cRu;
+    sm.rd[w * 32 + lane] = c.cRd;
+    sm.t[w * 32 + lane] = c.cT;
+    sm.u[w * 32 + lane] = c.cU * dtop;
+    sm.d[w * 32 + lane] = c.cD * dtop;
     __syncthreads();
     // 3. albedo and source at the chunk bottom (from the surface up), and the diffuse flux at
     //    the chunk top as fa * (TOA diffuse) + fb
     T alb = af, src = dsfc * ad, alb_in = af, src_in = dsfc * ad, fa = T(1), fb = T(0);
-    for (int c = nw - 1; c >= 0; --c) {
-        if (c == w) {
+    for (int q = nw - 1; q >= 0; --q) {
+        if (q == w) {
             alb_in = alb;
             src_in = src;
             if (w == 0) break;
         }
-        const T mRu = sm_ru[c * 32 + lane], mRd = sm_rd[c * 32 + lane], mT = sm_t[c * 32 + lane];
-        const T mU = sm_u[c * 32 + lane], mD = sm_d[c * 32 + lane];
+        const T mRu = sm.ru[q * 32 + lane], mRd = sm.rd[q * 32 + lane], mT = sm.t[q * 32 + lane];
+        const T mU = sm.u[q * 32 + lane], mD = sm.d[q * 32 + lane];
         const T den = adding_den(mRd, alb);
-        if (c < w) {
+        if (q < w) {
             const T F = mT * den, G = (mRd * src + mD) * den;
             fb = fa * G + fb;
             fa *= F;
@@ -411,41 +543,41 @@ __global__ void __launch_bounds__(MAXT, MINB) sw_solver_chunked(int ncol, int nl
     // 4. albedo and upward source at the top of every layer (bottom-up)
     T vA[CL];
     {
-        T a = alb_in, s = src_in;
+        T al = alb_in, so = src_in;
 #pragma unroll
         for (int i = CL - 1; i >= 0; --i) {
-            const T su = vSu[i] * dtop, sd = vSd[i] * dtop;
-            const T den = adding_den(vR[i], a);
-            const T na = vR[i] + vT[i] * vT[i] * a * den;
-            const T ns = su + vT[i] * (a * sd + s) * den;
-            vSd[i] = sd;
-            vSu[i] = ns;
+            const T su = c.vSu[i] * dtop, sd = c.vSd[i] * dtop;
+            const T den = adding_den(c.vR[i], al);
+            const T na = c.vR[i] + c.vT[i] * c.vT[i] * al * den;
+            const T ns = su + c.vT[i] * (al * sd + so) * den;
+            c.vSd[i] = sd;
+            c.vSu[i] = ns;
             vA[i] = na;
-            a = na;
-            s = ns;
+            al = na;
+            so = ns;
         }
     }
     // 5. diffuse fluxes (top-down) and the level outputs
     if (!cv) return;
-    const size_t off = ic + size_t(g) * ncv;
-    const ptrdiff_t step = top_at_1 ? ptrdiff_t(ncol) : -ptrdiff_t(ncol);
-    const ptrdiff_t o0 = top_at_1 ? ptrdiff_t(j0) * ncol : ptrdiff_t(nlay - j0) * ncol;   // level j0
-    T* const up = flux_up + off;
-    T* const dn = flux_dn + off;
-    T* const dr = flux_dir + off;
+    const size_t off = ic + size_t(g) * ncol * (nlay + 1);
+    const ptrdiff_t step = a.top_at_1 ? ptrdiff_t(ncol) : -ptrdiff_t(ncol);
+    const ptrdiff_t o0 = a.top_at_1 ? ptrdiff_t(j0) * ncol : ptrdiff_t(nlay - j0) * ncol;   // level j0
+    T* const up = a.flux_up + off;
+    T* const dn = a.flux_dn + off;
+    T* const dr = a.flux_dir + off;
     T fd = fa * fd_toa + fb;
 #pragma unroll
     for (int i = 0; i < CL; ++i) {
         const T a_n = (i + 1 < CL) ? vA[i + 1] : alb_in;
-        const T s_n = (i + 1 < CL) ? vSu[i + 1] : src_in;
+        const T s_n = (i + 1 < CL) ? c.vSu[i + 1] : src_in;
         if (j0 + i < nlay) {
-            const T dir = dtop * vP[i];
-            up[o0 + i * step] = fd * vA[i] + vSu[i];
+            const T dir = dtop * c.vP[i];
+            up[o0 + i * step] = fd * vA[i] + c.vSu[i];
             dn[o0 + i * step] = fd + dir;
             dr[o0 + i * step] = dir;
         }
-        const T den = adding_den(vR[i], a_n);
-        fd = (vT[i] * fd + vR[i] * s_n + vSd[i]) * den;
+        const T den = adding_den(c.vR[i], a_n);
+        fd = (c.vT[i] * fd + c.vR[i] * s_n + c.vSd[i]) * den;
     }
     if (j0 <= nlay - 1 && nlay - 1 < j0 + CL) {
         // fd is now at the chunk bottom (padding layers are the identity): the surface level
@@ -454,6 +586,42 @@ __global__ void __launch_bounds__(MAXT, MINB) sw_solver_chunked(int ncol, int nl
         dn[o] = fd + dsfc;
         dr[o] = dsfc;
     }
+}
+
+template <typename T, int CL, int MAXT, int MINB = 1>
+__global__ void __launch_bounds__(MAXT, MINB) sw_solver_chunked(const SwChunkArgs<T> a, const T* __restrict__ tau,
+                                                                const T* __restrict__ ssa, const T* __restrict__ gasy)
+{
+    __shared__ T sm_p[16 * 32];                                      // direct-beam product per chunk
+    __shared__ T sm_ru[16 * 32], sm_rd[16 * 32], sm_t[16 * 32], sm_u[16 * 32], sm_d[16 * 32];   // composites
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int ncol = a.ncol, nlay = a.nlay;
+    const int icol = blockIdx.x * 32 + lane;
+    const bool cv = icol < ncol;
+    const int ic = cv ? icol : 0;
+    const int g = blockIdx.y;
+    const size_t base = ic + size_t(g) * ncol * nlay;
+    const int band = a.gpt2band[g];
+    const T m0 = a.mu0[ic], m0_inv = T(1) / m0;
+    const T ad = a.alb_dir[band + size_t(ic) * a.nband], af = a.alb_dif[band + size_t(ic) * a.nband];
+    const T dir_toa = a.inc_dir[ic + size_t(g) * ncol] * m0;
+    const T fd_toa = a.inc_dif ? a.inc_dif[ic + size_t(g) * ncol] : T(0);
+    const int j0 = w * CL;
+
+    // 1. layer coefficients; direct beam relative to the chunk top; adding composite of the chunk
+    SwChunk<T, CL> c;
+#pragma unroll
+    for (int i = 0; i < CL; ++i) {
+        const int j = j0 + i;
+        T R = T(0), Tt = T(1), Rdir = T(0), Tdir = T(0), Tn = T(1);
+        if (cv && j < nlay) {
+            const size_t x = base + size_t(a.top_at_1 ? j : nlay - 1 - j) * ncol;
+            sw_layer_coeffs<T>(tau[x], ssa[x], gasy[x], m0, m0_inv, R, Tt, Rdir, Tdir, Tn);
+        }
+        c.add_layer(i, R, Tt, Rdir, Tdir, Tn);
+    }
+    sw_chunk_finish<T, CL>(a, c, SwChunkSmem<T>{sm_p, sm_ru, sm_rd, sm_t, sm_u, sm_d}, w, nw, lane, cv, ic, g,
+                           dir_toa, fd_toa, ad, af);
 }
 
 template <typename T>
@@ -467,6 +635,47 @@ int lw_smem_block(int nlay, size_t* smem)
     return 0;
 }
 
+// The TMA variant needs 16-byte row strides (ncol a multiple of 4) and 16-byte aligned arrays.
+inline bool lw_tma_ok(int ncol, int nlay, const float* tau, const float* lay, const float* dn, const float* up)
+{
+    auto al = [](const float* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+    return nlay <= kLwTmaMaxLay && ncol % 4 == 0 && al(tau) && al(lay) && al(dn) && al(up);
+}
+
+int lw_solver_tma_launch(const LwChunkArgs<float>& a, int ngpt, const float* tau, const float* lay,
+                         const float* lev_dn, const float* lev_up, void* stream)
+{
+    CUtensorMap m[4];
+    const float* src[4] = {tau, lay, lev_dn, lev_up};
+    for (int q = 0; q < 4; ++q) {
+        const int st = encode_map_3d_f32(&m[q], src[q], a.ncol, a.nlay, ngpt, 32, a.nlay);
+        if (st) return st;
+    }
+    const int cl = a.nlay <= 8 * 16 ? 8 : 16;
+    const int nw = ceil_div(a.nlay, cl);
+    const size_t smem = lw_tma_smem_bytes(a.nlay, nw);
+    const auto kernel = cl == 8 ? lw_solver_tma<8> : lw_solver_tma<16>;
+    static PerDeviceOnce attr;
+    const int ast = attr.run([] {
+        // the largest request: 192 layers in 16-layer chunks (the 8-layer kernel stops at 128)
+        const int most = int(lw_tma_smem_bytes(kLwTmaMaxLay, kLwTmaMaxLay / 16));
+        cudaError_t e = cudaFuncSetAttribute(lw_solver_tma<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(lw_solver_tma<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+        return e;
+    }, "rte_lw TMA attribute");
+    if (ast) return ast;
+    int dev = 0, nsm = 0, per_sm = 0;
+    RB_CUDA(cudaGetDevice(&dev), "rte_lw");
+    RB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "rte_lw");
+    RB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 32 * nw, smem), "rte_lw");
+    const long long ntiles = (long long)ceil_div(a.ncol, 32) * ngpt;
+    const int grid = int(std::min<long long>(ntiles, (long long)nsm * std::max(per_sm, 1)));
+    kernel<<<grid, 32 * nw, smem, as_stream(stream)>>>(m[0], m[1], m[2], m[3], a, ngpt);
+    RB_LAUNCH("lw_solver_tma");
+    return RRTMGP_B200_OK;
+}
+
 template <typename T>
 int rte_lw(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const T* tau, const T* lay_src,
            const T* lev_inc, const T* lev_dec, const T* sfc_src, const T* sfc_emis, const T* inc_flux,
@@ -478,17 +687,23 @@ int rte_lw(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const T* tau, 
     RB_CHECK_ARG(tau && lay_src && lev_inc && lev_dec && sfc_src && sfc_emis && flux_up && flux_dn,
                  "rte_lw: null array");
     if (nmus == 1 && nlay <= 16 * 16) {
+        const LwChunkArgs<T> a{ncol, nlay, b->nband, top_at_1, b->d_gpt2band, sfc_src, sfc_emis, inc_flux,
+                               sfc_src_jac, flux_up, flux_dn, flux_up_jac};
+        const T* lev_dn = top_at_1 ? lev_inc : lev_dec;
+        const T* lev_up = top_at_1 ? lev_dec : lev_inc;
+        if constexpr (sizeof(T) == 4) {
+            if (lw_tma_ok(ncol, nlay, tau, lay_src, lev_dn, lev_up))
+                return lw_solver_tma_launch(a, b->ngpt, tau, lay_src, lev_dn, lev_up, stream);
+        }
         const dim3 grid(ceil_div(ncol, 32), b->ngpt);
         // FP32 up to 128 layers: 8-layer chunks (more warps with fewer rows in flight each
         // measured faster than 16 at 8192 x 128); FP64 and deeper columns: 16-layer chunks
         if (sizeof(T) == 4 && nlay <= 8 * 16)
             lw_solver_chunked<T, 8, 512><<<grid, 32 * ceil_div(nlay, 8), 0, as_stream(stream)>>>(
-                ncol, nlay, b->nband, top_at_1, b->d_gpt2band, tau, lay_src, lev_inc, lev_dec, sfc_src, sfc_emis,
-                inc_flux, flux_up, flux_dn, sfc_src_jac, flux_up_jac);
+                a, tau, lay_src, lev_inc, lev_dec);
         else
             lw_solver_chunked<T, 16, 512><<<grid, 32 * ceil_div(nlay, 16), 0, as_stream(stream)>>>(
-                ncol, nlay, b->nband, top_at_1, b->d_gpt2band, tau, lay_src, lev_inc, lev_dec, sfc_src, sfc_emis,
-                inc_flux, flux_up, flux_dn, sfc_src_jac, flux_up_jac);
+                a, tau, lay_src, lev_inc, lev_dec);
         RB_LAUNCH("lw_solver_chunked");
         return RRTMGP_B200_OK;
     }
@@ -535,19 +750,15 @@ int rte_sw(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const T* tau, 
     // Chunked solver up to 256 layers (FP64: 128; its deeper columns would spill registers).
     constexpr bool fp64 = sizeof(T) == 8;
     if (nlay <= sw_chunked_max_nlay(fp64)) {
+        const SwChunkArgs<T> a{ncol, nlay, b->nband, top_at_1, b->d_gpt2band, mu0, inc_dir, alb_dir, alb_dif,
+                               inc_dif, flux_up, flux_dn, flux_dir};
         const dim3 grid(ceil_div(ncol, 32), b->ngpt);
         if constexpr (fp64) {
-            sw_solver_chunked<T, 16, 256><<<grid, 32 * ceil_div(nlay, 16), 0, as_stream(stream)>>>(
-                ncol, nlay, b->nband, top_at_1, b->d_gpt2band, tau, ssa, g, mu0, inc_dir, alb_dir, alb_dif, inc_dif,
-                flux_up, flux_dn, flux_dir);
+            sw_solver_chunked<T, 16, 256><<<grid, 32 * ceil_div(nlay, 16), 0, as_stream(stream)>>>(a, tau, ssa, g);
         } else if (nlay <= 128) {
-            sw_solver_chunked<T, 8, 512, 2><<<grid, 32 * ceil_div(nlay, 8), 0, as_stream(stream)>>>(
-                ncol, nlay, b->nband, top_at_1, b->d_gpt2band, tau, ssa, g, mu0, inc_dir, alb_dir, alb_dif, inc_dif,
-                flux_up, flux_dn, flux_dir);
+            sw_solver_chunked<T, 8, 512, 2><<<grid, 32 * ceil_div(nlay, 8), 0, as_stream(stream)>>>(a, tau, ssa, g);
         } else {
-            sw_solver_chunked<T, 16, 512><<<grid, 32 * ceil_div(nlay, 16), 0, as_stream(stream)>>>(
-                ncol, nlay, b->nband, top_at_1, b->d_gpt2band, tau, ssa, g, mu0, inc_dir, alb_dir, alb_dif, inc_dif,
-                flux_up, flux_dn, flux_dir);
+            sw_solver_chunked<T, 16, 512><<<grid, 32 * ceil_div(nlay, 16), 0, as_stream(stream)>>>(a, tau, ssa, g);
         }
         RB_LAUNCH("sw_solver_chunked");
         return RRTMGP_B200_OK;
@@ -672,5 +883,12 @@ int rrtmgp_b200_rte_sw_static_scratch_f32(rrtmgp_b200_bands b, int ncol, int nla
         const float* ssa, const float* g, const float* mu0, const float* inc_flux_dir, const float* sfc_alb_dir,
         const float* sfc_alb_dif, const float* inc_flux_dif, float* up, float* dn, float* dir, void* s)
 { return rte_sw_static(b, ncol, nlay, top_at_1, tau, ssa, g, mu0, inc_flux_dir, sfc_alb_dir, sfc_alb_dif, inc_flux_dif, up, dn, dir, s); }
+
+int rrtmgp_b200_device_wait_timeouts(unsigned int* count)
+{
+    RB_CHECK_ARG(count, "device_wait_timeouts: null count");
+    RB_CUDA(cudaMemcpyFromSymbol(count, g_tma_wait_timeouts, sizeof(unsigned int)), "device_wait_timeouts");
+    return RRTMGP_B200_OK;
+}
 
 }  // extern "C"

@@ -25,10 +25,11 @@ template <typename T> __device__ __forceinline__ T pi_value() { return T(3.14159
 // Transmissivity and linear-in-tau level sources of one layer for one angle
 // (lw_solver_noscat_step_1_kernel, rte_solver_kernels.cu:116-125; Clough et al. 1992).
 // FP64 uses the reference expressions.  In FP32, (1 - T)/tau - T cancels to a relative error
-// of eps/tau for thin layers, so the FP32 path takes 1 - T = -expm1(-tau) and, below
-// tau = 0.1, the series of fact = sum_n (-1)^(n+1) n/(n+1)! tau^n to n = 6
-// (truncation < 2e-11 relative), which equals the reference's 2-term series where that
-// one is used.
+// of eps/tau for thin layers, so the FP32 path forms 1 - T itself: below tau = 0.1 the Taylor
+// series of 1 - e^-x and of fact = sum_n (-1)^(n+1) n/(n+1)! tau^n, both to n = 6 (truncation
+// < 2e-11 relative; the fact series equals the reference's 2-term series where that one is
+// used); above, 1 - e^-x from the hardware exponential (__expf), whose error, scaled by
+// e^-x / (1 - e^-x) <= 10, stays near 2e-6 relative.
 template <typename T>
 __device__ __forceinline__ void lw_layer(T tau, T D, T lay, T lev_dn, T lev_up, T& trans, T& src_dn, T& src_up);
 
@@ -49,16 +50,15 @@ __device__ __forceinline__ void lw_layer<float>(float tau, float D, float lay, f
                                                float& trans, float& src_dn, float& src_up)
 {
     const float tl = tau * D;
-    const float em1 = expm1f(-tl);
-    const float omt = -em1;  // 1 - trans
-    trans = 1.f + em1;
-    float fact;
+    float omt, fact;   // 1 - T, (1 - T)/tl - T
     if (tl < 0.1f) {
-        // tau/2 - tau^2/3 + tau^3/8 - tau^4/30 + tau^5/144 - tau^6/840
+        omt = tl * (1.f - tl * (0.5f - tl * (1.f / 6.f - tl * (1.f / 24.f - tl * (1.f / 120.f - tl * (1.f / 720.f))))));
         fact = tl * (0.5f + tl * (-1.f / 3.f + tl * (0.125f + tl * (-1.f / 30.f + tl * (1.f / 144.f - tl * (1.f / 840.f))))));
     } else {
-        fact = omt / tl - trans;
+        omt = 1.f - __expf(-tl);
+        fact = __fdividef(omt, tl) - (1.f - omt);
     }
+    trans = 1.f - omt;
     src_dn = omt * lev_dn + 2.f * fact * (lay - lev_dn);
     src_up = omt * lev_up + 2.f * fact * (lay - lev_up);
 }

@@ -223,6 +223,7 @@ _SIGS = {
     "rrtmgp_b200_cloud_create": (_I, [C.POINTER(CloudTables), C.POINTER(_P)]),
     "rrtmgp_b200_cloud_destroy": (None, [_P]),
     "rrtmgp_b200_rte_sw_workspace_bytes": (_SZ, [_I, _I, _I, _I]),
+    "rrtmgp_b200_device_wait_timeouts": (_I, [C.POINTER(C.c_uint)]),
     "rrtmgp_b200_rte_sw_static_scratch_f32": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "rrtmgp_b200_forward_lw_f32": (_I, [_P, _P, _I, _I, _P, _P, _P, _P, _P, _P, C.POINTER(GasConc), _I,
                                         _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]),

@@ -312,6 +312,54 @@ def test_rte_lw_surface_temperature_jacobian(api, oracle_mod, tables, gpu, prec,
     assert np.max(jac) > 0
 
 
+def _wait_timeouts():
+    import ctypes
+    from rrtmgp_b200 import _abi
+    n = ctypes.c_uint(0)
+    assert _abi.load().rrtmgp_b200_device_wait_timeouts(ctypes.byref(n)) == 0
+    return n.value
+
+
+@pytest.mark.parametrize("top_at_1", [True, False])
+@pytest.mark.parametrize("ncol,nlay", [(36, 23), (68, 128), (4, 129), (100, 192), (2048, 40)])
+@pytest.mark.parametrize("with_inc", [False, True])
+def test_rte_lw_tma_tiles(api, oracle_mod, tables, gpu, top_at_1, ncol, nlay, with_inc):
+    """FP32, one angle, ncol a multiple of 4 and nlay <= 192: the solver copies its layer inputs
+    with TMA tiles of 32 columns x nlay layers (column tiles with idle lanes, 8- and 16-layer
+    chunks, several tiles per persistent block so both copy stages cycle).  Fluxes and the
+    surface-temperature Jacobian against the oracle, and bit-identical to the kernel that reads
+    global memory directly, which runs on ncol + 1 columns (not a multiple of 4) of the same
+    atmosphere; no copy timed out."""
+    import torch
+    dt = torch.float32
+    before = _wait_timeouts()
+    n1 = ncol + 1
+    atm = S.make_atmosphere(n1, nlay, seed=40 + nlay, clouds=False, top_at_1=top_at_1)
+    go = oracle_mod.GasOptics(tables["lw"], S.ATM_GASES).gas_optics_lw(
+        atm["play"], atm["plev"], atm["tlay"], atm["tsfc"], atm["gases"], atm["tlev"])
+    rng = np.random.default_rng(nlay)
+    emis = rng.uniform(0.8, 1.0, (n1, 16))
+    inc = rng.uniform(0, 2, (256, n1)) if with_inc else None
+    kd = api.Gas_optics_rrtmgp(tables["lw"], S.ATM_GASES)
+    keys = ("tau", "lay_src", "lev_src_inc", "lev_src_dec", "sfc_src", "sfc_src_jac")
+    full = {k: T(go[k], dt, gpu) for k in keys}
+    part = {k: T(go[k][..., :ncol], dt, gpu) for k in keys}
+    ref = api.Rte_lw.rte_lw(kd.bands, full["tau"], top_at_1, full, T(emis, dt, gpu),
+                            None if inc is None else T(inc, dt, gpu), 1, flux_up_jac=True)
+    got = api.Rte_lw.rte_lw(kd.bands, part["tau"], top_at_1, part, T(emis[:ncol], dt, gpu),
+                            None if inc is None else T(inc[:, :ncol], dt, gpu), 1, flux_up_jac=True)
+    torch.cuda.synchronize()
+    for name, g, r in zip(("flux_up", "flux_dn", "flux_up_jac"), got, ref):
+        assert torch.equal(g, r[..., :ncol]), f"{name}: TMA and direct kernels differ"
+    sub = {k: v[..., :ncol] for k, v in go.items()}
+    up, dn, jac = oracle_mod.rte_lw(tables["lw"]["bnd_limits_gpt"], sub["tau"], top_at_1, sub, emis[:ncol],
+                                    None if inc is None else inc[:, :ncol], 1, flux_up_jac=True)
+    cmp_flux("flux_up", N(got[0]), up, "f32")
+    cmp_flux("flux_dn", N(got[1]), dn, "f32")
+    cmp_flux("flux_up_jac", N(got[2]), jac, "f32")
+    assert _wait_timeouts() == before
+
+
 @pytest.mark.parametrize("prec", ["f32", "f64"])
 @pytest.mark.parametrize("top_at_1", [True, False])
 @pytest.mark.parametrize("with_dif", [False, True])

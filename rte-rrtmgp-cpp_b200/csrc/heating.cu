@@ -26,9 +26,24 @@ namespace {
 
 constexpr double kG0OverCp = 9.80665 / 1004.64;
 
-template <typename T> __device__ __forceinline__ T one_minus_exp_neg(T x);
-template <> __device__ __forceinline__ float one_minus_exp_neg<float>(float x) { return -expm1f(-x); }
-template <> __device__ __forceinline__ double one_minus_exp_neg<double>(double x) { return -expm1(-x); }
+// 1 - T and the layer sources: FP32 as the solvers (lw_layer_fast); FP64 the reference
+// expressions with 1 - T = -expm1(-tau D).
+template <typename T>
+__device__ __forceinline__ void lw_layer_terms(T tau, T D, T lay, T ldn, T lup, T& omt, T& sdn, T& sup);
+template <>
+__device__ __forceinline__ void lw_layer_terms<float>(float tau, float D, float lay, float ldn, float lup, float& omt,
+                                                      float& sdn, float& sup)
+{
+    lw_layer_fast(tau, D, lay, ldn, lup, omt, sdn, sup);
+}
+template <>
+__device__ __forceinline__ void lw_layer_terms<double>(double tau, double D, double lay, double ldn, double lup,
+                                                       double& omt, double& sdn, double& sup)
+{
+    double trans;
+    lw_layer(tau, D, lay, ldn, lup, trans, sdn, sup);
+    omt = -expm1(-tau * D);
+}
 
 template <typename T>
 __global__ void heating_rate_lw_layers_kernel(int ncol, int nlay, int ngpt, int top_at_1, const T* __restrict__ tau,
@@ -49,9 +64,8 @@ __global__ void heating_rate_lw_layers_kernel(int ncol, int nlay, int ngpt, int 
     double acc = 0.0;
     for (int g = 0; g < ngpt; ++g) {
         const size_t i = cl + size_t(g) * ncl;
-        T trans, sdn, sup;
-        lw_layer(tau[i], D, lay_src[i], lev_dn[i], lev_up[i], trans, sdn, sup);
-        const T omt = one_minus_exp_neg(tau[i] * D);
+        T omt, sdn, sup;
+        lw_layer_terms<T>(tau[i], D, lay_src[i], lev_dn[i], lev_up[i], omt, sdn, sup);
         const size_t ot = icol + size_t(lt) * ncol + size_t(g) * ncv, ob = icol + size_t(lb) * ncol + size_t(g) * ncv;
         acc += double(omt * (dn[ot] + up[ob]) - pi * (sdn + sup));
     }

@@ -54,28 +54,6 @@ struct LwGridIo {
     __device__ __forceinline__ const CloudArgs& cloud() const { return cld_; }
 };
 
-// Layer transmissivity complement and sources in FP32: series below tau = 0.1 (7 and 6 terms,
-// truncation < 2e-11 relative), exp/divide intrinsics above where no cancellation occurs.
-// Both forms are evaluated and one is selected, so the warp does not diverge.  Same physics
-// as lw_solver_noscat_step_1_kernel (rte_solver_kernels.cu:116-125).
-__device__ __forceinline__ void lw_layer_fast(float tau, float D, float lay, float ldn, float lup, float& omt,
-                                              float& sdn, float& sup)
-{
-    const float tl = tau * D;
-    const float s_omt = tl * (1.f + tl * (-0.5f + tl * (1.f / 6.f + tl * (-1.f / 24.f + tl * (1.f / 120.f +
-                        tl * (-1.f / 720.f + tl * (1.f / 5040.f)))))));
-    const float s_fact = tl * (0.5f + tl * (-1.f / 3.f + tl * (0.125f + tl * (-1.f / 30.f + tl * (1.f / 144.f -
-                         tl * (1.f / 840.f))))));
-    const float trans = __expf(-tl);
-    const float e_omt = 1.f - trans;
-    const float e_fact = __fdividef(e_omt, tl) - trans;
-    const bool thin = tl < 0.1f;
-    omt = thin ? s_omt : e_omt;
-    const float fact = thin ? s_fact : e_fact;
-    sdn = omt * ldn + 2.f * fact * (lay - ldn);
-    sup = omt * lup + 2.f * fact * (lay - lup);
-}
-
 __device__ __forceinline__ void build_lw_record(const KdistView<float>& k, Rec& R, const LayerState& s,
                                                 const float* cg, int nlay, int b, float tau_cld, bool bottom,
                                                 float tsfc)

@@ -114,6 +114,14 @@ class GasOptics:
         load().oracle_kdist_solar_source(self.h, _p(out))
         return out
 
+    def set_solar_variability(self, mg_index, sb_index):
+        """Gas_optics_rrtmgp::set_solar_variability (src/Gas_optics_rrtmgp.cpp:745-760)."""
+        lib = load()
+        lib.oracle_kdist_set_solar_variability.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        st = lib.oracle_kdist_set_solar_variability(self.h, float(mg_index), float(sb_index))
+        if st != 0:
+            raise RuntimeError(lib.oracle_last_error().decode())
+
     def gas_optics_lw(self, play, plev, tlay, tsfc, gases, tlev, col_dry=None):
         play, plev, tlay, tsfc, tlev = map(_f, (play, plev, tlay, tsfc, tlev))
         col_dry = None if col_dry is None else _f(col_dry)

@@ -312,6 +312,39 @@ def test_rte_lw_surface_temperature_jacobian(api, oracle_mod, tables, gpu, prec,
     assert np.max(jac) > 0
 
 
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_solar_variability_matches_oracle(api, oracle_mod, tables, gpu, prec):
+    """Gas_optics_rrtmgp_gpu::set_solar_variability (src_cuda/Gas_optics_rrtmgp.cu:1205-1217)
+    at indices away from the table defaults: the solar source, get_tsi (its sum), toa_src of
+    the gas optics and the fused shortwave forward against the oracle at the same indices,
+    and a return to the defaults."""
+    import torch
+    dt = dtypes()[prec]
+    atm = S.make_atmosphere(NCOL, NLAY, seed=71, clouds=True)
+    kd = api.Gas_optics_rrtmgp(tables["sw"], S.ATM_GASES)
+    ko = oracle_mod.GasOptics(tables["sw"], S.ATM_GASES)
+    g = gas_dict(atm, dt, gpu)
+    for mg, sb in ((0.13, 400.0), (0.2, 2500.0), (tables["sw"]["mg_default"], tables["sw"]["sb_default"])):
+        kd.set_solar_variability(mg, sb)
+        ko.set_solar_variability(mg, sb)
+        ref = ko.solar_source()
+        assert abs(kd.get_tsi() - ref.sum()) <= 1e-12 * ref.sum()
+        got = kd.gas_optics_sw(T(atm["play"], dt, gpu), T(atm["plev"], dt, gpu), T(atm["tlay"], dt, gpu), g)
+        want = ko.gas_optics_sw(atm["play"], atm["plev"], atm["tlay"], atm["gases"])
+        cmp("toa_src", N(got["toa_src"]), want["toa_src"], prec)
+    if prec == "f32":
+        from rrtmgp_b200.solver import Fused_solver, Radiation_solver, atm_to_device
+        base = Radiation_solver(tables["lw"], tables["sw"], tables["cloud_lw"], tables["cloud_sw"], S.ATM_GASES)
+        base.ksw.set_solar_variability(0.2, 2500.0)
+        ko.set_solar_variability(0.2, 2500.0)
+        sw = Fused_solver(base).solve_sw(atm_to_device(atm, torch.float32, gpu))
+        torch.cuda.synchronize()
+        rsw = oracle_mod.forward_sw(ko, oracle_mod.CloudOptics(tables["cloud_sw"]), atm)
+        for key in ("flux_up", "flux_dn", "flux_dn_dir"):
+            e = float(np.max(np.abs(N(sw[key]) - rsw[key])))
+            assert e < 5e-3, f"fused sw {key} at mg=0.2, sb=2500: {e:.3e} W/m2"
+
+
 def _wait_timeouts():
     import ctypes
     from rrtmgp_b200 import _abi

@@ -188,3 +188,20 @@ def test_forward_energy_budget(oracle_mod, tables):
     assert 150 < fl["flux_up"][0].mean() < 350
     np.testing.assert_allclose(fs["flux_dn"][0], atm["mu0"] * ksw.solar_source().sum(), rtol=1e-12)
     assert np.all(fs["flux_up"][0] < fs["flux_dn"][0])
+
+
+def test_solar_variability_formula(oracle_mod, tables):
+    """set_solar_variability (src/Gas_optics_rrtmgp.cpp:745-760): quiet + (mg - 0.1495954)
+    facular + (sb - 0.00066696) sunspot; the creation uses the table defaults, and the golden
+    toa_src fixtures of the reference pin that default path."""
+    t = tables["sw"]
+    q, f, s = (np.asarray(t[k], np.float64) for k in ("solar_source_quiet", "solar_source_facular",
+                                                      "solar_source_sunspot"))
+    k = oracle_mod.GasOptics(t, S.ATM_GASES)
+    want = q + (t["mg_default"] - 0.1495954) * f + (t["sb_default"] - 0.00066696) * s
+    np.testing.assert_allclose(k.solar_source(), want, rtol=1e-15)
+    for mg, sb in ((0.1495954, 0.00066696), (0.13, 400.0), (0.2, 2500.0)):
+        k.set_solar_variability(mg, sb)
+        np.testing.assert_allclose(k.solar_source(), q + (mg - 0.1495954) * f + (sb - 0.00066696) * s, rtol=1e-15)
+    with pytest.raises(RuntimeError):
+        oracle_mod.GasOptics(tables["lw"], S.ATM_GASES).set_solar_variability(0.15, 900.0)

@@ -66,6 +66,25 @@ def test_config2_grid_fused_forward_matches_oracle(oracle_mod, tables, gpu):
     _compare(sw, osw(host), cols, "8192x128 sw")
 
 
+def test_config2_grid_staged_fp32_matches_oracle(oracle_mod, tables, gpu):
+    """The class-API sequence in FP32 on the whole 8192 x 128 grid: gas optics on the packed
+    tables, the TMA-staged longwave solver, the chunked shortwave solver, broadband sums and
+    heating rates from absorbed flux; every 32nd column against the oracle."""
+    import torch
+    from rrtmgp_b200.solver import atm_to_device
+    base, _ = _solvers(tables)
+    atm = S.make_atmosphere(8192, 128, seed=42, clouds=True)
+    d = atm_to_device(atm, torch.float32, gpu)
+    top = bool(atm["play"][0, 0] < atm["play"][-1, 0])
+    lw, sw = base.solve_lw(d, top_at_1=top), base.solve_sw(d, top_at_1=top)
+    torch.cuda.synchronize()
+    cols = np.arange(0, 8192, 32)
+    host = _take(atm, cols)
+    olw, osw = _oracles(oracle_mod, tables)
+    _compare(lw, olw(host), cols, "staged 8192x128 lw")
+    _compare(sw, osw(host), cols, "staged 8192x128 sw")
+
+
 def _take(atm, cols):
     """The columns `cols` (any index array) of a host atmosphere."""
     out = {}

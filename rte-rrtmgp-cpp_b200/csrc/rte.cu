@@ -365,17 +365,30 @@ __global__ void __launch_bounds__(512, CL == 8 ? 2 : 1) lw_solver_tma(const __gr
     float* const sm_bu = sm_bd + nw * 32;
     uint64_t* const bar = reinterpret_cast<uint64_t*>(sm_bu + nw * 32);   // 8-byte aligned: nw * 32 floats
     const int nct = (ncol + 31) >> 5;
-    const long long ntiles = (long long)nct * ngpt;
-    const long long t0 = blockIdx.x, dt = gridDim.x;
     const unsigned tx_bytes = 4u * unsigned(tile_floats) * 4u;
+    // Tile cursor (g-point g, column tile ct): the block visits tiles blockIdx.x + k gridDim.x
+    // of g * nct + ct; one division at the start, then 32-bit steps (the host keeps
+    // nct * ngpt below 2^31).
+    const int dg = int(gridDim.x) / nct, dct = int(gridDim.x) - dg * nct;
+    auto advance = [&](int& gq, int& cq) {
+        cq += dct;
+        gq += dg;
+        if (cq >= nct) {
+            cq -= nct;
+            ++gq;
+        }
+    };
+    int g = int(blockIdx.x) / nct, ct = int(blockIdx.x) - g * nct;   // current tile
+    int gn = g, ctn = ct;                                              // next tile
+    advance(gn, ctn);
 
-    auto issue = [&](long long t) {
-        const int g = int(t / nct), x = int(t % nct) * 32;
+    auto issue = [&](int gq, int cq) {
+        const int x = cq * 32;
         tma::mbar_arrive_expect_tx(bar, tx_bytes);
-        tma::load_3d(stage, &m_tau, x, 0, g, bar);
-        tma::load_3d(stage + tile_floats, &m_lay, x, 0, g, bar);
-        tma::load_3d(stage + 2 * tile_floats, &m_dn, x, 0, g, bar);
-        tma::load_3d(stage + 3 * tile_floats, &m_up, x, 0, g, bar);
+        tma::load_3d(stage, &m_tau, x, 0, gq, bar);
+        tma::load_3d(stage + tile_floats, &m_lay, x, 0, gq, bar);
+        tma::load_3d(stage + 2 * tile_floats, &m_dn, x, 0, gq, bar);
+        tma::load_3d(stage + 3 * tile_floats, &m_up, x, 0, gq, bar);
     };
     if (threadIdx.x == 0) {
         tma::prefetch_map(&m_tau);
@@ -384,10 +397,9 @@ __global__ void __launch_bounds__(512, CL == 8 ? 2 : 1) lw_solver_tma(const __gr
         tma::prefetch_map(&m_up);
         tma::mbar_init(bar, 1);
         tma::fence_mbar_init();
-        if (t0 < ntiles) issue(t0);
+        if (g < ngpt) issue(g, ct);
     }
-    int k = 0;
-    for (long long t = t0; t < ntiles; t += dt, ++k) {
+    for (int k = 0; g < ngpt; ++k) {
         if (threadIdx.x == 0) s_ok = tma::mbar_wait(bar, k & 1);
         __syncthreads();
         if (!s_ok) {
@@ -414,15 +426,17 @@ __global__ void __launch_bounds__(512, CL == 8 ? 2 : 1) lw_solver_tma(const __gr
             }
         }
         __syncthreads();   // every read of the stage done
-        if (threadIdx.x == 0 && t + dt < ntiles) {
+        if (threadIdx.x == 0 && gn < ngpt) {
             tma::fence_proxy_async_smem();
-            issue(t + dt);
+            issue(gn, ctn);
         }
-        const int g = int(t / nct);
-        const int icol = int(t % nct) * 32 + lane;
+        const int icol = ct * 32 + lane;
         lw_chunk_maps<float, CL>(tr, lay, sdn, sup, sm_a, sm_bd, sm_bu, w, lane);
         __syncthreads();   // maps visible
         if (icol < ncol) lw_chunk_levels<float, CL>(a, tr, sdn, sup, sm_a, sm_bd, sm_bu, w, nw, lane, icol, g);
+        g = gn;
+        ct = ctn;
+        advance(gn, ctn);
     }
 }
 
@@ -636,10 +650,12 @@ int lw_smem_block(int nlay, size_t* smem)
 }
 
 // The TMA variant needs 16-byte row strides (ncol a multiple of 4) and 16-byte aligned arrays.
-inline bool lw_tma_ok(int ncol, int nlay, const float* tau, const float* lay, const float* dn, const float* up)
+inline bool lw_tma_ok(int ncol, int nlay, int ngpt, const float* tau, const float* lay, const float* dn,
+                      const float* up)
 {
     auto al = [](const float* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
-    return nlay <= kLwTmaMaxLay && ncol % 4 == 0 && al(tau) && al(lay) && al(dn) && al(up);
+    return nlay <= kLwTmaMaxLay && ncol % 4 == 0 && (long long)ceil_div(ncol, 32) * ngpt < (1ll << 31) - 1024 &&
+           al(tau) && al(lay) && al(dn) && al(up);
 }
 
 int lw_solver_tma_launch(const LwChunkArgs<float>& a, int ngpt, const float* tau, const float* lay,
@@ -692,7 +708,7 @@ int rte_lw(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const T* tau, 
         const T* lev_dn = top_at_1 ? lev_inc : lev_dec;
         const T* lev_up = top_at_1 ? lev_dec : lev_inc;
         if constexpr (sizeof(T) == 4) {
-            if (lw_tma_ok(ncol, nlay, tau, lay_src, lev_dn, lev_up))
+            if (lw_tma_ok(ncol, nlay, b->ngpt, tau, lay_src, lev_dn, lev_up))
                 return lw_solver_tma_launch(a, b->ngpt, tau, lay_src, lev_dn, lev_up, stream);
         }
         const dim3 grid(ceil_div(ncol, 32), b->ngpt);

@@ -205,9 +205,11 @@ gas_optics_lw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
     const float tl_dn = tlev[cl];
     const float ts = tsfc[icol];
 
-    // minor_g entries of the next g-point are loaded one iteration ahead, so that the kminor
-    // loads of an iteration do not wait on a dependent table load
-    int4 nx0 = __ldg(k.minor_g[0]), nx1 = __ldg(k.minor_g[1]);
+    // minor_g entries of the layer's own atmosphere (s.itropo), those of the next g-point
+    // loaded one iteration ahead, so that the kminor loads of an iteration do not wait on a
+    // dependent table load; the minor loop runs to this atmosphere's count
+    const int4* const mgt = k.minor_g[s.itropo];
+    int4 nx = __ldg(mgt);
     for (int b = 0; b < k.nband; ++b) {
         const int g0 = k.band_lims[2 * b], g1 = k.band_lims[2 * b + 1];
         fused::Rec R;
@@ -226,10 +228,9 @@ gas_optics_lw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
         // two g-points per iteration: their table loads overlap (LW 1.89 -> 1.77 ms at 8192 x 128)
 #pragma unroll 2
         for (int g = g0; g < g1; ++g) {
-            const int4 mg0 = nx0, mg1 = nx1;
-            nx0 = next_minor_row(k.minor_g[0], g + 1, k.ngpt);
-            nx1 = next_minor_row(k.minor_g[1], g + 1, k.ngpt);
-            const float ta = fused::tau_abs<DENSE>(k, R, g, R.a ? mg1 : mg0, max(mg0.x, mg1.x), scal, kThreads);
+            const int4 mg = nx;
+            nx = next_minor_row(mgt, g + 1, k.ngpt);
+            const float ta = fused::tau_abs<DENSE>(k, R, g, mg, mg.x, scal, kThreads);
             const float4 p0 = __ldg(k.pfrac4 + (R.kb.x + g));
             const float4 p1 = __ldg(k.pfrac4 + (R.kb.y + g));
             const float pfrac = (wp0.x * p0.x + wp0.y * p0.y + wp0.z * p0.z + wp0.w * p0.w) +
@@ -273,7 +274,8 @@ gas_optics_sw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
     const float col_rayl = cg[k.idx_h2o * kThreads] + cg[0];
     const float two_tmin = 2.f * FLT_MIN;
 
-    int4 nx0 = __ldg(k.minor_g[0]), nx1 = __ldg(k.minor_g[1]);
+    const int4* const mgt = k.minor_g[s.itropo];   // as the longwave kernel
+    int4 nx = __ldg(mgt);
     for (int b = 0; b < k.nband; ++b) {
         const int g0 = k.band_lims[2 * b], g1 = k.band_lims[2 * b + 1];
         fused::Rec R;
@@ -282,10 +284,9 @@ gas_optics_sw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
         // two g-points per iteration, as the longwave kernel
 #pragma unroll 2
         for (int g = g0; g < g1; ++g) {
-            const int4 mg0 = nx0, mg1 = nx1;
-            nx0 = next_minor_row(k.minor_g[0], g + 1, k.ngpt);
-            nx1 = next_minor_row(k.minor_g[1], g + 1, k.ngpt);
-            const float ta = fused::tau_abs<DENSE>(k, R, g, R.a ? mg1 : mg0, max(mg0.x, mg1.x), scal, kThreads);
+            const int4 mg = nx;
+            nx = next_minor_row(mgt, g + 1, k.ngpt);
+            const float ta = fused::tau_abs<DENSE>(k, R, g, mg, mg.x, scal, kThreads);
             const float2 r0 = __ldg(k.krayl2 + (kr0 + g));
             const float2 r1 = __ldg(k.krayl2 + (kr1 + g));
             const float tr = (R.fm.x * r0.x + R.fm.y * r0.y + R.fm.z * r1.x + R.fm.w * r1.y) * col_rayl;

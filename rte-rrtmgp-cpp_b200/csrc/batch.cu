@@ -127,7 +127,8 @@ struct SwItemIo : ItemIo {
 template <bool DENSE>
 __global__ void __launch_bounds__(kBatchThreads, 1)
 batch_forward_kernel(const KdistView<float> klw, const KdistView<float> ksw, const BatchItem* __restrict__ items,
-                     const long long* __restrict__ tile_start, int nitems, unsigned long long* __restrict__ counter)
+                     const long long* __restrict__ tile_start, const int* __restrict__ tile_item, int nitems,
+                     unsigned long long* __restrict__ counter)
 {
     __shared__ long long s_tile;
     __shared__ int s_item;
@@ -135,13 +136,8 @@ batch_forward_kernel(const KdistView<float> klw, const KdistView<float> ksw, con
     for (;;) {
         if (threadIdx.x == 0) {
             const long long t = (long long)atomicAdd(counter, 1ull);
-            int lo = 0, hi = nitems;   // last item with tile_start[item] <= t
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (tile_start[mid] <= t) lo = mid; else hi = mid;
-            }
             s_tile = t;
-            s_item = lo;
+            s_item = t < ntiles ? __ldg(tile_item + t) : 0;   // the item of tile t: one load
         }
         __syncthreads();
         const long long t = s_tile;
@@ -251,6 +247,8 @@ struct rrtmgp_b200_batch_t {
     size_t smem = 0;
     BatchItem* d_items = nullptr;
     long long* d_starts = nullptr;
+    int* d_tile_item = nullptr;        // item of every tile (work order)
+    size_t cap_tiles = 0;
     size_t cap_items = 0;
     unsigned long long* d_counter = nullptr;
     cudaStream_t cap_stream = nullptr;
@@ -358,6 +356,21 @@ int upload(rrtmgp_b200_batch_t* b, const std::vector<BatchItem>& list, long long
     ntiles = starts.back();
     int st = ensure_capacity(b, std::max<size_t>(list.size(), 1));
     if (st) return st;
+    std::vector<int> tile_item(size_t(std::max<long long>(ntiles, 1)), 0);
+    for (size_t i = 0; i < list.size(); ++i)
+        std::fill(tile_item.begin() + starts[i], tile_item.begin() + starts[i + 1], int(i));
+    if (tile_item.size() > b->cap_tiles) {
+        if (b->d_tile_item) cudaFree(b->d_tile_item);
+        b->d_tile_item = nullptr;
+        b->cap_tiles = 0;
+        if (cudaMalloc(&b->d_tile_item, sizeof(int) * tile_item.size()) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(RRTMGP_B200_ERR_ALLOC, "batch: tile table allocation failed");
+        }
+        b->cap_tiles = tile_item.size();
+    }
+    RB_CUDA(cudaMemcpy(b->d_tile_item, tile_item.data(), sizeof(int) * tile_item.size(), cudaMemcpyHostToDevice),
+            "batch: tile table upload");
     RB_CUDA(cudaMemcpy(b->d_items, list.data(), sizeof(BatchItem) * list.size(), cudaMemcpyHostToDevice),
             "batch: work table upload");
     RB_CUDA(cudaMemcpy(b->d_starts, starts.data(), sizeof(long long) * starts.size(), cudaMemcpyHostToDevice),
@@ -398,9 +411,11 @@ int launch_persistent(rrtmgp_b200_batch_t* b, const BatchItem* d_items, const lo
     const KdistView<float> klw = b->k[0] ? b->k[0]->v32 : KdistView<float>{};
     const KdistView<float> ksw = b->k[1] ? b->k[1]->v32 : KdistView<float>{};
     if (b->dense)
-        batch_forward_kernel<true><<<ctas, kBatchThreads, smem, s>>>(klw, ksw, d_items, d_starts, nitems, b->d_counter);
+        batch_forward_kernel<true><<<ctas, kBatchThreads, smem, s>>>(klw, ksw, d_items, d_starts, b->d_tile_item, nitems,
+                                                                     b->d_counter);
     else
-        batch_forward_kernel<false><<<ctas, kBatchThreads, smem, s>>>(klw, ksw, d_items, d_starts, nitems, b->d_counter);
+        batch_forward_kernel<false><<<ctas, kBatchThreads, smem, s>>>(klw, ksw, d_items, d_starts, b->d_tile_item,
+                                                                      nitems, b->d_counter);
     RB_LAUNCH("batch_forward_kernel");
     return RRTMGP_B200_OK;
 }
@@ -626,6 +641,7 @@ extern "C" int rrtmgp_b200_batch_destroy(rrtmgp_b200_batch b)
     if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
     if (b->d_items) cudaFree(b->d_items);
     if (b->d_starts) cudaFree(b->d_starts);
+    if (b->d_tile_item) cudaFree(b->d_tile_item);
     if (b->d_counter) cudaFree(b->d_counter);
     delete b;
     return RRTMGP_B200_OK;

@@ -97,7 +97,8 @@ __device__ __forceinline__ LocalAdj sw_local_adjoint(float tau, float w0, float 
     const float kk = 2.f * omw * kq;
     const bool kk_on = kk > 1.e-12f;
     const float kkc = fmaxf(kk, 1.e-12f);
-    const float k = kkc * rsqrtf(kkc);
+    const float rk = rsqrtf(kkc);   // 1 / k
+    const float k = kkc * rk;
     float E1, e1, En, Tn;
     one_minus_exp(k * tau, E1, e1);
     one_minus_exp(tau * mu0_inv, En, Tn);
@@ -203,18 +204,22 @@ __device__ __forceinline__ LocalAdj sw_local_adjoint(float tau, float w0, float 
             e2_b -= W_b * En;
             En_b -= W_b * (1.f + e2);
         }
-        w0_b += c_b * rt / (1.f + km);
-        rt_b += c_b * w0 / (1.f + km);
-        km_b -= c_b * cI / (1.f + km);
+        // divisions of the reverse mode as products with approximate reciprocals, like the
+        // forward's __fdividef (an IEEE division is a multi-instruction sequence)
+        const float i1km = __fdividef(1.f, 1.f + km);
+        w0_b += c_b * rt * i1km;
+        rt_b += c_b * w0 * i1km;
+        km_b -= c_b * cI * i1km;
         float x_b;
         if (xs) {
             const float dser = -.5f + xi * (1.f / 3.f - xi * (1.f / 8.f - xi * (1.f / 30.f)));
             e1_b += e1phi_b * ser;
             x_b = e1phi_b * e1 * dser;
         } else {
-            e1_b += e1phi_b / xi;
-            Tn_b -= e1phi_b / xi;
-            x_b = -e1phi_b * e1phi / xi;
+            const float ixi = __fdividef(1.f, xi);
+            e1_b += e1phi_b * ixi;
+            Tn_b -= e1phi_b * ixi;
+            x_b = -e1phi_b * e1phi * ixi;
         }
         tm_b += x_b * (1.f - km);
         km_b -= x_b * tmu;
@@ -267,9 +272,10 @@ __device__ __forceinline__ LocalAdj sw_local_adjoint(float tau, float w0, float 
             En_b -= W2_b * (1.f + e2);
         }
         // rt2 = w0 rt / fact, fact = 1 - km^2
-        w0_b += rt2_b * rt / fact;
-        rt_b += rt2_b * w0 / fact;
-        const float fact_b = -rt2_b * rt2 / fact;
+        const float ifact = __fdividef(1.f, fact);
+        w0_b += rt2_b * rt * ifact;
+        rt_b += rt2_b * w0 * ifact;
+        const float fact_b = -rt2_b * rt2 * ifact;
         km_b -= fact_b * 2.f * km;
     }
     k_b += km_b * mu0;
@@ -298,7 +304,7 @@ __device__ __forceinline__ LocalAdj sw_local_adjoint(float tau, float w0, float 
     const float xn_b = Tn * (En_b - Tn_b);
     tau_b += xn_b * mu0_inv;
     // k = sqrt(max(kk, 1e-12)), kk = 2 omw kq
-    const float kk_b = kk_on ? k_b * 0.5f / k : 0.f;
+    const float kk_b = kk_on ? k_b * 0.5f * rk : 0.f;
     omw_b += kk_b * 2.f * kq;
     w0_b += kk_b * 2.f * omw * (-.5f * (1.f + 3.f * g));
     g_b += kk_b * 2.f * omw * (-1.5f * w0);

@@ -715,7 +715,9 @@ def main():
     # block overlap the kernels of the other.  Each block has its own pinned host buffers and
     # device arrays (a caller with one large host array would stage it in blocks the same way);
     # blocks on one stream reuse its solver's output buffers in stream order.
-    nblk = 4 if args.ncol >= 4 * 256 else 1
+    # 8 blocks at 8192 columns (1024 per launch): the first block's input copy and the last
+    # block's output copy, the only ones not overlapped, are 1/8 of a step's copies
+    nblk = 8 if args.ncol >= 8 * 1024 else (4 if args.ncol >= 4 * 256 else 1)
     edges = [int(x) for x in np.linspace(0, args.ncol, nblk + 1)]
 
     def col_block(t, a, b):

@@ -510,7 +510,7 @@ struct SwChunkSmem {
 };
 
 // After every layer of the chunk is added (column ic, g-point g): the direct beam and the
-// adding composites exchanged between the chunks (two barriers), albedo and source at the
+// adding composites exchanged between the chunks (three barriers), albedo and source at the
 // chunk bottom, and the level outputs.  Threads of columns past ncol take part in the
 // barriers and write nothing.
 template <typename T, int CL>
@@ -533,27 +533,36 @@ __device__ __forceinline__ void sw_chunk_finish(const SwChunkArgs<T>& a, SwChunk
     sm.u[w * 32 + lane] = c.cU * dtop;
     sm.d[w * 32 + lane] = c.cD * dtop;
     __syncthreads();
-    // 3. albedo and source at the chunk bottom (from the surface up), and the diffuse flux at
-    //    the chunk top as fa * (TOA diffuse) + fb
-    T alb = af, src = dsfc * ad, alb_in = af, src_in = dsfc * ad, fa = T(1), fb = T(0);
-    for (int q = nw - 1; q >= 0; --q) {
-        if (q == w) {
-            alb_in = alb;
-            src_in = src;
-            if (w == 0) break;
+    // 3. One warp scans the chunk composites: from the surface up, the albedo and source at the
+    //    bottom of every chunk and the transfer of the diffuse flux through it (flux at the
+    //    chunk bottom = F * flux at its top + G); then from the top down, the diffuse flux
+    //    entering every chunk.  The results replace the composites in shared memory (a slot is
+    //    read before it is rewritten) and every warp reads its own chunk's after one more
+    //    barrier: with every warp scanning all chunks itself, the scans were O(chunks^2) loads
+    //    and divisions per tile.
+    if (w == 0) {
+        T alb = af, src = dsfc * ad;
+        for (int q = nw - 1; q >= 0; --q) {
+            const int x = q * 32 + lane;
+            const T mRu = sm.ru[x], mRd = sm.rd[x], mT = sm.t[x], mU = sm.u[x], mD = sm.d[x];
+            const T den = adding_den(mRd, alb);
+            sm.ru[x] = mT * den;                 // F
+            sm.rd[x] = (mRd * src + mD) * den;   // G
+            sm.t[x] = alb;                       // albedo and source at the chunk bottom
+            sm.u[x] = src;
+            const T nalb = mRu + mT * mT * alb * den;
+            src = mU + mT * (alb * mD + src) * den;
+            alb = nalb;
         }
-        const T mRu = sm.ru[q * 32 + lane], mRd = sm.rd[q * 32 + lane], mT = sm.t[q * 32 + lane];
-        const T mU = sm.u[q * 32 + lane], mD = sm.d[q * 32 + lane];
-        const T den = adding_den(mRd, alb);
-        if (q < w) {
-            const T F = mT * den, G = (mRd * src + mD) * den;
-            fb = fa * G + fb;
-            fa *= F;
+        T f = fd_toa;
+        for (int q = 0; q < nw; ++q) {
+            const int x = q * 32 + lane;
+            sm.d[x] = f;                         // diffuse flux at the chunk top
+            f = sm.ru[x] * f + sm.rd[x];
         }
-        const T nalb = mRu + mT * mT * alb * den;
-        src = mU + mT * (alb * mD + src) * den;
-        alb = nalb;
     }
+    __syncthreads();
+    const T alb_in = sm.t[w * 32 + lane], src_in = sm.u[w * 32 + lane], fd_in = sm.d[w * 32 + lane];
     // 4. albedo and upward source at the top of every layer (bottom-up)
     T vA[CL];
     {
@@ -579,7 +588,7 @@ __device__ __forceinline__ void sw_chunk_finish(const SwChunkArgs<T>& a, SwChunk
     T* const up = a.flux_up + off;
     T* const dn = a.flux_dn + off;
     T* const dr = a.flux_dir + off;
-    T fd = fa * fd_toa + fb;
+    T fd = fd_in;
 #pragma unroll
     for (int i = 0; i < CL; ++i) {
         const T a_n = (i + 1 < CL) ? vA[i + 1] : alb_in;

@@ -234,32 +234,51 @@ __device__ __forceinline__ void lw_chunk_maps(T (&tr)[CL], const T (&lay)[CL], T
     sm_bu[w * 32 + lane] = Bu;
 }
 
-// After the maps of all nw chunks are visible: the radiances entering the chunk (scan over the
-// chunks above, then below through the surface), and re-sweeps writing every level of the
-// chunk (column ic, g-point g; level j0 + i is the top of layer j0 + i).
+// After the maps of all nw chunks are visible, one warp (warp 0) turns them into the radiances
+// entering every chunk, each slot of the maps read before it is rewritten: from the top, the
+// downward radiance at each chunk top (into sm_bd); from the surface, the upward radiance at
+// each chunk bottom (into sm_bu; the last chunk's is the radiance leaving the surface) and,
+// with the Jacobian, the surface term carried to each chunk bottom (into sm_a).  With every
+// warp scanning the chunks above and below itself, the scans were O(chunks^2) loads per tile.
+template <typename T>
+__device__ __forceinline__ void lw_chunk_scan(const LwChunkArgs<T>& a, T* sm_a, T* sm_bd, T* sm_bu, int nw, int lane,
+                                              int ic, int g)
+{
+    const int ncol = a.ncol;
+    T x = (a.inc_flux ? a.inc_flux[ic + size_t(g) * ncol] : T(0)) / pi_value<T>();
+    for (int c = 0; c < nw; ++c) {
+        const T A = sm_a[c * 32 + lane], B = sm_bd[c * 32 + lane];
+        sm_bd[c * 32 + lane] = x;
+        x = A * x + B;
+    }
+    const T emis = a.sfc_emis[a.gpt2band[g] + size_t(ic) * a.nband];
+    T y = x * (T(1) - emis) + emis * a.sfc_src[ic + size_t(g) * ncol];   // leaving the surface
+    T yj = a.flux_up_jac ? emis * a.sfc_src_jac[ic + size_t(g) * ncol] : T(0);
+    for (int c = nw - 1; c >= 0; --c) {
+        const T A = sm_a[c * 32 + lane], B = sm_bu[c * 32 + lane];
+        sm_bu[c * 32 + lane] = y;
+        sm_a[c * 32 + lane] = yj;
+        y = A * y + B;
+        yj *= A;
+    }
+}
+
+// After lw_chunk_scan: re-sweeps writing every level of the chunk (column ic, g-point g; level
+// j0 + i is the top of layer j0 + i).
 template <typename T, int CL>
 __device__ __forceinline__ void lw_chunk_levels(const LwChunkArgs<T>& a, const T (&tr)[CL], const T (&sdn)[CL],
                                                 const T (&sup)[CL], const T* sm_a, const T* sm_bd, const T* sm_bu,
-                                                int w, int nw, int lane, int ic, int g)
+                                                int w, int lane, int ic, int g)
 {
     const int ncol = a.ncol, nlay = a.nlay;
     const size_t ncv = size_t(ncol) * (nlay + 1);
     const T two_pi_w = pi_value<T>();
     const int j0 = w * CL;
-    // radiance entering the chunk at its top, then at the surface
-    T radn = (a.inc_flux ? a.inc_flux[ic + size_t(g) * ncol] : T(0)) / two_pi_w;
-    for (int c = 0; c < w; ++c) radn = sm_a[c * 32 + lane] * radn + sm_bd[c * 32 + lane];
-    T rs = radn;
-    for (int c = w; c < nw; ++c) rs = sm_a[c * 32 + lane] * rs + sm_bd[c * 32 + lane];
-    const T emis = a.sfc_emis[a.gpt2band[g] + size_t(ic) * a.nband];
-    const T rsfc = rs * (T(1) - emis) + emis * a.sfc_src[ic + size_t(g) * ncol];   // leaving the surface
-    T rup = rsfc;
-    for (int c = nw - 1; c > w; --c) rup = sm_a[c * 32 + lane] * rup + sm_bu[c * 32 + lane];
-    // surface-temperature Jacobian: the surface term alone, attenuated by the chunks below
-    const T jsfc = a.flux_up_jac ? emis * a.sfc_src_jac[ic + size_t(g) * ncol] : T(0);
-    T rjac = jsfc;
-    if (a.flux_up_jac)
-        for (int c = nw - 1; c > w; --c) rjac *= sm_a[c * 32 + lane];
+    T radn = sm_bd[w * 32 + lane];          // entering the chunk at its top
+    T rup = sm_bu[w * 32 + lane];           // entering the chunk at its bottom
+    const T rsfc = rup;                     // for the last chunk: leaving the surface
+    T rjac = sm_a[w * 32 + lane];           // surface-temperature Jacobian at the chunk bottom
+    const T jsfc = rjac;
     T* const dn = a.flux_dn + ic + size_t(g) * ncv;
     T* const up = a.flux_up + ic + size_t(g) * ncv;
     const ptrdiff_t step = a.top_at_1 ? ptrdiff_t(ncol) : -ptrdiff_t(ncol);
@@ -321,8 +340,10 @@ __global__ void __launch_bounds__(MAXT) lw_solver_chunked(const LwChunkArgs<T> a
     }
     lw_chunk_maps<T, CL>(tr, lay, sdn, sup, sm_a, sm_bd, sm_bu, w, lane);
     __syncthreads();
+    if (w == 0) lw_chunk_scan<T>(a, sm_a, sm_bd, sm_bu, nw, lane, ic, g);
+    __syncthreads();
     if (!cv) return;
-    lw_chunk_levels<T, CL>(a, tr, sdn, sup, sm_a, sm_bd, sm_bu, w, nw, lane, ic, g);
+    lw_chunk_levels<T, CL>(a, tr, sdn, sup, sm_a, sm_bd, sm_bu, w, lane, ic, g);
 }
 
 // TMA-staged FP32 variant (nlay <= kLwTmaMaxLay).  A tile is the (32 columns x nlay layers)
@@ -433,7 +454,9 @@ __global__ void __launch_bounds__(512, CL == 8 ? 2 : 1) lw_solver_tma(const __gr
         const int icol = ct * 32 + lane;
         lw_chunk_maps<float, CL>(tr, lay, sdn, sup, sm_a, sm_bd, sm_bu, w, lane);
         __syncthreads();   // maps visible
-        if (icol < ncol) lw_chunk_levels<float, CL>(a, tr, sdn, sup, sm_a, sm_bd, sm_bu, w, nw, lane, icol, g);
+        if (w == 0) lw_chunk_scan<float>(a, sm_a, sm_bd, sm_bu, nw, lane, icol < ncol ? icol : 0, g);
+        __syncthreads();   // entering radiances visible
+        if (icol < ncol) lw_chunk_levels<float, CL>(a, tr, sdn, sup, sm_a, sm_bd, sm_bu, w, lane, icol, g);
         g = gn;
         ct = ctn;
         advance(gn, ctn);

@@ -218,30 +218,37 @@ __device__ __forceinline__ void sw_forward_column(const Cx& cx, const KdistView<
         cx.put(&sm_compd[w * 32 + lane], cD * dtop);
         cx.sync();
 
-        // 3. albedo and source at this chunk's bottom; incident diffuse flux at its top
+        // 3. albedo and source at this chunk's bottom; incident diffuse flux at its top.  Chunk 0's
+        //    warp scans the composites of all chunks: from the surface up, the albedo and source
+        //    at each chunk bottom and the chunk's transfer of the diffuse flux (flux at its bottom
+        //    = F * flux at its top + G); then from the top down, the diffuse flux entering each
+        //    chunk (no diffuse flux at the top of the atmosphere).  The results replace the
+        //    composites (each slot read before it is rewritten, through put for every CTA of a
+        //    cluster), and every warp reads its own chunk's after one more barrier: with every
+        //    warp scanning the chunks itself the scans were O(chunks^2) per group.
         const float ad = gv ? __ldg(io.alb_dir() + gband + size_t(cx.icol()) * nband) : 0.f;
         const float af = gv ? __ldg(io.alb_dif() + gband + size_t(cx.icol()) * nband) : 0.f;
-        float alb = af, src = dsfc * ad;
-        float alb_in = af, src_in = src;
-        float fa = 1.f, fb = 0.f;
-        for (int c = NW - 1; c >= 0; --c) {
-            if (c == w) {
-                alb_in = alb;
-                src_in = src;
-                if (w == 0) break;
+        if (w == 0) {
+            float alb = af, src = dsfc * ad;
+            for (int c = NW - 1; c >= 0; --c) {
+                const float4 m = sm_comp[c * 32 + lane];
+                const float D = sm_compd[c * 32 + lane];
+                const float den = __fdividef(1.f, fmaf(-m.y, alb, 1.f));
+                cx.put(&sm_comp[c * 32 + lane], make_float4(alb, src, m.z * den, fmaf(m.y, src, D) * den));
+                const float nalb = m.x + m.z * m.z * alb * den;
+                src = m.w + m.z * fmaf(alb, D, src) * den;
+                alb = nalb;
             }
-            const float4 m = sm_comp[c * 32 + lane];
-            const float D = sm_compd[c * 32 + lane];
-            const float den = __fdividef(1.f, fmaf(-m.y, alb, 1.f));
-            if (c < w) {
-                const float F = m.z * den, G = fmaf(m.y, src, D) * den;
-                fb = fmaf(fa, G, fb);
-                fa *= F;
+            float f = 0.f;
+            for (int c = 0; c < NW; ++c) {
+                cx.put(&sm_compd[c * 32 + lane], f);
+                const float4 r = sm_comp[c * 32 + lane];
+                f = fmaf(r.z, f, r.w);
             }
-            const float nalb = m.x + m.z * m.z * alb * den;
-            src = m.w + m.z * fmaf(alb, D, src) * den;
-            alb = nalb;
         }
+        cx.sync();
+        const float4 own = sm_comp[w * 32 + lane];
+        const float alb_in = own.x, src_in = own.y, fb = sm_compd[w * 32 + lane];
 
         // 4. pass 2 (bottom-up): albedo and upward source per level
         float vA[CL];

@@ -353,9 +353,10 @@ __global__ void __launch_bounds__(MAXT) lw_solver_chunked(const LwChunkArgs<T> a
 // registers, frees the stage, and thread 0 has the TMA unit copy tile k + 1 into it while the
 // block computes tile k (as lw_solver_chunked), so HBM reads continue through the compute and
 // store phases (the one-tile-per-block kernel above has its loads in flight only between its
-// start and its first use).  Lane = column: the stage reads are conflict-free rows.  Three
+// start and its first use).  Lane = column: the stage reads are conflict-free rows.  Four
 // barriers per tile: after thread 0's wait (hands out its outcome), after the stage reads
-// (frees the stage), after the maps (publishes them).
+// (frees the stage), after the maps (publishes them), after warp 0's scan of the maps
+// (lw_chunk_scan: publishes the radiances entering every chunk).
 // Shared memory: [array 4][layer nlay][32] floats, maps [3][nw][32], one mbarrier.
 constexpr int kLwTmaMaxLay = 192;
 
@@ -369,10 +370,10 @@ inline size_t lw_tma_smem_bytes(int nlay, int nw)
 
 template <int CL>
 __global__ void __launch_bounds__(512, CL == 8 ? 2 : 1) lw_solver_tma(const __grid_constant__ CUtensorMap m_tau,
-                                                     const __grid_constant__ CUtensorMap m_lay,
-                                                     const __grid_constant__ CUtensorMap m_dn,
-                                                     const __grid_constant__ CUtensorMap m_up,
-                                                     const LwChunkArgs<float> a, int ngpt)
+                                                                     const __grid_constant__ CUtensorMap m_lay,
+                                                                     const __grid_constant__ CUtensorMap m_dn,
+                                                                     const __grid_constant__ CUtensorMap m_up,
+                                                                     const LwChunkArgs<float> a, int ngpt)
 {
     extern __shared__ unsigned char smem_dyn[];
     __shared__ int s_ok;

@@ -9,6 +9,7 @@
 // (T, p, eta) corner are one 64-byte run.
 #include <cfloat>
 #include <cmath>
+#include <type_traits>
 
 #include "common.cuh"
 #include "fused_common.cuh"
@@ -142,6 +143,9 @@ gas_optics_sw_kernel(const KdistView<T> k, const GasSet<T> gases, int ncol, int 
 // are indexed per g-point, so they sit in shared memory, one column of max_nscal values per
 // thread (stride kThreads: no bank conflicts).
 // Usable when the tables satisfy the fused kernels' layout conditions (packed_tables_ok).
+// I32: every (column, layer, g-point) offset fits in 31 bits (packed_index32), so the output
+// offsets are 32-bit (one multiply-add per store address instead of 64-bit arithmetic and
+// fewer live registers at the occupancy's register cap).
 __host__ __device__ inline size_t packed_smem_bytes(int ngas, int nscal)
 {
     return sizeof(float) * size_t(ngas + 1 + nscal) * kThreads;
@@ -150,6 +154,11 @@ __host__ __device__ inline size_t packed_smem_bytes(int ngas, int nscal)
 inline bool packed_tables_ok(const KdistView<float>& v, bool lw)
 {
     return fused::fused_layout_ok(v, !lw, 1 << 30) && v.minor_g[0] && v.minor_g[1];
+}
+
+inline bool packed_index32(int ncol, int nlay, int ngpt)
+{
+    return size_t(ncol) * size_t(nlay) * size_t(ngpt) < (size_t(1) << 31);
 }
 
 // minor_g row of g-point g (unused slots already repeat the first one), zeros past the end.
@@ -173,7 +182,7 @@ __device__ __forceinline__ fused::LayerState thread_layer_state(const LayerInter
     return s;
 }
 
-template <bool DENSE>
+template <bool DENSE, bool I32>
 __global__ void __launch_bounds__(kThreads, 7)
 gas_optics_lw_packed_kernel(const KdistView<float> k, const GasSet<float> gases, int ncol, int nlay,
                             const float* __restrict__ play, const float* __restrict__ plev,
@@ -187,11 +196,12 @@ gas_optics_lw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
     float* cg = reinterpret_cast<float*>(smem_raw) + tid;                       // [ngas + 1]
     float* scal = reinterpret_cast<float*>(smem_raw) + (k.ngas + 1) * kThreads + tid;   // [max_nscal]
 
+    using Idx = typename std::conditional<I32, unsigned, size_t>::type;
     const int icol = blockIdx.x * kBX + threadIdx.x;
     const int ilay = blockIdx.y * kBY + threadIdx.y;
     if (icol >= ncol || ilay >= nlay) return;
-    const size_t cl = size_t(icol) + size_t(ilay) * ncol;
-    const size_t ncl = size_t(ncol) * nlay;
+    const Idx cl = Idx(icol) + Idx(ilay) * Idx(ncol);
+    const Idx ncl = Idx(ncol) * Idx(nlay);
 
     const float p = play[cl], t = tlay[cl];
     fill_col_gas(k, gases, ncol, nlay, icol, ilay, plev, col_dry_in, cg, kThreads);
@@ -235,20 +245,20 @@ gas_optics_lw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
             const float4 p1 = __ldg(k.pfrac4 + (R.kb.y + g));
             const float pfrac = (wp0.x * p0.x + wp0.y * p0.y + wp0.z * p0.z + wp0.w * p0.w) +
                                 (wp1.x * p1.x + wp1.y * p1.y + wp1.z * p1.z + wp1.w * p1.w);
-            const size_t o = cl + size_t(g) * ncl;
+            const Idx o = cl + Idx(g) * ncl;
             tau[o] = ta;
             lay_src[o] = pfrac * pl;
             lev_inc[o] = pfrac * pinc;
             lev_dec[o] = pfrac * pdec;
             if (at_sfc) {
-                sfc_src[icol + size_t(g) * ncol] = pfrac * ps;
-                sfc_jac[icol + size_t(g) * ncol] = pfrac * (ps2 - ps);
+                sfc_src[Idx(icol) + Idx(g) * Idx(ncol)] = pfrac * ps;
+                sfc_jac[Idx(icol) + Idx(g) * Idx(ncol)] = pfrac * (ps2 - ps);
             }
         }
     }
 }
 
-template <bool DENSE>
+template <bool DENSE, bool I32>
 __global__ void __launch_bounds__(kThreads, 8)
 gas_optics_sw_packed_kernel(const KdistView<float> k, const GasSet<float> gases, int ncol, int nlay,
                             const float* __restrict__ play, const float* __restrict__ plev,
@@ -260,11 +270,12 @@ gas_optics_sw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
     float* cg = reinterpret_cast<float*>(smem_raw) + tid;                       // [ngas + 1]
     float* scal = reinterpret_cast<float*>(smem_raw) + (k.ngas + 1) * kThreads + tid;   // [max_nscal]
 
+    using Idx = typename std::conditional<I32, unsigned, size_t>::type;
     const int icol = blockIdx.x * kBX + threadIdx.x;
     const int ilay = blockIdx.y * kBY + threadIdx.y;
     if (icol >= ncol || ilay >= nlay) return;
-    const size_t cl = size_t(icol) + size_t(ilay) * ncol;
-    const size_t ncl = size_t(ncol) * nlay;
+    const Idx cl = Idx(icol) + Idx(ilay) * Idx(ncol);
+    const Idx ncl = Idx(ncol) * Idx(nlay);
 
     const float p = play[cl], t = tlay[cl];
     fill_col_gas(k, gases, ncol, nlay, icol, ilay, plev, col_dry_in, cg, kThreads);
@@ -291,9 +302,10 @@ gas_optics_sw_packed_kernel(const KdistView<float> k, const GasSet<float> gases,
             const float2 r1 = __ldg(k.krayl2 + (kr1 + g));
             const float tr = (R.fm.x * r0.x + R.fm.y * r0.y + R.fm.z * r1.x + R.fm.w * r1.y) * col_rayl;
             const float tt = ta + tr;
-            const size_t o = cl + size_t(g) * ncl;
+            const Idx o = cl + Idx(g) * ncl;
             tau[o] = tt;
-            ssa[o] = tt > two_tmin ? tr / tt : 0.f;
+            // approximate division (2 ulp for normal divisors; tt is far below 2^126)
+            ssa[o] = tt > two_tmin ? __fdividef(tr, tt) : 0.f;
             gasy[o] = 0.f;
         }
     }
@@ -346,8 +358,11 @@ int gas_optics_lw(rrtmgp_b200_kdist k, int ncol, int nlay, const T* play, const 
     if constexpr (std::is_same<T, float>::value) {
         if (packed_tables_ok(k->v32, true)) {
             const size_t psm = packed_smem_bytes(k->info.ngas, k->v32.max_nscal);
-            const auto kernel = k->v32.max_minor_per_g > 3 ? gas_optics_lw_packed_kernel<true>
-                                                           : gas_optics_lw_packed_kernel<false>;
+            const bool dense = k->v32.max_minor_per_g > 3, i32 = packed_index32(ncol, nlay, k->info.ngpt);
+            const auto kernel = dense ? (i32 ? gas_optics_lw_packed_kernel<true, true>
+                                             : gas_optics_lw_packed_kernel<true, false>)
+                                      : (i32 ? gas_optics_lw_packed_kernel<false, true>
+                                             : gas_optics_lw_packed_kernel<false, false>);
             kernel<<<grid, block, psm, as_stream(stream)>>>(k->v32, gs, ncol, nlay, play, plev, tlay, tsfc, tlev,
                                                             col_dry, tau, lay_src, lev_inc, lev_dec, sfc_src, sfc_jac);
             RB_LAUNCH("gas_optics_lw_packed_kernel");
@@ -388,8 +403,11 @@ int gas_optics_sw(rrtmgp_b200_kdist k, int ncol, int nlay, const T* play, const 
     if constexpr (std::is_same<T, float>::value) {
         if (packed_tables_ok(k->v32, false)) {
             const size_t psm = packed_smem_bytes(k->info.ngas, k->v32.max_nscal);
-            const auto kernel = k->v32.max_minor_per_g > 3 ? gas_optics_sw_packed_kernel<true>
-                                                           : gas_optics_sw_packed_kernel<false>;
+            const bool dense = k->v32.max_minor_per_g > 3, i32 = packed_index32(ncol, nlay, k->info.ngpt);
+            const auto kernel = dense ? (i32 ? gas_optics_sw_packed_kernel<true, true>
+                                             : gas_optics_sw_packed_kernel<true, false>)
+                                      : (i32 ? gas_optics_sw_packed_kernel<false, true>
+                                             : gas_optics_sw_packed_kernel<false, false>);
             kernel<<<grid, block, psm, as_stream(stream)>>>(k->v32, gs, ncol, nlay, play, plev, tlay, col_dry, tau,
                                                             ssa, g);
             RB_LAUNCH("gas_optics_sw_packed_kernel");

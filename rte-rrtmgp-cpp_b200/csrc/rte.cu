@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <mutex>
+#include <type_traits>
 
 #include "common.cuh"
 #include "rte_device.cuh"
@@ -536,8 +537,9 @@ struct SwChunkSmem {
 // After every layer of the chunk is added (column ic, g-point g): the direct beam and the
 // adding composites exchanged between the chunks (three barriers), albedo and source at the
 // chunk bottom, and the level outputs.  Threads of columns past ncol take part in the
-// barriers and write nothing.
-template <typename T, int CL>
+// barriers and write nothing.  Idx: the signed type of the output offsets (int when every
+// (column, level, g-point) offset fits in 31 bits).
+template <typename T, int CL, typename Idx>
 __device__ __forceinline__ void sw_chunk_finish(const SwChunkArgs<T>& a, SwChunk<T, CL>& c, const SwChunkSmem<T>& sm,
                                                 int w, int nw, int lane, bool cv, int ic, int g, T dir_toa, T fd_toa,
                                                 T ad, T af)
@@ -606,12 +608,12 @@ __device__ __forceinline__ void sw_chunk_finish(const SwChunkArgs<T>& a, SwChunk
     }
     // 5. diffuse fluxes (top-down) and the level outputs
     if (!cv) return;
-    const size_t off = ic + size_t(g) * ncol * (nlay + 1);
-    const ptrdiff_t step = a.top_at_1 ? ptrdiff_t(ncol) : -ptrdiff_t(ncol);
-    const ptrdiff_t o0 = a.top_at_1 ? ptrdiff_t(j0) * ncol : ptrdiff_t(nlay - j0) * ncol;   // level j0
-    T* const up = a.flux_up + off;
-    T* const dn = a.flux_dn + off;
-    T* const dr = a.flux_dir + off;
+    const Idx off = Idx(ic) + Idx(g) * Idx(ncol) * Idx(nlay + 1);
+    const Idx step = a.top_at_1 ? Idx(ncol) : -Idx(ncol);
+    const Idx o0 = off + (a.top_at_1 ? Idx(j0) * Idx(ncol) : Idx(nlay - j0) * Idx(ncol));   // level j0
+    T* const up = a.flux_up;
+    T* const dn = a.flux_dn;
+    T* const dr = a.flux_dir;
     T fd = fd_in;
 #pragma unroll
     for (int i = 0; i < CL; ++i) {
@@ -628,17 +630,19 @@ __device__ __forceinline__ void sw_chunk_finish(const SwChunkArgs<T>& a, SwChunk
     }
     if (j0 <= nlay - 1 && nlay - 1 < j0 + CL) {
         // fd is now at the chunk bottom (padding layers are the identity): the surface level
-        const ptrdiff_t o = o0 + (nlay - j0) * step;
+        const Idx o = o0 + Idx(nlay - j0) * step;
         up[o] = fd * alb_in + src_in;
         dn[o] = fd + dsfc;
         dr[o] = dsfc;
     }
 }
 
-template <typename T, int CL, int MAXT, int MINB = 1>
+// I32: every (column, level, g-point) offset fits in 31 bits (sw_index32).
+template <typename T, int CL, int MAXT, int MINB = 1, bool I32 = false>
 __global__ void __launch_bounds__(MAXT, MINB) sw_solver_chunked(const SwChunkArgs<T> a, const T* __restrict__ tau,
                                                                 const T* __restrict__ ssa, const T* __restrict__ gasy)
 {
+    using Idx = typename std::conditional<I32, int, ptrdiff_t>::type;
     __shared__ T sm_p[16 * 32];                                      // direct-beam product per chunk
     __shared__ T sm_ru[16 * 32], sm_rd[16 * 32], sm_t[16 * 32], sm_u[16 * 32], sm_d[16 * 32];   // composites
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -647,7 +651,7 @@ __global__ void __launch_bounds__(MAXT, MINB) sw_solver_chunked(const SwChunkArg
     const bool cv = icol < ncol;
     const int ic = cv ? icol : 0;
     const int g = blockIdx.y;
-    const size_t base = ic + size_t(g) * ncol * nlay;
+    const Idx base = Idx(ic) + Idx(g) * Idx(ncol) * Idx(nlay);
     const int band = a.gpt2band[g];
     const T m0 = a.mu0[ic], m0_inv = T(1) / m0;
     const T ad = a.alb_dir[band + size_t(ic) * a.nband], af = a.alb_dif[band + size_t(ic) * a.nband];
@@ -655,20 +659,34 @@ __global__ void __launch_bounds__(MAXT, MINB) sw_solver_chunked(const SwChunkArg
     const T fd_toa = a.inc_dif ? a.inc_dif[ic + size_t(g) * ncol] : T(0);
     const int j0 = w * CL;
 
-    // 1. layer coefficients; direct beam relative to the chunk top; adding composite of the chunk
+    // 1. layer coefficients; direct beam relative to the chunk top; adding composite of the chunk.
+    //    The optical properties of layer i + 1 are loaded while layer i is computed, from an
+    //    address clamped to the column's last layer (ic is a valid column for every thread and
+    //    j0 < nlay for every warp), so the loads are unconditional: inside the per-layer branch
+    //    each layer waited for its own loads from memory.
+    const auto layer_at = [&](int j) {
+        const int jc = min(j, nlay - 1);
+        return base + Idx(a.top_at_1 ? jc : nlay - 1 - jc) * Idx(ncol);
+    };
     SwChunk<T, CL> c;
+    Idx x = layer_at(j0);
+    T nt = tau[x], ns = ssa[x], ng = gasy[x];
 #pragma unroll
     for (int i = 0; i < CL; ++i) {
         const int j = j0 + i;
-        T R = T(0), Tt = T(1), Rdir = T(0), Tdir = T(0), Tn = T(1);
-        if (cv && j < nlay) {
-            const size_t x = base + size_t(a.top_at_1 ? j : nlay - 1 - j) * ncol;
-            sw_layer_coeffs<T>(tau[x], ssa[x], gasy[x], m0, m0_inv, R, Tt, Rdir, Tdir, Tn);
+        const T tj = nt, sj = ns, gj = ng;
+        if (i + 1 < CL) {
+            x = layer_at(j + 1);
+            nt = tau[x];
+            ns = ssa[x];
+            ng = gasy[x];
         }
+        T R = T(0), Tt = T(1), Rdir = T(0), Tdir = T(0), Tn = T(1);
+        if (cv && j < nlay) sw_layer_coeffs<T>(tj, sj, gj, m0, m0_inv, R, Tt, Rdir, Tdir, Tn);
         c.add_layer(i, R, Tt, Rdir, Tdir, Tn);
     }
-    sw_chunk_finish<T, CL>(a, c, SwChunkSmem<T>{sm_p, sm_ru, sm_rd, sm_t, sm_u, sm_d}, w, nw, lane, cv, ic, g,
-                           dir_toa, fd_toa, ad, af);
+    sw_chunk_finish<T, CL, Idx>(a, c, SwChunkSmem<T>{sm_p, sm_ru, sm_rd, sm_t, sm_u, sm_d}, w, nw, lane, cv, ic, g,
+                                dir_toa, fd_toa, ad, af);
 }
 
 template <typename T>
@@ -781,6 +799,12 @@ int rte_lw(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const T* tau, 
 // Columns up to this depth run the chunked shortwave solver, which needs no workspace.
 constexpr int sw_chunked_max_nlay(bool fp64) { return fp64 ? 128 : 256; }
 
+// Every (column, level, g-point) offset of the shortwave fluxes fits in 31 bits.
+inline bool sw_index32(int ncol, int nlay, int ngpt)
+{
+    return size_t(ncol) * size_t(nlay + 1) * size_t(ngpt) < (size_t(1) << 31);
+}
+
 size_t sw_ws_bytes(int ncol, int nlay, int ngpt, int fp64)
 {
     if (ncol <= 0 || nlay <= 0 || ngpt <= 0 || nlay <= sw_chunked_max_nlay(fp64 != 0)) return 0;
@@ -802,12 +826,15 @@ int rte_sw(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const T* tau, 
         const SwChunkArgs<T> a{ncol, nlay, b->nband, top_at_1, b->d_gpt2band, mu0, inc_dir, alb_dir, alb_dif,
                                inc_dif, flux_up, flux_dn, flux_dir};
         const dim3 grid(ceil_div(ncol, 32), b->ngpt);
+        const bool i32 = sw_index32(ncol, nlay, b->ngpt);
         if constexpr (fp64) {
             sw_solver_chunked<T, 16, 256><<<grid, 32 * ceil_div(nlay, 16), 0, as_stream(stream)>>>(a, tau, ssa, g);
         } else if (nlay <= 128) {
-            sw_solver_chunked<T, 8, 512, 2><<<grid, 32 * ceil_div(nlay, 8), 0, as_stream(stream)>>>(a, tau, ssa, g);
+            const auto kernel = i32 ? sw_solver_chunked<T, 8, 512, 2, true> : sw_solver_chunked<T, 8, 512, 2, false>;
+            kernel<<<grid, 32 * ceil_div(nlay, 8), 0, as_stream(stream)>>>(a, tau, ssa, g);
         } else {
-            sw_solver_chunked<T, 16, 512><<<grid, 32 * ceil_div(nlay, 16), 0, as_stream(stream)>>>(a, tau, ssa, g);
+            const auto kernel = i32 ? sw_solver_chunked<T, 16, 512, 1, true> : sw_solver_chunked<T, 16, 512, 1, false>;
+            kernel<<<grid, 32 * ceil_div(nlay, 16), 0, as_stream(stream)>>>(a, tau, ssa, g);
         }
         RB_LAUNCH("sw_solver_chunked");
         return RRTMGP_B200_OK;

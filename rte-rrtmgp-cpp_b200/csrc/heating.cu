@@ -14,8 +14,12 @@
 // These equal the net-flux divergence of the solvers' recurrences exactly, but every FP32
 // rounding of a level flux enters multiplied by the layer's absorptance, which is small
 // exactly where the layers are thin.  HR = g/cp 86400 sum_g A_g / |Delta p| as
-// heating_rate_kernel.  One thread per (column, layer), lanes over consecutive columns.
+// heating_rate_kernel.  One thread per (column, layer), lanes over consecutive columns; the
+// inputs of g-point g + 1 are loaded while g-point g is computed (in the plain loop every
+// g-point waited for its own loads from memory), with 32-bit offsets (I32) when every
+// (column, level, g-point) offset fits in 31 bits.
 #include <cfloat>
+#include <type_traits>
 
 #include "common.cuh"
 #include "rte_device.cuh"
@@ -45,29 +49,47 @@ __device__ __forceinline__ void lw_layer_terms<double>(double tau, double D, dou
     omt = -expm1(-tau * D);
 }
 
-template <typename T>
+inline bool hr_index32(int ncol, int nlay, int ngpt)
+{
+    return size_t(ncol) * size_t(nlay + 1) * size_t(ngpt) < (size_t(1) << 31);
+}
+
+template <typename T, bool I32>
 __global__ void heating_rate_lw_layers_kernel(int ncol, int nlay, int ngpt, int top_at_1, const T* __restrict__ tau,
                                               const T* __restrict__ lay_src, const T* __restrict__ lev_inc,
                                               const T* __restrict__ lev_dec, const T* __restrict__ up,
                                               const T* __restrict__ dn, const T* __restrict__ plev,
                                               T* __restrict__ hr)
 {
+    using Idx = typename std::conditional<I32, unsigned, size_t>::type;
     const int icol = blockIdx.x * blockDim.x + threadIdx.x;
     const int l = blockIdx.y;
     if (icol >= ncol) return;
-    const size_t ncl = size_t(ncol) * nlay, ncv = size_t(ncol) * (nlay + 1);
-    const size_t cl = icol + size_t(l) * ncol;
+    const Idx ncl = Idx(ncol) * Idx(nlay), ncv = Idx(ncol) * Idx(nlay + 1);
+    const Idx cl = Idx(icol) + Idx(l) * Idx(ncol);
     const int lt = top_at_1 ? l : l + 1, lb = top_at_1 ? l + 1 : l;
     const T* lev_dn = top_at_1 ? lev_inc : lev_dec;
     const T* lev_up = top_at_1 ? lev_dec : lev_inc;
     const T D = T(1.66), pi = pi_value<T>();
+    Idx i = cl, ot = Idx(icol) + Idx(lt) * Idx(ncol), ob = Idx(icol) + Idx(lb) * Idx(ncol);
+    T n_tau = tau[i], n_lay = lay_src[i], n_ldn = lev_dn[i], n_lup = lev_up[i], n_dn = dn[ot], n_up = up[ob];
     double acc = 0.0;
     for (int g = 0; g < ngpt; ++g) {
-        const size_t i = cl + size_t(g) * ncl;
+        const T t = n_tau, ly = n_lay, ldn = n_ldn, lup = n_lup, fdn = n_dn, fup = n_up;
+        if (g + 1 < ngpt) {
+            i += ncl;
+            ot += ncv;
+            ob += ncv;
+            n_tau = tau[i];
+            n_lay = lay_src[i];
+            n_ldn = lev_dn[i];
+            n_lup = lev_up[i];
+            n_dn = dn[ot];
+            n_up = up[ob];
+        }
         T omt, sdn, sup;
-        lw_layer_terms<T>(tau[i], D, lay_src[i], lev_dn[i], lev_up[i], omt, sdn, sup);
-        const size_t ot = icol + size_t(lt) * ncol + size_t(g) * ncv, ob = icol + size_t(lb) * ncol + size_t(g) * ncv;
-        acc += double(omt * (dn[ot] + up[ob]) - pi * (sdn + sup));
+        lw_layer_terms<T>(t, D, ly, ldn, lup, omt, sdn, sup);
+        acc += double(omt * (fdn + fup) - pi * (sdn + sup));
     }
     const double dp = fabs(double(plev[icol + size_t(lb) * ncol]) - double(plev[icol + size_t(lt) * ncol]));
     hr[cl] = T(kG0OverCp * 86400.0 * acc / dp);
@@ -94,28 +116,40 @@ __device__ __forceinline__ void sw_absorptances<double>(double tau, double ssa, 
     adir = 1. - Tn - Rdir - Tdir;
 }
 
-template <typename T>
+template <typename T, bool I32>
 __global__ void heating_rate_sw_layers_kernel(int ncol, int nlay, int ngpt, int top_at_1, const T* __restrict__ tau,
                                               const T* __restrict__ ssa, const T* __restrict__ gasy,
                                               const T* __restrict__ mu0, const T* __restrict__ up,
                                               const T* __restrict__ dn, const T* __restrict__ dir,
                                               const T* __restrict__ plev, T* __restrict__ hr)
 {
+    using Idx = typename std::conditional<I32, unsigned, size_t>::type;
     const int icol = blockIdx.x * blockDim.x + threadIdx.x;
     const int l = blockIdx.y;
     if (icol >= ncol) return;
-    const size_t ncl = size_t(ncol) * nlay, ncv = size_t(ncol) * (nlay + 1);
-    const size_t cl = icol + size_t(l) * ncol;
+    const Idx ncl = Idx(ncol) * Idx(nlay), ncv = Idx(ncol) * Idx(nlay + 1);
+    const Idx cl = Idx(icol) + Idx(l) * Idx(ncol);
     const int lt = top_at_1 ? l : l + 1, lb = top_at_1 ? l + 1 : l;
     const T m0 = mu0[icol];
+    Idx i = cl, ot = Idx(icol) + Idx(lt) * Idx(ncol), ob = Idx(icol) + Idx(lb) * Idx(ncol);
+    T n_tau = tau[i], n_ssa = ssa[i], n_g = gasy[i], n_dir = dir[ot], n_dn = dn[ot], n_up = up[ob];
     double acc = 0.0;
     for (int g = 0; g < ngpt; ++g) {
-        const size_t i = cl + size_t(g) * ncl;
+        const T t = n_tau, w = n_ssa, gy = n_g, fdir = n_dir, fdn = n_dn, fup = n_up;
+        if (g + 1 < ngpt) {
+            i += ncl;
+            ot += ncv;
+            ob += ncv;
+            n_tau = tau[i];
+            n_ssa = ssa[i];
+            n_g = gasy[i];
+            n_dir = dir[ot];
+            n_dn = dn[ot];
+            n_up = up[ob];
+        }
         T adir, adif;
-        sw_absorptances<T>(tau[i], ssa[i], gasy[i], m0, adir, adif);
-        const size_t ot = icol + size_t(lt) * ncol + size_t(g) * ncv, ob = icol + size_t(lb) * ncol + size_t(g) * ncv;
-        const T fdir = dir[ot];
-        acc += double(fdir * adir + ((dn[ot] - fdir) + up[ob]) * adif);
+        sw_absorptances<T>(t, w, gy, m0, adir, adif);
+        acc += double(fdir * adir + ((fdn - fdir) + fup) * adif);
     }
     const double dp = fabs(double(plev[icol + size_t(lb) * ncol]) - double(plev[icol + size_t(lt) * ncol]));
     hr[cl] = T(kG0OverCp * 86400.0 * acc / dp);
@@ -128,8 +162,9 @@ int hr_lw_layers(int ncol, int nlay, int ngpt, int top_at_1, const T* tau, const
     RB_CHECK_ARG(ncol > 0 && nlay > 0 && ngpt > 0, "heating_rate_lw_layers: ncol, nlay and ngpt must be > 0");
     RB_CHECK_ARG(tau && lay && inc && dec && up && dn && plev && hr, "heating_rate_lw_layers: null array");
     const dim3 grid(ceil_div(ncol, 128), nlay);
-    heating_rate_lw_layers_kernel<T><<<grid, 128, 0, as_stream(stream)>>>(ncol, nlay, ngpt, top_at_1, tau, lay, inc,
-                                                                          dec, up, dn, plev, hr);
+    const auto kernel = hr_index32(ncol, nlay, ngpt) ? heating_rate_lw_layers_kernel<T, true>
+                                                     : heating_rate_lw_layers_kernel<T, false>;
+    kernel<<<grid, 128, 0, as_stream(stream)>>>(ncol, nlay, ngpt, top_at_1, tau, lay, inc, dec, up, dn, plev, hr);
     RB_LAUNCH("heating_rate_lw_layers_kernel");
     return RRTMGP_B200_OK;
 }
@@ -141,8 +176,9 @@ int hr_sw_layers(int ncol, int nlay, int ngpt, int top_at_1, const T* tau, const
     RB_CHECK_ARG(ncol > 0 && nlay > 0 && ngpt > 0, "heating_rate_sw_layers: ncol, nlay and ngpt must be > 0");
     RB_CHECK_ARG(tau && ssa && g && mu0 && up && dn && dir && plev && hr, "heating_rate_sw_layers: null array");
     const dim3 grid(ceil_div(ncol, 128), nlay);
-    heating_rate_sw_layers_kernel<T><<<grid, 128, 0, as_stream(stream)>>>(ncol, nlay, ngpt, top_at_1, tau, ssa, g,
-                                                                          mu0, up, dn, dir, plev, hr);
+    const auto kernel = hr_index32(ncol, nlay, ngpt) ? heating_rate_sw_layers_kernel<T, true>
+                                                     : heating_rate_sw_layers_kernel<T, false>;
+    kernel<<<grid, 128, 0, as_stream(stream)>>>(ncol, nlay, ngpt, top_at_1, tau, ssa, g, mu0, up, dn, dir, plev, hr);
     RB_LAUNCH("heating_rate_sw_layers_kernel");
     return RRTMGP_B200_OK;
 }

@@ -589,6 +589,12 @@ def main():
 
         for name, fn in (("gas_optics_lw", t_gas_lw), ("lw_solver", t_lw_solver), ("gas_optics_sw", t_gas_sw),
                          ("sw_solver", t_sw_solver), ("broadband_lw", t_bb_lw)):
+            # untimed launches first: on the fused path these kernels have not run yet in this
+            # process, and a first launch carries their one-time set-up (module load, shared-memory
+            # opt-in, tensor-map encoder lookup)
+            for _ in range(2):
+                fn()
+            torch.cuda.synchronize()
             ms = []
             for _ in range(reps):
                 flush.zero_()
@@ -648,7 +654,7 @@ def main():
                             "peak_source": peak_kind},
                     "kernel_ms": {k: round(v, 4) for k, v in breakdown.items()}}
     else:
-        breakdown = staged_breakdown(3)
+        breakdown = staged_breakdown(10)
         bpc = bytes_per_column(args.nlay)
         dom = max(breakdown, key=breakdown.get)
         achieved = bpc[dom] * args.ncol / (breakdown[dom] * 1e-3) / 1e9
@@ -661,7 +667,7 @@ def main():
     # Per-stage kernels of the class API (FP32), each against its HBM roofline.
     staged_kernels = None
     if args.path == "fused" and rank == 0:
-        sk = staged_breakdown(3)
+        sk = staged_breakdown(10)
         bpc_s = bytes_per_column(args.nlay)
         staged_kernels = {}
         for k, ms in sk.items():

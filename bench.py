@@ -952,7 +952,7 @@ def main():
                         "fp64_forward_columns_per_s": fp64["value"] * world,
                         "fp32_max_flux_err_w_m2": fwd_adj.get("fp32_max_flux_err_w_m2"),
                         "fp32_max_heating_rate_err_k_day": fwd_adj.get("fp32_max_heating_rate_err_k_day"),
-                        "target": ">= 3 (north-star), errors <= 0.05 W/m2 and 0.01 K/day"}
+                        "target": ">= 3x the plain FP64 forward, errors <= 0.05 W/m2 and 0.01 K/day"}
         line = {
             "metric": METRIC, "value": value, "unit": "columns/s", "headline": headline,
             "n_gpus": world, "steps": args.steps,

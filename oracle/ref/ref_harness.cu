@@ -1,7 +1,7 @@
 // ORACLE -- test infrastructure only.
 //
 // C entry points over the reference's own GPU classes (rte-rrtmgp-cpp src_cuda/ +
-// src_kernels_cuda/, compiled from /root/reference by oracle/ref/Makefile into
+// src_kernels_cuda/, compiled from the reference sources by oracle/ref/Makefile into
 // oracle/_ref/libref_rrtmgp_f64.so).  Used once, on the GPU box, by
 // tests/golden/make_ref_golden.py to produce fixtures that pin the FP64 oracle to the
 // reference implementation.  All arrays are host double arrays in the reference layouts;

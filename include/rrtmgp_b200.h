@@ -351,6 +351,17 @@ int rrtmgp_b200_rte_sw_f32(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1
         const float* inc_flux_dir, const float* sfc_alb_dir, const float* sfc_alb_dif,
         const float* inc_flux_dif, float* gpt_flux_up, float* gpt_flux_dn, float* gpt_flux_dir,
         void* workspace, size_t workspace_bytes, void* stream);
+/* rte_sw (FP32) that also returns the flux every layer absorbs (no reference counterpart):
+ * layer_abs (ncol, nlay, ngpt), laid out as tau, receives per g-point
+ * F_dir(top)(1 - Tn - Rdir - Tdir) + (F_dn(top) - F_dir(top) + F_up(bottom))(1 - R - T) with the
+ * solver's own two-stream terms, for rrtmgp_b200_heating_rate_from_layer_abs_f32.  The fluxes
+ * are those of rrtmgp_b200_rte_sw_f32.  Columns of up to 128 layers; deeper ones return
+ * RRTMGP_B200_ERR_UNSUPPORTED (use rte_sw and heating_rate_sw_layers).  No workspace. */
+int rrtmgp_b200_rte_sw_abs_f32(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1,
+        const float* tau, const float* ssa, const float* g, const float* mu0,
+        const float* inc_flux_dir, const float* sfc_alb_dir, const float* sfc_alb_dif,
+        const float* inc_flux_dif, float* gpt_flux_up, float* gpt_flux_dn, float* gpt_flux_dir,
+        float* layer_abs, void* stream);
 int rrtmgp_b200_rte_sw_f64(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1,
         const double* tau, const double* ssa, const double* g, const double* mu0,
         const double* inc_flux_dir, const double* sfc_alb_dir, const double* sfc_alb_dif,
@@ -437,6 +448,12 @@ int rrtmgp_b200_heating_rate_sw_layers_f64(int ncol, int nlay, int ngpt, int top
         const double* tau, const double* ssa, const double* g, const double* mu0,
         const double* gpt_flux_up, const double* gpt_flux_dn, const double* gpt_flux_dir,
         const double* plev, double* heating_rate, void* stream);
+/* Heating rate [K/day] from the per-layer absorbed flux of rrtmgp_b200_rte_sw_abs_f32 (no
+ * reference counterpart): sum over g-points of layer_abs in FP64, times g0 / cp_dry * 86400,
+ * over |p(l+1) - p(l)|; the same quantity as heating_rate_sw_layers without recomputing the
+ * two-stream or re-reading the optical properties and g-point fluxes. */
+int rrtmgp_b200_heating_rate_from_layer_abs_f32(int ncol, int nlay, int ngpt, const float* layer_abs,
+        const float* plev, float* heating_rate, void* stream);
 
 /* ------------------------------------------------------------------------------------ */
 /* Fused column forward (FP32 product path)                                              */

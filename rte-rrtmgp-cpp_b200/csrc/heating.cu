@@ -155,6 +155,47 @@ __global__ void heating_rate_sw_layers_kernel(int ncol, int nlay, int ngpt, int 
     hr[cl] = T(kG0OverCp * 86400.0 * acc / dp);
 }
 
+// Heating rate from the per-(layer, g-point) absorbed flux that rte_sw_abs writes: the sum over
+// g-points in FP64 per (column, layer), over |Delta p|.  The next g-point's row is loaded while
+// the current one is added.
+template <bool I32>
+__global__ void heating_rate_from_layer_abs_kernel(int ncol, int nlay, int ngpt, const float* __restrict__ layer_abs,
+                                                   const float* __restrict__ plev, float* __restrict__ hr)
+{
+    using Idx = typename std::conditional<I32, unsigned, size_t>::type;
+    const int icol = blockIdx.x * blockDim.x + threadIdx.x;
+    const int l = blockIdx.y;
+    if (icol >= ncol) return;
+    const Idx ncl = Idx(ncol) * Idx(nlay);
+    const Idx cl = Idx(icol) + Idx(l) * Idx(ncol);
+    Idx i = cl;
+    float next = layer_abs[i];
+    double acc = 0.0;
+    for (int g = 0; g < ngpt; ++g) {
+        const float v = next;
+        if (g + 1 < ngpt) {
+            i += ncl;
+            next = layer_abs[i];
+        }
+        acc += double(v);
+    }
+    const double dp = fabs(double(plev[icol + size_t(l + 1) * ncol]) - double(plev[icol + size_t(l) * ncol]));
+    hr[cl] = float(kG0OverCp * 86400.0 * acc / dp);
+}
+
+int hr_from_layer_abs(int ncol, int nlay, int ngpt, const float* layer_abs, const float* plev, float* hr,
+                      void* stream)
+{
+    RB_CHECK_ARG(ncol > 0 && nlay > 0 && ngpt > 0, "heating_rate_from_layer_abs: ncol, nlay and ngpt must be > 0");
+    RB_CHECK_ARG(layer_abs && plev && hr, "heating_rate_from_layer_abs: null array");
+    const dim3 grid(ceil_div(ncol, 128), nlay);
+    const auto kernel = hr_index32(ncol, nlay, ngpt) ? heating_rate_from_layer_abs_kernel<true>
+                                                     : heating_rate_from_layer_abs_kernel<false>;
+    kernel<<<grid, 128, 0, as_stream(stream)>>>(ncol, nlay, ngpt, layer_abs, plev, hr);
+    RB_LAUNCH("heating_rate_from_layer_abs_kernel");
+    return RRTMGP_B200_OK;
+}
+
 template <typename T>
 int hr_lw_layers(int ncol, int nlay, int ngpt, int top_at_1, const T* tau, const T* lay, const T* inc, const T* dec,
                  const T* up, const T* dn, const T* plev, T* hr, void* stream)
@@ -206,5 +247,9 @@ int rrtmgp_b200_heating_rate_sw_layers_f64(int ncol, int nlay, int ngpt, int top
         const double* ssa, const double* g, const double* mu0, const double* gpt_flux_up, const double* gpt_flux_dn,
         const double* gpt_flux_dir, const double* plev, double* heating_rate, void* s)
 { return hr_sw_layers<double>(ncol, nlay, ngpt, top_at_1, tau, ssa, g, mu0, gpt_flux_up, gpt_flux_dn, gpt_flux_dir, plev, heating_rate, s); }
+
+int rrtmgp_b200_heating_rate_from_layer_abs_f32(int ncol, int nlay, int ngpt, const float* layer_abs,
+        const float* plev, float* heating_rate, void* s)
+{ return hr_from_layer_abs(ncol, nlay, ngpt, layer_abs, plev, heating_rate, s); }
 
 }  // extern "C"

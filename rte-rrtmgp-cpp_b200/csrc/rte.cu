@@ -484,6 +484,14 @@ __device__ __forceinline__ void sw_layer_coeffs<double>(double tau, double ssa, 
 {
     sw_two_stream<double>(tau, ssa, g, mu0, R, Tt, Rdir, Tdir, Tn);
 }
+// FP32 coefficients together with the layer's diffuse and direct absorptances (1 - R - T and
+// 1 - Tn - Rdir - Tdir in sw_layer_fast's cancellation-free form).
+__device__ __forceinline__ void sw_layer_coeffs_abs(float tau, float ssa, float g, float mu0, float mu0_inv, float& R,
+                                                    float& Tt, float& Rdir, float& Tdir, float& Tn, float& adif,
+                                                    float& adir)
+{
+    fused::sw_layer_fast(tau, ssa, 1.f - ssa, g, mu0, mu0_inv, R, Tt, Rdir, Tdir, Tn, adif, adir);
+}
 
 template <typename T>
 __device__ __forceinline__ T adding_den(T R, T a) { return T(1) / (T(1) - R * a); }
@@ -497,6 +505,7 @@ struct SwChunkArgs {
     const int* gpt2band;
     const T *mu0, *inc_dir, *alb_dir, *alb_dif, *inc_dif;
     T *flux_up, *flux_dn, *flux_dir;
+    T* layer_abs = nullptr;   // ABS solvers: absorbed flux per (layer, g-point), laid out as tau
 };
 
 // Per-thread state of one chunk: its layers' diffuse reflectance and transmittance, direct
@@ -538,11 +547,13 @@ struct SwChunkSmem {
 // adding composites exchanged between the chunks (three barriers), albedo and source at the
 // chunk bottom, and the level outputs.  Threads of columns past ncol take part in the
 // barriers and write nothing.  Idx: the signed type of the output offsets (int when every
-// (column, level, g-point) offset fits in 31 bits).
-template <typename T, int CL, typename Idx>
+// (column, level, g-point) offset fits in 31 bits).  ABS: also the flux every layer absorbs,
+// F_dir(top) adir + (F_dif(top) + F_up(bottom)) adif, with the layer's absorptances read from
+// sm_abs ([2 i] adif, [2 i + 1] adir of chunk layer i, stride blockDim.x, this thread's slot).
+template <typename T, int CL, typename Idx, bool ABS = false>
 __device__ __forceinline__ void sw_chunk_finish(const SwChunkArgs<T>& a, SwChunk<T, CL>& c, const SwChunkSmem<T>& sm,
                                                 int w, int nw, int lane, bool cv, int ic, int g, T dir_toa, T fd_toa,
-                                                T ad, T af)
+                                                T ad, T af, const T* sm_abs = nullptr)
 {
     const int ncol = a.ncol, nlay = a.nlay;
     const int j0 = w * CL;
@@ -615,18 +626,43 @@ __device__ __forceinline__ void sw_chunk_finish(const SwChunkArgs<T>& a, SwChunk
     T* const dn = a.flux_dn;
     T* const dr = a.flux_dir;
     T fd = fd_in;
+    if constexpr (!ABS) {
 #pragma unroll
-    for (int i = 0; i < CL; ++i) {
-        const T a_n = (i + 1 < CL) ? vA[i + 1] : alb_in;
-        const T s_n = (i + 1 < CL) ? c.vSu[i + 1] : src_in;
-        if (j0 + i < nlay) {
-            const T dir = dtop * c.vP[i];
-            up[o0 + i * step] = fd * vA[i] + c.vSu[i];
-            dn[o0 + i * step] = fd + dir;
-            dr[o0 + i * step] = dir;
+        for (int i = 0; i < CL; ++i) {
+            const T a_n = (i + 1 < CL) ? vA[i + 1] : alb_in;
+            const T s_n = (i + 1 < CL) ? c.vSu[i + 1] : src_in;
+            if (j0 + i < nlay) {
+                const T dir = dtop * c.vP[i];
+                up[o0 + i * step] = fd * vA[i] + c.vSu[i];
+                dn[o0 + i * step] = fd + dir;
+                dr[o0 + i * step] = dir;
+            }
+            const T den = adding_den(c.vR[i], a_n);
+            fd = (c.vT[i] * fd + c.vR[i] * s_n + c.vSd[i]) * den;
         }
-        const T den = adding_den(c.vR[i], a_n);
-        fd = (c.vT[i] * fd + c.vR[i] * s_n + c.vSd[i]) * den;
+    } else {
+        const Idx lstep = a.top_at_1 ? Idx(ncol) : -Idx(ncol);
+        const Idx l0 = Idx(ic) + Idx(g) * Idx(ncol) * Idx(nlay) +
+                       (a.top_at_1 ? Idx(j0) * Idx(ncol) : Idx(nlay - 1 - j0) * Idx(ncol));   // layer j0
+#pragma unroll
+        for (int i = 0; i < CL; ++i) {
+            const T a_n = (i + 1 < CL) ? vA[i + 1] : alb_in;
+            const T s_n = (i + 1 < CL) ? c.vSu[i + 1] : src_in;
+            const T dir = dtop * c.vP[i];
+            if (j0 + i < nlay) {
+                up[o0 + i * step] = fd * vA[i] + c.vSu[i];
+                dn[o0 + i * step] = fd + dir;
+                dr[o0 + i * step] = dir;
+            }
+            const T den = adding_den(c.vR[i], a_n);
+            const T fdb = (c.vT[i] * fd + c.vR[i] * s_n + c.vSd[i]) * den;   // diffuse down at the layer bottom
+            if (j0 + i < nlay) {
+                const T adif = sm_abs[(2 * i) * blockDim.x + threadIdx.x];
+                const T adir = sm_abs[(2 * i + 1) * blockDim.x + threadIdx.x];
+                a.layer_abs[l0 + i * lstep] = dir * adir + (fd + fdb * a_n + s_n) * adif;
+            }
+            fd = fdb;
+        }
     }
     if (j0 <= nlay - 1 && nlay - 1 < j0 + CL) {
         // fd is now at the chunk bottom (padding layers are the identity): the surface level
@@ -637,14 +673,17 @@ __device__ __forceinline__ void sw_chunk_finish(const SwChunkArgs<T>& a, SwChunk
     }
 }
 
-// I32: every (column, level, g-point) offset fits in 31 bits (sw_index32).
-template <typename T, int CL, int MAXT, int MINB = 1, bool I32 = false>
+// I32: every (column, level, g-point) offset fits in 31 bits (sw_index32).  ABS (FP32): also
+// the flux every layer absorbs per g-point (a.layer_abs); the layers' absorptances wait in
+// shared memory (2 CL values per thread: kept in registers they spilled at the register cap).
+template <typename T, int CL, int MAXT, int MINB = 1, bool I32 = false, bool ABS = false>
 __global__ void __launch_bounds__(MAXT, MINB) sw_solver_chunked(const SwChunkArgs<T> a, const T* __restrict__ tau,
                                                                 const T* __restrict__ ssa, const T* __restrict__ gasy)
 {
     using Idx = typename std::conditional<I32, int, ptrdiff_t>::type;
     __shared__ T sm_p[16 * 32];                                      // direct-beam product per chunk
     __shared__ T sm_ru[16 * 32], sm_rd[16 * 32], sm_t[16 * 32], sm_u[16 * 32], sm_d[16 * 32];   // composites
+    __shared__ T sm_abs[ABS ? 2 * CL * MAXT : 1];                    // [2 CL][thread] absorptances
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int ncol = a.ncol, nlay = a.nlay;
     const int icol = blockIdx.x * 32 + lane;
@@ -682,11 +721,18 @@ __global__ void __launch_bounds__(MAXT, MINB) sw_solver_chunked(const SwChunkArg
             ng = gasy[x];
         }
         T R = T(0), Tt = T(1), Rdir = T(0), Tdir = T(0), Tn = T(1);
-        if (cv && j < nlay) sw_layer_coeffs<T>(tj, sj, gj, m0, m0_inv, R, Tt, Rdir, Tdir, Tn);
+        if constexpr (!ABS) {
+            if (cv && j < nlay) sw_layer_coeffs<T>(tj, sj, gj, m0, m0_inv, R, Tt, Rdir, Tdir, Tn);
+        } else {
+            T adif = T(0), adir = T(0);
+            if (cv && j < nlay) sw_layer_coeffs_abs(tj, sj, gj, m0, m0_inv, R, Tt, Rdir, Tdir, Tn, adif, adir);
+            sm_abs[(2 * i) * blockDim.x + threadIdx.x] = adif;
+            sm_abs[(2 * i + 1) * blockDim.x + threadIdx.x] = adir;
+        }
         c.add_layer(i, R, Tt, Rdir, Tdir, Tn);
     }
-    sw_chunk_finish<T, CL, Idx>(a, c, SwChunkSmem<T>{sm_p, sm_ru, sm_rd, sm_t, sm_u, sm_d}, w, nw, lane, cv, ic, g,
-                                dir_toa, fd_toa, ad, af);
+    sw_chunk_finish<T, CL, Idx, ABS>(a, c, SwChunkSmem<T>{sm_p, sm_ru, sm_rd, sm_t, sm_u, sm_d}, w, nw, lane, cv, ic,
+                                     g, dir_toa, fd_toa, ad, af, sm_abs);
 }
 
 template <typename T>
@@ -850,6 +896,31 @@ int rte_sw(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const T* tau, 
     return RRTMGP_B200_OK;
 }
 
+// rte_sw (FP32, chunked solver, nlay <= 128) that also writes the flux every layer absorbs per
+// g-point, for heating rates summed from it (heating.cu: heating_rate_from_layer_abs) instead
+// of recomputing the two-stream from tau, ssa and g and re-reading six g-point rows.
+int rte_sw_abs(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const float* tau, const float* ssa,
+               const float* g, const float* mu0, const float* inc_dir, const float* alb_dir, const float* alb_dif,
+               const float* inc_dif, float* flux_up, float* flux_dn, float* flux_dir, float* layer_abs, void* stream)
+{
+    RB_CHECK_ARG(b, "rte_sw_abs: null bands");
+    RB_CHECK_ARG(ncol > 0 && nlay > 0, "rte_sw_abs: ncol and nlay must be > 0");
+    RB_CHECK_ARG(tau && ssa && g && mu0 && inc_dir && alb_dir && alb_dif && flux_up && flux_dn && flux_dir &&
+                 layer_abs, "rte_sw_abs: null array");
+    if (nlay > 128)
+        return fail(RRTMGP_B200_ERR_UNSUPPORTED,
+                    "rte_sw_abs: more than 128 layers (use rte_sw and heating_rate_sw_layers)");
+    SwChunkArgs<float> a{ncol, nlay, b->nband, top_at_1, b->d_gpt2band, mu0, inc_dir, alb_dir, alb_dif,
+                         inc_dif, flux_up, flux_dn, flux_dir};
+    a.layer_abs = layer_abs;
+    const dim3 grid(ceil_div(ncol, 32), b->ngpt);
+    const auto kernel = sw_index32(ncol, nlay, b->ngpt) ? sw_solver_chunked<float, 8, 512, 2, true, true>
+                                                        : sw_solver_chunked<float, 8, 512, 2, false, true>;
+    kernel<<<grid, 32 * ceil_div(nlay, 8), 0, as_stream(stream)>>>(a, tau, ssa, g);
+    RB_LAUNCH("sw_solver_chunked (absorbed flux)");
+    return RRTMGP_B200_OK;
+}
+
 // Shortwave solver scratch for callers that cannot allocate device memory themselves.
 // Lives in this file-scope device array: RRTMGP_B200_SW_STATIC_SCRATCH_MAX_ELEMS entries per
 // workspace slice, four slices, i.e. 16 MiB that every GPU which loads this library keeps
@@ -949,6 +1020,11 @@ int rrtmgp_b200_rte_sw_f32(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1
         const float* sfc_alb_dif, const float* inc_flux_dif, float* up, float* dn, float* dir, void* ws,
         size_t ws_bytes, void* s)
 { return rte_sw<float>(b, ncol, nlay, top_at_1, tau, ssa, g, mu0, inc_flux_dir, sfc_alb_dir, sfc_alb_dif, inc_flux_dif, up, dn, dir, ws, ws_bytes, s); }
+int rrtmgp_b200_rte_sw_abs_f32(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const float* tau,
+        const float* ssa, const float* g, const float* mu0, const float* inc_flux_dir, const float* sfc_alb_dir,
+        const float* sfc_alb_dif, const float* inc_flux_dif, float* up, float* dn, float* dir, float* layer_abs,
+        void* s)
+{ return rte_sw_abs(b, ncol, nlay, top_at_1, tau, ssa, g, mu0, inc_flux_dir, sfc_alb_dir, sfc_alb_dif, inc_flux_dif, up, dn, dir, layer_abs, s); }
 int rrtmgp_b200_rte_sw_f64(rrtmgp_b200_bands b, int ncol, int nlay, int top_at_1, const double* tau,
         const double* ssa, const double* g, const double* mu0, const double* inc_flux_dir,
         const double* sfc_alb_dir, const double* sfc_alb_dif, const double* inc_flux_dif, double* up,

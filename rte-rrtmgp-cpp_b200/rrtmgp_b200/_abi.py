@@ -247,6 +247,8 @@ _SIGS = {
                                                     _P, _P, _P, _P,
                                                     _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
                                                     _P, _P, _P, _P, _P, _P]),
+    "rrtmgp_b200_rte_sw_abs_f32": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "rrtmgp_b200_heating_rate_from_layer_abs_f32": (_I, [_I, _I, _I, _P, _P, _P, _P]),
     "rrtmgp_b200_batch_create": (_I, [_P, _P, _P, _P, _I, _P, _I, C.POINTER(_P)]),
     "rrtmgp_b200_batch_destroy": (_I, [_P]),
     "rrtmgp_b200_batch_run": (_I, [_P, _I, _P]),

@@ -53,6 +53,9 @@ class Radiation_solver:
             for k in ("gpt_up", "gpt_dn", "gpt_dir"):
                 b[k] = torch.empty((ng, nlev, ncol), dtype=dt, device=dev)
             b["ws"] = api.Rte_sw.workspace(ncol, nlay, ng, like).clone()
+            if dt == torch.float32 and nlay <= 128:
+                # absorbed flux per (layer, g-point) for the heating rates (rte_sw_abs)
+                b["gpt_abs"] = torch.empty((ng, nlay, ncol), dtype=dt, device=dev)
         for k in ("flux_up", "flux_dn", "flux_net", "flux_dn_dir"):
             b[k] = torch.empty((nlev, ncol), dtype=dt, device=dev)
         b["heating_rate"] = torch.empty((nlay, ncol), dtype=dt, device=dev)
@@ -140,14 +143,24 @@ class Radiation_solver:
                 self.ksw.bands.handle, ncol, nlay, P(b["tau"]), P(b["ssa"]), P(b["g"]), P(a["tau"]),
                 P(a["ssa"]), P(a["g"]), nb, s))
         import ctypes as C
-        _abi.check(getattr(lib, "rrtmgp_b200_rte_sw" + sfx)(
-            self.ksw.bands.handle, ncol, nlay, int(top_at_1), P(b["tau"]), P(b["ssa"]), P(b["g"]), P(atm["mu0"]),
-            P(b["toa_src"]), P(atm["sfc_alb_dir"]), P(atm["sfc_alb_dif"]), None, P(b["gpt_up"]), P(b["gpt_dn"]),
-            P(b["gpt_dir"]), C.c_void_p(b["ws"].data_ptr()), C.c_size_t(b["ws"].numel()), s))
+        if "gpt_abs" in b:
+            # FP32 up to 128 layers: the solver also writes the flux each layer absorbs per g-point
+            _abi.check(lib.rrtmgp_b200_rte_sw_abs_f32(
+                self.ksw.bands.handle, ncol, nlay, int(top_at_1), P(b["tau"]), P(b["ssa"]), P(b["g"]),
+                P(atm["mu0"]), P(b["toa_src"]), P(atm["sfc_alb_dir"]), P(atm["sfc_alb_dif"]), None, P(b["gpt_up"]),
+                P(b["gpt_dn"]), P(b["gpt_dir"]), P(b["gpt_abs"]), s))
+        else:
+            _abi.check(getattr(lib, "rrtmgp_b200_rte_sw" + sfx)(
+                self.ksw.bands.handle, ncol, nlay, int(top_at_1), P(b["tau"]), P(b["ssa"]), P(b["g"]), P(atm["mu0"]),
+                P(b["toa_src"]), P(atm["sfc_alb_dir"]), P(atm["sfc_alb_dif"]), None, P(b["gpt_up"]), P(b["gpt_dn"]),
+                P(b["gpt_dir"]), C.c_void_p(b["ws"].data_ptr()), C.c_size_t(b["ws"].numel()), s))
         _abi.check(getattr(lib, "rrtmgp_b200_fluxes_broadband" + sfx)(
             ncol, nlay + 1, self.ksw.get_ngpt(), P(b["gpt_up"]), P(b["gpt_dn"]), P(b["gpt_dir"]), P(b["flux_up"]),
             P(b["flux_dn"]), P(b["flux_dn_dir"]), P(b["flux_net"]), s))
-        if play.dtype == torch.float32:   # as solve_lw
+        if "gpt_abs" in b:
+            _abi.check(lib.rrtmgp_b200_heating_rate_from_layer_abs_f32(
+                ncol, nlay, self.ksw.get_ngpt(), P(b["gpt_abs"]), P(atm["plev"]), P(b["heating_rate"]), s))
+        elif play.dtype == torch.float32:   # as solve_lw
             _abi.check(lib.rrtmgp_b200_heating_rate_sw_layers_f32(
                 ncol, nlay, self.ksw.get_ngpt(), int(top_at_1), P(b["tau"]), P(b["ssa"]), P(b["g"]), P(atm["mu0"]),
                 P(b["gpt_up"]), P(b["gpt_dn"]), P(b["gpt_dir"]), P(atm["plev"]), P(b["heating_rate"]), s))

@@ -554,3 +554,51 @@ def test_missing_gas_is_reported(api, tables, gpu):
         kd.gas_optics_sw(T(atm["play"], torch.float64, gpu), T(atm["plev"], torch.float64, gpu),
                          T(atm["tlay"], torch.float64, gpu), g)
     assert e.value.status == ERR_MISSING_GAS
+
+
+@pytest.mark.parametrize("top_at_1", [True, False])
+@pytest.mark.parametrize("ncol,nlay", [(37, 23), (300, 128), (5, 2)])
+def test_rte_sw_absorbed_flux_heating_rate(api, tables, gpu, top_at_1, ncol, nlay):
+    """rte_sw_abs returns rte_sw's fluxes plus each layer's absorbed flux per g-point, and the
+    heating rate summed from it equals heating_rate_sw_layers' (which recomputes the two-stream
+    from tau, ssa and g).  FP32: the fluxes within 2e-5 relative (the two kernel instances round
+    differently in the last bits), the heating rates within 2e-3 K/day + 1e-4 relative.  Deeper
+    than 128 layers is refused with RRTMGP_B200_ERR_UNSUPPORTED before any launch."""
+    import torch
+    from rrtmgp_b200 import _abi
+    dt = torch.float32
+    lib = _abi.load()
+    P, st = api._ptr, api._stream()
+    atm = S.make_atmosphere(ncol, nlay, seed=41, clouds=False, top_at_1=top_at_1)
+    kd = api.Gas_optics_rrtmgp(tables["sw"], S.ATM_GASES)
+    go = kd.gas_optics_sw(T(atm["play"], dt, gpu), T(atm["plev"], dt, gpu), T(atm["tlay"], dt, gpu),
+                          gas_dict(atm, dt, gpu))
+    mu0, plev = T(atm["mu0"], dt, gpu), T(atm["plev"], dt, gpu)
+    alb_dir, alb_dif = T(atm["sfc_alb_dir"], dt, gpu), T(atm["sfc_alb_dif"], dt, gpu)
+    up, dn, dr = api.Rte_sw.rte_sw(kd.bands, go["tau"], go["ssa"], go["g"], top_at_1, mu0, go["toa_src"],
+                                   alb_dir, alb_dif)
+    ng = go["tau"].shape[0]
+    hr_ref = torch.empty((nlay, ncol), dtype=dt, device=gpu)
+    _abi.check(lib.rrtmgp_b200_heating_rate_sw_layers_f32(
+        ncol, nlay, ng, int(top_at_1), P(go["tau"]), P(go["ssa"]), P(go["g"]), P(mu0), P(up), P(dn), P(dr),
+        P(plev), P(hr_ref), st))
+    up2, dn2, dr2 = (torch.empty_like(up) for _ in range(3))
+    layer_abs = torch.empty_like(go["tau"])
+    hr = torch.empty((nlay, ncol), dtype=dt, device=gpu)
+    _abi.check(lib.rrtmgp_b200_rte_sw_abs_f32(
+        kd.bands.handle, ncol, nlay, int(top_at_1), P(go["tau"]), P(go["ssa"]), P(go["g"]), P(mu0),
+        P(go["toa_src"]), P(alb_dir), P(alb_dif), None, P(up2), P(dn2), P(dr2), P(layer_abs), st))
+    _abi.check(lib.rrtmgp_b200_heating_rate_from_layer_abs_f32(ncol, nlay, ng, P(layer_abs), P(plev), P(hr), st))
+    torch.cuda.synchronize()
+    for name, a, b in (("flux_up", up2, up), ("flux_dn", dn2, dn), ("flux_dir", dr2, dr)):
+        cmp(name, N(a), N(b), "f32", floor_frac=1e-6, rtol=2e-5)
+    err = np.abs(N(hr) - N(hr_ref))
+    bound = 2e-3 + 1e-4 * np.abs(N(hr_ref))
+    assert np.all(err <= bound), f"heating rate: max diff {err.max():.3e} K/day"
+    if nlay == 128:
+        t = T(np.zeros((ng, 129, ncol)), dt, gpu)
+        f = T(np.zeros((ng, 130, ncol)), dt, gpu)
+        status = lib.rrtmgp_b200_rte_sw_abs_f32(
+            kd.bands.handle, ncol, 129, int(top_at_1), P(t), P(t), P(t), P(mu0), P(go["toa_src"]), P(alb_dir),
+            P(alb_dif), None, P(f), P(f), P(f), P(t), st)
+        assert status == _abi.ERR_UNSUPPORTED and b"128 layers" in lib.rrtmgp_b200_last_error()

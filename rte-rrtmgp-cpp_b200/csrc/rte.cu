@@ -10,7 +10,9 @@
 //     plus the output arrays themselves.
 // Every layer read and level write is a coalesced row either way.  The shortwave workspace is
 // needed only by the second kind.  The FP32 longwave solver up to 192 layers stages its layer
-// inputs through shared memory with TMA tile copies (lw_solver_tma).
+// inputs through shared memory with TMA tile copies (lw_solver_tma).  The FP32 shortwave solver
+// up to 128 layers can also write the flux each layer absorbs per g-point (rte_sw_abs), from
+// which heating.cu forms heating rates without a second pass over the g-point arrays.
 #include <algorithm>
 #include <cfloat>
 #include <mutex>

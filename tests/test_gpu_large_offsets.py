@@ -1,11 +1,11 @@
 """Staged FP32 kernels on a grid whose (column, level, g-point) offsets pass 2^31.
 
-The packed gas optics, the chunked shortwave solver and the per-layer heating-rate kernels
-use 32-bit offsets when every offset of a call fits in 31 bits and 64-bit offsets otherwise.
-Every other test runs the 32-bit instances; here a 1024-column atmosphere is tiled 586 times
-along the columns (600,064 columns of 16 layers, offsets up to 2.46e9), so the same kernels run
-their 64-bit instances, and every tiled block, the last one included, must reproduce the
-1024-column call.  About 60 GB of device memory at the peak; skipped when less is free.
+The packed gas optics, the chunked shortwave solver (with and without its absorbed-flux
+output) and the heating-rate kernels use 32-bit offsets when every offset of a call fits in
+31 bits and 64-bit offsets otherwise.  Every other test runs the 32-bit instances; here a
+1024-column atmosphere is tiled 586 times along the columns (600,064 columns of 16 layers,
+offsets up to 2.46e9), so the same kernels run their 64-bit instances, and every tiled block,
+the last one included, must reproduce the 1024-column call.  About 63 GB of device memory at the peak; skipped when less is free.
 """
 
 import numpy as np
@@ -98,7 +98,7 @@ def test_shortwave_offsets_past_2_31(tables, gpu, small_atm):
     import torch
     from rrtmgp_b200 import _abi, api
     assert NC * REPS * NLAY * 224 >= 2**31
-    _need_memory(gpu, 64)
+    _need_memory(gpu, 72)
     kd = api.Gas_optics_rrtmgp(tables["sw"], S.ATM_GASES)
     lib = _abi.load()
     top = bool(small_atm["play"][0, 0] < small_atm["play"][-1, 0])
@@ -112,7 +112,17 @@ def test_shortwave_offsets_past_2_31(tables, gpu, small_atm):
             ncol, NLAY, go["tau"].shape[0], int(top), api._ptr(go["tau"]), api._ptr(go["ssa"]),
             api._ptr(go["g"]), api._ptr(a["mu0"]), api._ptr(up), api._ptr(dn), api._ptr(dr),
             api._ptr(a["plev"]), api._ptr(hr), api._stream()))
-        return go, up, dn, dr, hr
+        # the solver that also writes each layer's absorbed flux (its fluxes, within FP32 rounding
+        # of rte_sw's, overwrite those), and the heating rate summed from it
+        layer_abs = torch.empty_like(go["tau"])
+        hr2 = torch.empty((NLAY, ncol), dtype=torch.float32, device=gpu)
+        _abi.check(lib.rrtmgp_b200_rte_sw_abs_f32(
+            kd.bands.handle, ncol, NLAY, int(top), api._ptr(go["tau"]), api._ptr(go["ssa"]), api._ptr(go["g"]),
+            api._ptr(a["mu0"]), api._ptr(go["toa_src"]), api._ptr(a["sfc_alb_dir"]), api._ptr(a["sfc_alb_dif"]),
+            None, api._ptr(up), api._ptr(dn), api._ptr(dr), api._ptr(layer_abs), api._stream()))
+        _abi.check(lib.rrtmgp_b200_heating_rate_from_layer_abs_f32(
+            ncol, NLAY, go["tau"].shape[0], api._ptr(layer_abs), api._ptr(a["plev"]), api._ptr(hr2), api._stream()))
+        return go, up, dn, dr, hr, layer_abs, hr2
 
     ref = run(small_atm, NC)
     big = run(_tile(small_atm), NC * REPS)
@@ -123,5 +133,7 @@ def test_shortwave_offsets_past_2_31(tables, gpu, small_atm):
     _blocks(big[2], ref[2], "rte_sw flux_dn")
     _blocks(big[3], ref[3], "rte_sw flux_dir")
     _blocks(big[4], ref[4], "heating_rate_sw_layers")
+    _blocks(big[5], ref[5], "rte_sw_abs layer_abs")
+    _blocks(big[6], ref[6], "heating_rate_from_layer_abs")
     del big
     torch.cuda.empty_cache()
